@@ -1,0 +1,397 @@
+#!/usr/bin/env python
+"""Benchmark of the in-HBM hot path: PageRank + SSSP on a seeded R-MAT graph.
+
+Workload (default): R-MAT scale 24, edge factor 16 (a,b,c = .57,.19,.19,
+uint32 weights uniform [1,63], self-loops/duplicates removed), graph
+resident in HBM.  One step = PageRank (damping 0.85) to L1 change <= 1e-6
+(max 100 iterations) + SSSP from 8 seeded sources, one at a time.
+
+Metric: GTEPS = traversed edges / s, with E per PageRank iteration and E per
+SSSP source (Graph500 convention), summed over all ranks (weak scaling:
+every rank solves its own replica; the path has no cross-rank exchange).
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
+
+Prints ONE JSON line (rank 0).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "PR/SSSP GTEPS (in/out-of-HBM) + served queries/s & p99 vs one-at-a-time"
+UNIT = "GTEPS"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--scale", type=int, default=24)
+    ap.add_argument("--edge-factor", type=int, default=16)
+    ap.add_argument("--sources", type=int, default=8)
+    ap.add_argument("--seed", type=int, default=20241203)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def load_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# --------------------------------------------------------------------------
+# clocks sampled during the timed region
+# --------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.out = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.out.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.out:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() in ("active", "1"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------------------------
+# distributed plumbing (one process per GPU; replicas, no data-path exchange)
+# --------------------------------------------------------------------------
+def dist_setup(gpus: int):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if gpus > 1 and world == 1:
+        raise SystemExit("--gpus > 1 needs torchrun (one process per GPU)")
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return rank, world, local, pg
+
+
+def barrier(pg):
+    import torch
+
+    if pg is not None:
+        pg.barrier()
+    torch.cuda.synchronize()
+
+
+def max_over_ranks(pg, x: float) -> float:
+    import torch
+
+    if pg is None:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+# --------------------------------------------------------------------------
+# CPU baseline: the reference's own CPU solvers on a bounded sample
+# --------------------------------------------------------------------------
+def cpu_sample(off, cols, w_f32, source):
+    """One PageRank iteration and one SSSP round of the reference's own
+    pagerank_cpu / sssp_cpu (each including its incoming-CSR build) on the
+    full graph.  Returns (edges traversed, seconds, kind)."""
+    from oracle.bindings import Oracle, Reference
+
+    E = int(cols.shape[0])
+    if Reference.available():
+        ref, kind = Reference(), "reference"
+        t0 = time.perf_counter()
+        ref.pagerank_cpu(off, cols, 0.85, 1e-6, 1)
+        ref.sssp_cpu(off, cols, w_f32, int(source), 1)
+    else:
+        ref, kind = Oracle(), "port"
+        t0 = time.perf_counter()
+        ref.pagerank_f32(off, cols, 0.85, 1e-6, 1)
+        ref.sssp(off, cols, w_f32, int(source), 1)
+    return 2 * E, time.perf_counter() - t0, kind
+
+
+def host_graph_from_device(dcsr):
+    """Pinned host copy of a device-generated CSR (setup, not timed)."""
+    import torch
+
+    V, E = dcsr.num_vertices, dcsr.num_edges
+    b = dcsr.buffers
+    off = torch.empty(V + 1, dtype=torch.int64, pin_memory=True)
+    cols = torch.empty(E, dtype=torch.int32, pin_memory=True)
+    w = torch.empty(E, dtype=torch.int32, pin_memory=True)
+    cudart = torch.cuda.cudart()
+    torch.cuda.synchronize()
+    for dst, src, n in [(off, b.row_offsets, (V + 1) * 8), (cols, b.column_indices, E * 4), (w, b.weights, E * 4)]:
+        assert cudart.cudaMemcpy(dst.data_ptr(), C.cast(src, C.c_void_p).value, n, 2) == 0
+    return off, cols, w
+
+
+# --------------------------------------------------------------------------
+def run_reference_arm(args, rank, pg):
+    """--impl reference: the reference's CPU implementation of the path on
+    this host's cores, same workload, metric and unit (rank 0 only)."""
+    if rank != 0:
+        return
+    import hytgraph_b200 as hyt
+
+    g = hyt.rmat(args.scale, args.edge_factor, args.seed) if args.scale <= 20 else None
+    if g is None:
+        d = hyt.rmat(args.scale, args.edge_factor, args.seed, device=True)
+        off_t, cols_t, w_t = host_graph_from_device(d)
+        d.free()
+        off = off_t.numpy().view(np.uint64)
+        cols = cols_t.numpy().view(np.uint32)
+        w = w_t.numpy().view(np.uint32)
+    else:
+        off, cols, w = g.row_offsets, g.column_indices, g.weights
+    w_f32 = w.astype(np.float32)
+    src = int(hyt.pick_sources(off, args.seed, 1)[0])
+    kind = "port"
+    times, edges = [], 0
+    for i in range(args.warmup + args.steps):
+        e, t, kind = cpu_sample(off, cols, w_f32, src)
+        if i >= args.warmup:
+            times.append(t)
+            edges += e
+    total = sum(times)
+    value = edges / total / 1e9
+    sample = (f"per step: 1 PageRank iteration + 1 SSSP round of the reference's pagerank_cpu/sssp_cpu "
+              f"(each incl. its incoming-CSR build) on the full R-MAT s{args.scale} ef{args.edge_factor} graph; "
+              f"E per iteration/round counted")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/u32",
+            "data": "synthetic", "config": workload_config(args, int(off.shape[0] - 1), int(cols.shape[0])),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(args, V, E):
+    return {"workload": f"in-HBM R-MAT scale {args.scale} edge factor {args.edge_factor}: PageRank to L1<=1e-6 "
+                        f"+ SSSP from {args.sources} seeded sources",
+            "scale": args.scale, "edge_factor": args.edge_factor, "vertices": V, "edges": E,
+            "sources": args.sources, "rmat_abc": [0.57, 0.19, 0.19], "weights": "uint32 uniform [1,63]",
+            "seed": args.seed, "parallelism": f"replicas x{args.gpus}",
+            "l2": "inputs larger than L2 (CSR + CSC + weights > 4 GB vs 126 MB L2)"}
+
+
+def main():
+    args = parse_args()
+    import torch
+
+    rank, world, local, pg = dist_setup(args.gpus)
+    if args.impl == "reference":
+        run_reference_arm(args, rank, pg)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
+
+    import hytgraph_b200 as hyt
+    from hytgraph_b200 import capi
+
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+    peak_gbs, peak_kind = load_peaks()
+
+    # ---- setup (untimed): generate on the GPU, build the resident graph ----
+    dcsr = hyt.rmat(args.scale, args.edge_factor, args.seed, device=True)
+    V, E = dcsr.num_vertices, dcsr.num_edges
+    off_h, cols_h, w_h = host_graph_from_device(dcsr)
+    off_np = off_h.numpy().view(np.uint64)
+    sources = [int(s) for s in hyt.pick_sources(off_np, args.seed, args.sources)]
+    graph = hyt.Graph(dcsr, stream=sptr)
+    dcsr.free()
+    ranks_out = torch.empty(V, dtype=torch.float32, device="cuda")
+    dist_out = torch.empty(V, dtype=torch.int32, device="cuda")
+
+    def step(collect):
+        _, st = graph.pagerank(out=ranks_out, stream=sptr)
+        collect["pr"].append(st)
+        for s in sources:
+            _, ss = graph.sssp(s, out=dist_out, stream=sptr)
+            collect["sssp"].append(ss)
+
+    warm = {"pr": [], "sssp": []}
+    for _ in range(args.warmup):
+        step(warm)
+
+    # ---- timed region: device-resident inputs ----
+    clocks = ClockSampler(local)
+    clocks.start()
+    timed = {"pr": [], "sssp": []}
+    barrier(pg)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step(timed)
+    ev1.record(stream)
+    barrier(pg)
+    clk = clocks.stop()
+    ms_local = ev0.elapsed_time(ev1)
+    ms = max_over_ranks(pg, ms_local)
+    pr_it = sum(s["iterations"] for s in timed["pr"])
+    traversed = E * pr_it + E * len(timed["sssp"])
+    value = traversed * world / (ms / 1e3) / 1e9
+
+    # roofline: dominant kernel of the step (PageRank iteration vs SSSP rounds)
+    pr_ms = sum(s["device_ms"] for s in timed["pr"])
+    ss_ms = sum(s["device_ms"] for s in timed["sssp"])
+    pr_bytes = sum(s["algorithmic_bytes"] for s in timed["pr"])
+    ss_bytes = sum(s["algorithmic_bytes"] for s in timed["sssp"])
+    pr_launch_ms = pr_ms / max(pr_it, 1)  # whole solve / iterations: includes init + loop overhead
+    pr_gbs = (pr_bytes / max(pr_it, 1)) / (pr_launch_ms / 1e3) / 1e9
+    ss_gbs = ss_bytes / (ss_ms / 1e3) / 1e9
+    # pure kernel time of one PageRank iteration (per-launch events), same inputs
+    _, prof = graph.pagerank(out=ranks_out, stream=sptr, flags=capi.HYT_RUN_PROFILE)
+    kern_ms = prof["kernel_ms"] / max(prof["kernel_launches"], 1)
+    dominant = "pr_iterate_kernel" if pr_ms >= ss_ms else "sssp_expand_kernel+sssp_hub_kernel"
+    if pr_ms >= ss_ms:
+        roof = {"kernel": dominant, "bound": "hbm", "achieved": pr_gbs, "peak": peak_gbs, "unit": "GB/s",
+                "frac": pr_gbs / peak_gbs, "traffic": None, "peak_kind": peak_kind,
+                "algorithmic_bytes_per_launch": pr_bytes / max(pr_it, 1), "avg_launch_ms": pr_launch_ms,
+                "kernel_only_launch_ms": kern_ms,
+                "kernel_only_frac": (pr_bytes / max(pr_it, 1)) / (kern_ms / 1e3) / 1e9 / peak_gbs}
+    else:
+        roof = {"kernel": dominant, "bound": "hbm", "achieved": ss_gbs, "peak": peak_gbs, "unit": "GB/s",
+                "frac": ss_gbs / peak_gbs, "traffic": None, "peak_kind": peak_kind}
+    traffic_file = ROOT / "profiles" / "traffic.json"
+    if traffic_file.exists():
+        tr = json.loads(traffic_file.read_text()).get(f"s{args.scale}_ef{args.edge_factor}", {})
+        roof["traffic"] = tr.get(roof["kernel"].split("+")[0])
+
+    launches = sum(s["total_launches"] for s in timed["pr"]) + sum(s["total_launches"] for s in timed["sssp"])
+
+    # ---- e2e: the C-ABI with HOST (pinned) buffers, copies inside the timed region ----
+    ranks_h = torch.empty(V, dtype=torch.float32, pin_memory=True)
+    dist_h = torch.empty(V, dtype=torch.int32, pin_memory=True)
+    csr_h = hyt.CSR(off_np, cols_h.numpy().view(np.uint32), w_h.numpy().view(np.uint32))
+    graph.close()
+    torch.cuda.empty_cache()
+
+    def e2e_step():
+        with hyt.Graph(csr_h, stream=sptr) as g2:
+            _, st = g2.pagerank(out=ranks_h, stream=sptr)
+            its = st["iterations"]
+            for s in sources:
+                g2.sssp(s, out=dist_h, stream=sptr)
+        return its
+
+    e2e_step()
+    barrier(pg)
+    t0 = time.perf_counter()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    e2e_it = 0
+    for _ in range(args.e2e_steps):
+        e2e_it += e2e_step()
+    e1.record(stream)
+    barrier(pg)
+    e2e_wall = time.perf_counter() - t0
+    e2e_ms = max_over_ranks(pg, max(e0.elapsed_time(e1), 1e3 * e2e_wall))
+    e2e_value = (E * e2e_it + E * len(sources) * args.e2e_steps) * world / (e2e_ms / 1e3) / 1e9
+    h2d = (V + 1) * 8 + E * 4 + E * 4
+    d2h = V * 4 * (1 + len(sources))
+
+    # ---- CPU baseline (rank 0, N=1 only) ----
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        e, t, kind = cpu_sample(off_np, csr_h.column_indices, csr_h.weights.astype(np.float32), sources[0])
+        cpu = {"value": e / t / 1e9, "unit": UNIT, "cores": 1, "kind": kind,
+               "sample": (f"1 PageRank iteration + 1 SSSP round of the reference's single-threaded "
+                          f"pagerank_cpu/sssp_cpu (each incl. its incoming-CSR build) on this graph, "
+                          f"{t:.1f} s; E counted per iteration/round")}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32 (PageRank) / u32 (SSSP)",
+                "data": "synthetic", "config": workload_config(args, V, E),
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                        "ms_per_step": e2e_ms / args.e2e_steps, "steps": args.e2e_steps},
+                "roofline": roof, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches,
+                "pagerank": {"iterations_per_solve": pr_it / args.steps, "ms_per_solve": pr_ms / args.steps,
+                             "gteps": E * pr_it / (pr_ms / 1e3) / 1e9, "achieved_gbs": pr_gbs},
+                "sssp": {"solves": len(timed["sssp"]), "ms_per_solve": ss_ms / len(timed["sssp"]),
+                         "gteps": E * len(timed["sssp"]) / (ss_ms / 1e3) / 1e9,
+                         "rounds_per_solve": sum(s["iterations"] for s in timed["sssp"]) / len(timed["sssp"]),
+                         "relaxations_per_edge": sum(s["edges_processed"] for s in timed["sssp"]) / (
+                             E * len(timed["sssp"])),
+                         "achieved_gbs": ss_gbs}}
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

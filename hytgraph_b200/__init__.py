@@ -1,0 +1,15 @@
+"""hytgraph_b200 -- B200-native hybrid-transfer graph processing.
+
+PageRank (pull over CSC), personalized PageRank and frontier SSSP as
+hand-written sm_100a CUDA behind a C ABI (include/hyt/capi.h), with the
+reference's C++ interfaces (include/graph, include/algorithms,
+include/transfer, include/scheduling, include/runtime) in libhytgraph.so.
+
+Importing the package loads lib/libhyt_core.so and fails if it is missing;
+there is no CPU fallback.
+"""
+from . import capi
+from .capi import HytError, device_count
+from .graph import CSR, DeviceCSR, Graph, pick_sources, rmat
+
+__all__ = ["capi", "HytError", "device_count", "CSR", "DeviceCSR", "Graph", "pick_sources", "rmat"]

@@ -1,0 +1,198 @@
+"""ctypes bindings of the C ABI in include/hyt/capi.h (libhyt_core.so).
+
+The library is loaded from hytgraph_b200/lib/ (built in-tree by
+``make -C hytgraph_b200``).  There is no fallback: if the shared library is
+missing, importing this module raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+LIB_DIR = Path(__file__).resolve().parent / "lib"
+CORE_PATH = LIB_DIR / "libhyt_core.so"
+
+HYT_OK = 0
+HYT_E_INVALID = 1
+HYT_E_CUDA = 2
+HYT_E_OOM = 3
+HYT_E_TIMEOUT = 4
+HYT_E_NO_DEVICE = 5
+HYT_E_UNSUPPORTED = 6
+HYT_E_INTERNAL = 7
+
+HYT_WEIGHTS_NONE = 0
+HYT_WEIGHTS_U32 = 1
+HYT_WEIGHTS_F32 = 2
+
+HYT_GRAPH_PULL = 1
+HYT_GRAPH_PUSH = 2
+HYT_GRAPH_ALL = 3
+
+HYT_RUN_PROFILE = 1
+HYT_RUN_NO_GRAPH = 2
+
+HYT_DIST_INF_U32 = 0xFFFFFFFF
+
+
+class hyt_csr(C.Structure):
+    _fields_ = [
+        ("num_vertices", C.c_uint64),
+        ("num_edges", C.c_uint64),
+        ("row_offsets", C.c_void_p),
+        ("column_indices", C.c_void_p),
+        ("weights", C.c_void_p),
+        ("weight_kind", C.c_uint32),
+    ]
+
+
+class hyt_graph_options(C.Structure):
+    _fields_ = [("flags", C.c_uint32), ("device", C.c_int), ("stream", C.c_void_p)]
+
+
+class hyt_graph_info(C.Structure):
+    _fields_ = [
+        ("num_vertices", C.c_uint64),
+        ("num_edges", C.c_uint64),
+        ("weight_kind", C.c_uint32),
+        ("flags", C.c_uint32),
+        ("device_bytes", C.c_uint64),
+        ("pull_tiles", C.c_uint64),
+        ("long_rows", C.c_uint64),
+        ("max_in_degree", C.c_uint64),
+        ("max_out_degree", C.c_uint64),
+        ("dangling_vertices", C.c_uint64),
+        ("build_ms", C.c_double),
+    ]
+
+
+class hyt_pagerank_params(C.Structure):
+    _fields_ = [
+        ("damping", C.c_float),
+        ("tolerance", C.c_float),
+        ("max_iterations", C.c_uint32),
+        ("flags", C.c_uint32),
+        ("stream", C.c_void_p),
+    ]
+
+
+class hyt_ppr_params(C.Structure):
+    _fields_ = [
+        ("source", C.c_uint32),
+        ("restart", C.c_float),
+        ("tolerance", C.c_float),
+        ("max_iterations", C.c_uint32),
+        ("flags", C.c_uint32),
+        ("stream", C.c_void_p),
+    ]
+
+
+class hyt_run_stats(C.Structure):
+    _fields_ = [
+        ("iterations", C.c_uint32),
+        ("converged", C.c_uint32),
+        ("residual", C.c_double),
+        ("device_ms", C.c_double),
+        ("kernel_ms", C.c_double),
+        ("kernel_launches", C.c_uint32),
+        ("total_launches", C.c_uint32),
+        ("edges_processed", C.c_uint64),
+        ("vertices_processed", C.c_uint64),
+        ("algorithmic_bytes", C.c_uint64),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class hyt_sssp_params(C.Structure):
+    _fields_ = [
+        ("source", C.c_uint32),
+        ("delta", C.c_uint32),
+        ("max_rounds", C.c_uint32),
+        ("flags", C.c_uint32),
+        ("stream", C.c_void_p),
+    ]
+
+
+class hyt_rmat_params(C.Structure):
+    _fields_ = [
+        ("scale", C.c_uint32),
+        ("edge_factor", C.c_uint32),
+        ("a", C.c_double),
+        ("b", C.c_double),
+        ("c", C.c_double),
+        ("seed", C.c_uint64),
+        ("weight_min", C.c_uint32),
+        ("weight_max", C.c_uint32),
+    ]
+
+
+class hyt_csr_buffers(C.Structure):
+    _fields_ = [
+        ("num_vertices", C.c_uint64),
+        ("num_edges", C.c_uint64),
+        ("row_offsets", C.POINTER(C.c_uint64)),
+        ("column_indices", C.POINTER(C.c_uint32)),
+        ("weights", C.POINTER(C.c_uint32)),
+        ("on_device", C.c_uint32),
+    ]
+
+
+class HytError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"[hyt status {code}] {message}")
+        self.code = code
+
+
+# (name, restype, argtypes)
+_SIGNATURES = [
+    ("hyt_last_error", C.c_char_p, []),
+    ("hyt_abi_version", C.c_int, []),
+    ("hyt_device_count", C.c_int, [C.POINTER(C.c_int)]),
+    ("hyt_graph_create", C.c_int, [C.POINTER(hyt_csr), C.POINTER(hyt_graph_options), C.POINTER(C.c_void_p)]),
+    ("hyt_graph_destroy", C.c_int, [C.c_void_p]),
+    ("hyt_graph_get_info", C.c_int, [C.c_void_p, C.POINTER(hyt_graph_info)]),
+    ("hyt_pagerank", C.c_int, [C.c_void_p, C.POINTER(hyt_pagerank_params), C.c_void_p, C.POINTER(hyt_run_stats)]),
+    ("hyt_ppr", C.c_int, [C.c_void_p, C.POINTER(hyt_ppr_params), C.c_void_p, C.POINTER(hyt_run_stats)]),
+    ("hyt_sssp", C.c_int, [C.c_void_p, C.POINTER(hyt_sssp_params), C.c_void_p, C.POINTER(hyt_run_stats)]),
+    ("hyt_rmat_generate", C.c_int, [C.POINTER(hyt_rmat_params), C.c_int, C.POINTER(hyt_csr_buffers)]),
+    ("hyt_csr_buffers_free", C.c_int, [C.POINTER(hyt_csr_buffers)]),
+    ("hyt_pick_sources", C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint32, C.c_void_p]),
+]
+
+EXPORTED = [name for name, _, _ in _SIGNATURES]
+
+
+def _load() -> C.CDLL:
+    if not CORE_PATH.exists():
+        raise ImportError(
+            f"{CORE_PATH} is missing: build it with `make -C {CORE_PATH.parent.parent}` "
+            "(or __graft_entry__.build()); there is no CPU fallback"
+        )
+    lib = C.CDLL(str(CORE_PATH), mode=os.RTLD_NOW | C.RTLD_GLOBAL)
+    for name, res, args in _SIGNATURES:
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def last_error() -> str:
+    msg = lib.hyt_last_error()
+    return msg.decode() if msg else ""
+
+
+def check(status: int) -> None:
+    if status != HYT_OK:
+        raise HytError(status, last_error())
+
+
+def device_count() -> int:
+    n = C.c_int(0)
+    check(lib.hyt_device_count(C.byref(n)))
+    return n.value

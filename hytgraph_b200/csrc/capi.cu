@@ -1,0 +1,210 @@
+// extern "C" entry points of libhyt_core.so (declared in include/hyt/capi.h).
+#include <cstring>
+#include <string>
+
+#include "common.cuh"
+#include "graph.cuh"
+#include "solvers.cuh"
+
+namespace hyt {
+namespace {
+thread_local std::string g_last_error;
+}
+
+void set_last_error(const std::string &msg) { g_last_error = msg; }
+void clear_last_error() { g_last_error.clear(); }
+
+bool is_device_pointer(const void *p) {
+    if (!p) return false;
+    cudaPointerAttributes attr{};
+    const cudaError_t e = cudaPointerGetAttributes(&attr, p);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        return false;
+    }
+    return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+}
+
+void copy_to_device(void *dst, const void *src, size_t bytes, cudaStream_t s) {
+    if (!bytes) return;
+    const cudaMemcpyKind kind = is_device_pointer(src) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    HYT_CUDA(cudaMemcpyAsync(dst, src, bytes, kind, s));
+    HYT_CUDA(cudaStreamSynchronize(s));
+}
+
+void copy_from_device(void *dst, const void *src, size_t bytes, cudaStream_t s) {
+    if (!bytes) return;
+    const cudaMemcpyKind kind = is_device_pointer(dst) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    HYT_CUDA(cudaMemcpyAsync(dst, src, bytes, kind, s));
+    HYT_CUDA(cudaStreamSynchronize(s));
+}
+
+int sm_count() {
+    static int n = 0;
+    if (n == 0) {
+        int dev = 0;
+        HYT_CUDA(cudaGetDevice(&dev));
+        HYT_CUDA(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
+    }
+    return n;
+}
+
+namespace {
+void require_device() {
+    int n = 0;
+    const cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        (void)cudaGetLastError();
+        fail(HYT_E_NO_DEVICE, "no CUDA device is available");
+    }
+}
+
+GraphImpl &impl(hyt_graph *g) {
+    if (!g) fail(HYT_E_INVALID, "graph handle is NULL");
+    return g->impl;
+}
+
+void use_device(const GraphImpl &g) { HYT_CUDA(cudaSetDevice(g.device)); }
+}  // namespace
+
+}  // namespace hyt
+
+using namespace hyt;
+
+extern "C" {
+
+const char *hyt_last_error(void) { return g_last_error.c_str(); }
+
+int hyt_abi_version(void) { return HYT_ABI_VERSION; }
+
+int hyt_device_count(int *count) {
+    return guarded([&] {
+        if (!count) fail(HYT_E_INVALID, "count is NULL");
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess) {
+            (void)cudaGetLastError();
+            n = 0;
+        }
+        *count = n;
+    });
+}
+
+int hyt_graph_create(const hyt_csr *csr, const hyt_graph_options *options, hyt_graph **out) {
+    return guarded([&] {
+        if (!csr || !out) fail(HYT_E_INVALID, "csr/out is NULL");
+        *out = nullptr;
+        require_device();
+        hyt_graph_options opt{};
+        if (options) opt = *options;
+        auto *g = new hyt_graph();
+        try {
+            g->impl.device = opt.device;
+            HYT_CUDA(cudaSetDevice(opt.device));
+            if (opt.stream) {
+                g->impl.stream = static_cast<cudaStream_t>(opt.stream);
+            } else {
+                HYT_CUDA(cudaStreamCreateWithFlags(&g->impl.stream, cudaStreamNonBlocking));
+                g->impl.own_stream = true;
+            }
+            g->impl.host_scratch.allocate(64);
+            graph_build(g->impl, *csr, opt.flags);
+        } catch (...) {
+            if (g->impl.own_stream && g->impl.stream) cudaStreamDestroy(g->impl.stream);
+            delete g;
+            throw;
+        }
+        *out = g;
+    });
+}
+
+int hyt_graph_destroy(hyt_graph *graph) {
+    return guarded([&] {
+        if (!graph) return;
+        cudaSetDevice(graph->impl.device);
+        cudaStreamSynchronize(graph->impl.stream);
+        const bool own = graph->impl.own_stream;
+        cudaStream_t s = graph->impl.stream;
+        delete graph;
+        if (own && s) cudaStreamDestroy(s);
+    });
+}
+
+int hyt_graph_get_info(const hyt_graph *graph, hyt_graph_info *out) {
+    return guarded([&] {
+        if (!graph || !out) fail(HYT_E_INVALID, "graph/out is NULL");
+        const GraphImpl &g = graph->impl;
+        std::memset(out, 0, sizeof(*out));
+        out->num_vertices = g.V;
+        out->num_edges = g.E;
+        out->weight_kind = g.weight_kind;
+        out->flags = g.flags;
+        out->device_bytes = g.device_bytes();
+        out->pull_tiles = g.num_tiles;
+        out->long_rows = g.num_long;
+        out->max_in_degree = g.max_in_degree;
+        out->max_out_degree = g.max_out_degree;
+        out->dangling_vertices = g.dangling;
+        out->build_ms = g.build_ms;
+    });
+}
+
+int hyt_pagerank(hyt_graph *graph, const hyt_pagerank_params *params, float *ranks_out, hyt_run_stats *stats) {
+    return guarded([&] {
+        if (!params) fail(HYT_E_INVALID, "params is NULL");
+        GraphImpl &g = impl(graph);
+        use_device(g);
+        if (stats) std::memset(stats, 0, sizeof(*stats));
+        pagerank_run(g, *params, ranks_out, stats);
+    });
+}
+
+int hyt_ppr(hyt_graph *graph, const hyt_ppr_params *params, float *ranks_out, hyt_run_stats *stats) {
+    return guarded([&] {
+        if (!params) fail(HYT_E_INVALID, "params is NULL");
+        GraphImpl &g = impl(graph);
+        use_device(g);
+        if (stats) std::memset(stats, 0, sizeof(*stats));
+        ppr_run(g, *params, ranks_out, stats);
+    });
+}
+
+int hyt_sssp(hyt_graph *graph, const hyt_sssp_params *params, uint32_t *dist_out, hyt_run_stats *stats) {
+    return guarded([&] {
+        if (!params) fail(HYT_E_INVALID, "params is NULL");
+        GraphImpl &g = impl(graph);
+        use_device(g);
+        if (stats) std::memset(stats, 0, sizeof(*stats));
+        sssp_run(g, *params, dist_out, stats);
+    });
+}
+
+int hyt_rmat_generate(const hyt_rmat_params *params, int on_device, hyt_csr_buffers *out) {
+    return guarded([&] {
+        if (!params) fail(HYT_E_INVALID, "params is NULL");
+        if (on_device) require_device();
+        rmat_generate(*params, on_device != 0, out);
+    });
+}
+
+int hyt_csr_buffers_free(hyt_csr_buffers *b) {
+    return guarded([&] {
+        if (!b) return;
+        if (b->on_device) {
+            if (b->row_offsets) cudaFree(b->row_offsets);
+            if (b->column_indices) cudaFree(b->column_indices);
+            if (b->weights) cudaFree(b->weights);
+        } else {
+            std::free(b->row_offsets);
+            std::free(b->column_indices);
+            std::free(b->weights);
+        }
+        std::memset(b, 0, sizeof(*b));
+    });
+}
+
+int hyt_pick_sources(const uint64_t *row_offsets, uint64_t num_vertices, uint64_t seed, uint32_t count,
+                     uint32_t *out) {
+    return guarded([&] { pick_sources(row_offsets, num_vertices, seed, count, out); });
+}
+
+}  // extern "C"

@@ -1,0 +1,276 @@
+// Device graph construction: upload + validation, out-degrees, the CSC
+// transpose and the PageRank pull work tiles.  Runs once per graph.
+//
+// The reference builds its incoming CSR on the host, single-threaded, on
+// every pagerank_gpu / sssp_gpu call (cuda/pagerank.cu:33-74,
+// cuda/sssp.cu:34-79).  Here the transpose is a stable radix sort on the
+// GPU, so sources stay ascending inside every in-row exactly as the
+// reference's counting pass leaves them.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+#include "graph.cuh"
+#include "prims.cuh"
+
+namespace hyt {
+namespace {
+
+enum : uint32_t { kBadOffsets = 1u, kBadColumn = 2u, kBadWeight = 4u, kBadTerminal = 8u };
+
+__global__ void validate_offsets_kernel(const uint64_t *off, uint64_t V, uint64_t E, uint32_t *err) {
+    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+    for (uint64_t v = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; v < V; v += stride) {
+        if (off[v + 1] < off[v]) atomicOr(err, kBadOffsets);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (off[0] != 0) atomicOr(err, kBadOffsets);
+        if (off[V] != E) atomicOr(err, kBadTerminal);
+    }
+}
+
+__global__ void validate_edges_kernel(const uint32_t *cols, const uint32_t *w, uint32_t wkind, uint64_t V,
+                                      uint64_t E, uint32_t *err) {
+    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+    uint32_t bad = 0;
+    for (uint64_t e = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; e < E; e += stride) {
+        if (cols[e] >= V) bad |= kBadColumn;
+        if (wkind == HYT_WEIGHTS_F32) {
+            const float x = __uint_as_float(w[e]);
+            if (!(x >= 0.0f) || isinf(x)) bad |= kBadWeight;  // NaN fails x >= 0
+        }
+    }
+    if (bad) atomicOr(err, bad);
+}
+
+__global__ void out_degree_kernel(const uint64_t *off, uint64_t V, uint32_t *deg, unsigned long long *dangling) {
+    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+    uint32_t nd = 0;
+    for (uint64_t v = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; v < V; v += stride) {
+        const uint32_t d = static_cast<uint32_t>(off[v + 1] - off[v]);
+        deg[v] = d;
+        nd += (d == 0);
+    }
+    if (nd) atomicAdd(dangling, (unsigned long long)nd);
+}
+
+// Writes the source vertex of every CSR edge.  A CTA owns 256 consecutive
+// rows; their edges are spread over all threads via an in-CTA prefix of the
+// degrees, so rows of any length are load-balanced inside the CTA.
+__global__ void __launch_bounds__(256) expand_sources_kernel(const uint64_t *off, uint64_t V, uint32_t *src) {
+    __shared__ uint64_t s_first[257];
+    const uint64_t v0 = uint64_t(blockIdx.x) * 256;
+    for (uint64_t base = v0; base < V; base += uint64_t(gridDim.x) * 256) {
+        const uint64_t v = base + threadIdx.x;
+        const uint64_t hi = (base + 256 < V) ? base + 256 : V;
+        if (v <= hi) s_first[threadIdx.x] = off[v];
+        if (threadIdx.x == 0) s_first[hi - base] = off[hi];
+        __syncthreads();
+        const uint64_t e0 = s_first[0], e1 = s_first[hi - base];
+        const int nrows = static_cast<int>(hi - base);
+        for (uint64_t e = e0 + threadIdx.x; e < e1; e += 256) {
+            // last row r with s_first[r] <= e
+            int lo = 0, hi2 = nrows - 1;
+            while (lo < hi2) {
+                const int mid = (lo + hi2 + 1) >> 1;
+                if (s_first[mid] <= e) lo = mid; else hi2 = mid - 1;
+            }
+            src[e] = static_cast<uint32_t>(base + lo);
+        }
+        __syncthreads();
+    }
+}
+
+// Row offsets of a sorted key array: off[v] = first position with key >= v.
+__global__ void offsets_from_sorted_kernel(const uint32_t *keys, uint64_t E, uint64_t V, uint64_t *off) {
+    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+    for (uint64_t e = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; e <= E; e += stride) {
+        const int64_t prev = (e == 0) ? -1 : static_cast<int64_t>(keys[e - 1]);
+        const int64_t cur = (e == E) ? static_cast<int64_t>(V) : static_cast<int64_t>(keys[e]);
+        for (int64_t v = prev + 1; v <= cur; ++v) off[v] = e;
+    }
+}
+
+// tile_start[k] = first row whose merge-path coordinate (row + in_offset)
+// reaches k * kTileCost.
+__global__ void tile_bounds_kernel(const uint64_t *in_off, uint64_t V, uint64_t E, uint64_t num_tiles,
+                                   uint32_t *tile_start) {
+    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+    for (uint64_t v = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; v <= V; v += stride) {
+        const int64_t p_prev = (v == 0) ? -1 : static_cast<int64_t>((v - 1) + in_off[v - 1]);
+        const int64_t p_cur = static_cast<int64_t>(v + in_off[v]);
+        int64_t k_lo = (p_prev < 0) ? 0 : p_prev / kTileCost + 1;
+        int64_t k_hi = (v == V) ? static_cast<int64_t>(num_tiles) : p_cur / kTileCost;
+        for (int64_t k = k_lo; k <= k_hi; ++k) tile_start[k] = static_cast<uint32_t>(v);
+    }
+}
+
+__global__ void in_degree_kernel(const uint64_t *in_off, uint64_t V, uint32_t *deg, uint8_t *is_long) {
+    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+    for (uint64_t v = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; v < V; v += stride) {
+        const uint32_t d = static_cast<uint32_t>(in_off[v + 1] - in_off[v]);
+        deg[v] = d;
+        is_long[v] = d >= kLongDegree;
+    }
+}
+
+__global__ void gather_u32_kernel(const uint32_t *src, const uint32_t *idx, uint64_t n, uint32_t *out) {
+    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += stride) out[i] = src[idx[i]];
+}
+
+int bits_for(uint64_t max_value) {
+    int b = 1;
+    while (b < 64 && (max_value >> b) != 0) ++b;
+    return b;
+}
+
+}  // namespace
+
+size_t GraphImpl::device_bytes() const {
+    size_t b = row_offsets.bytes() + cols.bytes() + weights.bytes() + out_degree.bytes() + in_offsets.bytes() +
+               in_sources.bytes() + tile_start.bytes() + long_rows.bytes() + chunk_tasks.bytes();
+    for (int i = 0; i < 2; ++i) b += rank[i].bytes() + contrib[i].bytes() + queue[i].bytes();
+    b += partial.bytes() + ticket.bytes() + pr_state.bytes() + dist.bytes() + stamp.bytes() + hub_tasks.bytes() +
+         sssp_state.bytes();
+    return b;
+}
+
+void graph_build(GraphImpl &g, const hyt_csr &csr, uint32_t flags) {
+    const uint64_t V = csr.num_vertices, E = csr.num_edges;
+    if (V == 0) fail(HYT_E_INVALID, "graph requires at least one vertex");
+    if (V > 0xFFFFFFFFull) fail(HYT_E_INVALID, "vertex ids are uint32: num_vertices must be < 2^32");
+    if (E > 0xFFFFFFFEull) fail(HYT_E_UNSUPPORTED, "in-HBM graphs hold fewer than 2^32 edges");
+    if (!csr.row_offsets) fail(HYT_E_INVALID, "row_offsets is NULL");
+    if (E > 0 && !csr.column_indices) fail(HYT_E_INVALID, "column_indices is NULL");
+    if (csr.weight_kind > HYT_WEIGHTS_F32) fail(HYT_E_INVALID, "unknown weight_kind");
+    if (csr.weight_kind != HYT_WEIGHTS_NONE && E > 0 && !csr.weights)
+        fail(HYT_E_INVALID, "weights is NULL for a weighted graph");
+    if (flags == 0) flags = HYT_GRAPH_ALL;
+
+    cudaStream_t s = g.stream;
+    EventTimer timer;
+    timer.start(s);
+
+    g.V = V;
+    g.E = E;
+    g.flags = flags;
+    g.weight_kind = csr.weight_kind;
+
+    g.row_offsets.allocate(V + 1);
+    copy_to_device(g.row_offsets.get(), csr.row_offsets, (V + 1) * sizeof(uint64_t), s);
+    g.cols.allocate(E ? E : 1);
+    if (E) copy_to_device(g.cols.get(), csr.column_indices, E * sizeof(uint32_t), s);
+    const bool keep_weights = (flags & HYT_GRAPH_PUSH) && csr.weight_kind != HYT_WEIGHTS_NONE;
+    if (keep_weights) {
+        g.weights.allocate(E ? E : 1);
+        if (E) copy_to_device(g.weights.get(), csr.weights, E * sizeof(uint32_t), s);
+    }
+
+    // Validation: malformed offsets or out-of-range ids would turn into
+    // out-of-bounds device accesses later, so they are rejected here.
+    DeviceArray<uint32_t> err(1);
+    DeviceArray<unsigned long long> counter(1);
+    HYT_CUDA(cudaMemsetAsync(err.get(), 0, sizeof(uint32_t), s));
+    HYT_CUDA(cudaMemsetAsync(counter.get(), 0, sizeof(unsigned long long), s));
+    validate_offsets_kernel<<<grid_for(V, 256), 256, 0, s>>>(g.row_offsets.get(), V, E, err.get());
+    HYT_CUDA(cudaGetLastError());
+    uint32_t h_err = 0;
+    HYT_CUDA(cudaMemcpyAsync(&h_err, err.get(), sizeof(h_err), cudaMemcpyDeviceToHost, s));
+    HYT_CUDA(cudaStreamSynchronize(s));
+    if (h_err & kBadOffsets) fail(HYT_E_INVALID, "row offsets must start at 0 and be non-decreasing");
+    if (h_err & kBadTerminal) fail(HYT_E_INVALID, "terminal row offset must equal the number of edges");
+    if (E) {
+        validate_edges_kernel<<<grid_for(E, 256), 256, 0, s>>>(g.cols.get(), keep_weights ? g.weights.get() : nullptr,
+                                                                keep_weights ? csr.weight_kind : 0u, V, E, err.get());
+        HYT_CUDA(cudaGetLastError());
+        HYT_CUDA(cudaMemcpyAsync(&h_err, err.get(), sizeof(h_err), cudaMemcpyDeviceToHost, s));
+        HYT_CUDA(cudaStreamSynchronize(s));
+        if (h_err & kBadColumn) fail(HYT_E_INVALID, "column index contains an invalid destination vertex ID");
+        // Negative / non-finite float weights are legal for PageRank; SSSP
+        // rejects them when it is called (reference: sssp.cpp:117-124).
+        g.weights_ok = (h_err & kBadWeight) == 0;
+    }
+
+    g.out_degree.allocate(V);
+    out_degree_kernel<<<grid_for(V, 256), 256, 0, s>>>(g.row_offsets.get(), V, g.out_degree.get(), counter.get());
+    HYT_CUDA(cudaGetLastError());
+    unsigned long long h_dangling = 0;
+    HYT_CUDA(cudaMemcpyAsync(&h_dangling, counter.get(), sizeof(h_dangling), cudaMemcpyDeviceToHost, s));
+    HYT_CUDA(cudaStreamSynchronize(s));
+    g.dangling = h_dangling;
+    g.max_out_degree = prims::reduce_max_u32(g.out_degree.get(), V, s);
+
+    if (flags & HYT_GRAPH_PULL) {
+        // CSC transpose: stable sort of (destination, source) by destination.
+        DeviceArray<uint32_t> keys(E ? E : 1);
+        g.in_sources.allocate(E ? E : 1);
+        if (E) {
+            HYT_CUDA(cudaMemcpyAsync(keys.get(), g.cols.get(), E * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+            const unsigned blocks = static_cast<unsigned>(std::min<uint64_t>((V + 255) / 256, 148ull * 64));
+            expand_sources_kernel<<<blocks, 256, 0, s>>>(g.row_offsets.get(), V, g.in_sources.get());
+            HYT_CUDA(cudaGetLastError());
+            prims::sort_pairs_u32(keys.get(), g.in_sources.get(), E, bits_for(V - 1), s);
+        }
+        g.in_offsets.allocate(V + 1);
+        offsets_from_sorted_kernel<<<grid_for(E + 1, 256), 256, 0, s>>>(keys.get(), E, V, g.in_offsets.get());
+        HYT_CUDA(cudaGetLastError());
+        keys.release();
+
+        // Work tiles along the merge path.
+        g.num_tiles = (V + E) / kTileCost + 1;
+        g.tile_start.allocate(g.num_tiles + 1);
+        tile_bounds_kernel<<<grid_for(V + 1, 256), 256, 0, s>>>(g.in_offsets.get(), V, E, g.num_tiles,
+                                                                 g.tile_start.get());
+        HYT_CUDA(cudaGetLastError());
+
+        // Long rows (in-degree >= kLongDegree) and their chunk tasks.
+        DeviceArray<uint32_t> in_deg(V);
+        DeviceArray<uint8_t> is_long(V);
+        in_degree_kernel<<<grid_for(V, 256), 256, 0, s>>>(g.in_offsets.get(), V, in_deg.get(), is_long.get());
+        HYT_CUDA(cudaGetLastError());
+        g.max_in_degree = prims::reduce_max_u32(in_deg.get(), V, s);
+        DeviceArray<uint32_t> long_ids(V);
+        g.num_long = prims::select_flagged_index(is_long.get(), long_ids.get(), V, s);
+        std::vector<LongRow> lr(g.num_long);
+        std::vector<uint2> tasks;
+        if (g.num_long) {
+            DeviceArray<uint32_t> long_deg(g.num_long);
+            gather_u32_kernel<<<grid_for(g.num_long, 256), 256, 0, s>>>(in_deg.get(), long_ids.get(), g.num_long,
+                                                                         long_deg.get());
+            HYT_CUDA(cudaGetLastError());
+            std::vector<uint32_t> ids(g.num_long), degs(g.num_long);
+            HYT_CUDA(cudaMemcpyAsync(ids.data(), long_ids.get(), g.num_long * 4, cudaMemcpyDeviceToHost, s));
+            HYT_CUDA(cudaMemcpyAsync(degs.data(), long_deg.get(), g.num_long * 4, cudaMemcpyDeviceToHost, s));
+            HYT_CUDA(cudaStreamSynchronize(s));
+            uint32_t next = 0;
+            for (uint64_t i = 0; i < g.num_long; ++i) {
+                const uint32_t nc = (degs[i] + kLongChunk - 1) / kLongChunk;
+                lr[i] = LongRow{ids[i], next, nc, 0};
+                for (uint32_t c = 0; c < nc; ++c) tasks.push_back(make_uint2(static_cast<uint32_t>(i), c));
+                next += nc;
+            }
+        }
+        g.num_chunks = tasks.size();
+        g.long_rows.allocate(std::max<uint64_t>(g.num_long, 1));
+        g.chunk_tasks.allocate(std::max<uint64_t>(g.num_chunks, 1));
+        if (g.num_long)
+            HYT_CUDA(cudaMemcpyAsync(g.long_rows.get(), lr.data(), lr.size() * sizeof(LongRow),
+                                     cudaMemcpyHostToDevice, s));
+        if (g.num_chunks)
+            HYT_CUDA(cudaMemcpyAsync(g.chunk_tasks.get(), tasks.data(), tasks.size() * sizeof(uint2),
+                                     cudaMemcpyHostToDevice, s));
+        HYT_CUDA(cudaStreamSynchronize(s));
+    }
+
+    if (!(flags & HYT_GRAPH_PUSH)) {
+        // Pull-only graphs keep the CSC; the CSR edges are not needed.
+        g.cols.release();
+        g.weights.release();
+    }
+    timer.stop(s);
+    g.build_ms = timer.ms();
+}
+
+}  // namespace hyt

@@ -1,0 +1,91 @@
+// Device-resident graph behind the opaque hyt_graph handle.
+//
+// HBM layout (E < 2^32 edges per graph on this path):
+//   push side (CSR, frontier SSSP):   row_offsets u64[V+1], cols u32[E],
+//                                     weights u32[E] (u32 or f32 bits)
+//   pull side (CSC, PageRank):        in_offsets u64[V+1], in_sources u32[E]
+//   per vertex:                       out_degree u32[V]
+//   PageRank work list:               tile_start u32[T+1] (short-row tiles),
+//                                     long rows + their chunk tasks
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "common.cuh"
+
+namespace hyt {
+
+// PageRank pull work decomposition.  Rows are cut into tiles along the
+// merge path (1 unit per row + 1 per in-edge): a tile spans kTileCost units,
+// so its rows hold at most kTileCost edges except for its last row.  A last
+// row with in-degree >= kLongDegree is a "long row": it is excluded from the
+// tile and split into chunks of kLongChunk edges processed by separate CTAs.
+constexpr uint32_t kTileCost = 4096;
+constexpr uint32_t kLongDegree = kTileCost;
+constexpr uint32_t kLongChunk = 8192;
+constexpr uint32_t kStageCap = kTileCost + kLongDegree;  // staged edges per tile
+
+struct LongRow {
+    uint32_t row;
+    uint32_t first_chunk;  // index of its first partial-sum slot
+    uint32_t num_chunks;
+    uint32_t pad;
+};
+
+struct GraphImpl {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+
+    uint64_t V = 0, E = 0;
+    uint32_t weight_kind = HYT_WEIGHTS_NONE;
+    uint32_t flags = 0;
+    bool weights_ok = true;  // F32 weights all finite and >= 0
+
+    // push side
+    DeviceArray<uint64_t> row_offsets;
+    DeviceArray<uint32_t> cols;
+    DeviceArray<uint32_t> weights;
+    DeviceArray<uint32_t> out_degree;
+
+    // pull side
+    DeviceArray<uint64_t> in_offsets;
+    DeviceArray<uint32_t> in_sources;
+    DeviceArray<uint32_t> tile_start;   // [num_tiles + 1]
+    DeviceArray<LongRow> long_rows;     // [num_long]
+    DeviceArray<uint2> chunk_tasks;     // [num_chunks] = (long row index, chunk)
+    uint64_t num_tiles = 0, num_long = 0, num_chunks = 0;
+
+    // host-side facts
+    uint64_t max_in_degree = 0, max_out_degree = 0, dangling = 0;
+    double build_ms = 0.0;
+
+    // Solver workspaces, grown on demand and reused across calls.
+    DeviceArray<float> rank[2];
+    DeviceArray<float> contrib[2];
+    DeviceArray<float> partial;        // long-row chunk partial sums (s, c)
+    DeviceArray<uint32_t> ticket;      // long-row arrival counters
+    DeviceArray<unsigned char> pr_state;
+    uint32_t pr_state_iters = 0;
+
+    DeviceArray<uint32_t> dist;
+    DeviceArray<uint32_t> stamp;
+    DeviceArray<uint32_t> queue[2];
+    DeviceArray<uint2> hub_tasks;
+    DeviceArray<unsigned char> sssp_state;
+    PinnedArray<uint64_t> host_scratch;  // small pinned readback area
+
+    size_t device_bytes() const;
+};
+
+// Builds the device graph from a CSR (host or device pointers).
+void graph_build(GraphImpl &g, const hyt_csr &csr, uint32_t flags);
+
+}  // namespace hyt
+
+struct hyt_graph {
+    hyt::GraphImpl impl;
+};

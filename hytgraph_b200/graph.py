@@ -1,0 +1,209 @@
+"""Python host API over the C ABI: CSR containers, the seeded R-MAT
+generator, and a device-resident graph handle with PageRank / personalized
+PageRank / SSSP solvers.
+
+Arrays may be numpy arrays (host) or any object exposing ``data_ptr()`` and
+``numel()`` (e.g. torch CUDA tensors) for device-resident inputs/outputs.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+from . import capi
+from .capi import check, lib
+
+RMAT_A, RMAT_B, RMAT_C = 0.57, 0.19, 0.19
+
+
+def _ptr(x) -> int:
+    if x is None:
+        return 0
+    if hasattr(x, "data_ptr"):
+        return int(x.data_ptr())
+    if isinstance(x, np.ndarray):
+        if not x.flags["C_CONTIGUOUS"]:
+            raise ValueError("arrays must be C-contiguous")
+        return int(x.ctypes.data)
+    raise TypeError(f"unsupported array type {type(x)!r}")
+
+
+@dataclass
+class CSR:
+    """Host CSR: row_offsets uint64[V+1], column_indices uint32[E], weights
+    uint32[E] / float32[E] / None."""
+
+    row_offsets: np.ndarray
+    column_indices: np.ndarray
+    weights: Optional[np.ndarray] = None
+
+    @property
+    def num_vertices(self) -> int:
+        return int(self.row_offsets.shape[0] - 1)
+
+    @property
+    def num_edges(self) -> int:
+        return int(self.column_indices.shape[0])
+
+    @property
+    def weight_kind(self) -> int:
+        if self.weights is None:
+            return capi.HYT_WEIGHTS_NONE
+        return capi.HYT_WEIGHTS_F32 if self.weights.dtype == np.float32 else capi.HYT_WEIGHTS_U32
+
+    def out_degree(self) -> np.ndarray:
+        return np.diff(self.row_offsets)
+
+    def to_c(self) -> capi.hyt_csr:
+        c = capi.hyt_csr()
+        c.num_vertices = self.num_vertices
+        c.num_edges = self.num_edges
+        c.row_offsets = _ptr(self.row_offsets)
+        c.column_indices = _ptr(self.column_indices) if self.num_edges else 0
+        c.weights = _ptr(self.weights) if (self.weights is not None and self.num_edges) else 0
+        c.weight_kind = self.weight_kind
+        return c
+
+
+@dataclass
+class DeviceCSR:
+    """A CSR whose arrays live in device memory (owned by the library)."""
+
+    buffers: capi.hyt_csr_buffers
+
+    @property
+    def num_vertices(self) -> int:
+        return int(self.buffers.num_vertices)
+
+    @property
+    def num_edges(self) -> int:
+        return int(self.buffers.num_edges)
+
+    def to_c(self) -> capi.hyt_csr:
+        b = self.buffers
+        c = capi.hyt_csr()
+        c.num_vertices = b.num_vertices
+        c.num_edges = b.num_edges
+        c.row_offsets = C.cast(b.row_offsets, C.c_void_p).value
+        c.column_indices = C.cast(b.column_indices, C.c_void_p).value
+        c.weights = C.cast(b.weights, C.c_void_p).value if b.weights else 0
+        c.weight_kind = capi.HYT_WEIGHTS_U32 if b.weights else capi.HYT_WEIGHTS_NONE
+        return c
+
+    def free(self) -> None:
+        check(lib.hyt_csr_buffers_free(C.byref(self.buffers)))
+
+    def __del__(self):
+        try:
+            if self.buffers.row_offsets:
+                lib.hyt_csr_buffers_free(C.byref(self.buffers))
+        except Exception:
+            pass
+
+
+def rmat_params(scale: int, edge_factor: int, seed: int, weight_min: int = 1, weight_max: int = 63,
+                a: float = RMAT_A, b: float = RMAT_B, c: float = RMAT_C) -> capi.hyt_rmat_params:
+    p = capi.hyt_rmat_params()
+    p.scale, p.edge_factor, p.seed = scale, edge_factor, seed
+    p.a, p.b, p.c = a, b, c
+    p.weight_min, p.weight_max = weight_min, weight_max
+    return p
+
+
+def rmat(scale: int, edge_factor: int, seed: int, weight_min: int = 1, weight_max: int = 63,
+         a: float = RMAT_A, b: float = RMAT_B, c: float = RMAT_C, device: bool = False):
+    """Seeded R-MAT graph (self-loops and duplicates removed, sorted by
+    (source, destination)).  Host: returns CSR of numpy copies.  device=True:
+    generated on the GPU and returned as a DeviceCSR."""
+    p = rmat_params(scale, edge_factor, seed, weight_min, weight_max, a, b, c)
+    buf = capi.hyt_csr_buffers()
+    check(lib.hyt_rmat_generate(C.byref(p), 1 if device else 0, C.byref(buf)))
+    if device:
+        return DeviceCSR(buf)
+    try:
+        V, E = int(buf.num_vertices), int(buf.num_edges)
+        off = np.ctypeslib.as_array(buf.row_offsets, shape=(V + 1,)).copy()
+        cols = np.ctypeslib.as_array(buf.column_indices, shape=(max(E, 1),))[:E].copy()
+        w = None
+        if buf.weights:
+            w = np.ctypeslib.as_array(buf.weights, shape=(max(E, 1),))[:E].copy()
+    finally:
+        check(lib.hyt_csr_buffers_free(C.byref(buf)))
+    return CSR(off, cols, w)
+
+
+def pick_sources(row_offsets: np.ndarray, seed: int, count: int) -> np.ndarray:
+    """`count` seeded vertices with out-degree > 0 (distinct while possible)."""
+    ro = np.ascontiguousarray(row_offsets, dtype=np.uint64)
+    out = np.zeros(count, dtype=np.uint32)
+    check(lib.hyt_pick_sources(_ptr(ro), ro.shape[0] - 1, seed, count, _ptr(out)))
+    return out
+
+
+class Graph:
+    """Device-resident graph (hyt_graph handle)."""
+
+    def __init__(self, csr, flags: int = capi.HYT_GRAPH_ALL, device: int = 0, stream: int = 0):
+        self._csr_ref = csr  # keep host arrays alive during creation
+        opts = capi.hyt_graph_options(flags, device, stream or None)
+        c = csr.to_c()
+        h = C.c_void_p()
+        check(lib.hyt_graph_create(C.byref(c), C.byref(opts), C.byref(h)))
+        self._h = h
+        self.num_vertices = int(c.num_vertices)
+        self.num_edges = int(c.num_edges)
+        self._csr_ref = None
+
+    @property
+    def handle(self) -> C.c_void_p:
+        if not self._h:
+            raise ValueError("graph is closed")
+        return self._h
+
+    def info(self) -> dict:
+        i = capi.hyt_graph_info()
+        check(lib.hyt_graph_get_info(self.handle, C.byref(i)))
+        return {name: getattr(i, name) for name, _ in i._fields_}
+
+    def pagerank(self, damping: float = 0.85, tolerance: float = 1e-6, max_iterations: int = 100,
+                 out=None, flags: int = 0, stream: int = 0):
+        p = capi.hyt_pagerank_params(damping, tolerance, max_iterations, flags, stream or None)
+        st = capi.hyt_run_stats()
+        res = np.empty(self.num_vertices, dtype=np.float32) if out is None else out
+        check(lib.hyt_pagerank(self.handle, C.byref(p), _ptr(res) if res is not False else None, C.byref(st)))
+        return res, st.as_dict()
+
+    def ppr(self, source: int, restart: float = 0.15, tolerance: float = 1e-6, max_iterations: int = 100,
+            out=None, flags: int = 0, stream: int = 0):
+        p = capi.hyt_ppr_params(source, restart, tolerance, max_iterations, flags, stream or None)
+        st = capi.hyt_run_stats()
+        res = np.empty(self.num_vertices, dtype=np.float32) if out is None else out
+        check(lib.hyt_ppr(self.handle, C.byref(p), _ptr(res) if res is not False else None, C.byref(st)))
+        return res, st.as_dict()
+
+    def sssp(self, source: int, out=None, flags: int = 0, max_rounds: int = 0, delta: int = 0, stream: int = 0):
+        p = capi.hyt_sssp_params(source, delta, max_rounds, flags, stream or None)
+        st = capi.hyt_run_stats()
+        res = np.empty(self.num_vertices, dtype=np.uint32) if out is None else out
+        check(lib.hyt_sssp(self.handle, C.byref(p), _ptr(res) if res is not False else None, C.byref(st)))
+        return res, st.as_dict()
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            check(lib.hyt_graph_destroy(self._h))
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

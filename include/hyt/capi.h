@@ -1,0 +1,224 @@
+/*
+ * hyt/capi.h -- C ABI of the B200 graph-processing core (libhyt_core.so).
+ *
+ * Plain C: opaque handles, plain pointers and sizes, int status codes.
+ * The C++ drop-in layer (include/algorithms, include/transfer, ...) and the
+ * Python bindings (hytgraph_b200/capi.py) are thin wrappers over this file.
+ *
+ * Conventions
+ *   - Every entry point returns HYT_OK (0) or one of the HYT_E_* codes; the
+ *     message of the last failure on the calling thread is hyt_last_error().
+ *   - Host buffers are owned by the caller.  A result pointer may be a host
+ *     pointer (pageable or pinned) or a device pointer; the library detects
+ *     which with cudaPointerGetAttributes and copies accordingly.
+ *   - Device memory behind a handle is owned by the library.
+ *   - One handle is used by one host thread at a time.
+ *   - `stream` fields take a cudaStream_t (NULL = the handle's own stream).
+ *     Calls are synchronous with respect to the host on return.
+ *
+ * Reference interfaces replaced (tanishbhongade/hytgraph):
+ *   hyt_pagerank   -> algorithms::pagerank_gpu   include/algorithms/pagerank.hpp:50-52
+ *                                                 (cuda/pagerank.cu:157-337)
+ *   hyt_sssp       -> algorithms::sssp_gpu       include/algorithms/sssp.hpp:49-51
+ *                                                 (cuda/sssp.cu:158-321)
+ *   hyt_graph_*    -> the device copy of graph::CSRGraph that pagerank_gpu /
+ *                     sssp_gpu build per call (cuda/pagerank.cu:184-244,
+ *                     cuda/sssp.cu:207-244); here it persists in a handle.
+ *   hyt_ppr        -> no reference symbol (personalized PageRank is new).
+ */
+#ifndef HYT_CAPI_H
+#define HYT_CAPI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HYT_ABI_VERSION 1
+
+enum hyt_status_code {
+    HYT_OK = 0,
+    HYT_E_INVALID = 1,     /* bad argument: std::invalid_argument in C++ */
+    HYT_E_CUDA = 2,        /* CUDA runtime error: std::runtime_error */
+    HYT_E_OOM = 3,         /* device/pinned allocation failed or over budget */
+    HYT_E_TIMEOUT = 4,     /* a bounded device-side wait ran out */
+    HYT_E_NO_DEVICE = 5,   /* no CUDA device is available */
+    HYT_E_UNSUPPORTED = 6, /* valid request this build does not implement */
+    HYT_E_INTERNAL = 7     /* an internal consistency check failed */
+};
+
+/* Message of the last failing call on this thread ("" if none). */
+const char *hyt_last_error(void);
+int hyt_abi_version(void);
+/* Number of visible CUDA devices (0 without error when there is none). */
+int hyt_device_count(int *count);
+
+/* ------------------------------------------------------------------ */
+/* CSR input                                                           */
+/* ------------------------------------------------------------------ */
+
+enum hyt_weight_kind {
+    HYT_WEIGHTS_NONE = 0, /* unweighted: every edge weighs 1 */
+    HYT_WEIGHTS_U32 = 1,  /* uint32 weights, exact integer distances */
+    HYT_WEIGHTS_F32 = 2   /* IEEE float weights (finite, >= 0) */
+};
+
+/* A CSR graph: row_offsets[V+1] (uint64), column_indices[E] (uint32),
+ * optional weights[E] whose type is given by weight_kind.  Pointers may be
+ * host or device memory.  Layout of graph::CSRGraph
+ * (include/graph/csr_graph.hpp:14-16, 63-69). */
+typedef struct hyt_csr {
+    uint64_t num_vertices;
+    uint64_t num_edges;
+    const uint64_t *row_offsets;
+    const uint32_t *column_indices;
+    const void *weights;
+    uint32_t weight_kind;
+} hyt_csr;
+
+/* ------------------------------------------------------------------ */
+/* Device-resident graph                                               */
+/* ------------------------------------------------------------------ */
+
+typedef struct hyt_graph hyt_graph;
+
+enum hyt_graph_flags {
+    HYT_GRAPH_PULL = 1u,   /* build the CSC + PageRank work tiles (pull) */
+    HYT_GRAPH_PUSH = 2u,   /* keep the CSR (+ weights) for frontier push */
+    HYT_GRAPH_ALL = 3u
+};
+
+typedef struct hyt_graph_options {
+    uint32_t flags;  /* HYT_GRAPH_* (0 = HYT_GRAPH_ALL) */
+    int device;      /* CUDA device ordinal */
+    void *stream;    /* cudaStream_t used for the upload (NULL = own) */
+} hyt_graph_options;
+
+typedef struct hyt_graph_info {
+    uint64_t num_vertices;
+    uint64_t num_edges;
+    uint32_t weight_kind;
+    uint32_t flags;
+    uint64_t device_bytes;      /* HBM held by the handle */
+    uint64_t pull_tiles;        /* PageRank work tiles */
+    uint64_t long_rows;         /* in-degree rows split across CTAs */
+    uint64_t max_in_degree;
+    uint64_t max_out_degree;
+    uint64_t dangling_vertices; /* out-degree 0 */
+    double build_ms;            /* device time of upload + CSC/tile build */
+} hyt_graph_info;
+
+int hyt_graph_create(const hyt_csr *csr, const hyt_graph_options *options,
+                     hyt_graph **out);
+int hyt_graph_destroy(hyt_graph *graph);
+int hyt_graph_get_info(const hyt_graph *graph, hyt_graph_info *out);
+
+/* ------------------------------------------------------------------ */
+/* PageRank (pull over CSC)                                            */
+/* ------------------------------------------------------------------ */
+
+enum hyt_run_flags {
+    HYT_RUN_PROFILE = 1u,   /* time every hot-kernel launch with events */
+    HYT_RUN_NO_GRAPH = 2u   /* host-driven loop instead of a CUDA graph */
+};
+
+typedef struct hyt_pagerank_params {
+    float damping;           /* [0, 1) */
+    float tolerance;         /* > 0: stop when the L1 change <= tolerance */
+    uint32_t max_iterations; /* > 0 */
+    uint32_t flags;          /* HYT_RUN_* */
+    void *stream;
+} hyt_pagerank_params;
+
+typedef struct hyt_run_stats {
+    uint32_t iterations;       /* PageRank iterations / SSSP rounds */
+    uint32_t converged;
+    double residual;           /* PageRank: FP64 L1 change of the last step */
+    double device_ms;          /* device time of the whole solve */
+    double kernel_ms;          /* summed hot-kernel time (HYT_RUN_PROFILE) */
+    uint32_t kernel_launches;  /* hot-kernel launches (HYT_RUN_PROFILE) */
+    uint32_t total_launches;   /* every kernel this call launched */
+    uint64_t edges_processed;  /* edges read (PR) / relaxed (SSSP) */
+    uint64_t vertices_processed;
+    uint64_t algorithmic_bytes;/* roofline numerator for the whole solve */
+} hyt_run_stats;
+
+/* ranks_out: [V] floats (host or device) or NULL to keep them on device. */
+int hyt_pagerank(hyt_graph *graph, const hyt_pagerank_params *params,
+                 float *ranks_out, hyt_run_stats *stats);
+
+/* Personalized PageRank from one source (no reference counterpart):
+ *   x' = d * sum_{u->v} x_u / deg(u) + [v == s] * ((1 - d) + d * dangling)
+ * with d = 1 - restart, x_0 = e_s, stop when the L1 change <= tolerance. */
+typedef struct hyt_ppr_params {
+    uint32_t source;
+    float restart;           /* (0, 1]; damping = 1 - restart */
+    float tolerance;
+    uint32_t max_iterations;
+    uint32_t flags;
+    void *stream;
+} hyt_ppr_params;
+
+int hyt_ppr(hyt_graph *graph, const hyt_ppr_params *params, float *ranks_out,
+            hyt_run_stats *stats);
+
+/* ------------------------------------------------------------------ */
+/* SSSP (frontier push over CSR, atomicMin relaxation)                  */
+/* ------------------------------------------------------------------ */
+
+#define HYT_DIST_INF_U32 0xFFFFFFFFu
+
+typedef struct hyt_sssp_params {
+    uint32_t source;
+    uint32_t delta;       /* near/far bucket width; 0 = chosen from weights */
+    uint32_t max_rounds;  /* 0 = unlimited (bounded by V*(V-1) relaxations) */
+    uint32_t flags;       /* HYT_RUN_* */
+    void *stream;
+} hyt_sssp_params;
+
+/* dist_out: [V] (host or device) or NULL.  U32/NONE graphs: exact integer
+ * distances, HYT_DIST_INF_U32 = unreachable.  F32 graphs: IEEE float bit
+ * patterns (0x7f800000 = +inf). */
+int hyt_sssp(hyt_graph *graph, const hyt_sssp_params *params,
+             uint32_t *dist_out, hyt_run_stats *stats);
+
+/* ------------------------------------------------------------------ */
+/* Seeded R-MAT generator (deterministic; same bytes on host and GPU)   */
+/* ------------------------------------------------------------------ */
+
+typedef struct hyt_rmat_params {
+    uint32_t scale;        /* V = 2^scale, 1..31 */
+    uint32_t edge_factor;  /* edge draws = edge_factor * V */
+    double a, b, c;        /* quadrant probabilities, d = 1 - a - b - c */
+    uint64_t seed;
+    uint32_t weight_min;   /* uint32 weights uniform in [min, max] */
+    uint32_t weight_max;   /* 0/0 = unweighted */
+} hyt_rmat_params;
+
+typedef struct hyt_csr_buffers {
+    uint64_t num_vertices;
+    uint64_t num_edges;
+    uint64_t *row_offsets;
+    uint32_t *column_indices;
+    uint32_t *weights;     /* NULL when unweighted */
+    uint32_t on_device;    /* 1: cudaMalloc'd, 0: malloc'd */
+} hyt_csr_buffers;
+
+/* on_device = 0: generated on the host CPU cores; 1: on the current GPU.
+ * Both produce identical bytes.  Free with hyt_csr_buffers_free. */
+int hyt_rmat_generate(const hyt_rmat_params *params, int on_device,
+                      hyt_csr_buffers *out);
+int hyt_csr_buffers_free(hyt_csr_buffers *buffers);
+
+/* Deterministic source choice: `count` vertices with out-degree > 0, drawn
+ * uniformly with the given seed (host row offsets). */
+int hyt_pick_sources(const uint64_t *row_offsets, uint64_t num_vertices,
+                     uint64_t seed, uint32_t count, uint32_t *out);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* HYT_CAPI_H */

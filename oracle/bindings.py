@@ -1,0 +1,190 @@
+"""ctypes access to the oracle (liboracle.so, the C restatement) and to the
+reference's own compiled CPU code (_ref/libhytref.so, optional).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+the CPU legs of bench.py, as the checker / CPU baseline.  The product
+package never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_SO = HERE / "liboracle.so"
+REF_SO = HERE / "_ref" / "libhytref.so"
+
+u64p = C.POINTER(C.c_uint64)
+
+
+def build(quiet: bool = True) -> None:
+    """Compile liboracle.so (and _ref when the reference sources exist)."""
+    subprocess.run(["make", "-C", str(HERE)], check=True,
+                   stdout=subprocess.DEVNULL if quiet else None)
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class HytmOptions(C.Structure):
+    _fields_ = [("alpha", C.c_double), ("beta", C.c_double), ("gamma", C.c_double), ("rtt", C.c_double),
+                ("cpu_throughput", C.c_double), ("m", C.c_uint64), ("mr", C.c_uint64), ("d1", C.c_uint64),
+                ("d2", C.c_uint64), ("align", C.c_uint64)]
+
+
+class HytmCosts(C.Structure):
+    _fields_ = [("active_vertices", C.c_uint64), ("active_edges", C.c_uint64), ("total_edges", C.c_uint64),
+                ("filter_bytes", C.c_uint64), ("compaction_bytes", C.c_uint64), ("zc_requests", C.c_uint64),
+                ("zc_alignment", C.c_uint64), ("filter_cost", C.c_double), ("compaction_cost", C.c_double),
+                ("zero_copy_cost", C.c_double), ("zc_rtt", C.c_double), ("engine", C.c_int)]
+
+
+class Oracle:
+    def __init__(self):
+        if not ORACLE_SO.exists():
+            build()
+        self.lib = C.CDLL(str(ORACLE_SO))
+
+    def pagerank_f32(self, off, cols, damping=0.85, tol=1e-6, max_iter=100):
+        V, E = off.shape[0] - 1, cols.shape[0]
+        r = np.empty(V, np.float32)
+        it, res, conv = C.c_uint64(), C.c_float(), C.c_int()
+        rc = self.lib.oracle_pagerank_f32(C.c_uint64(V), C.c_uint64(E), _p(off), _p(cols), C.c_float(damping),
+                                          C.c_float(tol), C.c_uint64(max_iter), _p(r), C.byref(it), C.byref(res),
+                                          C.byref(conv))
+        if rc:
+            raise ValueError(f"oracle_pagerank_f32 rc={rc}")
+        return r, it.value, res.value, bool(conv.value)
+
+    def pagerank_f64(self, off, cols, damping=0.85, tol=1e-6, max_iter=100):
+        V, E = off.shape[0] - 1, cols.shape[0]
+        r = np.empty(V, np.float64)
+        it, res, conv = C.c_uint64(), C.c_double(), C.c_int()
+        rc = self.lib.oracle_pagerank_f64(C.c_uint64(V), C.c_uint64(E), _p(off), _p(cols), C.c_double(damping),
+                                          C.c_double(tol), C.c_uint64(max_iter), _p(r), C.byref(it), C.byref(res),
+                                          C.byref(conv))
+        if rc:
+            raise ValueError(f"oracle_pagerank_f64 rc={rc}")
+        return r, it.value, res.value, bool(conv.value)
+
+    def ppr_f64(self, off, cols, source, restart=0.15, tol=1e-6, max_iter=100):
+        V, E = off.shape[0] - 1, cols.shape[0]
+        r = np.empty(V, np.float64)
+        it, res, conv = C.c_uint64(), C.c_double(), C.c_int()
+        rc = self.lib.oracle_ppr_f64(C.c_uint64(V), C.c_uint64(E), _p(off), _p(cols), C.c_uint32(source),
+                                     C.c_double(restart), C.c_double(tol), C.c_uint64(max_iter), _p(r),
+                                     C.byref(it), C.byref(res), C.byref(conv))
+        if rc:
+            raise ValueError(f"oracle_ppr_f64 rc={rc}")
+        return r, it.value, res.value, bool(conv.value)
+
+    def sssp(self, off, cols, weights_f32, source, max_iter=0):
+        V, E = off.shape[0] - 1, cols.shape[0]
+        d = np.empty(V, np.float32)
+        it, conv = C.c_uint64(), C.c_int()
+        rc = self.lib.oracle_sssp(C.c_uint64(V), C.c_uint64(E), _p(off), _p(cols), _p(weights_f32),
+                                  C.c_uint32(source), C.c_uint64(max_iter), _p(d), C.byref(it), C.byref(conv))
+        if rc:
+            raise ValueError(f"oracle_sssp rc={rc}")
+        return d, it.value, bool(conv.value)
+
+    def dijkstra(self, off, cols, weights_u32, source):
+        V, E = off.shape[0] - 1, cols.shape[0]
+        d = np.empty(V, np.uint64)
+        rc = self.lib.oracle_dijkstra_u32(C.c_uint64(V), C.c_uint64(E), _p(off), _p(cols), _p(weights_u32),
+                                          C.c_uint32(source), _p(d))
+        if rc:
+            raise ValueError(f"oracle_dijkstra_u32 rc={rc}")
+        return d
+
+    def hytm_partition(self, off, active_u8, vbegin, vend, opts: HytmOptions) -> HytmCosts:
+        c = HytmCosts()
+        self.lib.oracle_hytm_partition(_p(off), _p(active_u8), C.c_uint32(vbegin), C.c_uint32(vend),
+                                       C.byref(opts), C.byref(c))
+        return c
+
+    def select_engine(self, f, c, z, alpha, beta) -> int:
+        self.lib.oracle_select_engine.restype = C.c_int
+        return self.lib.oracle_select_engine(C.c_double(f), C.c_double(c), C.c_double(z), C.c_double(alpha),
+                                             C.c_double(beta))
+
+    def task_combine(self, engines, k):
+        e = np.ascontiguousarray(engines, dtype=np.int32)
+        n = e.shape[0]
+        top = np.zeros(max(n, 1), np.uint64)
+        teng = np.zeros(max(n, 1) + 2, np.int32)
+        tfirst = np.zeros(max(n, 1) + 2, np.uint64)
+        self.lib.oracle_task_combine.restype = C.c_uint64
+        nt = self.lib.oracle_task_combine(_p(e), C.c_uint64(n), C.c_uint64(k), _p(top), _p(teng), _p(tfirst))
+        return top[:n], teng[:nt], tfirst[:nt]
+
+
+class Reference:
+    """The reference's own CPU implementation (oracle/_ref/libhytref.so)."""
+
+    def __init__(self):
+        if not REF_SO.exists():
+            raise FileNotFoundError(f"{REF_SO} not built (needs the reference sources)")
+        self.lib = C.CDLL(str(REF_SO))
+        self.lib.ref_last_error.restype = C.c_char_p
+
+    @staticmethod
+    def available() -> bool:
+        return REF_SO.exists()
+
+    def _check(self, rc, what):
+        if rc:
+            raise ValueError(f"{what} rc={rc}: {self.lib.ref_last_error().decode()}")
+
+    def pagerank_cpu(self, off, cols, damping=0.85, tol=1e-6, max_iter=100):
+        V, E = off.shape[0] - 1, cols.shape[0]
+        r = np.empty(V, np.float32)
+        it, res, conv = C.c_uint64(), C.c_float(), C.c_int()
+        self._check(self.lib.ref_pagerank_cpu(C.c_uint64(V), C.c_uint64(E), _p(off), _p(cols), C.c_float(damping),
+                                              C.c_float(tol), C.c_uint64(max_iter), _p(r), C.byref(it),
+                                              C.byref(res), C.byref(conv)), "ref_pagerank_cpu")
+        return r, it.value, res.value, bool(conv.value)
+
+    def sssp_cpu(self, off, cols, weights_f32, source, max_iter=0):
+        V, E = off.shape[0] - 1, cols.shape[0]
+        d = np.empty(V, np.float32)
+        it, conv = C.c_uint64(), C.c_int()
+        self._check(self.lib.ref_sssp_cpu(C.c_uint64(V), C.c_uint64(E), _p(off), _p(cols), _p(weights_f32),
+                                          C.c_uint32(source), C.c_uint64(max_iter), _p(d), C.byref(it),
+                                          C.byref(conv)), "ref_sssp_cpu")
+        return d, it.value, bool(conv.value)
+
+    def hytm_evaluate(self, off, cols, active_u8, parts, dopts, uopts):
+        V, E = off.shape[0] - 1, cols.shape[0]
+        parts = np.ascontiguousarray(parts, np.uint32)
+        n = parts.shape[0]
+        metrics = np.zeros((n, 11), np.uint64)
+        costs = np.zeros((n, 4), np.float64)
+        eng = np.zeros(n, np.int32)
+        self._check(self.lib.ref_hytm_evaluate(C.c_uint64(V), C.c_uint64(E), _p(off), _p(cols), _p(active_u8),
+                                               C.c_uint64(n), _p(parts), _p(np.asarray(dopts, np.float64)),
+                                               _p(np.asarray(uopts, np.uint64)), _p(metrics), _p(costs), _p(eng)),
+                    "ref_hytm_evaluate")
+        return metrics, costs, eng
+
+    def select_engine(self, f, c, z, alpha, beta) -> int:
+        e = C.c_int()
+        self._check(self.lib.ref_select_engine(C.c_double(f), C.c_double(c), C.c_double(z), C.c_double(alpha),
+                                               C.c_double(beta), C.byref(e)), "ref_select_engine")
+        return e.value
+
+    def task_combine(self, engines, k):
+        e = np.ascontiguousarray(engines, dtype=np.int32)
+        n = e.shape[0]
+        top = np.zeros(max(n, 1), np.uint64)
+        teng = np.zeros(max(n, 1) + 2, np.int32)
+        tfirst = np.zeros(max(n, 1) + 2, np.uint64)
+        nt = C.c_uint64()
+        metrics = np.zeros(5, np.uint64)
+        self._check(self.lib.ref_task_combine(_p(e), C.c_uint64(n), C.c_uint64(k), _p(top), _p(teng), _p(tfirst),
+                                              C.byref(nt), _p(metrics)), "ref_task_combine")
+        return top[:n], teng[:nt.value], tfirst[:nt.value], metrics

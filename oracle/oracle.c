@@ -1,0 +1,378 @@
+/*
+ * oracle.c -- CPU restatement of the reference's algorithms for the hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Only tests/, __graft_entry__.smoke() and the
+ * cpu_baseline leg of bench.py load this library, as the checker.  The
+ * product (hytgraph_b200) never links or calls it.
+ *
+ * Parity pin: every routine here is checked against the reference's own
+ * compiled sources (oracle/_ref, built by oracle/Makefile from
+ * src/algorithms/{pagerank,sssp}.cpp) and against the reference's
+ * known-answer tests (tests/algorithm_tests.cpp:22-157,
+ * tests/cuda_algorithm_tests.cu:23-87, tests/unit_tests.cpp:2058-2204),
+ * frozen as fixtures in tests/golden/.
+ *
+ * Each function names the reference lines it restates.
+ */
+#include "oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* Incoming CSR (CSC) with sources in ascending order inside each row,
+ * built with the same counting pass as src/algorithms/pagerank.cpp:19-60
+ * (and sssp.cpp:21-80, which also carries the weights). */
+static int build_incoming(uint64_t V, uint64_t E, const uint64_t *off, const uint32_t *cols, const float *w_in,
+                          uint64_t **in_off_out, uint32_t **in_src_out, float **in_w_out) {
+    uint64_t *in_off = (uint64_t *)calloc(V + 1, sizeof(uint64_t));
+    uint32_t *in_src = (uint32_t *)malloc((E ? E : 1) * sizeof(uint32_t));
+    float *in_w = in_w_out ? (float *)malloc((E ? E : 1) * sizeof(float)) : NULL;
+    uint64_t *cursor = (uint64_t *)malloc((V + 1) * sizeof(uint64_t));
+    if (!in_off || !in_src || !cursor || (in_w_out && !in_w)) {
+        free(in_off); free(in_src); free(in_w); free(cursor);
+        return ORACLE_E_NOMEM;
+    }
+    for (uint64_t u = 0; u < V; ++u)
+        for (uint64_t e = off[u]; e < off[u + 1]; ++e) ++in_off[cols[e] + 1];
+    for (uint64_t v = 1; v <= V; ++v) in_off[v] += in_off[v - 1];
+    memcpy(cursor, in_off, (V + 1) * sizeof(uint64_t));
+    for (uint64_t u = 0; u < V; ++u)
+        for (uint64_t e = off[u]; e < off[u + 1]; ++e) {
+            const uint64_t pos = cursor[cols[e]]++;
+            in_src[pos] = (uint32_t)u;
+            if (in_w) in_w[pos] = w_in ? w_in[e] : 1.0f;
+        }
+    free(cursor);
+    *in_off_out = in_off;
+    *in_src_out = in_src;
+    if (in_w_out) *in_w_out = in_w;
+    return ORACLE_OK;
+}
+
+/* src/algorithms/pagerank.cpp:62-85 */
+static int pr_validate(uint64_t V, float damping, float tol, uint64_t max_iter) {
+    if (V == 0) return ORACLE_E_INVALID;
+    if (!(damping >= 0.0f && damping < 1.0f)) return ORACLE_E_INVALID;
+    if (!(tol > 0.0f) || !isfinite(tol)) return ORACLE_E_INVALID;
+    if (max_iter == 0) return ORACLE_E_INVALID;
+    return ORACLE_OK;
+}
+
+/* FP32 restatement of pagerank_cpu, src/algorithms/pagerank.cpp:89-163:
+ * same operation order, so it reproduces the reference bit for bit. */
+int oracle_pagerank_f32(uint64_t V, uint64_t E, const uint64_t *off, const uint32_t *cols, float damping,
+                        float tol, uint64_t max_iter, float *ranks, uint64_t *iterations, float *residual_out,
+                        int *converged) {
+    int rc = pr_validate(V, damping, tol, max_iter);
+    if (rc) return rc;
+    uint64_t *in_off;
+    uint32_t *in_src;
+    rc = build_incoming(V, E, off, cols, NULL, &in_off, &in_src, NULL);
+    if (rc) return rc;
+    const float n = (float)V;
+    const float base = (1.0f - damping) / n;
+    float *cur = (float *)malloc(V * sizeof(float)), *nxt = (float *)malloc(V * sizeof(float));
+    if (!cur || !nxt) { free(cur); free(nxt); free(in_off); free(in_src); return ORACLE_E_NOMEM; }
+    for (uint64_t v = 0; v < V; ++v) cur[v] = 1.0f / n;
+    *iterations = 0; *residual_out = 0.0f; *converged = 0;
+    memcpy(ranks, cur, V * sizeof(float));
+    for (uint64_t it = 0; it < max_iter; ++it) {
+        float dangling = 0.0f;
+        for (uint64_t u = 0; u < V; ++u)
+            if (off[u + 1] == off[u]) dangling += cur[u];
+        const float dshare = damping * dangling / n;
+        float residual = 0.0f;
+        for (uint64_t v = 0; v < V; ++v) {
+            float sum = 0.0f;
+            for (uint64_t p = in_off[v]; p < in_off[v + 1]; ++p) {
+                const uint32_t u = in_src[p];
+                const uint64_t deg = off[u + 1] - off[u];
+                if (deg != 0) sum += cur[u] / (float)deg;
+            }
+            nxt[v] = base + dshare + damping * sum;
+            residual += fabsf(nxt[v] - cur[v]);
+        }
+        float *t = cur; cur = nxt; nxt = t;
+        *iterations = it + 1;
+        *residual_out = residual;
+        memcpy(ranks, cur, V * sizeof(float));
+        if (residual <= tol) { *converged = 1; break; }
+    }
+    free(cur); free(nxt); free(in_off); free(in_src);
+    return ORACLE_OK;
+}
+
+/* FP64 restatement of the same iteration (pagerank.cpp:89-163 in double):
+ * x0 = 1/n; x' = (1-d)/n + d*dangling/n + d*sum x_u/deg_u; stop when the L1
+ * change <= tol.  This is the accuracy reference for the FP32 solvers. */
+int oracle_pagerank_f64(uint64_t V, uint64_t E, const uint64_t *off, const uint32_t *cols, double damping,
+                        double tol, uint64_t max_iter, double *ranks, uint64_t *iterations, double *residual_out,
+                        int *converged) {
+    if (V == 0 || !(damping >= 0.0 && damping < 1.0) || !(tol > 0.0) || max_iter == 0) return ORACLE_E_INVALID;
+    uint64_t *in_off;
+    uint32_t *in_src;
+    int rc = build_incoming(V, E, off, cols, NULL, &in_off, &in_src, NULL);
+    if (rc) return rc;
+    const double n = (double)V, base = (1.0 - damping) / n;
+    double *cur = (double *)malloc(V * sizeof(double)), *nxt = (double *)malloc(V * sizeof(double));
+    double *contrib = (double *)malloc(V * sizeof(double));
+    if (!cur || !nxt || !contrib) { free(cur); free(nxt); free(contrib); free(in_off); free(in_src); return ORACLE_E_NOMEM; }
+    for (uint64_t v = 0; v < V; ++v) cur[v] = 1.0 / n;
+    *iterations = 0; *residual_out = 0.0; *converged = 0;
+    memcpy(ranks, cur, V * sizeof(double));
+    for (uint64_t it = 0; it < max_iter; ++it) {
+        double dangling = 0.0;
+        for (uint64_t u = 0; u < V; ++u) {
+            const uint64_t deg = off[u + 1] - off[u];
+            if (deg == 0) dangling += cur[u];
+            contrib[u] = deg ? cur[u] / (double)deg : 0.0;
+        }
+        const double dshare = damping * dangling / n;
+        double residual = 0.0;
+        for (uint64_t v = 0; v < V; ++v) {
+            double sum = 0.0;
+            for (uint64_t p = in_off[v]; p < in_off[v + 1]; ++p) sum += contrib[in_src[p]];
+            nxt[v] = base + dshare + damping * sum;
+            residual += fabs(nxt[v] - cur[v]);
+        }
+        double *t = cur; cur = nxt; nxt = t;
+        *iterations = it + 1;
+        *residual_out = residual;
+        if (residual <= tol) { *converged = 1; break; }
+    }
+    memcpy(ranks, cur, V * sizeof(double));
+    free(cur); free(nxt); free(contrib); free(in_off); free(in_src);
+    return ORACLE_OK;
+}
+
+/* Personalized PageRank in FP64 (no reference counterpart; defined by this
+ * project on the structure of pagerank.cpp:89-163):
+ *   x0 = e_s;  x'[v] = d * sum_{u->v} x_u/deg_u + [v == s] * ((1-d) + d*dangling)
+ * with d = 1 - restart and dangling = sum of x over out-degree-0 vertices
+ * (dangling mass returns to the source); stop when the L1 change <= tol. */
+int oracle_ppr_f64(uint64_t V, uint64_t E, const uint64_t *off, const uint32_t *cols, uint32_t source,
+                   double restart, double tol, uint64_t max_iter, double *ranks, uint64_t *iterations,
+                   double *residual_out, int *converged) {
+    if (V == 0 || source >= V || !(restart > 0.0 && restart <= 1.0) || !(tol > 0.0) || max_iter == 0)
+        return ORACLE_E_INVALID;
+    uint64_t *in_off;
+    uint32_t *in_src;
+    int rc = build_incoming(V, E, off, cols, NULL, &in_off, &in_src, NULL);
+    if (rc) return rc;
+    const double d = 1.0 - restart;
+    double *cur = (double *)calloc(V, sizeof(double)), *nxt = (double *)malloc(V * sizeof(double));
+    double *contrib = (double *)malloc(V * sizeof(double));
+    if (!cur || !nxt || !contrib) { free(cur); free(nxt); free(contrib); free(in_off); free(in_src); return ORACLE_E_NOMEM; }
+    cur[source] = 1.0;
+    *iterations = 0; *residual_out = 0.0; *converged = 0;
+    for (uint64_t it = 0; it < max_iter; ++it) {
+        double dangling = 0.0;
+        for (uint64_t u = 0; u < V; ++u) {
+            const uint64_t deg = off[u + 1] - off[u];
+            if (deg == 0) dangling += cur[u];
+            contrib[u] = deg ? cur[u] / (double)deg : 0.0;
+        }
+        double residual = 0.0;
+        for (uint64_t v = 0; v < V; ++v) {
+            double sum = 0.0;
+            for (uint64_t p = in_off[v]; p < in_off[v + 1]; ++p) sum += contrib[in_src[p]];
+            nxt[v] = d * sum + (v == source ? (1.0 - d) + d * dangling : 0.0);
+            residual += fabs(nxt[v] - cur[v]);
+        }
+        double *t = cur; cur = nxt; nxt = t;
+        *iterations = it + 1;
+        *residual_out = residual;
+        if (residual <= tol) { *converged = 1; break; }
+    }
+    memcpy(ranks, cur, V * sizeof(double));
+    free(cur); free(nxt); free(contrib); free(in_off); free(in_src);
+    return ORACLE_OK;
+}
+
+/* FP32 restatement of sssp_cpu, src/algorithms/sssp.cpp:109-234: synchronous
+ * Bellman-Ford pulling over in-edges from sources active in the previous
+ * round; weights NULL means 1.0 per edge.  max_iter 0 selects V. */
+int oracle_sssp(uint64_t V, uint64_t E, const uint64_t *off, const uint32_t *cols, const float *weights,
+                uint32_t source, uint64_t max_iter, float *dist, uint64_t *iterations, int *converged) {
+    if (V == 0 || source >= V) return ORACLE_E_INVALID;
+    if (weights)
+        for (uint64_t e = 0; e < E; ++e)
+            if (!isfinite(weights[e]) || weights[e] < 0.0f) return ORACLE_E_INVALID;
+    uint64_t *in_off;
+    uint32_t *in_src;
+    float *in_w;
+    int rc = build_incoming(V, E, off, cols, weights, &in_off, &in_src, &in_w);
+    if (rc) return rc;
+    float *cur = (float *)malloc(V * sizeof(float)), *nxt = (float *)malloc(V * sizeof(float));
+    unsigned char *active = (unsigned char *)calloc(V, 1), *next_active = (unsigned char *)calloc(V, 1);
+    if (!cur || !nxt || !active || !next_active) {
+        free(cur); free(nxt); free(active); free(next_active); free(in_off); free(in_src); free(in_w);
+        return ORACLE_E_NOMEM;
+    }
+    for (uint64_t v = 0; v < V; ++v) cur[v] = INFINITY;
+    cur[source] = 0.0f;
+    active[source] = 1;
+    if (max_iter == 0) max_iter = V;
+    *iterations = 0; *converged = 0;
+    for (uint64_t it = 0; it < max_iter; ++it) {
+        memcpy(nxt, cur, V * sizeof(float));
+        memset(next_active, 0, V);
+        int changed = 0;
+        for (uint64_t v = 0; v < V; ++v) {
+            float best = cur[v];
+            for (uint64_t p = in_off[v]; p < in_off[v + 1]; ++p) {
+                const uint32_t u = in_src[p];
+                if (!active[u] || !isfinite(cur[u])) continue;
+                const float cand = cur[u] + in_w[p];
+                if (cand < best) best = cand;
+            }
+            nxt[v] = best;
+            if (best < cur[v]) { next_active[v] = 1; changed = 1; }
+        }
+        float *t = cur; cur = nxt; nxt = t;
+        unsigned char *ta = active; active = next_active; next_active = ta;
+        *iterations = it + 1;
+        if (!changed) { *converged = 1; break; }
+    }
+    memcpy(dist, cur, V * sizeof(float));
+    free(cur); free(nxt); free(active); free(next_active); free(in_off); free(in_src); free(in_w);
+    return ORACLE_OK;
+}
+
+/* Independent cross-check: Dijkstra with exact 64-bit integer distances on
+ * uint32 weights (NULL = unit weights); UINT64_MAX marks unreachable. */
+typedef struct { uint64_t d; uint32_t v; } heap_item;
+
+static void heap_push(heap_item *h, uint64_t *n, heap_item x) {
+    uint64_t i = (*n)++;
+    while (i > 0) {
+        uint64_t p = (i - 1) / 2;
+        if (h[p].d <= x.d) break;
+        h[i] = h[p];
+        i = p;
+    }
+    h[i] = x;
+}
+
+static heap_item heap_pop(heap_item *h, uint64_t *n) {
+    heap_item top = h[0], x = h[--(*n)];
+    uint64_t i = 0;
+    for (;;) {
+        uint64_t c = 2 * i + 1;
+        if (c >= *n) break;
+        if (c + 1 < *n && h[c + 1].d < h[c].d) ++c;
+        if (h[c].d >= x.d) break;
+        h[i] = h[c];
+        i = c;
+    }
+    if (*n) h[i] = x;
+    return top;
+}
+
+int oracle_dijkstra_u32(uint64_t V, uint64_t E, const uint64_t *off, const uint32_t *cols, const uint32_t *weights,
+                        uint32_t source, uint64_t *dist) {
+    if (V == 0 || source >= V) return ORACLE_E_INVALID;
+    heap_item *h = (heap_item *)malloc((E + 1) * sizeof(heap_item));
+    if (!h) return ORACLE_E_NOMEM;
+    for (uint64_t v = 0; v < V; ++v) dist[v] = UINT64_MAX;
+    uint64_t n = 0;
+    dist[source] = 0;
+    heap_push(h, &n, (heap_item){0, source});
+    while (n) {
+        heap_item t = heap_pop(h, &n);
+        if (t.d != dist[t.v]) continue;
+        for (uint64_t e = off[t.v]; e < off[t.v + 1]; ++e) {
+            const uint64_t nd = t.d + (weights ? weights[e] : 1u);
+            if (nd < dist[cols[e]]) {
+                dist[cols[e]] = nd;
+                heap_push(h, &n, (heap_item){nd, cols[e]});
+            }
+        }
+    }
+    free(h);
+    return ORACLE_OK;
+}
+
+/* HyTM per-partition metrics and costs: restates
+ * src/transfer/hytm_cost_model.cpp:330-452 (metrics), :454-484 (RTT_zc),
+ * :511-615 (formulas 1-3) and :649-715 (strict selector).
+ * Options: d1 = dest bytes, d2 = index bytes, m = payload, mr = requests per
+ * TLP, align = alignment bytes. */
+void oracle_hytm_partition(const uint64_t *off, const unsigned char *active, uint32_t vbegin, uint32_t vend,
+                           const oracle_hytm_options *o, oracle_hytm_costs *c) {
+    memset(c, 0, sizeof(*c));
+    c->total_edges = off[vend] - off[vbegin];
+    c->filter_bytes = c->total_edges * o->d1;
+    for (uint32_t v = vbegin; v < vend; ++v) {
+        if (!active[v]) continue;
+        const uint64_t deg = off[v + 1] - off[v];
+        c->active_vertices += 1;
+        c->active_edges += deg;
+        if (deg == 0) continue;
+        c->zc_requests += (deg * o->d1 + o->m - 1) / o->m;
+        if ((off[v] * o->d1) % o->align != 0) c->zc_alignment += 1;
+    }
+    c->compaction_bytes = c->active_edges * o->d1 + c->active_vertices * o->d2;
+    const uint64_t tlp_bytes = o->m * o->mr;
+    const uint64_t zc_total = c->zc_requests + c->zc_alignment;
+    c->filter_cost = (double)((c->filter_bytes + tlp_bytes - 1) / tlp_bytes) * o->rtt;
+    c->compaction_cost = (double)((c->compaction_bytes + tlp_bytes - 1) / tlp_bytes) * o->rtt +
+                         (double)c->compaction_bytes / o->cpu_throughput;
+    c->zc_rtt = c->total_edges == 0 ? o->gamma * o->rtt
+                                    : o->gamma * o->rtt +
+                                          (1.0 - o->gamma) * ((double)c->active_edges / (double)c->total_edges) * o->rtt;
+    c->zero_copy_cost = (double)((zc_total + o->mr - 1) / o->mr) * c->zc_rtt;
+    c->engine = oracle_select_engine(c->filter_cost, c->compaction_cost, c->zero_copy_cost, o->alpha, o->beta);
+}
+
+int oracle_select_engine(double f, double c, double z, double alpha, double beta) {
+    if (c < alpha * f && c < beta * z) return ORACLE_ENGINE_COMPACTION;
+    if (f < z) return ORACLE_ENGINE_FILTER;
+    return ORACLE_ENGINE_ZERO_COPY;
+}
+
+/* Task combining, src/scheduling/task_combiner.cpp:67-248: consecutive
+ * Filter partitions in groups of <= k, then one Compaction task and one
+ * Zero-Copy task, all ordered by first partition.  Writes, per partition,
+ * the index of its task; returns the number of tasks. */
+uint64_t oracle_task_combine(const int *engines, uint64_t n, uint64_t k, uint64_t *task_of_partition,
+                             int *task_engine, uint64_t *task_first) {
+    /* first pass: task ids in creation order */
+    uint64_t ntask = 0, comp_first = UINT64_MAX, zc_first = UINT64_MAX;
+    uint64_t *tmp_first = (uint64_t *)malloc((n + 2) * sizeof(uint64_t));
+    int *tmp_engine = (int *)malloc((n + 2) * sizeof(int));
+    uint64_t *tmp_task = (uint64_t *)malloc((n ? n : 1) * sizeof(uint64_t));
+    for (uint64_t i = 0; i < n;) {
+        if (engines[i] == ORACLE_ENGINE_FILTER) {
+            uint64_t g = 0;
+            tmp_first[ntask] = i;
+            tmp_engine[ntask] = ORACLE_ENGINE_FILTER;
+            while (i < n && engines[i] == ORACLE_ENGINE_FILTER && g < k) { tmp_task[i++] = ntask; ++g; }
+            ++ntask;
+        } else {
+            if (engines[i] == ORACLE_ENGINE_COMPACTION && comp_first == UINT64_MAX) comp_first = i;
+            if (engines[i] == ORACLE_ENGINE_ZERO_COPY && zc_first == UINT64_MAX) zc_first = i;
+            tmp_task[i] = UINT64_MAX;
+            ++i;
+        }
+    }
+    const uint64_t comp_task = comp_first != UINT64_MAX ? ntask++ : UINT64_MAX;
+    if (comp_task != UINT64_MAX) { tmp_first[comp_task] = comp_first; tmp_engine[comp_task] = ORACLE_ENGINE_COMPACTION; }
+    const uint64_t zc_task = zc_first != UINT64_MAX ? ntask++ : UINT64_MAX;
+    if (zc_task != UINT64_MAX) { tmp_first[zc_task] = zc_first; tmp_engine[zc_task] = ORACLE_ENGINE_ZERO_COPY; }
+    for (uint64_t i = 0; i < n; ++i)
+        if (tmp_task[i] == UINT64_MAX) tmp_task[i] = engines[i] == ORACLE_ENGINE_COMPACTION ? comp_task : zc_task;
+    /* rank tasks by first partition (all distinct) */
+    uint64_t *rank = (uint64_t *)malloc((ntask ? ntask : 1) * sizeof(uint64_t));
+    for (uint64_t t = 0; t < ntask; ++t) {
+        uint64_t r = 0;
+        for (uint64_t s = 0; s < ntask; ++s) r += tmp_first[s] < tmp_first[t];
+        rank[t] = r;
+        task_engine[r] = tmp_engine[t];
+        task_first[r] = tmp_first[t];
+    }
+    for (uint64_t i = 0; i < n; ++i) task_of_partition[i] = rank[tmp_task[i]];
+    free(rank); free(tmp_first); free(tmp_engine); free(tmp_task);
+    return ntask;
+}

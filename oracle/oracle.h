@@ -1,0 +1,51 @@
+/* oracle.h -- CPU restatement of the reference algorithms (test
+ * infrastructure only; see oracle.c). */
+#ifndef HYT_ORACLE_H
+#define HYT_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { ORACLE_OK = 0, ORACLE_E_INVALID = 1, ORACLE_E_NOMEM = 2 };
+enum { ORACLE_ENGINE_FILTER = 0, ORACLE_ENGINE_COMPACTION = 1, ORACLE_ENGINE_ZERO_COPY = 2 };
+
+int oracle_pagerank_f32(uint64_t V, uint64_t E, const uint64_t *off, const uint32_t *cols, float damping,
+                        float tol, uint64_t max_iter, float *ranks, uint64_t *iterations, float *residual,
+                        int *converged);
+int oracle_pagerank_f64(uint64_t V, uint64_t E, const uint64_t *off, const uint32_t *cols, double damping,
+                        double tol, uint64_t max_iter, double *ranks, uint64_t *iterations, double *residual,
+                        int *converged);
+int oracle_ppr_f64(uint64_t V, uint64_t E, const uint64_t *off, const uint32_t *cols, uint32_t source,
+                   double restart, double tol, uint64_t max_iter, double *ranks, uint64_t *iterations,
+                   double *residual, int *converged);
+int oracle_sssp(uint64_t V, uint64_t E, const uint64_t *off, const uint32_t *cols, const float *weights,
+                uint32_t source, uint64_t max_iter, float *dist, uint64_t *iterations, int *converged);
+int oracle_dijkstra_u32(uint64_t V, uint64_t E, const uint64_t *off, const uint32_t *cols, const uint32_t *weights,
+                        uint32_t source, uint64_t *dist);
+
+typedef struct {
+    double alpha, beta, gamma, rtt, cpu_throughput;
+    uint64_t m, mr, d1, d2, align;
+} oracle_hytm_options;
+
+typedef struct {
+    uint64_t active_vertices, active_edges, total_edges;
+    uint64_t filter_bytes, compaction_bytes, zc_requests, zc_alignment;
+    double filter_cost, compaction_cost, zero_copy_cost, zc_rtt;
+    int engine;
+} oracle_hytm_costs;
+
+void oracle_hytm_partition(const uint64_t *off, const unsigned char *active, uint32_t vbegin, uint32_t vend,
+                           const oracle_hytm_options *o, oracle_hytm_costs *c);
+int oracle_select_engine(double f, double c, double z, double alpha, double beta);
+uint64_t oracle_task_combine(const int *engines, uint64_t n, uint64_t k, uint64_t *task_of_partition,
+                             int *task_engine, uint64_t *task_first);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

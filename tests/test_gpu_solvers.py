@@ -1,0 +1,211 @@
+"""GPU parity: the CUDA path through the C ABI against the oracle.
+
+Tolerances: PageRank / personalized PageRank L1 <= 1e-5 against the FP64
+oracle (the bar the path is specified to), SSSP bit-exact.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+PR_L1_TOL = 1e-5
+
+
+def _graph_cases(hyt):
+    cases = [hyt.rmat(s, ef, seed) for s, ef, seed in [(8, 16, 1), (10, 8, 2), (12, 16, 3), (14, 16, 4), (16, 16, 5)]]
+    cases.append(hyt.rmat(11, 4, 6, 0, 0))  # unweighted, many dangling vertices
+    return cases
+
+
+def _csr(off, cols, w=None):
+    import hytgraph_b200 as hyt
+
+    return hyt.CSR(np.asarray(off, np.uint64), np.asarray(cols, np.uint32), None if w is None else np.asarray(w))
+
+
+def _special_graphs():
+    """Edge cases: single vertex, all dangling, 3-cycle, a hub with in- and
+    out-degree > 4096 (chunked long rows / hub tasks), warp-sized rows."""
+    out = [
+        _csr([0, 0], []),
+        _csr([0, 0, 0, 0, 0], []),
+        _csr([0, 1, 2, 3], [1, 2, 0], [1, 1, 1]),
+        _csr([0, 2, 3, 4], [1, 2, 2, 0], [3, 4, 5, 6]),
+    ]
+    n = 20000  # star in and out of vertex 0
+    off = np.concatenate([[0, n - 1], np.arange(n - 1) + n]).astype(np.uint64)
+    cols = np.concatenate([np.arange(1, n), np.zeros(n - 1)]).astype(np.uint32)
+    w = (np.arange(cols.shape[0]) % 63 + 1).astype(np.uint32)
+    out.append(_csr(off, cols, w))
+    rng = np.random.default_rng(0)  # rows of 30-40 edges hit the warp path
+    V = 3000
+    deg = rng.integers(0, 40, V)
+    off = np.concatenate([[0], np.cumsum(deg)]).astype(np.uint64)
+    cols = rng.integers(0, V, int(off[-1])).astype(np.uint32)
+    out.append(_csr(off, cols, rng.integers(1, 64, cols.shape[0]).astype(np.uint32)))
+    return out
+
+
+def test_pagerank_matches_fp64_oracle(hyt, oracle, gpu):
+    for g in _graph_cases(hyt) + _special_graphs():
+        ref, it_ref, _, conv_ref = oracle.pagerank_f64(g.row_offsets, g.column_indices)
+        with hyt.Graph(g) as dg:
+            r, st = dg.pagerank()
+        l1 = float(np.abs(r.astype(np.float64) - ref).sum())
+        assert l1 <= PR_L1_TOL, (g.num_vertices, l1, st)
+        assert st["converged"] == conv_ref
+        assert abs(st["iterations"] - it_ref) <= 1, (st["iterations"], it_ref)
+
+
+def test_pagerank_deterministic_across_modes(hyt, gpu):
+    g = hyt.rmat(15, 16, 11)
+    with hyt.Graph(g) as dg:
+        a, sa = dg.pagerank()
+        b, sb = dg.pagerank(flags=hyt.capi.HYT_RUN_NO_GRAPH)
+        c, sc = dg.pagerank(flags=hyt.capi.HYT_RUN_PROFILE)
+        d, _ = dg.pagerank()
+    assert sa["iterations"] == sb["iterations"] == sc["iterations"]
+    for x in (b, c, d):
+        assert np.array_equal(a.view(np.uint32), x.view(np.uint32))
+    assert sc["kernel_launches"] == sc["iterations"] and sc["kernel_ms"] > 0
+
+
+def test_pagerank_max_iterations_and_errors(hyt, oracle, gpu):
+    g = hyt.rmat(10, 8, 2)
+    ref, _, _, _ = oracle.pagerank_f64(g.row_offsets, g.column_indices, tol=1e-30, max_iter=3)
+    with hyt.Graph(g) as dg:
+        r, st = dg.pagerank(tolerance=1e-30, max_iterations=3)
+        assert st["iterations"] == 3 and not st["converged"]
+        assert np.abs(r - ref).sum() <= PR_L1_TOL
+        for kw in ({"damping": 1.0}, {"tolerance": 0.0}, {"max_iterations": 0}):
+            with pytest.raises(hyt.HytError) as e:
+                dg.pagerank(**kw)
+            assert e.value.code == hyt.capi.HYT_E_INVALID
+
+
+def test_ppr_matches_fp64_oracle(hyt, oracle, gpu):
+    for g in _graph_cases(hyt)[:5]:
+        with hyt.Graph(g) as dg:
+            for s in hyt.pick_sources(g.row_offsets, 3, 3):
+                ref, it_ref, _, _ = oracle.ppr_f64(g.row_offsets, g.column_indices, int(s))
+                r, st = dg.ppr(int(s))
+                l1 = float(np.abs(r.astype(np.float64) - ref).sum())
+                assert l1 <= PR_L1_TOL, (g.num_vertices, int(s), l1)
+                assert abs(st["iterations"] - it_ref) <= 1
+
+
+def test_sssp_bit_exact(hyt, oracle, gpu):
+    for g in _graph_cases(hyt) + _special_graphs():
+        V = g.num_vertices
+        srcs = hyt.pick_sources(g.row_offsets, 9, 3) if g.num_edges else np.zeros(1, np.uint32)
+        w32 = None if g.weights is None else g.weights.astype(np.float32)
+        with hyt.Graph(g) as dg:
+            for s in srcs:
+                d, st = dg.sssp(int(s))
+                ref, _, _ = oracle.sssp(g.row_offsets, g.column_indices, w32, int(s))
+                want = np.where(np.isfinite(ref), ref, 0).astype(np.uint64)
+                want = np.where(np.isfinite(ref), want, 0xFFFFFFFF).astype(np.uint32)
+                assert np.array_equal(d, want), (V, int(s))
+                assert st["converged"] == 1
+
+
+def test_sssp_float_weights_bit_identical_to_reference_float_path(hyt, oracle, gpu):
+    g = hyt.rmat(12, 16, 31)
+    rng = np.random.default_rng(2)
+    wf = (rng.random(g.num_edges) * 10).astype(np.float32)  # non-integer weights
+    gf = hyt.CSR(g.row_offsets, g.column_indices, wf)
+    with hyt.Graph(gf) as dg:
+        for s in hyt.pick_sources(g.row_offsets, 4, 3):
+            d, _ = dg.sssp(int(s))
+            ref, _, _ = oracle.sssp(g.row_offsets, g.column_indices, wf, int(s))
+            assert np.array_equal(d, ref.view(np.uint32))
+
+
+def test_sssp_modes_and_repeat(hyt, gpu):
+    g = hyt.rmat(15, 16, 12)
+    s = int(hyt.pick_sources(g.row_offsets, 1, 1)[0])
+    with hyt.Graph(g) as dg:
+        a, sa = dg.sssp(s)
+        b, sb = dg.sssp(s, flags=hyt.capi.HYT_RUN_NO_GRAPH)
+        c, sc = dg.sssp(s, flags=hyt.capi.HYT_RUN_PROFILE)
+        d, _ = dg.sssp(s)
+    assert np.array_equal(a, b) and np.array_equal(a, c) and np.array_equal(a, d)
+    assert sa["edges_processed"] >= g.num_edges * 0.5
+
+
+def test_sssp_errors(hyt, gpu):
+    g = hyt.rmat(8, 4, 1)
+    with hyt.Graph(g) as dg:
+        with pytest.raises(hyt.HytError) as e:
+            dg.sssp(g.num_vertices)
+        assert e.value.code == hyt.capi.HYT_E_INVALID
+    bad = hyt.CSR(g.row_offsets, g.column_indices, -np.ones(g.num_edges, np.float32))
+    with hyt.Graph(bad) as dg:  # PageRank ignores weights; SSSP rejects them
+        dg.pagerank()
+        with pytest.raises(hyt.HytError) as e:
+            dg.sssp(0)
+        assert "non-negative" in str(e.value)
+    with pytest.raises(hyt.HytError) as e:  # malformed CSR is rejected before any kernel reads it
+        hyt.Graph(hyt.CSR(np.array([0, 2, 1], np.uint64), np.array([0, 1], np.uint32)))
+    assert e.value.code == hyt.capi.HYT_E_INVALID
+    with pytest.raises(hyt.HytError):
+        hyt.Graph(hyt.CSR(np.array([0, 1], np.uint64), np.array([5], np.uint32)))
+
+
+def test_device_generator_matches_host(hyt, gpu):
+    import ctypes as C
+
+    for scale, ef, seed in [(8, 4, 1), (12, 16, 7), (16, 16, 12345)]:
+        h = hyt.rmat(scale, ef, seed)
+        d = hyt.rmat(scale, ef, seed, device=True)
+        assert d.num_edges == h.num_edges
+        # read the device arrays back through a graph built from them
+        with hyt.Graph(d) as dg:
+            info = dg.info()
+        assert info["num_edges"] == h.num_edges
+        import torch
+
+        off = torch.empty(h.num_vertices + 1, dtype=torch.int64, device="cuda")
+        cols = torch.empty(h.num_edges, dtype=torch.int32, device="cuda")
+        w = torch.empty(h.num_edges, dtype=torch.int32, device="cuda")
+        b = d.buffers
+        torch.cuda.synchronize()
+        cudart = torch.cuda.cudart()
+        for dst, src, n in [(off, b.row_offsets, off.numel() * 8), (cols, b.column_indices, cols.numel() * 4),
+                            (w, b.weights, w.numel() * 4)]:
+            assert cudart.cudaMemcpy(dst.data_ptr(), C.cast(src, C.c_void_p).value, n, 3) == 0
+        assert np.array_equal(off.cpu().numpy().view(np.uint64), h.row_offsets)
+        assert np.array_equal(cols.cpu().numpy().view(np.uint32), h.column_indices)
+        assert np.array_equal(w.cpu().numpy().view(np.uint32), h.weights)
+        d.free()
+
+
+def test_device_resident_inputs_and_outputs(hyt, oracle, gpu):
+    import torch
+
+    g = hyt.rmat(12, 16, 8)
+    t_off = torch.from_numpy(g.row_offsets.view(np.int64)).cuda()
+    t_cols = torch.from_numpy(g.column_indices.view(np.int32)).cuda()
+    t_w = torch.from_numpy(g.weights.view(np.int32)).cuda()
+    dcsr = hyt.CSR(g.row_offsets, g.column_indices, g.weights)
+    dcsr.to_c = lambda: _dev_csr(hyt, g, t_off, t_cols, t_w)
+    with hyt.Graph(dcsr) as dg:
+        out = torch.empty(g.num_vertices, dtype=torch.float32, device="cuda")
+        dg.pagerank(out=out)
+        ref, _, _, _ = oracle.pagerank_f64(g.row_offsets, g.column_indices)
+        assert np.abs(out.cpu().numpy() - ref).sum() <= PR_L1_TOL
+        dd = torch.empty(g.num_vertices, dtype=torch.int32, device="cuda")
+        s = int(hyt.pick_sources(g.row_offsets, 2, 1)[0])
+        dg.sssp(s, out=dd)
+        h, _ = dg.sssp(s)
+        assert np.array_equal(dd.cpu().numpy().view(np.uint32), h)
+
+
+def _dev_csr(hyt, g, t_off, t_cols, t_w):
+    c = hyt.capi.hyt_csr()
+    c.num_vertices, c.num_edges = g.num_vertices, g.num_edges
+    c.row_offsets, c.column_indices, c.weights = t_off.data_ptr(), t_cols.data_ptr(), t_w.data_ptr()
+    c.weight_kind = hyt.capi.HYT_WEIGHTS_U32
+    return c

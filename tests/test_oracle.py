@@ -1,0 +1,174 @@
+"""The oracle (C restatement of the reference) pinned against the reference's
+golden vectors, its known-answer tests and its compiled CPU code."""
+from __future__ import annotations
+
+import hashlib
+
+import numpy as np
+import pytest
+
+from conftest import ROOT  # noqa: F401
+
+
+def _digest(g):
+    h = hashlib.sha256()
+    h.update(g.row_offsets.astype("<u8").tobytes())
+    h.update(g.column_indices.astype("<u4").tobytes())
+    if g.weights is not None:
+        h.update(g.weights.astype("<u4").tobytes())
+    return h.hexdigest()
+
+
+def _graph(hyt, m):
+    w = (1, 63) if m["weighted"] else (0, 0)
+    return hyt.rmat(m["scale"], m["edge_factor"], m["seed"], *w)
+
+
+def test_generator_matches_golden_digest(hyt, golden):
+    for m in golden["meta"]["graphs"]:
+        g = _graph(hyt, m)
+        assert g.num_edges == m["num_edges"]
+        assert _digest(g) == m["csr_sha256"], m["key"]
+
+
+def test_oracle_pagerank_f32_bit_identical_to_reference_golden(hyt, oracle, golden):
+    for m in golden["meta"]["graphs"]:
+        g = _graph(hyt, m)
+        r, it, res, conv = oracle.pagerank_f32(g.row_offsets, g.column_indices)
+        assert it == m["pr_iterations"] and conv == m["pr_converged"]
+        assert np.array_equal(r.view(np.uint32), golden["npz"][f"{m['key']}_pr_bits"])
+
+
+def test_oracle_sssp_bit_identical_to_reference_golden(hyt, oracle, golden):
+    for m in golden["meta"]["graphs"]:
+        g = _graph(hyt, m)
+        w = g.weights.astype(np.float32) if g.weights is not None else None
+        bits = golden["npz"][f"{m['key']}_sssp_bits"]
+        for i, s in enumerate(m["sources"]):
+            d, rounds, conv = oracle.sssp(g.row_offsets, g.column_indices, w, s)
+            assert conv and rounds == m["sssp_rounds"][i]
+            assert np.array_equal(d.view(np.uint32), bits[i])
+
+
+def test_dijkstra_cross_check(hyt, oracle):
+    g = hyt.rmat(12, 16, 77)
+    for s in hyt.pick_sources(g.row_offsets, 5, 3):
+        d, _, _ = oracle.sssp(g.row_offsets, g.column_indices, g.weights.astype(np.float32), int(s))
+        dj = oracle.dijkstra(g.row_offsets, g.column_indices, g.weights, int(s))
+        reach = dj != np.iinfo(np.uint64).max
+        assert np.array_equal(np.isfinite(d), reach)
+        assert np.array_equal(d[reach].astype(np.uint64), dj[reach])
+
+
+def test_hand_known_answers(oracle, golden):
+    """The reference's hand-written cases (algorithm_tests.cpp:22-157,
+    cuda_algorithm_tests.cu:23-87) reproduced exactly by the oracle."""
+    for h in golden["meta"]["hand"]:
+        off = np.array(h["row_offsets"], np.uint64)
+        cols = np.array(h["column_indices"], np.uint32)
+        if "ranks" in h:
+            r, it, _, conv = oracle.pagerank_f32(off, cols, 0.85, 1e-6, 200)
+            assert conv and it == h["iterations"]
+            assert np.array_equal(r, np.array(h["ranks"], np.float32))
+        else:
+            w = None if h["weights"] is None else np.array(h["weights"], np.float32)
+            d, it, conv = oracle.sssp(off, cols, w, h["source"])
+            want = np.array([np.inf if x is None else x for x in h["distances"]], np.float32)
+            assert conv and it == h["iterations"] and np.array_equal(d, want)
+    # the reference's assertions themselves
+    by = {h["name"]: h for h in golden["meta"]["hand"]}
+    assert np.allclose(by["pr_cycle3"]["ranks"], 1 / 3, atol=1e-5)
+    assert abs(sum(by["pr_dangling"]["ranks"]) - 1.0) <= 1e-5
+    assert by["sssp_weighted4"]["distances"] == [0.0, 1.0, 3.0, 4.0]
+    assert by["sssp_unweighted4"]["distances"] == [0.0, 1.0, 2.0, None]
+
+
+def test_pagerank_f64_matches_f32_reference_semantics(hyt, oracle):
+    g = hyt.rmat(10, 16, 9)
+    r32, it32, _, _ = oracle.pagerank_f32(g.row_offsets, g.column_indices, tol=1e-9, max_iter=60)
+    r64, it64, _, _ = oracle.pagerank_f64(g.row_offsets, g.column_indices, tol=1e-9, max_iter=60)
+    assert abs(r64.sum() - 1.0) < 1e-12
+    assert np.abs(r32 - r64).sum() < 1e-4  # float drift of the FP32 restatement
+
+
+def test_ppr_oracle_hand_cases(oracle):
+    # 3-cycle 0->1->2->0 from source 0: x = r * sum_k d^k e_{k mod 3}
+    off = np.array([0, 1, 2, 3], np.uint64)
+    cols = np.array([1, 2, 0], np.uint32)
+    r, _, _, conv = oracle.ppr_f64(off, cols, 0, 0.15, 1e-14, 2000)
+    d = 0.85
+    want = np.array([1, d, d * d]) * (0.15 / (1 - d ** 3))
+    assert conv and np.allclose(r, want, atol=1e-12)
+    # star: 0 -> 1..4, leaves dangling (mass returns to the source)
+    off = np.array([0, 4, 4, 4, 4, 4], np.uint64)
+    cols = np.array([1, 2, 3, 4], np.uint32)
+    r, _, _, conv = oracle.ppr_f64(off, cols, 0, 0.15, 1e-14, 2000)
+    # fixed point: x0 = 0.15 + 0.85 * (1 - x0) ... leaves share d*x0/4 each
+    x0 = 1.0 / (1.0 + 0.85)
+    assert conv and abs(r[0] - x0) < 1e-12 and np.allclose(r[1:], 0.85 * x0 / 4, atol=1e-12)
+    assert abs(r.sum() - 1.0) < 1e-12
+
+
+def test_oracle_vs_reference_random(hyt, oracle, reference):
+    for seed, (scale, ef) in enumerate([(9, 4), (10, 8), (11, 16)]):
+        g = hyt.rmat(scale, ef, 1000 + seed)
+        a = oracle.pagerank_f32(g.row_offsets, g.column_indices)
+        b = reference.pagerank_cpu(g.row_offsets, g.column_indices)
+        assert np.array_equal(a[0].view(np.uint32), b[0].view(np.uint32)) and a[1] == b[1]
+        w = g.weights.astype(np.float32)
+        for s in hyt.pick_sources(g.row_offsets, seed, 2):
+            x = oracle.sssp(g.row_offsets, g.column_indices, w, int(s))
+            y = reference.sssp_cpu(g.row_offsets, g.column_indices, w, int(s))
+            assert np.array_equal(x[0].view(np.uint32), y[0].view(np.uint32)) and x[1] == y[1]
+
+
+def test_hytm_cost_model_known_answer(oracle, golden):
+    from oracle.bindings import HytmOptions
+
+    k = golden["meta"]["hytm"]
+    o = k["options"]
+    opts = HytmOptions(o["alpha"], o["beta"], o["gamma"], o["rtt"], o["cpu_throughput"], o["m"], o["mr"], 4, 8, 128)
+    c = oracle.hytm_partition(np.array(k["row_offsets"], np.uint64), np.array(k["active"], np.uint8), 0, 2, opts)
+    m = k["metrics"]  # vbegin, vend, Av, Ae, Ep, F bytes, C bytes, zc req, zc align, zc total, index
+    assert (c.active_vertices, c.active_edges, c.total_edges) == (m[2], m[3], m[4]) == (2, 3, 3)
+    assert (c.filter_bytes, c.compaction_bytes, c.zc_requests, c.zc_alignment) == (m[5], m[6], m[7], m[8])
+    assert (c.filter_cost, c.compaction_cost, c.zero_copy_cost, c.zc_rtt) == tuple(k["costs"]) == (2.0, 4.0, 2.0, 2.0)
+    assert c.engine == k["engine"]
+
+
+def test_selector_and_combiner_known_answers(oracle, golden):
+    for s in golden["meta"]["selector"]:
+        assert oracle.select_engine(s["f"], s["c"], s["z"], 0.8, 0.4) == s["engine"]
+    for c in golden["meta"]["combiner"]:
+        top, teng, tfirst = oracle.task_combine(c["engines"], c["k"])
+        assert top.tolist() == c["task_of_partition"]
+        assert teng.tolist() == c["task_engine"] and tfirst.tolist() == c["task_first"]
+
+
+def test_hytm_oracle_vs_reference_random(hyt, oracle, reference):
+    from oracle.bindings import HytmOptions
+
+    rng = np.random.default_rng(3)
+    g = hyt.rmat(12, 8, 21)
+    V = g.num_vertices
+    bounds = np.unique(np.concatenate([[0, V], rng.integers(0, V, 14)]))
+    parts = np.stack([bounds[:-1], bounds[1:]], 1).astype(np.uint32)
+    for frac in (0.0, 0.01, 0.2, 1.0):
+        act = (rng.random(V) < frac).astype(np.uint8)
+        for rtt, tput in [(1.0, 1.0), (2.0, 14.0), (3e-6, 2.5e10)]:
+            metrics, costs, eng = reference.hytm_evaluate(g.row_offsets, g.column_indices, act, parts,
+                                                          [0.8, 0.4, 0.625, rtt, tput], [128, 256])
+            opts = HytmOptions(0.8, 0.4, 0.625, rtt, tput, 128, 256, 4, 8, 128)
+            for i, (vb, ve) in enumerate(parts):
+                c = oracle.hytm_partition(g.row_offsets, act, int(vb), int(ve), opts)
+                assert (c.active_vertices, c.active_edges, c.total_edges, c.filter_bytes, c.compaction_bytes,
+                        c.zc_requests, c.zc_alignment) == tuple(int(x) for x in metrics[i, 2:9])
+                assert (c.filter_cost, c.compaction_cost, c.zero_copy_cost, c.zc_rtt) == tuple(costs[i])
+                assert c.engine == eng[i]
+    rng2 = np.random.default_rng(5)
+    for _ in range(50):
+        e = rng2.integers(0, 3, rng2.integers(0, 40))
+        k = int(rng2.integers(1, 6))
+        a = oracle.task_combine(e, k)
+        b = reference.task_combine(e, k)
+        assert all(np.array_equal(x, y) for x, y in zip(a, b[:3]))
