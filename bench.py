@@ -185,14 +185,11 @@ def host_graph_from_device(dcsr):
     import torch
 
     V, E = dcsr.num_vertices, dcsr.num_edges
-    b = dcsr.buffers
     off = torch.empty(V + 1, dtype=torch.int64, pin_memory=True)
     cols = torch.empty(E, dtype=torch.int32, pin_memory=True)
     w = torch.empty(E, dtype=torch.int32, pin_memory=True)
-    cudart = torch.cuda.cudart()
     torch.cuda.synchronize()
-    for dst, src, n in [(off, b.row_offsets, (V + 1) * 8), (cols, b.column_indices, E * 4), (w, b.weights, E * 4)]:
-        assert cudart.cudaMemcpy(dst.data_ptr(), C.cast(src, C.c_void_p).value, n, 2) == 0
+    dcsr.download(off.numpy().view(np.uint64), cols.numpy().view(np.uint32), w.numpy().view(np.uint32))
     return off, cols, w
 
 

@@ -151,6 +151,7 @@ _SIGNATURES = [
     ("hyt_last_error", C.c_char_p, []),
     ("hyt_abi_version", C.c_int, []),
     ("hyt_device_count", C.c_int, [C.POINTER(C.c_int)]),
+    ("hyt_copy", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p]),
     ("hyt_graph_create", C.c_int, [C.POINTER(hyt_csr), C.POINTER(hyt_graph_options), C.POINTER(C.c_void_p)]),
     ("hyt_graph_destroy", C.c_int, [C.c_void_p]),
     ("hyt_graph_get_info", C.c_int, [C.c_void_p, C.POINTER(hyt_graph_info)]),
@@ -190,6 +191,11 @@ def last_error() -> str:
 def check(status: int) -> None:
     if status != HYT_OK:
         raise HytError(status, last_error())
+
+
+def copy(dst: int, src: int, nbytes: int, stream: int = 0) -> None:
+    """Synchronous copy between host/device addresses (integers)."""
+    check(lib.hyt_copy(dst, src, nbytes, stream or None))
 
 
 def device_count() -> int:

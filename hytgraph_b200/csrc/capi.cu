@@ -89,6 +89,17 @@ int hyt_device_count(int *count) {
     });
 }
 
+int hyt_copy(void *dst, const void *src, uint64_t bytes, void *stream) {
+    return guarded([&] {
+        if (!bytes) return;
+        if (!dst || !src) fail(HYT_E_INVALID, "hyt_copy: NULL pointer");
+        require_device();
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        HYT_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, s));
+        HYT_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
 int hyt_graph_create(const hyt_csr *csr, const hyt_graph_options *options, hyt_graph **out) {
     return guarded([&] {
         if (!csr || !out) fail(HYT_E_INVALID, "csr/out is NULL");

@@ -58,6 +58,10 @@ class CSR:
         return np.diff(self.row_offsets)
 
     def to_c(self) -> capi.hyt_csr:
+        if self.row_offsets.dtype != np.uint64 or self.column_indices.dtype != np.uint32:
+            raise TypeError("row_offsets must be uint64 and column_indices uint32")
+        if self.weights is not None and self.weights.dtype not in (np.uint32, np.float32):
+            raise TypeError("weights must be uint32 or float32")
         c = capi.hyt_csr()
         c.num_vertices = self.num_vertices
         c.num_edges = self.num_edges
@@ -92,6 +96,23 @@ class DeviceCSR:
         c.weights = C.cast(b.weights, C.c_void_p).value if b.weights else 0
         c.weight_kind = capi.HYT_WEIGHTS_U32 if b.weights else capi.HYT_WEIGHTS_NONE
         return c
+
+    def download(self, row_offsets=None, column_indices=None, weights=None) -> CSR:
+        """Copies the device arrays into host arrays (numpy by default, or
+        caller-provided buffers such as pinned tensors viewed as numpy)."""
+        V, E = self.num_vertices, self.num_edges
+        b = self.buffers
+        off = np.empty(V + 1, np.uint64) if row_offsets is None else row_offsets
+        cols = np.empty(E, np.uint32) if column_indices is None else column_indices
+        w = None
+        if b.weights:
+            w = np.empty(E, np.uint32) if weights is None else weights
+        capi.copy(_ptr(off), C.cast(b.row_offsets, C.c_void_p).value, (V + 1) * 8)
+        if E:
+            capi.copy(_ptr(cols), C.cast(b.column_indices, C.c_void_p).value, E * 4)
+            if w is not None:
+                capi.copy(_ptr(w), C.cast(b.weights, C.c_void_p).value, E * 4)
+        return CSR(off, cols, w)
 
     def free(self) -> None:
         check(lib.hyt_csr_buffers_free(C.byref(self.buffers)))

@@ -54,6 +54,9 @@ const char *hyt_last_error(void);
 int hyt_abi_version(void);
 /* Number of visible CUDA devices (0 without error when there is none). */
 int hyt_device_count(int *count);
+/* Synchronous copy between any two host/device buffers (unified
+ * addressing decides the direction); stream NULL = a library stream. */
+int hyt_copy(void *dst, const void *src, uint64_t bytes, void *stream);
 
 /* ------------------------------------------------------------------ */
 /* CSR input                                                           */

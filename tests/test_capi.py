@@ -134,3 +134,14 @@ def test_host_library_exports(hyt):
                 "hytgraph::transfer::ExpTMFilter::plan", "hytgraph::graph::LogicalPartitioner::partition"]:
         assert sym in out, sym
     assert lib is not None
+
+
+def test_csr_rejects_wrong_dtypes(hyt):
+    off = np.array([0, 1, 2], np.uint64)
+    cols = np.array([1, 0], np.uint32)
+    with pytest.raises(TypeError):
+        hyt.CSR(off, cols, np.array([1, 1])).to_c()            # int64 weights
+    with pytest.raises(TypeError):
+        hyt.CSR(off.astype(np.int64), cols).to_c()
+    assert hyt.CSR(off, cols, np.array([1, 1], np.uint32)).to_c().weight_kind == hyt.capi.HYT_WEIGHTS_U32
+    assert hyt.CSR(off, cols, np.array([1, 1], np.float32)).to_c().weight_kind == hyt.capi.HYT_WEIGHTS_F32
