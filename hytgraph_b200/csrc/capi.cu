@@ -1,4 +1,5 @@
 // extern "C" entry points of libhyt_core.so (declared in include/hyt/capi.h).
+#include <cstdlib>
 #include <cstring>
 #include <string>
 
@@ -65,6 +66,17 @@ GraphImpl &impl(hyt_graph *g) {
 }
 
 void use_device(const GraphImpl &g) { HYT_CUDA(cudaSetDevice(g.device)); }
+
+// HYT_LAUNCH=host selects host-driven launch loops instead of CUDA graphs
+// with conditional nodes (same kernels, same work; profilers such as ncu
+// cannot attribute kernels inside conditional graphs).
+uint32_t launch_flags(uint32_t flags) {
+    static const bool host = [] {
+        const char *v = std::getenv("HYT_LAUNCH");
+        return v && std::strcmp(v, "host") == 0;
+    }();
+    return host ? (flags | HYT_RUN_NO_GRAPH) : flags;
+}
 }  // namespace
 
 }  // namespace hyt
@@ -165,7 +177,9 @@ int hyt_pagerank(hyt_graph *graph, const hyt_pagerank_params *params, float *ran
         GraphImpl &g = impl(graph);
         use_device(g);
         if (stats) std::memset(stats, 0, sizeof(*stats));
-        pagerank_run(g, *params, ranks_out, stats);
+        hyt_pagerank_params p = *params;
+        p.flags = launch_flags(p.flags);
+        pagerank_run(g, p, ranks_out, stats);
     });
 }
 
@@ -175,7 +189,9 @@ int hyt_ppr(hyt_graph *graph, const hyt_ppr_params *params, float *ranks_out, hy
         GraphImpl &g = impl(graph);
         use_device(g);
         if (stats) std::memset(stats, 0, sizeof(*stats));
-        ppr_run(g, *params, ranks_out, stats);
+        hyt_ppr_params p = *params;
+        p.flags = launch_flags(p.flags);
+        ppr_run(g, p, ranks_out, stats);
     });
 }
 
@@ -185,7 +201,9 @@ int hyt_sssp(hyt_graph *graph, const hyt_sssp_params *params, uint32_t *dist_out
         GraphImpl &g = impl(graph);
         use_device(g);
         if (stats) std::memset(stats, 0, sizeof(*stats));
-        sssp_run(g, *params, dist_out, stats);
+        hyt_sssp_params p = *params;
+        p.flags = launch_flags(p.flags);
+        sssp_run(g, p, dist_out, stats);
     });
 }
 

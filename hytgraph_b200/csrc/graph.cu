@@ -31,17 +31,23 @@ __global__ void validate_offsets_kernel(const uint64_t *off, uint64_t V, uint64_
 }
 
 __global__ void validate_edges_kernel(const uint32_t *cols, const uint32_t *w, uint32_t wkind, uint64_t V,
-                                      uint64_t E, uint32_t *err) {
+                                      uint64_t E, uint32_t *err, unsigned long long *weight_sum) {
     const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
     uint32_t bad = 0;
+    unsigned long long wsum = 0;
     for (uint64_t e = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; e < E; e += stride) {
         if (cols[e] >= V) bad |= kBadColumn;
         if (wkind == HYT_WEIGHTS_F32) {
             const float x = __uint_as_float(w[e]);
             if (!(x >= 0.0f) || isinf(x)) bad |= kBadWeight;  // NaN fails x >= 0
+        } else if (wkind == HYT_WEIGHTS_U32) {
+            wsum += w[e];
         }
     }
     if (bad) atomicOr(err, bad);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) wsum += __shfl_xor_sync(0xffffffffu, wsum, o);
+    if ((threadIdx.x & 31) == 0 && wsum) atomicAdd(weight_sum, wsum);
 }
 
 __global__ void out_degree_kernel(const uint64_t *off, uint64_t V, uint32_t *deg, unsigned long long *dangling) {
@@ -131,7 +137,7 @@ int bits_for(uint64_t max_value) {
 size_t GraphImpl::device_bytes() const {
     size_t b = row_offsets.bytes() + cols.bytes() + weights.bytes() + out_degree.bytes() + in_offsets.bytes() +
                in_sources.bytes() + tile_start.bytes() + long_rows.bytes() + chunk_tasks.bytes();
-    for (int i = 0; i < 2; ++i) b += rank[i].bytes() + contrib[i].bytes() + queue[i].bytes();
+    for (int i = 0; i < 2; ++i) b += rank[i].bytes() + contrib[i].bytes() + queue[i].bytes() + far[i].bytes();
     b += partial.bytes() + ticket.bytes() + pr_state.bytes() + dist.bytes() + stamp.bytes() + hub_tasks.bytes() +
          sssp_state.bytes();
     return b;
@@ -182,15 +188,24 @@ void graph_build(GraphImpl &g, const hyt_csr &csr, uint32_t flags) {
     if (h_err & kBadOffsets) fail(HYT_E_INVALID, "row offsets must start at 0 and be non-decreasing");
     if (h_err & kBadTerminal) fail(HYT_E_INVALID, "terminal row offset must equal the number of edges");
     if (E) {
+        DeviceArray<unsigned long long> wsum(1);
+        HYT_CUDA(cudaMemsetAsync(wsum.get(), 0, sizeof(unsigned long long), s));
         validate_edges_kernel<<<grid_for(E, 256), 256, 0, s>>>(g.cols.get(), keep_weights ? g.weights.get() : nullptr,
-                                                                keep_weights ? csr.weight_kind : 0u, V, E, err.get());
+                                                                keep_weights ? csr.weight_kind : 0u, V, E, err.get(),
+                                                                wsum.get());
         HYT_CUDA(cudaGetLastError());
+        unsigned long long h_wsum = 0;
         HYT_CUDA(cudaMemcpyAsync(&h_err, err.get(), sizeof(h_err), cudaMemcpyDeviceToHost, s));
+        HYT_CUDA(cudaMemcpyAsync(&h_wsum, wsum.get(), sizeof(h_wsum), cudaMemcpyDeviceToHost, s));
         HYT_CUDA(cudaStreamSynchronize(s));
         if (h_err & kBadColumn) fail(HYT_E_INVALID, "column index contains an invalid destination vertex ID");
         // Negative / non-finite float weights are legal for PageRank; SSSP
         // rejects them when it is called (reference: sssp.cpp:117-124).
         g.weights_ok = (h_err & kBadWeight) == 0;
+        if (keep_weights && csr.weight_kind == HYT_WEIGHTS_U32) {
+            const double mean = static_cast<double>(h_wsum) / static_cast<double>(E);
+            g.default_delta = static_cast<uint32_t>(std::min(4.0e9, std::max(1.0, 2.0 * mean)));
+        }
     }
 
     g.out_degree.allocate(V);

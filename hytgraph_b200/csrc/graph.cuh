@@ -20,12 +20,14 @@ namespace hyt {
 
 // PageRank pull work decomposition.  Rows are cut into tiles along the
 // merge path (1 unit per row + 1 per in-edge): a tile spans kTileCost units,
-// so its rows hold at most kTileCost edges except for its last row.  A last
-// row with in-degree >= kLongDegree is a "long row": it is excluded from the
-// tile and split into chunks of kLongChunk edges processed by separate CTAs.
-constexpr uint32_t kTileCost = 4096;
+// so its rows hold fewer than kTileCost edges except for its last row.  A
+// last row with in-degree >= kLongDegree is a "long row": it is excluded
+// from the tile and split into kLongChunk-edge chunks.  One warp processes
+// one task (tile or chunk), so a tile's staged contributions fit in a
+// per-warp shared-memory slice of kStageCap floats.
+constexpr uint32_t kTileCost = 512;
 constexpr uint32_t kLongDegree = kTileCost;
-constexpr uint32_t kLongChunk = 8192;
+constexpr uint32_t kLongChunk = 4096;
 constexpr uint32_t kStageCap = kTileCost + kLongDegree;  // staged edges per tile
 
 struct LongRow {
@@ -44,6 +46,7 @@ struct GraphImpl {
     uint32_t weight_kind = HYT_WEIGHTS_NONE;
     uint32_t flags = 0;
     bool weights_ok = true;  // F32 weights all finite and >= 0
+    uint32_t default_delta = 0;  // SSSP near/far bucket width (2x mean u32 weight)
 
     // push side
     DeviceArray<uint64_t> row_offsets;
@@ -74,6 +77,7 @@ struct GraphImpl {
     DeviceArray<uint32_t> dist;
     DeviceArray<uint32_t> stamp;
     DeviceArray<uint32_t> queue[2];
+    DeviceArray<uint32_t> far[2];
     DeviceArray<uint2> hub_tasks;
     DeviceArray<unsigned char> sssp_state;
     PinnedArray<uint64_t> host_scratch;  // small pinned readback area

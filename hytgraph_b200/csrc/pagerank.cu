@@ -33,8 +33,7 @@ namespace hyt {
 namespace {
 
 constexpr int kPRThreads = 256;
-constexpr uint32_t kWarpRowDegree = 32;
-constexpr uint32_t kMaxWarpRows = kStageCap / kWarpRowDegree + 1;
+constexpr uint32_t kWarpRowDegree = 16;  // rows with more in-edges are summed by a whole warp
 
 struct PRHeader {
     uint32_t iter;       // iterations completed
@@ -100,32 +99,45 @@ __device__ __forceinline__ void finalize_row(const PRArgs &a, const PRState &ps,
     if (od == 0) dang += static_cast<double>(nx);
 }
 
-// Compensated block reduction; result valid in thread 0.
-__device__ __forceinline__ dev::CSum block_csum(dev::CSum v, float2 *scratch) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    v = dev::warp_reduce(v);
-    __syncthreads();
-    if (lane == 0) scratch[warp] = make_float2(v.s, v.c);
-    __syncthreads();
-    dev::CSum t;
-    if (threadIdx.x == 0) {
-        const int nw = blockDim.x >> 5;
-        for (int w = 0; w < nw; ++w) {
-            dev::CSum x;
-            x.s = scratch[w].x;
-            x.c = scratch[w].y;
-            t.merge(x);
+// Gathers contributions for edges [lo, hi) of the in-source array into
+// registers: 4 x 128-bit streaming loads of source ids per lane, then 16
+// independent gathers, so every lane keeps 16 loads in flight.  Index
+// x = a0 + 4*i + c; edges outside [lo, hi) read contribution 0 (their
+// addresses are clamped to a valid row, the value is discarded).
+constexpr int kUnroll = 4;
+
+template <class Sink>
+__device__ __forceinline__ void gather_span(const uint32_t *in_src, const float *ccur, uint64_t lo, uint64_t hi,
+                                            uint64_t pol, int lane, Sink &&sink) {
+    const uint64_t a0 = lo & ~3ull;
+    const uint32_t nvec = static_cast<uint32_t>((hi - a0 + 3) >> 2);
+    const uint4 *src4 = reinterpret_cast<const uint4 *>(in_src + a0);
+    for (uint32_t base = 0; base < nvec; base += 32 * kUnroll) {
+        uint4 q[kUnroll];
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+            const uint32_t i = base + lane + 32 * u;
+            q[u] = (i < nvec) ? dev::ld_stream4(src4 + i) : make_uint4(0, 0, 0, 0);
         }
+        float v[kUnroll][4];
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+            const uint64_t x = a0 + 4ull * (base + lane + 32 * u);
+            const uint32_t ids[4] = {q[u].x, q[u].y, q[u].z, q[u].w};
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const bool ok = (x + c >= lo) && (x + c < hi);
+                v[u][c] = dev::ld_keep(ccur + (ok ? ids[c] : 0u), pol);
+                if (!ok) v[u][c] = 0.0f;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) sink(base + lane + 32 * u, v[u]);
     }
-    return t;
 }
 
-__global__ void __launch_bounds__(kPRThreads) pr_iterate_kernel(const PRArgs *__restrict__ args) {
-    __shared__ __align__(16) float s_vals[kStageCap + 8];
-    __shared__ uint32_t s_warp_rows[kMaxWarpRows];
-    __shared__ uint32_t s_nwarp_rows;
-    __shared__ uint32_t s_task;
-    __shared__ float2 s_red2[kPRThreads / 32];
+__global__ void __launch_bounds__(kPRThreads, 4) pr_iterate_kernel(const PRArgs *__restrict__ args) {
+    __shared__ __align__(16) float s_vals[kPRThreads / 32][kStageCap + 8];
     __shared__ double s_red[32];
 
     const PRArgs a = *args;
@@ -148,116 +160,97 @@ __global__ void __launch_bounds__(kPRThreads) pr_iterate_kernel(const PRArgs *__
     const uint64_t pol = dev::policy_evict_last();
     const uint64_t total_tasks = a.num_chunks + a.num_tiles;
     double res = 0.0, dang = 0.0;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int nwarps = kPRThreads / 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float *sv = s_vals[warp];
+    const uint64_t nwarps = uint64_t(gridDim.x) * (kPRThreads / 32);
 
-    for (;;) {
-        if (tid == 0) s_task = atomicAdd(&a.task_counter[it], 1u);
-        __syncthreads();
-        const uint32_t task = s_task;
-        __syncthreads();
-        if (task >= total_tasks) break;
-
+    // Static round-robin over tasks: every task costs at most one chunk of
+    // edges, so warps receive balanced work without a shared counter.
+    for (uint64_t task = uint64_t(blockIdx.x) * (kPRThreads / 32) + warp; task < total_tasks; task += nwarps) {
         if (task < a.num_chunks) {
-            // ---- slice of a long row ------------------------------------
+            // ---- slice of a long row -------------------------------------
             const uint2 t = a.chunk_tasks[task];
             const LongRow L = a.long_rows[t.x];
             const uint64_t rb = a.in_off[L.row], re = a.in_off[L.row + 1];
             const uint64_t b = rb + uint64_t(t.y) * kLongChunk;
             const uint64_t e = (b + kLongChunk < re) ? b + kLongChunk : re;
             dev::CSum acc;
-            const uint64_t b4 = b & ~3ull;
-            const uint64_t nvec = (e - b4 + 3) >> 2;
-            const uint4 *src4 = reinterpret_cast<const uint4 *>(a.in_src + b4);
-            for (uint64_t i = tid; i < nvec; i += kPRThreads) {
-                const uint4 q = dev::ld_stream4(src4 + i);
-                const uint64_t x = b4 + 4 * i;
-                const float v0 = (x + 0 >= b && x + 0 < e) ? dev::ld_keep(ccur + q.x, pol) : 0.f;
-                const float v1 = (x + 1 >= b && x + 1 < e) ? dev::ld_keep(ccur + q.y, pol) : 0.f;
-                const float v2 = (x + 2 >= b && x + 2 < e) ? dev::ld_keep(ccur + q.z, pol) : 0.f;
-                const float v3 = (x + 3 >= b && x + 3 < e) ? dev::ld_keep(ccur + q.w, pol) : 0.f;
-                acc.add(v0);
-                acc.add(v1);
-                acc.add(v2);
-                acc.add(v3);
-            }
-            const dev::CSum tot = block_csum(acc, s_red2);
-            if (tid == 0) {
-                a.partial[L.first_chunk + t.y] = make_float2(tot.s, tot.c);
+            gather_span(a.in_src, ccur, b, e, pol, lane, [&](uint32_t, const float (&v)[4]) {
+                acc.add(v[0]);
+                acc.add(v[1]);
+                acc.add(v[2]);
+                acc.add(v[3]);
+            });
+            acc = dev::warp_reduce(acc);
+            uint32_t last = 0;
+            if (lane == 0) {
+                a.partial[L.first_chunk + t.y] = make_float2(acc.s, acc.c);
                 __threadfence();
                 const uint32_t tk = atomicAdd(&a.ticket[t.x], 1u) + 1u;
-                if (tk % L.num_chunks == 0) {
-                    __threadfence();
-                    dev::CSum row;
-                    for (uint32_t j = 0; j < L.num_chunks; ++j) {
-                        const float2 p = __ldcg(a.partial + L.first_chunk + j);
-                        dev::CSum x;
-                        x.s = p.x;
-                        x.c = p.y;
-                        row.merge(x);
-                    }
-                    finalize_row(a, ps, L.row, row.value(), cur, nxt, cnxt, res, dang);
-                }
+                last = (tk % L.num_chunks == 0) ? 1u : 0u;
             }
-            __syncthreads();
+            last = __shfl_sync(0xffffffffu, last, 0);
+            if (last) {
+                // the last arriving warp merges every chunk of the row, in a
+                // fixed order: lane j takes chunks j, j+32, ...
+                __threadfence();
+                dev::CSum row;
+                for (uint32_t j = lane; j < L.num_chunks; j += 32) {
+                    const float2 p = __ldcg(a.partial + L.first_chunk + j);
+                    dev::CSum x;
+                    x.s = p.x;
+                    x.c = p.y;
+                    row.merge(x);
+                }
+                row = dev::warp_reduce(row);
+                if (lane == 0) finalize_row(a, ps, L.row, row.value(), cur, nxt, cnxt, res, dang);
+            }
         } else {
-            // ---- merge-path tile of consecutive rows --------------------
+            // ---- merge-path tile of consecutive rows ---------------------
             const uint64_t k = task - a.num_chunks;
             const uint32_t r0 = a.tile_start[k];
             const uint32_t r1 = a.tile_start[k + 1];
             if (r0 == r1) continue;
-            uint32_t rl = r1;  // rows [r0, rl) are staged; a long last row is chunked
             const uint64_t last_b = a.in_off[r1 - 1], last_e = a.in_off[r1];
-            if (last_e - last_b >= kLongDegree) rl = r1 - 1;
+            const uint32_t rl = (last_e - last_b >= kLongDegree) ? r1 - 1 : r1;  // long last row is chunked
             const uint64_t e0 = a.in_off[r0];
             const uint64_t e1 = (rl == r1) ? last_e : last_b;
             const uint64_t a0 = e0 & ~3ull;
-            const uint32_t nvec = static_cast<uint32_t>((e1 - a0 + 3) >> 2);
-            const uint4 *src4 = reinterpret_cast<const uint4 *>(a.in_src + a0);
-            float4 *sv4 = reinterpret_cast<float4 *>(s_vals);
-            if (tid == 0) s_nwarp_rows = 0;
-            for (uint32_t i = tid; i < nvec; i += kPRThreads) {
-                const uint4 q = dev::ld_stream4(src4 + i);
-                const uint64_t x = a0 + 4ull * i;
-                float4 v;
-                v.x = (x + 0 >= e0 && x + 0 < e1) ? dev::ld_keep(ccur + q.x, pol) : 0.f;
-                v.y = (x + 1 >= e0 && x + 1 < e1) ? dev::ld_keep(ccur + q.y, pol) : 0.f;
-                v.z = (x + 2 >= e0 && x + 2 < e1) ? dev::ld_keep(ccur + q.z, pol) : 0.f;
-                v.w = (x + 3 >= e0 && x + 3 < e1) ? dev::ld_keep(ccur + q.w, pol) : 0.f;
-                sv4[i] = v;
-            }
-            __syncthreads();
-            // rows with in-degree < 32: one thread each
-            for (uint32_t r = r0 + tid; r < rl; r += kPRThreads) {
-                const uint64_t b = a.in_off[r], e = a.in_off[r + 1];
-                if (e - b < kWarpRowDegree) {
+            float4 *sv4 = reinterpret_cast<float4 *>(sv);
+            gather_span(a.in_src, ccur, e0, e1, pol, lane, [&](uint32_t i, const float (&v)[4]) {
+                if (i < ((e1 - a0 + 3) >> 2)) sv4[i] = make_float4(v[0], v[1], v[2], v[3]);
+            });
+            __syncwarp();
+            for (uint32_t rb = r0; rb < rl; rb += 32) {
+                const uint32_t r = rb + lane;
+                const bool active = r < rl;
+                const uint64_t b = active ? a.in_off[r] : 0;
+                const uint64_t e = active ? a.in_off[r + 1] : 0;
+                if (active && e - b < kWarpRowDegree) {
                     dev::CSum acc;
-                    for (uint64_t x = b; x < e; ++x) acc.add(s_vals[x - a0]);
+                    for (uint64_t x = b; x < e; ++x) acc.add(sv[x - a0]);
                     finalize_row(a, ps, r, acc.value(), cur, nxt, cnxt, res, dang);
-                } else {
-                    const uint32_t slot = atomicAdd(&s_nwarp_rows, 1u);
-                    s_warp_rows[slot] = r;
+                }
+                uint32_t big = __ballot_sync(0xffffffffu, active && (e - b >= kWarpRowDegree));
+                while (big) {
+                    const int src = __ffs(big) - 1;
+                    big &= big - 1;
+                    const uint64_t bb = __shfl_sync(0xffffffffu, b, src);
+                    const uint64_t ee = __shfl_sync(0xffffffffu, e, src);
+                    dev::CSum acc;
+                    for (uint64_t x = bb + lane; x < ee; x += 32) acc.add(sv[x - a0]);
+                    acc = dev::warp_reduce(acc);
+                    if (lane == 0) finalize_row(a, ps, rb + src, acc.value(), cur, nxt, cnxt, res, dang);
                 }
             }
-            __syncthreads();
-            // rows with in-degree >= 32: one warp each
-            const uint32_t nwr = s_nwarp_rows;
-            for (uint32_t j = warp; j < nwr; j += nwarps) {
-                const uint32_t r = s_warp_rows[j];
-                const uint64_t b = a.in_off[r], e = a.in_off[r + 1];
-                dev::CSum acc;
-                for (uint64_t x = b + lane; x < e; x += 32) acc.add(s_vals[x - a0]);
-                acc = dev::warp_reduce(acc);
-                if (lane == 0) finalize_row(a, ps, r, acc.value(), cur, nxt, cnxt, res, dang);
-            }
-            __syncthreads();
+            __syncwarp();
         }
     }
 
     const double bres = dev::block_sum(res, s_red);
     __syncthreads();
     const double bdang = dev::block_sum(dang, s_red);
-    if (tid == 0) {
+    if (threadIdx.x == 0) {
         atomicAdd(&a.residual[it], bres);
         atomicAdd(&a.dangling[it + 1], bdang);
         __threadfence();

@@ -10,18 +10,26 @@
 // IEEE add the reference uses, compared as ordered bit patterns (valid for
 // non-negative floats).
 //
-// Per round only the frontier (vertices whose label dropped in the previous
-// round) is expanded.  A CTA stages 256 frontier vertices (row offset,
-// degree, label) in shared memory, prefix-sums their degrees, and all its
-// threads walk the combined edge list, so rows of any length are balanced
-// inside the CTA.  Rows of >= kHubDegree edges are cut into kHubChunk-edge
-// tasks for a second, grid-wide kernel.  A vertex joins the next frontier
-// once per round (round stamp), appended with one warp-aggregated atomic.
-// All round state lives on the device; inside a CUDA graph the rounds run
-// as a conditional while-loop with no host round trip.
+// Schedule: near/far buckets (Delta-stepping with one far pile).  Vertices
+// whose label drops below the current threshold T join the next near
+// frontier; the others go to the far pile.  When the near frontier runs
+// dry, T grows by Delta and the far pile is split: entries now below T
+// become the near frontier, entries below the old threshold are stale
+// (already settled) and are dropped.  Delta = infinity is plain frontier
+// Bellman-Ford (used for float weights).
+//
+// Expansion is warp-centric: a warp takes 32 frontier vertices, prefix-sums
+// their degrees with shuffles and walks the combined edge list 32 edges at
+// a time, finding each edge's owner with a 5-step shuffle binary search.
+// Rows of >= kHubDegree edges become kHubChunk-edge tasks for a grid-wide
+// second kernel.  A vertex joins a frontier once per round (round stamp) and
+// the far pile once per phase (phase stamp), appended with one
+// warp-aggregated atomic.  All round state lives on the device; inside a
+// CUDA graph the rounds run as a conditional while-loop.
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 
 #include "common.cuh"
@@ -36,15 +44,21 @@ namespace {
 constexpr int kSSThreads = 256;
 constexpr uint32_t kHubDegree = 4096;
 constexpr uint32_t kHubChunk = 4096;
+constexpr uint32_t kNoDelta = 0xFFFFFFFFu;
 
 struct SSHeader {
-    uint32_t round;     // rounds completed
+    uint32_t round;      // rounds completed
     uint32_t done;
     uint32_t converged;
-    uint32_t qsize[2];  // frontier sizes, indexed by round parity
+    uint32_t phase;      // far-pile generation
+    uint32_t pending;    // 1: this round starts by splitting the far pile
+    uint32_t threshold;  // near/far boundary T
+    uint32_t old_threshold;
+    uint32_t delta;
+    uint32_t qsize[2];   // near frontier sizes, by round parity
+    uint32_t fsize[2];   // far pile sizes, by phase parity
     uint32_t hub_count;
     uint32_t max_rounds;
-    uint32_t pad;
     unsigned long long relaxations;     // edges relaxed
     unsigned long long frontier_total;  // frontier vertices expanded
 };
@@ -54,8 +68,10 @@ struct SSArgs {
     const uint32_t *cols;
     const uint32_t *weights;
     uint32_t *dist;
-    uint32_t *stamp;
+    uint32_t *stamp;   // round in whose frontier a vertex sits
+    uint32_t *fstamp;  // far-pile generation that holds a vertex
     uint32_t *queue[2];
+    uint32_t *far[2];
     uint2 *hubs;
     SSHeader *hdr;
     uint32_t V;
@@ -84,108 +100,148 @@ __device__ __forceinline__ uint32_t extend(uint32_t d, uint32_t w) {
     }
 }
 
-__device__ __forceinline__ void relax(uint32_t *dist, uint32_t *stamp, uint32_t u, uint32_t nd,
-                                      uint32_t next_stamp, uint32_t *qnext, uint32_t *qnext_size) {
-    if (nd < __ldcg(dist + u)) {
-        const uint32_t old = atomicMin(dist + u, nd);
-        if (nd < old && atomicExch(stamp + u, next_stamp) != next_stamp) {
-            cg::coalesced_group g = cg::coalesced_threads();
-            uint32_t base = 0;
-            if (g.thread_rank() == 0) base = atomicAdd(qnext_size, g.size());
-            base = g.shfl(base, 0);
-            qnext[base + g.thread_rank()] = u;
+__device__ __forceinline__ void append(uint32_t *list, uint32_t *size, uint32_t v) {
+    cg::coalesced_group g = cg::coalesced_threads();
+    uint32_t base = 0;
+    if (g.thread_rank() == 0) base = atomicAdd(size, g.size());
+    base = g.shfl(base, 0);
+    list[base + g.thread_rank()] = v;
+}
+
+// Per-round view of the header, read once by every thread.
+struct RoundView {
+    uint32_t r, qn, threshold, next_stamp, far_stamp;
+    const uint32_t *q;
+    uint32_t *qnext, *qnext_size, *far, *far_size;
+};
+
+__device__ __forceinline__ RoundView round_view(const SSArgs &a) {
+    const SSHeader *h = a.hdr;
+    RoundView rv;
+    rv.r = *(volatile const uint32_t *)&h->round;
+    const uint32_t odd = rv.r & 1;
+    rv.qn = *(volatile const uint32_t *)(odd ? &h->qsize[1] : &h->qsize[0]);
+    rv.q = odd ? a.queue[1] : a.queue[0];
+    rv.qnext = odd ? a.queue[0] : a.queue[1];
+    rv.qnext_size = odd ? &a.hdr->qsize[0] : &a.hdr->qsize[1];
+    rv.threshold = *(volatile const uint32_t *)&h->threshold;
+    rv.next_stamp = rv.r + 1;
+    // During a split round the far pile of the next phase is already active.
+    const uint32_t p = *(volatile const uint32_t *)&h->phase + *(volatile const uint32_t *)&h->pending;
+    rv.far = (p & 1) ? a.far[1] : a.far[0];
+    rv.far_size = (p & 1) ? &a.hdr->fsize[1] : &a.hdr->fsize[0];
+    rv.far_stamp = p + 1;
+    return rv;
+}
+
+__device__ __forceinline__ void relax(const SSArgs &a, const RoundView &rv, uint32_t u, uint32_t nd) {
+    if (nd < __ldcg(a.dist + u)) {
+        const uint32_t old = atomicMin(a.dist + u, nd);
+        if (nd < old) {
+            if (nd < rv.threshold) {
+                if (atomicExch(a.stamp + u, rv.next_stamp) != rv.next_stamp) append(rv.qnext, rv.qnext_size, u);
+            } else {
+                if (atomicExch(a.fstamp + u, rv.far_stamp) != rv.far_stamp) append(rv.far, rv.far_size, u);
+            }
+        }
+    }
+}
+
+// Splits the far pile at the start of a round whose near frontier is empty.
+__global__ void __launch_bounds__(kSSThreads) sssp_split_kernel(const SSArgs *__restrict__ args) {
+    const SSArgs a = *args;
+    const SSHeader *h = a.hdr;
+    if (*(volatile const uint32_t *)&h->done || !*(volatile const uint32_t *)&h->pending) return;
+    const uint32_t r = h->round, p = h->phase;
+    const uint32_t lo = h->old_threshold, hi = h->threshold;
+    const uint32_t n = (p & 1) ? h->fsize[1] : h->fsize[0];
+    const uint32_t *src = (p & 1) ? a.far[1] : a.far[0];
+    uint32_t *dst = (p & 1) ? a.far[0] : a.far[1];
+    uint32_t *dst_size = (p & 1) ? &a.hdr->fsize[0] : &a.hdr->fsize[1];
+    uint32_t *near = (r & 1) ? a.queue[1] : a.queue[0];
+    uint32_t *near_size = (r & 1) ? &a.hdr->qsize[1] : &a.hdr->qsize[0];
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const uint32_t v = src[i];
+        const uint32_t d = __ldcg(a.dist + v);
+        if (d < lo) continue;  // settled in an earlier phase
+        if (d < hi) {
+            a.stamp[v] = r;
+            append(near, near_size, v);
+        } else {
+            a.fstamp[v] = p + 2;
+            append(dst, dst_size, v);
         }
     }
 }
 
 template <int WK>
 __global__ void __launch_bounds__(kSSThreads) sssp_expand_kernel(const SSArgs *__restrict__ args) {
-    __shared__ uint32_t s_scan[kSSThreads + 1];
-    __shared__ uint64_t s_off[kSSThreads];
-    __shared__ uint32_t s_d[kSSThreads];
-    __shared__ uint32_t s_wsum[kSSThreads / 32];
-
     const SSArgs a = *args;
     if (*(volatile uint32_t *)&a.hdr->done) return;
-    const uint32_t r = *(volatile uint32_t *)&a.hdr->round;
-    const uint32_t qn = *(volatile uint32_t *)((r & 1) ? &a.hdr->qsize[1] : &a.hdr->qsize[0]);
-    const uint32_t *q = (r & 1) ? a.queue[1] : a.queue[0];
-    uint32_t *qnext = (r & 1) ? a.queue[0] : a.queue[1];
-    uint32_t *qnext_size = (r & 1) ? &a.hdr->qsize[0] : &a.hdr->qsize[1];
-    const uint32_t next_stamp = r + 1;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const RoundView rv = round_view(a);
+    const int lane = threadIdx.x & 31;
+    const uint32_t gwarp = (blockIdx.x * kSSThreads + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * kSSThreads) >> 5;
     unsigned long long relaxed = 0;
 
-    for (uint32_t chunk = blockIdx.x; uint64_t(chunk) * kSSThreads < qn; chunk += gridDim.x) {
-        const uint32_t i = chunk * kSSThreads + tid;
+    for (uint32_t w = gwarp; uint64_t(w) * 32 < rv.qn; w += nwarps) {
+        const uint32_t i = w * 32 + lane;
         uint32_t deg = 0, d = a.inf;
         uint64_t off = 0;
-        if (i < qn) {
-            const uint32_t v = q[i];
+        if (i < rv.qn) {
+            const uint32_t v = rv.q[i];
             off = a.row_off[v];
             const uint64_t full = a.row_off[v + 1] - off;
             d = __ldcg(a.dist + v);
+            relaxed += full;
             if (full >= kHubDegree) {
                 const uint32_t nch = static_cast<uint32_t>((full + kHubChunk - 1) / kHubChunk);
                 const uint32_t base = atomicAdd(&a.hdr->hub_count, nch);
                 for (uint32_t c = 0; c < nch; ++c) a.hubs[base + c] = make_uint2(v, c);
-                relaxed += full;
             } else {
                 deg = static_cast<uint32_t>(full);
             }
         }
-        // block-wide exclusive prefix of the staged degrees
-        uint32_t x = deg;
+        // inclusive prefix of the 32 degrees
+        uint32_t incl = deg;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
         }
-        if (lane == 31) s_wsum[warp] = x;
-        __syncthreads();
-        if (warp == 0) {
-            uint32_t w = (lane < kSSThreads / 32) ? s_wsum[lane] : 0u;
+        const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+        for (uint32_t base = 0; base < total; base += 32) {
+            const uint32_t j = base + lane;
+            // owner = first lane whose inclusive prefix exceeds j
+            uint32_t lo = 0;
 #pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
-                if (lane >= o) w += y;
+            for (uint32_t step = 16; step > 0; step >>= 1) {
+                const uint32_t probe = __shfl_sync(0xffffffffu, incl, lo + step - 1);
+                if (probe <= j) lo += step;
             }
-            if (lane < kSSThreads / 32) s_wsum[lane] = w;
-        }
-        __syncthreads();
-        const uint32_t excl = x - deg + (warp > 0 ? s_wsum[warp - 1] : 0u);
-        s_scan[tid] = excl;
-        s_off[tid] = off;
-        s_d[tid] = d;
-        if (tid == kSSThreads - 1) s_scan[kSSThreads] = excl + deg;
-        __syncthreads();
-        const uint32_t total = s_scan[kSSThreads];
-        if (tid == 0) relaxed += total;
-        for (uint32_t j = tid; j < total; j += kSSThreads) {
-            int lo = 0, hi = kSSThreads - 1;  // last staged vertex whose prefix <= j
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (s_scan[mid] <= j) lo = mid; else hi = mid - 1;
+            const uint32_t o_incl = __shfl_sync(0xffffffffu, incl, lo);
+            const uint32_t o_deg = __shfl_sync(0xffffffffu, deg, lo);
+            const uint64_t o_off = __shfl_sync(0xffffffffu, off, lo);
+            const uint32_t o_d = __shfl_sync(0xffffffffu, d, lo);
+            if (j < total) {
+                const uint64_t e = o_off + (j - (o_incl - o_deg));
+                const uint32_t u = dev::ld_stream(a.cols + e);
+                relax(a, rv, u, extend<WK>(o_d, edge_weight<WK>(a.weights, e)));
             }
-            const uint64_t e = s_off[lo] + (j - s_scan[lo]);
-            const uint32_t u = dev::ld_stream(a.cols + e);
-            const uint32_t w = edge_weight<WK>(a.weights, e);
-            relax(a.dist, a.stamp, u, extend<WK>(s_d[lo], w), next_stamp, qnext, qnext_size);
         }
-        __syncthreads();
     }
-    if (relaxed) atomicAdd(&a.hdr->relaxations, relaxed);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) relaxed += __shfl_xor_sync(0xffffffffu, relaxed, o);
+    if (lane == 0 && relaxed) atomicAdd(&a.hdr->relaxations, relaxed);
 }
 
 template <int WK>
 __global__ void __launch_bounds__(kSSThreads) sssp_hub_kernel(const SSArgs *__restrict__ args) {
     const SSArgs a = *args;
     if (*(volatile uint32_t *)&a.hdr->done) return;
-    const uint32_t r = *(volatile uint32_t *)&a.hdr->round;
+    const RoundView rv = round_view(a);
     const uint32_t n = *(volatile uint32_t *)&a.hdr->hub_count;
-    uint32_t *qnext = (r & 1) ? a.queue[0] : a.queue[1];
-    uint32_t *qnext_size = (r & 1) ? &a.hdr->qsize[0] : &a.hdr->qsize[1];
-    const uint32_t next_stamp = r + 1;
     for (uint32_t t = blockIdx.x; t < n; t += gridDim.x) {
         const uint2 h = a.hubs[t];
         const uint64_t rb = a.row_off[h.x], re = a.row_off[h.x + 1];
@@ -194,7 +250,7 @@ __global__ void __launch_bounds__(kSSThreads) sssp_hub_kernel(const SSArgs *__re
         const uint32_t d = __ldcg(a.dist + h.x);
         for (uint64_t x = b + threadIdx.x; x < e; x += kSSThreads) {
             const uint32_t u = dev::ld_stream(a.cols + x);
-            relax(a.dist, a.stamp, u, extend<WK>(d, edge_weight<WK>(a.weights, x)), next_stamp, qnext, qnext_size);
+            relax(a, rv, u, extend<WK>(d, edge_weight<WK>(a.weights, x)));
         }
     }
 }
@@ -209,9 +265,26 @@ __global__ void sssp_round_end_kernel(const SSArgs *__restrict__ args) {
     h->qsize[r & 1] = 0;
     h->hub_count = 0;
     h->round = r + 1;
-    if (n_next == 0 || r + 1 >= h->max_rounds) {
+    if (h->pending) {  // the split of this round consumed the old far pile
+        h->fsize[h->phase & 1] = 0;
+        h->phase += 1;
+        h->pending = 0;
+    }
+    bool finish = false, conv = false;
+    if (n_next == 0) {
+        if (h->fsize[h->phase & 1] == 0) {
+            finish = conv = true;
+        } else {
+            h->pending = 1;
+            h->old_threshold = h->threshold;
+            const uint64_t t = uint64_t(h->threshold) + h->delta;
+            h->threshold = t >= 0xFFFFFFFFull ? 0xFFFFFFFFu : static_cast<uint32_t>(t);
+        }
+    }
+    if (!finish && r + 1 >= h->max_rounds) finish = true;
+    if (finish) {
         h->done = 1;
-        h->converged = (n_next == 0) ? 1u : 0u;
+        h->converged = conv ? 1u : 0u;
         if (a.use_cond) cudaGraphSetConditional(a.cond, 0);
     }
 }
@@ -223,31 +296,32 @@ __global__ void sssp_init_kernel(const SSArgs *__restrict__ args) {
         const bool s = (v == a.source);
         a.dist[v] = s ? 0u : a.inf;
         a.stamp[v] = s ? 0u : 0xFFFFFFFFu;
+        a.fstamp[v] = 0xFFFFFFFFu;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) a.queue[0][0] = a.source;
 }
 
 template <int WK>
-struct SSKernels {
-    static int grid() {
-        static int g = 0;
-        if (g == 0) {
-            int per_sm = 0;
-            HYT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sssp_expand_kernel<WK>, kSSThreads, 0));
-            g = sm_count() * std::max(per_sm, 1);
-        }
-        return g;
+int expand_grid() {
+    static int g = 0;
+    if (g == 0) {
+        int per_sm = 0;
+        HYT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sssp_expand_kernel<WK>, kSSThreads, 0));
+        g = sm_count() * std::max(per_sm, 1);
     }
-};
+    return g;
+}
 
 template <int WK>
-void sssp_solve(GraphImpl &g, uint32_t source, uint32_t max_rounds, uint32_t flags, cudaStream_t s,
+void sssp_solve(GraphImpl &g, uint32_t source, uint32_t delta, uint32_t max_rounds, uint32_t flags, cudaStream_t s,
                 uint32_t *dist_out, hyt_run_stats *stats) {
     const uint64_t V = g.V;
     if (g.dist.count < V) g.dist.allocate(V);
-    if (g.stamp.count < V) g.stamp.allocate(V);
-    for (int i = 0; i < 2; ++i)
+    if (g.stamp.count < 2 * V) g.stamp.allocate(2 * V);
+    for (int i = 0; i < 2; ++i) {
         if (g.queue[i].count < V) g.queue[i].allocate(V);
+        if (g.far[i].count < V) g.far[i].allocate(V);
+    }
     const uint64_t hub_cap = 2 * (g.E / kHubChunk) + 2;
     if (g.hub_tasks.count < hub_cap) g.hub_tasks.allocate(hub_cap);
     const size_t sb = 512 + sizeof(SSHeader);
@@ -261,8 +335,11 @@ void sssp_solve(GraphImpl &g, uint32_t source, uint32_t max_rounds, uint32_t fla
     a.weights = g.weights.get();
     a.dist = g.dist.get();
     a.stamp = g.stamp.get();
-    a.queue[0] = g.queue[0].get();
-    a.queue[1] = g.queue[1].get();
+    a.fstamp = g.stamp.get() + V;
+    for (int i = 0; i < 2; ++i) {
+        a.queue[i] = g.queue[i].get();
+        a.far[i] = g.far[i].get();
+    }
     a.hubs = g.hub_tasks.get();
     a.hdr = hdr;
     a.V = static_cast<uint32_t>(V);
@@ -272,6 +349,8 @@ void sssp_solve(GraphImpl &g, uint32_t source, uint32_t max_rounds, uint32_t fla
     SSHeader h0{};
     h0.qsize[0] = 1;
     h0.max_rounds = max_rounds;
+    h0.delta = delta;
+    h0.threshold = (WK == HYT_WEIGHTS_F32 || delta == kNoDelta) ? 0xFFFFFFFFu : delta;
 
     const bool use_graph = !(flags & HYT_RUN_NO_GRAPH) && !(flags & HYT_RUN_PROFILE);
     cudaGraph_t graph = nullptr;
@@ -281,7 +360,7 @@ void sssp_solve(GraphImpl &g, uint32_t source, uint32_t max_rounds, uint32_t fla
         HYT_CUDA(cudaGraphConditionalHandleCreate(&a.cond, graph, 1, cudaGraphCondAssignDefault));
         a.use_cond = 1;
     }
-    const int grid = SSKernels<WK>::grid();
+    const int grid = expand_grid<WK>();
 
     EventTimer total;
     total.start(s);
@@ -306,9 +385,11 @@ void sssp_solve(GraphImpl &g, uint32_t source, uint32_t max_rounds, uint32_t fla
         kp.kernelParams = kargs;
         kp.blockDim = dim3(kSSThreads);
         kp.gridDim = dim3(grid);
+        cudaGraphNode_t n0, n1, n2, n3;
+        kp.func = reinterpret_cast<void *>(sssp_split_kernel);
+        HYT_CUDA(cudaGraphAddKernelNode(&n0, body, nullptr, 0, &kp));
         kp.func = reinterpret_cast<void *>(sssp_expand_kernel<WK>);
-        cudaGraphNode_t n1, n2, n3;
-        HYT_CUDA(cudaGraphAddKernelNode(&n1, body, nullptr, 0, &kp));
+        HYT_CUDA(cudaGraphAddKernelNode(&n1, body, &n0, 1, &kp));
         kp.func = reinterpret_cast<void *>(sssp_hub_kernel<WK>);
         HYT_CUDA(cudaGraphAddKernelNode(&n2, body, &n1, 1, &kp));
         kp.func = reinterpret_cast<void *>(sssp_round_end_kernel);
@@ -321,13 +402,14 @@ void sssp_solve(GraphImpl &g, uint32_t source, uint32_t max_rounds, uint32_t fla
         EventTimer kt;
         for (uint32_t r = 0; r < max_rounds; ++r) {
             if (flags & HYT_RUN_PROFILE) kt.start(s);
+            sssp_split_kernel<<<grid, kSSThreads, 0, s>>>(d_args);
             sssp_expand_kernel<WK><<<grid, kSSThreads, 0, s>>>(d_args);
             sssp_hub_kernel<WK><<<grid, kSSThreads, 0, s>>>(d_args);
             if (flags & HYT_RUN_PROFILE) kt.stop(s);
             sssp_round_end_kernel<<<1, 1, 0, s>>>(d_args);
             HYT_CUDA(cudaGetLastError());
-            launches += 3;
-            hot += 2;
+            launches += 4;
+            hot += 3;
             uint32_t done = 0;
             HYT_CUDA(cudaMemcpyAsync(&done, &hdr->done, sizeof(done), cudaMemcpyDeviceToHost, s));
             HYT_CUDA(cudaStreamSynchronize(s));
@@ -341,7 +423,7 @@ void sssp_solve(GraphImpl &g, uint32_t source, uint32_t max_rounds, uint32_t fla
     const double total_ms = total.ms();
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
-    if (use_graph) launches += 3 * h.round;
+    if (use_graph) launches += 4 * h.round;
     if (dist_out) copy_from_device(dist_out, g.dist.get(), V * sizeof(uint32_t), s);
     if (stats) {
         stats->iterations = h.round;
@@ -361,18 +443,28 @@ void sssp_solve(GraphImpl &g, uint32_t source, uint32_t max_rounds, uint32_t fla
 
 }  // namespace
 
+uint32_t sssp_default_delta(const GraphImpl &g) {
+    // Near/far bucket width: twice the mean edge weight (measured on the
+    // device when the graph is built).  Unweighted graphs use 1 (BFS order).
+    if (g.weight_kind == HYT_WEIGHTS_F32) return kNoDelta;
+    if (g.weight_kind == HYT_WEIGHTS_NONE) return 1;
+    return g.default_delta ? g.default_delta : kNoDelta;
+}
+
 void sssp_run(GraphImpl &g, const hyt_sssp_params &p, uint32_t *dist_out, hyt_run_stats *stats) {
     if (!(g.flags & HYT_GRAPH_PUSH)) fail(HYT_E_INVALID, "graph was created without HYT_GRAPH_PUSH");
     if (p.source >= g.V) fail(HYT_E_INVALID, "SSSP source vertex is out of range");
     if (!g.weights_ok) fail(HYT_E_INVALID, "SSSP requires finite non-negative edge weights");
     cudaStream_t s = p.stream ? static_cast<cudaStream_t>(p.stream) : g.stream;
-    // Each round lowers at least one label; with non-negative weights the
-    // label-correcting frontier empties within V rounds.
-    const uint32_t max_rounds = p.max_rounds ? p.max_rounds : static_cast<uint32_t>(std::min<uint64_t>(g.V + 1, 0xFFFFFFF0ull));
+    // Termination is guaranteed (labels only decrease, weights >= 0); the
+    // round cap is a safety bound on the device loop.
+    const uint64_t cap = std::min<uint64_t>(4 * g.V + 1024, 0x7FFFFFFFull);
+    const uint32_t max_rounds = p.max_rounds ? p.max_rounds : static_cast<uint32_t>(cap);
+    const uint32_t delta = p.delta ? p.delta : sssp_default_delta(g);
     switch (g.weight_kind) {
-        case HYT_WEIGHTS_NONE: sssp_solve<HYT_WEIGHTS_NONE>(g, p.source, max_rounds, p.flags, s, dist_out, stats); break;
-        case HYT_WEIGHTS_U32: sssp_solve<HYT_WEIGHTS_U32>(g, p.source, max_rounds, p.flags, s, dist_out, stats); break;
-        case HYT_WEIGHTS_F32: sssp_solve<HYT_WEIGHTS_F32>(g, p.source, max_rounds, p.flags, s, dist_out, stats); break;
+        case HYT_WEIGHTS_NONE: sssp_solve<HYT_WEIGHTS_NONE>(g, p.source, delta, max_rounds, p.flags, s, dist_out, stats); break;
+        case HYT_WEIGHTS_U32: sssp_solve<HYT_WEIGHTS_U32>(g, p.source, delta, max_rounds, p.flags, s, dist_out, stats); break;
+        case HYT_WEIGHTS_F32: sssp_solve<HYT_WEIGHTS_F32>(g, p.source, kNoDelta, max_rounds, p.flags, s, dist_out, stats); break;
         default: fail(HYT_E_INTERNAL, "unknown weight kind");
     }
 }
