@@ -7,6 +7,7 @@
 // GPU, so sources stay ascending inside every in-row exactly as the
 // reference's counting pass leaves them.
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -99,26 +100,53 @@ __global__ void offsets_from_sorted_kernel(const uint32_t *keys, uint64_t E, uin
 }
 
 // tile_start[k] = first row whose merge-path coordinate (row + in_offset)
-// reaches k * kTileCost.
-__global__ void tile_bounds_kernel(const uint64_t *in_off, uint64_t V, uint64_t E, uint64_t num_tiles,
+// reaches k * tile.
+__global__ void tile_bounds_kernel(const uint64_t *in_off, uint64_t V, uint64_t E, uint64_t num_tiles, uint32_t tile,
                                    uint32_t *tile_start) {
     const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
     for (uint64_t v = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; v <= V; v += stride) {
         const int64_t p_prev = (v == 0) ? -1 : static_cast<int64_t>((v - 1) + in_off[v - 1]);
         const int64_t p_cur = static_cast<int64_t>(v + in_off[v]);
-        int64_t k_lo = (p_prev < 0) ? 0 : p_prev / kTileCost + 1;
-        int64_t k_hi = (v == V) ? static_cast<int64_t>(num_tiles) : p_cur / kTileCost;
+        int64_t k_lo = (p_prev < 0) ? 0 : p_prev / tile + 1;
+        int64_t k_hi = (v == V) ? static_cast<int64_t>(num_tiles) : p_cur / tile;
         for (int64_t k = k_lo; k <= k_hi; ++k) tile_start[k] = static_cast<uint32_t>(v);
     }
 }
 
-__global__ void in_degree_kernel(const uint64_t *in_off, uint64_t V, uint32_t *deg, uint8_t *is_long) {
+__global__ void in_degree_kernel(const uint64_t *in_off, uint64_t V, uint32_t long_degree, uint32_t *deg,
+                                 uint8_t *is_long) {
     const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
     for (uint64_t v = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; v < V; v += stride) {
         const uint32_t d = static_cast<uint32_t>(in_off[v + 1] - in_off[v]);
         deg[v] = d;
-        is_long[v] = d >= kLongDegree;
+        is_long[v] = d >= long_degree;
     }
+}
+
+__global__ void iota_kernel(uint32_t *out, uint64_t n) {
+    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += stride) out[i] = static_cast<uint32_t>(i);
+}
+
+__global__ void hot_slot_kernel(const uint32_t *hot, uint32_t n, uint32_t *slot) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) slot[hot[i]] = i;
+}
+
+// Replaces hot sources in the CSC by kHotTag | slot; counts them.
+__global__ void tag_hot_kernel(uint32_t *in_src, uint64_t E, const uint32_t *slot, unsigned long long *count) {
+    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+    unsigned long long c = 0;
+    for (uint64_t e = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; e < E; e += stride) {
+        const uint32_t s = slot[in_src[e]];
+        if (s != 0xFFFFFFFFu) {
+            in_src[e] = kHotTag | s;
+            ++c;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, c);
 }
 
 __global__ void gather_u32_kernel(const uint32_t *src, const uint32_t *idx, uint64_t n, uint32_t *out) {
@@ -154,6 +182,19 @@ void graph_build(GraphImpl &g, const hyt_csr &csr, uint32_t flags) {
     if (csr.weight_kind != HYT_WEIGHTS_NONE && E > 0 && !csr.weights)
         fail(HYT_E_INVALID, "weights is NULL for a weighted graph");
     if (flags == 0) flags = HYT_GRAPH_ALL;
+    // PageRank decomposition knobs (same work, different tiling): tile cost
+    // in {64..512} and hot-source cache size, bounded by shared memory.
+    g.tile_cost = kTileCostDefault;
+    if (const char *t = std::getenv("HYT_PR_TILE")) {
+        const unsigned long v = std::strtoul(t, nullptr, 10);
+        if (v >= 64 && v <= kTileCostMax) g.tile_cost = static_cast<uint32_t>(v);
+    }
+    uint32_t hot_request = kHotSourcesDefault;
+    if (const char *t = std::getenv("HYT_PR_HOT")) hot_request = static_cast<uint32_t>(std::strtoul(t, nullptr, 10));
+    hot_request = std::min(hot_request, kHotSourcesMax);
+    while (hot_request && pr_shared_bytes(hot_request, g.tile_cost) > kPRSmemMax) hot_request /= 2;
+    if ((flags & HYT_GRAPH_PULL) && V > (kHotTag >> 0) - 1)
+        fail(HYT_E_UNSUPPORTED, "pull graphs hold fewer than 2^31 vertices (bit 31 tags cached sources)");
 
     cudaStream_t s = g.stream;
     EventTimer timer;
@@ -233,17 +274,41 @@ void graph_build(GraphImpl &g, const hyt_csr &csr, uint32_t flags) {
         HYT_CUDA(cudaGetLastError());
         keys.release();
 
+        // Hot sources: largest out-degree first (ties by vertex id).
+        g.num_hot = static_cast<uint32_t>(std::min<uint64_t>(hot_request, V));
+        if (E && g.num_hot) {
+            DeviceArray<uint32_t> deg(V), ids(V), slot(V);
+            HYT_CUDA(cudaMemcpyAsync(deg.get(), g.out_degree.get(), V * 4, cudaMemcpyDeviceToDevice, s));
+            iota_kernel<<<grid_for(V, 256), 256, 0, s>>>(ids.get(), V);
+            HYT_CUDA(cudaGetLastError());
+            prims::sort_pairs_desc_u32(deg.get(), ids.get(), V, s);
+            g.hot_vertex.allocate(g.num_hot);
+            HYT_CUDA(cudaMemcpyAsync(g.hot_vertex.get(), ids.get(), g.num_hot * 4ull, cudaMemcpyDeviceToDevice, s));
+            HYT_CUDA(cudaMemsetAsync(slot.get(), 0xFF, V * 4, s));
+            hot_slot_kernel<<<(g.num_hot + 255) / 256, 256, 0, s>>>(g.hot_vertex.get(), g.num_hot, slot.get());
+            HYT_CUDA(cudaMemsetAsync(counter.get(), 0, sizeof(unsigned long long), s));
+            tag_hot_kernel<<<grid_for(E, 256), 256, 0, s>>>(g.in_sources.get(), E, slot.get(), counter.get());
+            HYT_CUDA(cudaGetLastError());
+            unsigned long long h_hot = 0;
+            HYT_CUDA(cudaMemcpyAsync(&h_hot, counter.get(), sizeof(h_hot), cudaMemcpyDeviceToHost, s));
+            HYT_CUDA(cudaStreamSynchronize(s));
+            g.hot_edges = h_hot;
+        } else {
+            g.num_hot = 0;
+        }
+
         // Work tiles along the merge path.
-        g.num_tiles = (V + E) / kTileCost + 1;
+        g.num_tiles = (V + E) / g.tile_cost + 1;
         g.tile_start.allocate(g.num_tiles + 1);
-        tile_bounds_kernel<<<grid_for(V + 1, 256), 256, 0, s>>>(g.in_offsets.get(), V, E, g.num_tiles,
+        tile_bounds_kernel<<<grid_for(V + 1, 256), 256, 0, s>>>(g.in_offsets.get(), V, E, g.num_tiles, g.tile_cost,
                                                                  g.tile_start.get());
         HYT_CUDA(cudaGetLastError());
 
-        // Long rows (in-degree >= kLongDegree) and their chunk tasks.
+        // Long rows (in-degree >= tile_cost) and their chunk tasks.
         DeviceArray<uint32_t> in_deg(V);
         DeviceArray<uint8_t> is_long(V);
-        in_degree_kernel<<<grid_for(V, 256), 256, 0, s>>>(g.in_offsets.get(), V, in_deg.get(), is_long.get());
+        in_degree_kernel<<<grid_for(V, 256), 256, 0, s>>>(g.in_offsets.get(), V, g.tile_cost, in_deg.get(),
+                                                           is_long.get());
         HYT_CUDA(cudaGetLastError());
         g.max_in_degree = prims::reduce_max_u32(in_deg.get(), V, s);
         DeviceArray<uint32_t> long_ids(V);

@@ -19,16 +19,19 @@
 namespace hyt {
 
 // PageRank pull work decomposition.  Rows are cut into tiles along the
-// merge path (1 unit per row + 1 per in-edge): a tile spans kTileCost units,
-// so its rows hold fewer than kTileCost edges except for its last row.  A
-// last row with in-degree >= kLongDegree is a "long row": it is excluded
-// from the tile and split into kLongChunk-edge chunks.  One warp processes
-// one task (tile or chunk), so a tile's staged contributions fit in a
-// per-warp shared-memory slice of kStageCap floats.
-constexpr uint32_t kTileCost = 512;
-constexpr uint32_t kLongDegree = kTileCost;
+// merge path (1 unit per row + 1 per in-edge): a tile spans tile_cost units,
+// so its rows hold fewer than tile_cost edges except for its last row.  A
+// last row with in-degree >= tile_cost is a "long row": it is excluded from
+// the tile and split into kLongChunk-edge chunks.  One warp processes one
+// task (tile or chunk), so a tile's staged contributions fit in a per-warp
+// shared-memory slice of 2 * tile_cost floats.
+constexpr uint32_t kTileCostDefault = 512;   // merge-path units per tile (tunable: HYT_PR_TILE)
+constexpr uint32_t kTileCostMax = 512;
 constexpr uint32_t kLongChunk = 4096;
-constexpr uint32_t kStageCap = kTileCost + kLongDegree;  // staged edges per tile
+constexpr uint32_t kHotSourcesDefault = 8192;   // shared-memory source cache (tunable: HYT_PR_HOT)
+constexpr uint32_t kHotSourcesMax = 32768;
+constexpr uint32_t kPRSmemMax = 226 * 1024;     // dynamic shared memory per CTA (227 KB opt-in - static)
+constexpr uint32_t kHotTag = 0x80000000u;       // in_sources tag: source is hot slot (low bits)
 
 struct LongRow {
     uint32_t row;
@@ -61,6 +64,13 @@ struct GraphImpl {
     DeviceArray<LongRow> long_rows;     // [num_long]
     DeviceArray<uint2> chunk_tasks;     // [num_chunks] = (long row index, chunk)
     uint64_t num_tiles = 0, num_long = 0, num_chunks = 0;
+    uint32_t tile_cost = kTileCostDefault;  // a row is long when its in-degree >= tile_cost
+    // Hot sources: the num_hot vertices of largest out-degree.  Their
+    // occurrences in in_sources carry kHotTag | slot, and each PageRank CTA
+    // keeps their contributions in shared memory for the iteration.
+    DeviceArray<uint32_t> hot_vertex;   // [num_hot], by slot
+    uint32_t num_hot = 0;
+    uint64_t hot_edges = 0;             // in-edges whose source is hot
 
     // host-side facts
     uint64_t max_in_degree = 0, max_out_degree = 0, dangling = 0;
@@ -84,6 +94,13 @@ struct GraphImpl {
 
     size_t device_bytes() const;
 };
+
+// PageRank CTA shape: kPRThreads threads; dynamic shared memory = hot cache
+// + one staging slice (2 * tile_cost + 8 floats) per warp.
+constexpr int kPRThreads = 1024;
+inline size_t pr_shared_bytes(uint32_t num_hot, uint32_t tile_cost) {
+    return (size_t(num_hot) + size_t(kPRThreads / 32) * (2 * size_t(tile_cost) + 8)) * sizeof(float);
+}
 
 // Builds the device graph from a CSR (host or device pointers).
 void graph_build(GraphImpl &g, const hyt_csr &csr, uint32_t flags);

@@ -32,7 +32,6 @@
 namespace hyt {
 namespace {
 
-constexpr int kPRThreads = 256;
 constexpr uint32_t kWarpRowDegree = 16;  // rows with more in-edges are summed by a whole warp
 
 struct PRHeader {
@@ -51,6 +50,9 @@ struct PRArgs {
     const uint32_t *tile_start;
     const LongRow *long_rows;
     const uint2 *chunk_tasks;
+    const uint32_t *hot_vertex;  // [num_hot] vertices cached in shared memory
+    uint32_t num_hot;
+    uint32_t tile_cost;
     float *rank[2];
     float *contrib[2];
     float2 *partial;
@@ -99,45 +101,46 @@ __device__ __forceinline__ void finalize_row(const PRArgs &a, const PRState &ps,
     if (od == 0) dang += static_cast<double>(nx);
 }
 
-// Gathers contributions for edges [lo, hi) of the in-source array into
-// registers: 4 x 128-bit streaming loads of source ids per lane, then 16
-// independent gathers, so every lane keeps 16 loads in flight.  Index
-// x = a0 + 4*i + c; edges outside [lo, hi) read contribution 0 (their
-// addresses are clamped to a valid row, the value is discarded).
-constexpr int kUnroll = 4;
+// Gathers the contributions of edges [lo, hi) of the in-source array.
+// Lane l of the warp takes edges lo + base + 32k + l (k < kBatch): each of
+// the kBatch id loads is one coalesced 128-byte access, and because the
+// sources of an in-row are sorted, the 32 addresses of each gather
+// instruction are ascending and neighbouring lanes often share an L2 sector
+// (dense for hub-heavy rows).  All kBatch gathers of a lane are issued
+// before any is consumed.  Edges past hi yield 0 and read a clamped address.
+constexpr int kBatch = 16;
 
 template <class Sink>
-__device__ __forceinline__ void gather_span(const uint32_t *in_src, const float *ccur, uint64_t lo, uint64_t hi,
-                                            uint64_t pol, int lane, Sink &&sink) {
-    const uint64_t a0 = lo & ~3ull;
-    const uint32_t nvec = static_cast<uint32_t>((hi - a0 + 3) >> 2);
-    const uint4 *src4 = reinterpret_cast<const uint4 *>(in_src + a0);
-    for (uint32_t base = 0; base < nvec; base += 32 * kUnroll) {
-        uint4 q[kUnroll];
+__device__ __forceinline__ void gather_span(const uint32_t *in_src, const float *ccur, const float *s_hot, uint64_t lo,
+                                            uint64_t hi, uint64_t pol, int lane, Sink &&sink) {
+    const uint32_t n = static_cast<uint32_t>(hi - lo);
+    const uint32_t *src = in_src + lo;
+    for (uint32_t base = 0; base < n; base += 32 * kBatch) {
+        uint32_t id[kBatch];
 #pragma unroll
-        for (int u = 0; u < kUnroll; ++u) {
-            const uint32_t i = base + lane + 32 * u;
-            q[u] = (i < nvec) ? dev::ld_stream4(src4 + i) : make_uint4(0, 0, 0, 0);
+        for (int k = 0; k < kBatch; ++k) {
+            const uint32_t i = base + 32 * k + lane;
+            id[k] = (i < n) ? dev::ld_stream(src + i) : 0u;
         }
-        float v[kUnroll][4];
+        float v[kBatch];
 #pragma unroll
-        for (int u = 0; u < kUnroll; ++u) {
-            const uint64_t x = a0 + 4ull * (base + lane + 32 * u);
-            const uint32_t ids[4] = {q[u].x, q[u].y, q[u].z, q[u].w};
-#pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                const bool ok = (x + c >= lo) && (x + c < hi);
-                v[u][c] = dev::ld_keep(ccur + (ok ? ids[c] : 0u), pol);
-                if (!ok) v[u][c] = 0.0f;
-            }
+        for (int k = 0; k < kBatch; ++k) {
+            v[k] = 0.0f;
+            if (!(id[k] & kHotTag)) v[k] = dev::ld_keep(ccur + id[k], pol);
         }
 #pragma unroll
-        for (int u = 0; u < kUnroll; ++u) sink(base + lane + 32 * u, v[u]);
+        for (int k = 0; k < kBatch; ++k)
+            if (id[k] & kHotTag) v[k] = s_hot[id[k] & ~kHotTag];
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k) {
+            const uint32_t i = base + 32 * k + lane;
+            if (i < n) sink(i, v[k]);
+        }
     }
 }
 
-__global__ void __launch_bounds__(kPRThreads, 4) pr_iterate_kernel(const PRArgs *__restrict__ args) {
-    __shared__ __align__(16) float s_vals[kPRThreads / 32][kStageCap + 8];
+__global__ void __launch_bounds__(kPRThreads, 1) pr_iterate_kernel(const PRArgs *__restrict__ args) {
+    extern __shared__ __align__(16) float s_dyn[];
     __shared__ double s_red[32];
 
     const PRArgs a = *args;
@@ -161,7 +164,26 @@ __global__ void __launch_bounds__(kPRThreads, 4) pr_iterate_kernel(const PRArgs 
     const uint64_t total_tasks = a.num_chunks + a.num_tiles;
     double res = 0.0, dang = 0.0;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    float *sv = s_vals[warp];
+    // Hot-source contributions for this iteration, loaded once per CTA.
+    float *s_hot = s_dyn;
+    for (uint32_t i0 = 0; i0 < a.num_hot; i0 += 8 * kPRThreads) {
+        uint32_t hv[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const uint32_t i = i0 + k * kPRThreads + threadIdx.x;
+            hv[k] = (i < a.num_hot) ? a.hot_vertex[i] : 0u;
+        }
+        float hc[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) hc[k] = ccur[hv[k]];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const uint32_t i = i0 + k * kPRThreads + threadIdx.x;
+            if (i < a.num_hot) s_hot[i] = hc[k];
+        }
+    }
+    __syncthreads();
+    float *sv = s_dyn + a.num_hot + warp * (2 * a.tile_cost + 8);
     const uint64_t nwarps = uint64_t(gridDim.x) * (kPRThreads / 32);
 
     // Static round-robin over tasks: every task costs at most one chunk of
@@ -175,12 +197,7 @@ __global__ void __launch_bounds__(kPRThreads, 4) pr_iterate_kernel(const PRArgs 
             const uint64_t b = rb + uint64_t(t.y) * kLongChunk;
             const uint64_t e = (b + kLongChunk < re) ? b + kLongChunk : re;
             dev::CSum acc;
-            gather_span(a.in_src, ccur, b, e, pol, lane, [&](uint32_t, const float (&v)[4]) {
-                acc.add(v[0]);
-                acc.add(v[1]);
-                acc.add(v[2]);
-                acc.add(v[3]);
-            });
+            gather_span(a.in_src, ccur, s_hot, b, e, pol, lane, [&](uint32_t, float v) { acc.add(v); });
             acc = dev::warp_reduce(acc);
             uint32_t last = 0;
             if (lane == 0) {
@@ -212,14 +229,11 @@ __global__ void __launch_bounds__(kPRThreads, 4) pr_iterate_kernel(const PRArgs 
             const uint32_t r1 = a.tile_start[k + 1];
             if (r0 == r1) continue;
             const uint64_t last_b = a.in_off[r1 - 1], last_e = a.in_off[r1];
-            const uint32_t rl = (last_e - last_b >= kLongDegree) ? r1 - 1 : r1;  // long last row is chunked
+            const uint32_t rl = (last_e - last_b >= a.tile_cost) ? r1 - 1 : r1;  // long last row is chunked
             const uint64_t e0 = a.in_off[r0];
             const uint64_t e1 = (rl == r1) ? last_e : last_b;
-            const uint64_t a0 = e0 & ~3ull;
-            float4 *sv4 = reinterpret_cast<float4 *>(sv);
-            gather_span(a.in_src, ccur, e0, e1, pol, lane, [&](uint32_t i, const float (&v)[4]) {
-                if (i < ((e1 - a0 + 3) >> 2)) sv4[i] = make_float4(v[0], v[1], v[2], v[3]);
-            });
+            const uint64_t a0 = e0;
+            gather_span(a.in_src, ccur, s_hot, e0, e1, pol, lane, [&](uint32_t i, float v) { sv[i] = v; });
             __syncwarp();
             for (uint32_t rb = r0; rb < rl; rb += 32) {
                 const uint32_t r = rb + lane;
@@ -297,7 +311,9 @@ int pr_occupancy_grid() {
     static int grid = 0;
     if (grid == 0) {
         int per_sm = 0;
-        HYT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pr_iterate_kernel, kPRThreads, 0));
+        HYT_CUDA(cudaFuncSetAttribute(pr_iterate_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(kPRSmemMax)));
+        HYT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pr_iterate_kernel, kPRThreads, kPRSmemMax));
         grid = sm_count() * std::max(per_sm, 1);
     }
     return grid;
@@ -348,6 +364,9 @@ static void pr_solve(GraphImpl &g, bool personalized, uint32_t source, float dam
     a.tile_start = g.tile_start.get();
     a.long_rows = g.long_rows.get();
     a.chunk_tasks = g.chunk_tasks.get();
+    a.hot_vertex = g.hot_vertex.get();
+    a.num_hot = g.num_hot;
+    a.tile_cost = g.tile_cost;
     for (int i = 0; i < 2; ++i) {
         a.rank[i] = g.rank[i].get();
         a.contrib[i] = g.contrib[i].get();
@@ -408,7 +427,7 @@ static void pr_solve(GraphImpl &g, bool personalized, uint32_t source, float dam
         kp.func = reinterpret_cast<void *>(pr_iterate_kernel);
         kp.gridDim = dim3(grid);
         kp.blockDim = dim3(kPRThreads);
-        kp.sharedMemBytes = 0;
+        kp.sharedMemBytes = static_cast<unsigned>(pr_shared_bytes(g.num_hot, g.tile_cost));
         kp.kernelParams = kargs;
         cudaGraphNode_t knode;
         HYT_CUDA(cudaGraphAddKernelNode(&knode, body, nullptr, 0, &kp));
@@ -418,7 +437,7 @@ static void pr_solve(GraphImpl &g, bool personalized, uint32_t source, float dam
         EventTimer kt;
         for (uint32_t i = 0; i < max_iter; ++i) {
             if (flags & HYT_RUN_PROFILE) kt.start(s);
-            pr_iterate_kernel<<<grid, kPRThreads, 0, s>>>(d_args);
+            pr_iterate_kernel<<<grid, kPRThreads, pr_shared_bytes(g.num_hot, g.tile_cost), s>>>(d_args);
             HYT_CUDA(cudaGetLastError());
             ++launches;
             if (flags & HYT_RUN_PROFILE) {

@@ -36,6 +36,21 @@ void sort_pairs_u32(uint32_t *keys, uint32_t *vals, size_t n, int end_bit, cudaS
     HYT_CUDA(cudaStreamSynchronize(s));
 }
 
+void sort_pairs_desc_u32(uint32_t *keys, uint32_t *vals, size_t n, cudaStream_t s) {
+    if (n < 2) return;
+    DeviceArray<uint32_t> k2(n), v2(n);
+    cub::DoubleBuffer<uint32_t> kb(keys, k2.get()), vb(vals, v2.get());
+    size_t tb = 0;
+    HYT_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, kb, vb, static_cast<int64_t>(n), 0, 32, s));
+    TempStorage tmp(tb);
+    HYT_CUDA(cub::DeviceRadixSort::SortPairsDescending(tmp.ptr, tb, kb, vb, static_cast<int64_t>(n), 0, 32, s));
+    if (kb.Current() != keys)
+        HYT_CUDA(cudaMemcpyAsync(keys, kb.Current(), n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+    if (vb.Current() != vals)
+        HYT_CUDA(cudaMemcpyAsync(vals, vb.Current(), n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+    HYT_CUDA(cudaStreamSynchronize(s));
+}
+
 void sort_keys_u64(uint64_t *keys, size_t n, int end_bit, cudaStream_t s) {
     if (n < 2) return;
     DeviceArray<uint64_t> k2(n);

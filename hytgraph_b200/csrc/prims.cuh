@@ -15,6 +15,9 @@ namespace hyt::prims {
 // keys/vals are sorted in place (temporary double buffers are allocated).
 void sort_pairs_u32(uint32_t *keys, uint32_t *vals, size_t n, int end_bit, cudaStream_t s);
 
+// Same, descending by key (stable: equal keys keep their input order).
+void sort_pairs_desc_u32(uint32_t *keys, uint32_t *vals, size_t n, cudaStream_t s);
+
 // Radix sort of 64-bit keys on bits [0, end_bit), in place.
 void sort_keys_u64(uint64_t *keys, size_t n, int end_bit, cudaStream_t s);
 

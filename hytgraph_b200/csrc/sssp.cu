@@ -21,10 +21,11 @@
 // Expansion is warp-centric: a warp takes 32 frontier vertices, prefix-sums
 // their degrees with shuffles and walks the combined edge list 32 edges at
 // a time, finding each edge's owner with a 5-step shuffle binary search.
-// Rows of >= kHubDegree edges become kHubChunk-edge tasks for a grid-wide
-// second kernel.  A vertex joins a frontier once per round (round stamp) and
-// the far pile once per phase (phase stamp), appended with one
-// warp-aggregated atomic.  All round state lives on the device; inside a
+// Rows of >= kHubDegree edges become kHubChunk-edge warp tasks for a second
+// grid-wide kernel, so no warp owns more than ~2K edges of a round.  Each
+// lane keeps 4 edges in flight through loads and atomics (relax_batch).  A
+// vertex joins a frontier once per round (round stamp) and the far pile once
+// per phase (phase stamp), appended with one warp-aggregated atomic.  All round state lives on the device; inside a
 // CUDA graph the rounds run as a conditional while-loop.
 #include <cooperative_groups.h>
 
@@ -42,9 +43,10 @@ namespace hyt {
 namespace {
 
 constexpr int kSSThreads = 256;
-constexpr uint32_t kHubDegree = 4096;
-constexpr uint32_t kHubChunk = 4096;
+constexpr uint32_t kHubDegree = 64;   // rows at least this long become warp tasks
+constexpr uint32_t kHubChunk = 512;   // edges per warp task
 constexpr uint32_t kNoDelta = 0xFFFFFFFFu;
+constexpr int kEdgeBatch = 4;  // 32-edge batches in flight per warp
 
 struct SSHeader {
     uint32_t round;      // rounds completed
@@ -134,17 +136,62 @@ __device__ __forceinline__ RoundView round_view(const SSArgs &a) {
     return rv;
 }
 
-__device__ __forceinline__ void relax(const SSArgs &a, const RoundView &rv, uint32_t u, uint32_t nd) {
-    if (nd < __ldcg(a.dist + u)) {
-        const uint32_t old = atomicMin(a.dist + u, nd);
-        if (nd < old) {
-            if (nd < rv.threshold) {
-                if (atomicExch(a.stamp + u, rv.next_stamp) != rv.next_stamp) append(rv.qnext, rv.qnext_size, u);
-            } else {
-                if (atomicExch(a.fstamp + u, rv.far_stamp) != rv.far_stamp) append(rv.far, rv.far_size, u);
+// Appends each lane's entries vals[k] with bit k set in `mask` to a list,
+// with one atomic per warp.  Must be called by all 32 lanes.
+template <int K>
+__device__ __forceinline__ void warp_append(uint32_t *list, uint32_t *size, const uint32_t (&vals)[K], uint32_t mask,
+                                            int lane) {
+    const uint32_t cnt = __popc(mask);
+    uint32_t incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    if (total == 0) return;
+    uint32_t base = 0;
+    if (lane == 31) base = atomicAdd(size, total);
+    base = __shfl_sync(0xffffffffu, base, 31) + incl - cnt;
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+        if ((mask >> k) & 1u) list[base + __popc(mask & ((1u << k) - 1u))] = vals[k];
+}
+
+// Relaxes K candidate edges per lane with all atomics of a phase in flight
+// together: atomicMin on every improving label, then the stamp exchange of
+// every success, then one warp-aggregated append per list.  nd[k] >= du[k]
+// (including padding lanes, whose nd is the infinity label) is a no-op.
+// Must be called by all 32 lanes.
+template <int K>
+__device__ __forceinline__ void relax_batch(const SSArgs &a, const RoundView &rv, const uint32_t (&u)[K],
+                                            const uint32_t (&nd)[K], const uint32_t (&du)[K], int lane,
+                                            unsigned long long &improved) {
+    uint32_t old[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) old[k] = (nd[k] < du[k]) ? atomicMin(a.dist + u[k], nd[k]) : 0u;
+    uint32_t st[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        st[k] = 0;
+        if (nd[k] < old[k])
+            st[k] = (nd[k] < rv.threshold) ? atomicExch(a.stamp + u[k], rv.next_stamp)
+                                           : atomicExch(a.fstamp + u[k], rv.far_stamp);
+    }
+    uint32_t nmask = 0, fmask = 0;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        if (nd[k] < old[k]) {
+            ++improved;
+            if (nd[k] < rv.threshold) {
+                if (st[k] != rv.next_stamp) nmask |= 1u << k;
+            } else if (st[k] != rv.far_stamp) {
+                fmask |= 1u << k;
             }
         }
     }
+    warp_append<K>(rv.qnext, rv.qnext_size, u, nmask, lane);
+    warp_append<K>(rv.far, rv.far_size, u, fmask, lane);
 }
 
 // Splits the far pile at the start of a round whose near frontier is empty.
@@ -183,7 +230,7 @@ __global__ void __launch_bounds__(kSSThreads) sssp_expand_kernel(const SSArgs *_
     const int lane = threadIdx.x & 31;
     const uint32_t gwarp = (blockIdx.x * kSSThreads + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * kSSThreads) >> 5;
-    unsigned long long relaxed = 0;
+    unsigned long long relaxed = 0, improved = 0;
 
     for (uint32_t w = gwarp; uint64_t(w) * 32 < rv.qn; w += nwarps) {
         const uint32_t i = w * 32 + lane;
@@ -196,6 +243,7 @@ __global__ void __launch_bounds__(kSSThreads) sssp_expand_kernel(const SSArgs *_
             d = __ldcg(a.dist + v);
             relaxed += full;
             if (full >= kHubDegree) {
+                // long rows: kHubChunk-edge warp tasks for the hub kernel
                 const uint32_t nch = static_cast<uint32_t>((full + kHubChunk - 1) / kHubChunk);
                 const uint32_t base = atomicAdd(&a.hdr->hub_count, nch);
                 for (uint32_t c = 0; c < nch; ++c) a.hubs[base + c] = make_uint2(v, c);
@@ -203,7 +251,7 @@ __global__ void __launch_bounds__(kSSThreads) sssp_expand_kernel(const SSArgs *_
                 deg = static_cast<uint32_t>(full);
             }
         }
-        // inclusive prefix of the 32 degrees
+        // inclusive prefix of the 32 short degrees
         uint32_t incl = deg;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -211,24 +259,35 @@ __global__ void __launch_bounds__(kSSThreads) sssp_expand_kernel(const SSArgs *_
             if (lane >= o) incl += y;
         }
         const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-        for (uint32_t base = 0; base < total; base += 32) {
-            const uint32_t j = base + lane;
-            // owner = first lane whose inclusive prefix exceeds j
-            uint32_t lo = 0;
+        // kEdgeBatch batches of 32 edges per pass: all column/weight loads,
+        // then all label loads, then all atomics are in flight together.
+        for (uint32_t base = 0; base < total; base += 32 * kEdgeBatch) {
+            uint32_t u[kEdgeBatch], nd[kEdgeBatch], du[kEdgeBatch];
 #pragma unroll
-            for (uint32_t step = 16; step > 0; step >>= 1) {
-                const uint32_t probe = __shfl_sync(0xffffffffu, incl, lo + step - 1);
-                if (probe <= j) lo += step;
+            for (int k = 0; k < kEdgeBatch; ++k) {
+                const uint32_t j = base + 32 * k + lane;
+                // owner = first lane whose inclusive prefix exceeds j
+                uint32_t lo = 0;
+#pragma unroll
+                for (uint32_t step = 16; step > 0; step >>= 1) {
+                    const uint32_t probe = __shfl_sync(0xffffffffu, incl, lo + step - 1);
+                    if (probe <= j) lo += step;
+                }
+                const uint32_t o_incl = __shfl_sync(0xffffffffu, incl, lo);
+                const uint32_t o_deg = __shfl_sync(0xffffffffu, deg, lo);
+                const uint64_t o_off = __shfl_sync(0xffffffffu, off, lo);
+                const uint32_t o_d = __shfl_sync(0xffffffffu, d, lo);
+                u[k] = 0;
+                nd[k] = a.inf;
+                if (j < total) {
+                    const uint64_t e = o_off + (j - (o_incl - o_deg));
+                    u[k] = dev::ld_stream(a.cols + e);
+                    nd[k] = extend<WK>(o_d, edge_weight<WK>(a.weights, e));
+                }
             }
-            const uint32_t o_incl = __shfl_sync(0xffffffffu, incl, lo);
-            const uint32_t o_deg = __shfl_sync(0xffffffffu, deg, lo);
-            const uint64_t o_off = __shfl_sync(0xffffffffu, off, lo);
-            const uint32_t o_d = __shfl_sync(0xffffffffu, d, lo);
-            if (j < total) {
-                const uint64_t e = o_off + (j - (o_incl - o_deg));
-                const uint32_t u = dev::ld_stream(a.cols + e);
-                relax(a, rv, u, extend<WK>(o_d, edge_weight<WK>(a.weights, e)));
-            }
+#pragma unroll
+            for (int k = 0; k < kEdgeBatch; ++k) du[k] = __ldcg(a.dist + u[k]);
+            relax_batch<kEdgeBatch>(a, rv, u, nd, du, lane, improved);
         }
     }
 #pragma unroll
@@ -236,21 +295,38 @@ __global__ void __launch_bounds__(kSSThreads) sssp_expand_kernel(const SSArgs *_
     if (lane == 0 && relaxed) atomicAdd(&a.hdr->relaxations, relaxed);
 }
 
+// One warp per kHubChunk-edge slice of a long frontier row.
 template <int WK>
 __global__ void __launch_bounds__(kSSThreads) sssp_hub_kernel(const SSArgs *__restrict__ args) {
     const SSArgs a = *args;
     if (*(volatile uint32_t *)&a.hdr->done) return;
     const RoundView rv = round_view(a);
     const uint32_t n = *(volatile uint32_t *)&a.hdr->hub_count;
-    for (uint32_t t = blockIdx.x; t < n; t += gridDim.x) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t gwarp = (blockIdx.x * kSSThreads + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * kSSThreads) >> 5;
+    unsigned long long improved = 0;
+    for (uint32_t t = gwarp; t < n; t += nwarps) {
         const uint2 h = a.hubs[t];
         const uint64_t rb = a.row_off[h.x], re = a.row_off[h.x + 1];
         const uint64_t b = rb + uint64_t(h.y) * kHubChunk;
-        const uint64_t e = (b + kHubChunk < re) ? b + kHubChunk : re;
+        const uint32_t len = static_cast<uint32_t>(((b + kHubChunk < re) ? b + kHubChunk : re) - b);
         const uint32_t d = __ldcg(a.dist + h.x);
-        for (uint64_t x = b + threadIdx.x; x < e; x += kSSThreads) {
-            const uint32_t u = dev::ld_stream(a.cols + x);
-            relax(a, rv, u, extend<WK>(d, edge_weight<WK>(a.weights, x)));
+        for (uint32_t base = 0; base < len; base += 32 * kEdgeBatch) {
+            uint32_t u[kEdgeBatch], nd[kEdgeBatch], du[kEdgeBatch];
+#pragma unroll
+            for (int k = 0; k < kEdgeBatch; ++k) {
+                const uint32_t j = base + 32 * k + lane;
+                u[k] = 0;
+                nd[k] = a.inf;
+                if (j < len) {
+                    u[k] = dev::ld_stream(a.cols + b + j);
+                    nd[k] = extend<WK>(d, edge_weight<WK>(a.weights, b + j));
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < kEdgeBatch; ++k) du[k] = __ldcg(a.dist + u[k]);
+            relax_batch<kEdgeBatch>(a, rv, u, nd, du, lane, improved);
         }
     }
 }
@@ -322,7 +398,8 @@ void sssp_solve(GraphImpl &g, uint32_t source, uint32_t delta, uint32_t max_roun
         if (g.queue[i].count < V) g.queue[i].allocate(V);
         if (g.far[i].count < V) g.far[i].allocate(V);
     }
-    const uint64_t hub_cap = 2 * (g.E / kHubChunk) + 2;
+    // each frontier vertex appears once per round: <= V rows, E/kHubChunk + V chunks
+    const uint64_t hub_cap = V + g.E / kHubChunk + 2;
     if (g.hub_tasks.count < hub_cap) g.hub_tasks.allocate(hub_cap);
     const size_t sb = 512 + sizeof(SSHeader);
     if (g.sssp_state.count < sb) g.sssp_state.allocate(sb);
