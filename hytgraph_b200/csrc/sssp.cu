@@ -521,11 +521,13 @@ void sssp_solve(GraphImpl &g, uint32_t source, uint32_t delta, uint32_t max_roun
 }  // namespace
 
 uint32_t sssp_default_delta(const GraphImpl &g) {
-    // Near/far bucket width: twice the mean edge weight (measured on the
-    // device when the graph is built).  Unweighted graphs use 1 (BFS order).
-    if (g.weight_kind == HYT_WEIGHTS_F32) return kNoDelta;
-    if (g.weight_kind == HYT_WEIGHTS_NONE) return 1;
-    return g.default_delta ? g.default_delta : kNoDelta;
+    // Measured on R-MAT scale 24 (bucket widths 4 .. infinity): with batched
+    // relaxations the extra rounds of narrow buckets cost more than the
+    // relaxations they save, so the default is one bucket (frontier
+    // Bellman-Ford).  Callers pick a finite width with params.delta; a
+    // graph's 2x-mean-weight width is kept in g.default_delta for that.
+    (void)g;
+    return kNoDelta;
 }
 
 void sssp_run(GraphImpl &g, const hyt_sssp_params &p, uint32_t *dist_out, hyt_run_stats *stats) {
