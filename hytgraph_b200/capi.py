@@ -34,6 +34,8 @@ HYT_RUN_PROFILE = 1
 HYT_RUN_NO_GRAPH = 2
 
 HYT_DIST_INF_U32 = 0xFFFFFFFF
+HYT_NOALLOC_MAX_VERTICES = 1 << 20  # hyt_sssp_noalloc capacity (include/hyt/capi.h)
+HYT_NOALLOC_MAX_EDGES = 1 << 24
 
 
 class hyt_csr(C.Structure):
@@ -158,6 +160,7 @@ _SIGNATURES = [
     ("hyt_pagerank", C.c_int, [C.c_void_p, C.POINTER(hyt_pagerank_params), C.c_void_p, C.POINTER(hyt_run_stats)]),
     ("hyt_ppr", C.c_int, [C.c_void_p, C.POINTER(hyt_ppr_params), C.c_void_p, C.POINTER(hyt_run_stats)]),
     ("hyt_sssp", C.c_int, [C.c_void_p, C.POINTER(hyt_sssp_params), C.c_void_p, C.POINTER(hyt_run_stats)]),
+    ("hyt_sssp_noalloc", C.c_int, [C.POINTER(hyt_csr), C.c_uint32, C.c_void_p, C.c_void_p, C.POINTER(hyt_run_stats)]),
     ("hyt_rmat_generate", C.c_int, [C.POINTER(hyt_rmat_params), C.c_int, C.POINTER(hyt_csr_buffers)]),
     ("hyt_csr_buffers_free", C.c_int, [C.POINTER(hyt_csr_buffers)]),
     ("hyt_pick_sources", C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint32, C.c_void_p]),

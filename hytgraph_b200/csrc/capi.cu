@@ -207,6 +207,14 @@ int hyt_sssp(hyt_graph *graph, const hyt_sssp_params *params, uint32_t *dist_out
     });
 }
 
+int hyt_sssp_noalloc(const hyt_csr *csr, uint32_t source, uint32_t *dist_out, void *stream, hyt_run_stats *stats) {
+    return guarded([&] {
+        if (!csr || !dist_out) fail(HYT_E_INVALID, "csr/dist_out is NULL");
+        require_device();
+        sssp_noalloc(*csr, source, dist_out, stream, stats);
+    });
+}
+
 int hyt_rmat_generate(const hyt_rmat_params *params, int on_device, hyt_csr_buffers *out) {
     return guarded([&] {
         if (!params) fail(HYT_E_INVALID, "params is NULL");

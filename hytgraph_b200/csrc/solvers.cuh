@@ -8,6 +8,7 @@ namespace hyt {
 void pagerank_run(GraphImpl &g, const hyt_pagerank_params &p, float *ranks_out, hyt_run_stats *stats);
 void ppr_run(GraphImpl &g, const hyt_ppr_params &p, float *ranks_out, hyt_run_stats *stats);
 void sssp_run(GraphImpl &g, const hyt_sssp_params &p, uint32_t *dist_out, hyt_run_stats *stats);
+void sssp_noalloc(const hyt_csr &csr, uint32_t source, uint32_t *dist_out, void *stream, hyt_run_stats *stats);
 
 void rmat_generate(const hyt_rmat_params &p, bool on_device, hyt_csr_buffers *out);
 void pick_sources(const uint64_t *row_offsets, uint64_t V, uint64_t seed, uint32_t count, uint32_t *out);

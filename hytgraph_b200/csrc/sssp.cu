@@ -32,6 +32,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
+#include <string>
 
 #include "common.cuh"
 #include "graph.cuh"
@@ -545,6 +547,185 @@ void sssp_run(GraphImpl &g, const hyt_sssp_params &p, uint32_t *dist_out, hyt_ru
         case HYT_WEIGHTS_U32: sssp_solve<HYT_WEIGHTS_U32>(g, p.source, delta, max_rounds, p.flags, s, dist_out, stats); break;
         case HYT_WEIGHTS_F32: sssp_solve<HYT_WEIGHTS_F32>(g, p.source, kNoDelta, max_rounds, p.flags, s, dist_out, stats); break;
         default: fail(HYT_E_INTERNAL, "unknown weight kind");
+    }
+}
+
+}  // namespace hyt
+
+namespace hyt {
+
+// ===========================================================================
+// SSSP that allocates nothing: hyt_sssp_noalloc (include/hyt/capi.h).
+//
+// For callers that cannot call cudaMalloc: a host application whose caching
+// allocator already holds the device's free memory, a latency-critical loop
+// that must not pay cudaMalloc's implicit device synchronisation, or a plugin
+// host that forbids its components to allocate.  The caller passes its CSR
+// and the output label array in device memory; every other buffer the solver
+// needs lives in one file-scope __device__ array of kNoAllocScratchBytes that
+// each GPU loading this library holds until the process exits.
+//
+// The first call on a device looks up the array's device address
+// (cudaGetSymbolAddress) with that device current and caches it; make that
+// first call before any stream capture.  Every call shares the array and it
+// keeps the previous call's contents; whatever must start at zero is cleared
+// by the call itself.  Calls whose work overlaps on the GPU (other streams,
+// other threads) race on the array.
+// ===========================================================================
+namespace {
+
+constexpr uint64_t kNoAllocMaxVertices = HYT_NOALLOC_MAX_VERTICES;
+constexpr uint64_t kNoAllocMaxEdges = HYT_NOALLOC_MAX_EDGES;
+constexpr uint64_t kNoAllocHubCap = kNoAllocMaxVertices + kNoAllocMaxEdges / kHubChunk + 2;
+// args (256 B) | header (256 B) | check word (64 B) | stamp+fstamp u32[2V] |
+// queue u32[2][V] | far u32[2][V] | hub tasks uint2[hub cap]
+constexpr size_t kNoAllocHeadBytes = 1024;
+constexpr size_t kNoAllocScratchBytes =
+    kNoAllocHeadBytes + 6 * sizeof(uint32_t) * kNoAllocMaxVertices + sizeof(uint2) * kNoAllocHubCap;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+void *g_noalloc_address[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch array on the current device.  In host code
+// the name g_noalloc_scratch is only a host-side stand-in, never passed to a
+// kernel.
+unsigned char *noalloc_scratch(int device) {
+    if (device < 0 || device >= kNoAllocMaxDevices) fail(HYT_E_UNSUPPORTED, "hyt_sssp_noalloc: device ordinal too large");
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_address[device]) {
+        void *p = nullptr;
+        HYT_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        g_noalloc_address[device] = p;
+    }
+    return static_cast<unsigned char *>(g_noalloc_address[device]);
+}
+
+// Rejects malformed CSR input before any kernel indexes with it.
+__global__ void noalloc_check_kernel(const uint64_t *off, const uint32_t *cols, const uint32_t *w, uint32_t wkind,
+                                     uint64_t V, uint64_t E, uint32_t *bad) {
+    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+    const uint64_t i0 = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
+    uint32_t b = 0;
+    for (uint64_t v = i0; v < V; v += stride)
+        if (off[v + 1] < off[v]) b |= 1u;
+    for (uint64_t e = i0; e < E; e += stride) {
+        if (cols[e] >= V) b |= 2u;
+        if (wkind == HYT_WEIGHTS_F32) {
+            const float x = __uint_as_float(w[e]);
+            if (!(x >= 0.0f) || isinf(x)) b |= 4u;
+        }
+    }
+    if (i0 == 0 && (off[0] != 0 || off[V] != E)) b |= 1u;
+    if (b) atomicOr(bad, b);
+}
+
+template <int WK>
+void sssp_noalloc_solve(const hyt_csr &csr, uint32_t source, uint32_t *dist, cudaStream_t s, unsigned char *scratch,
+                        hyt_run_stats *stats) {
+    const uint64_t V = csr.num_vertices, E = csr.num_edges;
+    SSArgs *d_args = reinterpret_cast<SSArgs *>(scratch);
+    SSHeader *hdr = reinterpret_cast<SSHeader *>(scratch + 256);
+    uint32_t *check = reinterpret_cast<uint32_t *>(scratch + 512);
+    uint32_t *stamp = reinterpret_cast<uint32_t *>(scratch + kNoAllocHeadBytes);
+    uint32_t *queue0 = stamp + 2 * kNoAllocMaxVertices;
+    uint32_t *queue1 = queue0 + kNoAllocMaxVertices;
+    uint32_t *far0 = queue1 + kNoAllocMaxVertices;
+    uint32_t *far1 = far0 + kNoAllocMaxVertices;
+    uint2 *hubs = reinterpret_cast<uint2 *>(far1 + kNoAllocMaxVertices);
+
+    HYT_CUDA(cudaMemsetAsync(check, 0, sizeof(uint32_t), s));
+    noalloc_check_kernel<<<grid_for(std::max(V, E), 256, 148 * 8), 256, 0, s>>>(
+        csr.row_offsets, csr.column_indices, static_cast<const uint32_t *>(csr.weights), WK, V, E, check);
+    HYT_CUDA(cudaGetLastError());
+    uint32_t bad = 0;
+    HYT_CUDA(cudaMemcpyAsync(&bad, check, sizeof(bad), cudaMemcpyDeviceToHost, s));
+    HYT_CUDA(cudaStreamSynchronize(s));
+    if (bad & 1u) fail(HYT_E_INVALID, "hyt_sssp_noalloc: row offsets must start at 0, be non-decreasing and end at E");
+    if (bad & 2u) fail(HYT_E_INVALID, "hyt_sssp_noalloc: column index contains an invalid destination vertex ID");
+    if (bad & 4u) fail(HYT_E_INVALID, "SSSP requires finite non-negative edge weights");
+
+    SSArgs a{};
+    a.row_off = csr.row_offsets;
+    a.cols = csr.column_indices;
+    a.weights = static_cast<const uint32_t *>(csr.weights);
+    a.dist = dist;
+    a.stamp = stamp;
+    a.fstamp = stamp + kNoAllocMaxVertices;
+    a.queue[0] = queue0;
+    a.queue[1] = queue1;
+    a.far[0] = far0;
+    a.far[1] = far1;
+    a.hubs = hubs;
+    a.hdr = hdr;
+    a.V = static_cast<uint32_t>(V);
+    a.source = source;
+    a.inf = (WK == HYT_WEIGHTS_F32) ? 0x7F800000u : HYT_DIST_INF_U32;
+    a.use_cond = 0;
+
+    SSHeader h0{};  // every counter of the round state starts at zero
+    h0.qsize[0] = 1;
+    h0.delta = kNoDelta;
+    h0.threshold = 0xFFFFFFFFu;
+    const uint32_t max_rounds = static_cast<uint32_t>(4 * V + 1024);
+    h0.max_rounds = max_rounds;
+
+    const int grid = expand_grid<WK>();
+    HYT_CUDA(cudaMemcpyAsync(d_args, &a, sizeof(a), cudaMemcpyHostToDevice, s));
+    HYT_CUDA(cudaMemcpyAsync(hdr, &h0, sizeof(h0), cudaMemcpyHostToDevice, s));
+    sssp_init_kernel<<<grid_for(V, 256, 148 * 8), 256, 0, s>>>(d_args);
+    HYT_CUDA(cudaGetLastError());
+    uint32_t launches = 2;
+    for (uint32_t r = 0; r < max_rounds; ++r) {
+        sssp_split_kernel<<<grid, kSSThreads, 0, s>>>(d_args);
+        sssp_expand_kernel<WK><<<grid, kSSThreads, 0, s>>>(d_args);
+        sssp_hub_kernel<WK><<<grid, kSSThreads, 0, s>>>(d_args);
+        sssp_round_end_kernel<<<1, 1, 0, s>>>(d_args);
+        HYT_CUDA(cudaGetLastError());
+        launches += 4;
+        uint32_t done = 0;
+        HYT_CUDA(cudaMemcpyAsync(&done, &hdr->done, sizeof(done), cudaMemcpyDeviceToHost, s));
+        HYT_CUDA(cudaStreamSynchronize(s));
+        if (done) break;
+    }
+    SSHeader h{};
+    HYT_CUDA(cudaMemcpyAsync(&h, hdr, sizeof(h), cudaMemcpyDeviceToHost, s));
+    HYT_CUDA(cudaStreamSynchronize(s));
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        stats->iterations = h.round;
+        stats->converged = h.converged;
+        stats->total_launches = launches;
+        stats->edges_processed = h.relaxations;
+        stats->vertices_processed = h.frontier_total;
+        stats->algorithmic_bytes = 16ull * h.frontier_total + 12ull * h.relaxations;
+    }
+}
+
+}  // namespace
+
+void sssp_noalloc(const hyt_csr &csr, uint32_t source, uint32_t *dist_out, void *stream, hyt_run_stats *stats) {
+    const uint64_t V = csr.num_vertices, E = csr.num_edges;
+    if (V == 0) fail(HYT_E_INVALID, "SSSP requires at least one vertex");
+    if (V > kNoAllocMaxVertices || E > kNoAllocMaxEdges)
+        fail(HYT_E_INVALID, "hyt_sssp_noalloc: graph exceeds the fixed scratch capacity (at most " +
+                                std::to_string(kNoAllocMaxVertices) + " vertices and " +
+                                std::to_string(kNoAllocMaxEdges) + " edges); use hyt_sssp for larger graphs");
+    if (source >= V) fail(HYT_E_INVALID, "SSSP source vertex is out of range");
+    if (csr.weight_kind > HYT_WEIGHTS_F32) fail(HYT_E_INVALID, "unknown weight_kind");
+    if (!is_device_pointer(csr.row_offsets) || (E && !is_device_pointer(csr.column_indices)) ||
+        (E && csr.weight_kind != HYT_WEIGHTS_NONE && !is_device_pointer(csr.weights)) || !is_device_pointer(dist_out))
+        fail(HYT_E_INVALID, "hyt_sssp_noalloc: the CSR arrays and dist_out must be device memory of the current device");
+    int device = 0;
+    HYT_CUDA(cudaGetDevice(&device));
+    unsigned char *scratch = noalloc_scratch(device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    switch (csr.weight_kind) {
+        case HYT_WEIGHTS_NONE: sssp_noalloc_solve<HYT_WEIGHTS_NONE>(csr, source, dist_out, s, scratch, stats); break;
+        case HYT_WEIGHTS_U32: sssp_noalloc_solve<HYT_WEIGHTS_U32>(csr, source, dist_out, s, scratch, stats); break;
+        default: sssp_noalloc_solve<HYT_WEIGHTS_F32>(csr, source, dist_out, s, scratch, stats); break;
     }
 }
 

@@ -187,6 +187,27 @@ typedef struct hyt_sssp_params {
 int hyt_sssp(hyt_graph *graph, const hyt_sssp_params *params,
              uint32_t *dist_out, hyt_run_stats *stats);
 
+/* SSSP that allocates nothing.  No counterpart in the reference: it exists
+ * for callers that cannot call cudaMalloc -- a host whose caching allocator
+ * already holds the device's free memory, a latency-critical loop that must
+ * not pay cudaMalloc's implicit device synchronisation, or a plugin host
+ * that forbids its components to allocate.
+ *
+ * csr: row_offsets / column_indices / weights in device memory of the
+ * current device; dist_out: [V] uint32 in device memory (same meaning as
+ * hyt_sssp).  All solver state lives in one fixed __device__ array inside
+ * the library (32.3 MiB per GPU that loads it, held until exit), so the
+ * graph may have at most HYT_NOALLOC_MAX_VERTICES vertices and
+ * HYT_NOALLOC_MAX_EDGES edges; larger graphs fail with HYT_E_INVALID.
+ * The first call on a device looks up that array's device address; make it
+ * before any stream capture.  Calls share the array: calls whose GPU work
+ * overlaps (other streams or threads) race.  stats: rounds, relaxations and
+ * launches; device_ms is not measured (no events are created). */
+#define HYT_NOALLOC_MAX_VERTICES (1u << 20)
+#define HYT_NOALLOC_MAX_EDGES (1u << 24)
+int hyt_sssp_noalloc(const hyt_csr *csr, uint32_t source, uint32_t *dist_out, void *stream,
+                     hyt_run_stats *stats);
+
 /* ------------------------------------------------------------------ */
 /* Seeded R-MAT generator (deterministic; same bytes on host and GPU)   */
 /* ------------------------------------------------------------------ */
