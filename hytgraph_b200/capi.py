@@ -142,6 +142,76 @@ class hyt_csr_buffers(C.Structure):
     ]
 
 
+class hyt_csc(C.Structure):
+    _fields_ = [
+        ("num_vertices", C.c_uint64),
+        ("num_edges", C.c_uint64),
+        ("in_offsets", C.c_void_p),
+        ("in_sources", C.c_void_p),
+    ]
+
+
+HYT_ENGINE_AUTO = 0
+HYT_ENGINE_FILTER = 1
+HYT_ENGINE_COMPACTION = 2
+HYT_ENGINE_ZERO_COPY = 3
+
+
+class hyt_hybrid_options(C.Structure):
+    _fields_ = [
+        ("flags", C.c_uint32),
+        ("device", C.c_int),
+        ("device_budget_bytes", C.c_uint64),
+        ("partition_vertices", C.c_uint32),
+        ("host_threads", C.c_uint32),
+        ("force_engine", C.c_uint32),
+        ("alpha", C.c_float),
+        ("beta", C.c_float),
+        ("gamma", C.c_float),
+    ]
+
+
+class hyt_hybrid_info(C.Structure):
+    _fields_ = [
+        ("partitions", C.c_uint64),
+        ("budget_bytes", C.c_uint64),
+        ("resident_bytes", C.c_uint64),
+        ("staging_bytes", C.c_uint64),
+        ("resident_push_partitions", C.c_uint64),
+        ("resident_pull_partitions", C.c_uint64),
+        ("device_bytes", C.c_uint64),
+        ("h2d_gbs", C.c_double),
+        ("zero_copy_gbs", C.c_double),
+        ("gather_gbs", C.c_double),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class hyt_hybrid_stats(C.Structure):
+    _fields_ = [
+        ("rounds", C.c_uint64),
+        ("resident_decisions", C.c_uint64),
+        ("filter_decisions", C.c_uint64),
+        ("compaction_decisions", C.c_uint64),
+        ("zero_copy_decisions", C.c_uint64),
+        ("filter_bytes", C.c_uint64),
+        ("compaction_bytes", C.c_uint64),
+        ("zero_copy_bytes", C.c_uint64),
+        ("link_bytes", C.c_uint64),
+        ("necessary_bytes", C.c_uint64),
+        ("copies", C.c_uint64),
+        ("compaction_host_ms", C.c_double),
+        ("device_ms", C.c_double),
+        ("link_gbs", C.c_double),
+        ("h2d_peak_gbs", C.c_double),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 class HytError(RuntimeError):
     def __init__(self, code: int, message: str):
         super().__init__(f"[hyt status {code}] {message}")
@@ -161,6 +231,17 @@ _SIGNATURES = [
     ("hyt_ppr", C.c_int, [C.c_void_p, C.POINTER(hyt_ppr_params), C.c_void_p, C.POINTER(hyt_run_stats)]),
     ("hyt_sssp", C.c_int, [C.c_void_p, C.POINTER(hyt_sssp_params), C.c_void_p, C.POINTER(hyt_run_stats)]),
     ("hyt_sssp_noalloc", C.c_int, [C.POINTER(hyt_csr), C.c_uint32, C.c_void_p, C.c_void_p, C.POINTER(hyt_run_stats)]),
+    ("hyt_graph_copy_csc", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("hyt_pinned_alloc", C.c_int, [C.c_uint64, C.POINTER(C.c_void_p)]),
+    ("hyt_pinned_free", C.c_int, [C.c_void_p]),
+    ("hyt_hybrid_create", C.c_int,
+     [C.POINTER(hyt_csr), C.POINTER(hyt_csc), C.POINTER(hyt_hybrid_options), C.POINTER(C.c_void_p)]),
+    ("hyt_hybrid_destroy", C.c_int, [C.c_void_p]),
+    ("hyt_hybrid_get_info", C.c_int, [C.c_void_p, C.POINTER(hyt_hybrid_info)]),
+    ("hyt_hybrid_pagerank", C.c_int,
+     [C.c_void_p, C.POINTER(hyt_pagerank_params), C.c_void_p, C.POINTER(hyt_run_stats), C.POINTER(hyt_hybrid_stats)]),
+    ("hyt_hybrid_sssp", C.c_int,
+     [C.c_void_p, C.POINTER(hyt_sssp_params), C.c_void_p, C.POINTER(hyt_run_stats), C.POINTER(hyt_hybrid_stats)]),
     ("hyt_rmat_generate", C.c_int, [C.POINTER(hyt_rmat_params), C.c_int, C.POINTER(hyt_csr_buffers)]),
     ("hyt_csr_buffers_free", C.c_int, [C.POINTER(hyt_csr_buffers)]),
     ("hyt_pick_sources", C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint32, C.c_void_p]),

@@ -112,6 +112,27 @@ int hyt_copy(void *dst, const void *src, uint64_t bytes, void *stream) {
     });
 }
 
+int hyt_pinned_alloc(uint64_t bytes, void **out) {
+    return guarded([&] {
+        if (!out) fail(HYT_E_INVALID, "out is NULL");
+        *out = nullptr;
+        if (!bytes) fail(HYT_E_INVALID, "hyt_pinned_alloc: zero bytes");
+        require_device();
+        const cudaError_t e = cudaHostAlloc(out, bytes, cudaHostAllocMapped | cudaHostAllocPortable);
+        if (e != cudaSuccess) {
+            (void)cudaGetLastError();
+            *out = nullptr;
+            fail(HYT_E_OOM, std::string("cudaHostAlloc failed: ") + cudaGetErrorString(e));
+        }
+    });
+}
+
+int hyt_pinned_free(void *ptr) {
+    return guarded([&] {
+        if (ptr) HYT_CUDA(cudaFreeHost(ptr));
+    });
+}
+
 int hyt_graph_create(const hyt_csr *csr, const hyt_graph_options *options, hyt_graph **out) {
     return guarded([&] {
         if (!csr || !out) fail(HYT_E_INVALID, "csr/out is NULL");
@@ -168,6 +189,15 @@ int hyt_graph_get_info(const hyt_graph *graph, hyt_graph_info *out) {
         out->max_out_degree = g.max_out_degree;
         out->dangling_vertices = g.dangling;
         out->build_ms = g.build_ms;
+    });
+}
+
+int hyt_graph_copy_csc(const hyt_graph *graph, uint64_t *in_offsets, uint32_t *in_sources) {
+    return guarded([&] {
+        if (!graph || !in_offsets || !in_sources) fail(HYT_E_INVALID, "NULL argument");
+        const GraphImpl &g = graph->impl;
+        HYT_CUDA(cudaSetDevice(g.device));
+        graph_copy_csc(g, in_offsets, in_sources);
     });
 }
 

@@ -160,7 +160,36 @@ int bits_for(uint64_t max_value) {
     return b;
 }
 
+__global__ void untag_sources_kernel(const uint32_t *in_src, uint64_t n, const uint32_t *hot_vertex, uint32_t *out) {
+    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += stride) {
+        const uint32_t u = in_src[i];
+        out[i] = (u & kHotTag) ? hot_vertex[u & ~kHotTag] : u;
+    }
+}
+
 }  // namespace
+
+void graph_copy_csc(const GraphImpl &g, uint64_t *in_offsets, uint32_t *in_sources) {
+    if (!(g.flags & HYT_GRAPH_PULL)) fail(HYT_E_INVALID, "graph was created without HYT_GRAPH_PULL");
+    cudaStream_t s = g.stream;
+    HYT_CUDA(cudaMemcpyAsync(in_offsets, g.in_offsets.get(), (g.V + 1) * 8, cudaMemcpyDefault, s));
+    if (g.num_hot == 0) {
+        HYT_CUDA(cudaMemcpyAsync(in_sources, g.in_sources.get(), g.E * 4, cudaMemcpyDefault, s));
+    } else {
+        const uint64_t chunk = std::min<uint64_t>(g.E, uint64_t(1) << 26);
+        DeviceArray<uint32_t> tmp(std::max<uint64_t>(chunk, 1));
+        for (uint64_t e0 = 0; e0 < g.E; e0 += chunk) {
+            const uint64_t n = std::min(chunk, g.E - e0);
+            untag_sources_kernel<<<grid_for(n, 256), 256, 0, s>>>(g.in_sources.get() + e0, n, g.hot_vertex.get(),
+                                                                  tmp.get());
+            HYT_CUDA(cudaGetLastError());
+            HYT_CUDA(cudaMemcpyAsync(in_sources + e0, tmp.get(), n * 4, cudaMemcpyDefault, s));
+            HYT_CUDA(cudaStreamSynchronize(s));  // tmp is reused by the next chunk
+        }
+    }
+    HYT_CUDA(cudaStreamSynchronize(s));
+}
 
 size_t GraphImpl::device_bytes() const {
     size_t b = row_offsets.bytes() + cols.bytes() + weights.bytes() + out_degree.bytes() + in_offsets.bytes() +
@@ -169,6 +198,58 @@ size_t GraphImpl::device_bytes() const {
     b += partial.bytes() + ticket.bytes() + pr_state.bytes() + dist.bytes() + stamp.bytes() + hub_tasks.bytes() +
          sssp_state.bytes();
     return b;
+}
+
+// Work tiles and long-row chunks of the pull side, from g.in_offsets on the
+// device (g.V, g.E, g.tile_cost set).  Shared by graph_build and the
+// out-of-HBM engine.
+void build_pull_tiles(GraphImpl &g, cudaStream_t s) {
+    const uint64_t V = g.V, E = g.E;
+    // Work tiles along the merge path.
+    g.num_tiles = (V + E) / g.tile_cost + 1;
+    g.tile_start.allocate(g.num_tiles + 1);
+    tile_bounds_kernel<<<grid_for(V + 1, 256), 256, 0, s>>>(g.in_offsets.get(), V, E, g.num_tiles, g.tile_cost,
+                                                             g.tile_start.get());
+    HYT_CUDA(cudaGetLastError());
+
+    // Long rows (in-degree >= tile_cost) and their chunk tasks.
+    DeviceArray<uint32_t> in_deg(V);
+    DeviceArray<uint8_t> is_long(V);
+    in_degree_kernel<<<grid_for(V, 256), 256, 0, s>>>(g.in_offsets.get(), V, g.tile_cost, in_deg.get(),
+                                                       is_long.get());
+    HYT_CUDA(cudaGetLastError());
+    g.max_in_degree = prims::reduce_max_u32(in_deg.get(), V, s);
+    DeviceArray<uint32_t> long_ids(V);
+    g.num_long = prims::select_flagged_index(is_long.get(), long_ids.get(), V, s);
+    std::vector<LongRow> lr(g.num_long);
+    std::vector<uint2> tasks;
+    if (g.num_long) {
+        DeviceArray<uint32_t> long_deg(g.num_long);
+        gather_u32_kernel<<<grid_for(g.num_long, 256), 256, 0, s>>>(in_deg.get(), long_ids.get(), g.num_long,
+                                                                     long_deg.get());
+        HYT_CUDA(cudaGetLastError());
+        std::vector<uint32_t> ids(g.num_long), degs(g.num_long);
+        HYT_CUDA(cudaMemcpyAsync(ids.data(), long_ids.get(), g.num_long * 4, cudaMemcpyDeviceToHost, s));
+        HYT_CUDA(cudaMemcpyAsync(degs.data(), long_deg.get(), g.num_long * 4, cudaMemcpyDeviceToHost, s));
+        HYT_CUDA(cudaStreamSynchronize(s));
+        uint32_t next = 0;
+        for (uint64_t i = 0; i < g.num_long; ++i) {
+            const uint32_t nc = (degs[i] + kLongChunk - 1) / kLongChunk;
+            lr[i] = LongRow{ids[i], next, nc, 0};
+            for (uint32_t c = 0; c < nc; ++c) tasks.push_back(make_uint2(static_cast<uint32_t>(i), c));
+            next += nc;
+        }
+    }
+    g.num_chunks = tasks.size();
+    g.long_rows.allocate(std::max<uint64_t>(g.num_long, 1));
+    g.chunk_tasks.allocate(std::max<uint64_t>(g.num_chunks, 1));
+    if (g.num_long)
+        HYT_CUDA(cudaMemcpyAsync(g.long_rows.get(), lr.data(), lr.size() * sizeof(LongRow),
+                                 cudaMemcpyHostToDevice, s));
+    if (g.num_chunks)
+        HYT_CUDA(cudaMemcpyAsync(g.chunk_tasks.get(), tasks.data(), tasks.size() * sizeof(uint2),
+                                 cudaMemcpyHostToDevice, s));
+    HYT_CUDA(cudaStreamSynchronize(s));
 }
 
 void graph_build(GraphImpl &g, const hyt_csr &csr, uint32_t flags) {
@@ -297,51 +378,7 @@ void graph_build(GraphImpl &g, const hyt_csr &csr, uint32_t flags) {
             g.num_hot = 0;
         }
 
-        // Work tiles along the merge path.
-        g.num_tiles = (V + E) / g.tile_cost + 1;
-        g.tile_start.allocate(g.num_tiles + 1);
-        tile_bounds_kernel<<<grid_for(V + 1, 256), 256, 0, s>>>(g.in_offsets.get(), V, E, g.num_tiles, g.tile_cost,
-                                                                 g.tile_start.get());
-        HYT_CUDA(cudaGetLastError());
-
-        // Long rows (in-degree >= tile_cost) and their chunk tasks.
-        DeviceArray<uint32_t> in_deg(V);
-        DeviceArray<uint8_t> is_long(V);
-        in_degree_kernel<<<grid_for(V, 256), 256, 0, s>>>(g.in_offsets.get(), V, g.tile_cost, in_deg.get(),
-                                                           is_long.get());
-        HYT_CUDA(cudaGetLastError());
-        g.max_in_degree = prims::reduce_max_u32(in_deg.get(), V, s);
-        DeviceArray<uint32_t> long_ids(V);
-        g.num_long = prims::select_flagged_index(is_long.get(), long_ids.get(), V, s);
-        std::vector<LongRow> lr(g.num_long);
-        std::vector<uint2> tasks;
-        if (g.num_long) {
-            DeviceArray<uint32_t> long_deg(g.num_long);
-            gather_u32_kernel<<<grid_for(g.num_long, 256), 256, 0, s>>>(in_deg.get(), long_ids.get(), g.num_long,
-                                                                         long_deg.get());
-            HYT_CUDA(cudaGetLastError());
-            std::vector<uint32_t> ids(g.num_long), degs(g.num_long);
-            HYT_CUDA(cudaMemcpyAsync(ids.data(), long_ids.get(), g.num_long * 4, cudaMemcpyDeviceToHost, s));
-            HYT_CUDA(cudaMemcpyAsync(degs.data(), long_deg.get(), g.num_long * 4, cudaMemcpyDeviceToHost, s));
-            HYT_CUDA(cudaStreamSynchronize(s));
-            uint32_t next = 0;
-            for (uint64_t i = 0; i < g.num_long; ++i) {
-                const uint32_t nc = (degs[i] + kLongChunk - 1) / kLongChunk;
-                lr[i] = LongRow{ids[i], next, nc, 0};
-                for (uint32_t c = 0; c < nc; ++c) tasks.push_back(make_uint2(static_cast<uint32_t>(i), c));
-                next += nc;
-            }
-        }
-        g.num_chunks = tasks.size();
-        g.long_rows.allocate(std::max<uint64_t>(g.num_long, 1));
-        g.chunk_tasks.allocate(std::max<uint64_t>(g.num_chunks, 1));
-        if (g.num_long)
-            HYT_CUDA(cudaMemcpyAsync(g.long_rows.get(), lr.data(), lr.size() * sizeof(LongRow),
-                                     cudaMemcpyHostToDevice, s));
-        if (g.num_chunks)
-            HYT_CUDA(cudaMemcpyAsync(g.chunk_tasks.get(), tasks.data(), tasks.size() * sizeof(uint2),
-                                     cudaMemcpyHostToDevice, s));
-        HYT_CUDA(cudaStreamSynchronize(s));
+        build_pull_tiles(g, s);
     }
 
     if (!(flags & HYT_GRAPH_PUSH)) {

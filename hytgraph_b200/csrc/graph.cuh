@@ -105,6 +105,9 @@ inline size_t pr_shared_bytes(uint32_t num_hot, uint32_t tile_cost) {
 // Builds the device graph from a CSR (host or device pointers).
 void graph_build(GraphImpl &g, const hyt_csr &csr, uint32_t flags);
 
+// Copies the CSC with hot tags removed into caller buffers (host or device).
+void graph_copy_csc(const GraphImpl &g, uint64_t *in_offsets, uint32_t *in_sources);
+
 }  // namespace hyt
 
 struct hyt_graph {

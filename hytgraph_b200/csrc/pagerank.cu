@@ -27,6 +27,7 @@
 
 #include "common.cuh"
 #include "graph.cuh"
+#include "hybrid.cuh"
 #include "solvers.cuh"
 
 namespace hyt {
@@ -139,7 +140,33 @@ __device__ __forceinline__ void gather_span(const uint32_t *in_src, const float 
     }
 }
 
-__global__ void __launch_bounds__(kPRThreads, 1) pr_iterate_kernel(const PRArgs *__restrict__ args) {
+// Stop rule of iteration `it` (thread 0 of the last CTA, or the separate
+// end kernel): residual <= tolerance or the iteration cap.
+__device__ __forceinline__ void end_iteration(const PRArgs &a, uint32_t it) {
+    const double r = atomicAdd(&a.residual[it], 0.0);
+    const uint32_t n_it = it + 1;
+    const bool conv = r <= static_cast<double>(a.tolerance);
+    a.hdr->last_residual = r;
+    a.hdr->iter = n_it;
+    if (conv || n_it >= a.max_iter) {
+        a.hdr->done = 1;
+        a.hdr->converged = conv ? 1u : 0u;
+        if (a.use_cond) cudaGraphSetConditional(a.cond, 0);
+    }
+}
+
+// One launch processes chunk tasks [chunk_begin, chunk_end) and tiles
+// [tile_begin, tile_end); in_src is the base of the source ids, addressed by
+// global edge index (a device array, a staging slot offset by its first
+// edge, or mapped host memory).  partial = 1: the iteration is closed later
+// by pr_iteration_end_kernel.
+struct PRRange {
+    const uint32_t *in_src;
+    uint64_t chunk_begin, chunk_end, tile_begin, tile_end;
+    uint32_t partial;
+};
+
+__global__ void __launch_bounds__(kPRThreads, 1) pr_iterate_kernel(const PRArgs *__restrict__ args, PRRange rg) {
     extern __shared__ __align__(16) float s_dyn[];
     __shared__ double s_red[32];
 
@@ -161,7 +188,9 @@ __global__ void __launch_bounds__(kPRThreads, 1) pr_iterate_kernel(const PRArgs 
     ps.tele = static_cast<float>((1.0 - static_cast<double>(a.damping)) + static_cast<double>(a.damping) * dmass);
 
     const uint64_t pol = dev::policy_evict_last();
-    const uint64_t total_tasks = a.num_chunks + a.num_tiles;
+    const uint64_t n_chunks = rg.chunk_end - rg.chunk_begin;
+    const uint64_t total_tasks = n_chunks + (rg.tile_end - rg.tile_begin);
+    const uint32_t *in_src = rg.in_src;
     double res = 0.0, dang = 0.0;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     // Hot-source contributions for this iteration, loaded once per CTA.
@@ -189,15 +218,15 @@ __global__ void __launch_bounds__(kPRThreads, 1) pr_iterate_kernel(const PRArgs 
     // Static round-robin over tasks: every task costs at most one chunk of
     // edges, so warps receive balanced work without a shared counter.
     for (uint64_t task = uint64_t(blockIdx.x) * (kPRThreads / 32) + warp; task < total_tasks; task += nwarps) {
-        if (task < a.num_chunks) {
+        if (task < n_chunks) {
             // ---- slice of a long row -------------------------------------
-            const uint2 t = a.chunk_tasks[task];
+            const uint2 t = a.chunk_tasks[rg.chunk_begin + task];
             const LongRow L = a.long_rows[t.x];
             const uint64_t rb = a.in_off[L.row], re = a.in_off[L.row + 1];
             const uint64_t b = rb + uint64_t(t.y) * kLongChunk;
             const uint64_t e = (b + kLongChunk < re) ? b + kLongChunk : re;
             dev::CSum acc;
-            gather_span(a.in_src, ccur, s_hot, b, e, pol, lane, [&](uint32_t, float v) { acc.add(v); });
+            gather_span(in_src, ccur, s_hot, b, e, pol, lane, [&](uint32_t, float v) { acc.add(v); });
             acc = dev::warp_reduce(acc);
             uint32_t last = 0;
             if (lane == 0) {
@@ -224,7 +253,7 @@ __global__ void __launch_bounds__(kPRThreads, 1) pr_iterate_kernel(const PRArgs 
             }
         } else {
             // ---- merge-path tile of consecutive rows ---------------------
-            const uint64_t k = task - a.num_chunks;
+            const uint64_t k = rg.tile_begin + (task - n_chunks);
             const uint32_t r0 = a.tile_start[k];
             const uint32_t r1 = a.tile_start[k + 1];
             if (r0 == r1) continue;
@@ -233,7 +262,7 @@ __global__ void __launch_bounds__(kPRThreads, 1) pr_iterate_kernel(const PRArgs 
             const uint64_t e0 = a.in_off[r0];
             const uint64_t e1 = (rl == r1) ? last_e : last_b;
             const uint64_t a0 = e0;
-            gather_span(a.in_src, ccur, s_hot, e0, e1, pol, lane, [&](uint32_t i, float v) { sv[i] = v; });
+            gather_span(in_src, ccur, s_hot, e0, e1, pol, lane, [&](uint32_t i, float v) { sv[i] = v; });
             __syncwarp();
             for (uint32_t rb = r0; rb < rl; rb += 32) {
                 const uint32_t r = rb + lane;
@@ -267,22 +296,22 @@ __global__ void __launch_bounds__(kPRThreads, 1) pr_iterate_kernel(const PRArgs 
     if (threadIdx.x == 0) {
         atomicAdd(&a.residual[it], bres);
         atomicAdd(&a.dangling[it + 1], bdang);
-        __threadfence();
-        const uint32_t t = atomicAdd(&a.finished[it], 1u);
-        if (t == gridDim.x - 1) {
+        if (!rg.partial) {
             __threadfence();
-            const double r = atomicAdd(&a.residual[it], 0.0);
-            const uint32_t n_it = it + 1;
-            const bool conv = r <= static_cast<double>(a.tolerance);
-            a.hdr->last_residual = r;
-            a.hdr->iter = n_it;
-            if (conv || n_it >= a.max_iter) {
-                a.hdr->done = 1;
-                a.hdr->converged = conv ? 1u : 0u;
-                if (a.use_cond) cudaGraphSetConditional(a.cond, 0);
+            const uint32_t t = atomicAdd(&a.finished[it], 1u);
+            if (t == gridDim.x - 1) {
+                __threadfence();
+                end_iteration(a, it);
             }
         }
     }
+}
+
+// Closes an iteration whose tasks ran as several partial launches.
+__global__ void pr_iteration_end_kernel(const PRArgs *__restrict__ args) {
+    const PRArgs a = *args;
+    if (a.hdr->done) return;
+    end_iteration(a, a.hdr->iter);
 }
 
 __global__ void pr_init_kernel(const PRArgs *__restrict__ args) {
@@ -328,9 +357,16 @@ struct SolveOut {
 }  // namespace
 
 // Shared by PageRank and personalized PageRank.
-static void pr_solve(GraphImpl &g, bool personalized, uint32_t source, float damping, float tolerance,
-                     uint32_t max_iter, uint32_t flags, cudaStream_t s, float *ranks_out, hyt_run_stats *stats) {
-    if (!(g.flags & HYT_GRAPH_PULL)) fail(HYT_E_INVALID, "graph was created without HYT_GRAPH_PULL");
+// Workspaces, device state layout and kernel arguments of one solve.
+struct PRSolveState {
+    PRArgs a;
+    PRArgs *d_args;
+    PRHeader *hdr;
+    size_t zero_bytes;
+};
+
+static PRSolveState pr_prepare(GraphImpl &g, bool personalized, uint32_t source, float damping, float tolerance,
+                               uint32_t max_iter) {
     const uint64_t V = g.V;
     // Workspaces (grown on demand, kept in the handle).
     for (int i = 0; i < 2; ++i) {
@@ -389,6 +425,18 @@ static void pr_solve(GraphImpl &g, bool personalized, uint32_t source, float dam
     a.personalized = personalized ? 1u : 0u;
     a.use_cond = 0;
 
+    return PRSolveState{a, d_args, hdr, zero_bytes};
+}
+
+static void pr_solve(GraphImpl &g, bool personalized, uint32_t source, float damping, float tolerance,
+                     uint32_t max_iter, uint32_t flags, cudaStream_t s, float *ranks_out, hyt_run_stats *stats) {
+    if (!(g.flags & HYT_GRAPH_PULL)) fail(HYT_E_INVALID, "graph was created without HYT_GRAPH_PULL");
+    const uint64_t V = g.V;
+    PRSolveState st0 = pr_prepare(g, personalized, source, damping, tolerance, max_iter);
+    PRArgs &a = st0.a;
+    PRArgs *d_args = st0.d_args;
+    PRHeader *hdr = st0.hdr;
+    const size_t zero_bytes = st0.zero_bytes;
     const bool use_graph = !(flags & HYT_RUN_NO_GRAPH) && !(flags & HYT_RUN_PROFILE);
     const int grid = pr_occupancy_grid();
 
@@ -412,6 +460,7 @@ static void pr_solve(GraphImpl &g, bool personalized, uint32_t source, float dam
     pr_init_kernel<<<grid_for(V, 256, 148 * 8), 256, 0, s>>>(d_args);
     HYT_CUDA(cudaGetLastError());
     ++launches;
+    PRRange full{g.in_sources.get(), 0, g.num_chunks, 0, g.num_tiles, 0};
 
     if (use_graph) {
         cudaGraphNodeParams cp = {};
@@ -423,7 +472,7 @@ static void pr_solve(GraphImpl &g, bool personalized, uint32_t source, float dam
         HYT_CUDA(cudaGraphAddNode(&cnode, graph, nullptr, 0, &cp));
         cudaGraph_t body = cp.conditional.phGraph_out[0];
         cudaKernelNodeParams kp = {};
-        void *kargs[] = {&d_args};
+        void *kargs[] = {&d_args, &full};
         kp.func = reinterpret_cast<void *>(pr_iterate_kernel);
         kp.gridDim = dim3(grid);
         kp.blockDim = dim3(kPRThreads);
@@ -437,7 +486,7 @@ static void pr_solve(GraphImpl &g, bool personalized, uint32_t source, float dam
         EventTimer kt;
         for (uint32_t i = 0; i < max_iter; ++i) {
             if (flags & HYT_RUN_PROFILE) kt.start(s);
-            pr_iterate_kernel<<<grid, kPRThreads, pr_shared_bytes(g.num_hot, g.tile_cost), s>>>(d_args);
+            pr_iterate_kernel<<<grid, kPRThreads, pr_shared_bytes(g.num_hot, g.tile_cost), s>>>(d_args, full);
             HYT_CUDA(cudaGetLastError());
             ++launches;
             if (flags & HYT_RUN_PROFILE) {
@@ -500,6 +549,60 @@ void ppr_run(GraphImpl &g, const hyt_ppr_params &p, float *ranks_out, hyt_run_st
     if (p.source >= g.V) fail(HYT_E_INVALID, "personalized PageRank source vertex is out of range");
     cudaStream_t s = p.stream ? static_cast<cudaStream_t>(p.stream) : g.stream;
     pr_solve(g, true, p.source, 1.0f - p.restart, p.tolerance, p.max_iterations, p.flags, s, ranks_out, stats);
+}
+
+void pagerank_partitioned(GraphImpl &g, PullSource &src, bool personalized, uint32_t source, float damping,
+                          float tolerance, uint32_t max_iter, cudaStream_t s, float *ranks_out, hyt_run_stats *stats) {
+    const uint64_t V = g.V;
+    PRSolveState st0 = pr_prepare(g, personalized, source, damping, tolerance, max_iter);
+    const PRArgs &a = st0.a;
+    const int grid = pr_occupancy_grid();
+    const size_t smem = pr_shared_bytes(a.num_hot, a.tile_cost);
+
+    EventTimer total, kt;
+    total.start(s);
+    HYT_CUDA(cudaMemsetAsync(st0.hdr, 0, st0.zero_bytes, s));
+    HYT_CUDA(cudaMemsetAsync(g.ticket.get(), 0, g.ticket.bytes(), s));
+    HYT_CUDA(cudaMemcpyAsync(st0.d_args, &a, sizeof(PRArgs), cudaMemcpyHostToDevice, s));
+    pr_init_kernel<<<grid_for(V, 256, 148 * 8), 256, 0, s>>>(st0.d_args);
+    HYT_CUDA(cudaGetLastError());
+    uint32_t launches = 1, hot = 0;
+    PRHeader h{};
+    for (uint32_t it = 0; it < max_iter; ++it) {
+        src.begin_iteration(s);
+        for (size_t p = 0; p < src.parts(); ++p) {
+            const PullPart pp = src.part(p);
+            if (pp.chunk_begin == pp.chunk_end && pp.tile_begin == pp.tile_end) continue;
+            const uint32_t *base = src.acquire(p, s);
+            const PRRange rg{base, pp.chunk_begin, pp.chunk_end, pp.tile_begin, pp.tile_end, 1u};
+            pr_iterate_kernel<<<grid, kPRThreads, smem, s>>>(st0.d_args, rg);
+            HYT_CUDA(cudaGetLastError());
+            src.release(p, s);
+            ++launches;
+            ++hot;
+        }
+        pr_iteration_end_kernel<<<1, 1, 0, s>>>(st0.d_args);
+        HYT_CUDA(cudaGetLastError());
+        ++launches;
+        HYT_CUDA(cudaMemcpyAsync(&h, st0.hdr, sizeof(h), cudaMemcpyDeviceToHost, s));
+        HYT_CUDA(cudaStreamSynchronize(s));
+        if (h.done) break;
+    }
+    total.stop(s);
+    const double total_ms = total.ms();
+    if (h.iter == 0) fail(HYT_E_INTERNAL, "PageRank made no progress");
+    if (ranks_out) copy_from_device(ranks_out, g.rank[h.iter & 1].get(), V * sizeof(float), s);
+    if (stats) {
+        stats->iterations = h.iter;
+        stats->converged = h.converged;
+        stats->residual = h.last_residual;
+        stats->device_ms = total_ms;
+        stats->kernel_launches = hot;
+        stats->total_launches = launches;
+        stats->edges_processed = uint64_t(h.iter) * g.E;
+        stats->vertices_processed = uint64_t(h.iter) * V;
+        stats->algorithmic_bytes = uint64_t(h.iter) * (8ull * g.E + 20ull * V);
+    }
 }
 
 }  // namespace hyt

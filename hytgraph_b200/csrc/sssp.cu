@@ -37,6 +37,7 @@
 
 #include "common.cuh"
 #include "graph.cuh"
+#include "hybrid.cuh"
 #include "solvers.cuh"
 
 namespace cg = cooperative_groups;
@@ -83,6 +84,8 @@ struct SSArgs {
     uint32_t inf;
     uint32_t use_cond;
     cudaGraphConditionalHandle cond;
+    const EdgeLoc *loc;   // per-partition edge location (partitioned solves)
+    uint32_t part_shift;  // partition of vertex v = v >> part_shift
 };
 
 template <int WK>
@@ -224,7 +227,10 @@ __global__ void __launch_bounds__(kSSThreads) sssp_split_kernel(const SSArgs *__
     }
 }
 
-template <int WK>
+// HYB: the edges of a vertex's partition are reached through a.loc
+// (partitioned solves); compacted partitions are expanded from their packed
+// payload by sssp_expand_packed_kernel instead.
+template <int WK, bool HYB = false>
 __global__ void __launch_bounds__(kSSThreads) sssp_expand_kernel(const SSArgs *__restrict__ args) {
     const SSArgs a = *args;
     if (*(volatile uint32_t *)&a.hdr->done) return;
@@ -238,10 +244,17 @@ __global__ void __launch_bounds__(kSSThreads) sssp_expand_kernel(const SSArgs *_
         const uint32_t i = w * 32 + lane;
         uint32_t deg = 0, d = a.inf;
         uint64_t off = 0;
+        const uint32_t *vc = a.cols, *vw = a.weights;  // edge arrays of this lane's vertex
         if (i < rv.qn) {
             const uint32_t v = rv.q[i];
             off = a.row_off[v];
-            const uint64_t full = a.row_off[v + 1] - off;
+            uint64_t full = a.row_off[v + 1] - off;
+            if constexpr (HYB) {
+                const EdgeLoc L = a.loc[v >> a.part_shift];
+                vc = L.cols;
+                vw = L.weights;
+                if (L.mode != kLocDirect) full = 0;
+            }
             d = __ldcg(a.dist + v);
             relaxed += full;
             if (full >= kHubDegree) {
@@ -279,12 +292,19 @@ __global__ void __launch_bounds__(kSSThreads) sssp_expand_kernel(const SSArgs *_
                 const uint32_t o_deg = __shfl_sync(0xffffffffu, deg, lo);
                 const uint64_t o_off = __shfl_sync(0xffffffffu, off, lo);
                 const uint32_t o_d = __shfl_sync(0xffffffffu, d, lo);
+                const uint32_t *oc = a.cols, *ow = a.weights;
+                if constexpr (HYB) {
+                    oc = reinterpret_cast<const uint32_t *>(
+                        __shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(vc), lo));
+                    ow = reinterpret_cast<const uint32_t *>(
+                        __shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(vw), lo));
+                }
                 u[k] = 0;
                 nd[k] = a.inf;
                 if (j < total) {
                     const uint64_t e = o_off + (j - (o_incl - o_deg));
-                    u[k] = dev::ld_stream(a.cols + e);
-                    nd[k] = extend<WK>(o_d, edge_weight<WK>(a.weights, e));
+                    u[k] = dev::ld_stream(oc + e);
+                    nd[k] = extend<WK>(o_d, edge_weight<WK>(ow, e));
                 }
             }
 #pragma unroll
@@ -298,7 +318,7 @@ __global__ void __launch_bounds__(kSSThreads) sssp_expand_kernel(const SSArgs *_
 }
 
 // One warp per kHubChunk-edge slice of a long frontier row.
-template <int WK>
+template <int WK, bool HYB = false>
 __global__ void __launch_bounds__(kSSThreads) sssp_hub_kernel(const SSArgs *__restrict__ args) {
     const SSArgs a = *args;
     if (*(volatile uint32_t *)&a.hdr->done) return;
@@ -314,6 +334,12 @@ __global__ void __launch_bounds__(kSSThreads) sssp_hub_kernel(const SSArgs *__re
         const uint64_t b = rb + uint64_t(h.y) * kHubChunk;
         const uint32_t len = static_cast<uint32_t>(((b + kHubChunk < re) ? b + kHubChunk : re) - b);
         const uint32_t d = __ldcg(a.dist + h.x);
+        const uint32_t *hc = a.cols, *hw = a.weights;
+        if constexpr (HYB) {
+            const EdgeLoc L = a.loc[h.x >> a.part_shift];
+            hc = L.cols;
+            hw = L.weights;
+        }
         for (uint32_t base = 0; base < len; base += 32 * kEdgeBatch) {
             uint32_t u[kEdgeBatch], nd[kEdgeBatch], du[kEdgeBatch];
 #pragma unroll
@@ -322,8 +348,8 @@ __global__ void __launch_bounds__(kSSThreads) sssp_hub_kernel(const SSArgs *__re
                 u[k] = 0;
                 nd[k] = a.inf;
                 if (j < len) {
-                    u[k] = dev::ld_stream(a.cols + b + j);
-                    nd[k] = extend<WK>(d, edge_weight<WK>(a.weights, b + j));
+                    u[k] = dev::ld_stream(hc + b + j);
+                    nd[k] = extend<WK>(d, edge_weight<WK>(hw, b + j));
                 }
             }
 #pragma unroll
@@ -377,6 +403,112 @@ __global__ void sssp_init_kernel(const SSArgs *__restrict__ args) {
         a.fstamp[v] = 0xFFFFFFFFu;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) a.queue[0][0] = a.source;
+}
+
+// ---- partitioned (out-of-HBM) solves -------------------------------------
+
+// Per-partition HyTM metrics of this round's frontier: active vertices,
+// active edges (out-edges of active vertices), zero-copy requests
+// ceil(deg * 4 / 128) and alignment overhead (row start not 128-byte aligned
+// in the logical id array), as in the reference's cost model
+// (src/transfer/hytm_cost_model.cpp:330-452).  Shared-memory histograms,
+// one global atomic per CTA and partition.
+constexpr uint32_t kMaxParts = 1024;
+
+__global__ void __launch_bounds__(kSSThreads) sssp_part_stats_kernel(const SSArgs *__restrict__ args, uint32_t parts,
+                                                                     PartMetrics *out) {
+    __shared__ unsigned long long s_m[4 * kMaxParts];
+    const SSArgs a = *args;
+    for (uint32_t i = threadIdx.x; i < 4 * parts; i += blockDim.x) s_m[i] = 0;
+    __syncthreads();
+    const RoundView rv = round_view(a);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < rv.qn; i += gridDim.x * blockDim.x) {
+        const uint32_t v = rv.q[i];
+        const uint32_t p = v >> a.part_shift;
+        const uint64_t off = a.row_off[v];
+        const uint64_t deg = a.row_off[v + 1] - off;
+        atomicAdd(&s_m[4 * p + 0], 1ull);
+        if (deg) {
+            atomicAdd(&s_m[4 * p + 1], static_cast<unsigned long long>(deg));
+            atomicAdd(&s_m[4 * p + 2], static_cast<unsigned long long>((deg * 4 + 127) / 128));
+            if ((off * 4) % 128) atomicAdd(&s_m[4 * p + 3], 1ull);
+        }
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < 4 * parts; i += blockDim.x)
+        if (s_m[i]) atomicAdd(reinterpret_cast<unsigned long long *>(out) + i, s_m[i]);
+}
+
+// Frontier vertices whose partition is compacted this round.
+__global__ void sssp_compacted_list_kernel(const SSArgs *__restrict__ args, uint32_t *list, uint32_t *count) {
+    const SSArgs a = *args;
+    const RoundView rv = round_view(a);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < rv.qn; i += gridDim.x * blockDim.x) {
+        const uint32_t v = rv.q[i];
+        if (a.loc[v >> a.part_shift].mode == kLocCompacted) append(list, count, v);
+    }
+}
+
+// Expands the packed rows of compacted partitions (row i: vertex verts[i],
+// edges [index[i], index[i+1]) of the packed cols / weights).
+template <int WK>
+__global__ void __launch_bounds__(kSSThreads) sssp_expand_packed_kernel(const SSArgs *__restrict__ args,
+                                                                        CompactPayload pk) {
+    const SSArgs a = *args;
+    if (*(volatile uint32_t *)&a.hdr->done) return;
+    const RoundView rv = round_view(a);
+    const int lane = threadIdx.x & 31;
+    const uint32_t gwarp = (blockIdx.x * kSSThreads + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * kSSThreads) >> 5;
+    unsigned long long relaxed = 0, improved = 0;
+    for (uint64_t w = gwarp; w * 32 < pk.rows; w += nwarps) {
+        const uint64_t i = w * 32 + lane;
+        uint32_t deg = 0, d = a.inf;
+        uint64_t off = 0;
+        if (i < pk.rows) {
+            off = pk.index[i];
+            deg = static_cast<uint32_t>(pk.index[i + 1] - off);
+            d = __ldcg(a.dist + pk.verts[i]);
+            relaxed += deg;
+        }
+        uint32_t incl = deg;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+        for (uint32_t base = 0; base < total; base += 32 * kEdgeBatch) {
+            uint32_t u[kEdgeBatch], nd[kEdgeBatch], du[kEdgeBatch];
+#pragma unroll
+            for (int k = 0; k < kEdgeBatch; ++k) {
+                const uint32_t j = base + 32 * k + lane;
+                uint32_t lo = 0;
+#pragma unroll
+                for (uint32_t step = 16; step > 0; step >>= 1) {
+                    const uint32_t probe = __shfl_sync(0xffffffffu, incl, lo + step - 1);
+                    if (probe <= j) lo += step;
+                }
+                const uint32_t o_incl = __shfl_sync(0xffffffffu, incl, lo);
+                const uint32_t o_deg = __shfl_sync(0xffffffffu, deg, lo);
+                const uint64_t o_off = __shfl_sync(0xffffffffu, off, lo);
+                const uint32_t o_d = __shfl_sync(0xffffffffu, d, lo);
+                u[k] = 0;
+                nd[k] = a.inf;
+                if (j < total) {
+                    const uint64_t e = o_off + (j - (o_incl - o_deg));
+                    u[k] = dev::ld_stream(pk.cols + e);
+                    nd[k] = extend<WK>(o_d, edge_weight<WK>(pk.weights, e));
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < kEdgeBatch; ++k) du[k] = __ldcg(a.dist + u[k]);
+            relax_batch<kEdgeBatch>(a, rv, u, nd, du, lane, improved);
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) relaxed += __shfl_xor_sync(0xffffffffu, relaxed, o);
+    if (lane == 0 && relaxed) atomicAdd(&a.hdr->relaxations, relaxed);
 }
 
 template <int WK>
@@ -546,6 +678,141 @@ void sssp_run(GraphImpl &g, const hyt_sssp_params &p, uint32_t *dist_out, hyt_ru
         case HYT_WEIGHTS_NONE: sssp_solve<HYT_WEIGHTS_NONE>(g, p.source, delta, max_rounds, p.flags, s, dist_out, stats); break;
         case HYT_WEIGHTS_U32: sssp_solve<HYT_WEIGHTS_U32>(g, p.source, delta, max_rounds, p.flags, s, dist_out, stats); break;
         case HYT_WEIGHTS_F32: sssp_solve<HYT_WEIGHTS_F32>(g, p.source, kNoDelta, max_rounds, p.flags, s, dist_out, stats); break;
+        default: fail(HYT_E_INTERNAL, "unknown weight kind");
+    }
+}
+
+// Round loop of an out-of-HBM solve: per round the frontier's partition
+// metrics go to the source, which places every partition's edges (resident,
+// staged, mapped host memory) or compacts them; then the usual expansion.
+template <int WK>
+static void sssp_partitioned_solve(GraphImpl &g, PushSource &src, uint32_t source, uint32_t max_rounds,
+                                   cudaStream_t s, uint32_t *dist_out, hyt_run_stats *stats) {
+    const uint64_t V = g.V;
+    const size_t P = src.parts();
+    if (P == 0 || P > kMaxParts) fail(HYT_E_UNSUPPORTED, "partitioned SSSP supports 1..1024 partitions");
+    if (g.dist.count < V) g.dist.allocate(V);
+    if (g.stamp.count < 2 * V) g.stamp.allocate(2 * V);
+    for (int i = 0; i < 2; ++i) {
+        if (g.queue[i].count < V) g.queue[i].allocate(V);
+        if (g.far[i].count < V) g.far[i].allocate(V);
+    }
+    const uint64_t hub_cap = V + g.E / kHubChunk + 2;
+    if (g.hub_tasks.count < hub_cap) g.hub_tasks.allocate(hub_cap);
+    const size_t sb = 512 + sizeof(SSHeader);
+    if (g.sssp_state.count < sb) g.sssp_state.allocate(sb);
+    SSArgs *d_args = reinterpret_cast<SSArgs *>(g.sssp_state.get());
+    SSHeader *hdr = reinterpret_cast<SSHeader *>(g.sssp_state.get() + 256);
+    DeviceArray<EdgeLoc> d_loc(P);
+    DeviceArray<PartMetrics> d_metrics(P);
+    DeviceArray<uint32_t> d_list(V + 1);
+    uint32_t *d_count = d_list.get() + V;
+    PinnedArray<uint32_t> h_list;
+
+    SSArgs a{};
+    a.row_off = g.row_offsets.get();
+    a.dist = g.dist.get();
+    a.stamp = g.stamp.get();
+    a.fstamp = g.stamp.get() + V;
+    for (int i = 0; i < 2; ++i) {
+        a.queue[i] = g.queue[i].get();
+        a.far[i] = g.far[i].get();
+    }
+    a.hubs = g.hub_tasks.get();
+    a.hdr = hdr;
+    a.V = static_cast<uint32_t>(V);
+    a.source = source;
+    a.inf = (WK == HYT_WEIGHTS_F32) ? 0x7F800000u : HYT_DIST_INF_U32;
+    a.loc = d_loc.get();
+    a.part_shift = src.part_shift();
+    SSHeader h0{};
+    h0.qsize[0] = 1;
+    h0.max_rounds = max_rounds;
+    h0.delta = kNoDelta;
+    h0.threshold = 0xFFFFFFFFu;
+
+    const int grid = expand_grid<WK>();
+    EventTimer total;
+    total.start(s);
+    HYT_CUDA(cudaMemcpyAsync(d_args, &a, sizeof(a), cudaMemcpyHostToDevice, s));
+    HYT_CUDA(cudaMemcpyAsync(hdr, &h0, sizeof(h0), cudaMemcpyHostToDevice, s));
+    sssp_init_kernel<<<grid_for(V, 256, 148 * 8), 256, 0, s>>>(d_args);
+    HYT_CUDA(cudaGetLastError());
+    uint32_t launches = 1;
+    std::vector<PartMetrics> metrics(P);
+    RoundPlan plan;
+    for (uint32_t r = 0; r < max_rounds; ++r) {
+        sssp_split_kernel<<<grid, kSSThreads, 0, s>>>(d_args);
+        HYT_CUDA(cudaMemsetAsync(d_metrics.get(), 0, P * sizeof(PartMetrics), s));
+        sssp_part_stats_kernel<<<sm_count() * 2, kSSThreads, 0, s>>>(d_args, static_cast<uint32_t>(P), d_metrics.get());
+        HYT_CUDA(cudaGetLastError());
+        HYT_CUDA(cudaMemcpyAsync(metrics.data(), d_metrics.get(), P * sizeof(PartMetrics), cudaMemcpyDeviceToHost, s));
+        HYT_CUDA(cudaStreamSynchronize(s));
+        src.plan_round(metrics, plan);
+        launches += 2;
+        for (size_t w = 0; w < plan.waves.size(); ++w) {
+            src.enter_wave(w, s);
+            HYT_CUDA(cudaMemcpyAsync(d_loc.get(), plan.waves[w].data(), P * sizeof(EdgeLoc), cudaMemcpyHostToDevice,
+                                     s));
+            sssp_expand_kernel<WK, true><<<grid, kSSThreads, 0, s>>>(d_args);
+            sssp_hub_kernel<WK, true><<<grid, kSSThreads, 0, s>>>(d_args);
+            HYT_CUDA(cudaGetLastError());
+            HYT_CUDA(cudaMemsetAsync(&hdr->hub_count, 0, sizeof(uint32_t), s));
+            src.leave_wave(w, s);
+            launches += 2;
+        }
+        if (plan.compacted) {
+            HYT_CUDA(cudaMemsetAsync(d_count, 0, sizeof(uint32_t), s));
+            sssp_compacted_list_kernel<<<grid_for(V, 256, 148 * 8), 256, 0, s>>>(d_args, d_list.get(), d_count);
+            HYT_CUDA(cudaGetLastError());
+            uint32_t n = 0;
+            HYT_CUDA(cudaMemcpyAsync(&n, d_count, sizeof(n), cudaMemcpyDeviceToHost, s));
+            HYT_CUDA(cudaStreamSynchronize(s));
+            if (n) {
+                if (h_list.count < n) h_list.allocate(std::max<size_t>(n, 1u << 20));
+                HYT_CUDA(cudaMemcpyAsync(h_list.ptr, d_list.get(), n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+                HYT_CUDA(cudaStreamSynchronize(s));
+                const CompactPayload pk = src.compact(h_list.ptr, n, s);
+                sssp_expand_packed_kernel<WK><<<grid, kSSThreads, 0, s>>>(d_args, pk);
+                HYT_CUDA(cudaGetLastError());
+                launches += 2;
+            }
+        }
+        sssp_round_end_kernel<<<1, 1, 0, s>>>(d_args);
+        HYT_CUDA(cudaGetLastError());
+        ++launches;
+        src.end_round(s);
+        uint32_t done = 0;
+        HYT_CUDA(cudaMemcpyAsync(&done, &hdr->done, sizeof(done), cudaMemcpyDeviceToHost, s));
+        HYT_CUDA(cudaStreamSynchronize(s));
+        if (done) break;
+    }
+    SSHeader h{};
+    HYT_CUDA(cudaMemcpyAsync(&h, hdr, sizeof(h), cudaMemcpyDeviceToHost, s));
+    total.stop(s);
+    const double total_ms = total.ms();
+    if (dist_out) copy_from_device(dist_out, g.dist.get(), V * sizeof(uint32_t), s);
+    if (stats) {
+        stats->iterations = h.round;
+        stats->converged = h.converged;
+        stats->device_ms = total_ms;
+        stats->total_launches = launches;
+        stats->edges_processed = h.relaxations;
+        stats->vertices_processed = h.frontier_total;
+        stats->algorithmic_bytes = 16ull * h.frontier_total + 12ull * h.relaxations;
+    }
+}
+
+void sssp_partitioned(GraphImpl &g, PushSource &src, uint32_t source, uint32_t max_rounds, cudaStream_t s,
+                      uint32_t *dist_out, hyt_run_stats *stats) {
+    if (source >= g.V) fail(HYT_E_INVALID, "SSSP source vertex is out of range");
+    if (!g.weights_ok) fail(HYT_E_INVALID, "SSSP requires finite non-negative edge weights");
+    const uint64_t cap = std::min<uint64_t>(4 * g.V + 1024, 0x7FFFFFFFull);
+    const uint32_t rounds = max_rounds ? max_rounds : static_cast<uint32_t>(cap);
+    switch (g.weight_kind) {
+        case HYT_WEIGHTS_NONE: sssp_partitioned_solve<HYT_WEIGHTS_NONE>(g, src, source, rounds, s, dist_out, stats); break;
+        case HYT_WEIGHTS_U32: sssp_partitioned_solve<HYT_WEIGHTS_U32>(g, src, source, rounds, s, dist_out, stats); break;
+        case HYT_WEIGHTS_F32: sssp_partitioned_solve<HYT_WEIGHTS_F32>(g, src, source, rounds, s, dist_out, stats); break;
         default: fail(HYT_E_INTERNAL, "unknown weight kind");
     }
 }

@@ -212,10 +212,135 @@ class Graph:
         check(lib.hyt_sssp(self.handle, C.byref(p), _ptr(res) if res is not False else None, C.byref(st)))
         return res, st.as_dict()
 
+    def copy_csc(self, in_offsets=None, in_sources=None):
+        """The graph's CSC (ascending sources per in-row) into host numpy
+        arrays, or caller buffers (host or device)."""
+        off = np.empty(self.num_vertices + 1, np.uint64) if in_offsets is None else in_offsets
+        src = np.empty(max(self.num_edges, 1), np.uint32) if in_sources is None else in_sources
+        check(lib.hyt_graph_copy_csc(self.handle, _ptr(off), _ptr(src)))
+        return off, (src[: self.num_edges] if in_sources is None else src)
+
     def close(self) -> None:
         if getattr(self, "_h", None):
             check(lib.hyt_graph_destroy(self._h))
             self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class PinnedBuffer:
+    """Pinned, device-mapped host memory (hyt_pinned_alloc) viewed as numpy."""
+
+    def __init__(self, count: int, dtype):
+        self.dtype = np.dtype(dtype)
+        self.count = int(count)
+        p = C.c_void_p()
+        check(lib.hyt_pinned_alloc(max(self.count, 1) * self.dtype.itemsize, C.byref(p)))
+        self._p = p.value
+        buf = (C.c_char * (max(self.count, 1) * self.dtype.itemsize)).from_address(self._p)
+        self.array = np.frombuffer(buf, dtype=self.dtype, count=self.count)
+
+    def data_ptr(self) -> int:
+        return self._p
+
+    def free(self) -> None:
+        if getattr(self, "_p", None):
+            self.array = None
+            check(lib.hyt_pinned_free(self._p))
+            self._p = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def pinned_copy(x: np.ndarray) -> PinnedBuffer:
+    b = PinnedBuffer(x.shape[0], x.dtype)
+    if x.shape[0]:
+        b.array[:] = x
+    return b
+
+
+class HybridGraph:
+    """Graph whose edges stay in pinned host memory (hyt_hybrid handle):
+    the CSR (push, SSSP) and CSC (pull, PageRank) edge arrays are read per
+    partition through resident HBM copies, staged copies, host compaction
+    or zero-copy, as the HyTM cost model decides.
+
+    Arrays are numpy (copied into pinned buffers that this object owns) or
+    PinnedBuffer objects (used in place); they must outlive the handle."""
+
+    def __init__(self, row_offsets, column_indices, weights=None, in_offsets=None, in_sources=None,
+                 flags: int = capi.HYT_GRAPH_ALL, device: int = 0, budget_bytes: int = 0,
+                 partition_vertices: int = 0, host_threads: int = 0, force_engine: int = capi.HYT_ENGINE_AUTO,
+                 alpha: float = 0.0, beta: float = 0.0, gamma: float = 0.0):
+        def pin(x):
+            if x is None or isinstance(x, PinnedBuffer):
+                return x
+            return pinned_copy(np.ascontiguousarray(x))
+
+        self._bufs = [pin(x) for x in (row_offsets, column_indices, weights, in_offsets, in_sources)]
+        off, cols, w, ioff, isrc = self._bufs
+        V = off.count - 1
+        E = cols.count
+        c = capi.hyt_csr(V, E, off.data_ptr(), cols.data_ptr(), w.data_ptr() if w is not None else None,
+                         capi.HYT_WEIGHTS_U32 if w is not None else capi.HYT_WEIGHTS_NONE)
+        cc = None
+        if ioff is not None:
+            cc = capi.hyt_csc(V, isrc.count, ioff.data_ptr(), isrc.data_ptr())
+        opts = capi.hyt_hybrid_options(flags, device, budget_bytes, partition_vertices, host_threads, force_engine,
+                                       alpha, beta, gamma)
+        h = C.c_void_p()
+        check(lib.hyt_hybrid_create(C.byref(c), C.byref(cc) if cc is not None else None, C.byref(opts),
+                                    C.byref(h)))
+        self._h = h
+        self.num_vertices = V
+        self.num_edges = E
+
+    @property
+    def handle(self) -> C.c_void_p:
+        if not self._h:
+            raise ValueError("hybrid graph is closed")
+        return self._h
+
+    def info(self) -> dict:
+        i = capi.hyt_hybrid_info()
+        check(lib.hyt_hybrid_get_info(self.handle, C.byref(i)))
+        return i.as_dict()
+
+    def pagerank(self, damping: float = 0.85, tolerance: float = 1e-6, max_iterations: int = 100, out=None):
+        p = capi.hyt_pagerank_params(damping, tolerance, max_iterations, 0, None)
+        st, ts = capi.hyt_run_stats(), capi.hyt_hybrid_stats()
+        res = np.empty(self.num_vertices, dtype=np.float32) if out is None else out
+        check(lib.hyt_hybrid_pagerank(self.handle, C.byref(p), _ptr(res) if res is not False else None,
+                                      C.byref(st), C.byref(ts)))
+        return res, st.as_dict(), ts.as_dict()
+
+    def sssp(self, source: int, out=None, max_rounds: int = 0):
+        p = capi.hyt_sssp_params(source, 0, max_rounds, 0, None)
+        st, ts = capi.hyt_run_stats(), capi.hyt_hybrid_stats()
+        res = np.empty(self.num_vertices, dtype=np.uint32) if out is None else out
+        check(lib.hyt_hybrid_sssp(self.handle, C.byref(p), _ptr(res) if res is not False else None,
+                                  C.byref(st), C.byref(ts)))
+        return res, st.as_dict(), ts.as_dict()
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            check(lib.hyt_hybrid_destroy(self._h))
+            self._h = None
+        self._bufs = []
 
     def __enter__(self):
         return self

@@ -209,6 +209,99 @@ int hyt_sssp_noalloc(const hyt_csr *csr, uint32_t source, uint32_t *dist_out, vo
                      hyt_run_stats *stats);
 
 /* ------------------------------------------------------------------ */
+/* Out-of-HBM hybrid transfer (edges in pinned host memory)            */
+/* ------------------------------------------------------------------ */
+
+/* Reverse graph: in_offsets[V+1] (uint64), in_sources[E] (uint32), the
+ * sources of each vertex's in-edges in ascending source order -- the
+ * IncomingCSR that the reference's PageRank builds
+ * (src/algorithms/pagerank.cpp:19-59). */
+typedef struct hyt_csc {
+    uint64_t num_vertices;
+    uint64_t num_edges;
+    const uint64_t *in_offsets;
+    const uint32_t *in_sources;
+} hyt_csc;
+
+/* Copies an in-HBM graph's CSC (built with HYT_GRAPH_PULL) into caller
+ * buffers (host or device): in_offsets[V+1], in_sources[E]. */
+int hyt_graph_copy_csc(const hyt_graph *graph, uint64_t *in_offsets, uint32_t *in_sources);
+
+/* Pinned, device-mapped, portable host memory (cudaHostAlloc) for the
+ * host-side arrays of hybrid graphs; free with hyt_pinned_free. */
+int hyt_pinned_alloc(uint64_t bytes, void **out);
+int hyt_pinned_free(void *ptr);
+
+typedef struct hyt_hybrid hyt_hybrid;
+
+/* Transfer engines of the HyTM model (transfer::TransferEngine,
+ * include/transfer/hytm_cost_model.hpp:17-21). */
+enum hyt_engine {
+    HYT_ENGINE_AUTO = 0,        /* cost model decides per partition per round */
+    HYT_ENGINE_FILTER = 1,      /* ExpTM-Filter: whole partition copied */
+    HYT_ENGINE_COMPACTION = 2,  /* ExpTM-Compaction: active rows gathered on
+                                   the host, shipped packed */
+    HYT_ENGINE_ZERO_COPY = 3    /* ImpTM: kernels read mapped host memory */
+};
+
+/* The CSR (and, with HYT_GRAPH_PULL, the CSC) stay in HOST memory owned by
+ * the caller for the handle's lifetime: pinned (cudaHostAlloc /
+ * cudaMallocHost with mapping) or pageable (then registered mapped and
+ * read-only here, unregistered on destroy).  Vertex arrays (offsets,
+ * degrees, labels, ranks, frontiers) live in HBM outside the budget. */
+typedef struct hyt_hybrid_options {
+    uint32_t flags;               /* HYT_GRAPH_* (0 = HYT_GRAPH_ALL) */
+    int device;
+    uint64_t device_budget_bytes; /* HBM for edge data: resident partitions +
+                                     staging (0 = 8 GiB) */
+    uint32_t partition_vertices;  /* power of two (0 = 2^20); <= 1024 parts */
+    uint32_t host_threads;        /* compaction / gather threads (0 = all) */
+    uint32_t force_engine;        /* HYT_ENGINE_* for partitions that are not
+                                     resident (AUTO = cost model) */
+    float alpha, beta, gamma;     /* HyTM selector thresholds
+                                     (0 = 0.8 / 0.4 / 0.625) */
+} hyt_hybrid_options;
+
+typedef struct hyt_hybrid_info {
+    uint64_t partitions;
+    uint64_t budget_bytes;
+    uint64_t resident_bytes;          /* edge bytes resident in HBM */
+    uint64_t staging_bytes;           /* filter slots + compaction buffer */
+    uint64_t resident_push_partitions;
+    uint64_t resident_pull_partitions;
+    uint64_t device_bytes;            /* all HBM held by the handle */
+    double h2d_gbs;                   /* measured pinned cudaMemcpy H2D */
+    double zero_copy_gbs;             /* measured in-kernel mapped reads */
+    double gather_gbs;                /* measured host gather (compaction) */
+} hyt_hybrid_info;
+
+/* Per solve: decisions are counted per (partition, round) with work. */
+typedef struct hyt_hybrid_stats {
+    uint64_t rounds;
+    uint64_t resident_decisions, filter_decisions, compaction_decisions, zero_copy_decisions;
+    uint64_t filter_bytes;      /* cudaMemcpyAsync'd partitions */
+    uint64_t compaction_bytes;  /* packed payloads shipped */
+    uint64_t zero_copy_bytes;   /* 128-byte lines read over the link */
+    uint64_t link_bytes;        /* sum of the three */
+    uint64_t necessary_bytes;   /* edge bytes of the active rows not resident */
+    uint64_t copies;            /* cudaMemcpyAsync calls of the filter engine */
+    double compaction_host_ms;  /* host gather time */
+    double device_ms;           /* device time of the solve */
+    double link_gbs;            /* link_bytes / device time */
+    double h2d_peak_gbs;        /* measured pinned-copy peak */
+} hyt_hybrid_stats;
+
+int hyt_hybrid_create(const hyt_csr *csr, const hyt_csc *csc, const hyt_hybrid_options *options,
+                      hyt_hybrid **out);
+int hyt_hybrid_destroy(hyt_hybrid *hybrid);
+int hyt_hybrid_get_info(const hyt_hybrid *hybrid, hyt_hybrid_info *out);
+/* Same semantics, stop rule and outputs as hyt_pagerank / hyt_sssp. */
+int hyt_hybrid_pagerank(hyt_hybrid *hybrid, const hyt_pagerank_params *params, float *ranks_out,
+                        hyt_run_stats *stats, hyt_hybrid_stats *transfer);
+int hyt_hybrid_sssp(hyt_hybrid *hybrid, const hyt_sssp_params *params, uint32_t *dist_out,
+                    hyt_run_stats *stats, hyt_hybrid_stats *transfer);
+
+/* ------------------------------------------------------------------ */
 /* Seeded R-MAT generator (deterministic; same bytes on host and GPU)   */
 /* ------------------------------------------------------------------ */
 
