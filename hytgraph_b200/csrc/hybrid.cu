@@ -13,10 +13,11 @@
 //   zero-copy TLPs scaled by measured H2D / zero-copy read bandwidth.
 // and executes the selected engine:
 //   resident    -- already in HBM, nothing crosses the link;
-//   ExpTM-Filter -- the whole partition is copied (cudaMemcpyAsync on a copy
-//                  stream) into a staging slot; consecutive filter
-//                  partitions (<= 4, TaskCombiner's rule) share one copy;
-//                  copies of the next wave overlap the current wave's kernels;
+//   ExpTM-Filter -- the partition is copied (cudaMemcpyAsync on a copy
+//                  stream) into one of two staging slots, piece by piece
+//                  when it is larger than a slot; consecutive filter pieces
+//                  (<= 4, TaskCombiner's rule) share one copy; the next
+//                  copy overlaps the kernels reading the current slot;
 //   ExpTM-Compaction -- host threads gather the active rows (ids and
 //                  weights) into pinned staging, one copy ships the packed
 //                  payload (layout of the reference's CompactedPartition);
@@ -129,6 +130,25 @@ const void *device_alias(const void *p, size_t bytes, std::vector<void *> &regis
     return d;
 }
 
+
+// A piece: a vertex range of one partition whose edges are contiguous in the
+// CSR (push) or CSC (pull).  A resident partition is one piece; any other is
+// cut into pieces of at most one staging slot so that ExpTM-Filter can ship
+// it slot by slot.
+struct Piece {
+    uint32_t part;
+    uint32_t v0, v1;
+    uint64_t e0, e1;
+    PullPart tasks;  // pull side: tiles and long-row chunks of the piece
+};
+
+// Consecutive filter pieces shipped by one copy (TaskCombiner's rule: at
+// most kFilterCombineK of them, and they must fit one slot).
+struct Group {
+    size_t first, last;  // pieces [first, last)
+    uint64_t e0, e1;
+};
+
 }  // namespace
 
 struct HybridImpl {
@@ -149,7 +169,10 @@ struct HybridImpl {
 
     // partition geometry: [e0, e1) of the CSR (push) and CSC (pull)
     std::vector<uint64_t> push_e0, push_e1, pull_e0, pull_e1;
-    std::vector<PullPart> pull_parts;
+    std::vector<Piece> push_pieces, pull_pieces;
+    std::vector<size_t> push_first, pull_first;  // first piece of each partition, [P + 1]
+    std::vector<uint64_t> pull_zc_bytes;          // 128-byte lines of each partition's CSC
+    std::vector<PartMetrics> pull_metrics;        // all vertices active
 
     // residency
     std::vector<uint8_t> push_res, pull_res;
@@ -157,7 +180,7 @@ struct HybridImpl {
     DeviceArray<uint32_t> push_res_cols, push_res_w, pull_res_src;
     uint64_t resident_bytes = 0;
 
-    // staging: two slot groups
+    // staging: two slots, shared by both sides
     DeviceArray<uint32_t> stage_a[2], stage_b[2];  // push: cols / weights; pull: ids in stage_a
     uint64_t stage_edges = 0;
     cudaEvent_t ev_ready[2] = {nullptr, nullptr}, ev_free[2] = {nullptr, nullptr};
@@ -182,6 +205,22 @@ struct HybridImpl {
     }
 
     uint64_t push_bytes_per_edge() const { return h_w ? 8 : 4; }
+
+    // Copies edges [e0, e1) of one side into slot `slot` on the copy stream,
+    // once the slot's previous readers are done.
+    void issue_copy(bool push_side, int slot, uint64_t e0, uint64_t e1) {
+        HYT_CUDA(cudaStreamWaitEvent(copy, ev_free[slot], 0));
+        const uint64_t n = e1 - e0;
+        const uint32_t *a = push_side ? h_cols : h_in_src;
+        HYT_CUDA(cudaMemcpyAsync(stage_a[slot].get(), a + e0, n * 4, cudaMemcpyHostToDevice, copy));
+        stats.filter_bytes += n * 4;
+        if (push_side && h_w) {
+            HYT_CUDA(cudaMemcpyAsync(stage_b[slot].get(), h_w + e0, n * 4, cudaMemcpyHostToDevice, copy));
+            stats.filter_bytes += n * 4;
+        }
+        HYT_CUDA(cudaEventRecord(ev_ready[slot], copy));
+        ++stats.copies;
+    }
 };
 
 namespace {
@@ -237,7 +276,15 @@ void measure_link(HybridImpl &h) {
     h.model.cpu_bps = h.link.gather_gbs * 1e9;
 }
 
-// Greedy residency: largest partitions first while they fit the budget.
+// Staging slot size (bytes) for a side's budget: an eighth of it, between
+// 1 MiB and 1 GiB (copies of 1 GiB already run at the link's peak).
+uint64_t slot_bytes_for(uint64_t side_budget) {
+    return std::min<uint64_t>(std::max<uint64_t>(side_budget / 8, uint64_t(1) << 20), uint64_t(1) << 30);
+}
+
+// Greedy residency: after the staging reserve, the largest partitions first
+// while they fit.  Every resident partition is one contiguous run of the
+// resident array, in partition order.
 void choose_residency(const std::vector<uint64_t> &e0, const std::vector<uint64_t> &e1, uint64_t bpe,
                       uint64_t budget, std::vector<uint8_t> &res, std::vector<uint64_t> &pos, uint64_t &used_edges) {
     const size_t P = e0.size();
@@ -249,13 +296,12 @@ void choose_residency(const std::vector<uint64_t> &e0, const std::vector<uint64_
     uint64_t used = 0;
     for (size_t p : order) {
         const uint64_t n = e1[p] - e0[p];
-        if (n == 0) continue;
-        if ((used + n) * bpe <= budget) {
+        if (n && (used + n) * bpe <= budget) {
             res[p] = 1;
             used += n;
         }
     }
-    used_edges = 0;  // positions in partition order (contiguous runs stay contiguous)
+    used_edges = 0;
     for (size_t p = 0; p < P; ++p)
         if (res[p]) {
             pos[p] = used_edges;
@@ -275,6 +321,118 @@ void upload_resident(HybridImpl &h, const std::vector<uint8_t> &res, const std::
     HYT_CUDA(cudaStreamSynchronize(h.g.stream));
 }
 
+// Push pieces: non-resident partitions cut at vertex boundaries so that a
+// piece holds at most `cap` edges (a single larger row is a piece alone).
+void build_push_pieces(HybridImpl &h, uint64_t cap) {
+    h.push_pieces.clear();
+    h.push_first.assign(h.P + 1, 0);
+    for (size_t p = 0; p < h.P; ++p) {
+        h.push_first[p] = h.push_pieces.size();
+        const uint64_t v0 = uint64_t(p) << h.part_shift;
+        const uint64_t v1 = std::min<uint64_t>(h.g.V, (uint64_t(p) + 1) << h.part_shift);
+        if (h.push_res[p] || h.push_e1[p] - h.push_e0[p] <= cap) {
+            h.push_pieces.push_back(Piece{static_cast<uint32_t>(p), static_cast<uint32_t>(v0),
+                                          static_cast<uint32_t>(v1), h.push_e0[p], h.push_e1[p], PullPart{}});
+            continue;
+        }
+        uint64_t a = v0;
+        while (a < v1) {
+            uint64_t b = a + 1;
+            while (b < v1 && h.h_off[b + 1] - h.h_off[a] <= cap) ++b;
+            h.push_pieces.push_back(Piece{static_cast<uint32_t>(p), static_cast<uint32_t>(a),
+                                          static_cast<uint32_t>(b), h.h_off[a], h.h_off[b], PullPart{}});
+            a = b;
+        }
+    }
+    h.push_first[h.P] = h.push_pieces.size();
+}
+
+// Pull pieces: tiles are first split at partition boundaries (no tile
+// straddles two partitions); non-resident partitions are then cut between
+// tiles so that a piece holds at most `cap` in-edges.  A long row's chunk
+// tasks belong to the piece of the tile it ends.
+void build_pull_pieces(HybridImpl &h, uint64_t cap) {
+    GraphImpl &g = h.g;
+    cudaStream_t s = g.stream;
+    std::vector<uint32_t> ts(g.num_tiles + 1);
+    HYT_CUDA(cudaMemcpyAsync(ts.data(), g.tile_start.get(), ts.size() * 4, cudaMemcpyDeviceToHost, s));
+    std::vector<LongRow> lr(g.num_long);
+    if (g.num_long)
+        HYT_CUDA(cudaMemcpyAsync(lr.data(), g.long_rows.get(), lr.size() * sizeof(LongRow), cudaMemcpyDeviceToHost, s));
+    HYT_CUDA(cudaStreamSynchronize(s));
+    std::vector<uint32_t> bounds;
+    bounds.reserve(ts.size() + h.P + 1);
+    for (uint32_t v : ts) bounds.push_back(v);
+    for (size_t p = 0; p <= h.P; ++p)
+        bounds.push_back(static_cast<uint32_t>(std::min<uint64_t>(g.V, uint64_t(p) << h.part_shift)));
+    std::sort(bounds.begin(), bounds.end());
+    bounds.erase(std::unique(bounds.begin(), bounds.end()), bounds.end());
+    g.num_tiles = bounds.size() - 1;
+    g.tile_start.allocate(bounds.size());
+    HYT_CUDA(cudaMemcpyAsync(g.tile_start.get(), bounds.data(), bounds.size() * 4, cudaMemcpyHostToDevice, s));
+    HYT_CUDA(cudaStreamSynchronize(s));
+
+    const uint64_t *off = h.h_in_off;
+    h.pull_pieces.clear();
+    h.pull_first.assign(h.P + 1, 0);
+    uint64_t t = 0, c = 0, li = 0;
+    auto close_piece = [&](size_t p, uint64_t t0, uint64_t t1, uint64_t c0) {
+        const uint32_t va = bounds[t0], vb = bounds[t1];
+        while (li < g.num_long && lr[li].row < vb) {
+            c = lr[li].first_chunk + lr[li].num_chunks;
+            ++li;
+        }
+        h.pull_pieces.push_back(Piece{static_cast<uint32_t>(p), va, vb, off[va], off[vb], PullPart{c0, c, t0, t1}});
+    };
+    for (size_t p = 0; p < h.P; ++p) {
+        h.pull_first[p] = h.pull_pieces.size();
+        const uint64_t v1 = std::min<uint64_t>(g.V, (uint64_t(p) + 1) << h.part_shift);
+        const uint64_t tb = t;
+        while (t < g.num_tiles && bounds[t] < v1) ++t;
+        const uint64_t te = t;
+        if (h.pull_res[p] || h.pull_e1[p] - h.pull_e0[p] <= cap) {
+            close_piece(p, tb, te, c);
+            continue;
+        }
+        uint64_t a = tb;
+        while (a < te) {
+            uint64_t b = a + 1;
+            while (b < te && off[bounds[b + 1]] - off[bounds[a]] <= cap) ++b;
+            close_piece(p, a, b, c);
+            a = b;
+        }
+    }
+    h.pull_first[h.P] = h.pull_pieces.size();
+}
+
+// Groups consecutive pieces whose partitions chose ExpTM-Filter.
+std::vector<Group> filter_groups(const std::vector<Piece> &pieces, const std::vector<uint32_t> &engine,
+                                 uint64_t slot_edges) {
+    std::vector<Group> out;
+    for (size_t i = 0; i < pieces.size();) {
+        if (engine[pieces[i].part] != kFilter) {
+            ++i;
+            continue;
+        }
+        Group gr{i, i, pieces[i].e0, pieces[i].e0};
+        while (i < pieces.size() && engine[pieces[i].part] == kFilter && gr.last - gr.first < kFilterCombineK &&
+               pieces[i].e0 == gr.e1 && pieces[i].e1 - gr.e0 <= slot_edges) {
+            gr.e1 = pieces[i].e1;
+            gr.last = ++i;
+        }
+        out.push_back(gr);
+    }
+    return out;
+}
+
+// A partition may use ExpTM-Filter only if each of its pieces fits a slot.
+bool filterable(const std::vector<Piece> &pieces, const std::vector<size_t> &first, size_t p, uint64_t slot_edges) {
+    if (first[p] == first[p + 1]) return false;
+    for (size_t i = first[p]; i < first[p + 1]; ++i)
+        if (pieces[i].e1 - pieces[i].e0 > slot_edges) return false;
+    return true;
+}
+
 // ------------------------------------------------------------ push source --
 class HybridPush final : public PushSource {
 public:
@@ -284,16 +442,12 @@ public:
 
     void plan_round(const std::vector<PartMetrics> &m, RoundPlan &plan) override {
         const size_t P = h_.P;
+        const uint64_t bpe = h_.push_bytes_per_edge();
         engines_.assign(P, kZeroCopy);
         std::vector<EdgeLoc> base(P);
-        for (size_t p = 0; p < P; ++p) {
-            base[p].cols = h_.z_cols;
-            base[p].weights = h_.z_w;
-            base[p].mode = kLocDirect;
-        }
+        for (size_t p = 0; p < P; ++p) base[p] = EdgeLoc{h_.z_cols, h_.z_w, kLocDirect, 0u, 0xFFFFFFFFu, 0u};
         uint64_t cpay = 0;
         for (size_t p = 0; p < P; ++p) {
-            const uint64_t n = h_.push_e1[p] - h_.push_e0[p];
             if (h_.push_res[p]) {
                 engines_[p] = kResident;
                 base[p].cols = h_.push_res_cols.get() + h_.push_res_pos[p] - h_.push_e0[p];
@@ -301,14 +455,11 @@ public:
                                                       : nullptr;
                 continue;
             }
-            if (m[p].active_vertices == 0) {
-                engines_[p] = kZeroCopy;  // nothing to read
-                continue;
-            }
-            uint32_t e = h_.force ? h_.force : h_.model.select(n, m[p]);
-            if (e == kFilter && n > h_.stage_edges) e = kZeroCopy;  // does not fit a staging slot
+            if (m[p].active_vertices == 0) continue;  // nothing to read this round
+            uint32_t e = h_.force ? h_.force : h_.model.select(h_.push_e1[p] - h_.push_e0[p], m[p]);
+            if (e == kFilter && !filterable(h_.push_pieces, h_.push_first, p, h_.stage_edges)) e = kZeroCopy;
             if (e == kCompaction) {
-                const uint64_t need = m[p].active_edges * h_.push_bytes_per_edge() + m[p].active_vertices * 12 + 64;
+                const uint64_t need = m[p].active_edges * bpe + m[p].active_vertices * 12 + 64;
                 if (cpay + need > h_.cbytes) {
                     e = kZeroCopy;
                 } else {
@@ -318,28 +469,9 @@ public:
             engines_[p] = e;
             if (e == kCompaction) base[p].mode = kLocCompacted;
         }
-        // Waves: wave 0 = resident + zero-copy partitions; each filter group
-        // (<= kFilterCombineK consecutive filter partitions that fit a
-        // staging slot) becomes the next wave.
-        groups_.clear();
-        for (size_t p = 0; p < P;) {
-            if (engines_[p] != kFilter) {
-                ++p;
-                continue;
-            }
-            Group gr{p, p, h_.push_e0[p], h_.push_e0[p]};
-            while (p < P && engines_[p] == kFilter && gr.last - gr.first < kFilterCombineK &&
-                   h_.push_e1[p] - gr.e0 <= h_.stage_edges && h_.push_e0[p] == gr.e1) {
-                gr.e1 = h_.push_e1[p];
-                gr.last = ++p;
-            }
-            if (gr.last == gr.first) {  // did not fit next to nothing: cannot happen (checked above)
-                engines_[p] = kZeroCopy;
-                ++p;
-                continue;
-            }
-            groups_.push_back(gr);
-        }
+        // wave 0: resident, zero-copy and compacted partitions; then one wave
+        // per filter group, with the window of each partition's pieces in it
+        groups_ = filter_groups(h_.push_pieces, engines_, h_.stage_edges);
         plan.compacted = false;
         for (size_t p = 0; p < P; ++p) plan.compacted |= engines_[p] == kCompaction;
         plan.waves.assign(1 + groups_.size(), base);
@@ -349,38 +481,33 @@ public:
             auto &wl = plan.waves[w + 1];
             const Group &gr = groups_[w];
             const int slot = static_cast<int>(w & 1);
-            for (size_t p = 0; p < P; ++p) {
-                if (wl[p].mode == kLocCompacted) continue;
-                if (p >= gr.first && p < gr.last) {
-                    wl[p].cols = h_.stage_a[slot].get() - gr.e0;
-                    wl[p].weights = h_.z_w ? h_.stage_b[slot].get() - gr.e0 : nullptr;
-                    wl[p].mode = kLocDirect;
+            for (size_t p = 0; p < P; ++p)
+                if (wl[p].mode != kLocCompacted) wl[p].mode = kLocSkip;
+            for (size_t i = gr.first; i < gr.last; ++i) {
+                const Piece &pc = h_.push_pieces[i];
+                EdgeLoc &L = wl[pc.part];
+                if (L.mode == kLocSkip) {
+                    L = EdgeLoc{h_.stage_a[slot].get() - gr.e0, h_.z_w ? h_.stage_b[slot].get() - gr.e0 : nullptr,
+                                kLocDirect, pc.v0, pc.v1, 0u};
                 } else {
-                    wl[p].mode = kLocSkip;
+                    L.vhi = pc.v1;  // pieces of a partition in one group are consecutive
                 }
             }
         }
         for (size_t p = 0; p < P; ++p) {
-            const uint64_t n = h_.push_e1[p] - h_.push_e0[p];
+            if (!m[p].active_vertices) continue;
             switch (engines_[p]) {
                 case kResident: ++h_.stats.resident_decisions; break;
-                case kFilter:
-                    ++h_.stats.filter_decisions;
-                    h_.stats.filter_bytes += n * h_.push_bytes_per_edge();
-                    break;
+                case kFilter: ++h_.stats.filter_decisions; break;
                 case kCompaction: ++h_.stats.compaction_decisions; break;
                 default:
-                    if (m[p].active_vertices) {
-                        ++h_.stats.zero_copy_decisions;
-                        // 128-byte lines of the ids (and weights) the kernel touches
-                        h_.stats.zero_copy_bytes += (m[p].zc_requests + m[p].zc_alignment) * 128 *
-                                                    (h_.z_w ? 2 : 1);
-                    }
+                    ++h_.stats.zero_copy_decisions;
+                    // 128-byte lines of the ids (and weights) the kernels touch
+                    h_.stats.zero_copy_bytes += (m[p].zc_requests + m[p].zc_alignment) * 128 * (h_.z_w ? 2 : 1);
             }
-            if (m[p].active_vertices) h_.stats.necessary_bytes += m[p].active_edges * h_.push_bytes_per_edge();
+            if (engines_[p] != kResident) h_.stats.necessary_bytes += m[p].active_edges * bpe;
         }
-        // prefetch the first two filter groups
-        for (size_t w = 0; w < std::min<size_t>(2, groups_.size()); ++w) issue_copy(w);
+        for (size_t w = 0; w < std::min<size_t>(2, groups_.size()); ++w) issue(w);
     }
 
     void enter_wave(size_t w, cudaStream_t s) override {
@@ -392,7 +519,7 @@ public:
         if (w == 0) return;
         const size_t gi = w - 1;
         HYT_CUDA(cudaEventRecord(h_.ev_free[gi & 1], s));
-        if (gi + 2 < groups_.size()) issue_copy(gi + 2);
+        if (gi + 2 < groups_.size()) issue(gi + 2);
     }
 
     CompactPayload compact(const uint32_t *verts, uint64_t n, cudaStream_t s) override {
@@ -431,8 +558,7 @@ public:
         pk.cols = reinterpret_cast<const uint32_t *>(h_.cdev.get() + o_cols);
         pk.weights = bpe == 8 ? reinterpret_cast<const uint32_t *>(h_.cdev.get() + o_w) : nullptr;
         pk.rows = n;
-        // the payload buffer is reused next round: wait for this round's kernels
-        pending_ = true;
+        pending_ = true;  // the buffers are reused next round
         return pk;
     }
 
@@ -445,21 +571,8 @@ public:
     }
 
 private:
-    struct Group {
-        size_t first, last;  // partitions [first, last)
-        uint64_t e0, e1;     // their edges
-    };
-
-    void issue_copy(size_t gi) {
-        const Group &gr = groups_[gi];
-        const int slot = static_cast<int>(gi & 1);
-        HYT_CUDA(cudaStreamWaitEvent(h_.copy, h_.ev_free[slot], 0));
-        const uint64_t n = gr.e1 - gr.e0;
-        HYT_CUDA(cudaMemcpyAsync(h_.stage_a[slot].get(), h_.h_cols + gr.e0, n * 4, cudaMemcpyHostToDevice, h_.copy));
-        if (h_.h_w)
-            HYT_CUDA(cudaMemcpyAsync(h_.stage_b[slot].get(), h_.h_w + gr.e0, n * 4, cudaMemcpyHostToDevice, h_.copy));
-        HYT_CUDA(cudaEventRecord(h_.ev_ready[slot], h_.copy));
-        ++h_.stats.copies;
+    void issue(size_t gi) {
+        h_.issue_copy(true, static_cast<int>(gi & 1), groups_[gi].e0, groups_[gi].e1);
     }
 
     HybridImpl &h_;
@@ -471,10 +584,10 @@ private:
 // ------------------------------------------------------------ pull source --
 class HybridPull final : public PullSource {
 public:
+    // Every vertex is active in every PageRank iteration, so each
+    // partition's decision is the same every iteration: it is taken once
+    // per solve from metrics over the partition's whole CSC.
     explicit HybridPull(HybridImpl &h) : h_(h) {
-        // Every vertex is active in every PageRank iteration, so the
-        // decision per partition is the same each iteration: metrics over
-        // the partition's in-rows (CSC), computed once.
         const size_t P = h_.P;
         engines_.assign(P, kZeroCopy);
         for (size_t p = 0; p < P; ++p) {
@@ -484,124 +597,67 @@ public:
                 continue;
             }
             if (n == 0) continue;
-            const uint64_t v0 = uint64_t(p) << h_.part_shift;
-            const uint64_t v1 = std::min<uint64_t>(h_.g.V, (uint64_t(p) + 1) << h_.part_shift);
-            PartMetrics pm{};
-            pm.active_vertices = v1 - v0;
-            pm.active_edges = n;
-            for (uint64_t v = v0; v < v1; ++v) {
-                const uint64_t d = h_.h_in_off[v + 1] - h_.h_in_off[v];
-                if (!d) continue;
-                pm.zc_requests += (d * 4 + 127) / 128;
-                if ((h_.h_in_off[v] * 4) % 128) ++pm.zc_alignment;
-            }
-            uint32_t e = h_.force ? h_.force : h_.model.select(n, pm);
+            uint32_t e = h_.force ? h_.force : h_.model.select(n, h_.pull_metrics[p]);
             if (e == kCompaction) e = kFilter;  // all rows active: the packed payload is the partition
-            if (e == kFilter && n > h_.stage_edges) e = kZeroCopy;
+            if (e == kFilter && !filterable(h_.pull_pieces, h_.pull_first, p, h_.stage_edges)) e = kZeroCopy;
             engines_[p] = e;
-            // a tile reads its partition's sources as one contiguous span
-            if (e == kZeroCopy) zc_bytes_ += (n * 4 + 127) / 128 * 128;
+            if (e == kZeroCopy) zc_bytes_ += h_.pull_zc_bytes[p];
         }
-        for (size_t p = 0; p < P; ++p)
-            if (engines_[p] == kFilter) filter_order_.push_back(p);
+        groups_ = filter_groups(h_.pull_pieces, engines_, h_.stage_edges);
+        group_of_.assign(h_.pull_pieces.size(), kNone);
+        for (size_t gi = 0; gi < groups_.size(); ++gi)
+            for (size_t i = groups_[gi].first; i < groups_[gi].last; ++i) group_of_[i] = gi;
     }
 
-    size_t parts() const override { return h_.P; }
-    PullPart part(size_t p) const override { return h_.pull_parts[p]; }
+    size_t parts() const override { return h_.pull_pieces.size(); }
+    PullPart part(size_t i) const override { return h_.pull_pieces[i].tasks; }
 
     void begin_iteration(cudaStream_t) override {
-        for (size_t i = 0; i < std::min<size_t>(2, filter_order_.size()); ++i) issue(i);
-        for (uint32_t e : engines_) {
-            if (e == kResident) ++h_.stats.resident_decisions;
-            if (e == kFilter) ++h_.stats.filter_decisions;
-            if (e == kZeroCopy) ++h_.stats.zero_copy_decisions;
+        for (size_t gi = 0; gi < std::min<size_t>(2, groups_.size()); ++gi) issue(gi);
+        for (size_t p = 0; p < h_.P; ++p) {
+            if (h_.pull_e1[p] == h_.pull_e0[p]) continue;
+            switch (engines_[p]) {
+                case kResident: ++h_.stats.resident_decisions; break;
+                case kFilter: ++h_.stats.filter_decisions; break;
+                default: ++h_.stats.zero_copy_decisions;
+            }
+            if (engines_[p] != kResident) h_.stats.necessary_bytes += (h_.pull_e1[p] - h_.pull_e0[p]) * 4;
         }
         h_.stats.zero_copy_bytes += zc_bytes_;
-        h_.stats.necessary_bytes += h_.g.E * 4;
         ++h_.stats.rounds;
     }
 
-    const uint32_t *acquire(size_t p, cudaStream_t s) override {
-        switch (engines_[p]) {
-            case kResident: return h_.pull_res_src.get() + h_.pull_res_pos[p] - h_.pull_e0[p];
+    const uint32_t *acquire(size_t i, cudaStream_t s) override {
+        const Piece &pc = h_.pull_pieces[i];
+        switch (engines_[pc.part]) {
+            case kResident: return h_.pull_res_src.get() + h_.pull_res_pos[pc.part] - h_.pull_e0[pc.part];
             case kFilter: {
-                const size_t k = rank_of(p);
-                HYT_CUDA(cudaStreamWaitEvent(s, h_.ev_ready[k & 1], 0));
-                return h_.stage_a[k & 1].get() - h_.pull_e0[p];
+                const size_t gi = group_of_[i];
+                if (i == groups_[gi].first) HYT_CUDA(cudaStreamWaitEvent(s, h_.ev_ready[gi & 1], 0));
+                return h_.stage_a[gi & 1].get() - groups_[gi].e0;
             }
             default: return h_.z_in_src;
         }
     }
 
-    void release(size_t p, cudaStream_t s) override {
-        if (engines_[p] != kFilter) return;
-        const size_t k = rank_of(p);
-        HYT_CUDA(cudaEventRecord(h_.ev_free[k & 1], s));
-        if (k + 2 < filter_order_.size()) issue(k + 2);
+    void release(size_t i, cudaStream_t s) override {
+        const size_t gi = group_of_[i];
+        if (gi == kNone || i + 1 != groups_[gi].last) return;
+        HYT_CUDA(cudaEventRecord(h_.ev_free[gi & 1], s));
+        if (gi + 2 < groups_.size()) issue(gi + 2);
     }
 
 private:
-    size_t rank_of(size_t p) const {
-        return static_cast<size_t>(std::lower_bound(filter_order_.begin(), filter_order_.end(), p) -
-                                   filter_order_.begin());
-    }
+    static constexpr size_t kNone = ~size_t(0);
 
-    void issue(size_t k) {
-        const size_t p = filter_order_[k];
-        const int slot = static_cast<int>(k & 1);
-        HYT_CUDA(cudaStreamWaitEvent(h_.copy, h_.ev_free[slot], 0));
-        const uint64_t n = h_.pull_e1[p] - h_.pull_e0[p];
-        HYT_CUDA(cudaMemcpyAsync(h_.stage_a[slot].get(), h_.h_in_src + h_.pull_e0[p], n * 4, cudaMemcpyHostToDevice,
-                                 h_.copy));
-        HYT_CUDA(cudaEventRecord(h_.ev_ready[slot], h_.copy));
-        h_.stats.filter_bytes += n * 4;
-        ++h_.stats.copies;
-    }
+    void issue(size_t gi) { h_.issue_copy(false, static_cast<int>(gi & 1), groups_[gi].e0, groups_[gi].e1); }
 
     HybridImpl &h_;
     std::vector<uint32_t> engines_;
-    std::vector<size_t> filter_order_;
+    std::vector<Group> groups_;
+    std::vector<size_t> group_of_;
     uint64_t zc_bytes_ = 0;
 };
-
-// Splits tiles at partition boundaries and records each partition's task
-// ranges (tiles never straddle two partitions; long rows belong to one).
-void partition_pull_tasks(HybridImpl &h) {
-    GraphImpl &g = h.g;
-    cudaStream_t s = g.stream;
-    std::vector<uint32_t> ts(g.num_tiles + 1);
-    HYT_CUDA(cudaMemcpyAsync(ts.data(), g.tile_start.get(), ts.size() * 4, cudaMemcpyDeviceToHost, s));
-    std::vector<LongRow> lr(g.num_long);
-    if (g.num_long)
-        HYT_CUDA(cudaMemcpyAsync(lr.data(), g.long_rows.get(), lr.size() * sizeof(LongRow), cudaMemcpyDeviceToHost, s));
-    HYT_CUDA(cudaStreamSynchronize(s));
-    std::vector<uint32_t> bounds;
-    bounds.reserve(ts.size() + h.P + 1);
-    for (uint32_t v : ts) bounds.push_back(v);
-    for (size_t p = 0; p <= h.P; ++p) bounds.push_back(static_cast<uint32_t>(std::min<uint64_t>(g.V, uint64_t(p) << h.part_shift)));
-    std::sort(bounds.begin(), bounds.end());
-    bounds.erase(std::unique(bounds.begin(), bounds.end()), bounds.end());
-    g.num_tiles = bounds.size() - 1;
-    g.tile_start.allocate(bounds.size());
-    HYT_CUDA(cudaMemcpyAsync(g.tile_start.get(), bounds.data(), bounds.size() * 4, cudaMemcpyHostToDevice, s));
-    HYT_CUDA(cudaStreamSynchronize(s));
-    h.pull_parts.assign(h.P, PullPart{});
-    uint64_t t = 0, c = 0, li = 0;
-    for (size_t p = 0; p < h.P; ++p) {
-        const uint64_t v1 = std::min<uint64_t>(g.V, (uint64_t(p) + 1) << h.part_shift);
-        PullPart pp{};
-        pp.tile_begin = t;
-        while (t < g.num_tiles && bounds[t] < v1) ++t;
-        pp.tile_end = t;
-        pp.chunk_begin = c;
-        while (li < g.num_long && lr[li].row < v1) {
-            c = lr[li].first_chunk + lr[li].num_chunks;
-            ++li;
-        }
-        pp.chunk_end = c;
-        h.pull_parts[p] = pp;
-    }
-}
 
 HybridImpl *impl(hyt_hybrid *x) {
     if (!x) fail(HYT_E_INVALID, "hybrid handle is NULL");
@@ -673,46 +729,62 @@ HybridImpl *hybrid_create(const hyt_csr *csr, const hyt_csc *csc, const hyt_hybr
         h->push_e0[p] = h->h_off[std::min<uint64_t>(V, uint64_t(p) << h->part_shift)];
         h->push_e1[p] = h->h_off[std::min<uint64_t>(V, (uint64_t(p) + 1) << h->part_shift)];
     }
-    uint64_t max_part = 0;
     if (push) {
         h->z_cols = static_cast<const uint32_t *>(device_alias(h->h_cols, E * 4, h->registered));
         if (h->h_w) h->z_w = static_cast<const uint32_t *>(device_alias(h->h_w, E * 4, h->registered));
-        for (size_t p = 0; p < h->P; ++p) max_part = std::max(max_part, h->push_e1[p] - h->push_e0[p]);
     }
     if (pull) {
         h->h_in_off = csc->in_offsets;
         h->h_in_src = csc->in_sources;
+        if (is_device_pointer(h->h_in_off) || is_device_pointer(h->h_in_src))
+            fail(HYT_E_INVALID, "hybrid graphs take host arrays, not device memory");
         if (h->h_in_off[0] != 0 || h->h_in_off[V] != E) fail(HYT_E_INVALID, "CSC offsets must start at 0 and end at E");
         h->z_in_src = static_cast<const uint32_t *>(device_alias(h->h_in_src, E * 4, h->registered));
         h->pull_e0.resize(h->P);
         h->pull_e1.resize(h->P);
+        h->pull_zc_bytes.assign(h->P, 0);
+        h->pull_metrics.assign(h->P, PartMetrics{});
         for (size_t p = 0; p < h->P; ++p) {
-            h->pull_e0[p] = h->h_in_off[std::min<uint64_t>(V, uint64_t(p) << h->part_shift)];
-            h->pull_e1[p] = h->h_in_off[std::min<uint64_t>(V, (uint64_t(p) + 1) << h->part_shift)];
-            max_part = std::max(max_part, h->pull_e1[p] - h->pull_e0[p]);
+            const uint64_t v0 = std::min<uint64_t>(V, uint64_t(p) << h->part_shift);
+            const uint64_t v1 = std::min<uint64_t>(V, (uint64_t(p) + 1) << h->part_shift);
+            h->pull_e0[p] = h->h_in_off[v0];
+            h->pull_e1[p] = h->h_in_off[v1];
+            PartMetrics &pm = h->pull_metrics[p];
+            pm.active_vertices = v1 - v0;
+            pm.active_edges = h->pull_e1[p] - h->pull_e0[p];
+            for (uint64_t v = v0; v < v1; ++v) {
+                const uint64_t d = h->h_in_off[v + 1] - h->h_in_off[v];
+                if (!d) continue;
+                pm.zc_requests += (d * 4 + 127) / 128;
+                if ((h->h_in_off[v] * 4) % 128) ++pm.zc_alignment;
+            }
+            // a tile reads its partition's sources as one contiguous span
+            h->pull_zc_bytes[p] = (pm.active_edges * 4 + 127) / 128 * 128;
         }
-        g.in_offsets.allocate(V + 1);
-        HYT_CUDA(cudaMemcpyAsync(g.in_offsets.get(), h->h_in_off, (V + 1) * 8, cudaMemcpyHostToDevice, g.stream));
-        HYT_CUDA(cudaStreamSynchronize(g.stream));
-        g.tile_cost = kTileCostDefault;
-        g.num_hot = 0;  // host sources are untagged
-        build_pull_tiles(g, g.stream);
-        partition_pull_tasks(*h);
     }
 
-    // budget: two staging slots (1/8 each), compaction buffer (1/8), rest resident
+    // Budget: two staging slots (+ the compaction buffer, half a slot, on
+    // the push side), the rest resident; both sides split it when both are
+    // built, and share the slots.
     const uint64_t bpe_push = h->h_w ? 8 : 4;
-    const uint64_t bpe = push ? bpe_push : 4;
-    const uint64_t slot_bytes = std::max<uint64_t>(h->budget / 8, 64ull << 20);
-    h->stage_edges = slot_bytes / bpe;
-    h->cbytes = push ? slot_bytes : 0;
-    const uint64_t reserve = 2 * slot_bytes + h->cbytes;
-    const uint64_t res_budget = h->budget > reserve ? h->budget - reserve : 0;
-    uint64_t res_edges = 0;
+    const uint64_t side_budget = (push && pull) ? h->budget / 2 : h->budget;
+    const uint64_t slot = slot_bytes_for(side_budget);
+    uint64_t slot_edges = 0;
     if (push) {
-        // SSSP and PageRank share the budget when both sides are requested
-        const uint64_t push_budget = pull ? res_budget / 2 : res_budget;
-        choose_residency(h->push_e0, h->push_e1, bpe_push, push_budget, h->push_res, h->push_res_pos, res_edges);
+        const uint64_t reserve = 2 * slot + slot / 2;
+        uint64_t res_edges = 0;
+        choose_residency(h->push_e0, h->push_e1, bpe_push, side_budget > reserve ? side_budget - reserve : 0,
+                         h->push_res, h->push_res_pos, res_edges);
+        build_push_pieces(*h, slot / bpe_push);
+        uint64_t need = 0, nonres = 0;  // slots no larger than the largest staged piece
+        for (const Piece &pc : h->push_pieces)
+            if (!h->push_res[pc.part]) {
+                need = std::max(need, std::min(pc.e1 - pc.e0, slot / bpe_push));
+                nonres += pc.e1 - pc.e0;
+            }
+        slot_edges = std::max(slot_edges, need);
+        h->cbytes = std::min(slot / 2, nonres * bpe_push + (uint64_t(1) << 16) * 12);
+        if (!nonres) h->cbytes = 0;
         h->push_res_cols.allocate(std::max<uint64_t>(res_edges, 1));
         if (h->h_w) h->push_res_w.allocate(std::max<uint64_t>(res_edges, 1));
         upload_resident(*h, h->push_res, h->push_e0, h->push_e1, h->push_res_pos, h->h_cols, h->h_w,
@@ -720,16 +792,30 @@ HybridImpl *hybrid_create(const hyt_csr *csr, const hyt_csc *csc, const hyt_hybr
         h->resident_bytes += res_edges * bpe_push;
     }
     if (pull) {
-        const uint64_t pull_budget = push ? res_budget / 2 : res_budget;
-        choose_residency(h->pull_e0, h->pull_e1, 4, pull_budget, h->pull_res, h->pull_res_pos, res_edges);
+        const uint64_t reserve = 2 * slot;
+        uint64_t res_edges = 0;
+        choose_residency(h->pull_e0, h->pull_e1, 4, side_budget > reserve ? side_budget - reserve : 0, h->pull_res,
+                         h->pull_res_pos, res_edges);
+        g.in_offsets.allocate(V + 1);
+        HYT_CUDA(cudaMemcpyAsync(g.in_offsets.get(), h->h_in_off, (V + 1) * 8, cudaMemcpyHostToDevice, g.stream));
+        HYT_CUDA(cudaStreamSynchronize(g.stream));
+        g.tile_cost = kTileCostDefault;
+        g.num_hot = 0;  // host sources are untagged
+        build_pull_tiles(g, g.stream);
+        build_pull_pieces(*h, slot / 4);
+        uint64_t need = 0;
+        for (const Piece &pc : h->pull_pieces)
+            if (!h->pull_res[pc.part]) need = std::max(need, std::min(pc.e1 - pc.e0, slot / 4));
+        slot_edges = std::max(slot_edges, need);
         h->pull_res_src.allocate(std::max<uint64_t>(res_edges, 1));
         upload_resident(*h, h->pull_res, h->pull_e0, h->pull_e1, h->pull_res_pos, h->h_in_src, nullptr,
                         h->pull_res_src.get(), nullptr);
         h->resident_bytes += res_edges * 4;
     }
+    h->stage_edges = slot_edges;
     for (int i = 0; i < 2; ++i) {
-        h->stage_a[i].allocate(h->stage_edges);
-        if (push && h->h_w) h->stage_b[i].allocate(h->stage_edges);
+        if (slot_edges) h->stage_a[i].allocate(slot_edges);
+        if (slot_edges && push && h->h_w) h->stage_b[i].allocate(slot_edges);
         HYT_CUDA(cudaEventRecord(h->ev_free[i], g.stream));
     }
     if (h->cbytes) {
@@ -737,7 +823,6 @@ HybridImpl *hybrid_create(const hyt_csr *csr, const hyt_csc *csc, const hyt_hybr
         h->chost.allocate(h->cbytes);
     }
     measure_link(*h);
-    (void)max_part;
     return h.release();
 }
 

@@ -20,15 +20,17 @@
 namespace hyt {
 
 // ---------------------------------------------------------------- pull ----
+// A piece: a vertex range of one partition whose in-edges are contiguous;
+// partitions larger than a staging slot are split into several pieces.
 struct PullPart {
-    uint64_t chunk_begin, chunk_end;  // long-row chunk tasks of the partition
-    uint64_t tile_begin, tile_end;    // tiles of the partition
+    uint64_t chunk_begin, chunk_end;  // long-row chunk tasks of the piece
+    uint64_t tile_begin, tile_end;    // tiles of the piece
 };
 
 class PullSource {
 public:
     virtual ~PullSource() = default;
-    virtual size_t parts() const = 0;
+    virtual size_t parts() const = 0;  // pieces, in vertex order
     virtual PullPart part(size_t p) const = 0;
     virtual void begin_iteration(cudaStream_t compute) = 0;
     // Makes partition p's source ids readable by work enqueued on `compute`
@@ -45,14 +47,17 @@ void pagerank_partitioned(GraphImpl &g, PullSource &src, bool personalized, uint
                           float tolerance, uint32_t max_iter, cudaStream_t s, float *ranks_out, hyt_run_stats *stats);
 
 // ---------------------------------------------------------------- push ----
-// kLocDirect: edges at cols/weights; kLocCompacted: expanded from the packed
-// payload; kLocSkip: not expanded in this wave (another wave covers it).
+// kLocDirect: edges at cols/weights (for the vertices of [vlo, vhi): a
+// partition larger than a staging slot is staged piece by piece, one piece
+// per wave); kLocCompacted: expanded from the packed payload; kLocSkip: not
+// expanded in this wave (another wave covers it).
 enum : uint32_t { kLocDirect = 0, kLocCompacted = 1, kLocSkip = 2 };
 
 struct EdgeLoc {
     const uint32_t *cols;     // global-edge-indexed (device slot - e0, or host)
     const uint32_t *weights;  // same addressing
-    uint32_t mode;            // kLocDirect or kLocCompacted
+    uint32_t mode;            // kLocDirect, kLocCompacted or kLocSkip
+    uint32_t vlo, vhi;        // kLocDirect: only vertices in [vlo, vhi) are expanded
     uint32_t pad;
 };
 

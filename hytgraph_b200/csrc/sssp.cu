@@ -253,7 +253,7 @@ __global__ void __launch_bounds__(kSSThreads) sssp_expand_kernel(const SSArgs *_
                 const EdgeLoc L = a.loc[v >> a.part_shift];
                 vc = L.cols;
                 vw = L.weights;
-                if (L.mode != kLocDirect) full = 0;
+                if (L.mode != kLocDirect || v < L.vlo || v >= L.vhi) full = 0;
             }
             d = __ldcg(a.dist + v);
             relaxed += full;

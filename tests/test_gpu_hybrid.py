@@ -43,10 +43,16 @@ def _hybrid(hyt, g, **kw):
     return hyt.HybridGraph(g.row_offsets, g.column_indices, g.weights, in_off, in_src, **kw)
 
 
-def _budget_partial(g):
-    """Budget whose resident share holds about half of the edges (the
-    engine keeps two 64 MiB staging slots and a 64 MiB compaction buffer)."""
-    return 192 * MiB + g.num_edges * 4
+def _push_budget(g):
+    """Budget whose resident share holds about half of the CSR edge bytes:
+    below 8 MiB the engine reserves two 1 MiB staging slots and a 0.5 MiB
+    compaction buffer, and keeps the largest partitions in what is left."""
+    return 5 * MiB // 2 + g.num_edges * 4
+
+
+def _pull_budget(g):
+    """Same for the CSC side: two 1 MiB slots, half of the 4-byte ids."""
+    return 2 * MiB + g.num_edges * 2
 
 
 ENGINES = ["FILTER", "COMPACTION", "ZERO_COPY"]
@@ -55,10 +61,12 @@ ENGINES = ["FILTER", "COMPACTION", "ZERO_COPY"]
 @pytest.mark.parametrize("engine", ENGINES)
 @pytest.mark.parametrize("resident", [False, True])
 def test_hybrid_sssp_forced_engines_bit_exact(hyt, oracle, gpu, engine, resident):
-    g = hyt.rmat(14, 16, 21)
+    # scale 16 with 2^12-vertex partitions: partition 0 holds ~1/3 of the
+    # edges, more than a 1 MiB staging slot, so it is staged in pieces
+    g = hyt.rmat(16, 16, 21)
     sources = hyt.pick_sources(g.row_offsets, 5, 2)
-    budget = _budget_partial(g) if resident else 1
-    with _hybrid(hyt, g, flags=hyt.capi.HYT_GRAPH_PUSH, budget_bytes=budget, partition_vertices=1 << 10,
+    budget = _push_budget(g) if resident else 1
+    with _hybrid(hyt, g, flags=hyt.capi.HYT_GRAPH_PUSH, budget_bytes=budget, partition_vertices=1 << 12,
                  force_engine=getattr(hyt.capi, "HYT_ENGINE_" + engine)) as hg:
         info = hg.info()
         assert info["partitions"] == 16
@@ -83,10 +91,10 @@ def test_hybrid_sssp_forced_engines_bit_exact(hyt, oracle, gpu, engine, resident
 @pytest.mark.parametrize("engine", ["FILTER", "ZERO_COPY"])
 @pytest.mark.parametrize("resident", [False, True])
 def test_hybrid_pagerank_forced_engines(hyt, oracle, gpu, engine, resident):
-    g = hyt.rmat(14, 16, 22)
+    g = hyt.rmat(16, 16, 22)
     ref, it_ref, _, conv_ref = oracle.pagerank_f64(g.row_offsets, g.column_indices)
-    budget = 128 * MiB + g.num_edges * 2 if resident else 1
-    with _hybrid(hyt, g, flags=hyt.capi.HYT_GRAPH_PULL, budget_bytes=budget, partition_vertices=1 << 10,
+    budget = _pull_budget(g) if resident else 1
+    with _hybrid(hyt, g, flags=hyt.capi.HYT_GRAPH_PULL, budget_bytes=budget, partition_vertices=1 << 12,
                  force_engine=getattr(hyt.capi, "HYT_ENGINE_" + engine)) as hg:
         info = hg.info()
         if resident:
@@ -111,7 +119,7 @@ def test_hybrid_cost_model_mixed_decisions(hyt, oracle, gpu):
     s = int(hyt.pick_sources(g.row_offsets, 9, 1)[0])
     ref = _dijkstra(oracle, g, s)
     pr_ref, _, _, _ = oracle.pagerank_f64(g.row_offsets, g.column_indices)
-    with _hybrid(hyt, g, budget_bytes=_budget_partial(g), partition_vertices=1 << 12) as hg:
+    with _hybrid(hyt, g, budget_bytes=2 * _push_budget(g), partition_vertices=1 << 12) as hg:
         d, st, ts = hg.sssp(s)
         assert np.array_equal(d, ref)
         decided = ts["resident_decisions"] + ts["filter_decisions"] + ts["compaction_decisions"] + \
