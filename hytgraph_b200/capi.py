@@ -212,6 +212,70 @@ class hyt_hybrid_stats(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+HYT_QUERY_SSSP = 0
+HYT_QUERY_PPR = 1
+
+
+class hyt_query(C.Structure):
+    _fields_ = [
+        ("graph", C.c_uint32),
+        ("kind", C.c_uint32),
+        ("source", C.c_uint32),
+        ("restart", C.c_float),
+        ("tolerance", C.c_float),
+        ("max_iterations", C.c_uint32),
+        ("out", C.c_void_p),
+    ]
+
+
+class hyt_query_result(C.Structure):
+    _fields_ = [
+        ("iterations", C.c_uint32),
+        ("converged", C.c_uint32),
+        ("residual", C.c_double),
+        ("edges_processed", C.c_uint64),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class hyt_batch_tuning(C.Structure):
+    _fields_ = [
+        ("delta_mult", C.c_uint32),
+        ("hub_degree", C.c_uint32),
+        ("ctas_per_sm", C.c_uint32),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class hyt_batch_options(C.Structure):
+    _fields_ = [
+        ("device", C.c_int),
+        ("state_budget_bytes", C.c_uint64),
+        ("tuning", hyt_batch_tuning),
+        ("flags", C.c_uint32),
+    ]
+
+
+class hyt_batch_stats(C.Structure):
+    _fields_ = [
+        ("device_ms", C.c_double),
+        ("supersteps", C.c_uint32),
+        ("waves", C.c_uint32),
+        ("graph_launches", C.c_uint32),
+        ("kernel_launches", C.c_uint32),
+        ("edges_processed", C.c_uint64),
+        ("algorithmic_bytes", C.c_uint64),
+        ("state_bytes", C.c_uint64),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 class HytError(RuntimeError):
     def __init__(self, code: int, message: str):
         super().__init__(f"[hyt status {code}] {message}")
@@ -242,6 +306,13 @@ _SIGNATURES = [
      [C.c_void_p, C.POINTER(hyt_pagerank_params), C.c_void_p, C.POINTER(hyt_run_stats), C.POINTER(hyt_hybrid_stats)]),
     ("hyt_hybrid_sssp", C.c_int,
      [C.c_void_p, C.POINTER(hyt_sssp_params), C.c_void_p, C.POINTER(hyt_run_stats), C.POINTER(hyt_hybrid_stats)]),
+    ("hyt_batch_create", C.c_int,
+     [C.POINTER(C.c_void_p), C.c_uint32, C.POINTER(hyt_batch_options), C.POINTER(C.c_void_p)]),
+    ("hyt_batch_destroy", C.c_int, [C.c_void_p]),
+    ("hyt_batch_run", C.c_int,
+     [C.c_void_p, C.POINTER(hyt_query), C.c_uint32, C.POINTER(hyt_query_result), C.POINTER(hyt_batch_stats)]),
+    ("hyt_batch_autotune", C.c_int, [C.c_void_p, C.POINTER(hyt_query), C.c_uint32, C.POINTER(hyt_batch_tuning)]),
+    ("hyt_batch_set_tuning", C.c_int, [C.c_void_p, C.POINTER(hyt_batch_tuning)]),
     ("hyt_rmat_generate", C.c_int, [C.POINTER(hyt_rmat_params), C.c_int, C.POINTER(hyt_csr_buffers)]),
     ("hyt_csr_buffers_free", C.c_int, [C.POINTER(hyt_csr_buffers)]),
     ("hyt_pick_sources", C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint32, C.c_void_p]),

@@ -1,0 +1,266 @@
+// Device building blocks of pull PageRank / personalized PageRank, shared
+// by the single-query solver (pagerank.cu), the partitioned out-of-HBM
+// solver and the batched multi-query engine (batch.cu): the per-row
+// finalisation, the batched contribution gather, and the two task kinds
+// (merge-path tile of short rows; chunk of a long row merged by its last
+// arriving warp).  Semantics are described at the top of pagerank.cu.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "common.cuh"
+#include "graph.cuh"
+
+namespace hyt {
+namespace prc {
+
+constexpr uint32_t kWarpRowDegree = 16;  // rows with more in-edges are summed by a whole warp
+
+struct PRHeader {
+    uint32_t iter;       // iterations completed
+    uint32_t done;
+    uint32_t converged;
+    uint32_t pad;
+    double last_residual;
+};
+
+// Device-resident arguments (a cached CUDA graph reads them every launch).
+struct PRArgs {
+    const uint64_t *in_off;
+    const uint32_t *in_src;
+    const uint32_t *out_deg;
+    const uint32_t *tile_start;
+    const LongRow *long_rows;
+    const uint2 *chunk_tasks;
+    const uint32_t *hot_vertex;  // [num_hot] vertices cached in shared memory
+    uint32_t num_hot;
+    uint32_t tile_cost;
+    float *rank[2];
+    float *contrib[2];
+    float2 *partial;
+    uint32_t *ticket;
+    PRHeader *hdr;
+    uint32_t *task_counter;  // [max_iter]
+    uint32_t *finished;      // [max_iter]
+    double *residual;        // [max_iter]
+    double *dangling;        // [max_iter + 1]
+    uint64_t num_tiles;
+    uint32_t num_chunks;
+    uint32_t V;
+    float damping;
+    float base;         // PR: (1-d)/n
+    float tolerance;
+    uint32_t max_iter;
+    uint32_t source;    // PPR
+    uint32_t personalized;
+    cudaGraphConditionalHandle cond;
+    uint32_t use_cond;
+};
+
+struct PRState {
+    // per-iteration scalars
+    float damping, base, teleport_scale;
+    float dshare;  // PR: d * dangling / n
+    float tele;    // PPR: (1-d) + d * dangling
+    uint32_t source;
+    bool personalized;
+};
+
+__device__ __forceinline__ void finalize_row(const PRArgs &a, const PRState &ps, uint32_t r, float sum,
+                                             const float *cur, float *nxt, float *cnxt, double &res, double &dang) {
+    float nx;
+    if (ps.personalized) {
+        nx = __fmul_rn(ps.damping, sum);
+        if (r == ps.source) nx = __fadd_rn(ps.tele, nx);
+    } else {
+        nx = __fadd_rn(ps.dshare, __fmul_rn(ps.damping, sum));
+    }
+    const float old = cur[r];
+    res += fabs(static_cast<double>(nx) - static_cast<double>(old));
+    nxt[r] = nx;
+    const uint32_t od = a.out_deg[r];
+    cnxt[r] = od ? __fdiv_rn(nx, static_cast<float>(od)) : 0.0f;
+    if (od == 0) dang += static_cast<double>(nx);
+}
+
+// Gathers the contributions of edges [lo, hi) of the in-source array.
+// Lane l of the warp takes edges lo + base + 32k + l (k < kBatch): each of
+// the kBatch id loads is one coalesced 128-byte access, and because the
+// sources of an in-row are sorted, the 32 addresses of each gather
+// instruction are ascending and neighbouring lanes often share an L2 sector
+// (dense for hub-heavy rows).  All kBatch gathers of a lane are issued
+// before any is consumed.  Edges past hi yield 0 and read a clamped address.
+constexpr int kBatch = 16;
+
+// kSmemHot: hot sources (tagged ids) read their contribution from the
+// CTA's shared-memory copy s_hot; otherwise from ccur[hot_vertex[slot]].
+template <bool kSmemHot, class Sink>
+__device__ __forceinline__ void gather_span(const uint32_t *in_src, const float *ccur, const float *s_hot,
+                                            const uint32_t *hot_vertex, uint64_t lo, uint64_t hi, uint64_t pol,
+                                            int lane, Sink &&sink) {
+    const uint32_t n = static_cast<uint32_t>(hi - lo);
+    const uint32_t *src = in_src + lo;
+    for (uint32_t base = 0; base < n; base += 32 * kBatch) {
+        uint32_t id[kBatch];
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k) {
+            const uint32_t i = base + 32 * k + lane;
+            id[k] = (i < n) ? dev::ld_stream(src + i) : 0u;
+        }
+        float v[kBatch];
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k) {
+            v[k] = 0.0f;
+            if (!(id[k] & kHotTag)) v[k] = dev::ld_keep(ccur + id[k], pol);
+        }
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k) {
+            if (id[k] & kHotTag) {
+                if constexpr (kSmemHot) {
+                    v[k] = s_hot[id[k] & ~kHotTag];
+                } else {
+                    v[k] = ccur[hot_vertex[id[k] & ~kHotTag]];
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k) {
+            const uint32_t i = base + 32 * k + lane;
+            if (i < n) sink(i, v[k]);
+        }
+    }
+}
+
+// Stop rule of iteration `it` (thread 0 of the last CTA, or the separate
+// end kernel): residual <= tolerance or the iteration cap.
+__device__ __forceinline__ void end_iteration(const PRArgs &a, uint32_t it) {
+    const double r = atomicAdd(&a.residual[it], 0.0);
+    const uint32_t n_it = it + 1;
+    const bool conv = r <= static_cast<double>(a.tolerance);
+    a.hdr->last_residual = r;
+    a.hdr->iter = n_it;
+    if (conv || n_it >= a.max_iter) {
+        a.hdr->done = 1;
+        a.hdr->converged = conv ? 1u : 0u;
+        if (a.use_cond) cudaGraphSetConditional(a.cond, 0);
+    }
+}
+
+
+// Solver scalars of an iteration whose dangling mass (sum of x over
+// out-degree-0 vertices) is dmass.
+__device__ __forceinline__ PRState make_state(const PRArgs &a, double dmass) {
+    PRState ps;
+    ps.damping = a.damping;
+    ps.source = a.source;
+    ps.personalized = a.personalized != 0;
+    ps.dshare = __fadd_rn(a.base, static_cast<float>(static_cast<double>(a.damping) * dmass / static_cast<double>(a.V)));
+    ps.tele = static_cast<float>((1.0 - static_cast<double>(a.damping)) + static_cast<double>(a.damping) * dmass);
+    return ps;
+}
+
+// Rank buffers of iteration `it` (Jacobi double buffering by parity).
+struct PRBuffers {
+    const float *cur, *ccur;
+    float *nxt, *cnxt;
+};
+
+__device__ __forceinline__ PRBuffers buffers(const PRArgs &a, uint32_t it) {
+    PRBuffers b;
+    b.cur = (it & 1) ? a.rank[1] : a.rank[0];
+    b.nxt = (it & 1) ? a.rank[0] : a.rank[1];
+    b.ccur = (it & 1) ? a.contrib[1] : a.contrib[0];
+    b.cnxt = (it & 1) ? a.contrib[0] : a.contrib[1];
+    return b;
+}
+
+// Chunk task `ci` (index into a.chunk_tasks): a kLongChunk-edge slice of a
+// long row.  The warp stores its compensated partial; the last arriving
+// warp of the row merges every partial in chunk order (lane j takes chunks
+// j, j+32, ...) and finalizes the row.  Returns the row's long-row index
+// when this warp finalized it (lane 0 holds res/dang), else ~0u.  Must be
+// called by all 32 lanes.
+template <bool kSmemHot>
+__device__ __forceinline__ uint32_t chunk_task(const PRArgs &a, const PRState &ps, const PRBuffers &b,
+                                               const uint32_t *in_src, const float *s_hot, uint64_t ci, uint64_t pol,
+                                               int lane, double &res, double &dang) {
+    const uint2 t = a.chunk_tasks[ci];
+    const LongRow L = a.long_rows[t.x];
+    const uint64_t rb = a.in_off[L.row], re = a.in_off[L.row + 1];
+    const uint64_t lo = rb + uint64_t(t.y) * kLongChunk;
+    const uint64_t hi = (lo + kLongChunk < re) ? lo + kLongChunk : re;
+    dev::CSum acc;
+    gather_span<kSmemHot>(in_src, b.ccur, s_hot, a.hot_vertex, lo, hi, pol, lane,
+                          [&](uint32_t, float v) { acc.add(v); });
+    acc = dev::warp_reduce(acc);
+    uint32_t last = 0;
+    if (lane == 0) {
+        a.partial[L.first_chunk + t.y] = make_float2(acc.s, acc.c);
+        __threadfence();
+        const uint32_t tk = atomicAdd(&a.ticket[t.x], 1u) + 1u;
+        last = (tk % L.num_chunks == 0) ? 1u : 0u;
+    }
+    last = __shfl_sync(0xffffffffu, last, 0);
+    if (!last) return ~0u;
+    __threadfence();
+    dev::CSum row;
+    for (uint32_t j = lane; j < L.num_chunks; j += 32) {
+        const float2 p = __ldcg(a.partial + L.first_chunk + j);
+        dev::CSum x;
+        x.s = p.x;
+        x.c = p.y;
+        row.merge(x);
+    }
+    row = dev::warp_reduce(row);
+    if (lane == 0) finalize_row(a, ps, L.row, row.value(), b.cur, b.nxt, b.cnxt, res, dang);
+    return t.x;
+}
+
+// Tile task k: rows [tile_start[k], tile_start[k+1]) minus a long last row
+// (chunked).  The tile's contributions are gathered into the warp's
+// shared-memory slice sv, then summed lane-per-row (in-degree <
+// kWarpRowDegree) or warp-per-row, in edge order.  Must be called by all 32
+// lanes.
+template <bool kSmemHot>
+__device__ __forceinline__ void tile_task(const PRArgs &a, const PRState &ps, const PRBuffers &b,
+                                          const uint32_t *in_src, const float *s_hot, float *sv, uint64_t k,
+                                          uint64_t pol, int lane, double &res, double &dang) {
+    const uint32_t r0 = a.tile_start[k];
+    const uint32_t r1 = a.tile_start[k + 1];
+    if (r0 == r1) return;
+    const uint64_t last_b = a.in_off[r1 - 1], last_e = a.in_off[r1];
+    const uint32_t rl = (last_e - last_b >= a.tile_cost) ? r1 - 1 : r1;  // long last row is chunked
+    const uint64_t e0 = a.in_off[r0];
+    const uint64_t e1 = (rl == r1) ? last_e : last_b;
+    gather_span<kSmemHot>(in_src, b.ccur, s_hot, a.hot_vertex, e0, e1, pol, lane,
+                          [&](uint32_t i, float v) { sv[i] = v; });
+    __syncwarp();
+    for (uint32_t rb = r0; rb < rl; rb += 32) {
+        const uint32_t r = rb + lane;
+        const bool active = r < rl;
+        const uint64_t lo = active ? a.in_off[r] : 0;
+        const uint64_t hi = active ? a.in_off[r + 1] : 0;
+        if (active && hi - lo < kWarpRowDegree) {
+            dev::CSum acc;
+            for (uint64_t x = lo; x < hi; ++x) acc.add(sv[x - e0]);
+            finalize_row(a, ps, r, acc.value(), b.cur, b.nxt, b.cnxt, res, dang);
+        }
+        uint32_t big = __ballot_sync(0xffffffffu, active && (hi - lo >= kWarpRowDegree));
+        while (big) {
+            const int src = __ffs(big) - 1;
+            big &= big - 1;
+            const uint64_t bb = __shfl_sync(0xffffffffu, lo, src);
+            const uint64_t ee = __shfl_sync(0xffffffffu, hi, src);
+            dev::CSum acc;
+            for (uint64_t x = bb + lane; x < ee; x += 32) acc.add(sv[x - e0]);
+            acc = dev::warp_reduce(acc);
+            if (lane == 0) finalize_row(a, ps, rb + src, acc.value(), b.cur, b.nxt, b.cnxt, res, dang);
+        }
+    }
+    __syncwarp();
+}
+
+}  // namespace prc
+}  // namespace hyt

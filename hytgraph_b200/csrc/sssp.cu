@@ -39,192 +39,21 @@
 #include "graph.cuh"
 #include "hybrid.cuh"
 #include "solvers.cuh"
-
-namespace cg = cooperative_groups;
+#include "sssp_core.cuh"
 
 namespace hyt {
 namespace {
 
-constexpr int kSSThreads = 256;
-constexpr uint32_t kHubDegree = 64;   // rows at least this long become warp tasks
-constexpr uint32_t kHubChunk = 512;   // edges per warp task
-constexpr uint32_t kNoDelta = 0xFFFFFFFFu;
-constexpr int kEdgeBatch = 4;  // 32-edge batches in flight per warp
-
-struct SSHeader {
-    uint32_t round;      // rounds completed
-    uint32_t done;
-    uint32_t converged;
-    uint32_t phase;      // far-pile generation
-    uint32_t pending;    // 1: this round starts by splitting the far pile
-    uint32_t threshold;  // near/far boundary T
-    uint32_t old_threshold;
-    uint32_t delta;
-    uint32_t qsize[2];   // near frontier sizes, by round parity
-    uint32_t fsize[2];   // far pile sizes, by phase parity
-    uint32_t hub_count;
-    uint32_t max_rounds;
-    unsigned long long relaxations;     // edges relaxed
-    unsigned long long frontier_total;  // frontier vertices expanded
-};
-
-struct SSArgs {
-    const uint64_t *row_off;
-    const uint32_t *cols;
-    const uint32_t *weights;
-    uint32_t *dist;
-    uint32_t *stamp;   // round in whose frontier a vertex sits
-    uint32_t *fstamp;  // far-pile generation that holds a vertex
-    uint32_t *queue[2];
-    uint32_t *far[2];
-    uint2 *hubs;
-    SSHeader *hdr;
-    uint32_t V;
-    uint32_t source;
-    uint32_t inf;
-    uint32_t use_cond;
-    cudaGraphConditionalHandle cond;
-    const EdgeLoc *loc;   // per-partition edge location (partitioned solves)
-    uint32_t part_shift;  // partition of vertex v = v >> part_shift
-};
-
-template <int WK>
-__device__ __forceinline__ uint32_t edge_weight(const uint32_t *w, uint64_t e) {
-    if constexpr (WK == HYT_WEIGHTS_NONE) {
-        return 1u;
-    } else {
-        return dev::ld_stream(w + e);
-    }
-}
-
-template <int WK>
-__device__ __forceinline__ uint32_t extend(uint32_t d, uint32_t w) {
-    if constexpr (WK == HYT_WEIGHTS_F32) {
-        return __float_as_uint(__fadd_rn(__uint_as_float(d), __uint_as_float(w)));
-    } else {
-        const uint64_t s = uint64_t(d) + w;
-        return s >= 0xFFFFFFFFull ? 0xFFFFFFFEu : static_cast<uint32_t>(s);
-    }
-}
-
-__device__ __forceinline__ void append(uint32_t *list, uint32_t *size, uint32_t v) {
-    cg::coalesced_group g = cg::coalesced_threads();
-    uint32_t base = 0;
-    if (g.thread_rank() == 0) base = atomicAdd(size, g.size());
-    base = g.shfl(base, 0);
-    list[base + g.thread_rank()] = v;
-}
-
-// Per-round view of the header, read once by every thread.
-struct RoundView {
-    uint32_t r, qn, threshold, next_stamp, far_stamp;
-    const uint32_t *q;
-    uint32_t *qnext, *qnext_size, *far, *far_size;
-};
-
-__device__ __forceinline__ RoundView round_view(const SSArgs &a) {
-    const SSHeader *h = a.hdr;
-    RoundView rv;
-    rv.r = *(volatile const uint32_t *)&h->round;
-    const uint32_t odd = rv.r & 1;
-    rv.qn = *(volatile const uint32_t *)(odd ? &h->qsize[1] : &h->qsize[0]);
-    rv.q = odd ? a.queue[1] : a.queue[0];
-    rv.qnext = odd ? a.queue[0] : a.queue[1];
-    rv.qnext_size = odd ? &a.hdr->qsize[0] : &a.hdr->qsize[1];
-    rv.threshold = *(volatile const uint32_t *)&h->threshold;
-    rv.next_stamp = rv.r + 1;
-    // During a split round the far pile of the next phase is already active.
-    const uint32_t p = *(volatile const uint32_t *)&h->phase + *(volatile const uint32_t *)&h->pending;
-    rv.far = (p & 1) ? a.far[1] : a.far[0];
-    rv.far_size = (p & 1) ? &a.hdr->fsize[1] : &a.hdr->fsize[0];
-    rv.far_stamp = p + 1;
-    return rv;
-}
-
-// Appends each lane's entries vals[k] with bit k set in `mask` to a list,
-// with one atomic per warp.  Must be called by all 32 lanes.
-template <int K>
-__device__ __forceinline__ void warp_append(uint32_t *list, uint32_t *size, const uint32_t (&vals)[K], uint32_t mask,
-                                            int lane) {
-    const uint32_t cnt = __popc(mask);
-    uint32_t incl = cnt;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += y;
-    }
-    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-    if (total == 0) return;
-    uint32_t base = 0;
-    if (lane == 31) base = atomicAdd(size, total);
-    base = __shfl_sync(0xffffffffu, base, 31) + incl - cnt;
-#pragma unroll
-    for (int k = 0; k < K; ++k)
-        if ((mask >> k) & 1u) list[base + __popc(mask & ((1u << k) - 1u))] = vals[k];
-}
-
-// Relaxes K candidate edges per lane with all atomics of a phase in flight
-// together: atomicMin on every improving label, then the stamp exchange of
-// every success, then one warp-aggregated append per list.  nd[k] >= du[k]
-// (including padding lanes, whose nd is the infinity label) is a no-op.
-// Must be called by all 32 lanes.
-template <int K>
-__device__ __forceinline__ void relax_batch(const SSArgs &a, const RoundView &rv, const uint32_t (&u)[K],
-                                            const uint32_t (&nd)[K], const uint32_t (&du)[K], int lane,
-                                            unsigned long long &improved) {
-    uint32_t old[K];
-#pragma unroll
-    for (int k = 0; k < K; ++k) old[k] = (nd[k] < du[k]) ? atomicMin(a.dist + u[k], nd[k]) : 0u;
-    uint32_t st[K];
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-        st[k] = 0;
-        if (nd[k] < old[k])
-            st[k] = (nd[k] < rv.threshold) ? atomicExch(a.stamp + u[k], rv.next_stamp)
-                                           : atomicExch(a.fstamp + u[k], rv.far_stamp);
-    }
-    uint32_t nmask = 0, fmask = 0;
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-        if (nd[k] < old[k]) {
-            ++improved;
-            if (nd[k] < rv.threshold) {
-                if (st[k] != rv.next_stamp) nmask |= 1u << k;
-            } else if (st[k] != rv.far_stamp) {
-                fmask |= 1u << k;
-            }
-        }
-    }
-    warp_append<K>(rv.qnext, rv.qnext_size, u, nmask, lane);
-    warp_append<K>(rv.far, rv.far_size, u, fmask, lane);
-}
+using namespace ssc;
 
 // Splits the far pile at the start of a round whose near frontier is empty.
 __global__ void __launch_bounds__(kSSThreads) sssp_split_kernel(const SSArgs *__restrict__ args) {
     const SSArgs a = *args;
     const SSHeader *h = a.hdr;
     if (*(volatile const uint32_t *)&h->done || !*(volatile const uint32_t *)&h->pending) return;
-    const uint32_t r = h->round, p = h->phase;
-    const uint32_t lo = h->old_threshold, hi = h->threshold;
-    const uint32_t n = (p & 1) ? h->fsize[1] : h->fsize[0];
-    const uint32_t *src = (p & 1) ? a.far[1] : a.far[0];
-    uint32_t *dst = (p & 1) ? a.far[0] : a.far[1];
-    uint32_t *dst_size = (p & 1) ? &a.hdr->fsize[0] : &a.hdr->fsize[1];
-    uint32_t *near = (r & 1) ? a.queue[1] : a.queue[0];
-    uint32_t *near_size = (r & 1) ? &a.hdr->qsize[1] : &a.hdr->qsize[0];
+    const uint32_t n = (h->phase & 1) ? h->fsize[1] : h->fsize[0];
     const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        const uint32_t v = src[i];
-        const uint32_t d = __ldcg(a.dist + v);
-        if (d < lo) continue;  // settled in an earlier phase
-        if (d < hi) {
-            a.stamp[v] = r;
-            append(near, near_size, v);
-        } else {
-            a.fstamp[v] = p + 2;
-            append(dst, dst_size, v);
-        }
-    }
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) split_entry(a, i);
 }
 
 // HYB: the edges of a vertex's partition are reached through a.loc
@@ -239,79 +68,12 @@ __global__ void __launch_bounds__(kSSThreads) sssp_expand_kernel(const SSArgs *_
     const uint32_t gwarp = (blockIdx.x * kSSThreads + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * kSSThreads) >> 5;
     unsigned long long relaxed = 0, improved = 0;
-
-    for (uint32_t w = gwarp; uint64_t(w) * 32 < rv.qn; w += nwarps) {
-        const uint32_t i = w * 32 + lane;
-        uint32_t deg = 0, d = a.inf;
-        uint64_t off = 0;
-        const uint32_t *vc = a.cols, *vw = a.weights;  // edge arrays of this lane's vertex
-        if (i < rv.qn) {
-            const uint32_t v = rv.q[i];
-            off = a.row_off[v];
-            uint64_t full = a.row_off[v + 1] - off;
-            if constexpr (HYB) {
-                const EdgeLoc L = a.loc[v >> a.part_shift];
-                vc = L.cols;
-                vw = L.weights;
-                if (L.mode != kLocDirect || v < L.vlo || v >= L.vhi) full = 0;
-            }
-            d = __ldcg(a.dist + v);
-            relaxed += full;
-            if (full >= kHubDegree) {
-                // long rows: kHubChunk-edge warp tasks for the hub kernel
-                const uint32_t nch = static_cast<uint32_t>((full + kHubChunk - 1) / kHubChunk);
-                const uint32_t base = atomicAdd(&a.hdr->hub_count, nch);
-                for (uint32_t c = 0; c < nch; ++c) a.hubs[base + c] = make_uint2(v, c);
-            } else {
-                deg = static_cast<uint32_t>(full);
-            }
-        }
-        // inclusive prefix of the 32 short degrees
-        uint32_t incl = deg;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += y;
-        }
-        const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-        // kEdgeBatch batches of 32 edges per pass: all column/weight loads,
-        // then all label loads, then all atomics are in flight together.
-        for (uint32_t base = 0; base < total; base += 32 * kEdgeBatch) {
-            uint32_t u[kEdgeBatch], nd[kEdgeBatch], du[kEdgeBatch];
-#pragma unroll
-            for (int k = 0; k < kEdgeBatch; ++k) {
-                const uint32_t j = base + 32 * k + lane;
-                // owner = first lane whose inclusive prefix exceeds j
-                uint32_t lo = 0;
-#pragma unroll
-                for (uint32_t step = 16; step > 0; step >>= 1) {
-                    const uint32_t probe = __shfl_sync(0xffffffffu, incl, lo + step - 1);
-                    if (probe <= j) lo += step;
-                }
-                const uint32_t o_incl = __shfl_sync(0xffffffffu, incl, lo);
-                const uint32_t o_deg = __shfl_sync(0xffffffffu, deg, lo);
-                const uint64_t o_off = __shfl_sync(0xffffffffu, off, lo);
-                const uint32_t o_d = __shfl_sync(0xffffffffu, d, lo);
-                const uint32_t *oc = a.cols, *ow = a.weights;
-                if constexpr (HYB) {
-                    oc = reinterpret_cast<const uint32_t *>(
-                        __shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(vc), lo));
-                    ow = reinterpret_cast<const uint32_t *>(
-                        __shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(vw), lo));
-                }
-                u[k] = 0;
-                nd[k] = a.inf;
-                if (j < total) {
-                    const uint64_t e = o_off + (j - (o_incl - o_deg));
-                    u[k] = dev::ld_stream(oc + e);
-                    nd[k] = extend<WK>(o_d, edge_weight<WK>(ow, e));
-                }
-            }
-#pragma unroll
-            for (int k = 0; k < kEdgeBatch; ++k) du[k] = __ldcg(a.dist + u[k]);
-            relax_batch<kEdgeBatch>(a, rv, u, nd, du, lane, improved);
-        }
-    }
+    auto hub = [&](uint32_t v, uint32_t nch) {
+        const uint32_t base = atomicAdd(&a.hdr->hub_count, nch);
+        for (uint32_t c = 0; c < nch; ++c) a.hubs[base + c] = make_uint2(v, c);
+    };
+    for (uint32_t w = gwarp; uint64_t(w) * 32 < rv.qn; w += nwarps)
+        expand_warp<WK, HYB>(a, rv, w * 32, lane, kHubDegree, relaxed, improved, hub);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) relaxed += __shfl_xor_sync(0xffffffffu, relaxed, o);
     if (lane == 0 && relaxed) atomicAdd(&a.hdr->relaxations, relaxed);
@@ -330,78 +92,26 @@ __global__ void __launch_bounds__(kSSThreads) sssp_hub_kernel(const SSArgs *__re
     unsigned long long improved = 0;
     for (uint32_t t = gwarp; t < n; t += nwarps) {
         const uint2 h = a.hubs[t];
-        const uint64_t rb = a.row_off[h.x], re = a.row_off[h.x + 1];
-        const uint64_t b = rb + uint64_t(h.y) * kHubChunk;
-        const uint32_t len = static_cast<uint32_t>(((b + kHubChunk < re) ? b + kHubChunk : re) - b);
-        const uint32_t d = __ldcg(a.dist + h.x);
         const uint32_t *hc = a.cols, *hw = a.weights;
         if constexpr (HYB) {
             const EdgeLoc L = a.loc[h.x >> a.part_shift];
             hc = L.cols;
             hw = L.weights;
         }
-        for (uint32_t base = 0; base < len; base += 32 * kEdgeBatch) {
-            uint32_t u[kEdgeBatch], nd[kEdgeBatch], du[kEdgeBatch];
-#pragma unroll
-            for (int k = 0; k < kEdgeBatch; ++k) {
-                const uint32_t j = base + 32 * k + lane;
-                u[k] = 0;
-                nd[k] = a.inf;
-                if (j < len) {
-                    u[k] = dev::ld_stream(hc + b + j);
-                    nd[k] = extend<WK>(d, edge_weight<WK>(hw, b + j));
-                }
-            }
-#pragma unroll
-            for (int k = 0; k < kEdgeBatch; ++k) du[k] = __ldcg(a.dist + u[k]);
-            relax_batch<kEdgeBatch>(a, rv, u, nd, du, lane, improved);
-        }
+        hub_chunk<WK>(a, rv, hc, hw, h.x, h.y, lane, improved);
     }
 }
 
 __global__ void sssp_round_end_kernel(const SSArgs *__restrict__ args) {
     const SSArgs a = *args;
-    SSHeader *h = a.hdr;
-    if (h->done) return;
-    const uint32_t r = h->round;
-    const uint32_t n_next = h->qsize[(r + 1) & 1];
-    h->frontier_total += h->qsize[r & 1];
-    h->qsize[r & 1] = 0;
-    h->hub_count = 0;
-    h->round = r + 1;
-    if (h->pending) {  // the split of this round consumed the old far pile
-        h->fsize[h->phase & 1] = 0;
-        h->phase += 1;
-        h->pending = 0;
-    }
-    bool finish = false, conv = false;
-    if (n_next == 0) {
-        if (h->fsize[h->phase & 1] == 0) {
-            finish = conv = true;
-        } else {
-            h->pending = 1;
-            h->old_threshold = h->threshold;
-            const uint64_t t = uint64_t(h->threshold) + h->delta;
-            h->threshold = t >= 0xFFFFFFFFull ? 0xFFFFFFFFu : static_cast<uint32_t>(t);
-        }
-    }
-    if (!finish && r + 1 >= h->max_rounds) finish = true;
-    if (finish) {
-        h->done = 1;
-        h->converged = conv ? 1u : 0u;
-        if (a.use_cond) cudaGraphSetConditional(a.cond, 0);
-    }
+    if (a.hdr->done) return;
+    if (round_end(a.hdr) && a.use_cond) cudaGraphSetConditional(a.cond, 0);
 }
 
 __global__ void sssp_init_kernel(const SSArgs *__restrict__ args) {
     const SSArgs a = *args;
     const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < a.V; v += stride) {
-        const bool s = (v == a.source);
-        a.dist[v] = s ? 0u : a.inf;
-        a.stamp[v] = s ? 0u : 0xFFFFFFFFu;
-        a.fstamp[v] = 0xFFFFFFFFu;
-    }
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < a.V; v += stride) init_vertex(a, v);
     if (blockIdx.x == 0 && threadIdx.x == 0) a.queue[0][0] = a.source;
 }
 

@@ -353,3 +353,85 @@ class HybridGraph:
             self.close()
         except Exception:
             pass
+
+
+class Batch:
+    """Many SSSP / personalized-PageRank queries over many resident graphs,
+    run together (hyt_batch handle): one CUDA-graph launch per batch.
+
+    queries: sequence of (graph_index, kind, source) or dicts with keys
+    graph, kind ("sssp" | "ppr" or HYT_QUERY_*), source, and optionally
+    restart, tolerance, max_iterations, out (an array to receive the result;
+    by default a numpy array is allocated per query)."""
+
+    def __init__(self, graphs, device: int = 0, state_budget_bytes: int = 0, delta_mult: int = 0,
+                 hub_degree: int = 0, ctas_per_sm: int = 0, flags: int = 0):
+        self._graphs = list(graphs)  # keep the graph handles alive
+        arr = (C.c_void_p * len(self._graphs))(*[g.handle.value for g in self._graphs])
+        opts = capi.hyt_batch_options(device, state_budget_bytes,
+                                      capi.hyt_batch_tuning(delta_mult, hub_degree, ctas_per_sm), flags)
+        h = C.c_void_p()
+        check(lib.hyt_batch_create(arr, len(self._graphs), C.byref(opts), C.byref(h)))
+        self._h = h
+
+    @property
+    def handle(self) -> C.c_void_p:
+        if not self._h:
+            raise ValueError("batch is closed")
+        return self._h
+
+    def _pack(self, queries, with_out: bool = True):
+        n = len(queries)
+        arr = (capi.hyt_query * n)()
+        outs = []
+        for i, q in enumerate(queries):
+            if not isinstance(q, dict):
+                q = {"graph": q[0], "kind": q[1], "source": q[2]}
+            kind = q["kind"]
+            if isinstance(kind, str):
+                kind = capi.HYT_QUERY_SSSP if kind == "sssp" else capi.HYT_QUERY_PPR
+            gi = q["graph"]
+            g = self._graphs[gi] if 0 <= gi < len(self._graphs) else None  # the library rejects bad indices
+            out = q.get("out")
+            if out is None and with_out and g is not None:
+                out = np.empty(g.num_vertices, np.uint32 if kind == capi.HYT_QUERY_SSSP else np.float32)
+            outs.append(out)
+            arr[i] = capi.hyt_query(q["graph"], kind, q["source"], q.get("restart", 0.0), q.get("tolerance", 0.0),
+                                    q.get("max_iterations", 0), _ptr(out) if out is not None else None)
+        return arr, outs
+
+    def run(self, queries):
+        """Returns (outputs, per-query result dicts, batch stats dict)."""
+        arr, outs = self._pack(queries)
+        n = len(queries)
+        res = (capi.hyt_query_result * max(n, 1))()
+        st = capi.hyt_batch_stats()
+        check(lib.hyt_batch_run(self.handle, arr, n, res, C.byref(st)))
+        return outs, [res[i].as_dict() for i in range(n)], st.as_dict()
+
+    def autotune(self, queries) -> dict:
+        arr, _ = self._pack(queries, with_out=False)
+        t = capi.hyt_batch_tuning()
+        check(lib.hyt_batch_autotune(self.handle, arr, len(queries), C.byref(t)))
+        return t.as_dict()
+
+    def set_tuning(self, delta_mult: int = 0, hub_degree: int = 0, ctas_per_sm: int = 0) -> None:
+        t = capi.hyt_batch_tuning(delta_mult, hub_degree, ctas_per_sm)
+        check(lib.hyt_batch_set_tuning(self.handle, C.byref(t)))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            check(lib.hyt_batch_destroy(self._h))
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -302,6 +302,80 @@ int hyt_hybrid_sssp(hyt_hybrid *hybrid, const hyt_sssp_params *params, uint32_t 
                     hyt_run_stats *stats, hyt_hybrid_stats *transfer);
 
 /* ------------------------------------------------------------------ */
+/* Batched queries: many SSSP / personalized-PageRank queries over many */
+/* resident graphs in one CUDA-graph launch                             */
+/* ------------------------------------------------------------------ */
+
+enum hyt_query_kind {
+    HYT_QUERY_SSSP = 0,
+    HYT_QUERY_PPR = 1
+};
+
+typedef struct hyt_query {
+    uint32_t graph;           /* index into the batch's graph list */
+    uint32_t kind;            /* HYT_QUERY_* */
+    uint32_t source;
+    float restart;            /* PPR: (0, 1]; 0 = 0.15 */
+    float tolerance;          /* PPR: L1 stop; 0 = 1e-6 */
+    uint32_t max_iterations;  /* PPR: 0 = 100; SSSP: round cap, 0 = none */
+    void *out;                /* SSSP: uint32 dist[V]; PPR: float ranks[V];
+                                 host or device memory, or NULL */
+} hyt_query;
+
+typedef struct hyt_query_result {
+    uint32_t iterations;      /* PPR iterations / SSSP rounds */
+    uint32_t converged;
+    double residual;          /* PPR: L1 change of the last iteration */
+    uint64_t edges_processed; /* PPR: iterations * E; SSSP: relaxations */
+} hyt_query_result;
+
+/* Knobs the autotuner chooses (0 = default). */
+typedef struct hyt_batch_tuning {
+    uint32_t delta_mult;   /* SSSP bucket width = delta_mult x mean edge
+                              weight of the query's graph; 0 = one bucket */
+    uint32_t hub_degree;   /* SSSP rows >= this many edges are split into
+                              512-edge warp tasks (default 64) */
+    uint32_t ctas_per_sm;  /* persistent work grid (0 = occupancy) */
+} hyt_batch_tuning;
+
+typedef struct hyt_batch_options {
+    int device;
+    uint64_t state_budget_bytes;  /* device bytes for per-query state
+                                     (0 = 16 GiB); larger batches run in
+                                     waves that fit */
+    hyt_batch_tuning tuning;
+    uint32_t flags;               /* HYT_RUN_NO_GRAPH: host-driven supersteps */
+} hyt_batch_options;
+
+typedef struct hyt_batch_stats {
+    double device_ms;          /* device time of the whole batch */
+    uint32_t supersteps;
+    uint32_t waves;            /* admission waves (1 when all fit) */
+    uint32_t graph_launches;   /* CUDA-graph launches */
+    uint32_t kernel_launches;  /* kernels executed (graph nodes included) */
+    uint64_t edges_processed;  /* sum over queries */
+    uint64_t algorithmic_bytes;
+    uint64_t state_bytes;      /* peak per-query state held */
+} hyt_batch_stats;
+
+typedef struct hyt_batch hyt_batch;
+
+/* graphs: handles built with HYT_GRAPH_ALL (borrowed; keep them alive). */
+int hyt_batch_create(hyt_graph *const *graphs, uint32_t num_graphs, const hyt_batch_options *options,
+                     hyt_batch **out);
+int hyt_batch_destroy(hyt_batch *batch);
+/* Runs every query; results[i] belongs to queries[i].  A query's result is
+ * the same whatever else is in the batch (SSSP: identical to hyt_sssp;
+ * PPR: identical across batches, within L1 1e-6 of hyt_ppr). */
+int hyt_batch_run(hyt_batch *batch, const hyt_query *queries, uint32_t num_queries,
+                  hyt_query_result *results, hyt_batch_stats *stats);
+/* Times the batch on a sample of `queries` under a grid of tunings and
+ * keeps the fastest for later runs; *chosen receives it. */
+int hyt_batch_autotune(hyt_batch *batch, const hyt_query *queries, uint32_t num_queries,
+                       hyt_batch_tuning *chosen);
+int hyt_batch_set_tuning(hyt_batch *batch, const hyt_batch_tuning *tuning);
+
+/* ------------------------------------------------------------------ */
 /* Seeded R-MAT generator (deterministic; same bytes on host and GPU)   */
 /* ------------------------------------------------------------------ */
 
