@@ -48,9 +48,12 @@ def parse_args():
     ap.add_argument("--seed", type=int, default=20241203)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["inhbm", "hybrid"], default="inhbm",
+    ap.add_argument("--workload", choices=["inhbm", "hybrid", "batch"], default="inhbm",
                     help="inhbm: graph resident in HBM (default); hybrid: edges in pinned host memory under a "
-                         "device budget (defaults to R-MAT scale 27, edge factor 32, 8 GiB)")
+                         "device budget (defaults to R-MAT scale 27, edge factor 32, 8 GiB); batch: 64 graphs of "
+                         "scales 12-20, 512 SSSP/PPR queries in one CUDA-graph launch")
+    ap.add_argument("--graphs", type=int, default=64)
+    ap.add_argument("--queries", type=int, default=512)
     ap.add_argument("--budget-gib", type=float, default=8.0)
     ap.add_argument("--partition-vertices", type=int, default=1 << 20)
     a = ap.parse_args()
@@ -346,6 +349,163 @@ def run_hybrid(args, rank, world, pg):
         raise SystemExit(f"hybrid results differ from the in-HBM solve: sssp_equal={sssp_equal} pr_l1={pr_l1}")
 
 
+def batch_workload(hyt, num_graphs, num_queries, seed, smin=12, smax=20, efmin=8, efmax=32):
+    """Seeded uneven batch: graph scales U{smin..smax}, edge factors
+    U{efmin..efmax}; 1-16 sources per graph adjusted to num_queries in
+    total; each query SSSP with probability 0.6, else PPR (restart 0.15,
+    tol 1e-6).  Returns (graph specs, queries)."""
+    rng = np.random.default_rng(seed)
+    specs = [(int(rng.integers(smin, smax + 1)), int(rng.integers(efmin, efmax + 1)), int(seed + 1000 + i))
+             for i in range(num_graphs)]
+    counts = rng.integers(1, 17, num_graphs)
+    while counts.sum() != num_queries:
+        i = int(rng.integers(0, num_graphs))
+        if counts.sum() > num_queries and counts[i] > 1:
+            counts[i] -= 1
+        elif counts.sum() < num_queries and counts[i] < 16:
+            counts[i] += 1
+    return specs, counts, rng
+
+
+def run_batch_workload(args, rank, world, pg):
+    """Batched uneven queries: every query of the batch in one
+    hyt_batch_run (one CUDA-graph launch), against the same queries solved
+    one at a time with hyt_sssp / hyt_ppr on the same graphs."""
+    import torch
+    import hytgraph_b200 as hyt
+    from hytgraph_b200 import capi
+
+    specs, counts, rng = batch_workload(hyt, args.graphs, args.queries, args.seed)
+    graphs, queries = [], []
+    for gi, (sc, ef, gseed) in enumerate(specs):
+        d = hyt.rmat(sc, ef, gseed, device=True)
+        off = np.empty(d.num_vertices + 1, np.uint64)
+        capi.copy(off.ctypes.data, C.cast(d.buffers.row_offsets, C.c_void_p).value, off.nbytes)
+        graphs.append(hyt.Graph(d))
+        d.free()
+        for s in hyt.pick_sources(off, gseed, int(counts[gi])):
+            kind = "sssp" if rng.random() < 0.6 else "ppr"
+            queries.append({"graph": gi, "kind": kind, "source": int(s), "restart": 0.15, "tolerance": 1e-6})
+    E_of = [g.num_edges for g in graphs]
+    V_of = [g.num_vertices for g in graphs]
+    # device outputs (the bench line); pinned host outputs (e2e)
+    dev_out = [torch.empty(V_of[q["graph"]], dtype=torch.int32 if q["kind"] == "sssp" else torch.float32,
+                           device="cuda") for q in queries]
+    host_out = [torch.empty(V_of[q["graph"]], dtype=torch.int32 if q["kind"] == "sssp" else torch.float32,
+                            pin_memory=True) for q in queries]
+    qd = [dict(q, out=o) for q, o in zip(queries, dev_out)]
+    qh = [dict(q, out=o) for q, o in zip(queries, host_out)]
+    torch.cuda.synchronize()
+    with hyt.Batch(graphs) as b:
+        t0 = time.perf_counter()
+        tuning = b.autotune(queries)
+        tune_s = time.perf_counter() - t0
+        for _ in range(args.warmup):
+            b.run(qd)
+        clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+        clocks.start()
+        barrier(pg)
+        ms_list, res, st = [], None, None
+        for _ in range(args.steps):
+            _, res, st = b.run(qd)
+            ms_list.append(st["device_ms"])
+        clk = clocks.stop()
+        ms = max_over_ranks(pg, sum(ms_list) / len(ms_list))
+        # e2e: results land in pinned host memory inside the timed call
+        b.run(qh)
+        t0 = time.perf_counter()
+        _, _, st_h = b.run(qh)
+        e2e_wall = time.perf_counter() - t0
+    traversed = sum(E_of[q["graph"]] * (r["iterations"] if q["kind"] == "ppr" else 1) for q, r in zip(queries, res))
+    n_q = len(queries)
+    # one at a time: the same queries through hyt_sssp / hyt_ppr, outputs on the device
+    for q, o in zip(queries[:8], dev_out[:8]):
+        g = graphs[q["graph"]]
+        (g.sssp(q["source"], out=o) if q["kind"] == "sssp" else g.ppr(q["source"], out=o))
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for q, o in zip(queries, dev_out):
+        g = graphs[q["graph"]]
+        (g.sssp(q["source"], out=o) if q["kind"] == "sssp" else g.ppr(q["source"], out=o))
+    e1.record()
+    e1.synchronize()
+    single_ms = e0.elapsed_time(e1)
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu = batch_cpu_sample(hyt, specs, queries)
+    if rank == 0:
+        gteps = traversed * world / (ms / 1e3) / 1e9
+        line = {"metric": METRIC, "value": gteps, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32 (PPR) / u32 (SSSP)", "data": "synthetic",
+                "config": {"workload": f"batched uneven queries: {len(graphs)} R-MAT graphs, scales U{{12..20}}, "
+                                       f"edge factors U{{8..32}}, {n_q} queries (60% SSSP / 40% PPR restart 0.15 "
+                                       f"tol 1e-6) in one hyt_batch_run",
+                           "graphs": len(graphs), "queries": n_q,
+                           "sssp_queries": sum(q["kind"] == "sssp" for q in queries),
+                           "total_edges": int(sum(E_of)), "total_vertices": int(sum(V_of)), "seed": args.seed,
+                           "scales": [s for s, _, _ in specs], "edge_factors": [e for _, e, _ in specs]},
+                "queries_per_s": n_q * world / (ms / 1e3),
+                "one_at_a_time": {"ms": single_ms, "queries_per_s": n_q / (single_ms / 1e3),
+                                  "speedup_of_batch": single_ms / ms},
+                "batch": {"supersteps": st["supersteps"], "kernel_launches": st["kernel_launches"],
+                          "graph_launches": st["graph_launches"], "state_bytes": st["state_bytes"],
+                          "algorithmic_bytes": st["algorithmic_bytes"],
+                          "achieved_gbs": st["algorithmic_bytes"] / (ms / 1e3) / 1e9,
+                          "tuning": tuning, "autotune_s": tune_s},
+                "e2e": {"value": traversed / e2e_wall / 1e9, "unit": UNIT, "queries_per_s": n_q / e2e_wall,
+                        "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": int(sum(V_of[q["graph"]] * 4 for q in queries)),
+                        "ms_per_step": e2e_wall * 1e3},
+                "roofline": {"bound": "hbm", "achieved": st["algorithmic_bytes"] / (ms / 1e3) / 1e9,
+                             "peak": load_peaks()[0], "unit": "GB/s",
+                             "frac": st["algorithmic_bytes"] / (ms / 1e3) / 1e9 / load_peaks()[0],
+                             "traffic": None, "peak_kind": load_peaks()[1]},
+                "cpu_baseline": cpu, "clocks": clk, "gpu_launches": st["kernel_launches"]}
+        print(json.dumps(line), flush=True)
+    for g in graphs:
+        g.close()
+
+
+def batch_cpu_sample(hyt, specs, queries):
+    """The reference's sssp_cpu on the first SSSP query of the two smallest
+    graphs and the FP64 PPR restatement on the first PPR query of the same
+    graphs (the reference has no PPR); queries/s extrapolated from the
+    sample's mean time per query."""
+    from oracle.bindings import Oracle, Reference
+
+    order = sorted(range(len(specs)), key=lambda i: (specs[i][0], specs[i][1]))[:2]
+    o = Oracle()
+    ref = Reference() if Reference.available() else None
+    t, n, kinds = 0.0, 0, set()
+    for gi in order:
+        sc, ef, gseed = specs[gi]
+        c = hyt.rmat(sc, ef, gseed)
+        for kind in ("sssp", "ppr"):
+            q = next((q for q in queries if q["graph"] == gi and q["kind"] == kind), None)
+            if q is None:
+                continue
+            t0 = time.perf_counter()
+            if kind == "sssp" and ref is not None:
+                ref.sssp_cpu(c.row_offsets, c.column_indices, c.weights.astype(np.float32), q["source"])
+                kinds.add("reference")
+            elif kind == "sssp":
+                o.sssp(c.row_offsets, c.column_indices, c.weights.astype(np.float32), q["source"])
+                kinds.add("port")
+            else:
+                o.ppr_f64(c.row_offsets, c.column_indices, q["source"])
+                kinds.add("port")
+            t += time.perf_counter() - t0
+            n += 1
+    if n == 0:
+        return None
+    return {"value": n / t, "unit": "queries/s", "cores": 1,
+            "kind": "reference" if kinds == {"reference"} else "port",
+            "sample": f"{n} queries on the two smallest graphs of the batch (reference sssp_cpu for SSSP, FP64 "
+                      f"PPR restatement for PPR), {t:.2f} s"}
+
+
 def workload_config(args, V, E):
     return {"workload": f"in-HBM R-MAT scale {args.scale} edge factor {args.edge_factor}: PageRank to L1<=1e-6 "
                         f"+ SSSP from {args.sources} seeded sources",
@@ -368,6 +528,11 @@ def main():
 
     if args.workload == "hybrid":
         run_hybrid(args, rank, world, pg)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
+    if args.workload == "batch":
+        run_batch_workload(args, rank, world, pg)
         if pg is not None:
             pg.destroy_process_group()
         return
