@@ -48,10 +48,13 @@ def parse_args():
     ap.add_argument("--seed", type=int, default=20241203)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["inhbm", "hybrid", "batch"], default="inhbm",
+    ap.add_argument("--workload", choices=["inhbm", "hybrid", "batch", "serve"], default="inhbm",
                     help="inhbm: graph resident in HBM (default); hybrid: edges in pinned host memory under a "
                          "device budget (defaults to R-MAT scale 27, edge factor 32, 8 GiB); batch: 64 graphs of "
                          "scales 12-20, 512 SSSP/PPR queries in one CUDA-graph launch")
+    ap.add_argument("--requests", type=int, default=20000)
+    ap.add_argument("--rates", type=str, default="200,500,1000,2000,5000")
+    ap.add_argument("--rate-seconds", type=float, default=8.0, help="serve: cap on each rate point's duration")
     ap.add_argument("--graphs", type=int, default=64)
     ap.add_argument("--queries", type=int, default=512)
     ap.add_argument("--budget-gib", type=float, default=8.0)
@@ -506,6 +509,129 @@ def batch_cpu_sample(hyt, specs, queries):
                       f"PPR restatement for PPR), {t:.2f} s"}
 
 
+def run_serve_workload(args, rank, world, pg):
+    """Served stream: 8 resident R-MAT graphs (scales 16-20, 22-24, edge
+    factor 16); requests 70% SSSP / 30% PPR (restart 0.15, tol 1e-6) on a
+    uniformly chosen graph from a source uniform over out-degree > 0;
+    admission by a 16 GiB per-query-state budget.  Measures: capacity
+    (every request submitted at once), open-loop Poisson sweeps (latency
+    p50 / p99 and achieved queries/s per offered rate), and the same
+    requests solved one at a time with hyt_sssp / hyt_ppr."""
+    import threading
+    import torch
+    import hytgraph_b200 as hyt
+    from hytgraph_b200 import capi
+
+    scales = [16, 17, 18, 19, 20, 22, 23, 24]
+    graphs, pools = [], []
+    for sc in scales:
+        d = hyt.rmat(sc, 16, args.seed + sc, device=True)
+        off = np.empty(d.num_vertices + 1, np.uint64)
+        capi.copy(off.ctypes.data, C.cast(d.buffers.row_offsets, C.c_void_p).value, off.nbytes)
+        graphs.append(hyt.Graph(d))
+        d.free()
+        pools.append(hyt.pick_sources(off, args.seed + 7 * sc, 4096))
+    V_of = [g.num_vertices for g in graphs]
+    E_of = [g.num_edges for g in graphs]
+
+    def make_requests(n, seed):
+        r = np.random.default_rng(seed)
+        gi = r.integers(0, len(graphs), n)
+        kind = np.where(r.random(n) < 0.7, "sssp", "ppr")
+        src = [int(pools[g][r.integers(0, len(pools[g]))]) for g in gi]
+        return [(int(g), str(k), s) for g, k, s in zip(gi, kind, src)]
+
+    # results land in a ring of 32 device buffers per (graph, kind): the
+    # result copy stays on the path without one buffer per request
+    ring = {(g, k): [torch.empty(V_of[g], dtype=torch.int32 if k == "sssp" else torch.float32, device="cuda")
+                     for _ in range(32)] for g in range(len(graphs)) for k in ("sssp", "ppr")}
+    ring_pos = {key: 0 for key in ring}
+
+    def take_out(g, k):
+        i = ring_pos[(g, k)]
+        ring_pos[(g, k)] = (i + 1) % 32
+        return ring[(g, k)][i]
+
+    def serve(srv, reqs, rate):
+        """Submits reqs open-loop at `rate` (None = all at once); returns
+        (latencies ms, seconds from the first arrival to the last completion)."""
+        lat, meta = [], {}
+        gaps = np.random.default_rng(len(reqs)).exponential(1.0 / rate, len(reqs)) if rate else np.zeros(len(reqs))
+        arrivals = np.cumsum(gaps)
+        t_start = time.perf_counter()
+
+        def submitter():
+            for (g, k, s), ta in zip(reqs, arrivals):
+                now = time.perf_counter() - t_start
+                if ta > now:
+                    time.sleep(ta - now)
+                t = srv.submit(g, k, s, out=take_out(g, k), restart=0.15, tolerance=1e-6)
+                meta[t] = True
+
+        th = threading.Thread(target=submitter)
+        th.start()
+        n_done, t_last = 0, t_start
+        while n_done < len(reqs):
+            for c in srv.poll(1024, wait_ms=5):
+                if c["status"] != 0:
+                    raise SystemExit(f"query failed with status {c['status']}")
+                lat.append(c["latency_ms"])
+                n_done += 1
+                t_last = time.perf_counter()
+        th.join()
+        return np.array(lat), t_last - t_start
+
+    with hyt.Server(graphs) as srv:
+        serve(srv, make_requests(200, 1), None)  # warm-up
+        reqs = make_requests(args.requests, 2)
+        clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+        clocks.start()
+        lat, wall = serve(srv, reqs, None)
+        clk = clocks.stop()
+        cap_qps = len(reqs) / wall
+        cap = {"requests": len(reqs), "wall_s": wall, "queries_per_s": cap_qps,
+               "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99))}
+        sweep = []
+        for rate in [float(x) for x in args.rates.split(",") if x]:
+            n = int(min(args.requests, max(50, rate * args.rate_seconds)))
+            lat, wall = serve(srv, make_requests(n, int(rate)), rate)
+            sweep.append({"offered_qps": rate, "requests": n, "achieved_qps": n / wall,
+                          "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                          "mean_ms": float(lat.mean())})
+        server_stats = srv.stats()
+    # one at a time: the same request mix, solved back to back
+    sample = make_requests(min(400, args.requests), 3)
+    for g, k, s in sample[:10]:
+        o = take_out(g, k)
+        (graphs[g].sssp(s, out=o) if k == "sssp" else graphs[g].ppr(s, out=o))
+    torch.cuda.synchronize()
+    lat1 = []
+    t0 = time.perf_counter()
+    for g, k, s in sample:
+        o = take_out(g, k)
+        ts = time.perf_counter()
+        (graphs[g].sssp(s, out=o) if k == "sssp" else graphs[g].ppr(s, out=o))
+        lat1.append((time.perf_counter() - ts) * 1e3)
+    single_qps = len(sample) / (time.perf_counter() - t0)
+    for g in graphs:
+        g.close()
+    if rank == 0:
+        line = {"metric": METRIC, "value": cap_qps * world, "unit": "queries/s", "n_gpus": world, "steps": 1,
+                "warmup": 1, "ms_per_step": 1e3 * cap["wall_s"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32 (PPR) / u32 (SSSP)", "data": "synthetic",
+                "config": {"workload": "served stream: 8 resident R-MAT graphs (scales 16,17,18,19,20,22,23,24, "
+                                       "edge factor 16), 70% SSSP / 30% PPR (restart 0.15, tol 1e-6), uniform "
+                                       "graph, source uniform over out-degree > 0, 16 GiB per-query-state budget, "
+                                       "continuous batching",
+                           "graphs_edges": E_of, "requests": args.requests, "seed": args.seed},
+                "capacity": cap, "sweep": sweep,
+                "one_at_a_time": {"requests": len(sample), "queries_per_s": single_qps,
+                                  "p50_ms": float(np.percentile(lat1, 50)), "p99_ms": float(np.percentile(lat1, 99))},
+                "speedup_vs_one_at_a_time": cap_qps / single_qps,
+                "server": server_stats, "clocks": clk, "gpu_launches": server_stats.get("graph_launches")}
+        print(json.dumps(line), flush=True)
+
+
 def workload_config(args, V, E):
     return {"workload": f"in-HBM R-MAT scale {args.scale} edge factor {args.edge_factor}: PageRank to L1<=1e-6 "
                         f"+ SSSP from {args.sources} seeded sources",
@@ -528,6 +654,11 @@ def main():
 
     if args.workload == "hybrid":
         run_hybrid(args, rank, world, pg)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
+    if args.workload == "serve":
+        run_serve_workload(args, rank, world, pg)
         if pg is not None:
             pg.destroy_process_group()
         return

@@ -276,6 +276,43 @@ class hyt_batch_stats(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class hyt_server_options(C.Structure):
+    _fields_ = [
+        ("device", C.c_int),
+        ("state_budget_bytes", C.c_uint64),
+        ("tuning", hyt_batch_tuning),
+        ("max_running", C.c_uint32),
+    ]
+
+
+class hyt_completion(C.Structure):
+    _fields_ = [
+        ("ticket", C.c_uint64),
+        ("status", C.c_int),
+        ("result", hyt_query_result),
+        ("queue_ms", C.c_double),
+        ("latency_ms", C.c_double),
+    ]
+
+
+class hyt_server_stats(C.Structure):
+    _fields_ = [
+        ("submitted", C.c_uint64),
+        ("completed", C.c_uint64),
+        ("supersteps", C.c_uint64),
+        ("graph_launches", C.c_uint64),
+        ("running", C.c_uint32),
+        ("waiting", C.c_uint32),
+        ("max_running", C.c_uint32),
+        ("state_bytes", C.c_uint64),
+        ("peak_state_bytes", C.c_uint64),
+        ("busy_ms", C.c_double),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 class HytError(RuntimeError):
     def __init__(self, code: int, message: str):
         super().__init__(f"[hyt status {code}] {message}")
@@ -313,6 +350,13 @@ _SIGNATURES = [
      [C.c_void_p, C.POINTER(hyt_query), C.c_uint32, C.POINTER(hyt_query_result), C.POINTER(hyt_batch_stats)]),
     ("hyt_batch_autotune", C.c_int, [C.c_void_p, C.POINTER(hyt_query), C.c_uint32, C.POINTER(hyt_batch_tuning)]),
     ("hyt_batch_set_tuning", C.c_int, [C.c_void_p, C.POINTER(hyt_batch_tuning)]),
+    ("hyt_server_create", C.c_int,
+     [C.POINTER(C.c_void_p), C.c_uint32, C.POINTER(hyt_server_options), C.POINTER(C.c_void_p)]),
+    ("hyt_server_submit", C.c_int, [C.c_void_p, C.POINTER(hyt_query), C.POINTER(C.c_uint64)]),
+    ("hyt_server_poll", C.c_int,
+     [C.c_void_p, C.POINTER(hyt_completion), C.c_uint32, C.POINTER(C.c_uint32), C.c_uint32]),
+    ("hyt_server_get_stats", C.c_int, [C.c_void_p, C.POINTER(hyt_server_stats)]),
+    ("hyt_server_destroy", C.c_int, [C.c_void_p]),
     ("hyt_rmat_generate", C.c_int, [C.POINTER(hyt_rmat_params), C.c_int, C.POINTER(hyt_csr_buffers)]),
     ("hyt_csr_buffers_free", C.c_int, [C.POINTER(hyt_csr_buffers)]),
     ("hyt_pick_sources", C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint32, C.c_void_p]),

@@ -378,6 +378,8 @@ QueryEngine::~QueryEngine() {
     cudaStreamSynchronize(stream_);
     if (exec_) cudaGraphExecDestroy(exec_);
     if (graph_) cudaGraphDestroy(graph_);
+    if (step_exec_) cudaGraphExecDestroy(step_exec_);
+    if (step_graph_) cudaGraphDestroy(step_graph_);
     if (pool_) cudaMemPoolDestroy(pool_);
 }
 
@@ -408,11 +410,13 @@ void QueryEngine::grow(uint32_t cap) {
     cap_ = cap;
     HYT_CUDA(cudaFuncSetAttribute(engine_work_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   work_kernel_smem(kMaxSlots)));
-    // the cached graph's grid sizes depend on the capacity
+    // the cached graphs' grid sizes depend on the capacity
     if (exec_) cudaGraphExecDestroy(exec_);
     if (graph_) cudaGraphDestroy(graph_);
-    exec_ = nullptr;
-    graph_ = nullptr;
+    if (step_exec_) cudaGraphExecDestroy(step_exec_);
+    if (step_graph_) cudaGraphDestroy(step_graph_);
+    exec_ = step_exec_ = nullptr;
+    graph_ = step_graph_ = nullptr;
     args_dirty_ = true;
 }
 
@@ -623,22 +627,7 @@ void QueryEngine::launch_superstep_kernels(cudaStream_t s) {
     HYT_CUDA(cudaGetLastError());
 }
 
-void QueryEngine::build_graph_exec() {
-    const int grid = work_grid();
-    if (exec_ && exec_grid_ == grid) return;
-    if (exec_) cudaGraphExecDestroy(exec_);
-    if (graph_) cudaGraphDestroy(graph_);
-    exec_ = nullptr;
-    HYT_CUDA(cudaGraphCreate(&graph_, 0));
-    HYT_CUDA(cudaGraphConditionalHandleCreate(&cond_, graph_, 1, cudaGraphCondAssignDefault));
-    cudaGraphNodeParams cp = {};
-    cp.type = cudaGraphNodeTypeConditional;
-    cp.conditional.handle = cond_;
-    cp.conditional.type = cudaGraphCondTypeWhile;
-    cp.conditional.size = 1;
-    cudaGraphNode_t cnode;
-    HYT_CUDA(cudaGraphAddNode(&cnode, graph_, nullptr, 0, &cp));
-    cudaGraph_t body = cp.conditional.phGraph_out[0];
+void QueryEngine::add_superstep_nodes(cudaGraph_t body, int grid) {
     EngineArgs *d = d_args_.get();
     void *kargs[] = {&d};
     struct K {
@@ -667,6 +656,46 @@ void QueryEngine::build_graph_exec() {
         HYT_CUDA(cudaGraphAddKernelNode(&node, body, prev ? &prev : nullptr, prev ? 1 : 0, &kp));
         prev = node;
     }
+}
+
+void QueryEngine::build_step_exec() {
+    const int grid = work_grid();
+    if (step_exec_ && step_grid_ == grid) return;
+    if (step_exec_) cudaGraphExecDestroy(step_exec_);
+    if (step_graph_) cudaGraphDestroy(step_graph_);
+    step_exec_ = nullptr;
+    HYT_CUDA(cudaGraphCreate(&step_graph_, 0));
+    add_superstep_nodes(step_graph_, grid);
+    HYT_CUDA(cudaGraphInstantiate(&step_exec_, step_graph_, 0));
+    step_grid_ = grid;
+}
+
+void QueryEngine::step() {
+    if (running_ == 0) return;
+    build_step_exec();
+    max_supersteps_ = 0x7FFFFFFF;
+    upload_args(false);
+    HYT_CUDA(cudaGraphLaunch(step_exec_, stream_));
+    ++launches_;
+}
+
+void QueryEngine::build_graph_exec() {
+    const int grid = work_grid();
+    if (exec_ && exec_grid_ == grid) return;
+    if (exec_) cudaGraphExecDestroy(exec_);
+    if (graph_) cudaGraphDestroy(graph_);
+    exec_ = nullptr;
+    HYT_CUDA(cudaGraphCreate(&graph_, 0));
+    HYT_CUDA(cudaGraphConditionalHandleCreate(&cond_, graph_, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = cond_;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t cnode;
+    HYT_CUDA(cudaGraphAddNode(&cnode, graph_, nullptr, 0, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    add_superstep_nodes(body, grid);
     HYT_CUDA(cudaGraphInstantiate(&exec_, graph_, 0));
     exec_grid_ = grid;
     args_dirty_ = true;

@@ -82,6 +82,8 @@ public:
     uint32_t run_to_completion(bool use_graph);
     // Runs exactly `n` supersteps (host-driven, for continuous batching).
     void run_supersteps(uint32_t n);
+    // Enqueues one superstep as one CUDA-graph launch (no conditional).
+    void step();
 
     // Slots whose query finished (synchronises the stream).  Each entry:
     // slot, tag.
@@ -107,6 +109,8 @@ private:
     void grow(uint32_t cap);
     void ensure_hub_capacity();
     void build_graph_exec();
+    void build_step_exec();
+    void add_superstep_nodes(cudaGraph_t body, int grid);
     void upload_args(bool use_cond);
     void launch_superstep_kernels(cudaStream_t s);
     int work_grid() const;
@@ -130,6 +134,9 @@ private:
     cudaGraphExec_t exec_ = nullptr;
     cudaGraphConditionalHandle cond_{};
     int exec_grid_ = 0;
+    cudaGraph_t step_graph_ = nullptr;
+    cudaGraphExec_t step_exec_ = nullptr;
+    int step_grid_ = 0;
     bool args_dirty_ = true;
 
 public:

@@ -435,3 +435,74 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+class Server:
+    """Continuous-batching query server (hyt_server handle): submit() from
+    any thread, poll() for completions.  A query's `out` array must stay
+    alive until its completion has been polled."""
+
+    def __init__(self, graphs, device: int = 0, state_budget_bytes: int = 0, delta_mult: int = 0,
+                 hub_degree: int = 0, ctas_per_sm: int = 0, max_running: int = 0):
+        self._graphs = list(graphs)
+        arr = (C.c_void_p * len(self._graphs))(*[g.handle.value for g in self._graphs])
+        opts = capi.hyt_server_options(device, state_budget_bytes,
+                                       capi.hyt_batch_tuning(delta_mult, hub_degree, ctas_per_sm), max_running)
+        h = C.c_void_p()
+        check(lib.hyt_server_create(arr, len(self._graphs), C.byref(opts), C.byref(h)))
+        self._h = h
+        self._outs = {}
+
+    @property
+    def handle(self) -> C.c_void_p:
+        if not self._h:
+            raise ValueError("server is closed")
+        return self._h
+
+    def submit(self, graph: int, kind, source: int, out=None, restart: float = 0.0, tolerance: float = 0.0,
+               max_iterations: int = 0) -> int:
+        if isinstance(kind, str):
+            kind = capi.HYT_QUERY_SSSP if kind == "sssp" else capi.HYT_QUERY_PPR
+        if out is None and 0 <= graph < len(self._graphs):
+            out = np.empty(self._graphs[graph].num_vertices, np.uint32 if kind == capi.HYT_QUERY_SSSP else np.float32)
+        q = capi.hyt_query(graph, kind, source, restart, tolerance, max_iterations,
+                           _ptr(out) if out is not None else None)
+        t = C.c_uint64()
+        check(lib.hyt_server_submit(self.handle, C.byref(q), C.byref(t)))
+        self._outs[t.value] = out
+        return t.value
+
+    def poll(self, max_items: int = 1024, wait_ms: int = 0):
+        """List of completion dicts: ticket, status, result, queue_ms,
+        latency_ms, out (the array holding the result)."""
+        buf = (capi.hyt_completion * max_items)()
+        n = C.c_uint32()
+        check(lib.hyt_server_poll(self.handle, buf, max_items, C.byref(n), wait_ms))
+        out = []
+        for i in range(n.value):
+            c = buf[i]
+            out.append({"ticket": c.ticket, "status": c.status, "result": c.result.as_dict(),
+                        "queue_ms": c.queue_ms, "latency_ms": c.latency_ms, "out": self._outs.pop(c.ticket, None)})
+        return out
+
+    def stats(self) -> dict:
+        st = capi.hyt_server_stats()
+        check(lib.hyt_server_get_stats(self.handle, C.byref(st)))
+        return st.as_dict()
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            check(lib.hyt_server_destroy(self._h))
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -376,6 +376,58 @@ int hyt_batch_autotune(hyt_batch *batch, const hyt_query *queries, uint32_t num_
 int hyt_batch_set_tuning(hyt_batch *batch, const hyt_batch_tuning *tuning);
 
 /* ------------------------------------------------------------------ */
+/* Serving: continuous batching of arriving queries                     */
+/* ------------------------------------------------------------------ */
+
+/* A server owns one worker thread and one stream.  Submitted queries wait
+ * in a FIFO; between supersteps the worker admits waiting queries while
+ * the per-query state budget and the slot table allow, advances every
+ * running query by one superstep (one SSSP round / one PPR iteration,
+ * a single CUDA-graph launch), and retires the finished ones: their result
+ * is copied to the query's `out` buffer (which must stay valid until the
+ * completion is polled) and a completion is queued.  A query's result is
+ * the same whatever else runs beside it (hyt_batch_run's guarantee). */
+typedef struct hyt_server hyt_server;
+
+typedef struct hyt_server_options {
+    int device;
+    uint64_t state_budget_bytes;  /* 0 = 16 GiB */
+    hyt_batch_tuning tuning;
+    uint32_t max_running;         /* cap on concurrently running queries
+                                     (0 = slot table size, 4096) */
+} hyt_server_options;
+
+typedef struct hyt_completion {
+    uint64_t ticket;
+    int status;                   /* HYT_OK or an HYT_E_* code (HYT_E_OOM:
+                                     the query's state exceeds the budget) */
+    hyt_query_result result;
+    double queue_ms;              /* submit -> admitted */
+    double latency_ms;            /* submit -> result in `out` */
+} hyt_completion;
+
+typedef struct hyt_server_stats {
+    uint64_t submitted, completed, supersteps, graph_launches;
+    uint32_t running, waiting, max_running;
+    uint64_t state_bytes, peak_state_bytes;
+    double busy_ms;               /* worker time with queries running */
+} hyt_server_stats;
+
+/* graphs: handles built with HYT_GRAPH_ALL (borrowed; keep them alive). */
+int hyt_server_create(hyt_graph *const *graphs, uint32_t num_graphs, const hyt_server_options *options,
+                      hyt_server **out);
+/* Thread-safe.  Validates the query (HYT_E_INVALID as hyt_batch_run) and
+ * queues it; *ticket identifies its completion. */
+int hyt_server_submit(hyt_server *server, const hyt_query *query, uint64_t *ticket);
+/* Up to `max` completions into out[]; *count receives how many.  Waits up
+ * to wait_ms milliseconds for the first one (0 = do not wait). */
+int hyt_server_poll(hyt_server *server, hyt_completion *out, uint32_t max, uint32_t *count, uint32_t wait_ms);
+int hyt_server_get_stats(hyt_server *server, hyt_server_stats *stats);
+/* Stops the worker after the running queries finish (their completions
+ * are discarded); queries still waiting for admission are dropped. */
+int hyt_server_destroy(hyt_server *server);
+
+/* ------------------------------------------------------------------ */
 /* Seeded R-MAT generator (deterministic; same bytes on host and GPU)   */
 /* ------------------------------------------------------------------ */
 
