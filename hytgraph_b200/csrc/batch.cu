@@ -27,10 +27,12 @@ enum : uint32_t { kFree = 0, kSSSP = 1, kPPR = 2 };
 
 constexpr uint32_t kMaxSlots = 4096;
 constexpr int kWorkThreads = 256;
-constexpr int kWorkWarps = kWorkThreads / 32;
 constexpr size_t kSliceFloats = 2 * size_t(kTileCostMax) + 8;  // PPR tile staging per warp
-constexpr int kSplitBlocks = 32;
+constexpr int kSplitBlocks = 4;
 constexpr int kInitBlocks = 64;
+constexpr uint32_t kEndBlocks = 16;  // blocks per PPR slot in the end reduction
+constexpr uint32_t kGrab = 4;        // units / hub tasks a warp takes at a time
+constexpr bool kHotGlobal = true;    // hot sources read from the slot's hot_contrib array
 
 struct Slot {
     uint32_t kind;        // kFree / kSSSP / kPPR
@@ -39,11 +41,18 @@ struct Slot {
     uint32_t delta;       // SSSP bucket width (kNoDelta = one bucket)
 };
 
-// PPR per-task partial sums: (residual, dangling) of tile k at [k], of long
-// row i at [num_tiles + i]; summed in index order by the end kernel.
+// PPR per-query extras.  task_sums: (residual, dangling) of tile k at [k],
+// of long row i at [num_tiles + i]; end blocks sum fixed stripes of it into
+// block_sums, the last block sums those in index order.  hot_contrib[p]:
+// the contributions of the graph's hot sources (tagged ids in in_sources)
+// for iteration parity p, gathered once per iteration so that tasks read
+// them with one load.
 struct PRExtra {
     double2 *task_sums;
-    uint32_t num_tiles, num_long, num_chunks, pad;
+    double2 *block_sums;  // [kEndBlocks]
+    uint32_t *end_ticket;
+    float *hot_contrib[2];
+    uint32_t num_tiles, num_long, num_chunks, num_hot;
 };
 
 struct SlotStatus {
@@ -59,13 +68,17 @@ struct EngineArgs {
     SSArgs *ss;
     PRArgs *pr;
     PRExtra *px;
+    RoundView *rvs;       // per-slot round snapshot (SSSP), written by prep
     uint32_t n;           // slots [0, n) are examined
     uint32_t hub_degree;
-    uint32_t *unit_base;  // [n + 1]
+    uint32_t *ss_base;    // [n + 1] SSSP unit prefix
+    uint32_t *pr_base;    // [n + 1] PPR unit prefix
     uint4 *hubs;          // (slot, vertex, chunk, -)
     uint32_t hub_cap;
     uint32_t max_supersteps;
-    uint32_t *counters;   // [0] hub tasks, [1] running after this superstep, [2] supersteps, [3] overflow
+    // [0] hub tasks, [1] running after this superstep, [2] supersteps,
+    // [3] overflow, [4] SSSP unit cursor, [5] hub cursor, [6] PPR unit cursor
+    uint32_t *counters;
     cudaGraphConditionalHandle cond;
     uint32_t use_cond;
 };
@@ -91,13 +104,17 @@ __global__ void engine_init_kernel(const EngineArgs *__restrict__ eap, uint32_t 
     } else if (sl.kind == kPPR) {
         // x_0 = e_s (the state block arrives zeroed)
         const PRArgs a = ea.pr[q];
+        const PRExtra x = ea.px[q];
+        const uint32_t s = a.source;
+        const uint32_t od = a.out_deg[s];
+        const float c0 = od ? __fdiv_rn(1.0f, static_cast<float>(od)) : 0.0f;
         if (blockIdx.x == 0 && threadIdx.x == 0) {
-            const uint32_t s = a.source;
-            const uint32_t od = a.out_deg[s];
             a.rank[0][s] = 1.0f;
-            a.contrib[0][s] = od ? __fdiv_rn(1.0f, static_cast<float>(od)) : 0.0f;
+            a.contrib[0][s] = c0;
             a.dangling[0] = od ? 0.0 : 1.0;
         }
+        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < x.num_hot; i += stride)
+            if (a.hot_vertex[i] == s) x.hot_contrib[0][i] = c0;
     }
 }
 
@@ -113,44 +130,39 @@ __global__ void engine_split_kernel(const EngineArgs *__restrict__ eap) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) split_entry(a, i);
 }
 
-__device__ __forceinline__ uint32_t slot_units(const EngineArgs &ea, uint32_t q) {
+// Work units of slot q this superstep (SSSP: 32-vertex frontier blocks,
+// PPR: chunk tasks + tiles); snapshots the SSSP round view.
+__device__ __forceinline__ void slot_units(const EngineArgs &ea, uint32_t q, uint32_t &ss, uint32_t &pr,
+                                           bool snapshot) {
+    ss = pr = 0;
     const Slot sl = ea.slot[q];
     if (sl.kind == kSSSP) {
-        const SSHeader *h = ea.ss[q].hdr;
-        if (*(volatile const uint32_t *)&h->done) return 0;
-        const uint32_t r = h->round;
-        const uint32_t qn = (r & 1) ? h->qsize[1] : h->qsize[0];
-        return (qn + 31) / 32;
-    }
-    if (sl.kind == kPPR) {
-        if (*(volatile const uint32_t *)&ea.pr[q].hdr->done) return 0;
+        const SSArgs a = ea.ss[q];
+        if (*(volatile const uint32_t *)&a.hdr->done) return;
+        const RoundView rv = round_view(a);
+        if (snapshot) ea.rvs[q] = rv;
+        ss = (rv.qn + 31) / 32;
+    } else if (sl.kind == kPPR) {
+        if (*(volatile const uint32_t *)&ea.pr[q].hdr->done) return;
         const PRExtra x = ea.px[q];
-        return x.num_chunks + x.num_tiles;
+        pr = x.num_chunks + x.num_tiles;
     }
-    return 0;
 }
 
-// One CTA of 1024 threads: per-slot work units and their exclusive prefix.
-__global__ void __launch_bounds__(1024) engine_prep_kernel(const EngineArgs *__restrict__ eap) {
-    __shared__ uint32_t s_warp[32];
-    const EngineArgs ea = *eap;
-    const uint32_t n = ea.n;
-    const uint32_t per = (n + blockDim.x - 1) / blockDim.x;
-    const uint32_t b = threadIdx.x * per, e = min(n, b + per);
-    uint32_t sum = 0;
-    for (uint32_t q = b; q < e; ++q) sum += slot_units(ea, q);
-    // block exclusive scan of the per-thread sums
+// Block-wide exclusive scan of one value per thread (1024 threads).
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t *s_warp, uint32_t &total) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint32_t incl = sum;
+    uint32_t incl = v;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
         const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
         if (lane >= o) incl += y;
     }
+    __syncthreads();
     if (lane == 31) s_warp[warp] = incl;
     __syncthreads();
     if (warp == 0) {
-        uint32_t w = (lane < static_cast<int>(blockDim.x >> 5)) ? s_warp[lane] : 0u;
+        const uint32_t w = (lane < static_cast<int>(blockDim.x >> 5)) ? s_warp[lane] : 0u;
         uint32_t wi = w;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -158,147 +170,256 @@ __global__ void __launch_bounds__(1024) engine_prep_kernel(const EngineArgs *__r
             if (lane >= o) wi += y;
         }
         s_warp[lane] = wi - w;
+        if (lane == 31) s_warp[32] = wi;
     }
     __syncthreads();
-    uint32_t base = s_warp[warp] + incl - sum;
-    for (uint32_t q = b; q < e; ++q) {
-        ea.unit_base[q] = base;
-        base += slot_units(ea, q);
-    }
-    if (threadIdx.x == blockDim.x - 1) ea.unit_base[n] = base;
-    if (threadIdx.x == 0) ea.counters[0] = 0;
+    total = s_warp[32];
+    return s_warp[warp] + incl - v;
 }
 
-template <int WK>
-__device__ __forceinline__ void expand_unit(const EngineArgs &ea, uint32_t q, uint32_t t, int lane) {
-    const SSArgs a = ea.ss[q];
-    const RoundView rv = round_view(a);
-    unsigned long long relaxed = 0, improved = 0;
-    auto hub = [&](uint32_t v, uint32_t nch) {
-        const uint32_t base = atomicAdd(&ea.counters[0], nch);
-        if (base + nch > ea.hub_cap) {  // cannot happen within the admitted bound; reported, never written
-            atomicExch(&ea.counters[3], 1u);
-            return;
+// One CTA of 1024 threads: per-slot SSSP and PPR unit prefixes, SSSP round
+// snapshots, cursors reset.
+__global__ void __launch_bounds__(1024) engine_prep_kernel(const EngineArgs *__restrict__ eap) {
+    __shared__ uint32_t s_warp[33];
+    const EngineArgs ea = *eap;
+    const uint32_t n = ea.n;
+    const uint32_t per = (n + blockDim.x - 1) / blockDim.x;
+    const uint32_t b = threadIdx.x * per, e = min(n, b + per);
+    uint32_t ss_sum = 0, pr_sum = 0;
+    for (uint32_t q = b; q < e; ++q) {
+        uint32_t s, p;
+        slot_units(ea, q, s, p, true);
+        ss_sum += s;
+        pr_sum += p;
+    }
+    uint32_t ss_total, pr_total;
+    uint32_t ss_at = block_exclusive_scan(ss_sum, s_warp, ss_total);
+    uint32_t pr_at = block_exclusive_scan(pr_sum, s_warp, pr_total);
+    for (uint32_t q = b; q < e; ++q) {
+        ea.ss_base[q] = ss_at;
+        ea.pr_base[q] = pr_at;
+        uint32_t s, p;
+        slot_units(ea, q, s, p, false);
+        ss_at += s;
+        pr_at += p;
+    }
+    if (threadIdx.x == 0) {
+        ea.ss_base[n] = ss_total;
+        ea.pr_base[n] = pr_total;
+        ea.counters[0] = 0;
+        ea.counters[4] = 0;
+        ea.counters[5] = 0;
+        ea.counters[6] = 0;
+    }
+}
+
+// Slot of unit u: the last q with base[q] <= u (base in shared memory).
+__device__ __forceinline__ uint32_t find_slot(const uint32_t *base, uint32_t n, uint32_t u) {
+    uint32_t lo = 0, hi = n;  // base[lo] <= u < base[hi]
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (base[mid] <= u) {
+            lo = mid;
+        } else {
+            hi = mid;
         }
-        for (uint32_t c = 0; c < nch; ++c) ea.hubs[base + c] = make_uint4(q, v, c, 0u);
-    };
-    expand_warp<WK, false>(a, rv, t * 32, lane, ea.hub_degree, relaxed, improved, hub);
+    }
+    return lo;
+}
+
+// Next kGrab-sized range of a global cursor for this warp (lane 0 takes it).
+__device__ __forceinline__ uint32_t grab(uint32_t *cursor, int lane) {
+    uint32_t c = 0;
+    if (lane == 0) c = atomicAdd(cursor, kGrab);
+    return __shfl_sync(0xffffffffu, c, 0);
+}
+
+// Adds the warp's relaxation count to the slot's header; all 32 lanes.
+__device__ __forceinline__ void flush_relaxed(const SSArgs &a, unsigned long long &relaxed, int lane) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) relaxed += __shfl_xor_sync(0xffffffffu, relaxed, o);
     if (lane == 0 && relaxed) atomicAdd(&a.hdr->relaxations, relaxed);
+    relaxed = 0;
 }
 
-// Persistent grid: warps take work units round-robin.
-__global__ void __launch_bounds__(kWorkThreads) engine_work_kernel(const EngineArgs *__restrict__ eap) {
+// SSSP frontier blocks of every SSSP slot.  Warps take kGrab consecutive
+// units at a time; a slot's arguments are reloaded only when the slot
+// changes.
+__global__ void __launch_bounds__(kWorkThreads, 4) engine_sssp_kernel(const EngineArgs *__restrict__ eap) {
+    extern __shared__ __align__(16) uint32_t s_base[];
+    const EngineArgs ea = *eap;
+    const uint32_t n = ea.n;
+    for (uint32_t i = threadIdx.x; i <= n; i += blockDim.x) s_base[i] = ea.ss_base[i];
+    __syncthreads();
+    const uint32_t total = s_base[n];
+    const int lane = threadIdx.x & 31;
+    uint32_t cq = ~0u, wk = 0;
+    SSArgs a{};
+    RoundView rv{};
+    unsigned long long relaxed = 0, improved = 0;
+    uint32_t *hub_count = ea.counters + 0;
+    for (uint32_t c = grab(ea.counters + 4, lane); c < total; c = grab(ea.counters + 4, lane)) {
+        const uint32_t end = min(total, c + kGrab);
+        for (uint32_t u = c; u < end; ++u) {
+            const uint32_t q = find_slot(s_base, n, u);
+            if (q != cq) {  // warp-uniform
+                if (cq != ~0u) flush_relaxed(a, relaxed, lane);
+                a = ea.ss[q];
+                rv = ea.rvs[q];
+                wk = ea.slot[q].wk;
+                cq = q;
+            }
+            auto hub = [&](uint32_t v, uint32_t nch) {
+                const uint32_t base = atomicAdd(hub_count, nch);
+                if (base + nch > ea.hub_cap) {  // cannot happen within the admitted bound; reported, never written
+                    atomicExch(&ea.counters[3], 1u);
+                    return;
+                }
+                for (uint32_t k = 0; k < nch; ++k) ea.hubs[base + k] = make_uint4(q, v, k, 0u);
+            };
+            const uint32_t i0 = (u - s_base[q]) * 32;
+            if (wk == HYT_WEIGHTS_U32) {
+                expand_warp<HYT_WEIGHTS_U32, false>(a, rv, i0, lane, ea.hub_degree, relaxed, improved, hub);
+            } else if (wk == HYT_WEIGHTS_NONE) {
+                expand_warp<HYT_WEIGHTS_NONE, false>(a, rv, i0, lane, ea.hub_degree, relaxed, improved, hub);
+            } else {
+                expand_warp<HYT_WEIGHTS_F32, false>(a, rv, i0, lane, ea.hub_degree, relaxed, improved, hub);
+            }
+        }
+    }
+    if (cq != ~0u) flush_relaxed(a, relaxed, lane);
+}
+
+// PPR tasks of every PPR slot: warps take units round-robin (every task
+// costs at most one long-row chunk; at any moment the grid works inside
+// one slot's unit range, so its contributions stay in L2); a slot's
+// arguments are read per unit (L1-resident); hot sources come from the
+// slot's hot_contrib array.
+__global__ void __launch_bounds__(kWorkThreads) engine_ppr_kernel(const EngineArgs *__restrict__ eap) {
     extern __shared__ __align__(16) float s_dyn[];
     const EngineArgs ea = *eap;
     const uint32_t n = ea.n;
-    uint32_t *s_base = reinterpret_cast<uint32_t *>(s_dyn + kWorkWarps * kSliceFloats);
-    for (uint32_t i = threadIdx.x; i <= n; i += blockDim.x) s_base[i] = ea.unit_base[i];
+    uint32_t *s_base = reinterpret_cast<uint32_t *>(s_dyn + (kWorkThreads / 32) * kSliceFloats);
+    for (uint32_t i = threadIdx.x; i <= n; i += blockDim.x) s_base[i] = ea.pr_base[i];
     __syncthreads();
     const uint32_t total = s_base[n];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     float *sv = s_dyn + warp * kSliceFloats;
     const uint64_t pol = dev::policy_evict_last();
-    for (uint32_t u = blockIdx.x * kWorkWarps + warp; u < total; u += gridDim.x * kWorkWarps) {
-        uint32_t lo = 0, hi = n;  // s_base[lo] <= u < s_base[hi]
-        while (hi - lo > 1) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (s_base[mid] <= u) {
-                lo = mid;
-            } else {
-                hi = mid;
-            }
-        }
-        const uint32_t q = lo, t = u - s_base[lo];
-        const Slot sl = ea.slot[q];
-        if (sl.kind == kSSSP) {
-            if (sl.wk == HYT_WEIGHTS_U32) {
-                expand_unit<HYT_WEIGHTS_U32>(ea, q, t, lane);
-            } else if (sl.wk == HYT_WEIGHTS_NONE) {
-                expand_unit<HYT_WEIGHTS_NONE>(ea, q, t, lane);
-            } else {
-                expand_unit<HYT_WEIGHTS_F32>(ea, q, t, lane);
-            }
+    const uint32_t nwarps = gridDim.x * (kWorkThreads / 32);
+    for (uint32_t u = blockIdx.x * (kWorkThreads / 32) + warp; u < total; u += nwarps) {
+        const uint32_t q = find_slot(s_base, n, u);
+        const uint32_t t = u - s_base[q];
+        const PRArgs a = ea.pr[q];
+        const PRExtra x = ea.px[q];
+        const uint32_t it = *(volatile uint32_t *)&a.hdr->iter;
+        const PRBuffers b = prc::buffers(a, it);
+        const PRState ps = prc::make_state(a, a.dangling[it]);
+        const float *hot = x.hot_contrib[it & 1];
+        double res = 0.0, dang = 0.0;
+        if (t < x.num_chunks) {
+            const uint32_t li = prc::chunk_task<kHotGlobal>(a, ps, b, a.in_src, hot, t, pol, lane, res, dang);
+            if (li != ~0u && lane == 0) x.task_sums[x.num_tiles + li] = make_double2(res, dang);
         } else {
-            const PRArgs a = ea.pr[q];
-            const PRExtra x = ea.px[q];
-            const uint32_t it = *(volatile uint32_t *)&a.hdr->iter;
-            const PRBuffers b = prc::buffers(a, it);
-            const PRState ps = prc::make_state(a, a.dangling[it]);
-            double res = 0.0, dang = 0.0;
-            if (t < x.num_chunks) {
-                const uint32_t li = prc::chunk_task<false>(a, ps, b, a.in_src, nullptr, t, pol, lane, res, dang);
-                if (li != ~0u && lane == 0) x.task_sums[x.num_tiles + li] = make_double2(res, dang);
-            } else {
-                const uint64_t k = t - x.num_chunks;
-                prc::tile_task<false>(a, ps, b, a.in_src, nullptr, sv, k, pol, lane, res, dang);
-                res = dev::warp_sum(res);
-                dang = dev::warp_sum(dang);
-                if (lane == 0) x.task_sums[k] = make_double2(res, dang);
-            }
+            const uint64_t k = t - x.num_chunks;
+            prc::tile_task<kHotGlobal>(a, ps, b, a.in_src, hot, sv, k, pol, lane, res, dang);
+            res = dev::warp_sum(res);
+            dang = dev::warp_sum(dang);
+            if (lane == 0) x.task_sums[k] = make_double2(res, dang);
         }
     }
 }
 
-__global__ void __launch_bounds__(kWorkThreads) engine_hub_kernel(const EngineArgs *__restrict__ eap) {
+__global__ void __launch_bounds__(kWorkThreads, 4) engine_hub_kernel(const EngineArgs *__restrict__ eap) {
     const EngineArgs ea = *eap;
     const uint32_t n = min(*(volatile uint32_t *)&ea.counters[0], ea.hub_cap);
     const int lane = threadIdx.x & 31;
-    const uint32_t gwarp = (blockIdx.x * kWorkThreads + threadIdx.x) >> 5;
-    const uint32_t nwarps = (gridDim.x * kWorkThreads) >> 5;
+    uint32_t cq = ~0u, wk = 0;
+    SSArgs a{};
+    RoundView rv{};
     unsigned long long improved = 0;
-    for (uint32_t t = gwarp; t < n; t += nwarps) {
-        const uint4 h = ea.hubs[t];
-        const SSArgs a = ea.ss[h.x];
-        const RoundView rv = round_view(a);
-        const uint32_t wk = ea.slot[h.x].wk;
-        if (wk == HYT_WEIGHTS_U32) {
-            hub_chunk<HYT_WEIGHTS_U32>(a, rv, a.cols, a.weights, h.y, h.z, lane, improved);
-        } else if (wk == HYT_WEIGHTS_NONE) {
-            hub_chunk<HYT_WEIGHTS_NONE>(a, rv, a.cols, a.weights, h.y, h.z, lane, improved);
-        } else {
-            hub_chunk<HYT_WEIGHTS_F32>(a, rv, a.cols, a.weights, h.y, h.z, lane, improved);
+    for (uint32_t c = grab(ea.counters + 5, lane); c < n; c = grab(ea.counters + 5, lane)) {
+        const uint32_t end = min(n, c + kGrab);
+        for (uint32_t t = c; t < end; ++t) {
+            const uint4 h = ea.hubs[t];
+            if (h.x != cq) {
+                a = ea.ss[h.x];
+                rv = ea.rvs[h.x];
+                wk = ea.slot[h.x].wk;
+                cq = h.x;
+            }
+            if (wk == HYT_WEIGHTS_U32) {
+                hub_chunk<HYT_WEIGHTS_U32>(a, rv, a.cols, a.weights, h.y, h.z, lane, improved);
+            } else if (wk == HYT_WEIGHTS_NONE) {
+                hub_chunk<HYT_WEIGHTS_NONE>(a, rv, a.cols, a.weights, h.y, h.z, lane, improved);
+            } else {
+                hub_chunk<HYT_WEIGHTS_F32>(a, rv, a.cols, a.weights, h.y, h.z, lane, improved);
+            }
         }
     }
 }
 
-// One CTA per slot: SSSP round end; PPR residual and dangling mass summed
-// over the task partials in index order (a fixed association, independent
-// of the other slots and of the grid), then the stop rule.
+// Grid (kEndBlocks, slots).  SSSP: block 0 closes the round.  PPR: block b
+// sums stripe b of the task partials and gathers stripe b of the next
+// iteration's hot contributions; the last block to arrive sums the
+// kEndBlocks stripe sums in index order (a fixed association, independent
+// of the other slots) and applies the stop rule.
 __global__ void engine_end_kernel(const EngineArgs *__restrict__ eap) {
     __shared__ double s_red[32];
+    __shared__ uint32_t s_last;
     const EngineArgs ea = *eap;
-    const uint32_t q = blockIdx.x;
+    const uint32_t q = blockIdx.y;
     if (q >= ea.n) return;
     const Slot sl = ea.slot[q];
     if (sl.kind == kSSSP) {
-        if (threadIdx.x == 0) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
             SSHeader *h = ea.ss[q].hdr;
             if (!h->done && !round_end(h)) atomicAdd(&ea.counters[1], 1u);
         }
-    } else if (sl.kind == kPPR) {
-        const PRArgs a = ea.pr[q];
-        if (*(volatile uint32_t *)&a.hdr->done) return;
-        const PRExtra x = ea.px[q];
-        const uint32_t it = a.hdr->iter;
-        const uint32_t m = x.num_tiles + x.num_long;
-        double r = 0.0, d = 0.0;
-        for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
-            const double2 v = x.task_sums[i];
-            r += v.x;
-            d += v.y;
-        }
-        r = dev::block_sum(r, s_red);
-        __syncthreads();
-        d = dev::block_sum(d, s_red);
-        if (threadIdx.x == 0) {
-            a.residual[it] = r;
-            a.dangling[it + 1] = d;
-            prc::end_iteration(a, it);
-            if (!a.hdr->done) atomicAdd(&ea.counters[1], 1u);
-        }
+        return;
     }
+    if (sl.kind != kPPR) return;
+    const PRArgs a = ea.pr[q];
+    if (*(volatile uint32_t *)&a.hdr->done) return;
+    const PRExtra x = ea.px[q];
+    const uint32_t it = a.hdr->iter;
+    const uint32_t m = x.num_tiles + x.num_long;
+    const uint32_t stripe = (m + kEndBlocks - 1) / kEndBlocks;
+    const uint32_t lo = min(m, blockIdx.x * stripe), hi = min(m, lo + stripe);
+    double r = 0.0, d = 0.0;
+    for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+        const double2 v = x.task_sums[i];
+        r += v.x;
+        d += v.y;
+    }
+    r = dev::block_sum(r, s_red);
+    __syncthreads();
+    d = dev::block_sum(d, s_red);
+    // hot contributions of the next iteration (its contributions are final now)
+    const float *cnxt = ((it + 1) & 1) ? a.contrib[1] : a.contrib[0];
+    float *hnxt = x.hot_contrib[(it + 1) & 1];
+    const uint32_t hs = (x.num_hot + kEndBlocks - 1) / kEndBlocks;
+    for (uint32_t i = blockIdx.x * hs + threadIdx.x; i < min(x.num_hot, (blockIdx.x + 1) * hs); i += blockDim.x)
+        hnxt[i] = cnxt[a.hot_vertex[i]];
+    if (threadIdx.x == 0) {
+        x.block_sums[blockIdx.x] = make_double2(r, d);
+        __threadfence();
+        const uint32_t t = atomicAdd(x.end_ticket, 1u) + 1u;
+        s_last = (t % kEndBlocks == 0) ? 1u : 0u;
+    }
+    __syncthreads();
+    if (!s_last || threadIdx.x != 0) return;
+    __threadfence();
+    double rs = 0.0, ds = 0.0;
+    for (uint32_t k = 0; k < kEndBlocks; ++k) {
+        const double2 v = __ldcg(x.block_sums + k);
+        rs += v.x;
+        ds += v.y;
+    }
+    a.residual[it] = rs;
+    a.dangling[it + 1] = ds;
+    prc::end_iteration(a, it);
+    if (!a.hdr->done) atomicAdd(&ea.counters[1], 1u);
 }
 
 __global__ void engine_cond_kernel(const EngineArgs *__restrict__ eap) {
@@ -335,9 +456,11 @@ __global__ void engine_status_kernel(const EngineArgs *__restrict__ eap, SlotSta
 
 uint64_t align256(uint64_t x) { return (x + 255) & ~uint64_t(255); }
 
-int work_kernel_smem(uint32_t cap) {
-    return static_cast<int>(kWorkWarps * kSliceFloats * sizeof(float) + (cap + 1) * sizeof(uint32_t));
+int ppr_kernel_smem(uint32_t cap) {
+    return static_cast<int>((kWorkThreads / 32) * kSliceFloats * sizeof(float) + (cap + 1) * sizeof(uint32_t));
 }
+
+int sssp_kernel_smem(uint32_t cap) { return static_cast<int>((cap + 1) * sizeof(uint32_t)); }
 
 }  // namespace
 
@@ -352,6 +475,7 @@ struct EngineHost {
     DeviceArray<SSArgs> d_ss;
     DeviceArray<PRArgs> d_pr;
     DeviceArray<PRExtra> d_px;
+    DeviceArray<RoundView> d_rvs;
     DeviceArray<SlotStatus> d_status;
     PinnedArray<SlotStatus> h_status;
 };
@@ -365,8 +489,8 @@ QueryEngine::QueryEngine(int device, cudaStream_t stream, uint64_t budget_bytes)
     HYT_CUDA(cudaMemPoolCreate(&pool_, &props));
     uint64_t keep = std::numeric_limits<uint64_t>::max();
     HYT_CUDA(cudaMemPoolSetAttribute(pool_, cudaMemPoolAttrReleaseThreshold, &keep));
-    counters_.allocate(4);
-    HYT_CUDA(cudaMemsetAsync(counters_.get(), 0, 16, stream_));
+    counters_.allocate(8);
+    HYT_CUDA(cudaMemsetAsync(counters_.get(), 0, 32, stream_));
     d_args_.allocate(1);
     grow(64);
 }
@@ -398,6 +522,7 @@ void QueryEngine::grow(uint32_t cap) {
     h.d_ss.allocate(cap);
     h.d_pr.allocate(cap);
     h.d_px.allocate(cap);
+    h.d_rvs.allocate(cap);
     h.d_status.allocate(cap);
     h.h_status.allocate(cap);
     HYT_CUDA(cudaMemcpyAsync(h.d_slot.get(), h.slot.data(), cap * sizeof(Slot), cudaMemcpyHostToDevice, stream_));
@@ -405,11 +530,11 @@ void QueryEngine::grow(uint32_t cap) {
     HYT_CUDA(cudaMemcpyAsync(h.d_pr.get(), h.pr.data(), cap * sizeof(PRArgs), cudaMemcpyHostToDevice, stream_));
     HYT_CUDA(cudaMemcpyAsync(h.d_px.get(), h.px.data(), cap * sizeof(PRExtra), cudaMemcpyHostToDevice, stream_));
     HYT_CUDA(cudaStreamSynchronize(stream_));
-    unit_base_.allocate(cap + 1);
+    unit_base_.allocate(2 * (cap + 1));  // SSSP prefix, then PPR prefix
     slots_.resize(cap);
     cap_ = cap;
-    HYT_CUDA(cudaFuncSetAttribute(engine_work_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  work_kernel_smem(kMaxSlots)));
+    HYT_CUDA(cudaFuncSetAttribute(engine_ppr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  ppr_kernel_smem(kMaxSlots)));
     // the cached graphs' grid sizes depend on the capacity
     if (exec_) cudaGraphExecDestroy(exec_);
     if (graph_) cudaGraphDestroy(graph_);
@@ -453,7 +578,8 @@ uint64_t QueryEngine::state_bytes(const hyt_query &q) const {
     if (q.kind == HYT_QUERY_SSSP) return align256(sizeof(SSHeader)) + 7 * align256(V * 4 + 16);
     const uint64_t it = ppr_iters(q);
     return align256(sizeof(PRHeader)) + 4 * align256(V * 4 + 16) + align256(g.num_chunks * 8 + 16) +
-           align256(g.num_long * 4 + 16) + align256((g.num_tiles + g.num_long) * 16 + 16) + 2 * align256((it + 2) * 8);
+           align256(g.num_long * 4 + 16) + align256((g.num_tiles + g.num_long) * 16 + 16) + 2 * align256((it + 2) * 8) +
+           align256(kEndBlocks * 16) + align256(16) + 2 * align256(uint64_t(g.num_hot) * 4 + 16);
 }
 
 int QueryEngine::admit(const hyt_query &q, uint64_t tag) {
@@ -533,8 +659,12 @@ int QueryEngine::admit(const hyt_query &q, uint64_t tag) {
         x.num_tiles = static_cast<uint32_t>(g.num_tiles);
         x.num_long = static_cast<uint32_t>(g.num_long);
         x.num_chunks = static_cast<uint32_t>(g.num_chunks);
+        x.num_hot = g.num_hot;
         a.residual = reinterpret_cast<double *>(take((it + 2) * 8));
         a.dangling = reinterpret_cast<double *>(take((it + 2) * 8));
+        x.block_sums = reinterpret_cast<double2 *>(take(kEndBlocks * 16));
+        x.end_ticket = reinterpret_cast<uint32_t *>(take(16));
+        for (int i = 0; i < 2; ++i) x.hot_contrib[i] = reinterpret_cast<float *>(take(uint64_t(g.num_hot) * 4 + 16));
         a.num_tiles = g.num_tiles;
         a.num_chunks = static_cast<uint32_t>(g.num_chunks);
         a.V = static_cast<uint32_t>(V);
@@ -582,13 +712,24 @@ void QueryEngine::ensure_hub_capacity() {
     args_dirty_ = true;
 }
 
+namespace {
+int occupancy(const void *f, int smem) {
+    int per_sm = 0;
+    HYT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f, kWorkThreads, smem));
+    return std::max(per_sm, 1);
+}
+}  // namespace
+
+int QueryEngine::ppr_grid() const {
+    static int per_sm = 0;
+    if (per_sm == 0) per_sm = occupancy(reinterpret_cast<const void *>(engine_ppr_kernel), ppr_kernel_smem(kMaxSlots));
+    return sm_count() * per_sm;
+}
+
 int QueryEngine::work_grid() const {
     static int per_sm = 0;
-    if (per_sm == 0) {
-        HYT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, engine_work_kernel, kWorkThreads,
-                                                               work_kernel_smem(kMaxSlots)));
-        per_sm = std::max(per_sm, 1);
-    }
+    if (per_sm == 0)
+        per_sm = occupancy(reinterpret_cast<const void *>(engine_sssp_kernel), sssp_kernel_smem(kMaxSlots));
     const int c = tuning_.ctas_per_sm ? std::min<int>(static_cast<int>(tuning_.ctas_per_sm), per_sm) : per_sm;
     return sm_count() * c;
 }
@@ -600,9 +741,11 @@ void QueryEngine::upload_args(bool use_cond) {
     a.ss = h.d_ss.get();
     a.pr = h.d_pr.get();
     a.px = h.d_px.get();
+    a.rvs = h.d_rvs.get();
     a.n = hi_;
     a.hub_degree = std::max<uint32_t>(tuning_.hub_degree, 1);
-    a.unit_base = unit_base_.get();
+    a.ss_base = unit_base_.get();
+    a.pr_base = unit_base_.get() + cap_ + 1;
     a.hubs = hubs_.get();
     a.hub_cap = static_cast<uint32_t>(std::min<uint64_t>(hubs_.count, 0xFFFFFFFFull));
     a.max_supersteps = max_supersteps_;
@@ -620,9 +763,10 @@ void QueryEngine::launch_superstep_kernels(cudaStream_t s) {
     const EngineArgs *d = d_args_.get();
     engine_split_kernel<<<dim3(kSplitBlocks, cap_), 256, 0, s>>>(d);
     engine_prep_kernel<<<1, 1024, 0, s>>>(d);
-    engine_work_kernel<<<grid, kWorkThreads, work_kernel_smem(cap_), s>>>(d);
+    engine_sssp_kernel<<<grid, kWorkThreads, sssp_kernel_smem(cap_), s>>>(d);
+    engine_ppr_kernel<<<ppr_grid(), kWorkThreads, ppr_kernel_smem(cap_), s>>>(d);
     engine_hub_kernel<<<grid, kWorkThreads, 0, s>>>(d);
-    engine_end_kernel<<<cap_, 256, 0, s>>>(d);
+    engine_end_kernel<<<dim3(kEndBlocks, cap_), 256, 0, s>>>(d);
     engine_cond_kernel<<<1, 1, 0, s>>>(d);
     HYT_CUDA(cudaGetLastError());
 }
@@ -638,10 +782,12 @@ void QueryEngine::add_superstep_nodes(cudaGraph_t body, int grid) {
     const K ks[] = {
         {reinterpret_cast<void *>(engine_split_kernel), dim3(kSplitBlocks, cap_), dim3(256), 0u},
         {reinterpret_cast<void *>(engine_prep_kernel), dim3(1), dim3(1024), 0u},
-        {reinterpret_cast<void *>(engine_work_kernel), dim3(grid), dim3(kWorkThreads),
-         static_cast<unsigned>(work_kernel_smem(cap_))},
+        {reinterpret_cast<void *>(engine_sssp_kernel), dim3(grid), dim3(kWorkThreads),
+         static_cast<unsigned>(sssp_kernel_smem(cap_))},
+        {reinterpret_cast<void *>(engine_ppr_kernel), dim3(ppr_grid()), dim3(kWorkThreads),
+         static_cast<unsigned>(ppr_kernel_smem(cap_))},
         {reinterpret_cast<void *>(engine_hub_kernel), dim3(grid), dim3(kWorkThreads), 0u},
-        {reinterpret_cast<void *>(engine_end_kernel), dim3(cap_), dim3(256), 0u},
+        {reinterpret_cast<void *>(engine_end_kernel), dim3(kEndBlocks, cap_), dim3(256), 0u},
         {reinterpret_cast<void *>(engine_cond_kernel), dim3(1), dim3(1), 0u},
     };
     cudaGraphNode_t prev = nullptr;
@@ -713,7 +859,7 @@ uint32_t QueryEngine::run_to_completion(bool use_graph) {
         cap = std::max(cap, c + 1);
     }
     max_supersteps_ = static_cast<uint32_t>(std::min<uint64_t>(cap, 0x7FFFFFFFull));
-    HYT_CUDA(cudaMemsetAsync(counters_.get(), 0, 16, stream_));
+    HYT_CUDA(cudaMemsetAsync(counters_.get(), 0, 32, stream_));
     uint32_t steps = 0;
     EngineHost &h = *host_;
     if (use_graph) {
@@ -730,7 +876,7 @@ uint32_t QueryEngine::run_to_completion(bool use_graph) {
         upload_args(false);
         for (;;) {
             launch_superstep_kernels(stream_);
-            launches_ += 6;
+            launches_ += 7;
             engine_status_kernel<<<(hi_ + 255) / 256, 256, 0, stream_>>>(d_args_.get(), h.d_status.get());
             uint32_t c[4] = {0, 0, 0, 0};
             HYT_CUDA(cudaMemcpyAsync(c, counters_.get(), 16, cudaMemcpyDeviceToHost, stream_));
@@ -753,7 +899,7 @@ void QueryEngine::run_supersteps(uint32_t n) {
     max_supersteps_ = 0x7FFFFFFF;
     upload_args(false);
     for (uint32_t i = 0; i < n; ++i) launch_superstep_kernels(stream_);
-    launches_ += 6ull * n;
+    launches_ += 7ull * n;
 }
 
 std::vector<std::pair<int, uint64_t>> QueryEngine::finished() {

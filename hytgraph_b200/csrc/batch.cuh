@@ -114,6 +114,7 @@ private:
     void upload_args(bool use_cond);
     void launch_superstep_kernels(cudaStream_t s);
     int work_grid() const;
+    int ppr_grid() const;
 
     int device_;
     cudaStream_t stream_;

