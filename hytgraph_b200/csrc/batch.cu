@@ -245,7 +245,7 @@ __device__ __forceinline__ void flush_relaxed(const SSArgs &a, unsigned long lon
 // SSSP frontier blocks of every SSSP slot.  Warps take kGrab consecutive
 // units at a time; a slot's arguments are reloaded only when the slot
 // changes.
-__global__ void __launch_bounds__(kWorkThreads, 4) engine_sssp_kernel(const EngineArgs *__restrict__ eap) {
+__global__ void __launch_bounds__(kWorkThreads, 3) engine_sssp_kernel(const EngineArgs *__restrict__ eap) {
     extern __shared__ __align__(16) uint32_t s_base[];
     const EngineArgs ea = *eap;
     const uint32_t n = ea.n;
@@ -330,7 +330,7 @@ __global__ void __launch_bounds__(kWorkThreads) engine_ppr_kernel(const EngineAr
     }
 }
 
-__global__ void __launch_bounds__(kWorkThreads, 4) engine_hub_kernel(const EngineArgs *__restrict__ eap) {
+__global__ void __launch_bounds__(kWorkThreads, 3) engine_hub_kernel(const EngineArgs *__restrict__ eap) {
     const EngineArgs ea = *eap;
     const uint32_t n = min(*(volatile uint32_t *)&ea.counters[0], ea.hub_cap);
     const int lane = threadIdx.x & 31;

@@ -23,7 +23,14 @@ constexpr int kSSThreads = 256;
 constexpr uint32_t kHubDegree = 64;   // rows at least this long become warp tasks
 constexpr uint32_t kHubChunk = 512;   // edges per warp task
 constexpr uint32_t kNoDelta = 0xFFFFFFFFu;
-constexpr int kEdgeBatch = 4;  // 32-edge batches in flight per warp
+#ifndef HYT_SS_EXPAND_BATCH
+#define HYT_SS_EXPAND_BATCH 8
+#endif
+#ifndef HYT_SS_HUB_BATCH
+#define HYT_SS_HUB_BATCH 8
+#endif
+constexpr int kEdgeBatch = HYT_SS_EXPAND_BATCH;  // 32-edge batches in flight per warp (short rows)
+constexpr int kHubBatch = HYT_SS_HUB_BATCH;      // the same for hub tasks
 
 struct SSHeader {
     uint32_t round;      // rounds completed
@@ -261,10 +268,10 @@ __device__ __forceinline__ void hub_chunk(const SSArgs &a, const RoundView &rv, 
     const uint64_t b = rb + uint64_t(c) * kHubChunk;
     const uint32_t len = static_cast<uint32_t>(((b + kHubChunk < re) ? b + kHubChunk : re) - b);
     const uint32_t d = __ldcg(a.dist + v);
-    for (uint32_t base = 0; base < len; base += 32 * kEdgeBatch) {
-        uint32_t u[kEdgeBatch], nd[kEdgeBatch], du[kEdgeBatch];
+    for (uint32_t base = 0; base < len; base += 32 * kHubBatch) {
+        uint32_t u[kHubBatch], nd[kHubBatch], du[kHubBatch];
 #pragma unroll
-        for (int k = 0; k < kEdgeBatch; ++k) {
+        for (int k = 0; k < kHubBatch; ++k) {
             const uint32_t j = base + 32 * k + lane;
             u[k] = 0;
             nd[k] = a.inf;
@@ -274,8 +281,8 @@ __device__ __forceinline__ void hub_chunk(const SSArgs &a, const RoundView &rv, 
             }
         }
 #pragma unroll
-        for (int k = 0; k < kEdgeBatch; ++k) du[k] = __ldcg(a.dist + u[k]);
-        relax_batch<kEdgeBatch>(a, rv, u, nd, du, lane, improved);
+        for (int k = 0; k < kHubBatch; ++k) du[k] = __ldcg(a.dist + u[k]);
+        relax_batch<kHubBatch>(a, rv, u, nd, du, lane, improved);
     }
 }
 
