@@ -193,7 +193,7 @@ void graph_copy_csc(const GraphImpl &g, uint64_t *in_offsets, uint32_t *in_sourc
 
 size_t GraphImpl::device_bytes() const {
     size_t b = row_offsets.bytes() + cols.bytes() + weights.bytes() + out_degree.bytes() + in_offsets.bytes() +
-               in_sources.bytes() + tile_start.bytes() + long_rows.bytes() + chunk_tasks.bytes();
+               in_sources.bytes() + in_weights.bytes() + tile_start.bytes() + long_rows.bytes() + chunk_tasks.bytes();
     for (int i = 0; i < 2; ++i) b += rank[i].bytes() + contrib[i].bytes() + queue[i].bytes() + far[i].bytes();
     b += partial.bytes() + ticket.bytes() + pr_state.bytes() + dist.bytes() + stamp.bytes() + hub_tasks.bytes() +
          sssp_state.bytes();
@@ -341,14 +341,32 @@ void graph_build(GraphImpl &g, const hyt_csr &csr, uint32_t flags) {
 
     if (flags & HYT_GRAPH_PULL) {
         // CSC transpose: stable sort of (destination, source) by destination.
+        // Graphs that keep both sides with weights also get the weights in
+        // CSC order (SSSP pull rounds): sort edge ids instead, then gather.
         DeviceArray<uint32_t> keys(E ? E : 1);
         g.in_sources.allocate(E ? E : 1);
+        const bool csc_weights = (flags & HYT_GRAPH_PUSH) && keep_weights && g.weights.get();
         if (E) {
             HYT_CUDA(cudaMemcpyAsync(keys.get(), g.cols.get(), E * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
             const unsigned blocks = static_cast<unsigned>(std::min<uint64_t>((V + 255) / 256, 148ull * 64));
-            expand_sources_kernel<<<blocks, 256, 0, s>>>(g.row_offsets.get(), V, g.in_sources.get());
-            HYT_CUDA(cudaGetLastError());
-            prims::sort_pairs_u32(keys.get(), g.in_sources.get(), E, bits_for(V - 1), s);
+            if (csc_weights) {
+                DeviceArray<uint32_t> perm(E);
+                iota_kernel<<<grid_for(E, 256), 256, 0, s>>>(perm.get(), E);
+                HYT_CUDA(cudaGetLastError());
+                prims::sort_pairs_u32(keys.get(), perm.get(), E, bits_for(V - 1), s);
+                DeviceArray<uint32_t> src(E);
+                expand_sources_kernel<<<blocks, 256, 0, s>>>(g.row_offsets.get(), V, src.get());
+                HYT_CUDA(cudaGetLastError());
+                gather_u32_kernel<<<grid_for(E, 256), 256, 0, s>>>(src.get(), perm.get(), E, g.in_sources.get());
+                g.in_weights.allocate(E);
+                gather_u32_kernel<<<grid_for(E, 256), 256, 0, s>>>(g.weights.get(), perm.get(), E, g.in_weights.get());
+                HYT_CUDA(cudaGetLastError());
+                HYT_CUDA(cudaStreamSynchronize(s));
+            } else {
+                expand_sources_kernel<<<blocks, 256, 0, s>>>(g.row_offsets.get(), V, g.in_sources.get());
+                HYT_CUDA(cudaGetLastError());
+                prims::sort_pairs_u32(keys.get(), g.in_sources.get(), E, bits_for(V - 1), s);
+            }
         }
         g.in_offsets.allocate(V + 1);
         offsets_from_sorted_kernel<<<grid_for(E + 1, 256), 256, 0, s>>>(keys.get(), E, V, g.in_offsets.get());

@@ -60,6 +60,7 @@ struct GraphImpl {
     // pull side
     DeviceArray<uint64_t> in_offsets;
     DeviceArray<uint32_t> in_sources;
+    DeviceArray<uint32_t> in_weights;   // [E] weights in CSC order (PUSH|PULL weighted graphs; SSSP pull rounds)
     DeviceArray<uint32_t> tile_start;   // [num_tiles + 1]
     DeviceArray<LongRow> long_rows;     // [num_long]
     DeviceArray<uint2> chunk_tasks;     // [num_chunks] = (long row index, chunk)

@@ -30,6 +30,7 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -62,7 +63,7 @@ __global__ void __launch_bounds__(kSSThreads) sssp_split_kernel(const SSArgs *__
 template <int WK, bool HYB = false>
 __global__ void __launch_bounds__(kSSThreads) sssp_expand_kernel(const SSArgs *__restrict__ args) {
     const SSArgs a = *args;
-    if (*(volatile uint32_t *)&a.hdr->done) return;
+    if (*(volatile uint32_t *)&a.hdr->done || pull_round(a)) return;
     const RoundView rv = round_view(a);
     const int lane = threadIdx.x & 31;
     const uint32_t gwarp = (blockIdx.x * kSSThreads + threadIdx.x) >> 5;
@@ -83,7 +84,7 @@ __global__ void __launch_bounds__(kSSThreads) sssp_expand_kernel(const SSArgs *_
 template <int WK, bool HYB = false>
 __global__ void __launch_bounds__(kSSThreads) sssp_hub_kernel(const SSArgs *__restrict__ args) {
     const SSArgs a = *args;
-    if (*(volatile uint32_t *)&a.hdr->done) return;
+    if (*(volatile uint32_t *)&a.hdr->done || pull_round(a)) return;
     const RoundView rv = round_view(a);
     const uint32_t n = *(volatile uint32_t *)&a.hdr->hub_count;
     const int lane = threadIdx.x & 31;
@@ -99,6 +100,158 @@ __global__ void __launch_bounds__(kSSThreads) sssp_hub_kernel(const SSArgs *__re
             hw = L.weights;
         }
         hub_chunk<WK>(a, rv, hc, hw, h.x, h.y, lane, improved);
+    }
+}
+
+// ---- pull sweeps (direction-optimised rounds) ------------------------------
+//
+// A round whose frontier carries more than E / pull_div out-edges is run as
+// a sweep over the CSC instead: every vertex takes the minimum of
+// d[u] + w(u, v) over its in-edges (no atomics on the edge path, streaming
+// reads of ids and weights, label gathers from L2), and improved vertices
+// form the next frontier.  Any label-correcting schedule reaches the same
+// fixed point, so distances are unchanged.  Single-bucket solves only.
+
+// CSC of the graph for pull sweeps (PageRank's tiles and long-row chunks).
+struct PullGraph {
+    const uint64_t *in_off;
+    const uint32_t *in_src;   // hot sources tagged kHotTag | slot
+    const uint32_t *in_w;     // weights in CSC order (NULL when unweighted)
+    const uint32_t *tile_start;
+    const LongRow *long_rows;
+    const uint2 *chunk_tasks;
+    const uint32_t *hot_vertex;
+    uint64_t num_tiles, num_chunks;
+    uint32_t tile_cost;
+};
+
+// Out-edges of the current frontier (for the push / pull decision).
+__global__ void __launch_bounds__(kSSThreads) sssp_frontier_edges_kernel(const SSArgs *__restrict__ args) {
+    const SSArgs a = *args;
+    if (*(volatile uint32_t *)&a.hdr->done) return;
+    const RoundView rv = round_view(a);
+    unsigned long long sum = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < rv.qn; i += gridDim.x * blockDim.x) {
+        const uint32_t v = rv.q[i];
+        sum += a.row_off[v + 1] - a.row_off[v];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    if ((threadIdx.x & 31) == 0 && sum) atomicAdd(&a.hdr->frontier_edges, sum);
+}
+
+// Candidate label of in-edge e: d[u] + w, or infinity when u is unreached.
+template <int WK>
+__device__ __forceinline__ uint32_t pull_candidate(const SSArgs &a, const PullGraph &pg, uint32_t u, uint64_t e) {
+    if (u & kHotTag) u = pg.hot_vertex[u & ~kHotTag];
+    const uint32_t du = __ldcg(a.dist + u);
+    if (du == a.inf) return a.inf;
+    return extend<WK>(du, edge_weight<WK>(pg.in_w, e));
+}
+
+// Lowers row r's label to c if that improves it; returns true when r joins
+// the next frontier for the first time this round.
+__device__ __forceinline__ bool pull_relax(const SSArgs &a, const RoundView &rv, uint32_t r, uint32_t c) {
+    if (c >= __ldcg(a.dist + r)) return false;
+    const uint32_t old = atomicMin(a.dist + r, c);
+    if (c >= old) return false;
+    return atomicExch(a.stamp + r, rv.next_stamp) != rv.next_stamp;
+}
+
+template <int WK>
+__global__ void __launch_bounds__(kSSThreads) sssp_pull_kernel(const SSArgs *__restrict__ args, PullGraph pg) {
+    extern __shared__ __align__(16) uint32_t s_cand[];
+    const SSArgs a = *args;
+    if (*(volatile uint32_t *)&a.hdr->done || !pull_round(a)) return;
+    const RoundView rv = round_view(a);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t *sv = s_cand + warp * (2 * pg.tile_cost + 8);
+    const uint64_t total = pg.num_chunks + pg.num_tiles;
+    const uint64_t gwarp = (uint64_t(blockIdx.x) * kSSThreads + threadIdx.x) >> 5;
+    const uint64_t nwarps = (uint64_t(gridDim.x) * kSSThreads) >> 5;
+    constexpr int B = 8;  // edges in flight per lane
+    for (uint64_t task = gwarp; task < total; task += nwarps) {
+        if (task < pg.num_chunks) {
+            // slice of a long row: warp minimum, then one relaxation
+            const uint2 t = pg.chunk_tasks[task];
+            const LongRow L = pg.long_rows[t.x];
+            const uint64_t rb = pg.in_off[L.row], re = pg.in_off[L.row + 1];
+            const uint64_t lo = rb + uint64_t(t.y) * kLongChunk;
+            const uint64_t hi = (lo + kLongChunk < re) ? lo + kLongChunk : re;
+            uint32_t best = a.inf;
+            for (uint64_t b0 = lo; b0 < hi; b0 += 32 * B) {
+                uint32_t id[B];
+#pragma unroll
+                for (int k = 0; k < B; ++k) {
+                    const uint64_t e = b0 + 32 * k + lane;
+                    id[k] = (e < hi) ? dev::ld_stream(pg.in_src + e) : 0u;
+                }
+#pragma unroll
+                for (int k = 0; k < B; ++k) {
+                    const uint64_t e = b0 + 32 * k + lane;
+                    if (e < hi) best = min(best, pull_candidate<WK>(a, pg, id[k], e));
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(0xffffffffu, best, o));
+            if (lane == 0 && pull_relax(a, rv, L.row, best)) append(rv.qnext, rv.qnext_size, L.row);
+        } else {
+            // merge-path tile of short rows: candidates staged per edge
+            const uint64_t k = task - pg.num_chunks;
+            const uint32_t r0 = pg.tile_start[k], r1 = pg.tile_start[k + 1];
+            if (r0 == r1) continue;
+            const uint64_t last_b = pg.in_off[r1 - 1], last_e = pg.in_off[r1];
+            const uint32_t rl = (last_e - last_b >= pg.tile_cost) ? r1 - 1 : r1;  // long last row is chunked
+            const uint64_t e0 = pg.in_off[r0];
+            const uint64_t e1 = (rl == r1) ? last_e : last_b;
+            const uint32_t n = static_cast<uint32_t>(e1 - e0);
+            for (uint32_t b0 = 0; b0 < n; b0 += 32 * B) {
+                uint32_t id[B];
+#pragma unroll
+                for (int j = 0; j < B; ++j) {
+                    const uint32_t i = b0 + 32 * j + lane;
+                    id[j] = (i < n) ? dev::ld_stream(pg.in_src + e0 + i) : 0u;
+                }
+#pragma unroll
+                for (int j = 0; j < B; ++j) {
+                    const uint32_t i = b0 + 32 * j + lane;
+                    if (i < n) sv[i] = pull_candidate<WK>(a, pg, id[j], e0 + i);
+                }
+            }
+            __syncwarp();
+            for (uint32_t rb = r0; rb < rl; rb += 32) {
+                const uint32_t r = rb + lane;
+                const bool active = r < rl;
+                const uint64_t lo = active ? pg.in_off[r] : 0;
+                const uint64_t hi = active ? pg.in_off[r + 1] : 0;
+                bool joined = false;
+                if (active && hi - lo < 16) {
+                    uint32_t best = a.inf;
+                    for (uint64_t x = lo; x < hi; ++x) best = min(best, sv[x - e0]);
+                    joined = pull_relax(a, rv, r, best);
+                }
+                uint32_t big = __ballot_sync(0xffffffffu, active && (hi - lo >= 16));
+                while (big) {
+                    const int src = __ffs(big) - 1;
+                    big &= big - 1;
+                    const uint64_t bb = __shfl_sync(0xffffffffu, lo, src);
+                    const uint64_t ee = __shfl_sync(0xffffffffu, hi, src);
+                    uint32_t best = a.inf;
+                    for (uint64_t x = bb + lane; x < ee; x += 32) best = min(best, sv[x - e0]);
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(0xffffffffu, best, o));
+                    const bool j = (lane == 0) && pull_relax(a, rv, rb + src, best);
+                    if (__shfl_sync(0xffffffffu, j ? 1u : 0u, 0) && lane == src) joined = true;
+                }
+                const uint32_t vals[1] = {r};
+                warp_append<1>(rv.qnext, rv.qnext_size, vals, joined ? 1u : 0u, lane);
+            }
+            __syncwarp();
+        }
+    }
+    if (gwarp == 0 && lane == 0) {
+        atomicAdd(&a.hdr->relaxations, static_cast<unsigned long long>(a.num_edges));
+        atomicAdd(&a.hdr->pull_rounds, 1u);
     }
 }
 
@@ -221,6 +374,28 @@ __global__ void __launch_bounds__(kSSThreads) sssp_expand_packed_kernel(const SS
     if (lane == 0 && relaxed) atomicAdd(&a.hdr->relaxations, relaxed);
 }
 
+// Pull sweeps when the frontier's out-edges exceed E / div (env
+// HYT_SSSP_PULL_DIV, 0 = never; default 4: a sweep reads every in-edge once,
+// which costs about what pushing a quarter of them does).
+uint32_t sssp_pull_div() {
+    static uint32_t div = [] {
+        const char *e = std::getenv("HYT_SSSP_PULL_DIV");
+        return e ? static_cast<uint32_t>(std::strtoul(e, nullptr, 10)) : 4u;
+    }();
+    return div;
+}
+
+template <int WK>
+int pull_grid(unsigned smem) {
+    static int g = 0;
+    if (g == 0) {
+        int per_sm = 0;
+        HYT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sssp_pull_kernel<WK>, kSSThreads, smem));
+        g = sm_count() * std::max(per_sm, 1);
+    }
+    return g;
+}
+
 template <int WK>
 int expand_grid() {
     static int g = 0;
@@ -266,6 +441,26 @@ void sssp_solve(GraphImpl &g, uint32_t source, uint32_t delta, uint32_t max_roun
     a.V = static_cast<uint32_t>(V);
     a.source = source;
     a.inf = (WK == HYT_WEIGHTS_F32) ? 0x7F800000u : HYT_DIST_INF_U32;
+    a.num_edges = g.E;
+    // pull sweeps need the CSC (and its weights) and a single bucket
+    const bool pull_ok = (g.flags & HYT_GRAPH_PULL) && (WK == HYT_WEIGHTS_NONE || g.in_weights.get()) &&
+                         delta == kNoDelta && g.E > 0;
+    a.pull_div = pull_ok ? sssp_pull_div() : 0u;
+    PullGraph pg{};
+    if (a.pull_div) {
+        pg.in_off = g.in_offsets.get();
+        pg.in_src = g.in_sources.get();
+        pg.in_w = g.in_weights.get();
+        pg.tile_start = g.tile_start.get();
+        pg.long_rows = g.long_rows.get();
+        pg.chunk_tasks = g.chunk_tasks.get();
+        pg.hot_vertex = g.hot_vertex.get();
+        pg.num_tiles = g.num_tiles;
+        pg.num_chunks = g.num_chunks;
+        pg.tile_cost = g.tile_cost;
+    }
+    const unsigned pull_smem = static_cast<unsigned>(kSSThreads / 32 * (2 * size_t(g.tile_cost) + 8) * 4);
+    const int pgrid = a.pull_div ? pull_grid<WK>(pull_smem) : 0;
 
     SSHeader h0{};
     h0.qsize[0] = 1;
@@ -306,17 +501,23 @@ void sssp_solve(GraphImpl &g, uint32_t source, uint32_t delta, uint32_t max_roun
         kp.kernelParams = kargs;
         kp.blockDim = dim3(kSSThreads);
         kp.gridDim = dim3(grid);
-        cudaGraphNode_t n0, n1, n2, n3;
-        kp.func = reinterpret_cast<void *>(sssp_split_kernel);
-        HYT_CUDA(cudaGraphAddKernelNode(&n0, body, nullptr, 0, &kp));
-        kp.func = reinterpret_cast<void *>(sssp_expand_kernel<WK>);
-        HYT_CUDA(cudaGraphAddKernelNode(&n1, body, &n0, 1, &kp));
-        kp.func = reinterpret_cast<void *>(sssp_hub_kernel<WK>);
-        HYT_CUDA(cudaGraphAddKernelNode(&n2, body, &n1, 1, &kp));
-        kp.func = reinterpret_cast<void *>(sssp_round_end_kernel);
-        kp.gridDim = dim3(1);
-        kp.blockDim = dim3(1);
-        HYT_CUDA(cudaGraphAddKernelNode(&n3, body, &n2, 1, &kp));
+        cudaGraphNode_t prev = nullptr, node;
+        auto add = [&](const void *f, dim3 gd, dim3 bd, unsigned smem, void **params) {
+            kp.func = const_cast<void *>(f);
+            kp.gridDim = gd;
+            kp.blockDim = bd;
+            kp.sharedMemBytes = smem;
+            kp.kernelParams = params;
+            HYT_CUDA(cudaGraphAddKernelNode(&node, body, prev ? &prev : nullptr, prev ? 1 : 0, &kp));
+            prev = node;
+        };
+        void *pargs[] = {&d_args, &pg};
+        add(reinterpret_cast<void *>(sssp_split_kernel), dim3(grid), dim3(kSSThreads), 0, kargs);
+        if (a.pull_div) add(reinterpret_cast<void *>(sssp_frontier_edges_kernel), dim3(grid), dim3(kSSThreads), 0, kargs);
+        add(reinterpret_cast<void *>(sssp_expand_kernel<WK>), dim3(grid), dim3(kSSThreads), 0, kargs);
+        add(reinterpret_cast<void *>(sssp_hub_kernel<WK>), dim3(grid), dim3(kSSThreads), 0, kargs);
+        if (a.pull_div) add(reinterpret_cast<void *>(sssp_pull_kernel<WK>), dim3(pgrid), dim3(kSSThreads), pull_smem, pargs);
+        add(reinterpret_cast<void *>(sssp_round_end_kernel), dim3(1), dim3(1), 0, kargs);
         HYT_CUDA(cudaGraphInstantiate(&exec, graph, 0));
         HYT_CUDA(cudaGraphLaunch(exec, s));
     } else {
@@ -324,13 +525,15 @@ void sssp_solve(GraphImpl &g, uint32_t source, uint32_t delta, uint32_t max_roun
         for (uint32_t r = 0; r < max_rounds; ++r) {
             if (flags & HYT_RUN_PROFILE) kt.start(s);
             sssp_split_kernel<<<grid, kSSThreads, 0, s>>>(d_args);
+            if (a.pull_div) sssp_frontier_edges_kernel<<<grid, kSSThreads, 0, s>>>(d_args);
             sssp_expand_kernel<WK><<<grid, kSSThreads, 0, s>>>(d_args);
             sssp_hub_kernel<WK><<<grid, kSSThreads, 0, s>>>(d_args);
+            if (a.pull_div) sssp_pull_kernel<WK><<<pgrid, kSSThreads, pull_smem, s>>>(d_args, pg);
             if (flags & HYT_RUN_PROFILE) kt.stop(s);
             sssp_round_end_kernel<<<1, 1, 0, s>>>(d_args);
             HYT_CUDA(cudaGetLastError());
-            launches += 4;
-            hot += 3;
+            launches += a.pull_div ? 6 : 4;
+            hot += a.pull_div ? 5 : 3;
             uint32_t done = 0;
             HYT_CUDA(cudaMemcpyAsync(&done, &hdr->done, sizeof(done), cudaMemcpyDeviceToHost, s));
             HYT_CUDA(cudaStreamSynchronize(s));

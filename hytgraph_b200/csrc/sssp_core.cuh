@@ -47,6 +47,9 @@ struct SSHeader {
     uint32_t max_rounds;
     unsigned long long relaxations;     // edges relaxed
     unsigned long long frontier_total;  // frontier vertices expanded
+    unsigned long long frontier_edges;  // out-edges of this round's frontier (pull-capable solves)
+    uint32_t pull_rounds;               // rounds run as pull sweeps
+    uint32_t pad;
 };
 
 struct SSArgs {
@@ -67,7 +70,18 @@ struct SSArgs {
     cudaGraphConditionalHandle cond;
     const EdgeLoc *loc;   // per-partition edge location (partitioned solves)
     uint32_t part_shift;  // partition of vertex v = v >> part_shift
+    uint32_t pull_div;    // > 0: a round whose frontier has more than E / pull_div out-edges is a pull sweep
+    uint64_t num_edges;
 };
+
+// True when this round runs as a pull sweep over the CSC instead of a push
+// expansion (decided from the frontier's out-edge count, identically by
+// every kernel of the round).
+__device__ __forceinline__ bool pull_round(const SSArgs &a) {
+    if (!a.pull_div) return false;
+    const unsigned long long fe = *(volatile const unsigned long long *)&a.hdr->frontier_edges;
+    return fe * a.pull_div > a.num_edges;
+}
 
 template <int WK>
 __device__ __forceinline__ uint32_t edge_weight(const uint32_t *w, uint64_t e) {
@@ -319,6 +333,7 @@ __device__ __forceinline__ bool round_end(SSHeader *h) {
     h->frontier_total += h->qsize[r & 1];
     h->qsize[r & 1] = 0;
     h->hub_count = 0;
+    h->frontier_edges = 0;
     h->round = r + 1;
     if (h->pending) {  // the split of this round consumed the old far pile
         h->fsize[h->phase & 1] = 0;
