@@ -161,17 +161,26 @@ def barrier(pg):
 
     if pg is not None:
         pg.barrier()
-    torch.cuda.synchronize()
+    if torch.cuda.is_available():
+        torch.cuda.synchronize()
 
 
 def max_over_ranks(pg, x: float) -> float:
+    """Max of a per-rank timing over all ranks (NCCL on GPUs; any backend)."""
     import torch
 
     if pg is None:
         return x
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    on_gpu = pg.get_backend() == "nccl"
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if on_gpu else "cpu")
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_value(units_per_rank: float, world: int, ms_max: float) -> float:
+    """Whole-job throughput of weak-scaled replicas: every rank processes
+    units_per_rank, the job takes the slowest rank's time."""
+    return units_per_rank * world / (ms_max / 1e3)
 
 
 # --------------------------------------------------------------------------
@@ -713,7 +722,7 @@ def main():
     ms = max_over_ranks(pg, ms_local)
     pr_it = sum(s["iterations"] for s in timed["pr"])
     traversed = E * pr_it + E * len(timed["sssp"])
-    value = traversed * world / (ms / 1e3) / 1e9
+    value = replica_value(traversed, world, ms) / 1e9
 
     # roofline: dominant kernel of the step (PageRank iteration vs SSSP rounds)
     pr_ms = sum(s["device_ms"] for s in timed["pr"])
