@@ -197,23 +197,25 @@ __device__ __forceinline__ void two_sum(float a, float b, float &s, float &e) {
     e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bp)), __fsub_rn(b, bp));
 }
 
-// Compensated accumulator (Kahan-Babuska/Neumaier): value = s + c.
+// Compensated accumulator: Kahan summation per element (4 adds; c holds
+// the negated low-order part, value = s - c), TwoSum when two partial sums
+// merge (warp reductions, long-row chunks).
 struct CSum {
     float s = 0.f;
     float c = 0.f;
     __device__ __forceinline__ void add(float x) {
-        float t, e;
-        two_sum(s, x, t, e);
+        const float y = __fsub_rn(x, c);
+        const float t = __fadd_rn(s, y);
+        c = __fsub_rn(__fsub_rn(t, s), y);
         s = t;
-        c = __fadd_rn(c, e);
     }
     __device__ __forceinline__ void merge(const CSum &o) {
         float t, e;
-        two_sum(s, o.s, t, e);
+        two_sum(s, o.s, t, e);  // s + o.s = t + e exactly
         s = t;
-        c = __fadd_rn(__fadd_rn(c, o.c), e);
+        c = __fsub_rn(__fadd_rn(c, o.c), e);
     }
-    __device__ __forceinline__ float value() const { return __fadd_rn(s, c); }
+    __device__ __forceinline__ float value() const { return __fsub_rn(s, c); }
 };
 
 __device__ __forceinline__ CSum warp_reduce(CSum v) {
