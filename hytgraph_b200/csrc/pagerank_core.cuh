@@ -16,7 +16,10 @@
 namespace hyt {
 namespace prc {
 
-constexpr uint32_t kWarpRowDegree = 16;  // rows with more in-edges are summed by a whole warp
+#ifndef HYT_PR_WARP_ROW
+#define HYT_PR_WARP_ROW 64
+#endif
+constexpr uint32_t kWarpRowDegree = HYT_PR_WARP_ROW;  // rows with more in-edges are summed by a whole warp
 
 struct PRHeader {
     uint32_t iter;       // iterations completed
