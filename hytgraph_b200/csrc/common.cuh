@@ -190,6 +190,14 @@ __device__ __forceinline__ float ld_keep(const float *p, uint64_t pol) {
     return v;
 }
 
+// Coherent 32-bit load with an L2 cache-eviction policy (for data other
+// threads may update during the kernel).
+__device__ __forceinline__ uint32_t ld_keep_u32(const uint32_t *p, uint64_t pol) {
+    uint32_t v;
+    asm volatile("ld.global.L2::cache_hint.b32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
+    return v;
+}
+
 // Error-free transformation (Knuth TwoSum): a + b = s + e exactly.
 __device__ __forceinline__ void two_sum(float a, float b, float &s, float &e) {
     s = __fadd_rn(a, b);

@@ -95,7 +95,10 @@ __device__ __forceinline__ void finalize_row(const PRArgs &a, const PRState &ps,
 // instruction are ascending and neighbouring lanes often share an L2 sector
 // (dense for hub-heavy rows).  All kBatch gathers of a lane are issued
 // before any is consumed.  Edges past hi yield 0 and read a clamped address.
-constexpr int kBatch = 16;
+#ifndef HYT_PR_BATCH
+#define HYT_PR_BATCH 16
+#endif
+constexpr int kBatch = HYT_PR_BATCH;
 
 // kSmemHot: hot sources (tagged ids) read their contribution from the
 // CTA's shared-memory copy s_hot; otherwise from ccur[hot_vertex[slot]].

@@ -123,6 +123,7 @@ struct PullGraph {
     const uint32_t *hot_vertex;
     uint64_t num_tiles, num_chunks;
     uint32_t tile_cost;
+    uint32_t num_hot;
 };
 
 // Out-edges of the current frontier (for the push / pull decision).
@@ -140,15 +141,6 @@ __global__ void __launch_bounds__(kSSThreads) sssp_frontier_edges_kernel(const S
     if ((threadIdx.x & 31) == 0 && sum) atomicAdd(&a.hdr->frontier_edges, sum);
 }
 
-// Candidate label of in-edge e: d[u] + w, or infinity when u is unreached.
-template <int WK>
-__device__ __forceinline__ uint32_t pull_candidate(const SSArgs &a, const PullGraph &pg, uint32_t u, uint64_t e) {
-    if (u & kHotTag) u = pg.hot_vertex[u & ~kHotTag];
-    const uint32_t du = __ldcg(a.dist + u);
-    if (du == a.inf) return a.inf;
-    return extend<WK>(du, edge_weight<WK>(pg.in_w, e));
-}
-
 // Lowers row r's label to c if that improves it; returns true when r joins
 // the next frontier for the first time this round.
 __device__ __forceinline__ bool pull_relax(const SSArgs &a, const RoundView &rv, uint32_t r, uint32_t c) {
@@ -158,19 +150,55 @@ __device__ __forceinline__ bool pull_relax(const SSArgs &a, const RoundView &rv,
     return atomicExch(a.stamp + r, rv.next_stamp) != rv.next_stamp;
 }
 
+// Candidate labels d[u] + w of in-edges [lo, hi), kPullBatch per lane in
+// flight: all ids and weights, hot slots mapped to vertex ids through the
+// CTA's shared-memory table, all labels gathered evict-last from L2, then
+// the sink.  Unreached sources give infinity.
+constexpr int kPullBatch = 8;
+
+template <int WK, class Sink>
+__device__ __forceinline__ void pull_span(const SSArgs &a, const PullGraph &pg, const uint32_t *s_hot, uint64_t lo,
+                                          uint64_t hi, uint64_t pol, int lane, Sink &&sink) {
+    const uint32_t n = static_cast<uint32_t>(hi - lo);
+    for (uint32_t base = 0; base < n; base += 32 * kPullBatch) {
+        uint32_t id[kPullBatch], w[kPullBatch], du[kPullBatch];
+#pragma unroll
+        for (int k = 0; k < kPullBatch; ++k) {
+            const uint32_t i = base + 32 * k + lane;
+            id[k] = (i < n) ? dev::ld_stream(pg.in_src + lo + i) : 0u;
+            w[k] = (i < n) ? edge_weight<WK>(pg.in_w, lo + i) : 0u;
+        }
+#pragma unroll
+        for (int k = 0; k < kPullBatch; ++k)
+            if (id[k] & kHotTag) id[k] = s_hot[id[k] & ~kHotTag];  // hot slot -> vertex id
+#pragma unroll
+        for (int k = 0; k < kPullBatch; ++k) du[k] = dev::ld_keep_u32(a.dist + id[k], pol);
+#pragma unroll
+        for (int k = 0; k < kPullBatch; ++k) {
+            const uint32_t i = base + 32 * k + lane;
+            if (i < n) sink(i, du[k] == a.inf ? a.inf : extend<WK>(du[k], w[k]));
+        }
+    }
+}
+
+constexpr int kPullThreads = 1024;  // one CTA per SM, like the PageRank kernel
+
 template <int WK>
-__global__ void __launch_bounds__(kSSThreads) sssp_pull_kernel(const SSArgs *__restrict__ args, PullGraph pg) {
-    extern __shared__ __align__(16) uint32_t s_cand[];
+__global__ void __launch_bounds__(kPullThreads, 1) sssp_pull_kernel(const SSArgs *__restrict__ args, PullGraph pg) {
+    extern __shared__ __align__(16) uint32_t s_dyn_u[];
     const SSArgs a = *args;
     if (*(volatile uint32_t *)&a.hdr->done || !pull_round(a)) return;
     const RoundView rv = round_view(a);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint32_t *sv = s_cand + warp * (2 * pg.tile_cost + 8);
+    // vertex ids of the hot slots (tagged sources in the CSC)
+    uint32_t *s_hot = s_dyn_u;
+    for (uint32_t i = threadIdx.x; i < pg.num_hot; i += blockDim.x) s_hot[i] = pg.hot_vertex[i];
+    __syncthreads();
+    uint32_t *sv = s_dyn_u + pg.num_hot + warp * (2 * pg.tile_cost + 8);
+    const uint64_t pol = dev::policy_evict_last();
     const uint64_t total = pg.num_chunks + pg.num_tiles;
-    const uint64_t gwarp = (uint64_t(blockIdx.x) * kSSThreads + threadIdx.x) >> 5;
-    const uint64_t nwarps = (uint64_t(gridDim.x) * kSSThreads) >> 5;
-    constexpr int B = 8;  // edges in flight per lane
-    for (uint64_t task = gwarp; task < total; task += nwarps) {
+    const uint64_t nwarps = uint64_t(gridDim.x) * (kPullThreads / 32);
+    for (uint64_t task = uint64_t(blockIdx.x) * (kPullThreads / 32) + warp; task < total; task += nwarps) {
         if (task < pg.num_chunks) {
             // slice of a long row: warp minimum, then one relaxation
             const uint2 t = pg.chunk_tasks[task];
@@ -179,19 +207,7 @@ __global__ void __launch_bounds__(kSSThreads) sssp_pull_kernel(const SSArgs *__r
             const uint64_t lo = rb + uint64_t(t.y) * kLongChunk;
             const uint64_t hi = (lo + kLongChunk < re) ? lo + kLongChunk : re;
             uint32_t best = a.inf;
-            for (uint64_t b0 = lo; b0 < hi; b0 += 32 * B) {
-                uint32_t id[B];
-#pragma unroll
-                for (int k = 0; k < B; ++k) {
-                    const uint64_t e = b0 + 32 * k + lane;
-                    id[k] = (e < hi) ? dev::ld_stream(pg.in_src + e) : 0u;
-                }
-#pragma unroll
-                for (int k = 0; k < B; ++k) {
-                    const uint64_t e = b0 + 32 * k + lane;
-                    if (e < hi) best = min(best, pull_candidate<WK>(a, pg, id[k], e));
-                }
-            }
+            pull_span<WK>(a, pg, s_hot, lo, hi, pol, lane, [&](uint32_t, uint32_t c) { best = min(best, c); });
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(0xffffffffu, best, o));
             if (lane == 0 && pull_relax(a, rv, L.row, best)) append(rv.qnext, rv.qnext_size, L.row);
@@ -204,20 +220,7 @@ __global__ void __launch_bounds__(kSSThreads) sssp_pull_kernel(const SSArgs *__r
             const uint32_t rl = (last_e - last_b >= pg.tile_cost) ? r1 - 1 : r1;  // long last row is chunked
             const uint64_t e0 = pg.in_off[r0];
             const uint64_t e1 = (rl == r1) ? last_e : last_b;
-            const uint32_t n = static_cast<uint32_t>(e1 - e0);
-            for (uint32_t b0 = 0; b0 < n; b0 += 32 * B) {
-                uint32_t id[B];
-#pragma unroll
-                for (int j = 0; j < B; ++j) {
-                    const uint32_t i = b0 + 32 * j + lane;
-                    id[j] = (i < n) ? dev::ld_stream(pg.in_src + e0 + i) : 0u;
-                }
-#pragma unroll
-                for (int j = 0; j < B; ++j) {
-                    const uint32_t i = b0 + 32 * j + lane;
-                    if (i < n) sv[i] = pull_candidate<WK>(a, pg, id[j], e0 + i);
-                }
-            }
+            pull_span<WK>(a, pg, s_hot, e0, e1, pol, lane, [&](uint32_t i, uint32_t c) { sv[i] = c; });
             __syncwarp();
             for (uint32_t rb = r0; rb < rl; rb += 32) {
                 const uint32_t r = rb + lane;
@@ -225,12 +228,12 @@ __global__ void __launch_bounds__(kSSThreads) sssp_pull_kernel(const SSArgs *__r
                 const uint64_t lo = active ? pg.in_off[r] : 0;
                 const uint64_t hi = active ? pg.in_off[r + 1] : 0;
                 bool joined = false;
-                if (active && hi - lo < 16) {
+                if (active && hi - lo < 64) {
                     uint32_t best = a.inf;
                     for (uint64_t x = lo; x < hi; ++x) best = min(best, sv[x - e0]);
                     joined = pull_relax(a, rv, r, best);
                 }
-                uint32_t big = __ballot_sync(0xffffffffu, active && (hi - lo >= 16));
+                uint32_t big = __ballot_sync(0xffffffffu, active && (hi - lo >= 64));
                 while (big) {
                     const int src = __ffs(big) - 1;
                     big &= big - 1;
@@ -249,7 +252,7 @@ __global__ void __launch_bounds__(kSSThreads) sssp_pull_kernel(const SSArgs *__r
             __syncwarp();
         }
     }
-    if (gwarp == 0 && lane == 0) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
         atomicAdd(&a.hdr->relaxations, static_cast<unsigned long long>(a.num_edges));
         atomicAdd(&a.hdr->pull_rounds, 1u);
     }
@@ -387,13 +390,15 @@ uint32_t sssp_pull_div() {
 
 template <int WK>
 int pull_grid(unsigned smem) {
-    static int g = 0;
-    if (g == 0) {
-        int per_sm = 0;
-        HYT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sssp_pull_kernel<WK>, kSSThreads, smem));
-        g = sm_count() * std::max(per_sm, 1);
+    static bool attr = false;
+    if (!attr) {
+        HYT_CUDA(cudaFuncSetAttribute(sssp_pull_kernel<WK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(kPRSmemMax)));
+        attr = true;
     }
-    return g;
+    int per_sm = 0;
+    HYT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sssp_pull_kernel<WK>, kPullThreads, smem));
+    return sm_count() * std::max(per_sm, 1);
 }
 
 template <int WK>
@@ -458,8 +463,10 @@ void sssp_solve(GraphImpl &g, uint32_t source, uint32_t delta, uint32_t max_roun
         pg.num_tiles = g.num_tiles;
         pg.num_chunks = g.num_chunks;
         pg.tile_cost = g.tile_cost;
+        pg.num_hot = g.num_hot;
     }
-    const unsigned pull_smem = static_cast<unsigned>(kSSThreads / 32 * (2 * size_t(g.tile_cost) + 8) * 4);
+    const unsigned pull_smem =
+        static_cast<unsigned>((g.num_hot + kPullThreads / 32 * (2 * size_t(g.tile_cost) + 8)) * 4);
     const int pgrid = a.pull_div ? pull_grid<WK>(pull_smem) : 0;
 
     SSHeader h0{};
@@ -516,7 +523,7 @@ void sssp_solve(GraphImpl &g, uint32_t source, uint32_t delta, uint32_t max_roun
         if (a.pull_div) add(reinterpret_cast<void *>(sssp_frontier_edges_kernel), dim3(grid), dim3(kSSThreads), 0, kargs);
         add(reinterpret_cast<void *>(sssp_expand_kernel<WK>), dim3(grid), dim3(kSSThreads), 0, kargs);
         add(reinterpret_cast<void *>(sssp_hub_kernel<WK>), dim3(grid), dim3(kSSThreads), 0, kargs);
-        if (a.pull_div) add(reinterpret_cast<void *>(sssp_pull_kernel<WK>), dim3(pgrid), dim3(kSSThreads), pull_smem, pargs);
+        if (a.pull_div) add(reinterpret_cast<void *>(sssp_pull_kernel<WK>), dim3(pgrid), dim3(kPullThreads), pull_smem, pargs);
         add(reinterpret_cast<void *>(sssp_round_end_kernel), dim3(1), dim3(1), 0, kargs);
         HYT_CUDA(cudaGraphInstantiate(&exec, graph, 0));
         HYT_CUDA(cudaGraphLaunch(exec, s));
@@ -528,7 +535,7 @@ void sssp_solve(GraphImpl &g, uint32_t source, uint32_t delta, uint32_t max_roun
             if (a.pull_div) sssp_frontier_edges_kernel<<<grid, kSSThreads, 0, s>>>(d_args);
             sssp_expand_kernel<WK><<<grid, kSSThreads, 0, s>>>(d_args);
             sssp_hub_kernel<WK><<<grid, kSSThreads, 0, s>>>(d_args);
-            if (a.pull_div) sssp_pull_kernel<WK><<<pgrid, kSSThreads, pull_smem, s>>>(d_args, pg);
+            if (a.pull_div) sssp_pull_kernel<WK><<<pgrid, kPullThreads, pull_smem, s>>>(d_args, pg);
             if (flags & HYT_RUN_PROFILE) kt.stop(s);
             sssp_round_end_kernel<<<1, 1, 0, s>>>(d_args);
             HYT_CUDA(cudaGetLastError());
