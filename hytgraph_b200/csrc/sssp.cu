@@ -154,7 +154,10 @@ __device__ __forceinline__ bool pull_relax(const SSArgs &a, const RoundView &rv,
 // flight: all ids and weights, hot slots mapped to vertex ids through the
 // CTA's shared-memory table, all labels gathered evict-last from L2, then
 // the sink.  Unreached sources give infinity.
-constexpr int kPullBatch = 8;
+#ifndef HYT_PULL_BATCH
+#define HYT_PULL_BATCH 16
+#endif
+constexpr int kPullBatch = HYT_PULL_BATCH;
 
 template <int WK, class Sink>
 __device__ __forceinline__ void pull_span(const SSArgs &a, const PullGraph &pg, const uint32_t *s_hot, uint64_t lo,
