@@ -10,9 +10,9 @@ there is no CPU fallback.
 """
 from . import capi
 from .capi import HytError, device_count
-from .graph import CSR, Batch, DeviceCSR, Graph, HybridGraph, PinnedBuffer, Server, pick_sources, rmat
+from .graph import CSR, Batch, DeviceCSR, Graph, HybridGraph, PinnedBuffer, Server, hub_sort, pick_sources, reorder, rmat
 
 __all__ = [
     "capi", "HytError", "device_count", "CSR", "Batch", "DeviceCSR", "Graph", "HybridGraph", "PinnedBuffer", "Server",
-    "pick_sources", "rmat",
+    "hub_sort", "pick_sources", "reorder", "rmat",
 ]

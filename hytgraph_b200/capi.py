@@ -357,6 +357,8 @@ _SIGNATURES = [
      [C.c_void_p, C.POINTER(hyt_completion), C.c_uint32, C.POINTER(C.c_uint32), C.c_uint32]),
     ("hyt_server_get_stats", C.c_int, [C.c_void_p, C.POINTER(hyt_server_stats)]),
     ("hyt_server_destroy", C.c_int, [C.c_void_p]),
+    ("hyt_hub_sort", C.c_int, [C.POINTER(hyt_csr), C.c_double, C.c_void_p, C.c_void_p, C.POINTER(C.c_uint64)]),
+    ("hyt_csr_reorder", C.c_int, [C.POINTER(hyt_csr), C.c_void_p, C.c_int, C.POINTER(hyt_csr_buffers)]),
     ("hyt_rmat_generate", C.c_int, [C.POINTER(hyt_rmat_params), C.c_int, C.POINTER(hyt_csr_buffers)]),
     ("hyt_csr_buffers_free", C.c_int, [C.POINTER(hyt_csr_buffers)]),
     ("hyt_pick_sources", C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint32, C.c_void_p]),

@@ -269,6 +269,23 @@ int hyt_csr_buffers_free(hyt_csr_buffers *b) {
     });
 }
 
+int hyt_hub_sort(const hyt_csr *csr, double hub_fraction, uint32_t *vertex_order, double *scores,
+                 uint64_t *hub_count) {
+    return guarded([&] {
+        if (!csr) fail(HYT_E_INVALID, "csr is NULL");
+        require_device();
+        hub_sort(*csr, hub_fraction, vertex_order, scores, hub_count);
+    });
+}
+
+int hyt_csr_reorder(const hyt_csr *csr, const uint32_t *vertex_order, int on_device, hyt_csr_buffers *out) {
+    return guarded([&] {
+        if (!csr) fail(HYT_E_INVALID, "csr is NULL");
+        require_device();
+        csr_reorder(*csr, vertex_order, on_device != 0, out);
+    });
+}
+
 int hyt_pick_sources(const uint64_t *row_offsets, uint64_t num_vertices, uint64_t seed, uint32_t count,
                      uint32_t *out) {
     return guarded([&] { pick_sources(row_offsets, num_vertices, seed, count, out); });

@@ -51,6 +51,23 @@ void sort_pairs_desc_u32(uint32_t *keys, uint32_t *vals, size_t n, cudaStream_t 
     HYT_CUDA(cudaStreamSynchronize(s));
 }
 
+void sort_pairs_desc_u64(uint64_t *keys, uint32_t *vals, size_t n, cudaStream_t s) {
+    if (n < 2) return;
+    DeviceArray<uint64_t> k2(n);
+    DeviceArray<uint32_t> v2(n);
+    cub::DoubleBuffer<uint64_t> kb(keys, k2.get());
+    cub::DoubleBuffer<uint32_t> vb(vals, v2.get());
+    size_t tb = 0;
+    HYT_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, kb, vb, static_cast<int64_t>(n), 0, 64, s));
+    TempStorage tmp(tb);
+    HYT_CUDA(cub::DeviceRadixSort::SortPairsDescending(tmp.ptr, tb, kb, vb, static_cast<int64_t>(n), 0, 64, s));
+    if (kb.Current() != keys)
+        HYT_CUDA(cudaMemcpyAsync(keys, kb.Current(), n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
+    if (vb.Current() != vals)
+        HYT_CUDA(cudaMemcpyAsync(vals, vb.Current(), n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+    HYT_CUDA(cudaStreamSynchronize(s));
+}
+
 void sort_keys_u64(uint64_t *keys, size_t n, int end_bit, cudaStream_t s) {
     if (n < 2) return;
     DeviceArray<uint64_t> k2(n);
@@ -110,17 +127,21 @@ size_t select_flagged_index(const uint8_t *flags, uint32_t *out, size_t n, cudaS
     return static_cast<size_t>(h);
 }
 
-uint32_t reduce_max_u32(const uint32_t *in, size_t n, cudaStream_t s) {
+template <class T>
+T reduce_max(const T *in, size_t n, cudaStream_t s) {
     if (n == 0) return 0;
-    DeviceArray<uint32_t> r(1);
+    DeviceArray<T> r(1);
     size_t tb = 0;
     HYT_CUDA(cub::DeviceReduce::Max(nullptr, tb, in, r.get(), static_cast<int64_t>(n), s));
     TempStorage tmp(tb);
     HYT_CUDA(cub::DeviceReduce::Max(tmp.ptr, tb, in, r.get(), static_cast<int64_t>(n), s));
-    uint32_t h = 0;
+    T h = 0;
     HYT_CUDA(cudaMemcpyAsync(&h, r.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
     HYT_CUDA(cudaStreamSynchronize(s));
     return h;
 }
+
+uint32_t reduce_max_u32(const uint32_t *in, size_t n, cudaStream_t s) { return reduce_max(in, n, s); }
+uint64_t reduce_max_u64(const uint64_t *in, size_t n, cudaStream_t s) { return reduce_max(in, n, s); }
 
 }  // namespace hyt::prims

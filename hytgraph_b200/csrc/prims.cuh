@@ -18,6 +18,9 @@ void sort_pairs_u32(uint32_t *keys, uint32_t *vals, size_t n, int end_bit, cudaS
 // Same, descending by key (stable: equal keys keep their input order).
 void sort_pairs_desc_u32(uint32_t *keys, uint32_t *vals, size_t n, cudaStream_t s);
 
+// Stable descending sort of (u64 key, u32 value) pairs, in place.
+void sort_pairs_desc_u64(uint64_t *keys, uint32_t *vals, size_t n, cudaStream_t s);
+
 // Radix sort of 64-bit keys on bits [0, end_bit), in place.
 void sort_keys_u64(uint64_t *keys, size_t n, int end_bit, cudaStream_t s);
 
@@ -33,5 +36,6 @@ size_t select_flagged_index(const uint8_t *flags, uint32_t *out, size_t n, cudaS
 
 // Max of a u32 array (0 for n == 0).
 uint32_t reduce_max_u32(const uint32_t *in, size_t n, cudaStream_t s);
+uint64_t reduce_max_u64(const uint64_t *in, size_t n, cudaStream_t s);
 
 }  // namespace hyt::prims

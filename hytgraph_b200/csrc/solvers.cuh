@@ -13,4 +13,8 @@ void sssp_noalloc(const hyt_csr &csr, uint32_t source, uint32_t *dist_out, void 
 void rmat_generate(const hyt_rmat_params &p, bool on_device, hyt_csr_buffers *out);
 void pick_sources(const uint64_t *row_offsets, uint64_t V, uint64_t seed, uint32_t count, uint32_t *out);
 
+// Hub sorting / vertex reordering (reorder.cu).
+void hub_sort(const hyt_csr &csr, double fraction, uint32_t *order_out, double *scores_out, uint64_t *hub_count);
+void csr_reorder(const hyt_csr &csr, const uint32_t *vertex_order, bool on_device, hyt_csr_buffers *out);
+
 }  // namespace hyt

@@ -14,7 +14,7 @@ from typing import Optional
 import numpy as np
 
 from . import capi
-from .capi import check, lib
+from .capi import HytError, check, lib
 
 RMAT_A, RMAT_B, RMAT_C = 0.57, 0.19, 0.19
 
@@ -77,6 +77,7 @@ class DeviceCSR:
     """A CSR whose arrays live in device memory (owned by the library)."""
 
     buffers: capi.hyt_csr_buffers
+    weight_kind: int = capi.HYT_WEIGHTS_U32  # of the weights, when present
 
     @property
     def num_vertices(self) -> int:
@@ -94,7 +95,7 @@ class DeviceCSR:
         c.row_offsets = C.cast(b.row_offsets, C.c_void_p).value
         c.column_indices = C.cast(b.column_indices, C.c_void_p).value
         c.weights = C.cast(b.weights, C.c_void_p).value if b.weights else 0
-        c.weight_kind = capi.HYT_WEIGHTS_U32 if b.weights else capi.HYT_WEIGHTS_NONE
+        c.weight_kind = self.weight_kind if b.weights else capi.HYT_WEIGHTS_NONE
         return c
 
     def download(self, row_offsets=None, column_indices=None, weights=None) -> CSR:
@@ -106,7 +107,8 @@ class DeviceCSR:
         cols = np.empty(E, np.uint32) if column_indices is None else column_indices
         w = None
         if b.weights:
-            w = np.empty(E, np.uint32) if weights is None else weights
+            w = np.empty(E, np.float32 if self.weight_kind == capi.HYT_WEIGHTS_F32 else np.uint32) \
+                if weights is None else weights
         capi.copy(_ptr(off), C.cast(b.row_offsets, C.c_void_p).value, (V + 1) * 8)
         if E:
             capi.copy(_ptr(cols), C.cast(b.column_indices, C.c_void_p).value, E * 4)
@@ -506,3 +508,38 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def hub_sort(csr, hub_fraction: float = 0.08):
+    """Hub-first vertex order on the GPU (hyt_hub_sort): returns
+    (vertex_order uint32[V], scores float64[V], hub_count)."""
+    c = csr.to_c()
+    V = int(c.num_vertices)
+    order = np.empty(V, np.uint32)
+    scores = np.empty(V, np.float64)
+    n = C.c_uint64()
+    check(lib.hyt_hub_sort(C.byref(c), hub_fraction, _ptr(order), _ptr(scores), C.byref(n)))
+    return order, scores, n.value
+
+
+def reorder(csr, vertex_order, device: bool = False):
+    """CSRGraph::reorder_vertices on the GPU (hyt_csr_reorder): a host CSR,
+    or a DeviceCSR when device=True."""
+    c = csr.to_c()
+    order = np.ascontiguousarray(vertex_order, np.uint32)
+    if order.shape != (csr.num_vertices,):
+        raise HytError(capi.HYT_E_INVALID,
+                       "CSRGraph::reorder_vertices: vertex_order must contain exactly one entry per vertex")
+    b = capi.hyt_csr_buffers()
+    check(lib.hyt_csr_reorder(C.byref(c), _ptr(order), 1 if device else 0, C.byref(b)))
+    if device:
+        return DeviceCSR(b, csr.weight_kind)
+    V, E = int(b.num_vertices), int(b.num_edges)
+    off = np.ctypeslib.as_array(b.row_offsets, shape=(V + 1,)).copy()
+    cols = np.ctypeslib.as_array(b.column_indices, shape=(max(E, 1),))[:E].copy() if E else np.zeros(0, np.uint32)
+    w = None
+    if b.weights:
+        wa = np.ctypeslib.as_array(b.weights, shape=(max(E, 1),))[:E].copy()
+        w = wa.view(np.float32) if csr.weight_kind == capi.HYT_WEIGHTS_F32 else wa
+    check(lib.hyt_csr_buffers_free(C.byref(b)))
+    return CSR(off, cols, w)

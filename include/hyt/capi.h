@@ -460,6 +460,29 @@ int hyt_csr_buffers_free(hyt_csr_buffers *buffers);
 int hyt_pick_sources(const uint64_t *row_offsets, uint64_t num_vertices,
                      uint64_t seed, uint32_t count, uint32_t *out);
 
+/* ------------------------------------------------------------------ */
+/* Hub sorting and vertex reordering on the GPU                         */
+/* ------------------------------------------------------------------ */
+
+/* Hub-first vertex order of scheduling::HubSorter::sort
+ * (src/scheduling/hub_sort.cpp:28-183): scores H(v) = Do(v) * Di(v) /
+ * (Do_max * Di_max); the round-or-ceil(V * hub_fraction) best first (ties:
+ * lower id), then the other vertices in id order.  csr: host or device
+ * arrays.  vertex_order[V] (new -> old), scores[V] (may be NULL) and
+ * *hub_count (may be NULL): host or device.  Scores are correctly rounded
+ * double quotients (the reference rounds a long-double quotient; the two can
+ * differ in the last place), the order is the reference's exactly. */
+int hyt_hub_sort(const hyt_csr *csr, double hub_fraction, uint32_t *vertex_order, double *scores,
+                 uint64_t *hub_count);
+
+/* graph::CSRGraph::reorder_vertices (src/graph/csr_graph.cpp:171-283) into
+ * new buffers: vertex_order[new] = old; each new row holds the old row's
+ * edges in their original order with destinations renamed, weights carried.
+ * on_device: 1 = cudaMalloc'd output, 0 = malloc'd; free with
+ * hyt_csr_buffers_free.  Rejects out-of-range or duplicate entries with the
+ * reference's messages. */
+int hyt_csr_reorder(const hyt_csr *csr, const uint32_t *vertex_order, int on_device, hyt_csr_buffers *out);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

@@ -123,6 +123,31 @@ class Oracle:
         return top[:n], teng[:nt], tfirst[:nt]
 
 
+    def hub_sort(self, off, cols, fraction=0.08):
+        V, E = off.shape[0] - 1, cols.shape[0]
+        order = np.empty(max(V, 1), np.uint32)
+        scores = np.empty(max(V, 1), np.float64)
+        n = C.c_uint64()
+        rc = self.lib.oracle_hub_sort(C.c_uint64(V), C.c_uint64(E), _p(off), _p(cols), C.c_double(fraction),
+                                      _p(order), _p(scores), C.byref(n))
+        if rc:
+            raise ValueError(f"oracle_hub_sort rc={rc}")
+        return order[:V], scores[:V], n.value
+
+    def reorder(self, off, cols, w, order):
+        """w: any 4-byte weight array or None; returns (offsets, columns, weights)."""
+        V, E = off.shape[0] - 1, cols.shape[0]
+        o = np.empty(V + 1, np.uint64)
+        c = np.empty(max(E, 1), np.uint32)
+        wo = np.empty(max(E, 1), np.uint32) if w is not None else None
+        rc = self.lib.oracle_reorder(C.c_uint64(V), C.c_uint64(E), _p(off), _p(cols),
+                                     _p(w.view(np.uint32)) if w is not None else None,
+                                     _p(np.ascontiguousarray(order, np.uint32)), _p(o), _p(c), _p(wo))
+        if rc:
+            raise ValueError(f"oracle_reorder rc={rc}")
+        return o, c[:E], (wo[:E].view(w.dtype) if w is not None else None)
+
+
 class Reference:
     """The reference's own CPU implementation (oracle/_ref/libhytref.so)."""
 
@@ -188,3 +213,23 @@ class Reference:
         self._check(self.lib.ref_task_combine(_p(e), C.c_uint64(n), C.c_uint64(k), _p(top), _p(teng), _p(tfirst),
                                               C.byref(nt), _p(metrics)), "ref_task_combine")
         return top[:n], teng[:nt.value], tfirst[:nt.value], metrics
+
+    def hub_sort(self, off, cols, fraction=0.08):
+        V, E = off.shape[0] - 1, cols.shape[0]
+        order = np.empty(V, np.uint32)
+        scores = np.empty(V, np.float64)
+        n = C.c_uint64()
+        self._check(self.lib.ref_hub_sort(C.c_uint64(V), C.c_uint64(E), _p(off), _p(cols), C.c_double(fraction),
+                                          _p(order), _p(scores), C.byref(n)), "ref_hub_sort")
+        return order, scores, n.value
+
+    def reorder(self, off, cols, w_f32, order):
+        V, E = off.shape[0] - 1, cols.shape[0]
+        o = np.empty(V + 1, np.uint64)
+        c = np.empty(max(E, 1), np.uint32)
+        w = np.empty(max(E, 1), np.float32) if w_f32 is not None else None
+        self._check(self.lib.ref_reorder(C.c_uint64(V), C.c_uint64(E), _p(off), _p(cols),
+                                         _p(w_f32) if w_f32 is not None else None,
+                                         _p(np.ascontiguousarray(order, np.uint32)), _p(o), _p(c),
+                                         _p(w) if w is not None else None), "ref_reorder")
+        return o, c[:E], (w[:E] if w is not None else None)

@@ -376,3 +376,87 @@ uint64_t oracle_task_combine(const int *engines, uint64_t n, uint64_t k, uint64_
     free(rank); free(tmp_first); free(tmp_engine); free(tmp_task);
     return ntask;
 }
+
+/* Hub sort, restating src/scheduling/hub_sort.cpp:28-183:
+ *   in-degree from the destination array, H(v) = Do*Di / (Do_max*Di_max)
+ *   in long double rounded to double (0 for an edgeless graph), hub count
+ *   round(V*f) when within 1e-12 of an integer else ceil(V*f), capped at V;
+ *   ranking by higher score, then lower id; hubs first, then every other
+ *   vertex in id order.  Returns 0, or ORACLE_E_INVALID for a fraction
+ *   outside [0, 1] (HubSorter's constructor, hub_sort.cpp:10-20). */
+static const double *g_hub_scores;
+static int hub_rank_cmp(const void *pa, const void *pb) {
+    const uint32_t a = *(const uint32_t *)pa, b = *(const uint32_t *)pb;
+    const double sa = g_hub_scores[a], sb = g_hub_scores[b];
+    if (sa != sb) return sa > sb ? -1 : 1;
+    return a < b ? -1 : (a > b);
+}
+
+int oracle_hub_sort(uint64_t V, uint64_t E, const uint64_t *off, const uint32_t *cols, double fraction,
+                    uint32_t *order, double *scores, uint64_t *hub_count) {
+    if (!isfinite(fraction) || fraction < 0.0 || fraction > 1.0) return ORACLE_E_INVALID;
+    *hub_count = 0;
+    if (V == 0) return 0;
+    uint64_t *indeg = (uint64_t *)calloc(V, sizeof(uint64_t));
+    uint32_t *ranked = (uint32_t *)malloc(V * sizeof(uint32_t));
+    unsigned char *hub = (unsigned char *)calloc(V, 1);
+    if (!indeg || !ranked || !hub) { free(indeg); free(ranked); free(hub); return ORACLE_E_NOMEM; }
+    for (uint64_t e = 0; e < E; ++e) ++indeg[cols[e]];
+    uint64_t max_out = 0, max_in = 0;
+    for (uint64_t v = 0; v < V; ++v) {
+        const uint64_t od = off[v + 1] - off[v];
+        if (od > max_out) max_out = od;
+        if (indeg[v] > max_in) max_in = indeg[v];
+    }
+    const long double den = (long double)max_out * (long double)max_in;
+    for (uint64_t v = 0; v < V; ++v) {
+        const long double num = (long double)(off[v + 1] - off[v]) * (long double)indeg[v];
+        scores[v] = den > 0.0L ? (double)(num / den) : 0.0;
+    }
+    const long double req = (long double)V * (long double)fraction;
+    const long double rnd = roundl(req);
+    const long double pick = fabsl(req - rnd) < 1e-12L ? rnd : ceill(req);
+    uint64_t hubs = (uint64_t)pick;
+    if (hubs > V) hubs = V;
+    for (uint64_t v = 0; v < V; ++v) ranked[v] = (uint32_t)v;
+    g_hub_scores = scores;
+    qsort(ranked, V, sizeof(uint32_t), hub_rank_cmp); /* total order: stability not needed */
+    uint64_t n = 0;
+    for (uint64_t r = 0; r < hubs; ++r) { hub[ranked[r]] = 1; order[n++] = ranked[r]; }
+    for (uint64_t v = 0; v < V; ++v)
+        if (!hub[v]) order[n++] = (uint32_t)v;
+    *hub_count = hubs;
+    free(indeg); free(ranked); free(hub);
+    return 0;
+}
+
+/* Vertex reordering, restating src/graph/csr_graph.cpp:171-283:
+ * order[new] = old must be a permutation (ORACLE_E_INVALID otherwise:
+ * out-of-range id, or duplicate id); row `new` takes old row `old`'s edges
+ * in order, destinations renamed through the inverse permutation, weights
+ * (any 4-byte type; w may be NULL) carried along. */
+int oracle_reorder(uint64_t V, uint64_t E, const uint64_t *off, const uint32_t *cols, const uint32_t *w,
+                   const uint32_t *order, uint64_t *off_out, uint32_t *cols_out, uint32_t *w_out) {
+    uint32_t *inv = (uint32_t *)malloc((V ? V : 1) * sizeof(uint32_t));
+    unsigned char *seen = (unsigned char *)calloc(V ? V : 1, 1);
+    if (!inv || !seen) { free(inv); free(seen); return ORACLE_E_NOMEM; }
+    for (uint64_t nv = 0; nv < V; ++nv) {
+        const uint32_t old = order[nv];
+        if (old >= V || seen[old]) { free(inv); free(seen); return ORACLE_E_INVALID; }
+        seen[old] = 1;
+        inv[old] = (uint32_t)nv;
+    }
+    uint64_t k = 0;
+    off_out[0] = 0;
+    for (uint64_t nv = 0; nv < V; ++nv) {
+        const uint32_t old = order[nv];
+        for (uint64_t e = off[old]; e < off[old + 1]; ++e, ++k) {
+            cols_out[k] = inv[cols[e]];
+            if (w && w_out) w_out[k] = w[e];
+        }
+        off_out[nv + 1] = k;
+    }
+    (void)E;
+    free(inv); free(seen);
+    return 0;
+}

@@ -43,6 +43,10 @@ void oracle_hytm_partition(const uint64_t *off, const unsigned char *active, uin
 int oracle_select_engine(double f, double c, double z, double alpha, double beta);
 uint64_t oracle_task_combine(const int *engines, uint64_t n, uint64_t k, uint64_t *task_of_partition,
                              int *task_engine, uint64_t *task_first);
+int oracle_hub_sort(uint64_t V, uint64_t E, const uint64_t *off, const uint32_t *cols, double fraction,
+                    uint32_t *order, double *scores, uint64_t *hub_count);
+int oracle_reorder(uint64_t V, uint64_t E, const uint64_t *off, const uint32_t *cols, const uint32_t *w,
+                   const uint32_t *order, uint64_t *off_out, uint32_t *cols_out, uint32_t *w_out);
 
 #ifdef __cplusplus
 }

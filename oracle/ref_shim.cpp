@@ -12,6 +12,7 @@
 #include "graph/activity_tracker.hpp"
 #include "graph/csr_graph.hpp"
 #include "graph/partition.hpp"
+#include "scheduling/hub_sort.hpp"
 #include "scheduling/task_combiner.hpp"
 #include "transfer/compaction_engine.hpp"
 #include "transfer/filter_engine.hpp"
@@ -157,6 +158,33 @@ int ref_task_combine(const int *engines, uint64_t n, uint64_t k, uint64_t *task_
         metrics[2] = plan.metrics.filter_partitions_combined;
         metrics[3] = plan.metrics.compaction_partitions_combined;
         metrics[4] = plan.metrics.zero_copy_partitions_combined;
+    })
+}
+
+// HubSorter::sort: vertex_order[V], scores[V], hub_count.
+int ref_hub_sort(uint64_t V, uint64_t E, const uint64_t *off, const uint32_t *cols, double fraction,
+                 uint32_t *order, double *scores, uint64_t *hub_count) {
+    REF_GUARD({
+        const auto g = make_graph(V, E, off, cols, nullptr);
+        hytgraph::scheduling::HubSortOptions o;
+        o.hub_fraction = fraction;
+        const auto r = hytgraph::scheduling::HubSorter(o).sort(g);
+        for (uint64_t i = 0; i < r.vertex_order.size(); ++i) order[i] = r.vertex_order[i];
+        for (uint64_t i = 0; i < r.scores.size(); ++i) scores[i] = r.scores[i];
+        *hub_count = r.hub_count;
+    })
+}
+
+// CSRGraph::reorder_vertices: outputs the reordered arrays (w may be NULL).
+int ref_reorder(uint64_t V, uint64_t E, const uint64_t *off, const uint32_t *cols, const float *w,
+                const uint32_t *order, uint64_t *off_out, uint32_t *cols_out, float *w_out) {
+    REF_GUARD({
+        auto g = make_graph(V, E, off, cols, w);
+        g.reorder_vertices(std::vector<uint32_t>(order, order + V));
+        for (uint64_t v = 0; v <= V; ++v) off_out[v] = g.row_offsets()[v];
+        for (uint64_t e = 0; e < E; ++e) cols_out[e] = g.column_indices()[e];
+        if (w && w_out)
+            for (uint64_t e = 0; e < E; ++e) w_out[e] = g.edge_weights()[e];
     })
 }
 

@@ -11,7 +11,10 @@ Fixtures:
       bits) / iterations from seeded sources.
   known_answers.json -- the reference's hand-written known-answer cases
       (tests/algorithm_tests.cpp:22-157, tests/cuda_algorithm_tests.cu:23-87,
-      tests/unit_tests.cpp:2058-2204, 2268-2466) evaluated by the reference.
+      tests/unit_tests.cpp:2058-2204, 2268-2466) evaluated by the reference,
+      the hub-sort and reorder cases (unit_tests.cpp:2468-2740), and per
+      R-MAT graph the reference HubSorter's order / scores digests and hub
+      count at hub_fraction 0.08 plus the digest of the CSR reordered by it.
 """
 from __future__ import annotations
 
@@ -62,10 +65,19 @@ def main() -> None:
             dists.append(d.view(np.uint32))
             rounds.append(r)
         arrays[f"{key}_sssp_bits"] = np.stack(dists)
+        order, scores, hubs = ref.hub_sort(g.row_offsets, g.column_indices, 0.08)
+        # u32 weights travel through the reference's float array bit for bit
+        r_off, r_cols, r_w = ref.reorder(g.row_offsets, g.column_indices,
+                                         None if g.weights is None else g.weights.view(np.float32), order)
+        reordered = hyt.CSR(r_off, r_cols, None if r_w is None else r_w.view(np.uint32))
         meta.append({"key": key, "scale": scale, "edge_factor": ef, "seed": seed, "weighted": weighted,
                      "num_vertices": g.num_vertices, "num_edges": g.num_edges, "csr_sha256": csr_digest(g),
                      "pr_iterations": it, "pr_residual": float(res), "pr_converged": conv,
-                     "sources": [int(s) for s in srcs], "source_seed": seed + 100, "sssp_rounds": rounds})
+                     "sources": [int(s) for s in srcs], "source_seed": seed + 100, "sssp_rounds": rounds,
+                     "hub_fraction": 0.08, "hub_count": int(hubs),
+                     "hub_order_sha256": hashlib.sha256(order.astype("<u4").tobytes()).hexdigest(),
+                     "hub_scores_sha256": hashlib.sha256(scores.astype("<f8").tobytes()).hexdigest(),
+                     "reordered_sha256": csr_digest(reordered)})
     np.savez_compressed(OUT / "rmat_reference.npz", **arrays)
 
     # Hand-written graphs from the reference's tests, evaluated by the reference.
@@ -109,9 +121,30 @@ def main() -> None:
         top, teng, tfirst, m = ref.task_combine(engines, k)
         combiner.append({"engines": engines, "k": k, "task_of_partition": top.tolist(),
                          "task_engine": teng.tolist(), "task_first": tfirst.tolist(), "metrics": m.tolist()})
+    # Hub sorting (unit_tests.cpp:2468-2602, 2709-2740) and reordering
+    # (unit_tests.cpp:2604-2707), evaluated by the reference.
+    hub = []
+    for name, off, cols, frac in [("scores3", [0, 2, 3, 4], [1, 2, 2, 0], 2.0 / 3.0),
+                                  ("hubs_first5", [0, 3, 4, 5, 6, 7], [1, 2, 3, 0, 0, 0, 0], 0.4),
+                                  ("permutation6", [0, 2, 3, 4, 5, 6, 6], [1, 2, 2, 3, 0, 0], 0.08),
+                                  ("edgeless4", [0, 0, 0, 0, 0], [], 0.08)]:
+        o, sc, n = ref.hub_sort(np.array(off, np.uint64), np.array(cols, np.uint32), frac)
+        hub.append({"name": name, "row_offsets": off, "column_indices": cols, "hub_fraction": frac,
+                    "vertex_order": o.tolist(), "scores": sc.tolist(), "hub_count": int(n)})
+    reorder = []
+    for name, off, cols, w, order in [("reorder3", [0, 2, 3, 4], [1, 2, 2, 0], None, [2, 0, 1]),
+                                      ("reorder3_weights", [0, 2, 3, 4], [1, 2, 2, 0], [1.0, 2.0, 3.0, 4.0],
+                                       [2, 0, 1]),
+                                      ("hub_reorder5", [0, 3, 4, 5, 6, 7], [1, 2, 3, 0, 0, 0, 0], None,
+                                       [0, 1, 2, 3, 4])]:
+        ro, rc, rw = ref.reorder(np.array(off, np.uint64), np.array(cols, np.uint32),
+                                 None if w is None else np.array(w, np.float32), np.array(order, np.uint32))
+        reorder.append({"name": name, "row_offsets": off, "column_indices": cols, "weights": w,
+                        "vertex_order": order, "new_row_offsets": ro.tolist(), "new_column_indices": rc.tolist(),
+                        "new_weights": None if rw is None else rw.tolist()})
     with open(OUT / "known_answers.json", "w") as f:
-        json.dump({"graphs": meta, "hand": hand, "hytm": hytm, "selector": selector, "combiner": combiner}, f,
-                  indent=1)
+        json.dump({"graphs": meta, "hand": hand, "hytm": hytm, "selector": selector, "combiner": combiner,
+                   "hub_sort": hub, "reorder": reorder}, f, indent=1)
     print("wrote", OUT / "rmat_reference.npz", OUT / "known_answers.json")
 
 

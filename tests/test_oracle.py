@@ -172,3 +172,57 @@ def test_hytm_oracle_vs_reference_random(hyt, oracle, reference):
         a = oracle.task_combine(e, k)
         b = reference.task_combine(e, k)
         assert all(np.array_equal(x, y) for x, y in zip(a, b[:3]))
+
+
+def test_hub_sort_known_answers(oracle, golden):
+    """HubSorter cases of the reference's unit tests (unit_tests.cpp:2468-2602),
+    frozen from the reference's own output."""
+    for c in golden["meta"]["hub_sort"]:
+        order, scores, n = oracle.hub_sort(np.array(c["row_offsets"], np.uint64),
+                                           np.array(c["column_indices"], np.uint32), c["hub_fraction"])
+        assert order.tolist() == c["vertex_order"], c["name"]
+        assert scores.tolist() == c["scores"] and n == c["hub_count"], c["name"]
+    with pytest.raises(ValueError):
+        oracle.hub_sort(np.array([0, 1, 1], np.uint64), np.array([1], np.uint32), 1.5)
+
+
+def test_reorder_known_answers(oracle, golden):
+    """CSRGraph::reorder_vertices cases (unit_tests.cpp:2604-2740)."""
+    for c in golden["meta"]["reorder"]:
+        w = None if c["weights"] is None else np.array(c["weights"], np.float32)
+        off, cols, nw = oracle.reorder(np.array(c["row_offsets"], np.uint64), np.array(c["column_indices"], np.uint32),
+                                       w, c["vertex_order"])
+        assert off.tolist() == c["new_row_offsets"] and cols.tolist() == c["new_column_indices"], c["name"]
+        assert (nw is None and c["new_weights"] is None) or nw.tolist() == c["new_weights"], c["name"]
+    off, cols = np.array([0, 1, 2, 3], np.uint64), np.array([1, 2, 0], np.uint32)
+    for bad in ([0, 1, 1], [0, 1, 3]):  # duplicate, out of range
+        with pytest.raises(ValueError):
+            oracle.reorder(off, cols, None, bad)
+
+
+def test_hub_sort_and_reorder_golden_graphs(hyt, oracle, golden):
+    """The oracle reproduces the reference HubSorter's order, scores and hub
+    count and the reordered CSR on every golden R-MAT graph."""
+    for m in golden["meta"]["graphs"]:
+        g = _graph(hyt, m)
+        order, scores, n = oracle.hub_sort(g.row_offsets, g.column_indices, m["hub_fraction"])
+        assert n == m["hub_count"], m["key"]
+        assert hashlib.sha256(order.astype("<u4").tobytes()).hexdigest() == m["hub_order_sha256"], m["key"]
+        assert hashlib.sha256(scores.astype("<f8").tobytes()).hexdigest() == m["hub_scores_sha256"], m["key"]
+        off, cols, w = oracle.reorder(g.row_offsets, g.column_indices, g.weights, order)
+        assert _digest(hyt.CSR(off, cols, w)) == m["reordered_sha256"], m["key"]
+
+
+def test_hub_sort_oracle_vs_reference_random(hyt, oracle, reference):
+    rng = np.random.default_rng(11)
+    for scale, ef, seed in [(6, 2, 1), (11, 16, 7), (13, 4, 8)]:
+        g = hyt.rmat(scale, ef, seed)
+        for frac in (0.0, 0.08, 1.0 / 3.0, 0.5, 1.0, float(rng.random())):
+            a = oracle.hub_sort(g.row_offsets, g.column_indices, frac)
+            b = reference.hub_sort(g.row_offsets, g.column_indices, frac)
+            assert np.array_equal(a[0], b[0]) and a[2] == b[2], (scale, frac)
+            assert np.array_equal(a[1].view(np.uint64), b[1].view(np.uint64)), (scale, frac)
+        order = rng.permutation(g.num_vertices).astype(np.uint32)
+        x = oracle.reorder(g.row_offsets, g.column_indices, g.weights, order)
+        y = reference.reorder(g.row_offsets, g.column_indices, g.weights.view(np.float32), order)
+        assert all(np.array_equal(p.view(np.uint8), q.view(np.uint8)) for p, q in zip(x, y)), scale
