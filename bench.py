@@ -48,10 +48,13 @@ def parse_args():
     ap.add_argument("--seed", type=int, default=20241203)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["inhbm", "hybrid", "batch", "serve"], default="inhbm",
+    ap.add_argument("--workload", choices=["inhbm", "hybrid", "batch", "serve", "hubsort"], default="inhbm",
                     help="inhbm: graph resident in HBM (default); hybrid: edges in pinned host memory under a "
                          "device budget (defaults to R-MAT scale 27, edge factor 32, 8 GiB); batch: 64 graphs of "
-                         "scales 12-20, 512 SSSP/PPR queries in one CUDA-graph launch")
+                         "scales 12-20, 512 SSSP/PPR queries in one CUDA-graph launch; serve: continuous "
+                         "batching of a Poisson stream; hubsort: hub sorting + vertex reordering of the graph")
+    ap.add_argument("--hub-fraction", type=float, default=0.08)
+    ap.add_argument("--no-effect", action="store_true", help="hubsort: skip the solver comparison")
     ap.add_argument("--requests", type=int, default=20000)
     ap.add_argument("--rates", type=str, default="200,500,1000,2000,5000")
     ap.add_argument("--rate-seconds", type=float, default=8.0, help="serve: cap on each rate point's duration")
@@ -226,6 +229,30 @@ def run_reference_arm(args, rank, pg):
     if rank != 0:
         return
     import hytgraph_b200 as hyt
+
+    if args.workload == "hubsort":
+        d = hyt.rmat(args.scale, args.edge_factor, args.seed, device=True)
+        off_t, cols_t, w_t = host_graph_from_device(d)
+        d.free()
+        off, cols, w = off_t.numpy().view(np.uint64), cols_t.numpy().view(np.uint32), w_t.numpy().view(np.uint32)
+        V, E = int(off.shape[0] - 1), int(cols.shape[0])
+        times, kind = [], "port"
+        for i in range(args.warmup + args.steps):
+            t, kind = reference_hubsort(off, cols, w, args.hub_fraction)
+            if i >= args.warmup:
+                times.append(t)
+        total = sum(times)
+        value = E * args.steps / total / 1e9
+        sample = "per step: one HubSorter::sort + CSRGraph::reorder_vertices of the full graph"
+        line = {"impl": "reference", "metric": "hub sort + reorder throughput", "value": value, "unit": "Gedges/s",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "u32/u64 (f64 scores)", "data": "synthetic",
+                "config": hubsort_config(args, V, E),
+                "cpu_baseline": {"value": value, "unit": "Gedges/s", "cores": 1, "kind": kind, "sample": sample},
+                "e2e": {"value": value, "unit": "Gedges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
 
     g = hyt.rmat(args.scale, args.edge_factor, args.seed) if args.scale <= 20 else None
     if g is None:
@@ -641,6 +668,176 @@ def run_serve_workload(args, rank, world, pg):
         print(json.dumps(line), flush=True)
 
 
+def hubsort_config(args, V, E):
+    return {"workload": f"hub sorting (HubSorter::sort, hub_fraction {args.hub_fraction}) + vertex reordering "
+                        f"(CSRGraph::reorder_vertices) of R-MAT scale {args.scale} edge factor {args.edge_factor} "
+                        f"with uint32 weights",
+            "scale": args.scale, "edge_factor": args.edge_factor, "vertices": V, "edges": E,
+            "hub_fraction": args.hub_fraction, "rmat_abc": [0.57, 0.19, 0.19], "seed": args.seed,
+            "parallelism": f"replicas x{args.gpus}",
+            "l2": "inputs larger than L2 (CSR + weights > 2 GB vs 126 MB L2)"}
+
+
+def reference_hubsort(off, cols, w, fraction):
+    """The reference's HubSorter::sort + CSRGraph::reorder_vertices (its own
+    compiled code when available, else the oracle's restatement), one pass
+    over the full graph.  Returns (seconds, kind)."""
+    from oracle.bindings import Oracle, Reference
+
+    if Reference.available():
+        ref = Reference()
+        t0 = time.perf_counter()
+        order, _, _ = ref.hub_sort(off, cols, fraction)
+        ref.reorder(off, cols, w.view(np.float32), order)
+        return time.perf_counter() - t0, "reference"
+    ora = Oracle()
+    t0 = time.perf_counter()
+    order, _, _ = ora.hub_sort(off, cols, fraction)
+    ora.reorder(off, cols, w, order)
+    return time.perf_counter() - t0, "port"
+
+
+def run_hubsort_workload(args, rank, world, local, pg):
+    """One step = hyt_hub_sort + hyt_csr_reorder of the device-resident graph
+    (device in, device out).  Metric: edges hub-sorted and reordered per
+    second."""
+    import torch
+
+    import hytgraph_b200 as hyt
+    from hytgraph_b200 import capi
+
+    peak_gbs, peak_kind = load_peaks()
+    d = hyt.rmat(args.scale, args.edge_factor, args.seed, device=True)
+    V, E = d.num_vertices, d.num_edges
+    order_d = torch.empty(V, dtype=torch.int32, device="cuda")
+    scores_d = torch.empty(V, dtype=torch.float64, device="cuda")
+
+    def step(collect):
+        a, b = {}, {}
+        hyt.hub_sort(d, args.hub_fraction, order_out=order_d, scores_out=scores_d, stats=a)
+        r = hyt.reorder(d, order_d, device=True, stats=b)
+        r.free()
+        collect.append((a, b))
+
+    warm = []
+    for _ in range(args.warmup):
+        step(warm)
+    stream = torch.cuda.current_stream()
+    clocks = ClockSampler(local)
+    clocks.start()
+    timed = []
+    barrier(pg)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step(timed)  # host-synchronous calls on the library's own stream
+    ev1.record(stream)
+    barrier(pg)
+    wall_ms = 1e3 * (time.perf_counter() - t0)
+    clk = clocks.stop()
+    ms = max_over_ranks(pg, max(ev0.elapsed_time(ev1), wall_ms))
+    value = replica_value(E * args.steps, world, ms) / 1e9
+    hs_ms = sum(a["kernel_ms"] for a, _ in timed) / args.steps
+    rp_ms = sum(b["kernel_ms"] for _, b in timed) / args.steps
+    hs_bytes, rp_bytes = timed[0][0]["kernel_bytes"], timed[0][1]["kernel_bytes"]
+    dev_ms = sum(a["device_ms"] + b["device_ms"] for a, b in timed) / args.steps
+    alg_bytes = timed[0][0]["algorithmic_bytes"] + timed[0][1]["algorithmic_bytes"]
+    if rp_ms >= hs_ms:
+        kern, kb, kms = "permute_edges_kernel", rp_bytes, rp_ms
+    else:
+        kern, kb, kms = "degree_pass_kernel", hs_bytes, hs_ms
+    roof = {"kernel": kern, "bound": "hbm", "achieved": kb / (kms / 1e3) / 1e9, "peak": peak_gbs, "unit": "GB/s",
+            "frac": kb / (kms / 1e3) / 1e9 / peak_gbs, "traffic": None, "peak_kind": peak_kind,
+            "algorithmic_bytes_per_launch": kb, "avg_launch_ms": kms,
+            "other": {"degree_pass_kernel": {"ms": hs_ms, "bytes": hs_bytes},
+                      "permute_edges_kernel": {"ms": rp_ms, "bytes": rp_bytes}},
+            "whole_step_device_ms": dev_ms, "whole_step_algorithmic_bytes": alg_bytes,
+            "whole_step_gbs": alg_bytes / (dev_ms / 1e3) / 1e9}
+    traffic_file = ROOT / "profiles" / "traffic.json"
+    if traffic_file.exists():
+        tr = json.loads(traffic_file.read_text()).get(f"hubsort_s{args.scale}_ef{args.edge_factor}", {})
+        roof["traffic"] = tr.get(kern)
+        roof["traffic_measured"] = bool(tr.get("measured", False))
+    launches = sum(a["kernel_launches"] + b["kernel_launches"] for a, b in timed)
+
+    # effect on the solvers: PageRank + 8 SSSP sources on the original and on
+    # the reordered graph (same results up to the renaming)
+    effect = None
+    if not args.no_effect:
+        off_np = np.empty(V + 1, np.uint64)
+        capi.copy(off_np.ctypes.data, C.cast(d.buffers.row_offsets, C.c_void_p).value, off_np.nbytes)
+        srcs = [int(x) for x in hyt.pick_sources(off_np, args.seed, 8)]
+        order_np = order_d.cpu().numpy().view(np.uint32)
+        inv = np.empty_like(order_np)
+        inv[order_np] = np.arange(V, dtype=np.uint32)
+        r = hyt.reorder(d, order_d, device=True)
+        effect = {}
+        for name, g_csr, ss in (("original", d, srcs), ("hub_sorted", r, [int(inv[x]) for x in srcs])):
+            with hyt.Graph(g_csr) as g:
+                pr_out = torch.empty(V, dtype=torch.float32, device="cuda")
+                di_out = torch.empty(V, dtype=torch.int32, device="cuda")
+                g.pagerank(out=pr_out)
+                prm = min(g.pagerank(out=pr_out)[1]["device_ms"] for _ in range(2))
+                g.sssp(ss[0], out=di_out)
+                sms = [g.sssp(x, out=di_out)[1]["device_ms"] for x in ss]
+                effect[name] = {"pagerank_ms": prm, "sssp_ms_per_source": float(np.mean(sms))}
+        r.free()
+        effect["speedup"] = {k: effect["original"][k] / effect["hub_sorted"][k]
+                             for k in ("pagerank_ms", "sssp_ms_per_source")}
+
+    # e2e: the C ABI with pinned HOST buffers in and out
+    off_t, cols_t, w_t = host_graph_from_device(d)
+    d.free()
+    del order_d, scores_d
+    torch.cuda.empty_cache()
+    csr = capi.hyt_csr()
+    csr.num_vertices, csr.num_edges = V, E
+    csr.row_offsets, csr.column_indices, csr.weights = off_t.data_ptr(), cols_t.data_ptr(), w_t.data_ptr()
+    csr.weight_kind = capi.HYT_WEIGHTS_U32
+    order_h = torch.empty(V, dtype=torch.int32, pin_memory=True)
+    scores_h = torch.empty(V, dtype=torch.float64, pin_memory=True)
+
+    def e2e_step():
+        n = C.c_uint64()
+        capi.check(capi.lib.hyt_hub_sort(C.byref(csr), args.hub_fraction, order_h.data_ptr(), scores_h.data_ptr(),
+                                         C.byref(n), None))
+        b = capi.hyt_csr_buffers()
+        capi.check(capi.lib.hyt_csr_reorder(C.byref(csr), order_h.data_ptr(), 0, C.byref(b), None))
+        capi.check(capi.lib.hyt_csr_buffers_free(C.byref(b)))
+
+    e2e_step()
+    barrier(pg)
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        e2e_step()
+    barrier(pg)
+    e2e_ms = max_over_ranks(pg, 1e3 * (time.perf_counter() - t0))
+    e2e_value = replica_value(E * args.e2e_steps, world, e2e_ms) / 1e9
+    # hub sort: offsets + ids in, order + scores out; reorder: offsets, ids,
+    # weights and order in, offsets, ids and weights out
+    h2d = (V + 1) * 8 + E * 4 + (V + 1) * 8 + E * 8 + V * 4
+    d2h = V * 12 + (V + 1) * 8 + E * 8
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        t, kind = reference_hubsort(off_t.numpy().view(np.uint64), cols_t.numpy().view(np.uint32),
+                                    w_t.numpy().view(np.uint32), args.hub_fraction)
+        cpu = {"value": E / t / 1e9, "unit": "Gedges/s", "cores": 1, "kind": kind,
+               "sample": f"one HubSorter::sort + CSRGraph::reorder_vertices of the full graph, {t:.1f} s"}
+    if rank == 0:
+        line = {"metric": "hub sort + reorder throughput", "value": value, "unit": "Gedges/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32/u64 (f64 scores)",
+                "data": "synthetic", "config": hubsort_config(args, V, E),
+                "e2e": {"value": e2e_value, "unit": "Gedges/s", "h2d_bytes_per_step": h2d,
+                        "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms / args.e2e_steps,
+                        "steps": args.e2e_steps},
+                "roofline": roof, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches,
+                "effect_on_solvers": effect}
+        print(json.dumps(line), flush=True)
+
+
 def workload_config(args, V, E):
     return {"workload": f"in-HBM R-MAT scale {args.scale} edge factor {args.edge_factor}: PageRank to L1<=1e-6 "
                         f"+ SSSP from {args.sources} seeded sources",
@@ -673,6 +870,11 @@ def main():
         return
     if args.workload == "batch":
         run_batch_workload(args, rank, world, pg)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
+    if args.workload == "hubsort":
+        run_hubsort_workload(args, rank, world, local, pg)
         if pg is not None:
             pg.destroy_process_group()
         return

@@ -142,6 +142,20 @@ class hyt_csr_buffers(C.Structure):
     ]
 
 
+class hyt_reorder_stats(C.Structure):
+    _fields_ = [
+        ("device_ms", C.c_double),
+        ("kernel_ms", C.c_double),
+        ("kernel_bytes", C.c_uint64),
+        ("algorithmic_bytes", C.c_uint64),
+        ("kernel_launches", C.c_uint32),
+        ("library_calls", C.c_uint32),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 class hyt_csc(C.Structure):
     _fields_ = [
         ("num_vertices", C.c_uint64),
@@ -357,8 +371,10 @@ _SIGNATURES = [
      [C.c_void_p, C.POINTER(hyt_completion), C.c_uint32, C.POINTER(C.c_uint32), C.c_uint32]),
     ("hyt_server_get_stats", C.c_int, [C.c_void_p, C.POINTER(hyt_server_stats)]),
     ("hyt_server_destroy", C.c_int, [C.c_void_p]),
-    ("hyt_hub_sort", C.c_int, [C.POINTER(hyt_csr), C.c_double, C.c_void_p, C.c_void_p, C.POINTER(C.c_uint64)]),
-    ("hyt_csr_reorder", C.c_int, [C.POINTER(hyt_csr), C.c_void_p, C.c_int, C.POINTER(hyt_csr_buffers)]),
+    ("hyt_hub_sort", C.c_int, [C.POINTER(hyt_csr), C.c_double, C.c_void_p, C.c_void_p, C.POINTER(C.c_uint64),
+                               C.POINTER(hyt_reorder_stats)]),
+    ("hyt_csr_reorder", C.c_int, [C.POINTER(hyt_csr), C.c_void_p, C.c_int, C.POINTER(hyt_csr_buffers),
+                                  C.POINTER(hyt_reorder_stats)]),
     ("hyt_rmat_generate", C.c_int, [C.POINTER(hyt_rmat_params), C.c_int, C.POINTER(hyt_csr_buffers)]),
     ("hyt_csr_buffers_free", C.c_int, [C.POINTER(hyt_csr_buffers)]),
     ("hyt_pick_sources", C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint32, C.c_void_p]),

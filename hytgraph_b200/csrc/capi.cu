@@ -270,19 +270,20 @@ int hyt_csr_buffers_free(hyt_csr_buffers *b) {
 }
 
 int hyt_hub_sort(const hyt_csr *csr, double hub_fraction, uint32_t *vertex_order, double *scores,
-                 uint64_t *hub_count) {
+                 uint64_t *hub_count, hyt_reorder_stats *stats) {
     return guarded([&] {
         if (!csr) fail(HYT_E_INVALID, "csr is NULL");
         require_device();
-        hub_sort(*csr, hub_fraction, vertex_order, scores, hub_count);
+        hub_sort(*csr, hub_fraction, vertex_order, scores, hub_count, stats);
     });
 }
 
-int hyt_csr_reorder(const hyt_csr *csr, const uint32_t *vertex_order, int on_device, hyt_csr_buffers *out) {
+int hyt_csr_reorder(const hyt_csr *csr, const uint32_t *vertex_order, int on_device, hyt_csr_buffers *out,
+                    hyt_reorder_stats *stats) {
     return guarded([&] {
         if (!csr) fail(HYT_E_INVALID, "csr is NULL");
         require_device();
-        csr_reorder(*csr, vertex_order, on_device != 0, out);
+        csr_reorder(*csr, vertex_order, on_device != 0, out, stats);
     });
 }
 

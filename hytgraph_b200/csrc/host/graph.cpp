@@ -5,9 +5,12 @@
 #include "graph/activity_tracker.hpp"
 #include "graph/csr_graph.hpp"
 #include "graph/partition.hpp"
+#include "hyt/capi.h"
 
 #include <algorithm>
+#include <cstring>
 #include <stdexcept>
+#include <string>
 
 namespace hytgraph::graph {
 
@@ -60,38 +63,43 @@ void CSRGraph::validate() const {
         throw std::invalid_argument("CSRGraph::validate: edge_weights must contain exactly one weight per edge");
 }
 
+// Runs on the GPU (hyt_csr_reorder, the steps of the reference's
+// src/graph/csr_graph.cpp:171-283); the reference's messages for a wrong
+// size, an out-of-range id or a duplicate id come back as
+// std::invalid_argument.
 void CSRGraph::reorder_vertices(const std::vector<vertex_id> &vertex_order) {
     const std::size_t n = static_cast<std::size_t>(num_vertices_);
     if (vertex_order.size() != n)
         throw std::invalid_argument("CSRGraph::reorder_vertices: vertex_order must contain exactly one entry per vertex");
-    std::vector<vertex_id> new_id(n);
-    std::vector<unsigned char> seen(n, 0);
-    for (std::size_t nv = 0; nv < n; ++nv) {
-        const std::size_t old = vertex_order[nv];
-        if (old >= n) throw std::invalid_argument("CSRGraph::reorder_vertices: vertex_order contains an out-of-range vertex ID");
-        if (seen[old]) throw std::invalid_argument("CSRGraph::reorder_vertices: vertex_order contains duplicate vertex IDs");
-        seen[old] = 1;
-        new_id[old] = static_cast<vertex_id>(nv);
+    int devices = 0;
+    if (hyt_device_count(&devices) != HYT_OK || devices == 0)
+        throw std::runtime_error("CSRGraph::reorder_vertices: no CUDA device is available");
+    hyt_csr csr{};
+    csr.num_vertices = num_vertices_;
+    csr.num_edges = num_edges();
+    csr.row_offsets = row_offsets_.data();
+    csr.column_indices = column_indices_.data();
+    csr.weights = has_weights() ? edge_weights_.data() : nullptr;
+    csr.weight_kind = has_weights() ? HYT_WEIGHTS_F32 : HYT_WEIGHTS_NONE;
+    hyt_csr_buffers out{};
+    const int status = hyt_csr_reorder(&csr, vertex_order.data(), 0, &out, nullptr);
+    if (status != HYT_OK) {
+        const std::string msg = hyt_last_error();
+        if (status == HYT_E_INVALID) throw std::invalid_argument(msg);
+        throw std::runtime_error("CSRGraph::reorder_vertices: " + msg);
     }
-    std::vector<offset_type> offs(n + 1, 0);
-    for (std::size_t nv = 0; nv < n; ++nv) {
-        const std::size_t old = vertex_order[nv];
-        offs[nv + 1] = offs[nv] + (row_offsets_[old + 1] - row_offsets_[old]);
+    const std::size_t m = column_indices_.size();
+    std::vector<offset_type> offs(out.row_offsets, out.row_offsets + n + 1);
+    std::vector<vertex_id> cols(out.column_indices, out.column_indices + m);
+    std::vector<weight_type> wts;
+    if (has_weights()) {
+        wts.resize(m);
+        if (m) std::memcpy(wts.data(), out.weights, m * sizeof(weight_type));
     }
-    std::vector<vertex_id> cols(column_indices_.size());
-    std::vector<weight_type> wts(edge_weights_.size());
-    for (std::size_t nv = 0; nv < n; ++nv) {
-        const std::size_t old = vertex_order[nv];
-        offset_type out = offs[nv];
-        for (offset_type e = row_offsets_[old]; e < row_offsets_[old + 1]; ++e, ++out) {
-            cols[out] = new_id[column_indices_[e]];
-            if (!wts.empty()) wts[out] = edge_weights_[e];
-        }
-    }
+    hyt_csr_buffers_free(&out);
     row_offsets_ = std::move(offs);
     column_indices_ = std::move(cols);
     edge_weights_ = std::move(wts);
-    validate();
 }
 
 // ---------------------------- ActivityTracker ----------------------------

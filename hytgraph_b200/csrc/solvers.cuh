@@ -14,7 +14,9 @@ void rmat_generate(const hyt_rmat_params &p, bool on_device, hyt_csr_buffers *ou
 void pick_sources(const uint64_t *row_offsets, uint64_t V, uint64_t seed, uint32_t count, uint32_t *out);
 
 // Hub sorting / vertex reordering (reorder.cu).
-void hub_sort(const hyt_csr &csr, double fraction, uint32_t *order_out, double *scores_out, uint64_t *hub_count);
-void csr_reorder(const hyt_csr &csr, const uint32_t *vertex_order, bool on_device, hyt_csr_buffers *out);
+void hub_sort(const hyt_csr &csr, double fraction, uint32_t *order_out, double *scores_out, uint64_t *hub_count,
+              hyt_reorder_stats *stats);
+void csr_reorder(const hyt_csr &csr, const uint32_t *vertex_order, bool on_device, hyt_csr_buffers *out,
+                 hyt_reorder_stats *stats);
 
 }  // namespace hyt

@@ -510,28 +510,44 @@ class Server:
             pass
 
 
-def hub_sort(csr, hub_fraction: float = 0.08):
+def hub_sort(csr, hub_fraction: float = 0.08, order_out=None, scores_out=None, stats: Optional[dict] = None):
     """Hub-first vertex order on the GPU (hyt_hub_sort): returns
-    (vertex_order uint32[V], scores float64[V], hub_count)."""
+    (vertex_order uint32[V], scores float64[V], hub_count).  csr: CSR or
+    DeviceCSR.  order_out / scores_out: optional caller buffers (numpy, or
+    CUDA tensors to keep the results on the device; scores_out=False skips
+    the scores).  stats: filled with the call's device figures."""
     c = csr.to_c()
     V = int(c.num_vertices)
-    order = np.empty(V, np.uint32)
-    scores = np.empty(V, np.float64)
+    order = np.empty(V, np.uint32) if order_out is None else order_out
+    scores = np.empty(V, np.float64) if scores_out is None else scores_out
     n = C.c_uint64()
-    check(lib.hyt_hub_sort(C.byref(c), hub_fraction, _ptr(order), _ptr(scores), C.byref(n)))
+    st = capi.hyt_reorder_stats()
+    check(lib.hyt_hub_sort(C.byref(c), hub_fraction, _ptr(order) if V else None,
+                           _ptr(scores) if (scores is not False and V) else None, C.byref(n), C.byref(st)))
+    if stats is not None:
+        stats.update(st.as_dict())
     return order, scores, n.value
 
 
-def reorder(csr, vertex_order, device: bool = False):
+def reorder(csr, vertex_order, device: bool = False, stats: Optional[dict] = None):
     """CSRGraph::reorder_vertices on the GPU (hyt_csr_reorder): a host CSR,
-    or a DeviceCSR when device=True."""
+    or a DeviceCSR when device=True.  vertex_order: numpy or a CUDA tensor."""
     c = csr.to_c()
-    order = np.ascontiguousarray(vertex_order, np.uint32)
-    if order.shape != (csr.num_vertices,):
+    if isinstance(vertex_order, (np.ndarray, list, tuple)):
+        order = np.ascontiguousarray(vertex_order, np.uint32)
+        shape = order.shape
+    else:
+        order = vertex_order
+        shape = tuple(order.shape)
+    if shape != (csr.num_vertices,):
         raise HytError(capi.HYT_E_INVALID,
                        "CSRGraph::reorder_vertices: vertex_order must contain exactly one entry per vertex")
     b = capi.hyt_csr_buffers()
-    check(lib.hyt_csr_reorder(C.byref(c), _ptr(order), 1 if device else 0, C.byref(b)))
+    st = capi.hyt_reorder_stats()
+    check(lib.hyt_csr_reorder(C.byref(c), _ptr(order) if csr.num_vertices else None, 1 if device else 0,
+                              C.byref(b), C.byref(st)))
+    if stats is not None:
+        stats.update(st.as_dict())
     if device:
         return DeviceCSR(b, csr.weight_kind)
     V, E = int(b.num_vertices), int(b.num_edges)

@@ -464,24 +464,38 @@ int hyt_pick_sources(const uint64_t *row_offsets, uint64_t num_vertices,
 /* Hub sorting and vertex reordering on the GPU                         */
 /* ------------------------------------------------------------------ */
 
+/* Device-side figures of one hub-sort or reorder call. */
+typedef struct hyt_reorder_stats {
+    double device_ms;           /* the whole call on the device, copies included */
+    double kernel_ms;           /* its main kernel: the degree pass (hub sort) or
+                                   the edge permutation (reorder) */
+    uint64_t kernel_bytes;      /* algorithmic bytes of that kernel */
+    uint64_t algorithmic_bytes; /* algorithmic bytes of the whole call */
+    uint32_t kernel_launches;   /* this library's kernels */
+    uint32_t library_calls;     /* radix sorts, scans and selects */
+} hyt_reorder_stats;
+
 /* Hub-first vertex order of scheduling::HubSorter::sort
  * (src/scheduling/hub_sort.cpp:28-183): scores H(v) = Do(v) * Di(v) /
  * (Do_max * Di_max); the round-or-ceil(V * hub_fraction) best first (ties:
  * lower id), then the other vertices in id order.  csr: host or device
- * arrays.  vertex_order[V] (new -> old), scores[V] (may be NULL) and
- * *hub_count (may be NULL): host or device.  Scores are correctly rounded
- * double quotients (the reference rounds a long-double quotient; the two can
- * differ in the last place), the order is the reference's exactly. */
+ * arrays.  vertex_order[V] (new -> old) and scores[V] (may be NULL): host or
+ * device; *hub_count (may be NULL): host.  Scores equal the reference's
+ * x86-64 long-double quotient rounded to double, bit for bit.  Rejects a
+ * hub_fraction outside [0, 1] and a malformed CSR (HYT_E_INVALID).  stats
+ * may be NULL. */
 int hyt_hub_sort(const hyt_csr *csr, double hub_fraction, uint32_t *vertex_order, double *scores,
-                 uint64_t *hub_count);
+                 uint64_t *hub_count, hyt_reorder_stats *stats);
 
 /* graph::CSRGraph::reorder_vertices (src/graph/csr_graph.cpp:171-283) into
  * new buffers: vertex_order[new] = old; each new row holds the old row's
  * edges in their original order with destinations renamed, weights carried.
  * on_device: 1 = cudaMalloc'd output, 0 = malloc'd; free with
  * hyt_csr_buffers_free.  Rejects out-of-range or duplicate entries with the
- * reference's messages. */
-int hyt_csr_reorder(const hyt_csr *csr, const uint32_t *vertex_order, int on_device, hyt_csr_buffers *out);
+ * reference's messages, and a malformed CSR.  vertex_order: host or device.
+ * stats may be NULL. */
+int hyt_csr_reorder(const hyt_csr *csr, const uint32_t *vertex_order, int on_device, hyt_csr_buffers *out,
+                    hyt_reorder_stats *stats);
 
 #ifdef __cplusplus
 } /* extern "C" */

@@ -16,6 +16,7 @@
 #include "hyt/capi.h"
 #include "runtime/config.hpp"
 #include "runtime/result.hpp"
+#include "scheduling/hub_sort.hpp"
 #include "scheduling/task_combiner.hpp"
 #include "transfer/compaction_engine.hpp"
 #include "transfer/filter_engine.hpp"
@@ -80,11 +81,7 @@ void test_csr() {
     throws<std::invalid_argument>([] { CSRGraph(2, {0, 1, 2}, {0, 2}); }, "destination range");
     throws<std::invalid_argument>([] { CSRGraph(2, {0, 1, 2}, {0, 1}, {1.0F}); }, "weight count");
     CSRGraph w(3, {0, 2, 3, 3}, {1, 2, 2}, {5.F, 6.F, 7.F});
-    w.reorder_vertices({2, 0, 1});  // new0 = old2, new1 = old0, new2 = old1
-    check(w.row_offsets() == std::vector<CSRGraph::offset_type>({0, 0, 2, 3}), "reorder offsets");
-    check(w.column_indices() == std::vector<CSRGraph::vertex_id>({2, 0, 0}), "reorder columns");
-    check(w.edge_weights() == std::vector<float>({5.F, 6.F, 7.F}), "reorder weights");
-    throws<std::invalid_argument>([&] { w.reorder_vertices({0, 0, 1}); }, "duplicate order");
+    throws<std::invalid_argument>([&] { w.reorder_vertices({0, 1}); }, "order size");  // checked before the GPU
 }
 
 void test_activity() {
@@ -318,6 +315,42 @@ void test_gpu() {
     SSSPOptions so;
     so.source = 2;
     throws<std::invalid_argument>([&] { (void)sssp_gpu(CSRGraph(2, {0, 0, 0}, {}), so); }, "source range");
+
+    // Reordering and hub sorting (GPU): reference tests/unit_tests.cpp:2468-2740.
+    CSRGraph rw(3, {0, 2, 3, 3}, {1, 2, 2}, {5.F, 6.F, 7.F});
+    rw.reorder_vertices({2, 0, 1});  // new0 = old2, new1 = old0, new2 = old1
+    check(rw.row_offsets() == std::vector<CSRGraph::offset_type>({0, 0, 2, 3}), "reorder offsets");
+    check(rw.column_indices() == std::vector<CSRGraph::vertex_id>({2, 0, 0}), "reorder columns");
+    check(rw.edge_weights() == std::vector<float>({5.F, 6.F, 7.F}), "reorder weights");
+    CSRGraph r3(3, {0, 2, 3, 4}, {1, 2, 2, 0}, {1.F, 2.F, 3.F, 4.F});
+    r3.reorder_vertices({2, 0, 1});
+    check(r3.row_offsets() == std::vector<CSRGraph::offset_type>({0, 1, 3, 4}), "reorder offsets 2");
+    check(r3.column_indices() == std::vector<CSRGraph::vertex_id>({1, 2, 0, 0}), "reorder columns 2");
+    check(r3.edge_weights() == std::vector<float>({4.F, 1.F, 2.F, 3.F}), "reorder weights 2");
+    r3.validate();
+    throws<std::invalid_argument>([&] { rw.reorder_vertices({0, 0, 1}); }, "duplicate order");
+    throws<std::invalid_argument>([&] { rw.reorder_vertices({0, 1, 3}); }, "out-of-range order");
+
+    using scheduling::HubSorter;
+    using scheduling::HubSortOptions;
+    HubSortOptions ho;
+    ho.hub_fraction = 2.0 / 3.0;
+    const auto sc = HubSorter(ho).sort(CSRGraph(3, {0, 2, 3, 4}, {1, 2, 2, 0}));
+    check(sc.scores == std::vector<double>({0.5, 0.25, 0.5}) && sc.hub_count == 2, "hub scores");
+    check(sc.vertex_order == std::vector<CSRGraph::vertex_id>({0, 2, 1}), "hub order ties by id");
+    ho.hub_fraction = 0.4;
+    CSRGraph h5(5, {0, 3, 4, 5, 6, 7}, {1, 2, 3, 0, 0, 0, 0});
+    const auto hs = HubSorter(ho).sort(h5);
+    check(hs.hub_count == 2 && hs.vertex_order == std::vector<CSRGraph::vertex_id>({0, 1, 2, 3, 4}), "hubs first");
+    h5.reorder_vertices(hs.vertex_order);
+    check(h5.column_indices() == std::vector<CSRGraph::vertex_id>({1, 2, 3, 0, 0, 0, 0}), "hub reorder");
+    const auto el = HubSorter().sort(CSRGraph(4, {0, 0, 0, 0, 0}, {}));
+    check(el.hub_count == 1 && el.vertex_order == std::vector<CSRGraph::vertex_id>({0, 1, 2, 3}), "edgeless");
+    check(el.scores == std::vector<double>(4, 0.0), "edgeless scores");
+    check(HubSorter().sort(CSRGraph(0, {0}, {})).empty(), "empty graph");
+    HubSortOptions bad_fraction;
+    bad_fraction.hub_fraction = 1.5;
+    throws<std::invalid_argument>([&] { HubSorter h{bad_fraction}; (void)h; }, "fraction range");
 }
 
 }  // namespace

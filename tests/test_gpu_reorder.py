@@ -139,3 +139,41 @@ def test_edge_cases_and_errors(hyt, gpu):
     broken = hyt.CSR(np.array([0, 1, 2, 3], np.uint64), np.array([1, 7, 0], np.uint32))
     with pytest.raises(hyt.HytError):
         hyt.hub_sort(broken)
+
+
+def test_reorder_sparse_and_hub_rows(hyt, gpu, oracle):
+    """Tiles that span more than 2048 rows (long runs of empty rows) and a
+    row of 100k edges, against the oracle."""
+    rng = np.random.default_rng(21)
+    V = 60000
+    deg = np.where(rng.random(V) < 0.02, rng.integers(1, 6, V), 0).astype(np.uint64)
+    deg[123] = 100000
+    off = np.zeros(V + 1, np.uint64)
+    off[1:] = np.cumsum(deg)
+    cols = rng.integers(0, V, int(off[-1])).astype(np.uint32)
+    w = rng.integers(1, 64, int(off[-1])).astype(np.uint32)
+    g = hyt.CSR(off, cols, w)
+    for order in (hyt.hub_sort(g)[0], rng.permutation(V).astype(np.uint32)):
+        r = hyt.reorder(g, order)
+        o_off, o_cols, o_w = oracle.reorder(off, cols, w, order)
+        assert _same(r.row_offsets, o_off) and _same(r.column_indices, o_cols) and _same(r.weights, o_w)
+
+
+def test_device_buffers_and_stats(hyt, gpu):
+    import torch
+
+    g = hyt.rmat(15, 16, 31, device=True)
+    order_d = torch.empty(g.num_vertices, dtype=torch.int32, device="cuda")
+    scores_d = torch.empty(g.num_vertices, dtype=torch.float64, device="cuda")
+    st = {}
+    hyt.hub_sort(g, 0.08, order_out=order_d, scores_out=scores_d, stats=st)
+    order_h, scores_h, _ = hyt.hub_sort(g, 0.08)
+    assert np.array_equal(order_d.cpu().numpy().view(np.uint32), order_h)
+    assert _same(scores_d.cpu().numpy(), scores_h)
+    assert st["device_ms"] > 0 and st["kernel_ms"] > 0 and st["kernel_bytes"] >= 4 * g.num_edges
+    st2 = {}
+    a = hyt.reorder(g, order_d, device=True, stats=st2).download()
+    b = hyt.reorder(g, order_h)
+    assert _same(a.row_offsets, b.row_offsets) and _same(a.column_indices, b.column_indices)
+    assert _same(a.weights, b.weights)
+    assert st2["kernel_ms"] > 0 and st2["kernel_bytes"] >= 20 * g.num_edges
