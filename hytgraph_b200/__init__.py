@@ -10,9 +10,10 @@ there is no CPU fallback.
 """
 from . import capi
 from .capi import HytError, device_count
-from .graph import CSR, Batch, DeviceCSR, Graph, HybridGraph, PinnedBuffer, Server, hub_sort, pick_sources, reorder, rmat
+from .graph import (CSR, Batch, DeviceCSR, Graph, HybridGraph, PinnedBuffer, Server, csr_from_edges, hub_sort,
+                    load_csr, load_edge_list, pick_sources, reorder, rmat, save_csr)
 
 __all__ = [
     "capi", "HytError", "device_count", "CSR", "Batch", "DeviceCSR", "Graph", "HybridGraph", "PinnedBuffer", "Server",
-    "hub_sort", "pick_sources", "reorder", "rmat",
+    "csr_from_edges", "hub_sort", "load_csr", "load_edge_list", "pick_sources", "reorder", "rmat", "save_csr",
 ]

@@ -21,6 +21,7 @@ HYT_E_TIMEOUT = 4
 HYT_E_NO_DEVICE = 5
 HYT_E_UNSUPPORTED = 6
 HYT_E_INTERNAL = 7
+HYT_E_IO = 8
 
 HYT_WEIGHTS_NONE = 0
 HYT_WEIGHTS_U32 = 1
@@ -139,6 +140,7 @@ class hyt_csr_buffers(C.Structure):
         ("column_indices", C.POINTER(C.c_uint32)),
         ("weights", C.POINTER(C.c_uint32)),
         ("on_device", C.c_uint32),
+        ("weight_kind", C.c_uint32),
     ]
 
 
@@ -154,6 +156,23 @@ class hyt_reorder_stats(C.Structure):
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class hyt_load_stats(C.Structure):
+    _fields_ = [
+        ("total_ms", C.c_double),
+        ("read_ms", C.c_double),
+        ("device_ms", C.c_double),
+        ("kernel_ms", C.c_double),
+        ("file_bytes", C.c_uint64),
+        ("num_edges", C.c_uint64),
+        ("kernel_bytes", C.c_uint64),
+        ("threads", C.c_uint32),
+        ("pad", C.c_uint32),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_ if name != "pad"}
 
 
 class hyt_csc(C.Structure):
@@ -373,6 +392,12 @@ _SIGNATURES = [
     ("hyt_server_destroy", C.c_int, [C.c_void_p]),
     ("hyt_hub_sort", C.c_int, [C.POINTER(hyt_csr), C.c_double, C.c_void_p, C.c_void_p, C.POINTER(C.c_uint64),
                                C.POINTER(hyt_reorder_stats)]),
+    ("hyt_load_edge_list", C.c_int, [C.c_char_p, C.c_uint64, C.c_int, C.c_int, C.POINTER(hyt_csr_buffers),
+                                     C.POINTER(hyt_load_stats)]),
+    ("hyt_csr_from_edges", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint64, C.c_uint64, C.c_int,
+                                     C.POINTER(hyt_csr_buffers), C.POINTER(hyt_load_stats)]),
+    ("hyt_csr_save", C.c_int, [C.c_char_p, C.POINTER(hyt_csr)]),
+    ("hyt_csr_load", C.c_int, [C.c_char_p, C.c_int, C.POINTER(hyt_csr_buffers), C.POINTER(hyt_load_stats)]),
     ("hyt_csr_reorder", C.c_int, [C.POINTER(hyt_csr), C.c_void_p, C.c_int, C.POINTER(hyt_csr_buffers),
                                   C.POINTER(hyt_reorder_stats)]),
     ("hyt_rmat_generate", C.c_int, [C.POINTER(hyt_rmat_params), C.c_int, C.POINTER(hyt_csr_buffers)]),

@@ -287,6 +287,38 @@ int hyt_csr_reorder(const hyt_csr *csr, const uint32_t *vertex_order, int on_dev
     });
 }
 
+int hyt_load_edge_list(const char *path, uint64_t num_vertices, int weighted, int on_device,
+                       hyt_csr_buffers *out, hyt_load_stats *stats) {
+    return guarded([&] {
+        require_device();
+        load_edge_list(path, num_vertices, weighted != 0, on_device != 0, out, stats);
+    });
+}
+
+int hyt_csr_from_edges(const uint32_t *src, const uint32_t *dst, const void *weights, uint32_t weight_kind,
+                       uint64_t num_edges, uint64_t num_vertices, int on_device, hyt_csr_buffers *out,
+                       hyt_load_stats *stats) {
+    return guarded([&] {
+        require_device();
+        csr_from_edges(src, dst, weights, weight_kind, num_edges, num_vertices, on_device != 0, out, stats);
+    });
+}
+
+int hyt_csr_save(const char *path, const hyt_csr *csr) {
+    return guarded([&] {
+        if (!csr) fail(HYT_E_INVALID, "csr is NULL");
+        require_device();
+        csr_save(path, *csr);
+    });
+}
+
+int hyt_csr_load(const char *path, int on_device, hyt_csr_buffers *out, hyt_load_stats *stats) {
+    return guarded([&] {
+        require_device();
+        csr_load(path, on_device != 0, out, stats);
+    });
+}
+
 int hyt_pick_sources(const uint64_t *row_offsets, uint64_t num_vertices, uint64_t seed, uint32_t count,
                      uint32_t *out) {
     return guarded([&] { pick_sources(row_offsets, num_vertices, seed, count, out); });

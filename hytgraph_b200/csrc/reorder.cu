@@ -32,6 +32,7 @@
 #include <thrust/iterator/counting_iterator.h>
 
 #include "common.cuh"
+#include "scratch.cuh"
 
 namespace hyt {
 namespace {
@@ -355,47 +356,6 @@ __global__ void __launch_bounds__(kPermThreads) permute_edges_kernel(
     if (b) atomicOr(bad, b);
 }
 
-// Scratch pool of the current device: stream-ordered allocations that keep
-// up to 2 GiB mapped between calls, so repeated calls do not pay for
-// mapping fresh memory (a scale-24 call needs about 0.8 GB of scratch).
-cudaMemPool_t scratch_pool() {
-    static std::mutex mu;
-    static std::unordered_map<int, cudaMemPool_t> pools;
-    int dev = 0;
-    HYT_CUDA(cudaGetDevice(&dev));
-    std::lock_guard<std::mutex> lk(mu);
-    auto it = pools.find(dev);
-    if (it != pools.end()) return it->second;
-    cudaMemPoolProps props{};
-    props.allocType = cudaMemAllocationTypePinned;
-    props.location.type = cudaMemLocationTypeDevice;
-    props.location.id = dev;
-    cudaMemPool_t pool = nullptr;
-    HYT_CUDA(cudaMemPoolCreate(&pool, &props));
-    uint64_t keep = uint64_t(2) << 30;
-    HYT_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
-    pools[dev] = pool;
-    return pool;
-}
-
-// Stream-ordered scratch (freed on the same stream at scope exit).
-template <class T>
-struct Scratch {
-    T *p = nullptr;
-    cudaStream_t s = nullptr;
-    Scratch(size_t n, cudaStream_t st) : s(st) {
-        void *q = nullptr;
-        HYT_CUDA(cudaMallocFromPoolAsync(&q, std::max<size_t>(n, 1) * sizeof(T) + 16, scratch_pool(), s));
-        p = static_cast<T *>(q);
-    }
-    ~Scratch() {
-        if (p) cudaFreeAsync(p, s);
-    }
-    Scratch(const Scratch &) = delete;
-    Scratch &operator=(const Scratch &) = delete;
-    T *get() const { return p; }
-};
-
 // Stable descending sort of (key, id) pairs on key bits [0, end_bit); the
 // result ends in *keys / *ids (which may swap with the alternate buffers).
 void sort_desc(uint64_t *&keys, uint64_t *keys_alt, uint32_t *&ids, uint32_t *ids_alt, uint64_t n, int end_bit,
@@ -427,16 +387,6 @@ void exclusive_scan(const uint64_t *in, uint64_t *out, uint64_t n, cudaStream_t 
     HYT_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), tb, in, out, static_cast<int64_t>(n), s));
 }
 
-// Device view of a host-or-device array: device pointers pass through, host
-// arrays are copied into `hold`.
-template <class T>
-const T *device_view(const T *p, uint64_t n, std::unique_ptr<Scratch<T>> &hold, cudaStream_t s) {
-    if (!p || n == 0 || is_device_pointer(p)) return p;
-    hold = std::make_unique<Scratch<T>>(n, s);
-    HYT_CUDA(cudaMemcpyAsync(hold->get(), p, n * sizeof(T), cudaMemcpyHostToDevice, s));
-    return hold->get();
-}
-
 // Hub count rule of the reference (its long-double arithmetic, on the host).
 uint64_t hub_count_for(uint64_t V, double fraction) {
     const long double requested = static_cast<long double>(V) * static_cast<long double>(fraction);
@@ -445,15 +395,6 @@ uint64_t hub_count_for(uint64_t V, double fraction) {
     const uint64_t n = pick <= 0.0L ? 0 : static_cast<uint64_t>(pick);
     return n < V ? n : V;
 }
-
-struct StreamHold {
-    cudaStream_t s = nullptr;
-    StreamHold() { HYT_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)); }
-    ~StreamHold() {
-        cudaStreamSynchronize(s);
-        cudaStreamDestroy(s);
-    }
-};
 
 uint32_t read_flags(const uint32_t *bad, cudaStream_t s) {
     uint32_t h = 0;
@@ -601,6 +542,7 @@ void csr_reorder(const hyt_csr &csr, const uint32_t *vertex_order, bool on_devic
     out->num_vertices = V;
     out->num_edges = E;
     out->on_device = on_device ? 1u : 0u;
+    out->weight_kind = weighted ? csr.weight_kind : HYT_WEIGHTS_NONE;
     out->row_offsets = static_cast<uint64_t *>(alloc((V + 1) * 8));
     out->column_indices = static_cast<uint32_t *>(alloc(E * 4));
     if (weighted) out->weights = static_cast<uint32_t *>(alloc(E * 4));

@@ -155,6 +155,7 @@ void generate_device(const hyt_rmat_params &p, const RmatKey &k, hyt_csr_buffers
     out->column_indices = cols;
     out->weights = w;
     out->on_device = 1;
+    out->weight_kind = w ? HYT_WEIGHTS_U32 : HYT_WEIGHTS_NONE;
 }
 
 // -------------------------------- host ---------------------------------
@@ -211,6 +212,7 @@ void generate_host(const hyt_rmat_params &p, const RmatKey &k, hyt_csr_buffers *
     out->column_indices = cols;
     out->weights = w;
     out->on_device = 0;
+    out->weight_kind = w ? HYT_WEIGHTS_U32 : HYT_WEIGHTS_NONE;
 }
 
 }  // namespace

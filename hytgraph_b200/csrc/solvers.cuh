@@ -18,5 +18,11 @@ void hub_sort(const hyt_csr &csr, double fraction, uint32_t *order_out, double *
               hyt_reorder_stats *stats);
 void csr_reorder(const hyt_csr &csr, const uint32_t *vertex_order, bool on_device, hyt_csr_buffers *out,
                  hyt_reorder_stats *stats);
+void csr_from_edges(const uint32_t *src, const uint32_t *dst, const void *weights, uint32_t wkind, uint64_t E,
+                    uint64_t V, bool on_device, hyt_csr_buffers *out, hyt_load_stats *stats);
+void load_edge_list(const char *path, uint64_t V, bool weighted, bool on_device, hyt_csr_buffers *out,
+                    hyt_load_stats *stats);
+void csr_save(const char *path, const hyt_csr &csr);
+void csr_load(const char *path, bool on_device, hyt_csr_buffers *out, hyt_load_stats *stats);
 
 }  // namespace hyt

@@ -550,12 +550,74 @@ def reorder(csr, vertex_order, device: bool = False, stats: Optional[dict] = Non
         stats.update(st.as_dict())
     if device:
         return DeviceCSR(b, csr.weight_kind)
+    return _host_csr(b)
+
+
+def _host_csr(b) -> "CSR":
+    """Host CSR of numpy copies of library-allocated host buffers (freed)."""
     V, E = int(b.num_vertices), int(b.num_edges)
     off = np.ctypeslib.as_array(b.row_offsets, shape=(V + 1,)).copy()
     cols = np.ctypeslib.as_array(b.column_indices, shape=(max(E, 1),))[:E].copy() if E else np.zeros(0, np.uint32)
     w = None
     if b.weights:
-        wa = np.ctypeslib.as_array(b.weights, shape=(max(E, 1),))[:E].copy()
-        w = wa.view(np.float32) if csr.weight_kind == capi.HYT_WEIGHTS_F32 else wa
+        wa = np.ctypeslib.as_array(b.weights, shape=(max(E, 1),))[:E].copy() if E else np.zeros(0, np.uint32)
+        w = wa.view(np.float32) if b.weight_kind == capi.HYT_WEIGHTS_F32 else wa
     check(lib.hyt_csr_buffers_free(C.byref(b)))
     return CSR(off, cols, w)
+
+
+def _wrap(b, device: bool):
+    return DeviceCSR(b, int(b.weight_kind) or capi.HYT_WEIGHTS_U32) if device else _host_csr(b)
+
+
+def load_edge_list(path, num_vertices: int, weighted: bool = False, device: bool = False,
+                   stats: Optional[dict] = None):
+    """GraphLoader::load_edge_list (hyt_load_edge_list): a text edge list ->
+    CSR (float weights when weighted), or a DeviceCSR when device=True."""
+    b, st = capi.hyt_csr_buffers(), capi.hyt_load_stats()
+    check(lib.hyt_load_edge_list(str(path).encode(), num_vertices, 1 if weighted else 0, 1 if device else 0,
+                                 C.byref(b), C.byref(st)))
+    if stats is not None:
+        stats.update(st.as_dict())
+    return _wrap(b, device)
+
+
+def csr_from_edges(src, dst, num_vertices: int, weights=None, device: bool = False, stats: Optional[dict] = None):
+    """CSR of an edge array on the GPU (hyt_csr_from_edges): edges grouped by
+    source in input order, parallel edges kept.  Arrays: numpy or CUDA
+    tensors; weights uint32 / float32 (or int32 / float32 tensors)."""
+    def arr(x, dt):
+        return np.ascontiguousarray(x, dt) if isinstance(x, (np.ndarray, list, tuple)) else x
+    s, d = arr(src, np.uint32), arr(dst, np.uint32)
+    E = int(s.shape[0])
+    if tuple(d.shape) != (E,) or (weights is not None and tuple(weights.shape) != (E,)):
+        raise HytError(capi.HYT_E_INVALID, "src, dst and weights must have one entry per edge")
+    kind = capi.HYT_WEIGHTS_NONE
+    if weights is not None:
+        is_f32 = str(getattr(weights, "dtype", "")).endswith("float32")
+        kind = capi.HYT_WEIGHTS_F32 if is_f32 else capi.HYT_WEIGHTS_U32
+        if isinstance(weights, np.ndarray) and not is_f32:
+            weights = np.ascontiguousarray(weights, np.uint32)
+    b, st = capi.hyt_csr_buffers(), capi.hyt_load_stats()
+    check(lib.hyt_csr_from_edges(_ptr(s) if E else None, _ptr(d) if E else None,
+                                 _ptr(weights) if (weights is not None and E) else None, kind, E, num_vertices,
+                                 1 if device else 0, C.byref(b), C.byref(st)))
+    if stats is not None:
+        stats.update(st.as_dict())
+    return _wrap(b, device)
+
+
+def save_csr(csr, path) -> None:
+    """Writes the binary CSR file (hyt_csr_save); csr: CSR or DeviceCSR."""
+    c = csr.to_c()
+    check(lib.hyt_csr_save(str(path).encode(), C.byref(c)))
+
+
+def load_csr(path, device: bool = False, stats: Optional[dict] = None):
+    """Reads a binary CSR file (hyt_csr_load), checking its checksum and
+    structure: a CSR, or a DeviceCSR when device=True."""
+    b, st = capi.hyt_csr_buffers(), capi.hyt_load_stats()
+    check(lib.hyt_csr_load(str(path).encode(), 1 if device else 0, C.byref(b), C.byref(st)))
+    if stats is not None:
+        stats.update(st.as_dict())
+    return _wrap(b, device)

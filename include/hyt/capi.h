@@ -46,7 +46,9 @@ enum hyt_status_code {
     HYT_E_TIMEOUT = 4,     /* a bounded device-side wait ran out */
     HYT_E_NO_DEVICE = 5,   /* no CUDA device is available */
     HYT_E_UNSUPPORTED = 6, /* valid request this build does not implement */
-    HYT_E_INTERNAL = 7     /* an internal consistency check failed */
+    HYT_E_INTERNAL = 7,    /* an internal consistency check failed */
+    HYT_E_IO = 8           /* a file could not be opened, read or written:
+                              std::runtime_error */
 };
 
 /* Message of the last failing call on this thread ("" if none). */
@@ -447,6 +449,7 @@ typedef struct hyt_csr_buffers {
     uint32_t *column_indices;
     uint32_t *weights;     /* NULL when unweighted */
     uint32_t on_device;    /* 1: cudaMalloc'd, 0: malloc'd */
+    uint32_t weight_kind;  /* HYT_WEIGHTS_* of `weights` */
 } hyt_csr_buffers;
 
 /* on_device = 0: generated on the host CPU cores; 1: on the current GPU.
@@ -496,6 +499,65 @@ int hyt_hub_sort(const hyt_csr *csr, double hub_fraction, uint32_t *vertex_order
  * stats may be NULL. */
 int hyt_csr_reorder(const hyt_csr *csr, const uint32_t *vertex_order, int on_device, hyt_csr_buffers *out,
                     hyt_reorder_stats *stats);
+
+/* ------------------------------------------------------------------ */
+/* Graph construction and loading                                       */
+/* ------------------------------------------------------------------ */
+
+/* Host / device figures of one construction or load call. */
+typedef struct hyt_load_stats {
+    double total_ms;        /* the whole call (host clock) */
+    double read_ms;         /* reading and parsing the file on host threads */
+    double device_ms;       /* the device part (uploads, kernels, downloads) */
+    double kernel_ms;       /* the main device step: the CSR construction
+                               (sort + offsets + unpack) or the load checks */
+    uint64_t file_bytes;    /* bytes read from the file */
+    uint64_t num_edges;
+    uint64_t kernel_bytes;  /* algorithmic bytes of the main device step */
+    uint32_t threads;       /* host threads used */
+    uint32_t pad;
+} hyt_load_stats;
+
+/* graph::GraphLoader::load_edge_list (src/graph/graph_loader.cpp:39-179):
+ * a text edge list, one "source destination [weight]" record per line;
+ * blank lines and lines starting with '#' are skipped; ids >= num_vertices,
+ * malformed records, a missing weight (weighted) and trailing data fail
+ * with HYT_E_INVALID and the reference's message and line number; a file
+ * that cannot be opened fails with HYT_E_IO.  The CSR keeps the file's
+ * edge order within each source and keeps parallel edges.  Weights are
+ * float (HYT_WEIGHTS_F32).  The file is parsed by host threads; the CSR is
+ * built on the GPU.  on_device: 1 = cudaMalloc'd output, 0 = malloc'd;
+ * free with hyt_csr_buffers_free.  stats may be NULL. */
+int hyt_load_edge_list(const char *path, uint64_t num_vertices, int weighted, int on_device,
+                       hyt_csr_buffers *out, hyt_load_stats *stats);
+
+/* The CSR of an edge array (the construction step of load_edge_list) on the
+ * GPU: edges stably grouped by source, parallel edges kept.  src, dst and
+ * weights (4-byte values of weight_kind, or NULL) on host or device.  An id
+ * >= num_vertices fails with HYT_E_INVALID naming the edge. */
+int hyt_csr_from_edges(const uint32_t *src, const uint32_t *dst, const void *weights, uint32_t weight_kind,
+                       uint64_t num_edges, uint64_t num_vertices, int on_device, hyt_csr_buffers *out,
+                       hyt_load_stats *stats);
+
+/* Binary CSR file (no counterpart in the reference, which reads text only).
+ * Layout, little-endian: a 64-byte header (magic "HYTCSR01", u32 version 1,
+ * u32 weight kind, u64 V, u64 E, u64 payload bytes, u64 payload checksum,
+ * u64 header checksum, u64 0), then row offsets (8 (V+1) B), column ids
+ * (4 E B) and weights (4 E B, when weighted), each padded to 8 bytes.  The
+ * checksum is the wrapping sum over the payload's 64-bit words w_i of
+ * splitmix64(w_i ^ (i * 0x9E3779B97F4A7C15)), so it is computed in
+ * parallel.  hyt_csr_save writes `path` through a temporary file and a
+ * rename; csr arrays on host or device. */
+int hyt_csr_save(const char *path, const hyt_csr *csr);
+
+/* Reads a file written by hyt_csr_save: the header, the sizes against the
+ * file size, the payload checksum and the CSR structure (offsets from 0,
+ * non-decreasing, ending at E; ids < V) are checked (HYT_E_INVALID names
+ * the failed check; HYT_E_IO for a file that cannot be read).  on_device 1
+ * streams the payload through pinned buffers into cudaMalloc'd arrays and
+ * checks it on the GPU; 0 reads into malloc'd arrays and checks on host
+ * threads. */
+int hyt_csr_load(const char *path, int on_device, hyt_csr_buffers *out, hyt_load_stats *stats);
 
 #ifdef __cplusplus
 } /* extern "C" */

@@ -147,6 +147,38 @@ class Oracle:
             raise ValueError(f"oracle_reorder rc={rc}")
         return o, c[:E], (wo[:E].view(w.dtype) if w is not None else None)
 
+    LOAD_ERRORS = {1: "unable to open file: {path}", 2: "malformed edge at line {line}",
+                   3: "vertex ID out of range at line {line}", 4: "missing edge weight at line {line}",
+                   5: "unexpected data at line {line}"}
+
+    def load_edge_list(self, path, V, weighted):
+        """GraphLoader::load_edge_list restated; returns (offsets, columns,
+        weights or None) or raises ValueError with the reference's message."""
+        E, line = C.c_uint64(), C.c_uint64()
+        rc = self.lib.oracle_load_edge_list(str(path).encode(), C.c_uint64(V), C.c_int(1 if weighted else 0),
+                                            C.byref(E), C.byref(line))
+        if rc:
+            raise ValueError("GraphLoader::load_edge_list: " + self.LOAD_ERRORS[rc].format(path=path, line=line.value))
+        o = np.empty(V + 1, np.uint64)
+        c = np.empty(max(E.value, 1), np.uint32)
+        w = np.empty(max(E.value, 1), np.float32) if weighted else None
+        self.lib.oracle_loaded_copy(_p(o), _p(c), _p(w) if w is not None else None)
+        self.lib.oracle_loaded_free()
+        return o, c[:E.value], (w[:E.value] if w is not None else None)
+
+    def csr_from_edges(self, V, src, dst, w=None):
+        E = int(src.shape[0])
+        o = np.empty(V + 1, np.uint64)
+        c = np.empty(max(E, 1), np.uint32)
+        wo = np.empty(max(E, 1), np.uint32) if w is not None else None
+        self.lib.oracle_csr_from_edges.restype = C.c_uint64
+        bad = self.lib.oracle_csr_from_edges(C.c_uint64(V), C.c_uint64(E), _p(np.ascontiguousarray(src, np.uint32)),
+                                             _p(np.ascontiguousarray(dst, np.uint32)),
+                                             _p(w.view(np.uint32)) if w is not None else None, _p(o), _p(c), _p(wo))
+        if bad:
+            raise ValueError(f"edge {bad - 1} has a vertex id >= {V}")
+        return o, c[:E], (wo[:E].view(w.dtype) if w is not None else None)
+
 
 class Reference:
     """The reference's own CPU implementation (oracle/_ref/libhytref.so)."""
@@ -233,3 +265,14 @@ class Reference:
                                          _p(np.ascontiguousarray(order, np.uint32)), _p(o), _p(c),
                                          _p(w) if w is not None else None), "ref_reorder")
         return o, c[:E], (w[:E] if w is not None else None)
+
+    def load_edge_list(self, path, V, weighted):
+        """GraphLoader::load_edge_list; returns (offsets, columns, weights or None)."""
+        E = C.c_uint64()
+        self._check(self.lib.ref_load_edge_list(str(path).encode(), C.c_uint64(V), C.c_int(1 if weighted else 0),
+                                                C.byref(E)), "ref_load_edge_list")
+        o = np.empty(V + 1, np.uint64)
+        c = np.empty(max(E.value, 1), np.uint32)
+        w = np.empty(max(E.value, 1), np.float32) if weighted else None
+        self.lib.ref_loaded_copy(_p(o), _p(c), _p(w) if w is not None else None)
+        return o, c[:E.value], (w[:E.value] if w is not None else None)

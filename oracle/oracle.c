@@ -17,6 +17,7 @@
 #include "oracle.h"
 
 #include <math.h>
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -458,5 +459,196 @@ int oracle_reorder(uint64_t V, uint64_t E, const uint64_t *off, const uint32_t *
     }
     (void)E;
     free(inv); free(seen);
+    return 0;
+}
+
+/* ---------------------------------------------------------------------
+ * Edge-list loading, restating GraphLoader::load_edge_list
+ * (src/graph/graph_loader.cpp:39-179) with the extraction rules of the
+ * C++ streams it uses (`stream >> uint64_t`, `stream >> float`,
+ * `stream >> std::string`, libstdc++):
+ *   lines split at '\n'; a line that is empty or starts with '#' after
+ *   trimming " \t\r\n" is skipped; then source, destination (unsigned:
+ *   whitespace, optional sign, decimal digits, overflow fails, '-' negates
+ *   modulo 2^64), the weight when weighted ([sign] digits [. digits]
+ *   [e [sign] digits] as accumulated by num_get, converted by strtof;
+ *   nothing converted, unconverted characters or an infinite result fail),
+ *   and any further non-blank character is an error.  Ids >= V fail.
+ *   CSR: edges stably ordered by source (file order kept within a source,
+ *   duplicates kept), offsets by counting.
+ * Error kinds: 1 cannot open, 2 malformed edge, 3 vertex id out of range,
+ * 4 missing edge weight, 5 unexpected data; *err_line = 1-based line.
+ * ------------------------------------------------------------------- */
+static int ws_char(char c) { return c == ' ' || c == '\t' || c == '\n' || c == '\v' || c == '\f' || c == '\r'; }
+static int trim_char(char c) { return c == ' ' || c == '\t' || c == '\r' || c == '\n'; }
+
+static const char *skip_ws(const char *p, const char *e) {
+    while (p < e && ws_char(*p)) ++p;
+    return p;
+}
+
+/* stream >> uint64_t */
+static int extract_u64(const char **pp, const char *e, uint64_t *out) {
+    const char *p = skip_ws(*pp, e);
+    int neg = 0, digits = 0, overflow = 0;
+    uint64_t v = 0;
+    if (p < e && (*p == '-' || *p == '+')) { neg = *p == '-'; ++p; }
+    while (p < e && *p >= '0' && *p <= '9') {
+        const uint64_t d = (uint64_t)(*p - '0');
+        if (v > (UINT64_MAX - d) / 10) overflow = 1;
+        v = v * 10 + d;
+        ++digits;
+        ++p;
+    }
+    *pp = p;
+    if (!digits || overflow) return 0;
+    *out = neg ? (uint64_t)0 - v : v;
+    return 1;
+}
+
+/* stream >> float */
+static int extract_f32(const char **pp, const char *e, float *out) {
+    const char *p = skip_ws(*pp, e);
+    char buf[512];
+    size_t n = 0;
+    int mant = 0, dec = 0, sci = 0;
+#define PUT(ch) do { if (n + 1 < sizeof(buf)) buf[n++] = (ch); } while (0)
+    if (p < e && (*p == '+' || *p == '-')) { PUT(*p); ++p; }
+    while (p < e && *p == '0') { /* leading zeros collapse to one */
+        if (!mant) { PUT('0'); mant = 1; }
+        ++p;
+    }
+    while (p < e) {
+        const char c = *p;
+        if (c == '.' && !dec && !sci) { PUT('.'); dec = 1; }
+        else if (c >= '0' && c <= '9') { PUT(c); mant = 1; }
+        else if ((c == 'e' || c == 'E') && !sci && mant) {
+            PUT('e');
+            sci = 1;
+            ++p;
+            if (p >= e) break;
+            if (*p == '+' || *p == '-') PUT(*p);
+            else continue;
+        } else break;
+        ++p;
+    }
+#undef PUT
+    buf[n] = '\0';
+    *pp = p;
+    char *end = NULL;
+    const float v = strtof(buf, &end);
+    if (end == buf || *end != '\0') return 0;
+    if (isinf(v)) return 0;
+    *out = v;
+    return 1;
+}
+
+static uint64_t g_loaded_V, g_loaded_E;
+static uint64_t *g_loaded_off;
+static uint32_t *g_loaded_cols;
+static float *g_loaded_w;
+
+void oracle_loaded_free(void) {
+    free(g_loaded_off); free(g_loaded_cols); free(g_loaded_w);
+    g_loaded_off = NULL; g_loaded_cols = NULL; g_loaded_w = NULL;
+    g_loaded_V = g_loaded_E = 0;
+}
+
+int oracle_load_edge_list(const char *path, uint64_t V, int weighted, uint64_t *E_out, uint64_t *err_line) {
+    oracle_loaded_free();
+    *E_out = 0;
+    *err_line = 0;
+    FILE *f = fopen(path, "rb");
+    if (!f) return 1;
+    fseek(f, 0, SEEK_END);
+    const long size = ftell(f);
+    fseek(f, 0, SEEK_SET);
+    char *text = (char *)malloc(size > 0 ? (size_t)size : 1);
+    if (size > 0 && fread(text, 1, (size_t)size, f) != (size_t)size) { fclose(f); free(text); return 1; }
+    fclose(f);
+    uint64_t cap = 1024, E = 0, line_no = 0;
+    uint32_t *src = (uint32_t *)malloc(cap * 4), *dst = (uint32_t *)malloc(cap * 4);
+    float *wt = (float *)malloc(cap * 4);
+    int rc = 0;
+    const char *p = text, *end = text + (size > 0 ? size : 0);
+    while (p < end) {
+        const char *nl = memchr(p, '\n', (size_t)(end - p));
+        const char *le = nl ? nl : end;
+        ++line_no;
+        const char *a = p, *b = le;
+        while (a < b && trim_char(*a)) ++a;
+        while (b > a && trim_char(b[-1])) --b;
+        p = nl ? nl + 1 : end;
+        if (a == b || *a == '#') continue;
+        uint64_t s = 0, d = 0;
+        float w = 0.0f;
+        const char *q = a;
+        if (!extract_u64(&q, b, &s) || !extract_u64(&q, b, &d)) { rc = 2; break; }
+        if (s >= V || d >= V) { rc = 3; break; }
+        if (weighted && !extract_f32(&q, b, &w)) { rc = 4; break; }
+        if (skip_ws(q, b) != b) { rc = 5; break; }
+        if (E == cap) {
+            cap *= 2;
+            src = (uint32_t *)realloc(src, cap * 4);
+            dst = (uint32_t *)realloc(dst, cap * 4);
+            wt = (float *)realloc(wt, cap * 4);
+        }
+        src[E] = (uint32_t)s;
+        dst[E] = (uint32_t)d;
+        wt[E] = w;
+        ++E;
+    }
+    free(text);
+    if (rc) {
+        *err_line = line_no;
+        free(src); free(dst); free(wt);
+        return rc;
+    }
+    /* stable counting sort by source */
+    uint64_t *off = (uint64_t *)calloc(V + 1, 8);
+    uint64_t *cur = (uint64_t *)malloc((V + 1) * 8);
+    uint32_t *cols = (uint32_t *)malloc((E ? E : 1) * 4);
+    float *wo = weighted ? (float *)malloc((E ? E : 1) * 4) : NULL;
+    for (uint64_t i = 0; i < E; ++i) ++off[src[i] + 1];
+    for (uint64_t v = 0; v < V; ++v) off[v + 1] += off[v];
+    memcpy(cur, off, (V + 1) * 8);
+    for (uint64_t i = 0; i < E; ++i) {
+        const uint64_t k = cur[src[i]]++;
+        cols[k] = dst[i];
+        if (wo) wo[k] = wt[i];
+    }
+    free(cur); free(src); free(dst); free(wt);
+    g_loaded_V = V;
+    g_loaded_E = E;
+    g_loaded_off = off;
+    g_loaded_cols = cols;
+    g_loaded_w = wo;
+    *E_out = E;
+    return 0;
+}
+
+void oracle_loaded_copy(uint64_t *off, uint32_t *cols, float *w) {
+    memcpy(off, g_loaded_off, (g_loaded_V + 1) * 8);
+    if (g_loaded_E) memcpy(cols, g_loaded_cols, g_loaded_E * 4);
+    if (w && g_loaded_w && g_loaded_E) memcpy(w, g_loaded_w, g_loaded_E * 4);
+}
+
+/* CSR from edge arrays (the loader's construction step): stable by source;
+ * returns 0, or 1 + the index of the first edge with an id >= V. */
+uint64_t oracle_csr_from_edges(uint64_t V, uint64_t E, const uint32_t *src, const uint32_t *dst, const uint32_t *w,
+                               uint64_t *off, uint32_t *cols, uint32_t *w_out) {
+    for (uint64_t i = 0; i < E; ++i)
+        if (src[i] >= V || dst[i] >= V) return i + 1;
+    memset(off, 0, (V + 1) * 8);
+    for (uint64_t i = 0; i < E; ++i) ++off[src[i] + 1];
+    for (uint64_t v = 0; v < V; ++v) off[v + 1] += off[v];
+    uint64_t *cur = (uint64_t *)malloc((V + 1) * 8);
+    memcpy(cur, off, (V + 1) * 8);
+    for (uint64_t i = 0; i < E; ++i) {
+        const uint64_t k = cur[src[i]]++;
+        cols[k] = dst[i];
+        if (w && w_out) w_out[k] = w[i];
+    }
+    free(cur);
     return 0;
 }

@@ -45,6 +45,11 @@ uint64_t oracle_task_combine(const int *engines, uint64_t n, uint64_t k, uint64_
                              int *task_engine, uint64_t *task_first);
 int oracle_hub_sort(uint64_t V, uint64_t E, const uint64_t *off, const uint32_t *cols, double fraction,
                     uint32_t *order, double *scores, uint64_t *hub_count);
+int oracle_load_edge_list(const char *path, uint64_t V, int weighted, uint64_t *E_out, uint64_t *err_line);
+void oracle_loaded_copy(uint64_t *off, uint32_t *cols, float *w);
+void oracle_loaded_free(void);
+uint64_t oracle_csr_from_edges(uint64_t V, uint64_t E, const uint32_t *src, const uint32_t *dst, const uint32_t *w,
+                               uint64_t *off, uint32_t *cols, uint32_t *w_out);
 int oracle_reorder(uint64_t V, uint64_t E, const uint64_t *off, const uint32_t *cols, const uint32_t *w,
                    const uint32_t *order, uint64_t *off_out, uint32_t *cols_out, uint32_t *w_out);
 

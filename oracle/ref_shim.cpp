@@ -12,6 +12,7 @@
 #include "graph/activity_tracker.hpp"
 #include "graph/csr_graph.hpp"
 #include "graph/partition.hpp"
+#include "graph/graph_loader.hpp"
 #include "scheduling/hub_sort.hpp"
 #include "scheduling/task_combiner.hpp"
 #include "transfer/compaction_engine.hpp"
@@ -159,6 +160,25 @@ int ref_task_combine(const int *engines, uint64_t n, uint64_t k, uint64_t *task_
         metrics[3] = plan.metrics.compaction_partitions_combined;
         metrics[4] = plan.metrics.zero_copy_partitions_combined;
     })
+}
+
+// GraphLoader::load_edge_list: loads into a holder, *E_out = edge count;
+// ref_loaded_copy then copies the arrays out (w may be NULL).
+static hytgraph::graph::CSRGraph g_loaded;
+int ref_load_edge_list(const char *path, uint64_t V, int weighted, uint64_t *E_out) {
+    REF_GUARD({
+        g_loaded = hytgraph::graph::GraphLoader::load_edge_list(path, V, weighted != 0);
+        *E_out = g_loaded.num_edges();
+    })
+}
+void ref_loaded_copy(uint64_t *off, uint32_t *cols, float *w) {
+    const auto &o = g_loaded.row_offsets();
+    const auto &c = g_loaded.column_indices();
+    const auto &x = g_loaded.edge_weights();
+    for (size_t i = 0; i < o.size(); ++i) off[i] = o[i];
+    for (size_t i = 0; i < c.size(); ++i) cols[i] = c[i];
+    if (w)
+        for (size_t i = 0; i < x.size(); ++i) w[i] = x[i];
 }
 
 // HubSorter::sort: vertex_order[V], scores[V], hub_count.

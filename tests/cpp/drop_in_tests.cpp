@@ -12,6 +12,7 @@
 #include "algorithms/sssp.hpp"
 #include "graph/activity_tracker.hpp"
 #include "graph/csr_graph.hpp"
+#include "graph/graph_loader.hpp"
 #include "graph/partition.hpp"
 #include "hyt/capi.h"
 #include "runtime/config.hpp"
@@ -24,7 +25,10 @@
 #include "transfer/zero_copy_engine.hpp"
 
 #include <cmath>
+#include <cstdio>
 #include <cstring>
+#include <fstream>
+#include <unistd.h>
 #include <functional>
 #include <iostream>
 #include <limits>
@@ -348,6 +352,28 @@ void test_gpu() {
     check(el.hub_count == 1 && el.vertex_order == std::vector<CSRGraph::vertex_id>({0, 1, 2, 3}), "edgeless");
     check(el.scores == std::vector<double>(4, 0.0), "edgeless scores");
     check(HubSorter().sort(CSRGraph(0, {0}, {})).empty(), "empty graph");
+    // GraphLoader (GPU construction): reference tests/unit_tests.cpp:374-599.
+    const std::string dir = "/tmp/hyt_dropin_" + std::to_string(::getpid());
+    const std::string f1 = dir + "_unweighted.el", f2 = dir + "_weighted.el", f3 = dir + "_bad.el",
+                      f4 = dir + ".csr";
+    std::ofstream(f1) << "# simple directed graph\n0 1\n0 2\n1 2\n2 0\n";
+    std::ofstream(f2) << "# weighted graph\n0 1 0.5\n0 2 1.25\n1 2 2.5\n";
+    std::ofstream(f3) << "0 1\n0 3\n";
+    const auto lg = graph::GraphLoader::load_edge_list(f1, 4, false);
+    check(lg.num_edges() == 4 && lg.out_degree(0) == 2 && lg.out_degree(3) == 0 && lg.neighbor_at(3) == 0,
+          "loaded unweighted graph");
+    const auto lw = graph::GraphLoader::load_edge_list(f2, 3, true);
+    check(lw.has_weights() && lw.weight_at(1) == 1.25F, "loaded weighted graph");
+    throws<std::invalid_argument>([&] { (void)graph::GraphLoader::load_edge_list(f3, 3, false); }, "id range");
+    throws<std::runtime_error>([&] { (void)graph::GraphLoader::load_edge_list(dir + "_none", 3, false); },
+                               "missing file");
+    graph::GraphLoader::save_csr(lw, f4);
+    const auto back = graph::GraphLoader::load_csr(f4);
+    check(back.row_offsets() == lw.row_offsets() && back.column_indices() == lw.column_indices() &&
+              back.edge_weights() == lw.edge_weights(),
+          "binary CSR round trip");
+    for (const auto &f : {f1, f2, f3, f4}) std::remove(f.c_str());
+
     HubSortOptions bad_fraction;
     bad_fraction.hub_fraction = 1.5;
     throws<std::invalid_argument>([&] { HubSorter h{bad_fraction}; (void)h; }, "fraction range");

@@ -226,3 +226,107 @@ def test_hub_sort_oracle_vs_reference_random(hyt, oracle, reference):
         x = oracle.reorder(g.row_offsets, g.column_indices, g.weights, order)
         y = reference.reorder(g.row_offsets, g.column_indices, g.weights.view(np.float32), order)
         assert all(np.array_equal(p.view(np.uint8), q.view(np.uint8)) for p, q in zip(x, y)), scale
+
+
+# ---------------------------------------------------------------- loader --
+LOADER_CASES = [
+    # GraphLoader cases of the reference's unit tests (unit_tests.cpp:374-599)
+    ("unweighted", "# simple directed graph\n0 1\n0 2\n1 2\n2 0\n", 4, False),
+    ("weighted", "# weighted graph\n0 1 0.5\n0 2 1.25\n1 2 2.5\n", 3, True),
+    ("parallel", "0 1\n0 1\n0 2\n", 3, False),
+    ("bad_vertex", "0 3\n", 3, False),
+    ("missing_weight", "0 1\n", 2, True),
+    ("malformed", "this is not an edge\n", 2, False),
+]
+
+
+def test_loader_known_answers(oracle, tmp_path):
+    """The expectations of unit_tests.cpp:374-599, on the oracle."""
+    got = {}
+    for name, text, V, weighted in LOADER_CASES:
+        (tmp_path / name).write_text(text)
+        try:
+            got[name] = oracle.load_edge_list(tmp_path / name, V, weighted)
+        except ValueError as e:
+            got[name] = str(e)
+    off, cols, w = got["unweighted"]
+    assert np.diff(off).tolist() == [2, 1, 1, 0] and cols.tolist() == [1, 2, 2, 0] and w is None
+    off, cols, w = got["weighted"]
+    assert cols.tolist() == [1, 2, 2] and w.tolist() == [0.5, 1.25, 2.5]
+    off, cols, w = got["parallel"]
+    assert off.tolist() == [0, 3, 3, 3] and cols.tolist() == [1, 1, 2]
+    assert got["bad_vertex"] == "GraphLoader::load_edge_list: vertex ID out of range at line 1"
+    assert got["missing_weight"] == "GraphLoader::load_edge_list: missing edge weight at line 1"
+    assert got["malformed"] == "GraphLoader::load_edge_list: malformed edge at line 1"
+
+
+def loader_corpus(seed: int, n: int):
+    """Seeded edge-list files with the record forms the reference's stream
+    extraction treats specially: signs, overflow, exponents, leading zeros,
+    comments, blank lines, CRLF, tabs, vertical tabs, trailing data."""
+    rng = np.random.default_rng(seed)
+    ints = ["0", "1", "7", "+1", "-0", "-1", "007", "18446744073709551615", "18446744073709551616", "1x", "x",
+            "", "+", "-", "2.0", "0x1", "4294967296"]
+    flts = ["0.5", "1", "-2.5", "1e3", "1E-3", ".5", "5.", ".", "1.5e", "1e+", "1e-50", "1e50", "inf", "nan",
+            "+.5e+2", "00.25", "0x1p3", "1.2.3", "3.4028235e38", "3.4028236e38", "1e-45", "7e-46", "-0", "1e5x",
+            "", "e5", "+e5", "0.1", "123456789", "1.00000005960464477539062500001"]
+    seps = [" ", "\t", "  ", " \t ", "\v", ","]
+
+    def line(weighted):
+        if rng.random() < 0.05:
+            return str(rng.choice(["", "   ", "\t", "# comment", "  # c", "#", "\r"]))
+        parts = [str(rng.choice(ints)) if rng.random() < 0.08 else str(rng.integers(0, 8)) for _ in range(2)]
+        if weighted and rng.random() < 0.97:
+            parts.append(str(rng.choice(flts)) if rng.random() < 0.5 else f"{rng.random() * 10:.{rng.integers(0, 9)}f}")
+        if rng.random() < 0.05:
+            parts.append(str(rng.choice(["x", "1", "#"])))
+        s = parts[0]
+        for p in parts[1:]:
+            s += str(rng.choice(seps)) + p
+        if rng.random() < 0.2:
+            s = str(rng.choice([" ", "\t", "\r"])) + s
+        if rng.random() < 0.2:
+            s += str(rng.choice([" ", "\t", "\r", "\r\r"]))
+        return s
+
+    for _ in range(n):
+        weighted = bool(rng.integers(0, 2))
+        text = "\n".join(line(weighted) for _ in range(int(rng.integers(1, 6))))
+        yield text + ("\n" if rng.random() < 0.5 else ""), 8, weighted
+
+
+def _load_or_error(loader, path, V, weighted):
+    try:
+        return loader(path, V, weighted)
+    except ValueError as e:
+        return str(e).split(": ", 1)[1] if str(e).startswith("ref_") else str(e)
+
+
+def test_loader_oracle_vs_reference_corpus(oracle, reference, tmp_path):
+    """The oracle's record rules equal the reference's GraphLoader (run here
+    from its own sources) on 1500 seeded files: same arrays, or the same
+    error message and line."""
+    path = tmp_path / "f.el"
+    for i, (text, V, weighted) in enumerate(loader_corpus(7, 1500)):
+        path.write_text(text)
+        a = _load_or_error(oracle.load_edge_list, path, V, weighted)
+        b = _load_or_error(reference.load_edge_list, path, V, weighted)
+        if isinstance(a, str) or isinstance(b, str):
+            assert a == b, (i, text)
+            continue
+        for x, y in zip(a, b):
+            assert (x is None and y is None) or np.array_equal(x.view(np.uint8), y.view(np.uint8)), (i, text)
+
+
+def test_csr_from_edges_oracle(oracle):
+    rng = np.random.default_rng(4)
+    V, E = 300, 5000
+    src = rng.integers(0, V, E).astype(np.uint32)
+    dst = rng.integers(0, V, E).astype(np.uint32)
+    w = rng.random(E).astype(np.float32)
+    off, cols, wo = oracle.csr_from_edges(V, src, dst, w)
+    order = np.argsort(src, kind="stable")
+    assert np.array_equal(cols, dst[order]) and np.array_equal(wo, w[order])
+    assert np.array_equal(off, np.concatenate([[0], np.cumsum(np.bincount(src, minlength=V))]).astype(np.uint64))
+    with pytest.raises(ValueError):
+        oracle.csr_from_edges(V, np.array([1, V], np.uint32), np.array([0, 0], np.uint32))
