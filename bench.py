@@ -48,12 +48,14 @@ def parse_args():
     ap.add_argument("--seed", type=int, default=20241203)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["inhbm", "hybrid", "batch", "serve", "hubsort"], default="inhbm",
+    ap.add_argument("--workload", choices=["inhbm", "hybrid", "batch", "serve", "hubsort", "load"], default="inhbm",
                     help="inhbm: graph resident in HBM (default); hybrid: edges in pinned host memory under a "
                          "device budget (defaults to R-MAT scale 27, edge factor 32, 8 GiB); batch: 64 graphs of "
                          "scales 12-20, 512 SSSP/PPR queries in one CUDA-graph launch; serve: continuous "
-                         "batching of a Poisson stream; hubsort: hub sorting + vertex reordering of the graph")
+                         "batching of a Poisson stream; hubsort: hub sorting + vertex reordering of the graph; load: "
+                         "text edge list -> CSR in HBM (GraphLoader) and the binary CSR file")
     ap.add_argument("--hub-fraction", type=float, default=0.08)
+    ap.add_argument("--text-scale", type=int, default=22, help="load: R-MAT scale of the text edge list")
     ap.add_argument("--no-effect", action="store_true", help="hubsort: skip the solver comparison")
     ap.add_argument("--requests", type=int, default=20000)
     ap.add_argument("--rates", type=str, default="200,500,1000,2000,5000")
@@ -838,6 +840,170 @@ def run_hubsort_workload(args, rank, world, local, pg):
         print(json.dumps(line), flush=True)
 
 
+def write_edge_text(path, src, dst, w=None, V=1):
+    """Writes "source destination [weight]" lines with fixed-width decimal
+    fields (leading zeros are plain decimal to the loader), vectorised."""
+    nd = max(1, len(str(max(V - 1, 1))))
+    nw = 0 if w is None else max(1, len(str(int(w.max()) if w.size else 1)))
+
+    def digits(x, n):
+        out = np.empty((x.shape[0], n), np.uint8)
+        y = x.astype(np.uint64)
+        for k in range(n - 1, -1, -1):
+            out[:, k] = (y % 10).astype(np.uint8) + 48
+            y //= 10
+        return out
+
+    with open(path, "wb") as f:
+        f.write(b"# R-MAT edge list: source destination" + (b" weight" if w is not None else b"") + b"\n")
+        step = 1 << 22
+        for b in range(0, src.shape[0], step):
+            e = min(b + step, src.shape[0])
+            n = e - b
+            parts = [digits(src[b:e], nd), np.full((n, 1), 32, np.uint8), digits(dst[b:e], nd)]
+            if w is not None:
+                parts += [np.full((n, 1), 32, np.uint8), digits(w[b:e], nw)]
+            parts.append(np.full((n, 1), 10, np.uint8))
+            f.write(np.concatenate(parts, axis=1).tobytes())
+
+
+def pinned_h2d_gbs():
+    """Best pinned host->device copy bandwidth of 256 MiB (GB/s)."""
+    import torch
+
+    h = torch.empty(256 << 20, dtype=torch.uint8, pin_memory=True)
+    d = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    best = 0.0
+    for _ in range(6):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        d.copy_(h, non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize()
+        best = max(best, (256 << 20) / (e0.elapsed_time(e1) / 1e3) / 1e9)
+    return best
+
+
+def load_config(args, V, E, Vt, Et):
+    return {"workload": f"GraphLoader::load_edge_list of an R-MAT scale {args.text_scale} edge factor "
+                        f"{args.edge_factor} text edge list with uint weights (file -> CSR in HBM), and the binary "
+                        f"CSR file of R-MAT scale {args.scale} (file -> CSR in HBM), page cache warm",
+            "text_scale": args.text_scale, "text_vertices": Vt, "text_edges": Et, "binary_scale": args.scale,
+            "binary_vertices": V, "binary_edges": E, "edge_factor": args.edge_factor, "seed": args.seed,
+            "parallelism": f"replicas x{args.gpus}"}
+
+
+def run_load_workload(args, rank, world, local, pg):
+    """One step = hyt_load_edge_list of the text file to the device + the
+    CSR construction; the binary file's device load is timed beside it."""
+    import shutil
+    import tempfile
+
+    import torch
+
+    import hytgraph_b200 as hyt
+
+    peak_gbs, peak_kind = load_peaks()
+    tmp = tempfile.mkdtemp(prefix="hyt_load_")
+    try:
+        # text edge list, records in CSR order
+        t = hyt.rmat(args.text_scale, args.edge_factor, args.seed)
+        Vt, Et = t.num_vertices, t.num_edges
+        src = np.repeat(np.arange(Vt, dtype=np.uint32), np.diff(t.row_offsets).astype(np.int64))
+        text_path = os.path.join(tmp, "g.el")
+        write_edge_text(text_path, src, t.column_indices, t.weights, Vt)
+        text_bytes = os.path.getsize(text_path)
+        sample_path = os.path.join(tmp, "sample.el")
+        ns = min(Et, 1 << 21)
+        write_edge_text(sample_path, src[:ns], t.column_indices[:ns], t.weights[:ns], Vt)
+        del t, src
+        # binary file of the larger graph
+        d = hyt.rmat(args.scale, args.edge_factor, args.seed, device=True)
+        V, E = d.num_vertices, d.num_edges
+        bin_path = os.path.join(tmp, "g.csr")
+        hyt.save_csr(d, bin_path)
+        d.free()
+        bin_bytes = os.path.getsize(bin_path)
+
+        def step(collect):
+            st = {}
+            g = hyt.load_edge_list(text_path, Vt, True, device=True, stats=st)
+            g.free()
+            collect.append(st)
+
+        warm = []
+        for _ in range(args.warmup):
+            step(warm)
+        clocks = ClockSampler(local)
+        clocks.start()
+        timed = []
+        barrier(pg)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            step(timed)
+        barrier(pg)
+        ms = max_over_ranks(pg, 1e3 * (time.perf_counter() - t0))
+        clk = clocks.stop()
+        value = replica_value(Et * args.steps, world, ms) / 1e9
+        kms = sum(x["kernel_ms"] for x in timed) / args.steps
+        kb = timed[0]["kernel_bytes"]
+        roof = {"kernel": "CSR construction (pack + radix sort + offsets + unpack)", "bound": "hbm",
+                "achieved": kb / (kms / 1e3) / 1e9, "peak": peak_gbs, "unit": "GB/s",
+                "frac": kb / (kms / 1e3) / 1e9 / peak_gbs, "traffic": None, "peak_kind": peak_kind,
+                "algorithmic_bytes_per_launch": kb, "avg_launch_ms": kms,
+                "note": "algorithmic bytes = edges read and written once + offsets; the radix sort's passes "
+                        "are the overhead"}
+        parse_ms = sum(x["read_ms"] for x in timed) / args.steps
+        # binary file -> device
+        link = pinned_h2d_gbs()
+        bl = []
+        for i in range(args.warmup + args.steps):
+            st = {}
+            g = hyt.load_csr(bin_path, device=True, stats=st)
+            g.free()
+            if i >= args.warmup:
+                bl.append(st)
+        b_ms = sum(x["total_ms"] for x in bl) / len(bl)
+        binary = {"file_bytes": bin_bytes, "ms_per_load": b_ms, "gbs": bin_bytes / (b_ms / 1e3) / 1e9,
+                  "pinned_h2d_gbs": link, "frac_of_h2d": bin_bytes / (b_ms / 1e3) / 1e9 / link,
+                  "read_threads": bl[0]["threads"], "check_ms": sum(x["kernel_ms"] for x in bl) / len(bl),
+                  "edges_per_s": E / (b_ms / 1e3)}
+        cpu = None
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            tc, kind = reference_load(sample_path, Vt)
+            cpu = {"value": ns / tc / 1e9, "unit": "Gedges/s", "cores": 1, "kind": kind,
+                   "sample": f"GraphLoader::load_edge_list of the first {ns} edges of the same file, {tc:.1f} s"}
+        if rank == 0:
+            line = {"metric": "edge-list load throughput (file -> CSR in HBM)", "value": value, "unit": "Gedges/s",
+                    "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+                    "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                    "dtype": "u32 ids, f32 weights", "data": "synthetic", "config": load_config(args, V, E, Vt, Et),
+                    "e2e": {"value": value, "unit": "Gedges/s", "h2d_bytes_per_step": Et * 12,
+                            "d2h_bytes_per_step": 0, "note": "the step is already host file -> device CSR"},
+                    "text": {"file_bytes": text_bytes, "parse_ms": parse_ms,
+                             "parse_gbs": text_bytes / (parse_ms / 1e3) / 1e9, "threads": timed[0]["threads"],
+                             "device_ms": sum(x["device_ms"] for x in timed) / args.steps},
+                    "binary": binary, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
+                    "gpu_launches": 5 * args.steps}
+            print(json.dumps(line), flush=True)
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
+def reference_load(path, V):
+    """The reference's GraphLoader::load_edge_list (its own compiled code when
+    available, else the oracle's restatement) on `path`: (seconds, kind)."""
+    from oracle.bindings import Oracle, Reference
+
+    if Reference.available():
+        t0 = time.perf_counter()
+        Reference().load_edge_list(path, V, True)
+        return time.perf_counter() - t0, "reference"
+    t0 = time.perf_counter()
+    Oracle().load_edge_list(path, V, True)
+    return time.perf_counter() - t0, "port"
+
+
 def workload_config(args, V, E):
     return {"workload": f"in-HBM R-MAT scale {args.scale} edge factor {args.edge_factor}: PageRank to L1<=1e-6 "
                         f"+ SSSP from {args.sources} seeded sources",
@@ -870,6 +1036,11 @@ def main():
         return
     if args.workload == "batch":
         run_batch_workload(args, rank, world, pg)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
+    if args.workload == "load":
+        run_load_workload(args, rank, world, local, pg)
         if pg is not None:
             pg.destroy_process_group()
         return

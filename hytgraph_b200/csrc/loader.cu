@@ -2,17 +2,21 @@
 // hyt_csr_save, hyt_csr_load.
 //
 // Text edge lists follow GraphLoader::load_edge_list
-// (src/graph/graph_loader.cpp:39-179).  The file is mapped and cut into
-// line-aligned chunks parsed by host threads with the reference's record
-// rules (the extraction rules of `stream >> uint64_t`, `stream >> float` and
-// `stream >> std::string`, as libstdc++ applies them); the first failing
-// line in file order is reported, with the reference's message.  The edges
-// then go to the GPU, which builds the CSR: a stable radix sort of
-// (source, destination[, weight]) pairs on the source bits keeps the file
-// order within a source and keeps parallel edges (the reference's
-// std::stable_sort by source), row offsets come from a lower-bound search
-// per vertex, and the sorted pairs are unpacked into the column and weight
-// arrays.
+// (src/graph/graph_loader.cpp:39-179).  The file's bytes stream into HBM
+// through the pinned ring; the GPU finds the line starts (a select over
+// byte positions), parses every line in its own thread with the
+// reference's record rules (the extraction rules of `stream >> uint64_t`,
+// `stream >> float` and `stream >> std::string`, as libstdc++ applies them),
+// and reports the first failing line in file order with the reference's
+// message.  A weight whose strtof value is one correctly rounded float
+// division (at most 7 significant and 10 fractional digits, no exponent)
+// is converted on the GPU; the host re-parses the rare other forms with
+// the exact rules.  The kept records are compacted in file order and the
+// GPU builds the CSR: a stable radix sort of (source, destination[,
+// weight]) pairs on the source bits keeps the file order within a source
+// and keeps parallel edges (the reference's std::stable_sort by source),
+// row offsets come from a lower-bound search per vertex, and the sorted
+// pairs are unpacked into the column and weight arrays.
 //
 // The binary CSR format is this library's own (the reference reads text
 // only); its layout and checksum are declared in hyt/capi.h.  Loading to
@@ -36,6 +40,7 @@
 #include <vector>
 
 #include <cub/cub.cuh>
+#include <thrust/iterator/counting_iterator.h>
 
 #include "common.cuh"
 #include "scratch.cuh"
@@ -46,6 +51,8 @@ namespace {
 using Clock = std::chrono::steady_clock;
 
 double ms_since(Clock::time_point t0) { return std::chrono::duration<double, std::milli>(Clock::now() - t0).count(); }
+
+unsigned grid_sm(unsigned per_sm) { return static_cast<unsigned>(sm_count()) * per_sm; }
 
 unsigned host_threads(uint64_t work_bytes, uint64_t bytes_per_thread = uint64_t(4) << 20) {
     unsigned n = std::thread::hardware_concurrency();
@@ -91,17 +98,17 @@ struct Fd {
 
 enum : int { kRecOk = 0, kRecMalformed = 2, kRecRange = 3, kRecMissingWeight = 4, kRecTrailing = 5 };
 
-inline bool ws_char(char c) { return c == ' ' || c == '\t' || c == '\n' || c == '\v' || c == '\f' || c == '\r'; }
-inline bool trim_char(char c) { return c == ' ' || c == '\t' || c == '\r' || c == '\n'; }
+__host__ __device__ inline bool ws_char(char c) { return c == ' ' || c == '\t' || c == '\n' || c == '\v' || c == '\f' || c == '\r'; }
+__host__ __device__ inline bool trim_char(char c) { return c == ' ' || c == '\t' || c == '\r' || c == '\n'; }
 
-inline const char *skip_ws(const char *p, const char *e) {
+__host__ __device__ inline const char *skip_ws(const char *p, const char *e) {
     while (p < e && ws_char(*p)) ++p;
     return p;
 }
 
 // `stream >> uint64_t`: whitespace, an optional sign, decimal digits; no
 // digit or overflow fails; '-' negates modulo 2^64.
-bool extract_u64(const char *&p, const char *e, uint64_t &out) {
+__host__ __device__ bool extract_u64(const char *&p, const char *e, uint64_t &out) {
     p = skip_ws(p, e);
     bool neg = false, overflow = false;
     int digits = 0;
@@ -180,54 +187,173 @@ bool extract_f32(const char *&p, const char *e, float &out) {
     return true;
 }
 
-struct Chunk {
-    const char *b = nullptr, *e = nullptr;
-    std::vector<uint32_t> src, dst;
-    std::vector<float> w;
-    uint64_t lines = 0;
-    int err = kRecOk;
-    uint64_t err_line = 0;  // 1-based within the chunk
+// The record of one line, on the host (the exact rules, for lines the GPU
+// hands back): status kRecOk (edge), 1 (blank / comment) or an error kind.
+int host_record(const char *a, const char *z, uint64_t V, bool weighted, uint32_t &s32, uint32_t &d32, uint32_t &w32) {
+    while (a < z && trim_char(*a)) ++a;
+    while (z > a && trim_char(z[-1])) --z;
+    if (a == z || *a == '#') return 1;
+    uint64_t s = 0, d = 0;
+    float wt = 0.0f;
+    const char *q = a;
+    if (!extract_u64(q, z, s) || !extract_u64(q, z, d)) return kRecMalformed;
+    if (s >= V || d >= V) return kRecRange;
+    if (weighted && !extract_f32(q, z, wt)) return kRecMissingWeight;
+    if (skip_ws(q, z) != z) return kRecTrailing;
+    s32 = static_cast<uint32_t>(s);
+    d32 = static_cast<uint32_t>(d);
+    std::memcpy(&w32, &wt, 4);
+    return kRecOk;
+}
+
+// ------------------------------ records on the GPU ------------------------
+
+constexpr uint8_t kLineSkip = 1;  // blank or comment
+constexpr uint8_t kLineSlow = 6;  // a weight the GPU leaves to the host
+
+__global__ void count_newlines_kernel(const char *__restrict__ text, uint64_t n, unsigned long long *count) {
+    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+    uint64_t c = 0;
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += stride) c += text[i] == '\n';
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, static_cast<unsigned long long>(c));
+}
+
+struct LineStart {
+    const char *text;
+    __device__ bool operator()(uint64_t p) const { return p == 0 || text[p - 1] == '\n'; }
 };
 
-// Parses the lines of [c.b, c.e) (both ends at line starts); stops at the
-// chunk's first failing record.
-void parse_chunk(Chunk &c, uint64_t V, bool weighted) {
-    const uint64_t guess = static_cast<uint64_t>(c.e - c.b) / 8 + 16;
-    c.src.reserve(guess);
-    c.dst.reserve(guess);
-    if (weighted) c.w.reserve(guess);
-    const char *p = c.b;
-    while (p < c.e) {
-        const char *nl = static_cast<const char *>(std::memchr(p, '\n', static_cast<size_t>(c.e - p)));
-        const char *le = nl ? nl : c.e;
-        ++c.lines;
-        const char *a = p, *z = le;
-        p = nl ? nl + 1 : c.e;
+// `stream >> float` for the forms whose strtof result one correctly rounded
+// float division gives: [sign] digits [. digits], at most 7 significant
+// digits and 10 fractional digits, no exponent.  m and 10^k are then exact
+// floats and m / 10^k rounds once, as strtof does.  Returns 1 (value), 0
+// (no number: the reference fails) or 2 (another form: the host decides).
+__device__ int extract_f32_fast(const char *&p, const char *e, float &out) {
+    p = skip_ws(p, e);
+    bool neg = false, dec = false, mant = false;
+    if (p < e && (*p == '+' || *p == '-')) {
+        neg = *p == '-';
+        ++p;
+    }
+    uint32_t m = 0;
+    int sig = 0, frac = 0;
+    for (; p < e; ++p) {
+        const char c = *p;
+        if (c == '.' && !dec) {
+            dec = true;
+        } else if (c >= '0' && c <= '9') {
+            mant = true;
+            if (dec) ++frac;
+            if (m == 0 && c == '0') continue;  // leading zero
+            if (++sig > 7) return 2;
+            m = m * 10 + static_cast<uint32_t>(c - '0');
+        } else {
+            break;
+        }
+    }
+    if (!mant) return 0;
+    if (p < e && (*p == 'e' || *p == 'E')) return 2;
+    if (frac > 10) return 2;
+    const float pow10[11] = {1e0f, 1e1f, 1e2f, 1e3f, 1e4f, 1e5f, 1e6f, 1e7f, 1e8f, 1e9f, 1e10f};
+    const float v = __fdiv_rn(static_cast<float>(m), pow10[frac]);
+    out = neg ? -v : v;
+    return 1;
+}
+
+// One thread per line: the line's status and, for an edge, its fields.
+__global__ void parse_lines_kernel(const char *__restrict__ text, uint64_t size, const uint64_t *__restrict__ ls,
+                                   uint64_t L, uint64_t V, bool weighted, uint8_t *__restrict__ status,
+                                   uint32_t *__restrict__ s_out, uint32_t *__restrict__ d_out,
+                                   uint32_t *__restrict__ w_out, unsigned long long *__restrict__ first_error,
+                                   unsigned long long *__restrict__ slow) {
+    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < L; i += stride) {
+        const char *a = text + ls[i];
+        const char *z = text + (i + 1 < L ? ls[i + 1] : size);
         while (a < z && trim_char(*a)) ++a;
         while (z > a && trim_char(z[-1])) --z;
-        if (a == z || *a == '#') continue;
-        uint64_t s = 0, d = 0;
-        float wt = 0.0f;
-        const char *q = a;
-        int rc = kRecOk;
-        if (!extract_u64(q, z, s) || !extract_u64(q, z, d)) {
-            rc = kRecMalformed;
-        } else if (s >= V || d >= V) {
-            rc = kRecRange;
-        } else if (weighted && !extract_f32(q, z, wt)) {
-            rc = kRecMissingWeight;
-        } else if (skip_ws(q, z) != z) {
-            rc = kRecTrailing;
+        uint8_t st = kRecOk;
+        uint32_t s32 = 0, d32 = 0, w32 = 0;
+        if (a == z || *a == '#') {
+            st = kLineSkip;
+        } else {
+            uint64_t sv = 0, dv = 0;
+            const char *q = a;
+            if (!extract_u64(q, z, sv) || !extract_u64(q, z, dv)) {
+                st = kRecMalformed;
+            } else if (sv >= V || dv >= V) {
+                st = kRecRange;
+            } else {
+                float wt = 0.0f;
+                const int r = weighted ? extract_f32_fast(q, z, wt) : 1;
+                if (r == 0) {
+                    st = kRecMissingWeight;
+                } else if (r == 2) {
+                    st = kLineSlow;
+                } else if (skip_ws(q, z) != z) {
+                    st = kRecTrailing;
+                }
+                s32 = static_cast<uint32_t>(sv);
+                d32 = static_cast<uint32_t>(dv);
+                w32 = __float_as_uint(wt);
+            }
         }
-        if (rc != kRecOk) {
-            c.err = rc;
-            c.err_line = c.lines;
-            return;
-        }
-        c.src.push_back(static_cast<uint32_t>(s));
-        c.dst.push_back(static_cast<uint32_t>(d));
-        if (weighted) c.w.push_back(wt);
+        status[i] = st;
+        s_out[i] = s32;
+        d_out[i] = d32;
+        if (w_out) w_out[i] = w32;
+        if (st >= kRecMalformed && st <= kRecTrailing) atomicMin(first_error, static_cast<unsigned long long>(i));
+        if (st == kLineSlow) atomicAdd(slow, 1ull);
     }
+}
+
+// The host's verdicts for the lines the GPU left to it.
+__global__ void patch_lines_kernel(const uint64_t *__restrict__ idx, const uint8_t *__restrict__ st,
+                                   const uint32_t *__restrict__ sv, const uint32_t *__restrict__ dv,
+                                   const uint32_t *__restrict__ wv, uint64_t n, uint8_t *__restrict__ status,
+                                   uint32_t *__restrict__ s, uint32_t *__restrict__ d, uint32_t *__restrict__ w) {
+    for (uint64_t k = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; k < n; k += uint64_t(gridDim.x) * blockDim.x) {
+        const uint64_t i = idx[k];
+        status[i] = st[k];
+        s[i] = sv[k];
+        d[i] = dv[k];
+        if (w) w[i] = wv[k];
+    }
+}
+
+__global__ void line_bounds_kernel(const uint64_t *__restrict__ ls, uint64_t L, uint64_t size,
+                                   const uint64_t *__restrict__ idx, uint64_t n, uint64_t *__restrict__ b,
+                                   uint64_t *__restrict__ e) {
+    for (uint64_t k = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; k < n; k += uint64_t(gridDim.x) * blockDim.x) {
+        const uint64_t i = idx[k];
+        b[k] = ls[i];
+        e[k] = i + 1 < L ? ls[i + 1] : size;
+    }
+}
+
+__global__ void edge_flags_kernel(const uint8_t *__restrict__ status, uint64_t L, uint64_t *__restrict__ flag) {
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < L; i += uint64_t(gridDim.x) * blockDim.x)
+        flag[i] = status[i] == kRecOk;
+}
+
+__global__ void compact_edges_kernel(const uint8_t *__restrict__ status, const uint64_t *__restrict__ pos, uint64_t L,
+                                     const uint32_t *__restrict__ s, const uint32_t *__restrict__ d,
+                                     const uint32_t *__restrict__ w, uint32_t *__restrict__ cs,
+                                     uint32_t *__restrict__ cd, uint32_t *__restrict__ cw) {
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < L; i += uint64_t(gridDim.x) * blockDim.x) {
+        if (status[i] != kRecOk) continue;
+        const uint64_t k = pos[i];
+        cs[k] = s[i];
+        cd[k] = d[i];
+        if (w) cw[k] = w[i];
+    }
+}
+
+__global__ void slow_flags_kernel(const uint8_t *__restrict__ status, uint64_t L, uint8_t *__restrict__ flag) {
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < L; i += uint64_t(gridDim.x) * blockDim.x)
+        flag[i] = status[i] == kLineSlow;
 }
 
 // ------------------------------ CSR construction --------------------------
@@ -537,12 +663,13 @@ void write_all(int fd, const void *p, uint64_t n, const std::string &path) {
     }
 }
 
-void read_all(int fd, void *p, uint64_t n, uint64_t at, const std::string &path) {
+// Reads n bytes at `at`; `what` names the file in the error message.
+void read_all(int fd, void *p, uint64_t n, uint64_t at, const std::string &what) {
     char *c = static_cast<char *>(p);
     while (n) {
         const ssize_t k = ::pread(fd, c, std::min<uint64_t>(n, uint64_t(1) << 30), static_cast<off_t>(at));
         if (k < 0 && errno == EINTR) continue;
-        if (k <= 0) fail(HYT_E_IO, "error while reading file: " + path);
+        if (k <= 0) fail(HYT_E_IO, what);
         c += k;
         n -= static_cast<uint64_t>(k);
         at += static_cast<uint64_t>(k);
@@ -573,6 +700,50 @@ struct Piece {
     char *dst;
     uint64_t bytes;
 };
+
+// Streams file pieces into device memory through the pinned ring: reader
+// thread t owns ring buffer t and its own stream, reads its pieces (t,
+// t + threads, ...) and copies each one once the buffer's previous copy has
+// finished.  Returns the number of reader threads.
+unsigned stream_to_device(int fd, const std::vector<Piece> &pieces, const std::string &path) {
+    int dev = 0;
+    HYT_CUDA(cudaGetDevice(&dev));
+    PinnedRing &r = ring();
+    std::lock_guard<std::mutex> lk(r.mu);
+    r.init();
+    const unsigned threads = static_cast<unsigned>(std::min<size_t>(kRing, std::max<size_t>(pieces.size(), 1)));
+    parallel_for(threads, [&](unsigned t) {
+        HYT_CUDA(cudaSetDevice(dev));
+        cudaStream_t cs = nullptr;
+        cudaEvent_t done = nullptr;
+        HYT_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        HYT_CUDA(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+        struct Release {
+            cudaStream_t s;
+            cudaEvent_t e;
+            ~Release() {
+                cudaStreamSynchronize(s);
+                cudaEventDestroy(e);
+                cudaStreamDestroy(s);
+            }
+        } rel{cs, done};
+        bool pending = false;
+        for (size_t k = t; k < pieces.size(); k += threads) {
+            if (pending) HYT_CUDA(cudaEventSynchronize(done));  // this buffer's last copy
+            read_all(fd, r.buf[t], pieces[k].bytes, pieces[k].file_at, path);
+            HYT_CUDA(cudaMemcpyAsync(pieces[k].dst, r.buf[t], pieces[k].bytes, cudaMemcpyHostToDevice, cs));
+            HYT_CUDA(cudaEventRecord(done, cs));
+            pending = true;
+        }
+    });
+    return threads;
+}
+
+std::vector<Piece> cut(uint64_t file_at, char *dst, uint64_t bytes) {
+    std::vector<Piece> v;
+    for (uint64_t d = 0; d < bytes; d += kRingBytes) v.push_back({file_at + d, dst + d, std::min(kRingBytes, bytes - d)});
+    return v;
+}
 
 }  // namespace
 
@@ -635,65 +806,142 @@ void load_edge_list(const char *path, uint64_t V, bool weighted, bool on_device,
     struct stat sb {};
     if (::fstat(f.fd, &sb) != 0) fail(HYT_E_IO, "GraphLoader::load_edge_list: error while reading file: " + p);
     const uint64_t size = static_cast<uint64_t>(sb.st_size);
-    const char *text = nullptr;
-    if (size) {
-        void *m = ::mmap(nullptr, size, PROT_READ, MAP_PRIVATE, f.fd, 0);
-        if (m == MAP_FAILED) fail(HYT_E_IO, "GraphLoader::load_edge_list: error while reading file: " + p);
-        ::madvise(m, size, MADV_SEQUENTIAL | MADV_WILLNEED);
-        text = static_cast<const char *>(m);
-    }
-    struct Unmap {
-        const char *t;
-        uint64_t n;
-        ~Unmap() {
-            if (t) ::munmap(const_cast<char *>(t), n);
-        }
-    } unmap{text, size};
-    // line-aligned chunks: chunk i starts at the first line start >= i*size/T
-    const unsigned T = size ? host_threads(size) : 1;
-    std::vector<uint64_t> start(T + 1, size);
-    start[0] = 0;
-    for (unsigned i = 1; i < T; ++i) {
-        const uint64_t b = size * i / T;
-        const char *nl = static_cast<const char *>(std::memchr(text + b - 1, '\n', size - (b - 1)));
-        start[i] = nl ? static_cast<uint64_t>(nl - text) + 1 : size;
-        start[i] = std::max(start[i], start[i - 1]);
-    }
-    std::vector<Chunk> chunks(T);
-    for (unsigned i = 0; i < T; ++i) {
-        chunks[i].b = text + start[i];
-        chunks[i].e = text + std::max(start[i], start[i + 1]);
-    }
-    parallel_for(T, [&](unsigned i) { parse_chunk(chunks[i], V, weighted); });
-    uint64_t lines_before = 0, E = 0;
-    for (const Chunk &c : chunks) {
-        if (c.err != kRecOk) {
-            static const char *what[] = {"", "", "malformed edge", "vertex ID out of range", "missing edge weight",
-                                         "unexpected data"};
-            fail(HYT_E_INVALID, std::string("GraphLoader::load_edge_list: ") + what[c.err] + " at line " +
-                                    std::to_string(lines_before + c.err_line));
-        }
-        lines_before += c.lines;
-        E += c.src.size();
-    }
-    const double read_ms = ms_since(t0);
     StreamHold st;
     cudaStream_t s = st.s;
+    // 1. the raw bytes into HBM (zero padding after them)
+    Scratch<char> text(size + 64, s);
+    HYT_CUDA(cudaMemsetAsync(text.get() + size, 0, 64, s));
+    HYT_CUDA(cudaStreamSynchronize(s));
+    const unsigned threads = size ? stream_to_device(f.fd, cut(0, text.get(), size),
+                                                        "GraphLoader::load_edge_list: error while reading file: " + p) : 1;
+    const double read_ms = ms_since(t0);
     EventTimer whole;
     whole.start(s);
-    Scratch<uint32_t> ds(E, s), dd(E, s);
-    std::unique_ptr<Scratch<uint32_t>> dw;
-    if (weighted) dw = std::make_unique<Scratch<uint32_t>>(E, s);
-    uint64_t at = 0;
-    for (const Chunk &c : chunks) {
-        const uint64_t n = c.src.size();
-        if (!n) continue;
-        HYT_CUDA(cudaMemcpyAsync(ds.get() + at, c.src.data(), n * 4, cudaMemcpyHostToDevice, s));
-        HYT_CUDA(cudaMemcpyAsync(dd.get() + at, c.dst.data(), n * 4, cudaMemcpyHostToDevice, s));
-        if (weighted) HYT_CUDA(cudaMemcpyAsync(dw->get() + at, c.w.data(), n * 4, cudaMemcpyHostToDevice, s));
-        at += n;
+    // 2. line starts: position 0 and every position after a '\n'
+    uint64_t L = 0;
+    if (size) {
+        Scratch<unsigned long long> cnt(1, s);
+        HYT_CUDA(cudaMemsetAsync(cnt.get(), 0, 8, s));
+        count_newlines_kernel<<<grid_sm(8), 256, 0, s>>>(text.get(), size - 1, cnt.get());
+        unsigned long long h = 0;
+        HYT_CUDA(cudaMemcpyAsync(&h, cnt.get(), 8, cudaMemcpyDeviceToHost, s));
+        HYT_CUDA(cudaStreamSynchronize(s));
+        L = h + 1;  // newlines before the last byte each start a line
     }
-    const double kms = build_csr(ds.get(), dd.get(), weighted ? dw->get() : nullptr, E, V,
+    Scratch<uint64_t> ls(L + 1, s), nsel(1, s);
+    if (L) {
+        thrust::counting_iterator<uint64_t> it(0);
+        LineStart pred{text.get()};
+        size_t tb = 0;
+        HYT_CUDA(cub::DeviceSelect::If(nullptr, tb, it, ls.get(), nsel.get(), static_cast<int64_t>(size), pred, s));
+        Scratch<uint8_t> tmp(tb, s);
+        HYT_CUDA(cub::DeviceSelect::If(tmp.get(), tb, it, ls.get(), nsel.get(), static_cast<int64_t>(size), pred, s));
+    }
+    // 3. every line's record
+    Scratch<uint8_t> status(L, s);
+    Scratch<uint32_t> sv(L, s), dv(L, s);
+    std::unique_ptr<Scratch<uint32_t>> wv;
+    if (weighted) wv = std::make_unique<Scratch<uint32_t>>(L, s);
+    Scratch<unsigned long long> first(1, s), slow(1, s);
+    HYT_CUDA(cudaMemsetAsync(first.get(), 0xFF, 8, s));
+    HYT_CUDA(cudaMemsetAsync(slow.get(), 0, 8, s));
+    if (L)
+        parse_lines_kernel<<<grid_sm(8), 256, 0, s>>>(text.get(), size, ls.get(), L, V, weighted, status.get(), sv.get(),
+                                                      dv.get(), weighted ? wv->get() : nullptr, first.get(), slow.get());
+    HYT_CUDA(cudaGetLastError());
+    unsigned long long h_first = 0, h_slow = 0;
+    HYT_CUDA(cudaMemcpyAsync(&h_first, first.get(), 8, cudaMemcpyDeviceToHost, s));
+    HYT_CUDA(cudaMemcpyAsync(&h_slow, slow.get(), 8, cudaMemcpyDeviceToHost, s));
+    HYT_CUDA(cudaStreamSynchronize(s));
+    // 4. weights in other forms (exponents, many digits): the host parses
+    //    those lines with the exact rules, from the same file
+    int err_kind = 0;
+    uint64_t err_line = ~uint64_t(0);
+    if (h_first != ~0ull) {
+        uint8_t k = 0;
+        HYT_CUDA(cudaMemcpyAsync(&k, status.get() + h_first, 1, cudaMemcpyDeviceToHost, s));
+        HYT_CUDA(cudaStreamSynchronize(s));
+        err_kind = k;
+        err_line = h_first;
+    }
+    if (h_slow) {
+        Scratch<uint8_t> flag(L, s);
+        Scratch<uint64_t> idx(h_slow, s);
+        slow_flags_kernel<<<grid_sm(8), 256, 0, s>>>(status.get(), L, flag.get());
+        thrust::counting_iterator<uint64_t> it(0);
+        size_t tb = 0;
+        HYT_CUDA(cub::DeviceSelect::Flagged(nullptr, tb, it, flag.get(), idx.get(), nsel.get(), static_cast<int64_t>(L), s));
+        Scratch<uint8_t> tmp(tb, s);
+        HYT_CUDA(cub::DeviceSelect::Flagged(tmp.get(), tb, it, flag.get(), idx.get(), nsel.get(), static_cast<int64_t>(L), s));
+        Scratch<uint64_t> bb(h_slow, s), be(h_slow, s);
+        line_bounds_kernel<<<grid_for(h_slow, 256), 256, 0, s>>>(ls.get(), L, size, idx.get(), h_slow, bb.get(), be.get());
+        HYT_CUDA(cudaGetLastError());
+        std::vector<uint64_t> hidx(h_slow), hb(h_slow), he(h_slow);
+        HYT_CUDA(cudaMemcpyAsync(hidx.data(), idx.get(), h_slow * 8, cudaMemcpyDeviceToHost, s));
+        HYT_CUDA(cudaMemcpyAsync(hb.data(), bb.get(), h_slow * 8, cudaMemcpyDeviceToHost, s));
+        HYT_CUDA(cudaMemcpyAsync(he.data(), be.get(), h_slow * 8, cudaMemcpyDeviceToHost, s));
+        HYT_CUDA(cudaStreamSynchronize(s));
+        void *m = ::mmap(nullptr, size, PROT_READ, MAP_PRIVATE, f.fd, 0);
+        if (m == MAP_FAILED) fail(HYT_E_IO, "GraphLoader::load_edge_list: error while reading file: " + p);
+        struct Unmap {
+            void *m;
+            uint64_t n;
+            ~Unmap() { ::munmap(m, n); }
+        } unmap{m, size};
+        const char *ht = static_cast<const char *>(m);
+        std::vector<uint8_t> hst(h_slow);
+        std::vector<uint32_t> hs(h_slow), hd(h_slow), hw(h_slow);
+        const unsigned T = host_threads(h_slow * 64, uint64_t(1) << 20);
+        parallel_for(T, [&](unsigned t) {
+            for (uint64_t k = h_slow * t / T, e = h_slow * (t + 1) / T; k < e; ++k)
+                hst[k] = static_cast<uint8_t>(host_record(ht + hb[k], ht + he[k], V, weighted, hs[k], hd[k], hw[k]));
+        });
+        for (uint64_t k = 0; k < h_slow; ++k) {
+            if (hst[k] >= kRecMalformed && hidx[k] < err_line) {
+                err_line = hidx[k];
+                err_kind = hst[k];
+            }
+        }
+        Scratch<uint8_t> dst_(h_slow, s);
+        Scratch<uint32_t> ds_(h_slow, s), dd_(h_slow, s), dw_(h_slow, s);
+        HYT_CUDA(cudaMemcpyAsync(dst_.get(), hst.data(), h_slow, cudaMemcpyHostToDevice, s));
+        HYT_CUDA(cudaMemcpyAsync(ds_.get(), hs.data(), h_slow * 4, cudaMemcpyHostToDevice, s));
+        HYT_CUDA(cudaMemcpyAsync(dd_.get(), hd.data(), h_slow * 4, cudaMemcpyHostToDevice, s));
+        HYT_CUDA(cudaMemcpyAsync(dw_.get(), hw.data(), h_slow * 4, cudaMemcpyHostToDevice, s));
+        patch_lines_kernel<<<grid_for(h_slow, 256), 256, 0, s>>>(idx.get(), dst_.get(), ds_.get(), dd_.get(), dw_.get(),
+                                                                 h_slow, status.get(), sv.get(), dv.get(),
+                                                                 weighted ? wv->get() : nullptr);
+        HYT_CUDA(cudaGetLastError());
+        HYT_CUDA(cudaStreamSynchronize(s));
+    }
+    if (err_kind) {
+        static const char *what[] = {"", "", "malformed edge", "vertex ID out of range", "missing edge weight",
+                                     "unexpected data"};
+        fail(HYT_E_INVALID, std::string("GraphLoader::load_edge_list: ") + what[err_kind] + " at line " +
+                                std::to_string(err_line + 1));
+    }
+    // 5. the edges in file order
+    Scratch<uint64_t> flag(L + 1, s), pos(L + 1, s);
+    if (L) edge_flags_kernel<<<grid_sm(8), 256, 0, s>>>(status.get(), L, flag.get());
+    HYT_CUDA(cudaMemsetAsync(flag.get() + L, 0, 8, s));
+    {
+        size_t tb = 0;
+        HYT_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, flag.get(), pos.get(), static_cast<int64_t>(L + 1), s));
+        Scratch<uint8_t> tmp(tb, s);
+        HYT_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), tb, flag.get(), pos.get(), static_cast<int64_t>(L + 1), s));
+    }
+    uint64_t E = 0;
+    HYT_CUDA(cudaMemcpyAsync(&E, pos.get() + L, 8, cudaMemcpyDeviceToHost, s));
+    HYT_CUDA(cudaStreamSynchronize(s));
+    Scratch<uint32_t> cs(E, s), cd(E, s);
+    std::unique_ptr<Scratch<uint32_t>> cw;
+    if (weighted) cw = std::make_unique<Scratch<uint32_t>>(E, s);
+    if (L)
+        compact_edges_kernel<<<grid_sm(8), 256, 0, s>>>(status.get(), pos.get(), L, sv.get(), dv.get(),
+                                                        weighted ? wv->get() : nullptr, cs.get(), cd.get(),
+                                                        weighted ? cw->get() : nullptr);
+    HYT_CUDA(cudaGetLastError());
+    const double kms = build_csr(cs.get(), cd.get(), weighted ? cw->get() : nullptr, E, V,
                                  weighted ? HYT_WEIGHTS_F32 : HYT_WEIGHTS_NONE, on_device, out, s);
     whole.stop(s);
     if (stats) {
@@ -703,7 +951,7 @@ void load_edge_list(const char *path, uint64_t V, bool weighted, bool on_device,
         stats->file_bytes = size;
         stats->num_edges = E;
         stats->kernel_bytes = construction_bytes(E, V, weighted);
-        stats->threads = T;
+        stats->threads = threads;
         stats->total_ms = ms_since(t0);
     }
 }
@@ -830,7 +1078,7 @@ void csr_load(const char *path, bool on_device, hyt_csr_buffers *out, hyt_load_s
     const uint64_t size = static_cast<uint64_t>(sb.st_size);
     if (size < sizeof(FileHeader)) fail(HYT_E_INVALID, "not a hytgraph CSR file (shorter than its header): " + p);
     FileHeader h{};
-    read_all(f.fd, &h, sizeof(h), 0, p);
+    read_all(f.fd, &h, sizeof(h), 0, "error while reading file: " + p);
     if (std::memcmp(h.magic, kMagic, 8) != 0) fail(HYT_E_INVALID, "not a hytgraph CSR file (bad magic): " + p);
     if (h.version != 1) fail(HYT_E_INVALID, "unsupported hytgraph CSR file version " + std::to_string(h.version));
     if (header_check(h) != h.header_check) fail(HYT_E_INVALID, "corrupt hytgraph CSR header: " + p);
@@ -861,7 +1109,7 @@ void csr_load(const char *path, bool on_device, hyt_csr_buffers *out, hyt_load_s
         std::atomic<size_t> next{0};
         parallel_for(threads, [&](unsigned) {
             for (size_t k; (k = next.fetch_add(1)) < pieces.size();)
-                read_all(f.fd, pieces[k].dst, pieces[k].bytes, pieces[k].file_at, p);
+                read_all(f.fd, pieces[k].dst, pieces[k].bytes, pieces[k].file_at, "error while reading file: " + p);
         });
         read_ms = ms_since(t0);
         sum = host_checksum(reinterpret_cast<const uint32_t *>(out->row_offsets), L.off_bytes / 4, 0) +
@@ -869,42 +1117,13 @@ void csr_load(const char *path, bool on_device, hyt_csr_buffers *out, hyt_load_s
               (weighted ? host_checksum(out->weights, E, L.w_at / 8) : 0);
         if (sum == h.checksum) bad = host_structure(out->row_offsets, out->column_indices, V, E);
     } else {
-        // a ring of pinned buffers, one reader thread and one stream each
-        int dev = 0;
-        HYT_CUDA(cudaGetDevice(&dev));
-        PinnedRing &r = ring();
-        std::lock_guard<std::mutex> lk(r.mu);
-        r.init();
         std::vector<Piece> pieces;
-        for (const Piece &x : secs)
-            for (uint64_t d = 0; d < x.bytes; d += kRingBytes)
-                pieces.push_back({x.file_at + d, x.dst + d, std::min(kRingBytes, x.bytes - d)});
-        threads = static_cast<unsigned>(std::min<size_t>(kRing, std::max<size_t>(pieces.size(), 1)));
+        for (const Piece &x : secs) {
+            const auto v = cut(x.file_at, x.dst, x.bytes);
+            pieces.insert(pieces.end(), v.begin(), v.end());
+        }
         const auto tr = Clock::now();
-        parallel_for(threads, [&](unsigned t) {
-            HYT_CUDA(cudaSetDevice(dev));
-            cudaStream_t cs = nullptr;
-            cudaEvent_t done = nullptr;
-            HYT_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
-            HYT_CUDA(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
-            struct Release {
-                cudaStream_t s;
-                cudaEvent_t e;
-                ~Release() {
-                    cudaStreamSynchronize(s);
-                    cudaEventDestroy(e);
-                    cudaStreamDestroy(s);
-                }
-            } rel{cs, done};
-            bool pending = false;
-            for (size_t k = t; k < pieces.size(); k += threads) {
-                if (pending) HYT_CUDA(cudaEventSynchronize(done));  // this buffer's last copy
-                read_all(f.fd, r.buf[t], pieces[k].bytes, pieces[k].file_at, p);
-                HYT_CUDA(cudaMemcpyAsync(pieces[k].dst, r.buf[t], pieces[k].bytes, cudaMemcpyHostToDevice, cs));
-                HYT_CUDA(cudaEventRecord(done, cs));
-                pending = true;
-            }
-        });
+        threads = stream_to_device(f.fd, pieces, "error while reading file: " + p);
         read_ms = ms_since(tr);
         StreamHold st;
         cudaStream_t s = st.s;
