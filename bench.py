@@ -48,12 +48,14 @@ def parse_args():
     ap.add_argument("--seed", type=int, default=20241203)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["inhbm", "hybrid", "batch", "serve", "hubsort", "load"], default="inhbm",
+    ap.add_argument("--workload", choices=["inhbm", "hybrid", "batch", "serve", "hubsort", "load", "contrib"],
+                    default="inhbm",
                     help="inhbm: graph resident in HBM (default); hybrid: edges in pinned host memory under a "
                          "device budget (defaults to R-MAT scale 27, edge factor 32, 8 GiB); batch: 64 graphs of "
                          "scales 12-20, 512 SSSP/PPR queries in one CUDA-graph launch; serve: continuous "
                          "batching of a Poisson stream; hubsort: hub sorting + vertex reordering of the graph; load: "
-                         "text edge list -> CSR in HBM (GraphLoader) and the binary CSR file")
+                         "text edge list -> CSR in HBM (GraphLoader) and the binary CSR file; contrib: PageRank "
+                         "contributions + contribution schedule of every vertex + partition priorities")
     ap.add_argument("--hub-fraction", type=float, default=0.08)
     ap.add_argument("--text-scale", type=int, default=22, help="load: R-MAT scale of the text edge list")
     ap.add_argument("--no-effect", action="store_true", help="hubsort: skip the solver comparison")
@@ -1004,6 +1006,111 @@ def reference_load(path, V):
     return time.perf_counter() - t0, "port"
 
 
+def run_contrib_workload(args, rank, world, local, pg):
+    """One step = pagerank_contributions of every vertex (mid-solve ranks),
+    ContributionScheduler::schedule of all V vertices by contribution, and
+    the per-partition priorities (2^20-vertex partitions)."""
+    import torch
+
+    import hytgraph_b200 as hyt
+    from hytgraph_b200 import capi
+
+    peak_gbs, peak_kind = load_peaks()
+    d = hyt.rmat(args.scale, args.edge_factor, args.seed, device=True)
+    V, E = d.num_vertices, d.num_edges
+    off_np = np.empty(V + 1, np.uint64)
+    capi.copy(off_np.ctypes.data, C.cast(d.buffers.row_offsets, C.c_void_p).value, off_np.nbytes)
+    g = hyt.Graph(d)
+    ranks = torch.empty(V, dtype=torch.float32, device="cuda")
+    g.pagerank(max_iterations=3, tolerance=1e-30, out=ranks)
+    contrib = torch.empty(V, dtype=torch.float64, device="cuda")
+    items = torch.arange(V, dtype=torch.int64, device="cuda")
+    ordered = torch.empty(V, dtype=torch.int64, device="cuda")
+    P = max(1, (V + args.partition_vertices - 1) // args.partition_vertices)
+    bounds = torch.tensor([min(i * args.partition_vertices, V) for i in range(P + 1)], dtype=torch.int64,
+                          device="cuda")
+    prio = torch.empty(P, dtype=torch.float64, device="cuda")
+
+    def step(collect):
+        t0 = time.perf_counter()
+        g.pagerank_contributions(ranks, 0.85, out=contrib)
+        t1 = time.perf_counter()
+        _, m = hyt.contribution_schedule(items, contrib, out=ordered)
+        t2 = time.perf_counter()
+        hyt.partition_contributions(contrib, bounds, out=prio)
+        t3 = time.perf_counter()
+        collect.append((1e3 * (t1 - t0), 1e3 * (t2 - t1), 1e3 * (t3 - t2), m))
+
+    warm = []
+    for _ in range(args.warmup):
+        step(warm)
+    clocks = ClockSampler(local)
+    clocks.start()
+    timed = []
+    barrier(pg)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step(timed)
+    barrier(pg)
+    ms = max_over_ranks(pg, 1e3 * (time.perf_counter() - t0))
+    clk = clocks.stop()
+    value = replica_value(V * args.steps, world, ms) / 1e9
+    c_ms = sum(x[0] for x in timed) / args.steps
+    s_ms = sum(x[1] for x in timed) / args.steps
+    p_ms = sum(x[2] for x in timed) / args.steps
+    kb = 12 * E + 20 * V  # source id, rank and degree gathers per in-edge; offsets, rank, output per vertex
+    roof = {"kernel": "pagerank_contrib_kernel (+ dangling partials)", "bound": "hbm",
+            "achieved": kb / (c_ms / 1e3) / 1e9, "peak": peak_gbs, "unit": "GB/s",
+            "frac": kb / (c_ms / 1e3) / 1e9 / peak_gbs, "traffic": None, "peak_kind": peak_kind,
+            "algorithmic_bytes_per_launch": kb, "avg_launch_ms": c_ms,
+            "note": "launch time from the host clock around the synchronous call"}
+    # e2e: host arrays in and out through the C ABI
+    ranks_h = ranks.cpu().numpy()
+    t0 = time.perf_counter()
+    ch = g.pagerank_contributions(ranks_h, 0.85)
+    oh, _ = hyt.contribution_schedule(np.arange(V, dtype=np.uint64), ch)
+    e2e_ms = 1e3 * (time.perf_counter() - t0)
+    g.close()
+    d.free()
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle.bindings import Reference
+
+        host = hyt.rmat(args.scale, args.edge_factor, args.seed) if args.scale <= 20 else None
+        if host is None:
+            dd = hyt.rmat(args.scale, args.edge_factor, args.seed, device=True)
+            off_t, cols_t, _ = host_graph_from_device(dd)
+            dd.free()
+            hoff, hcols = off_t.numpy().view(np.uint64), cols_t.numpy().view(np.uint32)
+        else:
+            hoff, hcols = host.row_offsets, host.column_indices
+        if Reference.available():
+            ref = Reference()
+            tt = time.perf_counter()
+            rc = ref.pagerank_contributions(hoff, hcols, ranks_h, 0.85)
+            ref.contribution_schedule(np.arange(V, dtype=np.uint64), rc)
+            tc = time.perf_counter() - tt
+            cpu = {"value": V / tc / 1e9, "unit": "Gvertices/s", "cores": 1, "kind": "reference",
+                   "sample": f"one pagerank_contributions + ContributionScheduler::schedule of all V on the full "
+                             f"graph, {tc:.1f} s"}
+    if rank == 0:
+        line = {"metric": "contribution pass + schedule throughput", "value": value, "unit": "Gvertices/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64 contributions",
+                "data": "synthetic",
+                "config": {"workload": f"pagerank_contributions (ranks after 3 iterations) + schedule of every "
+                                       f"vertex + priorities of {P} partitions, R-MAT scale {args.scale} edge "
+                                       f"factor {args.edge_factor}",
+                           "vertices": V, "edges": E, "partitions": P, "seed": args.seed,
+                           "parallelism": f"replicas x{args.gpus}"},
+                "e2e": {"value": V / (e2e_ms / 1e3) / 1e9, "unit": "Gvertices/s", "h2d_bytes_per_step": V * 12,
+                        "d2h_bytes_per_step": V * 16, "ms_per_step": e2e_ms},
+                "phases_ms": {"pagerank_contributions": c_ms, "schedule": s_ms, "partition_priorities": p_ms},
+                "schedule_metrics": timed[0][3], "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
+                "gpu_launches": 10 * args.steps}
+        print(json.dumps(line), flush=True)
+
+
 def workload_config(args, V, E):
     return {"workload": f"in-HBM R-MAT scale {args.scale} edge factor {args.edge_factor}: PageRank to L1<=1e-6 "
                         f"+ SSSP from {args.sources} seeded sources",
@@ -1036,6 +1143,11 @@ def main():
         return
     if args.workload == "batch":
         run_batch_workload(args, rank, world, pg)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
+    if args.workload == "contrib":
+        run_contrib_workload(args, rank, world, local, pg)
         if pg is not None:
             pg.destroy_process_group()
         return

@@ -10,10 +10,12 @@ there is no CPU fallback.
 """
 from . import capi
 from .capi import HytError, device_count
-from .graph import (CSR, Batch, DeviceCSR, Graph, HybridGraph, PinnedBuffer, Server, csr_from_edges, hub_sort,
-                    load_csr, load_edge_list, pick_sources, reorder, rmat, save_csr)
+from .graph import (CSR, Batch, DeviceCSR, Graph, HybridGraph, PinnedBuffer, Server, contribution_schedule,
+                    csr_from_edges, hub_sort, load_csr, load_edge_list, partition_contributions, pick_sources, reorder,
+                    rmat, save_csr, sssp_contributions)
 
 __all__ = [
     "capi", "HytError", "device_count", "CSR", "Batch", "DeviceCSR", "Graph", "HybridGraph", "PinnedBuffer", "Server",
-    "csr_from_edges", "hub_sort", "load_csr", "load_edge_list", "pick_sources", "reorder", "rmat", "save_csr",
+    "contribution_schedule", "csr_from_edges", "hub_sort", "load_csr", "load_edge_list", "partition_contributions",
+    "pick_sources", "reorder", "rmat", "save_csr", "sssp_contributions",
 ]

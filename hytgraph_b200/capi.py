@@ -175,6 +175,21 @@ class hyt_load_stats(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_ if name != "pad"}
 
 
+class hyt_contribution_metrics(C.Structure):
+    _fields_ = [
+        ("input_item_count", C.c_uint64),
+        ("scheduled_item_count", C.c_uint64),
+        ("reordered_item_count", C.c_uint64),
+        ("zero_contribution_count", C.c_uint64),
+        ("scheduling_overhead", C.c_double),
+        ("stale_work_count", C.c_uint64),
+        ("redundant_work_count", C.c_uint64),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 class hyt_csc(C.Structure):
     _fields_ = [
         ("num_vertices", C.c_uint64),
@@ -398,6 +413,11 @@ _SIGNATURES = [
                                      C.POINTER(hyt_csr_buffers), C.POINTER(hyt_load_stats)]),
     ("hyt_csr_save", C.c_int, [C.c_char_p, C.POINTER(hyt_csr)]),
     ("hyt_csr_load", C.c_int, [C.c_char_p, C.c_int, C.POINTER(hyt_csr_buffers), C.POINTER(hyt_load_stats)]),
+    ("hyt_pagerank_contributions", C.c_int, [C.c_void_p, C.c_void_p, C.c_float, C.c_void_p]),
+    ("hyt_sssp_contributions", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_float, C.c_void_p]),
+    ("hyt_contribution_schedule", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_int, C.c_double, C.c_void_p,
+                                            C.POINTER(hyt_contribution_metrics)]),
+    ("hyt_partition_contributions", C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_void_p]),
     ("hyt_csr_reorder", C.c_int, [C.POINTER(hyt_csr), C.c_void_p, C.c_int, C.POINTER(hyt_csr_buffers),
                                   C.POINTER(hyt_reorder_stats)]),
     ("hyt_rmat_generate", C.c_int, [C.POINTER(hyt_rmat_params), C.c_int, C.POINTER(hyt_csr_buffers)]),

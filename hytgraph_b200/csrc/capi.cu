@@ -319,6 +319,40 @@ int hyt_csr_load(const char *path, int on_device, hyt_csr_buffers *out, hyt_load
     });
 }
 
+int hyt_pagerank_contributions(hyt_graph *graph, const float *current_ranks, float damping,
+                               double *contributions) {
+    return guarded([&] {
+        if (!graph) fail(HYT_E_INVALID, "graph is NULL");
+        pagerank_contributions(graph->impl, current_ranks, damping, contributions, nullptr);
+    });
+}
+
+int hyt_sssp_contributions(const float *current_distances, const float *candidate_distances, uint64_t n,
+                           float tolerance, double *contributions) {
+    return guarded([&] {
+        require_device();
+        sssp_contributions(current_distances, candidate_distances, n, tolerance, contributions);
+    });
+}
+
+int hyt_contribution_schedule(const uint64_t *item_indices, const double *contributions, uint64_t n,
+                              int deterministic_tie_break, double zero_contribution_epsilon,
+                              uint64_t *ordered_items, hyt_contribution_metrics *metrics) {
+    return guarded([&] {
+        require_device();
+        contribution_schedule(item_indices, contributions, n, deterministic_tie_break != 0, zero_contribution_epsilon,
+                              ordered_items, metrics);
+    });
+}
+
+int hyt_partition_contributions(const double *vertex_contributions, uint64_t num_vertices, const uint64_t *bounds,
+                                uint64_t num_partitions, double *out) {
+    return guarded([&] {
+        require_device();
+        partition_contributions(vertex_contributions, num_vertices, bounds, num_partitions, out);
+    });
+}
+
 int hyt_pick_sources(const uint64_t *row_offsets, uint64_t num_vertices, uint64_t seed, uint32_t count,
                      uint32_t *out) {
     return guarded([&] { pick_sources(row_offsets, num_vertices, seed, count, out); });

@@ -149,4 +149,38 @@ SSSPResultU32 sssp_gpu_u32(const graph::CSRGraph &graph, const SSSPOptions &opti
     return r;
 }
 
+std::vector<PageRankContribution> pagerank_contributions_gpu(const graph::CSRGraph &graph,
+                                                             const std::vector<float> &current_ranks,
+                                                             const PageRankOptions &options) {
+    if (graph.num_vertices() == 0U) throw std::invalid_argument("PageRank requires at least one vertex");
+    if (!(options.damping_factor >= 0.0F && options.damping_factor < 1.0F))
+        throw std::invalid_argument("PageRank damping_factor must be in [0, 1)");
+    if (current_ranks.size() != graph.num_vertices())
+        throw std::invalid_argument("PageRank current_ranks size must match graph vertex count");
+    require_device("pagerank_contributions_gpu");
+    DeviceGraph dg(graph, nullptr, HYT_WEIGHTS_NONE, HYT_GRAPH_PULL, "pagerank_contributions_gpu");
+    std::vector<double> c(current_ranks.size());
+    check(hyt_pagerank_contributions(dg.g, current_ranks.data(), options.damping_factor, c.data()),
+          "pagerank_contributions_gpu");
+    std::vector<PageRankContribution> out(c.size());
+    for (std::size_t v = 0; v < c.size(); ++v) out[v] = {v, c[v]};
+    return out;
+}
+
+std::vector<SSSPContribution> sssp_contributions_gpu(const std::vector<float> &current_distances,
+                                                     const std::vector<float> &candidate_distances, float tolerance) {
+    if (!(tolerance >= 0.0F) || !std::isfinite(tolerance))
+        throw std::invalid_argument("SSSP contribution tolerance must be finite and non-negative");
+    if (current_distances.size() != candidate_distances.size())
+        throw std::invalid_argument("SSSP contribution distance vectors must have equal size");
+    std::vector<SSSPContribution> out(current_distances.size());
+    if (out.empty()) return out;
+    require_device("sssp_contributions_gpu");
+    std::vector<double> c(out.size());
+    check(hyt_sssp_contributions(current_distances.data(), candidate_distances.data(), c.size(), tolerance, c.data()),
+          "sssp_contributions_gpu");
+    for (std::size_t v = 0; v < c.size(); ++v) out[v] = {v, c[v]};
+    return out;
+}
+
 }  // namespace hytgraph::algorithms

@@ -23,6 +23,11 @@ void csr_from_edges(const uint32_t *src, const uint32_t *dst, const void *weight
 void load_edge_list(const char *path, uint64_t V, bool weighted, bool on_device, hyt_csr_buffers *out,
                     hyt_load_stats *stats);
 void csr_save(const char *path, const hyt_csr &csr);
+void pagerank_contributions(GraphImpl &g, const float *ranks, float damping, double *out, double *device_ms);
+void sssp_contributions(const float *cur, const float *cand, uint64_t n, float tol, double *out);
+void contribution_schedule(const uint64_t *item, const double *contribution, uint64_t n, bool deterministic,
+                           double eps, uint64_t *ordered, hyt_contribution_metrics *m);
+void partition_contributions(const double *contrib, uint64_t V, const uint64_t *bounds, uint64_t parts, double *out);
 void csr_load(const char *path, bool on_device, hyt_csr_buffers *out, hyt_load_stats *stats);
 
 }  // namespace hyt

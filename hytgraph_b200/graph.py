@@ -207,6 +207,14 @@ class Graph:
         check(lib.hyt_ppr(self.handle, C.byref(p), _ptr(res) if res is not False else None, C.byref(st)))
         return res, st.as_dict()
 
+    def pagerank_contributions(self, current_ranks, damping: float = 0.85, out=None):
+        """|next - current| of one synchronous PageRank pull step per vertex
+        (hyt_pagerank_contributions); float64 [V], numpy or a CUDA tensor."""
+        cur = np.ascontiguousarray(current_ranks, np.float32) if isinstance(current_ranks, np.ndarray) else current_ranks
+        res = np.empty(self.num_vertices, np.float64) if out is None else out
+        check(lib.hyt_pagerank_contributions(self.handle, _ptr(cur), damping, _ptr(res)))
+        return res
+
     def sssp(self, source: int, out=None, flags: int = 0, max_rounds: int = 0, delta: int = 0, stream: int = 0):
         p = capi.hyt_sssp_params(source, delta, max_rounds, flags, stream or None)
         st = capi.hyt_run_stats()
@@ -621,3 +629,46 @@ def load_csr(path, device: bool = False, stats: Optional[dict] = None):
     if stats is not None:
         stats.update(st.as_dict())
     return _wrap(b, device)
+
+
+def sssp_contributions(current, candidate, tolerance: float = 0.0, out=None):
+    """sssp_contributions on the GPU (hyt_sssp_contributions): float64 [n]."""
+    c = np.ascontiguousarray(current, np.float32) if isinstance(current, np.ndarray) else current
+    d = np.ascontiguousarray(candidate, np.float32) if isinstance(candidate, np.ndarray) else candidate
+    n = int(c.shape[0])
+    if tuple(d.shape) != (n,):
+        raise HytError(capi.HYT_E_INVALID, "SSSP contribution distance vectors must have equal size")
+    res = np.empty(n, np.float64) if out is None else out
+    check(lib.hyt_sssp_contributions(_ptr(c) if n else None, _ptr(d) if n else None, n, tolerance,
+                                     _ptr(res) if n else None))
+    return res
+
+
+def contribution_schedule(items, contributions, deterministic_tie_break: bool = True,
+                          zero_contribution_epsilon: float = 0.0, out=None):
+    """ContributionScheduler::schedule on the GPU (hyt_contribution_schedule):
+    returns (ordered item indices uint64 [n], metrics dict)."""
+    it = np.ascontiguousarray(items, np.uint64) if not hasattr(items, "data_ptr") else items
+    c = np.ascontiguousarray(contributions, np.float64) if not hasattr(contributions, "data_ptr") else contributions
+    n = int(it.shape[0])
+    if tuple(c.shape) != (n,):
+        raise HytError(capi.HYT_E_INVALID, "contribution priority inputs must have equal size")
+    res = np.empty(n, np.uint64) if out is None else out
+    m = capi.hyt_contribution_metrics()
+    check(lib.hyt_contribution_schedule(_ptr(it) if n else None, _ptr(c) if n else None, n,
+                                        1 if deterministic_tie_break else 0, zero_contribution_epsilon,
+                                        _ptr(res) if n else None, C.byref(m)))
+    return res, m.as_dict()
+
+
+def partition_contributions(vertex_contributions, bounds, out=None):
+    """Per-partition sums of vertex contributions over [bounds[i], bounds[i+1])
+    (hyt_partition_contributions): the priorities of the transfer queue."""
+    c = np.ascontiguousarray(vertex_contributions, np.float64) if isinstance(vertex_contributions, np.ndarray) \
+        else vertex_contributions
+    b = np.ascontiguousarray(bounds, np.uint64) if not hasattr(bounds, "data_ptr") else bounds
+    parts = int(b.shape[0]) - 1
+    res = np.empty(max(parts, 0), np.float64) if out is None else out
+    check(lib.hyt_partition_contributions(_ptr(c), int(c.shape[0]), _ptr(b), max(parts, 0),
+                                          _ptr(res) if parts > 0 else None))
+    return res

@@ -44,5 +44,10 @@ PageRankResult pagerank_cpu(const graph::CSRGraph &graph, const PageRankOptions 
 // input (same messages as the CPU solver) and std::runtime_error for CUDA
 // failures or when no device is present.
 PageRankResult pagerank_gpu(const graph::CSRGraph &graph, const PageRankOptions &options = {});
+// pagerank_contributions on the GPU (hyt_pagerank_contributions; sums in
+// FP64, so values agree with the FP32 reference to its rounding).
+[[nodiscard]] std::vector<PageRankContribution> pagerank_contributions_gpu(const graph::CSRGraph &graph,
+                                                                           const std::vector<float> &current_ranks,
+                                                                           const PageRankOptions &options = {});
 
 }  // namespace hytgraph::algorithms

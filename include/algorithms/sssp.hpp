@@ -28,6 +28,10 @@ struct SSSPContribution {
 [[nodiscard]] std::vector<SSSPContribution> sssp_contributions(const std::vector<float> &current_distances,
                                                                const std::vector<float> &candidate_distances,
                                                                float tolerance = 0.0F);
+// sssp_contributions on the GPU (hyt_sssp_contributions), bit for bit.
+[[nodiscard]] std::vector<SSSPContribution> sssp_contributions_gpu(const std::vector<float> &current_distances,
+                                                                   const std::vector<float> &candidate_distances,
+                                                                   float tolerance = 0.0F);
 
 struct SSSPResult {
     std::vector<float> distances;  // +inf for unreachable vertices

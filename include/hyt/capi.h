@@ -559,6 +559,51 @@ int hyt_csr_save(const char *path, const hyt_csr *csr);
  * threads. */
 int hyt_csr_load(const char *path, int on_device, hyt_csr_buffers *out, hyt_load_stats *stats);
 
+/* ------------------------------------------------------------------ */
+/* Contribution-driven scheduling                                       */
+/* ------------------------------------------------------------------ */
+
+/* scheduling::ContributionSchedulingMetrics. */
+typedef struct hyt_contribution_metrics {
+    uint64_t input_item_count;
+    uint64_t scheduled_item_count;
+    uint64_t reordered_item_count;    /* positions whose item changed */
+    uint64_t zero_contribution_count; /* |contribution| <= epsilon */
+    double scheduling_overhead;       /* log2(n): the reference's model */
+    uint64_t stale_work_count;        /* 0 here (observations are host-side) */
+    uint64_t redundant_work_count;    /* repeated item indices */
+} hyt_contribution_metrics;
+
+/* algorithms::pagerank_contributions (src/algorithms/pagerank.cpp:165-241)
+ * on an in-HBM graph (HYT_GRAPH_PULL): contributions[v] = |next(v) -
+ * current(v)| of one synchronous pull step, sums in FP64 (the reference
+ * sums in FP32; the two agree to its rounding).  current_ranks [V] and
+ * contributions [V]: host or device. */
+int hyt_pagerank_contributions(hyt_graph *graph, const float *current_ranks, float damping,
+                               double *contributions);
+
+/* algorithms::sssp_contributions (src/algorithms/sssp.cpp:236-290) on the
+ * GPU, bit for bit: current - candidate when both are finite and the
+ * improvement exceeds the tolerance, 1 when an unreachable vertex becomes
+ * reachable, else 0.  Arrays of n: host or device. */
+int hyt_sssp_contributions(const float *current_distances, const float *candidate_distances, uint64_t n,
+                           float tolerance, double *contributions);
+
+/* scheduling::ContributionScheduler::schedule
+ * (src/scheduling/contribution_scheduler.cpp:23-121) on the GPU: items by
+ * descending contribution; ties by lower item index when
+ * deterministic_tie_break, else in input order; a non-finite contribution
+ * fails with HYT_E_INVALID.  ordered_items [n]: host or device. */
+int hyt_contribution_schedule(const uint64_t *item_indices, const double *contributions, uint64_t n,
+                              int deterministic_tie_break, double zero_contribution_epsilon,
+                              uint64_t *ordered_items, hyt_contribution_metrics *metrics);
+
+/* Per-partition priorities for the transfer queue: out[i] = sum of
+ * vertex_contributions over [bounds[i], bounds[i + 1]).  Arrays: host or
+ * device. */
+int hyt_partition_contributions(const double *vertex_contributions, uint64_t num_vertices, const uint64_t *bounds,
+                                uint64_t num_partitions, double *out);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

@@ -179,6 +179,41 @@ class Oracle:
             raise ValueError(f"edge {bad - 1} has a vertex id >= {V}")
         return o, c[:E], (wo[:E].view(w.dtype) if w is not None else None)
 
+    def pagerank_contributions(self, off, cols, cur, damping=0.85, fp64=False):
+        V, E = off.shape[0] - 1, cols.shape[0]
+        out = np.empty(V, np.float64)
+        rc = self.lib.oracle_pagerank_contributions(C.c_uint64(V), C.c_uint64(E), _p(off), _p(cols),
+                                                    _p(np.ascontiguousarray(cur, np.float32)), C.c_float(damping),
+                                                    C.c_int(1 if fp64 else 0), _p(out))
+        if rc:
+            raise ValueError(f"oracle_pagerank_contributions rc={rc}")
+        return out
+
+    def sssp_contributions(self, cur, cand, tol=0.0):
+        n = cur.shape[0]
+        out = np.empty(n, np.float64)
+        self.lib.oracle_sssp_contributions(C.c_uint64(n), _p(np.ascontiguousarray(cur, np.float32)),
+                                           _p(np.ascontiguousarray(cand, np.float32)), C.c_float(tol), _p(out))
+        return out
+
+    def contribution_schedule(self, items, contrib, deterministic=True, eps=0.0):
+        n = len(items)
+        it = np.ascontiguousarray(items, np.uint64)
+        c = np.ascontiguousarray(contrib, np.float64)
+        out = np.empty(max(n, 1), np.uint64)
+        m = np.zeros(7, np.uint64)
+        rc = self.lib.oracle_contribution_schedule(C.c_uint64(n), _p(it), _p(c), C.c_int(1 if deterministic else 0),
+                                                   C.c_double(eps), _p(out), _p(m))
+        if rc:
+            raise ValueError("contribution priority must be finite")
+        return out[:n], _metrics(m)
+
+
+def _metrics(m):
+    return {"input_item_count": int(m[0]), "scheduled_item_count": int(m[1]), "reordered_item_count": int(m[2]),
+            "zero_contribution_count": int(m[3]), "scheduling_overhead": float(m[4:5].view(np.float64)[0]),
+            "stale_work_count": int(m[5]), "redundant_work_count": int(m[6])}
+
 
 class Reference:
     """The reference's own CPU implementation (oracle/_ref/libhytref.so)."""
@@ -276,3 +311,30 @@ class Reference:
         w = np.empty(max(E.value, 1), np.float32) if weighted else None
         self.lib.ref_loaded_copy(_p(o), _p(c), _p(w) if w is not None else None)
         return o, c[:E.value], (w[:E.value] if w is not None else None)
+
+    def pagerank_contributions(self, off, cols, cur, damping=0.85):
+        V, E = off.shape[0] - 1, cols.shape[0]
+        out = np.empty(V, np.float64)
+        self._check(self.lib.ref_pagerank_contributions(C.c_uint64(V), C.c_uint64(E), _p(off), _p(cols),
+                                                        _p(np.ascontiguousarray(cur, np.float32)), C.c_float(damping),
+                                                        _p(out)), "ref_pagerank_contributions")
+        return out
+
+    def sssp_contributions(self, cur, cand, tol=0.0):
+        n = cur.shape[0]
+        out = np.empty(n, np.float64)
+        self._check(self.lib.ref_sssp_contributions(C.c_uint64(n), _p(np.ascontiguousarray(cur, np.float32)),
+                                                    _p(np.ascontiguousarray(cand, np.float32)), C.c_float(tol),
+                                                    _p(out)), "ref_sssp_contributions")
+        return out
+
+    def contribution_schedule(self, items, contrib, deterministic=True, eps=0.0):
+        n = len(items)
+        it = np.ascontiguousarray(items, np.uint64)
+        c = np.ascontiguousarray(contrib, np.float64)
+        out = np.empty(max(n, 1), np.uint64)
+        m = np.zeros(7, np.uint64)
+        self._check(self.lib.ref_contribution_schedule(C.c_uint64(n), _p(it), _p(c),
+                                                       C.c_int(1 if deterministic else 0), C.c_double(eps), _p(out),
+                                                       _p(m)), "ref_contribution_schedule")
+        return out[:n], _metrics(m)

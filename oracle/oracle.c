@@ -652,3 +652,109 @@ uint64_t oracle_csr_from_edges(uint64_t V, uint64_t E, const uint32_t *src, cons
     free(cur);
     return 0;
 }
+
+/* ---------------------------------------------------------------------
+ * Contribution-driven scheduling, restating
+ * src/algorithms/pagerank.cpp:165-241 (pagerank_contributions, FP32 in the
+ * reference's operation order), src/algorithms/sssp.cpp:236-290
+ * (sssp_contributions) and src/scheduling/contribution_scheduler.cpp:23-121
+ * (ContributionScheduler::schedule and its metrics).
+ * ------------------------------------------------------------------- */
+int oracle_pagerank_contributions(uint64_t V, uint64_t E, const uint64_t *off, const uint32_t *cols,
+                                  const float *cur, float damping, int fp64, double *out) {
+    uint64_t *in_off = NULL;
+    uint32_t *in_src = NULL;
+    const int rc = build_incoming(V, E, off, cols, NULL, &in_off, &in_src, NULL);
+    if (rc) return rc;
+    if (fp64) {
+        double dm = 0.0;
+        for (uint64_t u = 0; u < V; ++u)
+            if (off[u + 1] == off[u]) dm += cur[u];
+        const double share = (1.0 - damping) / (double)V + (double)damping * dm / (double)V;
+        for (uint64_t v = 0; v < V; ++v) {
+            double s = 0.0;
+            for (uint64_t e = in_off[v]; e < in_off[v + 1]; ++e) {
+                const uint32_t u = in_src[e];
+                s += (double)cur[u] / (double)(off[u + 1] - off[u]);
+            }
+            out[v] = fabs(share + (double)damping * s - (double)cur[v]);
+        }
+    } else {
+        const float base = (1.0f - damping) / (float)V;
+        float dm = 0.0f;
+        for (uint64_t u = 0; u < V; ++u)
+            if (off[u + 1] == off[u]) dm += cur[u];
+        const float share = damping * dm / (float)V;
+        for (uint64_t v = 0; v < V; ++v) {
+            float s = 0.0f;
+            for (uint64_t e = in_off[v]; e < in_off[v + 1]; ++e) {
+                const uint32_t u = in_src[e];
+                const uint64_t deg = off[u + 1] - off[u];
+                if (deg) s += cur[u] / (float)deg;
+            }
+            const float next = base + share + damping * s;
+            out[v] = (double)fabsf(next - cur[v]);
+        }
+    }
+    free(in_off); free(in_src);
+    return 0;
+}
+
+void oracle_sssp_contributions(uint64_t n, const float *cur, const float *cand, float tol, double *out) {
+    for (uint64_t v = 0; v < n; ++v) {
+        const float c = cur[v], d = cand[v];
+        double r = 0.0;
+        if (isfinite(c) && isfinite(d)) {
+            const float imp = c - d;
+            if (imp > tol) r = (double)imp;
+        } else if (!isfinite(c) && isfinite(d)) {
+            r = 1.0;
+        }
+        out[v] = r;
+    }
+}
+
+static const uint64_t *g_sched_item;
+static const double *g_sched_c;
+static int g_sched_det;
+static int sched_cmp(const void *pa, const void *pb) {
+    const uint64_t a = *(const uint64_t *)pa, b = *(const uint64_t *)pb;
+    const double ca = g_sched_c[a], cb = g_sched_c[b];
+    if (ca != cb) return ca > cb ? -1 : 1;
+    if (g_sched_det && g_sched_item[a] != g_sched_item[b]) return g_sched_item[a] < g_sched_item[b] ? -1 : 1;
+    return a < b ? -1 : (a > b); /* stable: input position */
+}
+static int u64_cmp(const void *pa, const void *pb) {
+    const uint64_t a = *(const uint64_t *)pa, b = *(const uint64_t *)pb;
+    return a < b ? -1 : (a > b);
+}
+
+/* metrics[0..6] = input, scheduled, reordered, zero, overhead (as double
+ * bits), stale (0), redundant.  Returns ORACLE_E_INVALID on a non-finite
+ * contribution. */
+int oracle_contribution_schedule(uint64_t n, const uint64_t *item, const double *c, int det, double eps,
+                                 uint64_t *ordered, uint64_t *metrics) {
+    for (uint64_t i = 0; i < n; ++i)
+        if (!isfinite(c[i])) return ORACLE_E_INVALID;
+    uint64_t *order = (uint64_t *)malloc((n ? n : 1) * 8), *sorted = (uint64_t *)malloc((n ? n : 1) * 8);
+    uint64_t zero = 0, moved = 0, dup = 0;
+    for (uint64_t i = 0; i < n; ++i) {
+        order[i] = i;
+        sorted[i] = item[i];
+        if (fabs(c[i]) <= eps) ++zero;
+    }
+    g_sched_item = item; g_sched_c = c; g_sched_det = det;
+    qsort(order, n, 8, sched_cmp);
+    qsort(sorted, n, 8, u64_cmp);
+    for (uint64_t i = 1; i < n; ++i) dup += sorted[i] == sorted[i - 1];
+    for (uint64_t p = 0; p < n; ++p) {
+        ordered[p] = item[order[p]];
+        moved += order[p] != p;
+    }
+    const double overhead = n ? log2((double)n) : 0.0;
+    metrics[0] = n; metrics[1] = n; metrics[2] = moved; metrics[3] = zero;
+    memcpy(&metrics[4], &overhead, 8);
+    metrics[5] = 0; metrics[6] = dup;
+    free(order); free(sorted);
+    return 0;
+}

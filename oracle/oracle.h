@@ -50,6 +50,11 @@ void oracle_loaded_copy(uint64_t *off, uint32_t *cols, float *w);
 void oracle_loaded_free(void);
 uint64_t oracle_csr_from_edges(uint64_t V, uint64_t E, const uint32_t *src, const uint32_t *dst, const uint32_t *w,
                                uint64_t *off, uint32_t *cols, uint32_t *w_out);
+int oracle_pagerank_contributions(uint64_t V, uint64_t E, const uint64_t *off, const uint32_t *cols,
+                                  const float *cur, float damping, int fp64, double *out);
+void oracle_sssp_contributions(uint64_t n, const float *cur, const float *cand, float tol, double *out);
+int oracle_contribution_schedule(uint64_t n, const uint64_t *item, const double *c, int det, double eps,
+                                 uint64_t *ordered, uint64_t *metrics);
 int oracle_reorder(uint64_t V, uint64_t E, const uint64_t *off, const uint32_t *cols, const uint32_t *w,
                    const uint32_t *order, uint64_t *off_out, uint32_t *cols_out, uint32_t *w_out);
 

@@ -13,6 +13,7 @@
 #include "graph/csr_graph.hpp"
 #include "graph/partition.hpp"
 #include "graph/graph_loader.hpp"
+#include "scheduling/contribution_scheduler.hpp"
 #include "scheduling/hub_sort.hpp"
 #include "scheduling/task_combiner.hpp"
 #include "transfer/compaction_engine.hpp"
@@ -179,6 +180,48 @@ void ref_loaded_copy(uint64_t *off, uint32_t *cols, float *w) {
     for (size_t i = 0; i < c.size(); ++i) cols[i] = c[i];
     if (w)
         for (size_t i = 0; i < x.size(); ++i) w[i] = x[i];
+}
+
+// pagerank_contributions: out[V] (vertex order as returned).
+int ref_pagerank_contributions(uint64_t V, uint64_t E, const uint64_t *off, const uint32_t *cols, const float *cur,
+                               float damping, double *out) {
+    REF_GUARD({
+        const auto g = make_graph(V, E, off, cols, nullptr);
+        hytgraph::algorithms::PageRankOptions o;
+        o.damping_factor = damping;
+        const auto r = hytgraph::algorithms::pagerank_contributions(g, std::vector<float>(cur, cur + V), o);
+        for (const auto &c : r) out[c.vertex] = c.contribution;
+    })
+}
+
+int ref_sssp_contributions(uint64_t n, const float *cur, const float *cand, float tol, double *out) {
+    REF_GUARD({
+        const auto r = hytgraph::algorithms::sssp_contributions(std::vector<float>(cur, cur + n),
+                                                                std::vector<float>(cand, cand + n), tol);
+        for (const auto &c : r) out[c.vertex] = c.contribution;
+    })
+}
+
+// ContributionScheduler::schedule: ordered[n]; metrics[7] as in the oracle.
+int ref_contribution_schedule(uint64_t n, const uint64_t *item, const double *c, int det, double eps, uint64_t *ordered,
+                              uint64_t *metrics) {
+    REF_GUARD({
+        hytgraph::scheduling::ContributionSchedulerOptions o;
+        o.deterministic_tie_break = det != 0;
+        o.zero_contribution_epsilon = eps;
+        std::vector<hytgraph::scheduling::ContributionPriority> p(n);
+        for (uint64_t i = 0; i < n; ++i) p[i] = {static_cast<std::size_t>(item[i]), c[i]};
+        const auto plan = hytgraph::scheduling::ContributionScheduler(o).schedule(p);
+        for (uint64_t i = 0; i < n; ++i) ordered[i] = plan.ordered_item_indices[i];
+        const auto &m = plan.metrics;
+        metrics[0] = m.input_item_count;
+        metrics[1] = m.scheduled_item_count;
+        metrics[2] = m.reordered_item_count;
+        metrics[3] = m.zero_contribution_count;
+        std::memcpy(&metrics[4], &m.scheduling_overhead, 8);
+        metrics[5] = m.stale_work_count;
+        metrics[6] = m.redundant_work_count;
+    })
 }
 
 // HubSorter::sort: vertex_order[V], scores[V], hub_count.

@@ -17,6 +17,7 @@
 #include "hyt/capi.h"
 #include "runtime/config.hpp"
 #include "runtime/result.hpp"
+#include "scheduling/contribution_scheduler.hpp"
 #include "scheduling/hub_sort.hpp"
 #include "scheduling/task_combiner.hpp"
 #include "transfer/compaction_engine.hpp"
@@ -373,6 +374,34 @@ void test_gpu() {
               back.edge_weights() == lw.edge_weights(),
           "binary CSR round trip");
     for (const auto &f : {f1, f2, f3, f4}) std::remove(f.c_str());
+
+    // ContributionScheduler (GPU): reference tests/unit_tests.cpp:2751-2880.
+    using scheduling::ContributionPriority;
+    using scheduling::ContributionScheduler;
+    const auto cp = ContributionScheduler().schedule({{0U, 0.10}, {1U, 0.90}, {2U, 0.30}, {3U, 0.70}});
+    check(cp.ordered_item_indices == std::vector<std::size_t>({1U, 3U, 2U, 0U}) &&
+              std::fabs(cp.metrics.scheduling_overhead - 2.0) < 1e-12,
+          "contribution order");
+    check(ContributionScheduler().schedule({{3U, 0.5}, {1U, 0.5}, {2U, 0.9}, {0U, 0.5}}).ordered_item_indices ==
+              std::vector<std::size_t>({2U, 0U, 1U, 3U}),
+          "contribution ties");
+    scheduling::ContributionSchedulerOptions zo;
+    zo.zero_contribution_epsilon = 1e-6;
+    check(ContributionScheduler(zo).schedule({{0U, 0.0}, {1U, 1e-8}, {2U, 0.25}, {3U, -1e-8}})
+                  .metrics.zero_contribution_count == 3U,
+          "zero contributions");
+    throws<std::invalid_argument>(
+        [] { (void)ContributionScheduler().schedule({{0U, std::numeric_limits<double>::infinity()}}); },
+        "non-finite contribution");
+    const auto pc = pagerank_contributions_gpu(CSRGraph(3, {0, 2, 3, 3}, {1, 2, 2}), {1.F, 0.F, 0.F});
+    check(std::fabs(pc[0].contribution - 0.95) < 1e-5 && std::fabs(pc[1].contribution - 0.475) < 1e-5 &&
+              std::fabs(pc[2].contribution - 0.475) < 1e-5,
+          "pagerank contributions");
+    const auto sc2 = sssp_contributions_gpu({0.F, 5.F, std::numeric_limits<float>::infinity(), 10.F},
+                                            {0.F, 3.F, 7.F, 12.F});
+    check(sc2[0].contribution == 0.0 && sc2[1].contribution == 2.0 && sc2[2].contribution == 1.0 &&
+              sc2[3].contribution == 0.0,
+          "sssp contributions");
 
     HubSortOptions bad_fraction;
     bad_fraction.hub_fraction = 1.5;

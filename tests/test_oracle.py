@@ -330,3 +330,49 @@ def test_csr_from_edges_oracle(oracle):
     assert np.array_equal(off, np.concatenate([[0], np.cumsum(np.bincount(src, minlength=V))]).astype(np.uint64))
     with pytest.raises(ValueError):
         oracle.csr_from_edges(V, np.array([1, V], np.uint32), np.array([0, 0], np.uint32))
+
+
+# ---------------------------------------------------- contribution scheduling --
+def test_contribution_known_answers(oracle):
+    """unit_tests.cpp:2751-3005 on the oracle."""
+    o, m = oracle.contribution_schedule([0, 1, 2, 3], [0.10, 0.90, 0.30, 0.70])
+    assert o.tolist() == [1, 3, 2, 0] and m["input_item_count"] == 4 and m["scheduled_item_count"] == 4
+    assert abs(m["scheduling_overhead"] - 2.0) < 1e-12
+    assert oracle.contribution_schedule([3, 1, 2, 0], [0.5, 0.5, 0.9, 0.5])[0].tolist() == [2, 0, 1, 3]
+    o, m = oracle.contribution_schedule([0, 1, 2, 3], [0.0, 1e-8, 0.25, -1e-8], eps=1e-6)
+    assert m["zero_contribution_count"] == 3 and o.tolist() == [2, 1, 0, 3]
+    assert oracle.contribution_schedule([0, 1, 2], [0.1, 0.9, 0.3])[1]["reordered_item_count"] == 3
+    off = np.array([0, 2, 3, 3], np.uint64)
+    cols = np.array([1, 2, 2], np.uint32)
+    c = oracle.pagerank_contributions(off, cols, np.array([1, 0, 0], np.float32))
+    assert np.allclose(c, [0.95, 0.475, 0.475], atol=1e-5)
+    s = oracle.sssp_contributions(np.array([0, 5, np.inf, 10], np.float32), np.array([0, 3, 7, 12], np.float32))
+    assert s.tolist() == [0.0, 2.0, 1.0, 0.0]
+
+
+def test_contribution_oracle_vs_reference(hyt, oracle, reference):
+    rng = np.random.default_rng(9)
+    g = hyt.rmat(12, 8, 17)
+    V = g.num_vertices
+    for trial in range(4):
+        cur = rng.random(V).astype(np.float32)
+        cur /= cur.sum()
+        a = oracle.pagerank_contributions(g.row_offsets, g.column_indices, cur, 0.85)
+        b = reference.pagerank_contributions(g.row_offsets, g.column_indices, cur, 0.85)
+        assert np.array_equal(a.view(np.uint64), b.view(np.uint64)), trial
+        c64 = oracle.pagerank_contributions(g.row_offsets, g.column_indices, cur, 0.85, fp64=True)
+        assert np.max(np.abs(c64 - b)) < 1e-7
+    for trial in range(20):
+        n = int(rng.integers(0, 300))
+        cur = rng.choice([0.0, 1.0, 2.5, np.inf, np.nan, 7.0], n).astype(np.float32)
+        cand = rng.choice([0.0, 1.0, 2.5, np.inf, np.nan, 3.0], n).astype(np.float32)
+        for tol in (0.0, 0.5):
+            assert np.array_equal(oracle.sssp_contributions(cur, cand, tol), reference.sssp_contributions(cur, cand, tol))
+    for trial in range(60):
+        n = int(rng.integers(0, 400))
+        items = rng.integers(0, max(n, 1) * 2 if trial % 2 else 50, n)
+        contrib = rng.choice([0.0, -0.0, 0.5, 0.25, 1e-9, -1e-9, 3.0], n) if trial % 3 else rng.normal(size=n)
+        for det in (True, False):
+            a = oracle.contribution_schedule(items, contrib, det, 1e-6)
+            b = reference.contribution_schedule(items, contrib, det, 1e-6)
+            assert a[0].tolist() == b[0].tolist() and a[1] == b[1], (trial, det)
