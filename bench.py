@@ -3,7 +3,9 @@
 
 Workload (default): R-MAT scale 24, edge factor 16 (a,b,c = .57,.19,.19,
 uint32 weights uniform [1,63], self-loops/duplicates removed), graph
-resident in HBM.  One step = PageRank (damping 0.85) to L1 change <= 1e-6
+resident in HBM, stored in the reference's hub order (HubSorter ranking,
+built at graph creation; sources and results in the generator's ids;
+--vertex-order input keeps the generator's order).  One step = PageRank (damping 0.85) to L1 change <= 1e-6
 (max 100 iterations) + SSSP from 8 seeded sources, one at a time.
 
 Metric: GTEPS = traversed edges / s, with E per PageRank iteration and E per
@@ -57,6 +59,8 @@ def parse_args():
                          "text edge list -> CSR in HBM (GraphLoader) and the binary CSR file; contrib: PageRank "
                          "contributions + contribution schedule of every vertex + partition priorities")
     ap.add_argument("--hub-fraction", type=float, default=0.08)
+    ap.add_argument("--vertex-order", choices=["input", "hub"], default="hub",
+                    help="inhbm: store the graph in hub order (HYT_GRAPH_HUB_ORDER); results stay in input ids")
     ap.add_argument("--text-scale", type=int, default=22, help="load: R-MAT scale of the text edge list")
     ap.add_argument("--no-effect", action="store_true", help="hubsort: skip the solver comparison")
     ap.add_argument("--requests", type=int, default=20000)
@@ -1117,6 +1121,8 @@ def workload_config(args, V, E):
             "scale": args.scale, "edge_factor": args.edge_factor, "vertices": V, "edges": E,
             "sources": args.sources, "rmat_abc": [0.57, 0.19, 0.19], "weights": "uint32 uniform [1,63]",
             "seed": args.seed, "parallelism": f"replicas x{args.gpus}",
+            "vertex_order": ("hub: stored in the reference's HubSorter order (built at graph creation, inside the "
+                             "e2e step); sources and results in input ids") if args.vertex_order == "hub" else "input",
             "l2": "inputs larger than L2 (CSR + CSC + weights > 4 GB vs 126 MB L2)"}
 
 
@@ -1175,7 +1181,8 @@ def main():
     off_h, cols_h, w_h = host_graph_from_device(dcsr)
     off_np = off_h.numpy().view(np.uint64)
     sources = [int(s) for s in hyt.pick_sources(off_np, args.seed, args.sources)]
-    graph = hyt.Graph(dcsr, stream=sptr)
+    gflags = capi.HYT_GRAPH_ALL | (capi.HYT_GRAPH_HUB_ORDER if args.vertex_order == "hub" else 0)
+    graph = hyt.Graph(dcsr, stream=sptr, flags=gflags)
     dcsr.free()
     ranks_out = torch.empty(V, dtype=torch.float32, device="cuda")
     dist_out = torch.empty(V, dtype=torch.int32, device="cuda")
@@ -1249,7 +1256,7 @@ def main():
     torch.cuda.empty_cache()
 
     def e2e_step():
-        with hyt.Graph(csr_h, stream=sptr) as g2:
+        with hyt.Graph(csr_h, stream=sptr, flags=gflags) as g2:
             _, st = g2.pagerank(out=ranks_h, stream=sptr)
             its = st["iterations"]
             for s in sources:

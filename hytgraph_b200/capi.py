@@ -30,6 +30,7 @@ HYT_WEIGHTS_F32 = 2
 HYT_GRAPH_PULL = 1
 HYT_GRAPH_PUSH = 2
 HYT_GRAPH_ALL = 3
+HYT_GRAPH_HUB_ORDER = 4
 
 HYT_RUN_PROFILE = 1
 HYT_RUN_NO_GRAPH = 2

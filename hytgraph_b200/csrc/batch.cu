@@ -548,6 +548,7 @@ void QueryEngine::grow(uint32_t cap) {
 void QueryEngine::validate(const hyt_query &q) const {
     if (q.graph >= graphs_.size()) fail(HYT_E_INVALID, "query graph index is out of range");
     const GraphImpl &g = *graphs_[q.graph];
+    graph_require_caller_order(g, "the batch engine");
     if (q.kind == HYT_QUERY_SSSP) {
         if (!(g.flags & HYT_GRAPH_PUSH)) fail(HYT_E_INVALID, "SSSP queries need graphs built with HYT_GRAPH_PUSH");
         if (q.source >= g.V) fail(HYT_E_INVALID, "SSSP source vertex is out of range");

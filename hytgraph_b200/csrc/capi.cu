@@ -151,7 +151,7 @@ int hyt_graph_create(const hyt_csr *csr, const hyt_graph_options *options, hyt_g
                 g->impl.own_stream = true;
             }
             g->impl.host_scratch.allocate(64);
-            graph_build(g->impl, *csr, opt.flags);
+            graph_create(g->impl, *csr, opt.flags);
         } catch (...) {
             if (g->impl.own_stream && g->impl.stream) cudaStreamDestroy(g->impl.stream);
             delete g;

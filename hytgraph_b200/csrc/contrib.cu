@@ -233,6 +233,7 @@ void sort_pairs(K *&keys, K *keys_alt, V *&vals, V *vals_alt, uint64_t n, bool d
 }  // namespace
 
 void pagerank_contributions(GraphImpl &g, const float *ranks, float damping, double *out, double *device_ms) {
+    graph_require_caller_order(g, "hyt_pagerank_contributions");
     if (!(g.flags & HYT_GRAPH_PULL)) fail(HYT_E_INVALID, "graph was created without HYT_GRAPH_PULL");
     if (!ranks || !out) fail(HYT_E_INVALID, "NULL argument");
     if (!(damping >= 0.0f && damping < 1.0f)) fail(HYT_E_INVALID, "PageRank damping_factor must be in [0, 1)");

@@ -14,6 +14,8 @@
 #include "common.cuh"
 #include "graph.cuh"
 #include "prims.cuh"
+#include "scratch.cuh"
+#include "solvers.cuh"
 
 namespace hyt {
 namespace {
@@ -170,7 +172,85 @@ __global__ void untag_sources_kernel(const uint32_t *in_src, uint64_t n, const u
 
 }  // namespace
 
+namespace {
+
+__global__ void invert_kernel(const uint32_t *__restrict__ perm, uint64_t V, uint32_t *__restrict__ inv) {
+    for (uint64_t n = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; n < V; n += uint64_t(gridDim.x) * blockDim.x)
+        inv[perm[n]] = static_cast<uint32_t>(n);
+}
+
+// dst[v] = src[inv[v]]: values back in the caller's vertex order.
+__global__ void emit_kernel(const uint32_t *__restrict__ src, const uint32_t *__restrict__ inv, uint64_t V,
+                            uint32_t *__restrict__ dst) {
+    for (uint64_t v = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; v < V; v += uint64_t(gridDim.x) * blockDim.x)
+        dst[v] = src[inv[v]];
+}
+
+}  // namespace
+
+void graph_create(GraphImpl &g, const hyt_csr &csr, uint32_t flags) {
+    if (!(flags & HYT_GRAPH_HUB_ORDER)) {
+        graph_build(g, csr, flags);
+        return;
+    }
+    const uint64_t V = csr.num_vertices;
+    if (V == 0) fail(HYT_E_INVALID, "graph requires at least one vertex");
+    if (V > 0xFFFFFFFFull) fail(HYT_E_INVALID, "vertex ids are uint32: num_vertices must be < 2^32");
+    // the reference's HubSorter with every vertex ranked, then the CSR
+    // renumbered (both on the GPU)
+    DeviceArray<uint32_t> perm(V);
+    hub_sort(csr, 1.0, perm.get(), nullptr, nullptr, nullptr);
+    hyt_csr_buffers b{};
+    csr_reorder(csr, perm.get(), true, &b, nullptr);
+    struct Free {
+        hyt_csr_buffers *b;
+        ~Free() { hyt_csr_buffers_free(b); }
+    } release{&b};
+    hyt_csr r = csr;
+    r.row_offsets = b.row_offsets;
+    r.column_indices = b.column_indices;
+    r.weights = b.weights;
+    graph_build(g, r, flags & ~uint32_t(HYT_GRAPH_HUB_ORDER));
+    g.inv.allocate(V);
+    invert_kernel<<<grid_for(V, 256), 256, 0, g.stream>>>(perm.get(), V, g.inv.get());
+    HYT_CUDA(cudaGetLastError());
+    HYT_CUDA(cudaStreamSynchronize(g.stream));
+    g.perm = std::move(perm);
+}
+
+uint32_t graph_vertex(const GraphImpl &g, uint32_t v, cudaStream_t s) {
+    if (!g.inv.get()) return v;
+    uint32_t n = 0;
+    HYT_CUDA(cudaMemcpyAsync(&n, g.inv.get() + v, 4, cudaMemcpyDeviceToHost, s));
+    HYT_CUDA(cudaStreamSynchronize(s));
+    return n;
+}
+
+void graph_emit(const GraphImpl &g, void *dst, const void *src, cudaStream_t s) {
+    const uint64_t V = g.V;
+    if (!g.inv.get()) {
+        copy_from_device(dst, src, V * 4, s);
+        return;
+    }
+    if (is_device_pointer(dst)) {
+        emit_kernel<<<grid_for(V, 256), 256, 0, s>>>(static_cast<const uint32_t *>(src), g.inv.get(), V,
+                                                     static_cast<uint32_t *>(dst));
+        HYT_CUDA(cudaGetLastError());
+        return;
+    }
+    Scratch<uint32_t> tmp(V, s);
+    emit_kernel<<<grid_for(V, 256), 256, 0, s>>>(static_cast<const uint32_t *>(src), g.inv.get(), V, tmp.get());
+    HYT_CUDA(cudaGetLastError());
+    copy_from_device(dst, tmp.get(), V * 4, s);
+    HYT_CUDA(cudaStreamSynchronize(s));
+}
+
+void graph_require_caller_order(const GraphImpl &g, const char *what) {
+    if (g.perm.get()) fail(HYT_E_UNSUPPORTED, std::string(what) + " does not take graphs built with HYT_GRAPH_HUB_ORDER");
+}
+
 void graph_copy_csc(const GraphImpl &g, uint64_t *in_offsets, uint32_t *in_sources) {
+    graph_require_caller_order(g, "hyt_graph_copy_csc");
     if (!(g.flags & HYT_GRAPH_PULL)) fail(HYT_E_INVALID, "graph was created without HYT_GRAPH_PULL");
     cudaStream_t s = g.stream;
     HYT_CUDA(cudaMemcpyAsync(in_offsets, g.in_offsets.get(), (g.V + 1) * 8, cudaMemcpyDefault, s));

@@ -56,6 +56,9 @@ struct GraphImpl {
     DeviceArray<uint32_t> cols;
     DeviceArray<uint32_t> weights;
     DeviceArray<uint32_t> out_degree;
+    // HYT_GRAPH_HUB_ORDER: perm[new] = caller id, inv[caller id] = new
+    // (empty otherwise)
+    DeviceArray<uint32_t> perm, inv;
 
     // pull side
     DeviceArray<uint64_t> in_offsets;
@@ -108,6 +111,15 @@ void graph_build(GraphImpl &g, const hyt_csr &csr, uint32_t flags);
 
 // Copies the CSC with hot tags removed into caller buffers (host or device).
 void graph_copy_csc(const GraphImpl &g, uint64_t *in_offsets, uint32_t *in_sources);
+// Builds the graph; with HYT_GRAPH_HUB_ORDER in flags, in hub order.
+void graph_create(GraphImpl &g, const hyt_csr &csr, uint32_t flags);
+// The internal id of a caller's vertex (identity without a hub order).
+uint32_t graph_vertex(const GraphImpl &g, uint32_t v, cudaStream_t s);
+// Writes V 4-byte per-vertex values (internal order, device) to dst (host
+// or device) in the caller's vertex order.
+void graph_emit(const GraphImpl &g, void *dst, const void *src, cudaStream_t s);
+// Fails with HYT_E_UNSUPPORTED for a hub-ordered graph.
+void graph_require_caller_order(const GraphImpl &g, const char *what);
 
 }  // namespace hyt
 

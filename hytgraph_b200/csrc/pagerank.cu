@@ -318,7 +318,7 @@ static void pr_solve(GraphImpl &g, bool personalized, uint32_t source, float dam
     if (graph) cudaGraphDestroy(graph);
     if (use_graph) launches += h.iter;
     if (h.iter == 0) fail(HYT_E_INTERNAL, "PageRank made no progress");
-    if (ranks_out) copy_from_device(ranks_out, g.rank[h.iter & 1].get(), V * sizeof(float), s);
+    if (ranks_out) graph_emit(g, ranks_out, g.rank[h.iter & 1].get(), s);
 
     if (stats) {
         stats->iterations = h.iter;
@@ -352,7 +352,8 @@ void ppr_run(GraphImpl &g, const hyt_ppr_params &p, float *ranks_out, hyt_run_st
     if (p.max_iterations == 0) fail(HYT_E_INVALID, "personalized PageRank max_iterations must be greater than zero");
     if (p.source >= g.V) fail(HYT_E_INVALID, "personalized PageRank source vertex is out of range");
     cudaStream_t s = p.stream ? static_cast<cudaStream_t>(p.stream) : g.stream;
-    pr_solve(g, true, p.source, 1.0f - p.restart, p.tolerance, p.max_iterations, p.flags, s, ranks_out, stats);
+    pr_solve(g, true, graph_vertex(g, p.source, s), 1.0f - p.restart, p.tolerance, p.max_iterations, p.flags, s,
+             ranks_out, stats);
 }
 
 void pagerank_partitioned(GraphImpl &g, PullSource &src, bool personalized, uint32_t source, float damping,

@@ -558,7 +558,7 @@ void sssp_solve(GraphImpl &g, uint32_t source, uint32_t delta, uint32_t max_roun
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
     if (use_graph) launches += 4 * h.round;
-    if (dist_out) copy_from_device(dist_out, g.dist.get(), V * sizeof(uint32_t), s);
+    if (dist_out) graph_emit(g, dist_out, g.dist.get(), s);
     if (stats) {
         stats->iterations = h.round;
         stats->converged = h.converged;
@@ -597,10 +597,11 @@ void sssp_run(GraphImpl &g, const hyt_sssp_params &p, uint32_t *dist_out, hyt_ru
     const uint64_t cap = std::min<uint64_t>(4 * g.V + 1024, 0x7FFFFFFFull);
     const uint32_t max_rounds = p.max_rounds ? p.max_rounds : static_cast<uint32_t>(cap);
     const uint32_t delta = p.delta ? p.delta : sssp_default_delta(g);
+    const uint32_t src = graph_vertex(g, p.source, s);
     switch (g.weight_kind) {
-        case HYT_WEIGHTS_NONE: sssp_solve<HYT_WEIGHTS_NONE>(g, p.source, delta, max_rounds, p.flags, s, dist_out, stats); break;
-        case HYT_WEIGHTS_U32: sssp_solve<HYT_WEIGHTS_U32>(g, p.source, delta, max_rounds, p.flags, s, dist_out, stats); break;
-        case HYT_WEIGHTS_F32: sssp_solve<HYT_WEIGHTS_F32>(g, p.source, kNoDelta, max_rounds, p.flags, s, dist_out, stats); break;
+        case HYT_WEIGHTS_NONE: sssp_solve<HYT_WEIGHTS_NONE>(g, src, delta, max_rounds, p.flags, s, dist_out, stats); break;
+        case HYT_WEIGHTS_U32: sssp_solve<HYT_WEIGHTS_U32>(g, src, delta, max_rounds, p.flags, s, dist_out, stats); break;
+        case HYT_WEIGHTS_F32: sssp_solve<HYT_WEIGHTS_F32>(g, src, kNoDelta, max_rounds, p.flags, s, dist_out, stats); break;
         default: fail(HYT_E_INTERNAL, "unknown weight kind");
     }
 }

@@ -92,7 +92,15 @@ typedef struct hyt_graph hyt_graph;
 enum hyt_graph_flags {
     HYT_GRAPH_PULL = 1u,   /* build the CSC + PageRank work tiles (pull) */
     HYT_GRAPH_PUSH = 2u,   /* keep the CSR (+ weights) for frontier push */
-    HYT_GRAPH_ALL = 3u
+    HYT_GRAPH_ALL = 3u,
+    /* Store the graph in hub order: vertices renumbered by the reference's
+     * hub score Do*Di (HubSorter with hub_fraction 1, hyt_hub_sort), so the
+     * high-degree vertices' values share cache lines.  Sources and results
+     * stay in the caller's vertex ids (mapped on the way in and out).
+     * hyt_pagerank, hyt_ppr and hyt_sssp only: hyt_graph_copy_csc,
+     * hyt_pagerank_contributions and the batch / server engines reject such
+     * graphs (HYT_E_UNSUPPORTED). */
+    HYT_GRAPH_HUB_ORDER = 4u
 };
 
 typedef struct hyt_graph_options {

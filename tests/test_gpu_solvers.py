@@ -199,3 +199,41 @@ def _dev_csr(hyt, g, t_off, t_cols, t_w):
     c.row_offsets, c.column_indices, c.weights = t_off.data_ptr(), t_cols.data_ptr(), t_w.data_ptr()
     c.weight_kind = hyt.capi.HYT_WEIGHTS_U32
     return c
+
+
+def test_hub_ordered_graph_same_results(hyt, gpu, oracle):
+    """HYT_GRAPH_HUB_ORDER renumbers vertices internally by hub score; every
+    source and result stays in the caller's ids: SSSP distances identical,
+    PageRank / PPR within the FP64 tolerance, unsupported paths rejected."""
+    g = hyt.rmat(14, 16, 77)
+    srcs = hyt.pick_sources(g.row_offsets, 5, 4)
+    gf = hyt.CSR(g.row_offsets, g.column_indices, g.weights.astype(np.float32) / 2)
+    gn = hyt.CSR(g.row_offsets, g.column_indices)
+    for csr in (g, gf, gn):
+        with hyt.Graph(csr) as a, hyt.Graph(csr, flags=hyt.capi.HYT_GRAPH_ALL | hyt.capi.HYT_GRAPH_HUB_ORDER) as b:
+            for s in srcs:
+                assert np.array_equal(a.sssp(int(s))[0], b.sssp(int(s))[0])
+    ref = oracle.pagerank_f64(g.row_offsets, g.column_indices, 0.85, 1e-10, 200)[0]
+    with hyt.Graph(g, flags=hyt.capi.HYT_GRAPH_HUB_ORDER) as b:
+        r, st = b.pagerank(tolerance=1e-7, max_iterations=200)
+        assert np.abs(r.astype(np.float64) - ref).sum() <= 1e-5
+        s = int(srcs[0])
+        p, _ = b.ppr(s, tolerance=1e-9, max_iterations=300)
+        want = oracle.ppr_f64(g.row_offsets, g.column_indices, s, 0.15, 1e-12, 500)[0]
+        assert np.abs(p.astype(np.float64) - want).sum() <= 1e-5
+        import torch
+
+        out = torch.empty(g.num_vertices, dtype=torch.int32, device="cuda")
+        b.sssp(s, out=out)  # device output: mapped on the device
+        with hyt.Graph(g) as a:
+            assert np.array_equal(out.cpu().numpy().view(np.uint32), a.sssp(s)[0])
+        with pytest.raises(hyt.HytError) as e:
+            b.copy_csc()
+        assert e.value.code == hyt.capi.HYT_E_UNSUPPORTED
+        with pytest.raises(hyt.HytError) as e:
+            b.pagerank_contributions(r)
+        assert e.value.code == hyt.capi.HYT_E_UNSUPPORTED
+        with hyt.Batch([b]) as bt:
+            with pytest.raises(hyt.HytError) as e:
+                bt.run([{"graph": 0, "kind": "sssp", "source": s}])
+            assert e.value.code == hyt.capi.HYT_E_UNSUPPORTED
