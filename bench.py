@@ -48,7 +48,7 @@ def parse_args():
     ap.add_argument("--edge-factor", type=int, default=16)
     ap.add_argument("--sources", type=int, default=8)
     ap.add_argument("--seed", type=int, default=20241203)
-    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", choices=["inhbm", "hybrid", "batch", "serve", "hubsort", "load", "contrib"],
                     default="inhbm",
