@@ -197,11 +197,35 @@ void graph_create(GraphImpl &g, const hyt_csr &csr, uint32_t flags) {
     if (V == 0) fail(HYT_E_INVALID, "graph requires at least one vertex");
     if (V > 0xFFFFFFFFull) fail(HYT_E_INVALID, "vertex ids are uint32: num_vertices must be < 2^32");
     // the reference's HubSorter with every vertex ranked, then the CSR
-    // renumbered (both on the GPU)
+    // renumbered (both on the GPU, from one device copy of a host CSR)
+    const uint64_t E = csr.num_edges;
+    const bool weighted = csr.weight_kind != HYT_WEIGHTS_NONE && E;
+    DeviceArray<uint64_t> d_off;
+    DeviceArray<uint32_t> d_cols, d_w;
+    hyt_csr dev = csr;
+    if (csr.row_offsets && !is_device_pointer(csr.row_offsets)) {
+        d_off.allocate(V + 1);
+        copy_to_device(d_off.get(), csr.row_offsets, (V + 1) * 8, g.stream);
+        dev.row_offsets = d_off.get();
+    }
+    if (E && csr.column_indices && !is_device_pointer(csr.column_indices)) {
+        d_cols.allocate(E);
+        copy_to_device(d_cols.get(), csr.column_indices, E * 4, g.stream);
+        dev.column_indices = d_cols.get();
+    }
+    if (weighted && csr.weights && !is_device_pointer(csr.weights)) {
+        d_w.allocate(E);
+        copy_to_device(d_w.get(), csr.weights, E * 4, g.stream);
+        dev.weights = d_w.get();
+    }
+    HYT_CUDA(cudaStreamSynchronize(g.stream));
     DeviceArray<uint32_t> perm(V);
-    hub_sort(csr, 1.0, perm.get(), nullptr, nullptr, nullptr);
+    hub_sort(dev, 1.0, perm.get(), nullptr, nullptr, nullptr);
     hyt_csr_buffers b{};
-    csr_reorder(csr, perm.get(), true, &b, nullptr);
+    csr_reorder(dev, perm.get(), true, &b, nullptr);
+    d_off.release();
+    d_cols.release();
+    d_w.release();
     struct Free {
         hyt_csr_buffers *b;
         ~Free() { hyt_csr_buffers_free(b); }
