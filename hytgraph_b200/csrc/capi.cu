@@ -1,9 +1,12 @@
 // extern "C" entry points of libhyt_core.so (declared in include/hyt/capi.h).
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
+#include <unordered_map>
 #include <string>
 
 #include "common.cuh"
+#include "scratch.cuh"
 #include "graph.cuh"
 #include "solvers.cuh"
 
@@ -14,6 +17,24 @@ thread_local std::string g_last_error;
 
 void set_last_error(const std::string &msg) { g_last_error = msg; }
 void clear_last_error() { g_last_error.clear(); }
+
+cudaMemPool_t graph_pool(int device) {
+    static std::mutex mu;
+    static std::unordered_map<int, cudaMemPool_t> pools;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = pools.find(device);
+    if (it != pools.end()) return it->second;
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaMemPool_t pool = nullptr;
+    HYT_CUDA(cudaMemPoolCreate(&pool, &props));
+    uint64_t keep = kGraphPoolKeep;
+    HYT_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    pools[device] = pool;
+    return pool;
+}
 
 bool is_device_pointer(const void *p) {
     if (!p) return false;
@@ -350,6 +371,19 @@ int hyt_partition_contributions(const double *vertex_contributions, uint64_t num
     return guarded([&] {
         require_device();
         partition_contributions(vertex_contributions, num_vertices, bounds, num_partitions, out);
+    });
+}
+
+int hyt_trim_device_memory(int device) {
+    return guarded([&] {
+        require_device();
+        int cur = 0;
+        HYT_CUDA(cudaGetDevice(&cur));
+        HYT_CUDA(cudaSetDevice(device));
+        HYT_CUDA(cudaDeviceSynchronize());
+        HYT_CUDA(cudaMemPoolTrimTo(graph_pool(device), 0));
+        HYT_CUDA(cudaMemPoolTrimTo(scratch_pool(), 0));
+        HYT_CUDA(cudaSetDevice(cur));
     });
 }
 

@@ -97,6 +97,68 @@ struct DeviceArray {
     T *get() const { return ptr; }
 };
 
+// Device pool for long-lived graph arrays: stream-ordered allocations from
+// one pool per device that keeps up to kGraphPoolKeep bytes mapped after
+// they are freed, so creating and destroying graphs repeatedly does not pay
+// for mapping fresh memory each time (hyt_trim_device_memory returns it).
+constexpr uint64_t kGraphPoolKeep = uint64_t(16) << 30;
+cudaMemPool_t graph_pool(int device);
+
+// Owning device buffer from the graph pool; same interface as DeviceArray.
+// Allocation completes before allocate() returns; release() waits for the
+// device (as cudaFree does) before handing the memory back.
+template <class T>
+struct GraphArray {
+    T *ptr = nullptr;
+    size_t count = 0;
+    int dev = 0;
+
+    GraphArray() = default;
+    explicit GraphArray(size_t n) { allocate(n); }
+    GraphArray(const GraphArray &) = delete;
+    GraphArray &operator=(const GraphArray &) = delete;
+    GraphArray(GraphArray &&o) noexcept : ptr(o.ptr), count(o.count), dev(o.dev) { o.ptr = nullptr; o.count = 0; }
+    GraphArray &operator=(GraphArray &&o) noexcept {
+        if (this != &o) {
+            release();
+            ptr = o.ptr;
+            count = o.count;
+            dev = o.dev;
+            o.ptr = nullptr;
+            o.count = 0;
+        }
+        return *this;
+    }
+    ~GraphArray() { release(); }
+
+    void allocate(size_t n) {
+        release();
+        if (n == 0) return;
+        HYT_CUDA(cudaGetDevice(&dev));
+        void *p = nullptr;
+        // 16 bytes of tail padding, as DeviceArray
+        HYT_CUDA(cudaMallocFromPoolAsync(&p, n * sizeof(T) + 16, graph_pool(dev), cudaStreamLegacy));
+        HYT_CUDA(cudaStreamSynchronize(cudaStreamLegacy));
+        ptr = static_cast<T *>(p);
+        count = n;
+    }
+    void release() noexcept {
+        if (ptr) {
+            int cur = 0;
+            cudaGetDevice(&cur);
+            if (cur != dev) cudaSetDevice(dev);
+            cudaDeviceSynchronize();  // no kernel may still use it
+            cudaFreeAsync(ptr, cudaStreamLegacy);
+            cudaStreamSynchronize(cudaStreamLegacy);
+            if (cur != dev) cudaSetDevice(cur);
+        }
+        ptr = nullptr;
+        count = 0;
+    }
+    size_t bytes() const { return count * sizeof(T); }
+    T *get() const { return ptr; }
+};
+
 // Owning pinned host buffer.
 template <class T>
 struct PinnedArray {

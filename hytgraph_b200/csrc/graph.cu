@@ -219,7 +219,7 @@ void graph_create(GraphImpl &g, const hyt_csr &csr, uint32_t flags) {
         dev.weights = d_w.get();
     }
     HYT_CUDA(cudaStreamSynchronize(g.stream));
-    DeviceArray<uint32_t> perm(V);
+    GraphArray<uint32_t> perm(V);
     hub_sort(dev, 1.0, perm.get(), nullptr, nullptr, nullptr);
     hyt_csr_buffers b{};
     csr_reorder(dev, perm.get(), true, &b, nullptr);

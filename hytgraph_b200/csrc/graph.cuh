@@ -52,27 +52,27 @@ struct GraphImpl {
     uint32_t default_delta = 0;  // SSSP near/far bucket width (2x mean u32 weight)
 
     // push side
-    DeviceArray<uint64_t> row_offsets;
-    DeviceArray<uint32_t> cols;
-    DeviceArray<uint32_t> weights;
-    DeviceArray<uint32_t> out_degree;
+    GraphArray<uint64_t> row_offsets;
+    GraphArray<uint32_t> cols;
+    GraphArray<uint32_t> weights;
+    GraphArray<uint32_t> out_degree;
     // HYT_GRAPH_HUB_ORDER: perm[new] = caller id, inv[caller id] = new
     // (empty otherwise)
-    DeviceArray<uint32_t> perm, inv;
+    GraphArray<uint32_t> perm, inv;
 
     // pull side
-    DeviceArray<uint64_t> in_offsets;
-    DeviceArray<uint32_t> in_sources;
-    DeviceArray<uint32_t> in_weights;   // [E] weights in CSC order (PUSH|PULL weighted graphs; SSSP pull rounds)
-    DeviceArray<uint32_t> tile_start;   // [num_tiles + 1]
-    DeviceArray<LongRow> long_rows;     // [num_long]
-    DeviceArray<uint2> chunk_tasks;     // [num_chunks] = (long row index, chunk)
+    GraphArray<uint64_t> in_offsets;
+    GraphArray<uint32_t> in_sources;
+    GraphArray<uint32_t> in_weights;   // [E] weights in CSC order (PUSH|PULL weighted graphs; SSSP pull rounds)
+    GraphArray<uint32_t> tile_start;   // [num_tiles + 1]
+    GraphArray<LongRow> long_rows;     // [num_long]
+    GraphArray<uint2> chunk_tasks;     // [num_chunks] = (long row index, chunk)
     uint64_t num_tiles = 0, num_long = 0, num_chunks = 0;
     uint32_t tile_cost = kTileCostDefault;  // a row is long when its in-degree >= tile_cost
     // Hot sources: the num_hot vertices of largest out-degree.  Their
     // occurrences in in_sources carry kHotTag | slot, and each PageRank CTA
     // keeps their contributions in shared memory for the iteration.
-    DeviceArray<uint32_t> hot_vertex;   // [num_hot], by slot
+    GraphArray<uint32_t> hot_vertex;   // [num_hot], by slot
     uint32_t num_hot = 0;
     uint64_t hot_edges = 0;             // in-edges whose source is hot
 
@@ -81,19 +81,19 @@ struct GraphImpl {
     double build_ms = 0.0;
 
     // Solver workspaces, grown on demand and reused across calls.
-    DeviceArray<float> rank[2];
-    DeviceArray<float> contrib[2];
-    DeviceArray<float> partial;        // long-row chunk partial sums (s, c)
-    DeviceArray<uint32_t> ticket;      // long-row arrival counters
-    DeviceArray<unsigned char> pr_state;
+    GraphArray<float> rank[2];
+    GraphArray<float> contrib[2];
+    GraphArray<float> partial;        // long-row chunk partial sums (s, c)
+    GraphArray<uint32_t> ticket;      // long-row arrival counters
+    GraphArray<unsigned char> pr_state;
     uint32_t pr_state_iters = 0;
 
-    DeviceArray<uint32_t> dist;
-    DeviceArray<uint32_t> stamp;
-    DeviceArray<uint32_t> queue[2];
-    DeviceArray<uint32_t> far[2];
-    DeviceArray<uint2> hub_tasks;
-    DeviceArray<unsigned char> sssp_state;
+    GraphArray<uint32_t> dist;
+    GraphArray<uint32_t> stamp;
+    GraphArray<uint32_t> queue[2];
+    GraphArray<uint32_t> far[2];
+    GraphArray<uint2> hub_tasks;
+    GraphArray<unsigned char> sssp_state;
     PinnedArray<uint64_t> host_scratch;  // small pinned readback area
 
     size_t device_bytes() const;

@@ -109,6 +109,13 @@ typedef struct hyt_graph_options {
     void *stream;    /* cudaStream_t used for the upload (NULL = own) */
 } hyt_graph_options;
 
+/* In-HBM graph arrays and the one-shot transforms' scratch come from
+ * per-device memory pools that keep freed memory mapped (graph arrays: up to
+ * 16 GiB; scratch: up to 2 GiB), so repeated graph creation does not map
+ * fresh memory each time.  This returns that cached memory of `device` to
+ * the driver (after waiting for the device). */
+int hyt_trim_device_memory(int device);
+
 typedef struct hyt_graph_info {
     uint64_t num_vertices;
     uint64_t num_edges;
