@@ -200,8 +200,8 @@ void graph_create(GraphImpl &g, const hyt_csr &csr, uint32_t flags) {
     // renumbered (both on the GPU, from one device copy of a host CSR)
     const uint64_t E = csr.num_edges;
     const bool weighted = csr.weight_kind != HYT_WEIGHTS_NONE && E;
-    DeviceArray<uint64_t> d_off;
-    DeviceArray<uint32_t> d_cols, d_w;
+    GraphArray<uint64_t> d_off;
+    GraphArray<uint32_t> d_cols, d_w;
     hyt_csr dev = csr;
     if (csr.row_offsets && !is_device_pointer(csr.row_offsets)) {
         d_off.allocate(V + 1);
@@ -222,13 +222,13 @@ void graph_create(GraphImpl &g, const hyt_csr &csr, uint32_t flags) {
     GraphArray<uint32_t> perm(V);
     hub_sort(dev, 1.0, perm.get(), nullptr, nullptr, nullptr);
     hyt_csr_buffers b{};
-    csr_reorder(dev, perm.get(), true, &b, nullptr);
+    csr_reorder(dev, perm.get(), true, &b, nullptr, true);
     d_off.release();
     d_cols.release();
     d_w.release();
     struct Free {
         hyt_csr_buffers *b;
-        ~Free() { hyt_csr_buffers_free(b); }
+        ~Free() { free_pooled_buffers(b); }
     } release{&b};
     hyt_csr r = csr;
     r.row_offsets = b.row_offsets;
@@ -317,18 +317,18 @@ void build_pull_tiles(GraphImpl &g, cudaStream_t s) {
     HYT_CUDA(cudaGetLastError());
 
     // Long rows (in-degree >= tile_cost) and their chunk tasks.
-    DeviceArray<uint32_t> in_deg(V);
-    DeviceArray<uint8_t> is_long(V);
+    Scratch<uint32_t> in_deg(V, s);
+    Scratch<uint8_t> is_long(V, s);
     in_degree_kernel<<<grid_for(V, 256), 256, 0, s>>>(g.in_offsets.get(), V, g.tile_cost, in_deg.get(),
                                                        is_long.get());
     HYT_CUDA(cudaGetLastError());
     g.max_in_degree = prims::reduce_max_u32(in_deg.get(), V, s);
-    DeviceArray<uint32_t> long_ids(V);
+    Scratch<uint32_t> long_ids(V, s);
     g.num_long = prims::select_flagged_index(is_long.get(), long_ids.get(), V, s);
     std::vector<LongRow> lr(g.num_long);
     std::vector<uint2> tasks;
     if (g.num_long) {
-        DeviceArray<uint32_t> long_deg(g.num_long);
+        Scratch<uint32_t> long_deg(g.num_long, s);
         gather_u32_kernel<<<grid_for(g.num_long, 256), 256, 0, s>>>(in_deg.get(), long_ids.get(), g.num_long,
                                                                      long_deg.get());
         HYT_CUDA(cudaGetLastError());
@@ -402,8 +402,8 @@ void graph_build(GraphImpl &g, const hyt_csr &csr, uint32_t flags) {
 
     // Validation: malformed offsets or out-of-range ids would turn into
     // out-of-bounds device accesses later, so they are rejected here.
-    DeviceArray<uint32_t> err(1);
-    DeviceArray<unsigned long long> counter(1);
+    Scratch<uint32_t> err(1, s);
+    Scratch<unsigned long long> counter(1, s);
     HYT_CUDA(cudaMemsetAsync(err.get(), 0, sizeof(uint32_t), s));
     HYT_CUDA(cudaMemsetAsync(counter.get(), 0, sizeof(unsigned long long), s));
     validate_offsets_kernel<<<grid_for(V, 256), 256, 0, s>>>(g.row_offsets.get(), V, E, err.get());
@@ -414,7 +414,7 @@ void graph_build(GraphImpl &g, const hyt_csr &csr, uint32_t flags) {
     if (h_err & kBadOffsets) fail(HYT_E_INVALID, "row offsets must start at 0 and be non-decreasing");
     if (h_err & kBadTerminal) fail(HYT_E_INVALID, "terminal row offset must equal the number of edges");
     if (E) {
-        DeviceArray<unsigned long long> wsum(1);
+        Scratch<unsigned long long> wsum(1, s);
         HYT_CUDA(cudaMemsetAsync(wsum.get(), 0, sizeof(unsigned long long), s));
         validate_edges_kernel<<<grid_for(E, 256), 256, 0, s>>>(g.cols.get(), keep_weights ? g.weights.get() : nullptr,
                                                                 keep_weights ? csr.weight_kind : 0u, V, E, err.get(),
@@ -447,18 +447,18 @@ void graph_build(GraphImpl &g, const hyt_csr &csr, uint32_t flags) {
         // CSC transpose: stable sort of (destination, source) by destination.
         // Graphs that keep both sides with weights also get the weights in
         // CSC order (SSSP pull rounds): sort edge ids instead, then gather.
-        DeviceArray<uint32_t> keys(E ? E : 1);
+        Scratch<uint32_t> keys(E ? E : 1, s);
         g.in_sources.allocate(E ? E : 1);
         const bool csc_weights = (flags & HYT_GRAPH_PUSH) && keep_weights && g.weights.get();
         if (E) {
             HYT_CUDA(cudaMemcpyAsync(keys.get(), g.cols.get(), E * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
             const unsigned blocks = static_cast<unsigned>(std::min<uint64_t>((V + 255) / 256, 148ull * 64));
             if (csc_weights) {
-                DeviceArray<uint32_t> perm(E);
+                Scratch<uint32_t> perm(E, s);
                 iota_kernel<<<grid_for(E, 256), 256, 0, s>>>(perm.get(), E);
                 HYT_CUDA(cudaGetLastError());
                 prims::sort_pairs_u32(keys.get(), perm.get(), E, bits_for(V - 1), s);
-                DeviceArray<uint32_t> src(E);
+                Scratch<uint32_t> src(E, s);
                 expand_sources_kernel<<<blocks, 256, 0, s>>>(g.row_offsets.get(), V, src.get());
                 HYT_CUDA(cudaGetLastError());
                 gather_u32_kernel<<<grid_for(E, 256), 256, 0, s>>>(src.get(), perm.get(), E, g.in_sources.get());
@@ -480,7 +480,7 @@ void graph_build(GraphImpl &g, const hyt_csr &csr, uint32_t flags) {
         // Hot sources: largest out-degree first (ties by vertex id).
         g.num_hot = static_cast<uint32_t>(std::min<uint64_t>(hot_request, V));
         if (E && g.num_hot) {
-            DeviceArray<uint32_t> deg(V), ids(V), slot(V);
+            Scratch<uint32_t> deg(V, s), ids(V, s), slot(V, s);
             HYT_CUDA(cudaMemcpyAsync(deg.get(), g.out_degree.get(), V * 4, cudaMemcpyDeviceToDevice, s));
             iota_kernel<<<grid_for(V, 256), 256, 0, s>>>(ids.get(), V);
             HYT_CUDA(cudaGetLastError());

@@ -4,31 +4,18 @@
 
 #include "common.cuh"
 #include "prims.cuh"
+#include "scratch.cuh"
 
 namespace hyt::prims {
-namespace {
-
-struct TempStorage {
-    void *ptr = nullptr;
-    size_t bytes = 0;
-    explicit TempStorage(size_t b) : bytes(b) {
-        if (b) HYT_CUDA(cudaMalloc(&ptr, b));
-    }
-    ~TempStorage() {
-        if (ptr) cudaFree(ptr);
-    }
-};
-
-}  // namespace
 
 void sort_pairs_u32(uint32_t *keys, uint32_t *vals, size_t n, int end_bit, cudaStream_t s) {
     if (n < 2) return;
-    DeviceArray<uint32_t> k2(n), v2(n);
+    Scratch<uint32_t> k2(n, s), v2(n, s);
     cub::DoubleBuffer<uint32_t> kb(keys, k2.get()), vb(vals, v2.get());
     size_t tb = 0;
     HYT_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, kb, vb, static_cast<int64_t>(n), 0, end_bit, s));
-    TempStorage tmp(tb);
-    HYT_CUDA(cub::DeviceRadixSort::SortPairs(tmp.ptr, tb, kb, vb, static_cast<int64_t>(n), 0, end_bit, s));
+    Scratch<uint8_t> tmp(tb, s);
+    HYT_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), tb, kb, vb, static_cast<int64_t>(n), 0, end_bit, s));
     if (kb.Current() != keys)
         HYT_CUDA(cudaMemcpyAsync(keys, kb.Current(), n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
     if (vb.Current() != vals)
@@ -38,12 +25,12 @@ void sort_pairs_u32(uint32_t *keys, uint32_t *vals, size_t n, int end_bit, cudaS
 
 void sort_pairs_desc_u32(uint32_t *keys, uint32_t *vals, size_t n, cudaStream_t s) {
     if (n < 2) return;
-    DeviceArray<uint32_t> k2(n), v2(n);
+    Scratch<uint32_t> k2(n, s), v2(n, s);
     cub::DoubleBuffer<uint32_t> kb(keys, k2.get()), vb(vals, v2.get());
     size_t tb = 0;
     HYT_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, kb, vb, static_cast<int64_t>(n), 0, 32, s));
-    TempStorage tmp(tb);
-    HYT_CUDA(cub::DeviceRadixSort::SortPairsDescending(tmp.ptr, tb, kb, vb, static_cast<int64_t>(n), 0, 32, s));
+    Scratch<uint8_t> tmp(tb, s);
+    HYT_CUDA(cub::DeviceRadixSort::SortPairsDescending(tmp.get(), tb, kb, vb, static_cast<int64_t>(n), 0, 32, s));
     if (kb.Current() != keys)
         HYT_CUDA(cudaMemcpyAsync(keys, kb.Current(), n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
     if (vb.Current() != vals)
@@ -53,14 +40,14 @@ void sort_pairs_desc_u32(uint32_t *keys, uint32_t *vals, size_t n, cudaStream_t 
 
 void sort_pairs_desc_u64(uint64_t *keys, uint32_t *vals, size_t n, cudaStream_t s) {
     if (n < 2) return;
-    DeviceArray<uint64_t> k2(n);
-    DeviceArray<uint32_t> v2(n);
+    Scratch<uint64_t> k2(n, s);
+    Scratch<uint32_t> v2(n, s);
     cub::DoubleBuffer<uint64_t> kb(keys, k2.get());
     cub::DoubleBuffer<uint32_t> vb(vals, v2.get());
     size_t tb = 0;
     HYT_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, kb, vb, static_cast<int64_t>(n), 0, 64, s));
-    TempStorage tmp(tb);
-    HYT_CUDA(cub::DeviceRadixSort::SortPairsDescending(tmp.ptr, tb, kb, vb, static_cast<int64_t>(n), 0, 64, s));
+    Scratch<uint8_t> tmp(tb, s);
+    HYT_CUDA(cub::DeviceRadixSort::SortPairsDescending(tmp.get(), tb, kb, vb, static_cast<int64_t>(n), 0, 64, s));
     if (kb.Current() != keys)
         HYT_CUDA(cudaMemcpyAsync(keys, kb.Current(), n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
     if (vb.Current() != vals)
@@ -70,12 +57,12 @@ void sort_pairs_desc_u64(uint64_t *keys, uint32_t *vals, size_t n, cudaStream_t 
 
 void sort_keys_u64(uint64_t *keys, size_t n, int end_bit, cudaStream_t s) {
     if (n < 2) return;
-    DeviceArray<uint64_t> k2(n);
+    Scratch<uint64_t> k2(n, s);
     cub::DoubleBuffer<uint64_t> kb(keys, k2.get());
     size_t tb = 0;
     HYT_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, tb, kb, static_cast<int64_t>(n), 0, end_bit, s));
-    TempStorage tmp(tb);
-    HYT_CUDA(cub::DeviceRadixSort::SortKeys(tmp.ptr, tb, kb, static_cast<int64_t>(n), 0, end_bit, s));
+    Scratch<uint8_t> tmp(tb, s);
+    HYT_CUDA(cub::DeviceRadixSort::SortKeys(tmp.get(), tb, kb, static_cast<int64_t>(n), 0, end_bit, s));
     if (kb.Current() != keys)
         HYT_CUDA(cudaMemcpyAsync(keys, kb.Current(), n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
     HYT_CUDA(cudaStreamSynchronize(s));
@@ -85,8 +72,8 @@ void exclusive_scan_u64(const uint64_t *in, uint64_t *out, size_t n, cudaStream_
     if (n == 0) return;
     size_t tb = 0;
     HYT_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, in, out, static_cast<int64_t>(n), s));
-    TempStorage tmp(tb);
-    HYT_CUDA(cub::DeviceScan::ExclusiveSum(tmp.ptr, tb, in, out, static_cast<int64_t>(n), s));
+    Scratch<uint8_t> tmp(tb, s);
+    HYT_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), tb, in, out, static_cast<int64_t>(n), s));
     HYT_CUDA(cudaStreamSynchronize(s));
 }
 
@@ -94,19 +81,19 @@ void exclusive_scan_u32(const uint32_t *in, uint32_t *out, size_t n, cudaStream_
     if (n == 0) return;
     size_t tb = 0;
     HYT_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, in, out, static_cast<int64_t>(n), s));
-    TempStorage tmp(tb);
-    HYT_CUDA(cub::DeviceScan::ExclusiveSum(tmp.ptr, tb, in, out, static_cast<int64_t>(n), s));
+    Scratch<uint8_t> tmp(tb, s);
+    HYT_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), tb, in, out, static_cast<int64_t>(n), s));
     HYT_CUDA(cudaStreamSynchronize(s));
 }
 
 size_t select_flagged_u64(const uint64_t *in, const uint8_t *flags, uint64_t *out, size_t n,
                           cudaStream_t s) {
     if (n == 0) return 0;
-    DeviceArray<uint64_t> cnt(1);
+    Scratch<uint64_t> cnt(1, s);
     size_t tb = 0;
     HYT_CUDA(cub::DeviceSelect::Flagged(nullptr, tb, in, flags, out, cnt.get(), static_cast<int64_t>(n), s));
-    TempStorage tmp(tb);
-    HYT_CUDA(cub::DeviceSelect::Flagged(tmp.ptr, tb, in, flags, out, cnt.get(), static_cast<int64_t>(n), s));
+    Scratch<uint8_t> tmp(tb, s);
+    HYT_CUDA(cub::DeviceSelect::Flagged(tmp.get(), tb, in, flags, out, cnt.get(), static_cast<int64_t>(n), s));
     uint64_t h = 0;
     HYT_CUDA(cudaMemcpyAsync(&h, cnt.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
     HYT_CUDA(cudaStreamSynchronize(s));
@@ -115,12 +102,12 @@ size_t select_flagged_u64(const uint64_t *in, const uint8_t *flags, uint64_t *ou
 
 size_t select_flagged_index(const uint8_t *flags, uint32_t *out, size_t n, cudaStream_t s) {
     if (n == 0) return 0;
-    DeviceArray<uint64_t> cnt(1);
+    Scratch<uint64_t> cnt(1, s);
     thrust::counting_iterator<uint32_t> it(0);
     size_t tb = 0;
     HYT_CUDA(cub::DeviceSelect::Flagged(nullptr, tb, it, flags, out, cnt.get(), static_cast<int64_t>(n), s));
-    TempStorage tmp(tb);
-    HYT_CUDA(cub::DeviceSelect::Flagged(tmp.ptr, tb, it, flags, out, cnt.get(), static_cast<int64_t>(n), s));
+    Scratch<uint8_t> tmp(tb, s);
+    HYT_CUDA(cub::DeviceSelect::Flagged(tmp.get(), tb, it, flags, out, cnt.get(), static_cast<int64_t>(n), s));
     uint64_t h = 0;
     HYT_CUDA(cudaMemcpyAsync(&h, cnt.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
     HYT_CUDA(cudaStreamSynchronize(s));
@@ -130,11 +117,11 @@ size_t select_flagged_index(const uint8_t *flags, uint32_t *out, size_t n, cudaS
 template <class T>
 T reduce_max(const T *in, size_t n, cudaStream_t s) {
     if (n == 0) return 0;
-    DeviceArray<T> r(1);
+    Scratch<T> r(1, s);
     size_t tb = 0;
     HYT_CUDA(cub::DeviceReduce::Max(nullptr, tb, in, r.get(), static_cast<int64_t>(n), s));
-    TempStorage tmp(tb);
-    HYT_CUDA(cub::DeviceReduce::Max(tmp.ptr, tb, in, r.get(), static_cast<int64_t>(n), s));
+    Scratch<uint8_t> tmp(tb, s);
+    HYT_CUDA(cub::DeviceReduce::Max(tmp.get(), tb, in, r.get(), static_cast<int64_t>(n), s));
     T h = 0;
     HYT_CUDA(cudaMemcpyAsync(&h, r.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
     HYT_CUDA(cudaStreamSynchronize(s));

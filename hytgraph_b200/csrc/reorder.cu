@@ -33,6 +33,7 @@
 
 #include "common.cuh"
 #include "scratch.cuh"
+#include "solvers.cuh"
 
 namespace hyt {
 namespace {
@@ -488,7 +489,7 @@ void hub_sort(const hyt_csr &csr, double fraction, uint32_t *order_out, double *
 }
 
 void csr_reorder(const hyt_csr &csr, const uint32_t *vertex_order, bool on_device, hyt_csr_buffers *out,
-                 hyt_reorder_stats *stats) {
+                 hyt_reorder_stats *stats, bool pooled) {
     const uint64_t V = csr.num_vertices, E = csr.num_edges;
     if (stats) std::memset(stats, 0, sizeof(*stats));
     if (!out || (!vertex_order && V)) fail(HYT_E_INVALID, "NULL argument");
@@ -524,7 +525,12 @@ void csr_reorder(const hyt_csr &csr, const uint32_t *vertex_order, bool on_devic
     fail_on_csr_flags(h);
     auto alloc = [&](size_t bytes) -> void * {
         void *p = nullptr;
-        if (on_device) {
+        if (on_device && pooled) {
+            int dev = 0;
+            HYT_CUDA(cudaGetDevice(&dev));
+            HYT_CUDA(cudaMallocFromPoolAsync(&p, bytes ? bytes : 16, graph_pool(dev), cudaStreamLegacy));
+            HYT_CUDA(cudaStreamSynchronize(cudaStreamLegacy));
+        } else if (on_device) {
             HYT_CUDA(cudaMalloc(&p, bytes ? bytes : 16));
         } else {
             p = std::malloc(bytes ? bytes : 16);
@@ -534,11 +540,17 @@ void csr_reorder(const hyt_csr &csr, const uint32_t *vertex_order, bool on_devic
     };
     struct OutGuard {  // frees the outputs if a later step fails
         hyt_csr_buffers *o;
+        bool pooled;
         bool armed = true;
         ~OutGuard() {
-            if (armed) hyt_csr_buffers_free(o);
+            if (!armed) return;
+            if (pooled) {
+                free_pooled_buffers(o);
+            } else {
+                hyt_csr_buffers_free(o);
+            }
         }
-    } guard{out};
+    } guard{out, pooled && on_device};
     out->num_vertices = V;
     out->num_edges = E;
     out->on_device = on_device ? 1u : 0u;
@@ -593,6 +605,16 @@ void csr_reorder(const hyt_csr &csr, const uint32_t *vertex_order, bool on_devic
         stats->kernel_launches = E ? 3 : 1;
         stats->library_calls = 1;
     }
+}
+
+void free_pooled_buffers(hyt_csr_buffers *b) {
+    if (!b) return;
+    cudaDeviceSynchronize();
+    for (void *p : {static_cast<void *>(b->row_offsets), static_cast<void *>(b->column_indices),
+                    static_cast<void *>(b->weights)})
+        if (p) cudaFreeAsync(p, cudaStreamLegacy);
+    cudaStreamSynchronize(cudaStreamLegacy);
+    std::memset(b, 0, sizeof(*b));
 }
 
 }  // namespace hyt

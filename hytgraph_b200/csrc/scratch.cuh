@@ -12,8 +12,9 @@
 namespace hyt {
 
 // Scratch pool of the current device: stream-ordered allocations that keep
-// up to 2 GiB mapped between calls, so repeated calls do not pay for
-// mapping fresh memory (a scale-24 call needs about 0.8 GB of scratch).
+// up to 8 GiB mapped between calls, so repeated calls do not pay for
+// mapping fresh memory (building a scale-24 graph needs a few GB of
+// temporaries; hyt_trim_device_memory returns them).
 inline cudaMemPool_t scratch_pool() {
     static std::mutex mu;
     static std::unordered_map<int, cudaMemPool_t> pools;
@@ -28,7 +29,7 @@ inline cudaMemPool_t scratch_pool() {
     props.location.id = dev;
     cudaMemPool_t pool = nullptr;
     HYT_CUDA(cudaMemPoolCreate(&pool, &props));
-    uint64_t keep = uint64_t(2) << 30;
+    uint64_t keep = uint64_t(8) << 30;
     HYT_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
     pools[dev] = pool;
     return pool;
@@ -44,8 +45,10 @@ struct Scratch {
         HYT_CUDA(cudaMallocFromPoolAsync(&q, std::max<size_t>(n, 1) * sizeof(T) + 16, scratch_pool(), s));
         p = static_cast<T *>(q);
     }
-    ~Scratch() {
+    ~Scratch() { release(); }
+    void release() {
         if (p) cudaFreeAsync(p, s);
+        p = nullptr;
     }
     Scratch(const Scratch &) = delete;
     Scratch &operator=(const Scratch &) = delete;

@@ -16,8 +16,11 @@ void pick_sources(const uint64_t *row_offsets, uint64_t V, uint64_t seed, uint32
 // Hub sorting / vertex reordering (reorder.cu).
 void hub_sort(const hyt_csr &csr, double fraction, uint32_t *order_out, double *scores_out, uint64_t *hub_count,
               hyt_reorder_stats *stats);
+// pooled (with on_device): the outputs come from the graph pool and are
+// released with free_pooled_buffers, not hyt_csr_buffers_free.
 void csr_reorder(const hyt_csr &csr, const uint32_t *vertex_order, bool on_device, hyt_csr_buffers *out,
-                 hyt_reorder_stats *stats);
+                 hyt_reorder_stats *stats, bool pooled = false);
+void free_pooled_buffers(hyt_csr_buffers *b);
 void csr_from_edges(const uint32_t *src, const uint32_t *dst, const void *weights, uint32_t wkind, uint64_t E,
                     uint64_t V, bool on_device, hyt_csr_buffers *out, hyt_load_stats *stats);
 void load_edge_list(const char *path, uint64_t V, bool weighted, bool on_device, hyt_csr_buffers *out,
