@@ -206,25 +206,24 @@ __global__ void duplicates_kernel(const uint64_t *__restrict__ sorted, uint64_t 
 
 unsigned grid_sm(unsigned per_sm) { return static_cast<unsigned>(sm_count()) * per_sm; }
 
+// Stable radix sort of (key, value) pairs on key bits [0, bits).
 template <class K, class V>
-void sort_pairs(K *&keys, K *keys_alt, V *&vals, V *vals_alt, uint64_t n, bool descending, cudaStream_t s) {
+void sort_pairs(K *&keys, K *keys_alt, V *&vals, V *vals_alt, uint64_t n, bool descending, cudaStream_t s,
+                int bits = int(sizeof(K) * 8)) {
     if (n < 2) return;
     cub::DoubleBuffer<K> kb(keys, keys_alt);
     cub::DoubleBuffer<V> vb(vals, vals_alt);
     size_t tb = 0;
     if (descending) {
-        HYT_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, kb, vb, static_cast<int64_t>(n), 0,
-                                                           int(sizeof(K) * 8), s));
+        HYT_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, kb, vb, static_cast<int64_t>(n), 0, bits, s));
     } else {
-        HYT_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, kb, vb, static_cast<int64_t>(n), 0, int(sizeof(K) * 8), s));
+        HYT_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, kb, vb, static_cast<int64_t>(n), 0, bits, s));
     }
     Scratch<uint8_t> tmp(tb, s);
     if (descending) {
-        HYT_CUDA(cub::DeviceRadixSort::SortPairsDescending(tmp.get(), tb, kb, vb, static_cast<int64_t>(n), 0,
-                                                           int(sizeof(K) * 8), s));
+        HYT_CUDA(cub::DeviceRadixSort::SortPairsDescending(tmp.get(), tb, kb, vb, static_cast<int64_t>(n), 0, bits, s));
     } else {
-        HYT_CUDA(
-            cub::DeviceRadixSort::SortPairs(tmp.get(), tb, kb, vb, static_cast<int64_t>(n), 0, int(sizeof(K) * 8), s));
+        HYT_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), tb, kb, vb, static_cast<int64_t>(n), 0, bits, s));
     }
     keys = kb.Current();
     vals = vb.Current();
@@ -317,6 +316,19 @@ void contribution_schedule(const uint64_t *item, const double *contribution, uin
     HYT_CUDA(cudaMemsetAsync(counts.get(), 0, 32, s));
     schedule_prep_kernel<<<grid_for(n, 256, 148u * 8u), 256, 0, s>>>(c, n, eps, pos.get(), counts.get());
     HYT_CUDA(cudaGetLastError());
+    // item sorts run on the bits the largest item index needs
+    int item_bits = 1;
+    {
+        Scratch<uint64_t> mx(1, s);
+        size_t tb = 0;
+        HYT_CUDA(cub::DeviceReduce::Max(nullptr, tb, it, mx.get(), static_cast<int64_t>(n), s));
+        Scratch<uint8_t> tmp(tb, s);
+        HYT_CUDA(cub::DeviceReduce::Max(tmp.get(), tb, it, mx.get(), static_cast<int64_t>(n), s));
+        uint64_t h = 0;
+        HYT_CUDA(cudaMemcpyAsync(&h, mx.get(), 8, cudaMemcpyDeviceToHost, s));
+        HYT_CUDA(cudaStreamSynchronize(s));
+        item_bits = h ? 64 - __builtin_clzll(h) : 1;
+    }
     // redundant work: equal neighbours among the sorted item indices
     HYT_CUDA(cudaMemcpyAsync(key.get(), it, n * 8, cudaMemcpyDeviceToDevice, s));
     uint64_t *vp = pos.get();
@@ -325,9 +337,9 @@ void contribution_schedule(const uint64_t *item, const double *contribution, uin
         uint64_t *k_alt = key_alt.get();
         size_t tb = 0;
         cub::DoubleBuffer<uint64_t> kb(k, k_alt);
-        HYT_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, tb, kb, static_cast<int64_t>(n), 0, 64, s));
+        HYT_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, tb, kb, static_cast<int64_t>(n), 0, item_bits, s));
         Scratch<uint8_t> tmp(tb, s);
-        HYT_CUDA(cub::DeviceRadixSort::SortKeys(tmp.get(), tb, kb, static_cast<int64_t>(n), 0, 64, s));
+        HYT_CUDA(cub::DeviceRadixSort::SortKeys(tmp.get(), tb, kb, static_cast<int64_t>(n), 0, item_bits, s));
         duplicates_kernel<<<grid_for(n, 256, 148u * 8u), 256, 0, s>>>(kb.Current(), n, counts.get());
         HYT_CUDA(cudaGetLastError());
     }
@@ -336,7 +348,7 @@ void contribution_schedule(const uint64_t *item, const double *contribution, uin
     if (deterministic) {
         HYT_CUDA(cudaMemcpyAsync(key.get(), it, n * 8, cudaMemcpyDeviceToDevice, s));
         uint64_t *kp = key.get();
-        sort_pairs(kp, key_alt.get(), vp, pos_alt.get(), n, false, s);
+        sort_pairs(kp, key_alt.get(), vp, pos_alt.get(), n, false, s, item_bits);
     }
     uint64_t *ck = key.get(), *ck_alt = key_alt.get();
     uint64_t *vp_alt = vp == pos.get() ? pos_alt.get() : pos.get();
