@@ -237,3 +237,13 @@ def test_hub_ordered_graph_same_results(hyt, gpu, oracle):
             with pytest.raises(hyt.HytError) as e:
                 bt.run([{"graph": 0, "kind": "sssp", "source": s}])
             assert e.value.code == hyt.capi.HYT_E_UNSUPPORTED
+
+
+def test_trim_device_memory(hyt, gpu):
+    """Cached pool memory goes back to the driver; graphs still build after."""
+    g = hyt.rmat(12, 8, 3)
+    with hyt.Graph(g):
+        pass
+    hyt.capi.check(hyt.capi.lib.hyt_trim_device_memory(0))
+    with hyt.Graph(g) as a:
+        assert a.sssp(int(hyt.pick_sources(g.row_offsets, 1, 1)[0]))[0].shape == (g.num_vertices,)
