@@ -50,14 +50,16 @@ def parse_args():
     ap.add_argument("--seed", type=int, default=20241203)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["inhbm", "hybrid", "batch", "serve", "hubsort", "load", "contrib"],
+    ap.add_argument("--workload", choices=["inhbm", "hybrid", "batch", "serve", "hubsort", "load", "contrib",
+                                           "ppr8"],
                     default="inhbm",
                     help="inhbm: graph resident in HBM (default); hybrid: edges in pinned host memory under a "
                          "device budget (defaults to R-MAT scale 27, edge factor 32, 8 GiB); batch: 64 graphs of "
                          "scales 12-20, 512 SSSP/PPR queries in one CUDA-graph launch; serve: continuous "
                          "batching of a Poisson stream; hubsort: hub sorting + vertex reordering of the graph; load: "
                          "text edge list -> CSR in HBM (GraphLoader) and the binary CSR file; contrib: PageRank "
-                         "contributions + contribution schedule of every vertex + partition priorities")
+                         "contributions + contribution schedule of every vertex + partition priorities; ppr8: 8 personalized "
+                         "PageRank queries packed into one solve vs one at a time")
     ap.add_argument("--hub-fraction", type=float, default=0.08)
     ap.add_argument("--vertex-order", choices=["input", "hub"], default="hub",
                     help="inhbm: store the graph in hub order (HYT_GRAPH_HUB_ORDER); results stay in input ids")
@@ -1115,6 +1117,98 @@ def run_contrib_workload(args, rank, world, local, pg):
         print(json.dumps(line), flush=True)
 
 
+def run_ppr8_workload(args, rank, world, local, pg):
+    """One step = 8 personalized PageRank queries (restart 0.15, tol 1e-6)
+    from seeded sources, packed into one hyt_ppr_multi call; the same 8
+    queries through hyt_ppr one at a time are timed beside it."""
+    import torch
+
+    import hytgraph_b200 as hyt
+    from hytgraph_b200 import capi
+
+    peak_gbs, peak_kind = load_peaks()
+    d = hyt.rmat(args.scale, args.edge_factor, args.seed, device=True)
+    V, E = d.num_vertices, d.num_edges
+    off_np = np.empty(V + 1, np.uint64)
+    capi.copy(off_np.ctypes.data, C.cast(d.buffers.row_offsets, C.c_void_p).value, off_np.nbytes)
+    gflags = capi.HYT_GRAPH_ALL | (capi.HYT_GRAPH_HUB_ORDER if args.vertex_order == "hub" else 0)
+    g = hyt.Graph(d, flags=gflags)
+    d.free()
+    out = torch.empty((8, V), dtype=torch.float32, device="cuda")
+    one = torch.empty(V, dtype=torch.float32, device="cuda")
+    step_no = [0]
+
+    def sources():
+        step_no[0] += 1
+        return np.array(hyt.pick_sources(off_np, args.seed + step_no[0], 8), np.uint32)
+
+    def step(collect):
+        _, st = g.ppr_multi(sources(), out=out)
+        collect.append(st)
+
+    warm = []
+    for _ in range(args.warmup):
+        step(warm)
+    clocks = ClockSampler(local)
+    clocks.start()
+    timed = []
+    barrier(pg)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step(timed)
+    barrier(pg)
+    ms = max_over_ranks(pg, 1e3 * (time.perf_counter() - t0))
+    clk = clocks.stop()
+    value = replica_value(8 * args.steps, world, ms)
+    # one at a time: the same kind of queries through hyt_ppr
+    g.ppr(int(sources()[0]), out=one)
+    t1 = time.perf_counter()
+    singles = []
+    for s in sources():
+        _, st = g.ppr(int(s), out=one)
+        singles.append(st)
+    single_ms = 1e3 * (time.perf_counter() - t1)
+    dev_ms = sum(x[0]["device_ms"] for x in timed) / args.steps
+    iters = sum(max(y["iterations"] for y in x) for x in timed) / args.steps
+    kb = timed[0][0]["algorithmic_bytes"] / max(max(y["iterations"] for y in timed[0]), 1)
+    it_ms = dev_ms / max(iters, 1)
+    roof = {"kernel": "ppr8 iteration (prep + rows + long rows)", "bound": "hbm",
+            "achieved": kb / (it_ms / 1e3) / 1e9, "peak": peak_gbs, "unit": "GB/s",
+            "frac": kb / (it_ms / 1e3) / 1e9 / peak_gbs, "traffic": None, "peak_kind": peak_kind,
+            "algorithmic_bytes_per_launch": kb, "avg_launch_ms": it_ms,
+            "note": "per iteration of the packed solve: 36 B per in-edge (id + a 32-byte sector of the 8 "
+                    "queries' contributions) + 108 B per vertex"}
+    g.close()
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle.bindings import Oracle
+
+        host = hyt.rmat(min(args.scale, 20), args.edge_factor, args.seed)
+        src = int(hyt.pick_sources(host.row_offsets, args.seed, 1)[0])
+        tt = time.perf_counter()
+        Oracle().ppr_f64(host.row_offsets, host.column_indices, src, 0.15, 1e-6, 100)
+        tc = time.perf_counter() - tt
+        cpu = {"value": 1.0 / tc * (host.num_edges / E), "unit": "queries/s (scaled to this graph's edges)",
+               "cores": 1, "kind": "port",
+               "sample": f"one FP64 personalized PageRank (the oracle's restatement; the reference has no PPR) on "
+                         f"R-MAT scale {min(args.scale, 20)}, {tc:.1f} s, scaled by the edge ratio"}
+    if rank == 0:
+        line = {"metric": "personalized PageRank queries/s (8 packed per solve)", "value": value,
+                "unit": "queries/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32 values, f64 sums", "data": "synthetic",
+                "config": {"workload": f"8 PPR queries (restart 0.15, tol 1e-6) per step on R-MAT scale {args.scale} "
+                                       f"edge factor {args.edge_factor}, sources seeded per step",
+                           "vertices": V, "edges": E, "vertex_order": args.vertex_order, "seed": args.seed,
+                           "parallelism": f"replicas x{args.gpus}"},
+                "one_at_a_time": {"queries_per_s": 8 / (single_ms / 1e3), "ms_per_query": single_ms / 8,
+                                  "iterations": [s_["iterations"] for s_ in singles]},
+                "speedup_vs_one_at_a_time": value / (8 / (single_ms / 1e3)),
+                "packed": {"device_ms_per_solve": dev_ms, "iterations_per_solve": iters},
+                "roofline": roof, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": None}
+        print(json.dumps(line), flush=True)
+
+
 def workload_config(args, V, E):
     return {"workload": f"in-HBM R-MAT scale {args.scale} edge factor {args.edge_factor}: PageRank to L1<=1e-6 "
                         f"+ SSSP from {args.sources} seeded sources",
@@ -1149,6 +1243,11 @@ def main():
         return
     if args.workload == "batch":
         run_batch_workload(args, rank, world, pg)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
+    if args.workload == "ppr8":
+        run_ppr8_workload(args, rank, world, local, pg)
         if pg is not None:
             pg.destroy_process_group()
         return

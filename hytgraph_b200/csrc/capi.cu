@@ -234,6 +234,15 @@ int hyt_pagerank(hyt_graph *graph, const hyt_pagerank_params *params, float *ran
     });
 }
 
+int hyt_ppr_multi(hyt_graph *graph, const uint32_t *sources, uint32_t num_sources, float restart, float tolerance,
+                  uint32_t max_iterations, float *ranks_out, hyt_run_stats *stats) {
+    return guarded([&] {
+        GraphImpl &g = impl(graph);
+        use_device(g);
+        ppr_multi(g, sources, num_sources, restart, tolerance, max_iterations, ranks_out, stats);
+    });
+}
+
 int hyt_ppr(hyt_graph *graph, const hyt_ppr_params *params, float *ranks_out, hyt_run_stats *stats) {
     return guarded([&] {
         if (!params) fail(HYT_E_INVALID, "params is NULL");

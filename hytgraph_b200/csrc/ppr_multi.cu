@@ -1,0 +1,313 @@
+// Packed personalized PageRank: up to 8 queries on one graph share every
+// pass over the CSC (hyt_ppr_multi).
+//
+// Each query keeps the single-source definition (hyt_ppr; the oracle's
+// personalized PageRank):
+//   x' = d * sum_{u->v} x_u / deg(u) + [v == s] * ((1 - d) + d * dangling),
+//   d = 1 - restart, x_0 = e_s, stop after the step whose L1 change is
+//   <= tolerance.
+// The 8 lanes of a vertex are stored together (32 bytes), so one in-edge
+// costs one source id and one 32-byte sector of contributions for all 8
+// queries, instead of 8 id reads and 8 scattered gathers.  A warp takes a
+// row 4 in-edges at a time (thread t: edge t / 8, lane t % 8), sums in FP64
+// and folds the 4 edge slots with shuffles; rows at or above the graph's
+// long-row threshold use its 4096-edge chunk tasks, summed per row in chunk
+// order.  The thread layout does not depend on how many lanes are in use,
+// so a query's result is the same bit for bit alone or packed with others.
+// A lane whose step met its tolerance stops (its values are carried
+// unchanged) while the others continue.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+#include "graph.cuh"
+#include "scratch.cuh"
+#include "solvers.cuh"
+
+namespace hyt {
+namespace {
+
+constexpr int kLanes = 8;
+constexpr int kPartBlocks = 512;
+
+// c[u][l] = x[u][l] / deg(u) (0 when dangling); per-block partial sums of
+// the dangling values, per lane.
+__global__ void ppr8_prep_kernel(const uint32_t *__restrict__ deg, const float *__restrict__ x, uint64_t V,
+                                 float *__restrict__ c, double *__restrict__ dpart) {
+    __shared__ double s_part[kLanes][8];
+    double acc[kLanes] = {};
+    for (uint64_t u = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; u < V; u += uint64_t(gridDim.x) * blockDim.x) {
+        const uint32_t d = deg[u];
+        const float4 a = reinterpret_cast<const float4 *>(x)[2 * u];
+        const float4 b = reinterpret_cast<const float4 *>(x)[2 * u + 1];
+        const float v[kLanes] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+        float o[kLanes];
+#pragma unroll
+        for (int l = 0; l < kLanes; ++l) {
+            o[l] = d ? __fdiv_rn(v[l], float(d)) : 0.0f;
+            if (!d) acc[l] += v[l];
+        }
+        reinterpret_cast<float4 *>(c)[2 * u] = make_float4(o[0], o[1], o[2], o[3]);
+        reinterpret_cast<float4 *>(c)[2 * u + 1] = make_float4(o[4], o[5], o[6], o[7]);
+    }
+    const int warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int l = 0; l < kLanes; ++l) {
+        double a = acc[l];
+#pragma unroll
+        for (int sh = 16; sh > 0; sh >>= 1) a += __shfl_xor_sync(0xffffffffu, a, sh);
+        if ((threadIdx.x & 31) == 0) s_part[l][warp] = a;
+    }
+    __syncthreads();
+    if (threadIdx.x < kLanes) {
+        double a = 0.0;
+        for (int w = 0; w < 8; ++w) a += s_part[threadIdx.x][w];
+        dpart[blockIdx.x * kLanes + threadIdx.x] = a;
+    }
+}
+
+// Sum over in-edges [b, e) of c[u][lane]: thread t takes edge slot t / 8 and
+// lane t % 8; the result is complete in every thread of the lane.
+__device__ __forceinline__ double row_lane_sum(const uint32_t *__restrict__ in_src,
+                                               const uint32_t *__restrict__ hot_vertex, const float *__restrict__ c,
+                                               uint64_t b, uint64_t e, int t) {
+    const int slot = t >> 3, lane = t & 7;
+    double acc = 0.0;
+    for (uint64_t i = b + slot; i < e; i += 4) {
+        uint32_t u = in_src[i];
+        if (u & kHotTag) u = hot_vertex[u & ~kHotTag];
+        acc += double(c[uint64_t(u) * kLanes + lane]);
+    }
+    acc += __shfl_xor_sync(0xffffffffu, acc, 8);
+    acc += __shfl_xor_sync(0xffffffffu, acc, 16);
+    return acc;
+}
+
+struct LaneParams {
+    uint32_t source[kLanes];   // internal ids; lanes >= k unused
+    uint32_t active;           // bit l: lane l still iterates
+    double d;                  // damping
+};
+
+// Per-lane dangling mass from the prep partials (fixed order).
+__device__ __forceinline__ void lane_dangling(const double *__restrict__ dpart, double *s_dm) {
+    if (threadIdx.x < kLanes) {
+        double a = 0.0;
+        for (int i = 0; i < kPartBlocks; ++i) a += dpart[i * kLanes + threadIdx.x];
+        s_dm[threadIdx.x] = a;
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ float lane_next(uint64_t v, int lane, double sum, const LaneParams &p, const double *s_dm,
+                                           float cur) {
+    if (!((p.active >> lane) & 1u)) return cur;
+    double nx = p.d * sum;
+    if (v == p.source[lane]) nx += (1.0 - p.d) + p.d * s_dm[lane];
+    return float(nx);
+}
+
+// One warp per short row: next values and per-block residual partials.
+__global__ void ppr8_rows_kernel(const uint64_t *__restrict__ in_off, const uint32_t *__restrict__ in_src,
+                                 const uint32_t *__restrict__ hot_vertex, const float *__restrict__ c,
+                                 const float *__restrict__ x, uint64_t V, uint64_t long_from, LaneParams p,
+                                 const double *__restrict__ dpart, float *__restrict__ nxt, double *__restrict__ rpart) {
+    __shared__ double s_dm[kLanes];
+    __shared__ double s_res[kLanes][8];
+    lane_dangling(dpart, s_dm);
+    const int t = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t warps = uint64_t(gridDim.x) * (blockDim.x >> 5);
+    double res = 0.0;  // lane t (t < 8)
+    for (uint64_t v = (blockIdx.x * uint64_t(blockDim.x) + threadIdx.x) >> 5; v < V; v += warps) {
+        const uint64_t b = in_off[v], e = in_off[v + 1];
+        if (e - b >= long_from) continue;  // summed by the chunk kernels
+        const double sum = row_lane_sum(in_src, hot_vertex, c, b, e, t);
+        if (t < kLanes) {
+            const float cur = x[v * kLanes + t];
+            const float nx = lane_next(v, t, sum, p, s_dm, cur);
+            nxt[v * kLanes + t] = nx;
+            res += fabs(double(nx) - double(cur));
+        }
+    }
+    if (t < kLanes) s_res[t][warp] = res;
+    __syncthreads();
+    if (threadIdx.x < kLanes) {
+        double a = 0.0;
+        for (int w = 0; w < 8; ++w) a += s_res[threadIdx.x][w];
+        rpart[blockIdx.x * kLanes + threadIdx.x] = a;
+    }
+}
+
+// One warp per chunk of a long row: per-lane partial sums.
+__global__ void ppr8_chunks_kernel(const uint64_t *__restrict__ in_off, const uint32_t *__restrict__ in_src,
+                                   const uint32_t *__restrict__ hot_vertex, const float *__restrict__ c,
+                                   const LongRow *__restrict__ long_rows, const uint2 *__restrict__ tasks,
+                                   uint64_t num_tasks, double *__restrict__ chunk_sum) {
+    const int t = threadIdx.x & 31;
+    const uint64_t warps = uint64_t(gridDim.x) * (blockDim.x >> 5);
+    for (uint64_t k = (blockIdx.x * uint64_t(blockDim.x) + threadIdx.x) >> 5; k < num_tasks; k += warps) {
+        const uint2 task = tasks[k];
+        const LongRow lr = long_rows[task.x];
+        const uint64_t b = in_off[lr.row] + uint64_t(task.y) * kLongChunk;
+        const uint64_t e = min(b + kLongChunk, in_off[lr.row + 1]);
+        const double sum = row_lane_sum(in_src, hot_vertex, c, b, e, t);
+        if (t < kLanes) chunk_sum[(uint64_t(lr.first_chunk) + task.y) * kLanes + t] = sum;
+    }
+}
+
+// One warp per long row: chunk partials in order, next values, residual.
+__global__ void ppr8_long_rows_kernel(const LongRow *__restrict__ long_rows, uint64_t num_long,
+                                      const double *__restrict__ chunk_sum, const float *__restrict__ x, LaneParams p,
+                                      const double *__restrict__ dpart, float *__restrict__ nxt,
+                                      double *__restrict__ rpart) {
+    __shared__ double s_dm[kLanes];
+    __shared__ double s_res[kLanes][8];
+    lane_dangling(dpart, s_dm);
+    const int t = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t warps = uint64_t(gridDim.x) * (blockDim.x >> 5);
+    double res = 0.0;
+    for (uint64_t i = (blockIdx.x * uint64_t(blockDim.x) + threadIdx.x) >> 5; i < num_long; i += warps) {
+        const LongRow lr = long_rows[i];
+        if (t < kLanes) {
+            double sum = 0.0;
+            for (uint32_t k = 0; k < lr.num_chunks; ++k) sum += chunk_sum[(uint64_t(lr.first_chunk) + k) * kLanes + t];
+            const uint64_t v = lr.row;
+            const float cur = x[v * kLanes + t];
+            const float nx = lane_next(v, t, sum, p, s_dm, cur);
+            nxt[v * kLanes + t] = nx;
+            res += fabs(double(nx) - double(cur));
+        }
+    }
+    if (t < kLanes) s_res[t][warp] = res;
+    __syncthreads();
+    if (threadIdx.x < kLanes) {
+        double a = 0.0;
+        for (int w = 0; w < 8; ++w) a += s_res[threadIdx.x][w];
+        rpart[blockIdx.x * kLanes + threadIdx.x] = a;
+    }
+}
+
+// residual[l] = rows partials then long-row partials, each in block order.
+__global__ void ppr8_residual_kernel(const double *__restrict__ rows, int nrows, const double *__restrict__ longs,
+                                     int nlong, double *__restrict__ residual) {
+    if (threadIdx.x < kLanes) {
+        double a = 0.0;
+        for (int i = 0; i < nrows; ++i) a += rows[i * kLanes + threadIdx.x];
+        for (int i = 0; i < nlong; ++i) a += longs[i * kLanes + threadIdx.x];
+        residual[threadIdx.x] = a;
+    }
+}
+
+__global__ void ppr8_init_kernel(float *__restrict__ x, uint64_t V, LaneParams p, int k) {
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < V * kLanes;
+         i += uint64_t(gridDim.x) * blockDim.x) {
+        const int lane = int(i & 7);
+        const uint64_t v = i >> 3;
+        x[i] = (lane < k && v == p.source[lane]) ? 1.0f : 0.0f;
+    }
+}
+
+__global__ void ppr8_lane_kernel(const float *__restrict__ x, uint64_t V, int lane, float *__restrict__ out) {
+    for (uint64_t v = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; v < V; v += uint64_t(gridDim.x) * blockDim.x)
+        out[v] = x[v * kLanes + lane];
+}
+
+unsigned grid_sm(unsigned per_sm) { return static_cast<unsigned>(sm_count()) * per_sm; }
+
+}  // namespace
+
+void ppr_multi(GraphImpl &g, const uint32_t *sources, uint32_t k, float restart, float tolerance, uint32_t max_iter,
+               float *out, hyt_run_stats *stats) {
+    if (!(g.flags & HYT_GRAPH_PULL)) fail(HYT_E_INVALID, "graph was created without HYT_GRAPH_PULL");
+    if (k == 0 || k > kLanes) fail(HYT_E_INVALID, "hyt_ppr_multi takes 1 to 8 sources");
+    if (!sources) fail(HYT_E_INVALID, "sources is NULL");
+    if (!(restart > 0.0f && restart <= 1.0f)) fail(HYT_E_INVALID, "personalized PageRank restart must be in (0, 1]");
+    if (!(tolerance > 0.0f) || !std::isfinite(tolerance))
+        fail(HYT_E_INVALID, "personalized PageRank tolerance must be finite and positive");
+    if (max_iter == 0) fail(HYT_E_INVALID, "personalized PageRank max_iterations must be greater than zero");
+    const uint64_t V = g.V;
+    for (uint32_t l = 0; l < k; ++l)
+        if (sources[l] >= V) fail(HYT_E_INVALID, "personalized PageRank source vertex is out of range");
+    if (stats) std::memset(stats, 0, sizeof(hyt_run_stats) * k);
+    HYT_CUDA(cudaSetDevice(g.device));
+    cudaStream_t s = g.stream;
+    LaneParams p{};
+    for (uint32_t l = 0; l < kLanes; ++l) p.source[l] = l < k ? graph_vertex(g, sources[l], s) : 0xFFFFFFFFu;
+    p.active = (1u << k) - 1u;
+    p.d = 1.0 - double(restart);
+    const unsigned rows_grid = grid_sm(8);
+    const uint64_t chunks = g.num_long ? g.num_chunks : 0;
+    const uint64_t long_from = g.num_long ? g.tile_cost : ~uint64_t(0);
+    const unsigned long_grid = g.num_long ? grid_for(g.num_long * 32, 256) : 0;
+    Scratch<float> xa(V * kLanes, s), xb(V * kLanes, s), c(V * kLanes, s);
+    Scratch<double> dpart(uint64_t(kPartBlocks) * kLanes, s), rpart(uint64_t(rows_grid) * kLanes, s),
+        lpart(uint64_t(std::max(long_grid, 1u)) * kLanes, s), chunk_sum(std::max<uint64_t>(chunks, 1) * kLanes, s),
+        residual(kLanes, s);
+    double *h_res = reinterpret_cast<double *>(g.host_scratch.ptr);  // 64 pinned bytes
+    float *x = xa.get(), *nx = xb.get();
+    ppr8_init_kernel<<<grid_sm(8), 256, 0, s>>>(x, V, p, int(k));
+    HYT_CUDA(cudaGetLastError());
+    std::vector<uint32_t> iters(k, 0);
+    std::vector<double> last(k, 0.0);
+    EventTimer timer;
+    timer.start(s);
+    uint64_t launches = 1;
+    for (uint32_t it = 0; it < max_iter && p.active; ++it) {
+        ppr8_prep_kernel<<<kPartBlocks, 256, 0, s>>>(g.out_degree.get(), x, V, c.get(), dpart.get());
+        ppr8_rows_kernel<<<rows_grid, 256, 0, s>>>(g.in_offsets.get(), g.in_sources.get(), g.hot_vertex.get(),
+                                                   c.get(), x, V, long_from, p, dpart.get(), nx, rpart.get());
+        launches += 2;
+        if (chunks) {
+            ppr8_chunks_kernel<<<grid_sm(8), 256, 0, s>>>(g.in_offsets.get(), g.in_sources.get(), g.hot_vertex.get(),
+                                                          c.get(), g.long_rows.get(), g.chunk_tasks.get(), chunks,
+                                                          chunk_sum.get());
+            ppr8_long_rows_kernel<<<long_grid, 256, 0, s>>>(g.long_rows.get(), g.num_long, chunk_sum.get(), x, p,
+                                                            dpart.get(), nx, lpart.get());
+            launches += 2;
+        }
+        ppr8_residual_kernel<<<1, 32, 0, s>>>(rpart.get(), int(rows_grid), lpart.get(), int(chunks ? long_grid : 0),
+                                              residual.get());
+        ++launches;
+        HYT_CUDA(cudaGetLastError());
+        HYT_CUDA(cudaMemcpyAsync(h_res, residual.get(), kLanes * 8, cudaMemcpyDeviceToHost, s));
+        HYT_CUDA(cudaStreamSynchronize(s));
+        std::swap(x, nx);
+        for (uint32_t l = 0; l < k; ++l) {
+            if (!((p.active >> l) & 1u)) continue;
+            iters[l] = it + 1;
+            last[l] = h_res[l];
+            if (h_res[l] <= double(tolerance)) p.active &= ~(1u << l);
+        }
+    }
+    timer.stop(s);
+    const double ms = timer.ms();
+    if (out) {
+        Scratch<float> lane(V, s);
+        for (uint32_t l = 0; l < k; ++l) {
+            ppr8_lane_kernel<<<grid_for(V, 256), 256, 0, s>>>(x, V, int(l), lane.get());
+            HYT_CUDA(cudaGetLastError());
+            graph_emit(g, out + uint64_t(l) * V, lane.get(), s);
+        }
+    }
+    HYT_CUDA(cudaStreamSynchronize(s));
+    if (stats) {
+        for (uint32_t l = 0; l < k; ++l) {
+            stats[l].iterations = iters[l];
+            stats[l].converged = ((p.active >> l) & 1u) ? 0u : 1u;
+            stats[l].residual = last[l];
+            stats[l].device_ms = ms;
+            stats[l].total_launches = static_cast<uint32_t>(launches);
+            stats[l].edges_processed = g.E * iters[l];
+            stats[l].vertices_processed = V * iters[l];
+        }
+        // one pass for all lanes: source id + one 32-byte contribution sector
+        // per in-edge; per vertex: offsets, the 8 lanes read and written,
+        // contributions written
+        const uint64_t iterations = *std::max_element(iters.begin(), iters.end());
+        stats[0].algorithmic_bytes = iterations * (36 * g.E + (8 + 32 + 32 + 32 + 4) * V);
+    }
+}
+
+}  // namespace hyt

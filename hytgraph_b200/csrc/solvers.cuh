@@ -7,6 +7,8 @@ namespace hyt {
 
 void pagerank_run(GraphImpl &g, const hyt_pagerank_params &p, float *ranks_out, hyt_run_stats *stats);
 void ppr_run(GraphImpl &g, const hyt_ppr_params &p, float *ranks_out, hyt_run_stats *stats);
+void ppr_multi(GraphImpl &g, const uint32_t *sources, uint32_t k, float restart, float tolerance, uint32_t max_iter,
+               float *out, hyt_run_stats *stats);
 void sssp_run(GraphImpl &g, const hyt_sssp_params &p, uint32_t *dist_out, hyt_run_stats *stats);
 void sssp_noalloc(const hyt_csr &csr, uint32_t source, uint32_t *dist_out, void *stream, hyt_run_stats *stats);
 

@@ -169,6 +169,17 @@ typedef struct hyt_run_stats {
 int hyt_pagerank(hyt_graph *graph, const hyt_pagerank_params *params,
                  float *ranks_out, hyt_run_stats *stats);
 
+/* Personalized PageRank from 1 to 8 sources at once (no reference
+ * counterpart): each query as hyt_ppr defines it, all of them sharing every
+ * pass over the CSC (one source id and one 32-byte sector of the 8 queries'
+ * contributions per in-edge).  A query's result does not depend on which
+ * other queries share the call; each stops after its own converging step.
+ * ranks_out: [num_sources][V] floats (host or device) or NULL; stats:
+ * num_sources entries or NULL (stats[0].algorithmic_bytes covers the call).
+ * Defined in the same terms as hyt_ppr below. */
+int hyt_ppr_multi(hyt_graph *graph, const uint32_t *sources, uint32_t num_sources, float restart, float tolerance,
+                  uint32_t max_iterations, float *ranks_out, hyt_run_stats *stats);
+
 /* Personalized PageRank from one source (no reference counterpart):
  *   x' = d * sum_{u->v} x_u / deg(u) + [v == s] * ((1 - d) + d * dangling)
  * with d = 1 - restart, x_0 = e_s, stop when the L1 change <= tolerance. */
