@@ -426,11 +426,12 @@ def run_batch_workload(args, rank, world, pg):
 
     specs, counts, rng = batch_workload(hyt, args.graphs, args.queries, args.seed)
     graphs, queries = [], []
+    gflags = capi.HYT_GRAPH_ALL | (capi.HYT_GRAPH_HUB_ORDER if args.vertex_order == "hub" else 0)
     for gi, (sc, ef, gseed) in enumerate(specs):
         d = hyt.rmat(sc, ef, gseed, device=True)
         off = np.empty(d.num_vertices + 1, np.uint64)
         capi.copy(off.ctypes.data, C.cast(d.buffers.row_offsets, C.c_void_p).value, off.nbytes)
-        graphs.append(hyt.Graph(d))
+        graphs.append(hyt.Graph(d, flags=gflags))
         d.free()
         for s in hyt.pick_sources(off, gseed, int(counts[gi])):
             kind = "sssp" if rng.random() < 0.6 else "ppr"
@@ -512,6 +513,7 @@ def run_batch_workload(args, rank, world, pg):
                              "frac": st["algorithmic_bytes"] / (ms / 1e3) / 1e9 / load_peaks()[0],
                              "traffic": None, "peak_kind": load_peaks()[1]},
                 "cpu_baseline": cpu, "clocks": clk, "gpu_launches": st["kernel_launches"]}
+        line["config"]["vertex_order"] = args.vertex_order
         print(json.dumps(line), flush=True)
     for g in graphs:
         g.close()
@@ -570,11 +572,12 @@ def run_serve_workload(args, rank, world, pg):
 
     scales = [16, 17, 18, 19, 20, 22, 23, 24]
     graphs, pools = [], []
+    gflags = capi.HYT_GRAPH_ALL | (capi.HYT_GRAPH_HUB_ORDER if args.vertex_order == "hub" else 0)
     for sc in scales:
         d = hyt.rmat(sc, 16, args.seed + sc, device=True)
         off = np.empty(d.num_vertices + 1, np.uint64)
         capi.copy(off.ctypes.data, C.cast(d.buffers.row_offsets, C.c_void_p).value, off.nbytes)
-        graphs.append(hyt.Graph(d))
+        graphs.append(hyt.Graph(d, flags=gflags))
         d.free()
         pools.append(hyt.pick_sources(off, args.seed + 7 * sc, 4096))
     V_of = [g.num_vertices for g in graphs]
@@ -675,6 +678,7 @@ def run_serve_workload(args, rank, world, pg):
                                   "p50_ms": float(np.percentile(lat1, 50)), "p99_ms": float(np.percentile(lat1, 99))},
                 "speedup_vs_one_at_a_time": cap_qps / single_qps,
                 "server": server_stats, "clocks": clk, "gpu_launches": server_stats.get("graph_launches")}
+        line["config"]["vertex_order"] = args.vertex_order
         print(json.dumps(line), flush=True)
 
 

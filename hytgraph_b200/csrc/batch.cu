@@ -548,7 +548,6 @@ void QueryEngine::grow(uint32_t cap) {
 void QueryEngine::validate(const hyt_query &q) const {
     if (q.graph >= graphs_.size()) fail(HYT_E_INVALID, "query graph index is out of range");
     const GraphImpl &g = *graphs_[q.graph];
-    graph_require_caller_order(g, "the batch engine");
     if (q.kind == HYT_QUERY_SSSP) {
         if (!(g.flags & HYT_GRAPH_PUSH)) fail(HYT_E_INVALID, "SSSP queries need graphs built with HYT_GRAPH_PUSH");
         if (q.source >= g.V) fail(HYT_E_INVALID, "SSSP source vertex is out of range");
@@ -625,7 +624,7 @@ int QueryEngine::admit(const hyt_query &q, uint64_t tag) {
             a.far[i] = reinterpret_cast<uint32_t *>(take(V * 4 + 16));
         }
         a.V = static_cast<uint32_t>(V);
-        a.source = q.source;
+        a.source = graph_vertex(g, q.source, stream_);  // internal id on hub-ordered graphs
         a.inf = (g.weight_kind == HYT_WEIGHTS_F32) ? 0x7F800000u : HYT_DIST_INF_U32;
         h.ss[s] = a;
         sl.kind = kSSSP;
@@ -673,7 +672,7 @@ int QueryEngine::admit(const hyt_query &q, uint64_t tag) {
         a.base = 0.0f;
         a.tolerance = q.tolerance > 0.0f ? q.tolerance : 1e-6f;
         a.max_iter = it;
-        a.source = q.source;
+        a.source = graph_vertex(g, q.source, stream_);
         a.personalized = 1;
         a.use_cond = 0;
         h.pr[s] = a;
@@ -932,7 +931,11 @@ void QueryEngine::retire(int s, hyt_query_result *res) {
     if (sh.q.out) {
         const void *src = sh.q.kind == HYT_QUERY_SSSP ? static_cast<const void *>(h.ss[s].dist)
                                                       : static_cast<const void *>(h.pr[s].rank[st.iterations & 1]);
-        HYT_CUDA(cudaMemcpyAsync(sh.q.out, src, g.V * 4, cudaMemcpyDefault, stream_));
+        if (g.inv.get()) {
+            graph_emit(g, sh.q.out, src, stream_);  // back to the caller's ids
+        } else {
+            HYT_CUDA(cudaMemcpyAsync(sh.q.out, src, g.V * 4, cudaMemcpyDefault, stream_));
+        }
     }
     if (res) {
         res->iterations = st.iterations;

@@ -97,9 +97,9 @@ enum hyt_graph_flags {
      * hub score Do*Di (HubSorter with hub_fraction 1, hyt_hub_sort), so the
      * high-degree vertices' values share cache lines.  Sources and results
      * stay in the caller's vertex ids (mapped on the way in and out).
-     * hyt_pagerank, hyt_ppr and hyt_sssp only: hyt_graph_copy_csc,
-     * hyt_pagerank_contributions and the batch / server engines reject such
-     * graphs (HYT_E_UNSUPPORTED). */
+     * hyt_pagerank, hyt_ppr, hyt_ppr_multi, hyt_sssp and the batch / server
+     * engines map ids; hyt_graph_copy_csc and hyt_pagerank_contributions
+     * reject such graphs (HYT_E_UNSUPPORTED). */
     HYT_GRAPH_HUB_ORDER = 4u
 };
 

@@ -203,8 +203,9 @@ def _dev_csr(hyt, g, t_off, t_cols, t_w):
 
 def test_hub_ordered_graph_same_results(hyt, gpu, oracle):
     """HYT_GRAPH_HUB_ORDER renumbers vertices internally by hub score; every
-    source and result stays in the caller's ids: SSSP distances identical,
-    PageRank / PPR within the FP64 tolerance, unsupported paths rejected."""
+    source and result stays in the caller's ids (single solves and the batch
+    engine): SSSP distances identical, PageRank / PPR within the FP64
+    tolerance, paths exposing internal ids rejected."""
     g = hyt.rmat(14, 16, 77)
     srcs = hyt.pick_sources(g.row_offsets, 5, 4)
     gf = hyt.CSR(g.row_offsets, g.column_indices, g.weights.astype(np.float32) / 2)
@@ -233,10 +234,15 @@ def test_hub_ordered_graph_same_results(hyt, gpu, oracle):
         with pytest.raises(hyt.HytError) as e:
             b.pagerank_contributions(r)
         assert e.value.code == hyt.capi.HYT_E_UNSUPPORTED
-        with hyt.Batch([b]) as bt:
-            with pytest.raises(hyt.HytError) as e:
-                bt.run([{"graph": 0, "kind": "sssp", "source": s}])
-            assert e.value.code == hyt.capi.HYT_E_UNSUPPORTED
+        # the batch engine maps ids too: same distances, PPR within tolerance
+        with hyt.Graph(g) as a, hyt.Batch([b, a]) as bt:
+            outs, res, _ = bt.run([{"graph": 0, "kind": "sssp", "source": s},
+                                   {"graph": 1, "kind": "sssp", "source": s},
+                                   {"graph": 0, "kind": "ppr", "source": s},
+                                   {"graph": 1, "kind": "ppr", "source": s}])
+            assert np.array_equal(outs[0], outs[1])
+            assert np.array_equal(outs[0], a.sssp(s)[0])
+            assert np.abs(outs[2].astype(np.float64) - outs[3]).sum() <= 2e-5
 
 
 def test_trim_device_memory(hyt, gpu):
