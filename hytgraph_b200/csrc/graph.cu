@@ -238,16 +238,14 @@ void graph_create(GraphImpl &g, const hyt_csr &csr, uint32_t flags) {
     g.inv.allocate(V);
     invert_kernel<<<grid_for(V, 256), 256, 0, g.stream>>>(perm.get(), V, g.inv.get());
     HYT_CUDA(cudaGetLastError());
+    g.h_inv.resize(V);
+    HYT_CUDA(cudaMemcpyAsync(g.h_inv.data(), g.inv.get(), V * 4, cudaMemcpyDeviceToHost, g.stream));
     HYT_CUDA(cudaStreamSynchronize(g.stream));
     g.perm = std::move(perm);
 }
 
-uint32_t graph_vertex(const GraphImpl &g, uint32_t v, cudaStream_t s) {
-    if (!g.inv.get()) return v;
-    uint32_t n = 0;
-    HYT_CUDA(cudaMemcpyAsync(&n, g.inv.get() + v, 4, cudaMemcpyDeviceToHost, s));
-    HYT_CUDA(cudaStreamSynchronize(s));
-    return n;
+uint32_t graph_vertex(const GraphImpl &g, uint32_t v, cudaStream_t) {
+    return g.h_inv.empty() ? v : g.h_inv[v];
 }
 
 void graph_emit(const GraphImpl &g, void *dst, const void *src, cudaStream_t s) {

@@ -59,6 +59,7 @@ struct GraphImpl {
     // HYT_GRAPH_HUB_ORDER: perm[new] = caller id, inv[caller id] = new
     // (empty otherwise)
     GraphArray<uint32_t> perm, inv;
+    std::vector<uint32_t> h_inv;  // host copy of inv: sources map without a device round trip
 
     // pull side
     GraphArray<uint64_t> in_offsets;
