@@ -51,7 +51,7 @@ def parse_args():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", choices=["inhbm", "hybrid", "batch", "serve", "hubsort", "load", "contrib",
-                                           "ppr8"],
+                                           "ppr8", "shard"],
                     default="inhbm",
                     help="inhbm: graph resident in HBM (default); hybrid: edges in pinned host memory under a "
                          "device budget (defaults to R-MAT scale 27, edge factor 32, 8 GiB); batch: 64 graphs of "
@@ -59,7 +59,8 @@ def parse_args():
                          "batching of a Poisson stream; hubsort: hub sorting + vertex reordering of the graph; load: "
                          "text edge list -> CSR in HBM (GraphLoader) and the binary CSR file; contrib: PageRank "
                          "contributions + contribution schedule of every vertex + partition priorities; ppr8: 8 personalized "
-                         "PageRank queries packed into one solve vs one at a time")
+                         "PageRank queries packed into one solve vs one at a time; shard: the inhbm step on ONE graph "
+                         "split by vertex range over all ranks (strong scaling, vectors exchanged over NCCL)")
     ap.add_argument("--hub-fraction", type=float, default=0.08)
     ap.add_argument("--vertex-order", choices=["input", "hub"], default="hub",
                     help="inhbm: store the graph in hub order (HYT_GRAPH_HUB_ORDER); results stay in input ids")
@@ -1213,6 +1214,114 @@ def run_ppr8_workload(args, rank, world, local, pg):
         print(json.dumps(line), flush=True)
 
 
+def run_shard_workload(args, rank, world, local, pg):
+    """The inhbm step (PageRank to L1 <= 1e-6 + SSSP from the seeded
+    sources) on ONE graph split by vertex range over all ranks
+    (hytgraph_b200.ShardedGraph): every rank builds the same graph, computes
+    its range, and the vectors move over NCCL between iterations / rounds.
+    Strong scaling: the total work is fixed as ranks are added."""
+    import torch
+
+    import hytgraph_b200 as hyt
+    from hytgraph_b200 import capi
+
+    peak_gbs, peak_kind = load_peaks()
+    stream = torch.cuda.current_stream()
+    d = hyt.rmat(args.scale, args.edge_factor, args.seed, device=True)
+    V, E = d.num_vertices, d.num_edges
+    off_h, cols_h, w_h = host_graph_from_device(d)
+    off_np = off_h.numpy().view(np.uint64)
+    sources = [int(x) for x in hyt.pick_sources(off_np, args.seed, args.sources)]
+    gflags = capi.HYT_GRAPH_ALL | (capi.HYT_GRAPH_HUB_ORDER if args.vertex_order == "hub" else 0)
+    g = hyt.Graph(d, flags=gflags)
+    d.free()
+    sg = hyt.ShardedGraph(g)
+    ranks_out = torch.empty(V, dtype=torch.float32, device="cuda")
+    dist_out = torch.empty(V, dtype=torch.int32, device="cuda")
+
+    def step(collect):
+        _, st = sg.pagerank(out=ranks_out)
+        collect["pr"].append(st)
+        for s_ in sources:
+            _, ss = sg.sssp(s_, out=dist_out)
+            collect["sssp"].append(ss)
+
+    warm = {"pr": [], "sssp": []}
+    for _ in range(args.warmup):
+        step(warm)
+    clocks = ClockSampler(local)
+    clocks.start()
+    timed = {"pr": [], "sssp": []}
+    barrier(pg)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step(timed)
+    ev1.record(stream)
+    barrier(pg)
+    clk = clocks.stop()
+    ms = max_over_ranks(pg, ev0.elapsed_time(ev1))
+    pr_it = sum(x["iterations"] for x in timed["pr"])
+    rounds = sum(x["iterations"] for x in timed["sssp"])
+    value = (E * pr_it + E * len(timed["sssp"])) / (ms / 1e3) / 1e9
+    pr_ms = sum(x["ms"] for x in timed["pr"])
+    ss_ms = sum(x["ms"] for x in timed["sssp"])
+    pull, push = sg.kernels.info(capi.HYT_SHARD_PULL), sg.kernels.info(capi.HYT_SHARD_PUSH)
+    it_bytes = 8 * E + 20 * V  # one PageRank iteration over the whole graph (as hyt_pagerank counts it)
+    it_ms = pr_ms / max(pr_it, 1)
+    roof = {"kernel": "shard_pr_step_kernel + slice broadcasts", "bound": "hbm",
+            "achieved": it_bytes / (it_ms / 1e3) / 1e9, "peak": peak_gbs * world, "unit": "GB/s",
+            "frac": it_bytes / (it_ms / 1e3) / 1e9 / (peak_gbs * world), "traffic": None, "peak_kind": peak_kind,
+            "algorithmic_bytes_per_launch": it_bytes, "avg_launch_ms": it_ms,
+            "note": "per PageRank iteration of the whole graph (all ranks' steps + the exchange, host-timed); "
+                    "peak = measured HBM copy bandwidth x ranks"}
+    launches = sum(1 + x["iterations"] for x in timed["pr"]) + sum(2 + 2 * x["iterations"] for x in timed["sssp"])
+    sg.close()
+    g.close()
+
+    # e2e: host CSR in, graph built and split, results back on the host
+    csr_h = hyt.CSR(off_np, cols_h.numpy().view(np.uint32), w_h.numpy().view(np.uint32))
+
+    def e2e_step():
+        with hyt.Graph(csr_h, flags=gflags) as g2, hyt.ShardedGraph(g2) as sg2:
+            _, st = sg2.pagerank()
+            for s_ in sources:
+                sg2.sssp(s_)
+        return st["iterations"]
+
+    e2e_step()
+    barrier(pg)
+    t0 = time.perf_counter()
+    e2e_it = 0
+    for _ in range(args.e2e_steps):
+        e2e_it += e2e_step()
+    barrier(pg)
+    e2e_ms = max_over_ranks(pg, 1e3 * (time.perf_counter() - t0))
+    e2e_value = (E * e2e_it + E * len(sources) * args.e2e_steps) / (e2e_ms / 1e3) / 1e9
+    if rank == 0:
+        line = {"metric": "PR/SSSP GTEPS on one graph split over the ranks", "value": value, "unit": UNIT,
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+                "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+                "dtype": "f32 (PageRank) / u32 (SSSP)", "data": "synthetic",
+                "config": dict(workload_config(args, V, E), parallelism=f"vertex-range shards x{world} (NCCL)",
+                               workload=f"one R-MAT scale {args.scale} edge factor {args.edge_factor} graph split "
+                                        f"by vertex range: PageRank to L1<=1e-6 + SSSP from {args.sources} "
+                                        f"seeded sources"),
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": (V + 1) * 8 + 8 * E,
+                        "d2h_bytes_per_step": 4 * V * (1 + len(sources)), "ms_per_step": e2e_ms / args.e2e_steps,
+                        "steps": args.e2e_steps},
+                "roofline": roof, "cpu_baseline": None, "clocks": clk, "gpu_launches": launches,
+                "pagerank": {"iterations_per_solve": pr_it / args.steps, "ms_per_solve": pr_ms / args.steps,
+                             "exchanged_bytes_per_solve": timed["pr"][0]["exchanged_bytes"]},
+                "sssp": {"solves": len(timed["sssp"]), "ms_per_solve": ss_ms / len(timed["sssp"]),
+                         "rounds_per_solve": rounds / len(timed["sssp"]),
+                         "relaxations_per_edge_rank0_last_solve": push["edges_relaxed"] / E},
+                "rank0_shard": {"pull_vertices": pull["vertex_end"] - pull["vertex_begin"],
+                                "pull_edges": pull["edges"], "push_vertices": push["vertex_end"] - push["vertex_begin"],
+                                "push_edges": push["edges"]}}
+        print(json.dumps(line), flush=True)
+
+
 def workload_config(args, V, E):
     return {"workload": f"in-HBM R-MAT scale {args.scale} edge factor {args.edge_factor}: PageRank to L1<=1e-6 "
                         f"+ SSSP from {args.sources} seeded sources",
@@ -1262,6 +1371,11 @@ def main():
         return
     if args.workload == "load":
         run_load_workload(args, rank, world, local, pg)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
+    if args.workload == "shard":
+        run_shard_workload(args, rank, world, local, pg)
         if pg is not None:
             pg.destroy_process_group()
         return

@@ -36,6 +36,8 @@ HYT_RUN_PROFILE = 1
 HYT_RUN_NO_GRAPH = 2
 
 HYT_DIST_INF_U32 = 0xFFFFFFFF
+HYT_SHARD_PULL = 1  # vertex-range shard kinds (hyt_shard_bounds / hyt_shard_create)
+HYT_SHARD_PUSH = 2
 HYT_NOALLOC_MAX_VERTICES = 1 << 20  # hyt_sssp_noalloc capacity (include/hyt/capi.h)
 HYT_NOALLOC_MAX_EDGES = 1 << 24
 
@@ -362,6 +364,41 @@ class hyt_server_stats(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class hyt_shard_info(C.Structure):
+    _fields_ = [
+        ("kind", C.c_uint32),
+        ("part", C.c_uint32),
+        ("parts", C.c_uint32),
+        ("vertex_begin", C.c_uint32),
+        ("vertex_end", C.c_uint32),
+        ("pad", C.c_uint32),
+        ("num_vertices", C.c_uint64),
+        ("edges", C.c_uint64),
+        ("tasks", C.c_uint64),
+        ("edges_relaxed", C.c_uint64),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_ if name != "pad"}
+
+
+class hyt_shard_pagerank(C.Structure):
+    _fields_ = [
+        ("rank", C.c_void_p * 2),
+        ("contrib", C.c_void_p * 2),
+        ("sums", C.c_void_p),
+        ("damping", C.c_float),
+        ("personalized", C.c_uint32),
+        ("source", C.c_uint32),
+        ("pad", C.c_uint32),
+        ("stream", C.c_void_p),
+    ]
+
+
+class hyt_shard_sssp(C.Structure):
+    _fields_ = [("keys", C.c_void_p), ("source", C.c_uint32), ("pad", C.c_uint32), ("stream", C.c_void_p)]
+
+
 class HytError(RuntimeError):
     def __init__(self, code: int, message: str):
         super().__init__(f"[hyt status {code}] {message}")
@@ -427,6 +464,17 @@ _SIGNATURES = [
     ("hyt_rmat_generate", C.c_int, [C.POINTER(hyt_rmat_params), C.c_int, C.POINTER(hyt_csr_buffers)]),
     ("hyt_csr_buffers_free", C.c_int, [C.POINTER(hyt_csr_buffers)]),
     ("hyt_pick_sources", C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint32, C.c_void_p]),
+    ("hyt_shard_bounds", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p]),
+    ("hyt_shard_create", C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_uint32,
+                                   C.POINTER(C.c_void_p)]),
+    ("hyt_shard_destroy", C.c_int, [C.c_void_p]),
+    ("hyt_shard_get_info", C.c_int, [C.c_void_p, C.POINTER(hyt_shard_info)]),
+    ("hyt_shard_pagerank_init", C.c_int, [C.c_void_p, C.POINTER(hyt_shard_pagerank)]),
+    ("hyt_shard_pagerank_step", C.c_int, [C.c_void_p, C.POINTER(hyt_shard_pagerank), C.c_uint32, C.c_double]),
+    ("hyt_shard_sssp_init", C.c_int, [C.c_void_p, C.POINTER(hyt_shard_sssp)]),
+    ("hyt_shard_sssp_round", C.c_int, [C.c_void_p, C.POINTER(hyt_shard_sssp)]),
+    ("hyt_shard_sssp_labels", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("hyt_shard_emit", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
 ]
 
 EXPORTED = [name for name, _, _ in _SIGNATURES]

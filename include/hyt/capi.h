@@ -630,6 +630,89 @@ int hyt_contribution_schedule(const uint64_t *item_indices, const double *contri
 int hyt_partition_contributions(const double *vertex_contributions, uint64_t num_vertices, const uint64_t *bounds,
                                 uint64_t num_partitions, double *out);
 
+/* ---- Vertex-range shards: one process per GPU ----------------------------
+ *
+ * Every process creates the same graph (same CSR, same flags) on its own GPU
+ * and takes one contiguous range of internal vertex ids.  A PageRank step
+ * computes the rank of the range's rows; an SSSP round expands the range's
+ * improved vertices.  Between steps the caller exchanges the whole-graph
+ * vectors with its collective library (hytgraph_b200.shard drives this with
+ * torch.distributed over NCCL): PageRank broadcasts each owner's slice of
+ * the contribution vector and sums two doubles; SSSP min-reduces the key
+ * vector.  The vectors are caller-owned device memory, so collectives write
+ * them in place.  The reference runs on one GPU; there is no reference
+ * interface for this part.  A shard borrows its graph (destroy shards
+ * first) and, like the graph's own solvers, runs one solve at a time. */
+#define HYT_SHARD_PULL 1u /* PageRank / personalized PageRank over CSC rows */
+#define HYT_SHARD_PUSH 2u /* SSSP over CSR rows */
+
+typedef struct hyt_shard hyt_shard;
+
+/* Cuts the internal vertex ids into `parts` contiguous ranges of balanced
+ * work (rows + in-edges for PULL, rows + out-edges for PUSH); PULL cuts fall
+ * on PageRank row tiles.  bounds[parts + 1], host.  Deterministic: every
+ * process holding the same graph gets the same bounds. */
+int hyt_shard_bounds(hyt_graph *graph, uint32_t kind, uint32_t parts, uint32_t *bounds);
+/* Shard `part` of `bounds` (PULL bounds must come from hyt_shard_bounds). */
+int hyt_shard_create(hyt_graph *graph, uint32_t kind, const uint32_t *bounds, uint32_t parts, uint32_t part,
+                     hyt_shard **out);
+int hyt_shard_destroy(hyt_shard *shard);
+
+typedef struct hyt_shard_info {
+    uint32_t kind, part, parts;
+    uint32_t vertex_begin, vertex_end; /* internal ids [begin, end) */
+    uint32_t pad;
+    uint64_t num_vertices;  /* of the whole graph */
+    uint64_t edges;         /* in-edges (PULL) / out-edges (PUSH) of the range's rows */
+    uint64_t tasks;         /* PULL: tile + chunk tasks of one step */
+    uint64_t edges_relaxed; /* PUSH: out-edges expanded since the last init */
+} hyt_shard_info;
+int hyt_shard_get_info(hyt_shard *shard, hyt_shard_info *out);
+
+typedef struct hyt_shard_pagerank {
+    float *rank[2];    /* device [V]: the iterate, by parity of the iteration */
+    float *contrib[2]; /* device [V]: rank / out-degree (0 for dangling vertices) */
+    double *sums;      /* device [2]: L1 change and dangling mass of the range's rows */
+    float damping;     /* PageRank damping; personalized PageRank: 1 - restart */
+    uint32_t personalized;
+    uint32_t source;   /* personalized: the caller's vertex id */
+    uint32_t pad;
+    void *stream;      /* NULL: the graph's stream */
+} hyt_shard_pagerank;
+
+/* The initial iterate of EVERY vertex into rank[0] / contrib[0] (1/n, or
+ * the source indicator); sums = {0, dangling mass of the range's rows}. */
+int hyt_shard_pagerank_init(hyt_shard *shard, const hyt_shard_pagerank *args);
+/* Step `iteration` (0-based) of pagerank_gpu's synchronous pull
+ * (src/algorithms/pagerank.cpp:89-163) over the range's rows: reads
+ * rank/contrib[iteration & 1] (every vertex current), writes
+ * rank/contrib[(iteration + 1) & 1] at the range's rows, and sets sums to
+ * the range's L1 change and new dangling mass.  `dangling` = the whole
+ * graph's dangling mass of the iterate read.  Asynchronous on the stream. */
+int hyt_shard_pagerank_step(hyt_shard *shard, const hyt_shard_pagerank *args, uint32_t iteration,
+                            double dangling);
+
+typedef struct hyt_shard_sssp {
+    int32_t *keys;    /* device [V + 1]: label XOR 0x80000000 as int32 (signed order = label order); [V] = idle flag */
+    uint32_t source;  /* the caller's vertex id */
+    uint32_t pad;
+    void *stream;     /* NULL: the graph's stream */
+} hyt_shard_sssp;
+
+/* keys: every label infinite (HYT_DIST_INF_U32, +inf bits for F32 weights)
+ * except the source's 0; the shard forgets what it expanded. */
+int hyt_shard_sssp_init(hyt_shard *shard, const hyt_shard_sssp *args);
+/* One round: expands the owned vertices whose label dropped since their
+ * last expansion into keys (atomic min) and sets keys[V] = 1 when there
+ * were none, else 0.  The caller then min-reduces keys[0..V] over all
+ * shards and stops when keys[V] is 1.  Asynchronous on the stream. */
+int hyt_shard_sssp_round(hyt_shard *shard, const hyt_shard_sssp *args);
+/* u32 labels (caller's vertex order) of keys[0..V) into out [V]: host or device. */
+int hyt_shard_sssp_labels(hyt_shard *shard, const int32_t *keys, uint32_t *out, void *stream);
+/* V 4-byte values in internal order (device) into out [V] in the caller's
+ * vertex order: host or device. */
+int hyt_shard_emit(hyt_shard *shard, const void *values, void *out, void *stream);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif
