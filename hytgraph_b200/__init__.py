@@ -12,14 +12,14 @@ Importing the package loads lib/libhyt_core.so and fails if it is missing;
 there is no CPU fallback.
 """
 from . import capi
-from .capi import HytError, device_count
+from .capi import HytError, device_count, measure_peaks
 from .graph import (CSR, Batch, DeviceCSR, Graph, HybridGraph, PinnedBuffer, Server, contribution_schedule,
                     csr_from_edges, hub_sort, load_csr, load_edge_list, partition_contributions, pick_sources, reorder,
                     rmat, save_csr, sssp_contributions)
 from .shard import CudaShardKernels, ShardedGraph
 
 __all__ = [
-    "capi", "HytError", "device_count", "CSR", "Batch", "DeviceCSR", "Graph", "HybridGraph", "PinnedBuffer", "Server",
+    "capi", "HytError", "device_count", "measure_peaks", "CSR", "Batch", "DeviceCSR", "Graph", "HybridGraph", "PinnedBuffer", "Server",
     "contribution_schedule", "csr_from_edges", "hub_sort", "load_csr", "load_edge_list", "partition_contributions",
     "pick_sources", "reorder", "rmat", "save_csr", "sssp_contributions", "CudaShardKernels", "ShardedGraph",
 ]

@@ -399,6 +399,24 @@ class hyt_shard_sssp(C.Structure):
     _fields_ = [("keys", C.c_void_p), ("source", C.c_uint32), ("pad", C.c_uint32), ("stream", C.c_void_p)]
 
 
+class hyt_peaks(C.Structure):
+    _fields_ = [
+        ("hbm_copy_gbs", C.c_double),
+        ("h2d_gbs", C.c_double),
+        ("d2h_gbs", C.c_double),
+        ("zero_copy_gbs", C.c_double),
+        ("hbm_bytes", C.c_uint64),
+        ("l2_bytes", C.c_uint64),
+        ("copy_bytes", C.c_uint64),
+        ("link_bytes", C.c_uint64),
+        ("sm_count", C.c_uint32),
+        ("mem_bus_bits", C.c_uint32),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 class HytError(RuntimeError):
     def __init__(self, code: int, message: str):
         super().__init__(f"[hyt status {code}] {message}")
@@ -464,6 +482,7 @@ _SIGNATURES = [
     ("hyt_rmat_generate", C.c_int, [C.POINTER(hyt_rmat_params), C.c_int, C.POINTER(hyt_csr_buffers)]),
     ("hyt_csr_buffers_free", C.c_int, [C.POINTER(hyt_csr_buffers)]),
     ("hyt_pick_sources", C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint32, C.c_void_p]),
+    ("hyt_measure_peaks", C.c_int, [C.c_int, C.c_uint64, C.POINTER(hyt_peaks)]),
     ("hyt_shard_bounds", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p]),
     ("hyt_shard_create", C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_uint32,
                                    C.POINTER(C.c_void_p)]),
@@ -510,6 +529,14 @@ def check(status: int) -> None:
 def copy(dst: int, src: int, nbytes: int, stream: int = 0) -> None:
     """Synchronous copy between host/device addresses (integers)."""
     check(lib.hyt_copy(dst, src, nbytes, stream or None))
+
+
+def measure_peaks(device: int = 0, copy_bytes: int = 0) -> dict:
+    """Measured HBM copy, pinned host-link and zero-copy bandwidths of one
+    GPU (hyt_measure_peaks), GB/s, plus its memory and SM facts."""
+    p = hyt_peaks()
+    check(lib.hyt_measure_peaks(device, copy_bytes, C.byref(p)))
+    return p.as_dict()
 
 
 def device_count() -> int:

@@ -630,6 +630,28 @@ int hyt_contribution_schedule(const uint64_t *item_indices, const double *contri
 int hyt_partition_contributions(const double *vertex_contributions, uint64_t num_vertices, const uint64_t *bounds,
                                 uint64_t num_partitions, double *out);
 
+/* ---- Measured peaks ------------------------------------------------------
+ * The denominators of the path's rooflines, measured on `device`: a
+ * device-to-device copy of copy_bytes (0: 1 GiB; read + write bytes over
+ * time), pinned host<->device copies and kernel reads of mapped pinned host
+ * memory (min(copy_bytes, 256 MiB) each), best of several repetitions.
+ * Needs 2 x copy_bytes of free device memory (else HYT_E_OOM).  The
+ * reference has no counterpart (its cost model uses fixed placeholders:
+ * src/transfer/hytm_cost_model.cpp). */
+typedef struct hyt_peaks {
+    double hbm_copy_gbs;   /* device-to-device copy, GB/s */
+    double h2d_gbs;        /* pinned host -> device, GB/s */
+    double d2h_gbs;        /* device -> pinned host, GB/s */
+    double zero_copy_gbs;  /* kernel reads of mapped pinned host memory, GB/s */
+    uint64_t hbm_bytes;    /* device memory */
+    uint64_t l2_bytes;
+    uint64_t copy_bytes;   /* bytes per device copy timed */
+    uint64_t link_bytes;   /* bytes per host-link copy timed */
+    uint32_t sm_count;
+    uint32_t mem_bus_bits;
+} hyt_peaks;
+int hyt_measure_peaks(int device, uint64_t copy_bytes, hyt_peaks *out);
+
 /* ---- Vertex-range shards: one process per GPU ----------------------------
  *
  * Every process creates the same graph (same CSR, same flags) on its own GPU

@@ -38,6 +38,9 @@ def test_abi_version_and_errors_without_device(hyt):
             hyt.Graph(g)
         assert e.value.code == hyt.capi.HYT_E_NO_DEVICE
         assert "no CUDA device" in hyt.capi.last_error()
+        with pytest.raises(hyt.HytError) as e:
+            hyt.measure_peaks()
+        assert e.value.code == hyt.capi.HYT_E_NO_DEVICE
 
 
 def test_invalid_generator_params(hyt):
