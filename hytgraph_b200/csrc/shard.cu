@@ -605,11 +605,9 @@ int hyt_shard_create(hyt_graph *graph, uint32_t kind, const uint32_t *bounds, ui
 }
 
 int hyt_shard_destroy(hyt_shard *shard) {
-    return guarded([&] {
-        if (!shard) return;
-        HYT_CUDA(cudaSetDevice(shard->impl.g->device));
-        delete shard;
-    });
+    // Touches only the shard's own arrays (each frees on the device it was
+    // allocated on), so it is safe after the graph was destroyed.
+    return guarded([&] { delete shard; });
 }
 
 int hyt_shard_get_info(hyt_shard *shard, hyt_shard_info *out) {

@@ -176,6 +176,7 @@ class Graph:
         h = C.c_void_p()
         check(lib.hyt_graph_create(C.byref(c), C.byref(opts), C.byref(h)))
         self._h = h
+        self.device = int(device)
         self.num_vertices = int(c.num_vertices)
         self.num_edges = int(c.num_edges)
         self._csr_ref = None

@@ -50,7 +50,7 @@ class PageRankVectors:
 
 class CudaShardKernels:
     """The shard entry points of the C ABI for one process: shard `part` of
-    `parts` of `graph`, on the graph's GPU (the current CUDA device)."""
+    `parts` of `graph`, with its vectors on the graph's GPU."""
 
     def __init__(self, graph, part: int, parts: int):
         import torch
@@ -59,7 +59,7 @@ class CudaShardKernels:
         self.graph = graph
         self.part, self.parts = int(part), int(parts)
         self.num_vertices = int(graph.num_vertices)
-        self.device = torch.device("cuda", torch.cuda.current_device())
+        self.device = torch.device("cuda", getattr(graph, "device", torch.cuda.current_device()))
         self._bounds = {}
         self._shards = {}
 
