@@ -1275,7 +1275,8 @@ def run_shard_workload(args, rank, world, local, pg):
             "algorithmic_bytes_per_launch": it_bytes, "avg_launch_ms": it_ms,
             "note": "per PageRank iteration of the whole graph (all ranks' steps + the exchange, host-timed); "
                     "peak = measured HBM copy bandwidth x ranks"}
-    launches = sum(1 + x["iterations"] for x in timed["pr"]) + sum(2 + 2 * x["iterations"] for x in timed["sssp"])
+    # PageRank: init + one step per iteration + emit; SSSP: init + (collect, expand, sweep) per round + labels
+    launches = sum(2 + x["iterations"] for x in timed["pr"]) + sum(3 + 3 * x["iterations"] for x in timed["sssp"])
     sg.close()
     g.close()
 

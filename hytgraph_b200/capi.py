@@ -396,7 +396,8 @@ class hyt_shard_pagerank(C.Structure):
 
 
 class hyt_shard_sssp(C.Structure):
-    _fields_ = [("keys", C.c_void_p), ("source", C.c_uint32), ("pad", C.c_uint32), ("stream", C.c_void_p)]
+    _fields_ = [("keys", C.c_void_p), ("source", C.c_uint32), ("pad", C.c_uint32), ("stream", C.c_void_p),
+                ("frontier_edges", C.c_void_p)]
 
 
 class hyt_peaks(C.Structure):
@@ -491,6 +492,8 @@ _SIGNATURES = [
     ("hyt_shard_pagerank_init", C.c_int, [C.c_void_p, C.POINTER(hyt_shard_pagerank)]),
     ("hyt_shard_pagerank_step", C.c_int, [C.c_void_p, C.POINTER(hyt_shard_pagerank), C.c_uint32, C.c_double]),
     ("hyt_shard_sssp_init", C.c_int, [C.c_void_p, C.POINTER(hyt_shard_sssp)]),
+    ("hyt_shard_sssp_collect", C.c_int, [C.c_void_p, C.POINTER(hyt_shard_sssp)]),
+    ("hyt_shard_sssp_relax", C.c_int, [C.c_void_p, C.POINTER(hyt_shard_sssp)]),
     ("hyt_shard_sssp_round", C.c_int, [C.c_void_p, C.POINTER(hyt_shard_sssp)]),
     ("hyt_shard_sssp_labels", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("hyt_shard_emit", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),

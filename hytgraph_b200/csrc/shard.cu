@@ -43,13 +43,15 @@ namespace hyt {
 constexpr uint32_t kSegEdges = 256;           // out-edges per SSSP expansion segment
 constexpr uint32_t kKeyBias = 0x80000000u;    // label -> ordered int32 key
 constexpr int kExpandBatch = 4;               // 32-edge batches in flight per warp
+constexpr uint32_t kShardPullDiv = 4;         // pull sweep when frontier out-edges > E / 4 (as hyt_sssp)
 
 struct ShardImpl {
     GraphImpl *g = nullptr;
     uint32_t kind = 0, part = 0, parts = 0;
     uint32_t vb = 0, ve = 0;
     uint64_t edges = 0;  // in-edges (pull) or out-edges (push) of the range's rows
-    // pull: the range's PageRank tasks and their long-row workspaces
+    // pull (and the pull sweeps of push shards): the range's PageRank tasks
+    // and their long-row workspaces
     uint64_t chunk_begin = 0, chunk_end = 0, tile_begin = 0, tile_end = 0;
     GraphArray<float> partial;
     GraphArray<uint32_t> ticket;
@@ -60,6 +62,10 @@ struct ShardImpl {
     GraphArray<uint4> segs;
     GraphArray<unsigned long long> ctr;
     uint32_t inf = HYT_DIST_INF_U32;
+    // push: pull sweeps (rounds with a dense frontier) over this shard's
+    // PageRank task range of the PULL bounds (fields above)
+    bool pull_ok = false;
+    uint64_t pull_edges = 0;
 };
 
 namespace {
@@ -147,8 +153,35 @@ struct SSShard {
     uint32_t *prev;      // [ve - vb]
     uint4 *segs;         // (vertex, label, first edge, end edge)
     unsigned long long *ctr;
+    const unsigned long long *frontier;  // out-edges of every shard's frontier this round
+    uint64_t num_edges;
     uint32_t vb, ve, V;
+    uint32_t pull_div;   // > 0: a round whose frontier has more than E / pull_div out-edges is a pull sweep
+    uint32_t inf;
 };
+
+// The shard's pull sweep: its PageRank row tiles and long-row chunks over
+// the CSC (in-sources tagged like PageRank's, weights in CSC order).
+struct SSPull {
+    const uint64_t *in_off;
+    const uint32_t *in_src;
+    const uint32_t *in_w;
+    const uint32_t *tile_start;
+    const LongRow *long_rows;
+    const uint2 *chunk_tasks;
+    const uint32_t *hot_vertex;
+    uint64_t chunk_begin, chunk_end, tile_begin, tile_end;
+    uint64_t edges;  // in-edges of the sweep's rows
+    uint32_t num_hot, tile_cost;
+};
+
+// Same answer in every kernel of a round and on every shard (the count is
+// the caller's sum over shards).
+__device__ __forceinline__ bool shard_pull_round(const SSShard &a) {
+    if (!a.pull_div) return false;
+    const unsigned long long fe = *(volatile const unsigned long long *)a.frontier;
+    return fe * a.pull_div > a.num_edges;
+}
 
 __global__ void shard_sssp_init_kernel(int32_t *keys, uint32_t V, uint32_t source, uint32_t inf, uint32_t *prev,
                                        uint32_t n_owned) {
@@ -161,7 +194,7 @@ __global__ void shard_sssp_init_kernel(int32_t *keys, uint32_t V, uint32_t sourc
 
 // Owned vertices whose label dropped since their last expansion: record the
 // label and append the row as kSegEdges-edge segments (one warp-aggregated
-// atomic per warp).
+// atomic per warp); ctr[3] += their out-edges.
 __global__ void __launch_bounds__(256) shard_sssp_collect_kernel(SSShard a) {
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t n = a.ve - a.vb;
@@ -182,6 +215,10 @@ __global__ void __launch_bounds__(256) shard_sssp_collect_kernel(SSShard a) {
             }
         }
         const uint32_t amask = __ballot_sync(0xffffffffu, act);
+        unsigned long long fe = hi - lo;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) fe += __shfl_xor_sync(0xffffffffu, fe, o);
+        if (lane == 0 && fe) atomicAdd(&a.ctr[3], fe);
         uint32_t incl = nseg;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -205,11 +242,13 @@ __global__ void __launch_bounds__(256) shard_sssp_collect_kernel(SSShard a) {
 // A warp takes 32 segments, prefix-sums their lengths and walks the combined
 // edge list 32 edges at a time (kExpandBatch batches in flight), finding
 // each edge's segment with a 5-step shuffle search.  Thread 0 of block 0
-// writes the idle flag from the round's expanded-vertex count.
+// writes the idle flag from the round's expanded-vertex count; a pull round
+// does nothing else here.
 template <int WK>
 __global__ void __launch_bounds__(256) shard_sssp_expand_kernel(SSShard a) {
     const uint64_t nseg = a.ctr[1];
     if (blockIdx.x == 0 && threadIdx.x == 0) a.keys[a.V] = a.ctr[0] ? 0 : 1;
+    if (shard_pull_round(a)) return;
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t gw = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     const uint64_t nw = (uint64_t(gridDim.x) * blockDim.x) >> 5;
@@ -262,6 +301,111 @@ __global__ void __launch_bounds__(256) shard_sssp_expand_kernel(SSShard a) {
     if (lane == 0 && relaxed) atomicAdd(&a.ctr[2], relaxed);
 }
 
+// Candidate labels d[u] + w of in-edges [lo, hi) (infinity from unreached
+// sources), 16 per lane in flight: ids and weights streamed, hot slots
+// mapped to vertex ids through the CTA's table, labels gathered from L2.
+constexpr int kShardPullBatch = 16;
+
+template <int WK, class Sink>
+__device__ __forceinline__ void shard_pull_span(const SSShard &a, const SSPull &p, const uint32_t *s_hot,
+                                                uint64_t lo, uint64_t hi, uint64_t pol, int lane, Sink &&sink) {
+    const uint32_t n = static_cast<uint32_t>(hi - lo);
+    for (uint32_t base = 0; base < n; base += 32 * kShardPullBatch) {
+        uint32_t id[kShardPullBatch], w[kShardPullBatch], du[kShardPullBatch];
+#pragma unroll
+        for (int k = 0; k < kShardPullBatch; ++k) {
+            const uint32_t i = base + 32 * k + lane;
+            id[k] = (i < n) ? dev::ld_stream(p.in_src + lo + i) : 0u;
+            w[k] = (i < n) ? ssc::edge_weight<WK>(p.in_w, lo + i) : 0u;
+        }
+#pragma unroll
+        for (int k = 0; k < kShardPullBatch; ++k)
+            if (id[k] & kHotTag) id[k] = s_hot[id[k] & ~kHotTag];
+#pragma unroll
+        for (int k = 0; k < kShardPullBatch; ++k)
+            du[k] = static_cast<uint32_t>(dev::ld_keep_u32(reinterpret_cast<const uint32_t *>(a.keys) + id[k], pol)) ^
+                    kKeyBias;
+#pragma unroll
+        for (int k = 0; k < kShardPullBatch; ++k) {
+            const uint32_t i = base + 32 * k + lane;
+            if (i < n) sink(i, du[k] == a.inf ? a.inf : ssc::extend<WK>(du[k], w[k]));
+        }
+    }
+}
+
+__device__ __forceinline__ void shard_pull_relax(const SSShard &a, uint32_t r, uint32_t c) {
+    if (c < (static_cast<uint32_t>(__ldcg(a.keys + r)) ^ kKeyBias))
+        atomicMin(a.keys + r, static_cast<int32_t>(c ^ kKeyBias));
+}
+
+// Pull round: every row of the shard's sweep range takes the minimum over
+// its in-edges of d[u] + w (the single-GPU sweep's task decomposition:
+// merge-path tiles of short rows staged per warp, long rows in chunks whose
+// minima meet in an atomic min).  Nothing in a push round.
+template <int WK>
+__global__ void __launch_bounds__(kPRThreads, 1) shard_sssp_pull_kernel(SSShard a, SSPull p) {
+    extern __shared__ __align__(16) uint32_t s_pull[];
+    if (!shard_pull_round(a)) return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t *s_hot = s_pull;
+    for (uint32_t i = threadIdx.x; i < p.num_hot; i += blockDim.x) s_hot[i] = p.hot_vertex[i];
+    __syncthreads();
+    uint32_t *sv = s_pull + p.num_hot + warp * (2 * p.tile_cost + 8);
+    const uint64_t pol = dev::policy_evict_last();
+    const uint64_t n_chunks = p.chunk_end - p.chunk_begin;
+    const uint64_t total = n_chunks + (p.tile_end - p.tile_begin);
+    const uint64_t nwarps = uint64_t(gridDim.x) * (kPRThreads / 32);
+    for (uint64_t task = uint64_t(blockIdx.x) * (kPRThreads / 32) + warp; task < total; task += nwarps) {
+        if (task < n_chunks) {
+            const uint2 t = p.chunk_tasks[p.chunk_begin + task];
+            const LongRow L = p.long_rows[t.x];
+            const uint64_t rb = p.in_off[L.row], re = p.in_off[L.row + 1];
+            const uint64_t lo = rb + uint64_t(t.y) * kLongChunk;
+            const uint64_t hi = (lo + kLongChunk < re) ? lo + kLongChunk : re;
+            uint32_t best = a.inf;
+            shard_pull_span<WK>(a, p, s_hot, lo, hi, pol, lane, [&](uint32_t, uint32_t c) { best = min(best, c); });
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(0xffffffffu, best, o));
+            if (lane == 0) shard_pull_relax(a, L.row, best);
+        } else {
+            const uint64_t k = p.tile_begin + (task - n_chunks);
+            const uint32_t r0 = p.tile_start[k], r1 = p.tile_start[k + 1];
+            if (r0 == r1) continue;
+            const uint64_t last_b = p.in_off[r1 - 1], last_e = p.in_off[r1];
+            const uint32_t rl = (last_e - last_b >= p.tile_cost) ? r1 - 1 : r1;  // long last row is chunked
+            const uint64_t e0 = p.in_off[r0];
+            const uint64_t e1 = (rl == r1) ? last_e : last_b;
+            shard_pull_span<WK>(a, p, s_hot, e0, e1, pol, lane, [&](uint32_t i, uint32_t c) { sv[i] = c; });
+            __syncwarp();
+            for (uint32_t rb = r0; rb < rl; rb += 32) {
+                const uint32_t r = rb + lane;
+                const bool active = r < rl;
+                const uint64_t lo = active ? p.in_off[r] : 0;
+                const uint64_t hi = active ? p.in_off[r + 1] : 0;
+                if (active && hi - lo < 64) {
+                    uint32_t best = a.inf;
+                    for (uint64_t x = lo; x < hi; ++x) best = min(best, sv[x - e0]);
+                    shard_pull_relax(a, r, best);
+                }
+                uint32_t big = __ballot_sync(0xffffffffu, active && (hi - lo >= 64));
+                while (big) {
+                    const int src = __ffs(big) - 1;
+                    big &= big - 1;
+                    const uint64_t bb = __shfl_sync(0xffffffffu, lo, src);
+                    const uint64_t ee = __shfl_sync(0xffffffffu, hi, src);
+                    uint32_t best = a.inf;
+                    for (uint64_t x = bb + lane; x < ee; x += 32) best = min(best, sv[x - e0]);
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(0xffffffffu, best, o));
+                    if (lane == 0) shard_pull_relax(a, rb + src, best);
+                }
+            }
+            __syncwarp();
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && p.edges) atomicAdd(&a.ctr[2], static_cast<unsigned long long>(p.edges));
+}
+
 __global__ void shard_keys_to_labels_kernel(const int32_t *keys, uint64_t V, uint32_t *labels) {
     for (uint64_t v = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; v < V; v += uint64_t(gridDim.x) * blockDim.x)
         labels[v] = static_cast<uint32_t>(keys[v]) ^ kKeyBias;
@@ -277,10 +421,34 @@ SSShard sssp_view(ShardImpl &sh, int32_t *keys) {
     a.prev = sh.prev.get();
     a.segs = sh.segs.get();
     a.ctr = sh.ctr.get();
+    a.frontier = sh.ctr.get() + 3;
+    a.num_edges = g.E;
     a.vb = sh.vb;
     a.ve = sh.ve;
     a.V = static_cast<uint32_t>(g.V);
+    a.pull_div = 0;
+    a.inf = sh.inf;
     return a;
+}
+
+SSPull pull_view(const ShardImpl &sh) {
+    const GraphImpl &g = *sh.g;
+    SSPull p{};
+    p.in_off = g.in_offsets.get();
+    p.in_src = g.in_sources.get();
+    p.in_w = g.in_weights.get();
+    p.tile_start = g.tile_start.get();
+    p.long_rows = g.long_rows.get();
+    p.chunk_tasks = g.chunk_tasks.get();
+    p.hot_vertex = g.hot_vertex.get();
+    p.chunk_begin = sh.chunk_begin;
+    p.chunk_end = sh.chunk_end;
+    p.tile_begin = sh.tile_begin;
+    p.tile_end = sh.tile_end;
+    p.edges = sh.pull_edges;
+    p.num_hot = g.num_hot;
+    p.tile_cost = g.tile_cost;
+    return p;
 }
 
 cudaStream_t stream_of(const ShardImpl &sh, void *stream) {
@@ -346,6 +514,50 @@ void shard_bounds(GraphImpl &g, uint32_t kind, uint32_t parts, uint32_t *bounds)
     }
 }
 
+namespace {
+
+// PageRank task range of the rows [vb, ve) (bounds on row tiles) into sh's
+// tile / chunk fields; returns the rows' in-edges.
+uint64_t pull_tasks(GraphImpl &g, uint32_t vb, uint32_t ve, ShardImpl &sh) {
+    const cudaStream_t s = g.stream;
+    const std::vector<uint32_t> ts = download(g.tile_start.get(), g.num_tiles + 1, s);
+    auto tile_of = [&](uint32_t v) -> uint64_t {
+        const auto it = std::lower_bound(ts.begin(), ts.end(), v);
+        if (it == ts.end() || *it != v) fail(HYT_E_INVALID, "pull shard bounds must fall on row tiles (hyt_shard_bounds)");
+        return static_cast<uint64_t>(it - ts.begin());
+    };
+    // the first tile starting at each bound: neighbouring shards split the
+    // tile list without overlap even where empty tiles repeat a start
+    sh.tile_begin = tile_of(vb);
+    sh.tile_end = tile_of(ve);
+    // long rows end tiles, so the range's long rows are those with a row in
+    // [vb, ve); their chunk tasks are one contiguous run
+    const std::vector<LongRow> lr = download(g.long_rows.get(), g.num_long, s);
+    const std::vector<uint2> ct = download(g.chunk_tasks.get(), g.num_chunks, s);
+    uint64_t li = 0;
+    while (li < lr.size() && lr[li].row < vb) ++li;
+    uint64_t lj = li;
+    while (lj < lr.size() && lr[lj].row < ve) ++lj;
+    for (uint64_t k = li; k < lj; ++k) {
+        if (k + 1 < lj && lr[k + 1].first_chunk != lr[k].first_chunk + lr[k].num_chunks)
+            fail(HYT_E_INTERNAL, "long-row chunk tasks are not contiguous");
+        for (uint32_t j = 0; j < lr[k].num_chunks; ++j) {
+            const uint64_t c = uint64_t(lr[k].first_chunk) + j;
+            if (c >= ct.size() || ct[c].x != k || ct[c].y != j)
+                fail(HYT_E_INTERNAL, "long-row chunk tasks are not in long-row order");
+        }
+    }
+    sh.chunk_begin = (li < lj) ? lr[li].first_chunk : 0;
+    sh.chunk_end = (li < lj) ? uint64_t(lr[lj - 1].first_chunk) + lr[lj - 1].num_chunks : 0;
+    uint64_t e[2] = {0, 0};
+    HYT_CUDA(cudaMemcpyAsync(&e[0], g.in_offsets.get() + vb, 8, cudaMemcpyDeviceToHost, s));
+    HYT_CUDA(cudaMemcpyAsync(&e[1], g.in_offsets.get() + ve, 8, cudaMemcpyDeviceToHost, s));
+    HYT_CUDA(cudaStreamSynchronize(s));
+    return e[1] - e[0];
+}
+
+}  // namespace
+
 void shard_create(GraphImpl &g, uint32_t kind, const uint32_t *bounds, uint32_t parts, uint32_t part,
                   ShardImpl &sh) {
     if (!bounds) fail(HYT_E_INVALID, "bounds is NULL");
@@ -362,40 +574,7 @@ void shard_create(GraphImpl &g, uint32_t kind, const uint32_t *bounds, uint32_t 
     sh.ve = bounds[part + 1];
     if (kind == HYT_SHARD_PULL) {
         if (!(g.flags & HYT_GRAPH_PULL)) fail(HYT_E_INVALID, "pull shards need a graph created with HYT_GRAPH_PULL");
-        const std::vector<uint32_t> ts = download(g.tile_start.get(), g.num_tiles + 1, s);
-        auto tile_of = [&](uint32_t v) -> uint64_t {
-            const auto it = std::lower_bound(ts.begin(), ts.end(), v);
-            if (it == ts.end() || *it != v) fail(HYT_E_INVALID, "pull shard bounds must fall on row tiles (hyt_shard_bounds)");
-            return static_cast<uint64_t>(it - ts.begin());
-        };
-        // the first tile starting at each bound: neighbouring shards split
-        // the tile list without overlap even where empty tiles repeat a start
-        sh.tile_begin = tile_of(sh.vb);
-        sh.tile_end = tile_of(sh.ve);
-        // long rows end tiles, so the range's long rows are those with a row
-        // in [vb, ve); their chunk tasks are one contiguous run
-        const std::vector<LongRow> lr = download(g.long_rows.get(), g.num_long, s);
-        const std::vector<uint2> ct = download(g.chunk_tasks.get(), g.num_chunks, s);
-        uint64_t li = 0;
-        while (li < lr.size() && lr[li].row < sh.vb) ++li;
-        uint64_t lj = li;
-        while (lj < lr.size() && lr[lj].row < sh.ve) ++lj;
-        for (uint64_t k = li; k < lj; ++k) {
-            if (k + 1 < lj && lr[k + 1].first_chunk != lr[k].first_chunk + lr[k].num_chunks)
-                fail(HYT_E_INTERNAL, "long-row chunk tasks are not contiguous");
-            for (uint32_t j = 0; j < lr[k].num_chunks; ++j) {
-                const uint64_t c = uint64_t(lr[k].first_chunk) + j;
-                if (c >= ct.size() || ct[c].x != k || ct[c].y != j)
-                    fail(HYT_E_INTERNAL, "long-row chunk tasks are not in long-row order");
-            }
-        }
-        sh.chunk_begin = (li < lj) ? lr[li].first_chunk : 0;
-        sh.chunk_end = (li < lj) ? uint64_t(lr[lj - 1].first_chunk) + lr[lj - 1].num_chunks : 0;
-        uint64_t e[2] = {0, 0};
-        HYT_CUDA(cudaMemcpyAsync(&e[0], g.in_offsets.get() + sh.vb, 8, cudaMemcpyDeviceToHost, s));
-        HYT_CUDA(cudaMemcpyAsync(&e[1], g.in_offsets.get() + sh.ve, 8, cudaMemcpyDeviceToHost, s));
-        HYT_CUDA(cudaStreamSynchronize(s));
-        sh.edges = e[1] - e[0];
+        sh.edges = pull_tasks(g, sh.vb, sh.ve, sh);
         sh.partial.allocate(2 * std::max<uint64_t>(g.num_chunks, 1));
         sh.ticket.allocate(std::max<uint64_t>(g.num_long, 1));
         HYT_CUDA(cudaMemsetAsync(sh.ticket.get(), 0, sh.ticket.count * sizeof(uint32_t), s));
@@ -417,6 +596,15 @@ void shard_create(GraphImpl &g, uint32_t kind, const uint32_t *bounds, uint32_t 
         HYT_CUDA(cudaMemsetAsync(sh.ctr.get(), 0, 4 * sizeof(unsigned long long), s));
         HYT_CUDA(cudaStreamSynchronize(s));
         sh.inf = (g.weight_kind == HYT_WEIGHTS_F32) ? 0x7F800000u : HYT_DIST_INF_U32;
+        // Pull sweeps cover the rows of this shard's part of the PULL bounds
+        // (a second partition of the same vertices, derived identically by
+        // every process); they need the CSC and its weights.
+        if ((g.flags & HYT_GRAPH_PULL) && (g.weight_kind == HYT_WEIGHTS_NONE || g.in_weights.get()) && g.E > 0) {
+            std::vector<uint32_t> pb(parts + 1);
+            shard_bounds(g, HYT_SHARD_PULL, parts, pb.data());
+            sh.pull_edges = pull_tasks(g, pb[part], pb[part + 1], sh);
+            sh.pull_ok = true;
+        }
     } else {
         fail(HYT_E_INVALID, "shard kind must be HYT_SHARD_PULL or HYT_SHARD_PUSH");
     }
@@ -498,26 +686,75 @@ void shard_sssp_init(ShardImpl &sh, const hyt_shard_sssp &p) {
     HYT_CUDA(cudaGetLastError());
 }
 
-void shard_sssp_round(ShardImpl &sh, const hyt_shard_sssp &p) {
+namespace {
+
+void check_ss_args(const ShardImpl &sh, const hyt_shard_sssp &p) {
     if (sh.kind != HYT_SHARD_PUSH) fail(HYT_E_INVALID, "SSSP runs on push shards");
     if (!p.keys) fail(HYT_E_INVALID, "shard SSSP keys must be a non-NULL device pointer");
-    GraphImpl &g = *sh.g;
+}
+
+int pull_grid_for(const void *fn) {
+    int per_sm = 0;
+    HYT_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kPRSmemMax)));
+    HYT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kPRThreads, kPRSmemMax));
+    return sm_count() * std::max(per_sm, 1);
+}
+
+template <int WK>
+void launch_relax(const ShardImpl &sh, const SSShard &a, cudaStream_t s) {
+    shard_sssp_expand_kernel<WK><<<static_cast<unsigned>(sm_count()) * 8u, 256, 0, s>>>(a);
+    HYT_CUDA(cudaGetLastError());
+    if (!a.pull_div) return;
+    const SSPull p = pull_view(sh);
+    const uint64_t tasks = (p.chunk_end - p.chunk_begin) + (p.tile_end - p.tile_begin);
+    if (tasks == 0) return;
+    static const int full = pull_grid_for(reinterpret_cast<const void *>(shard_sssp_pull_kernel<WK>));
+    const uint64_t want = (tasks + kPRThreads / 32 - 1) / (kPRThreads / 32);
+    const int grid = static_cast<int>(std::min<uint64_t>(full, want));
+    shard_sssp_pull_kernel<WK><<<grid, kPRThreads, pr_shared_bytes(p.num_hot, p.tile_cost), s>>>(a, p);
+    HYT_CUDA(cudaGetLastError());
+}
+
+}  // namespace
+
+void shard_sssp_collect(ShardImpl &sh, const hyt_shard_sssp &p) {
+    check_ss_args(sh, p);
     const cudaStream_t s = stream_of(sh, p.stream);
     HYT_CUDA(cudaMemsetAsync(sh.ctr.get(), 0, 2 * sizeof(unsigned long long), s));
+    HYT_CUDA(cudaMemsetAsync(sh.ctr.get() + 3, 0, sizeof(unsigned long long), s));
     const SSShard a = sssp_view(sh, p.keys);
     const uint64_t n = sh.ve - sh.vb;
     if (n) {
         shard_sssp_collect_kernel<<<grid_for(n, 256, 148 * 16), 256, 0, s>>>(a);
         HYT_CUDA(cudaGetLastError());
     }
-    const unsigned grid = static_cast<unsigned>(sm_count()) * 8u;
+    if (p.frontier_edges)
+        HYT_CUDA(cudaMemcpyAsync(p.frontier_edges, sh.ctr.get() + 3, sizeof(int64_t), cudaMemcpyDeviceToDevice, s));
+}
+
+// Pull sweeps need one decision for all shards: the caller's summed
+// frontier count, or a single shard deciding alone.
+void shard_sssp_relax(ShardImpl &sh, const hyt_shard_sssp &p) {
+    check_ss_args(sh, p);
+    GraphImpl &g = *sh.g;
+    const cudaStream_t s = stream_of(sh, p.stream);
+    SSShard a = sssp_view(sh, p.keys);
+    if (p.frontier_edges) a.frontier = reinterpret_cast<const unsigned long long *>(p.frontier_edges);
+    const bool shared_decision = p.frontier_edges != nullptr || sh.parts == 1;
+    a.pull_div = (sh.pull_ok && shared_decision) ? kShardPullDiv : 0u;
     switch (g.weight_kind) {
-        case HYT_WEIGHTS_NONE: shard_sssp_expand_kernel<HYT_WEIGHTS_NONE><<<grid, 256, 0, s>>>(a); break;
-        case HYT_WEIGHTS_U32: shard_sssp_expand_kernel<HYT_WEIGHTS_U32><<<grid, 256, 0, s>>>(a); break;
-        case HYT_WEIGHTS_F32: shard_sssp_expand_kernel<HYT_WEIGHTS_F32><<<grid, 256, 0, s>>>(a); break;
+        case HYT_WEIGHTS_NONE: launch_relax<HYT_WEIGHTS_NONE>(sh, a, s); break;
+        case HYT_WEIGHTS_U32: launch_relax<HYT_WEIGHTS_U32>(sh, a, s); break;
+        case HYT_WEIGHTS_F32: launch_relax<HYT_WEIGHTS_F32>(sh, a, s); break;
         default: fail(HYT_E_INTERNAL, "unknown weight kind");
     }
-    HYT_CUDA(cudaGetLastError());
+}
+
+void shard_sssp_round(ShardImpl &sh, const hyt_shard_sssp &p) {
+    hyt_shard_sssp q = p;
+    q.frontier_edges = nullptr;
+    shard_sssp_collect(sh, q);
+    shard_sssp_relax(sh, q);
 }
 
 void shard_sssp_labels(ShardImpl &sh, const int32_t *keys, uint32_t *out, void *stream) {
@@ -635,6 +872,20 @@ int hyt_shard_sssp_init(hyt_shard *shard, const hyt_shard_sssp *args) {
     return guarded([&] {
         if (!args) fail(HYT_E_INVALID, "args is NULL");
         shard_sssp_init(shard_impl(shard), *args);
+    });
+}
+
+int hyt_shard_sssp_collect(hyt_shard *shard, const hyt_shard_sssp *args) {
+    return guarded([&] {
+        if (!args) fail(HYT_E_INVALID, "args is NULL");
+        shard_sssp_collect(shard_impl(shard), *args);
+    });
+}
+
+int hyt_shard_sssp_relax(hyt_shard *shard, const hyt_shard_sssp *args) {
+    return guarded([&] {
+        if (!args) fail(HYT_E_INVALID, "args is NULL");
+        shard_sssp_relax(shard_impl(shard), *args);
     });
 }
 

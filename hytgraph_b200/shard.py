@@ -11,10 +11,13 @@ sums the (L1 change, dangling mass) pair, so every process takes the same
 stop decision as the single-GPU solver (residual <= tolerance, or the
 iteration cap).
 
-SSSP, per round: every process expands its improved vertices into its copy
-of the key vector (label XOR 0x80000000 as int32), then one MIN all-reduce
-over V + 1 words merges the copies and the idle flags; the solve ends in
-the first round in which no shard expanded anything.  Labels are
+SSSP, per round: every process collects its improved vertices and one
+all-reduce sums their out-edges; when that frontier is dense (more than
+E / 4 out-edges, the single-GPU rule) every process sweeps its rows over
+the CSC (pull), else it pushes its frontier's out-edges into its copy of
+the key vector (label XOR 0x80000000 as int32).  One MIN all-reduce over
+V + 1 words then merges the copies and the idle flags; the solve ends in
+the first round in which no shard had a frontier.  Labels are
 bit-identical to the single-GPU solver.
 
 The kernels sit behind a small interface (``CudaShardKernels`` is the
@@ -124,16 +127,24 @@ class CudaShardKernels:
         return out
 
     # -- SSSP ----------------------------------------------------------------
-    def _ss_args(self, keys, source: int = 0) -> capi.hyt_shard_sssp:
-        return capi.hyt_shard_sssp(_ptr(keys), int(source), 0, self._stream())
+    def _ss_args(self, keys, source: int = 0, frontier=None) -> capi.hyt_shard_sssp:
+        return capi.hyt_shard_sssp(_ptr(keys), int(source), 0, self._stream(), _ptr(frontier) or None)
 
     def sssp_init(self, keys, source: int) -> None:
         a = self._ss_args(keys, source)
         check(lib.hyt_shard_sssp_init(self._shard(capi.HYT_SHARD_PUSH), C.byref(a)))
 
-    def sssp_round(self, keys) -> None:
-        a = self._ss_args(keys)
-        check(lib.hyt_shard_sssp_round(self._shard(capi.HYT_SHARD_PUSH), C.byref(a)))
+    def sssp_collect(self, keys, frontier) -> None:
+        """This shard's frontier of the round; its out-edge count into
+        frontier (int64 [1])."""
+        a = self._ss_args(keys, frontier=frontier)
+        check(lib.hyt_shard_sssp_collect(self._shard(capi.HYT_SHARD_PUSH), C.byref(a)))
+
+    def sssp_relax(self, keys, frontier) -> None:
+        """Push (or, when the summed frontier count in `frontier` is dense,
+        pull-sweep) relaxations into keys; keys[V] = this shard's idle flag."""
+        a = self._ss_args(keys, frontier=frontier)
+        check(lib.hyt_shard_sssp_relax(self._shard(capi.HYT_SHARD_PUSH), C.byref(a)))
 
     def sssp_labels(self, keys, out=None):
         out = np.empty(self.num_vertices, np.uint32) if out is None else out
@@ -253,11 +264,14 @@ class ShardedGraph:
         V = self.num_vertices
         cap = int(max_rounds) if max_rounds else min(4 * V + 1024, 0x7FFFFFFF)
         keys = k.empty(V + 1, torch.int32)
+        frontier = k.empty(1, torch.int64)
         t0 = time.perf_counter()
         k.sssp_init(keys, source)
         rounds, converged = 0, False
         while rounds < cap:
-            k.sssp_round(keys)
+            k.sssp_collect(keys, frontier)
+            self._sum(frontier)  # one push / pull decision for all shards
+            k.sssp_relax(keys, frontier)
             self._min(keys)
             rounds += 1
             if int(keys[V].item()) == 1:
@@ -268,7 +282,7 @@ class ShardedGraph:
         bounds = k.bounds(capi.HYT_SHARD_PUSH)
         return labels, {"iterations": rounds, "converged": int(converged), "ms": ms, "part": self.part,
                         "parts": self.parts, "vertex_begin": bounds[self.part], "vertex_end": bounds[self.part + 1],
-                        "exchanged_bytes": 4 * (V + 1) * rounds if self.dist else 0}
+                        "exchanged_bytes": (4 * (V + 1) + 8) * rounds if self.dist else 0}
 
     def close(self) -> None:
         close = getattr(self.kernels, "close", None)

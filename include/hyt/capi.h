@@ -719,15 +719,28 @@ typedef struct hyt_shard_sssp {
     uint32_t source;  /* the caller's vertex id */
     uint32_t pad;
     void *stream;     /* NULL: the graph's stream */
+    int64_t *frontier_edges; /* device [1] or NULL: out-edges of the round's frontier, summed over shards by the caller */
 } hyt_shard_sssp;
 
 /* keys: every label infinite (HYT_DIST_INF_U32, +inf bits for F32 weights)
  * except the source's 0; the shard forgets what it expanded. */
 int hyt_shard_sssp_init(hyt_shard *shard, const hyt_shard_sssp *args);
-/* One round: expands the owned vertices whose label dropped since their
- * last expansion into keys (atomic min) and sets keys[V] = 1 when there
- * were none, else 0.  The caller then min-reduces keys[0..V] over all
- * shards and stops when keys[V] is 1.  Asynchronous on the stream. */
+/* One round, in two calls around one small exchange:
+ *   hyt_shard_sssp_collect: the owned vertices whose label dropped since
+ *     their last expansion form this shard's frontier; their out-edge count
+ *     goes to *frontier_edges;
+ *   (caller: sum-reduce frontier_edges over all shards)
+ *   hyt_shard_sssp_relax: when the summed count exceeds E / 4 every shard
+ *     runs a pull sweep over its rows of the PULL bounds (graphs created
+ *     with PULL as well), else it pushes its frontier's out-edges into keys
+ *     (atomic min); keys[V] = 1 when this shard's frontier was empty, else 0.
+ * The caller then min-reduces keys[0..V] over all shards and stops when
+ * keys[V] is 1.  Without frontier_edges a shard decides alone, which only
+ * a single shard may do (with several, relax then never sweeps).
+ * hyt_shard_sssp_round = collect + relax, deciding alone.  Asynchronous on
+ * the stream. */
+int hyt_shard_sssp_collect(hyt_shard *shard, const hyt_shard_sssp *args);
+int hyt_shard_sssp_relax(hyt_shard *shard, const hyt_shard_sssp *args);
 int hyt_shard_sssp_round(hyt_shard *shard, const hyt_shard_sssp *args);
 /* u32 labels (caller's vertex order) of keys[0..V) into out [V]: host or device. */
 int hyt_shard_sssp_labels(hyt_shard *shard, const int32_t *keys, uint32_t *out, void *stream);

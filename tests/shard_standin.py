@@ -24,6 +24,8 @@ class NumpyShardKernels:
         src = np.repeat(np.arange(V, dtype=np.uint32), np.diff(self.off).astype(np.int64))
         order = np.argsort(self.cols, kind="stable")
         self.in_src = src[order]
+        self.in_w = None if self.w is None else self.w[order]
+        self.in_dst = self.cols[order]
         self.in_off = np.concatenate([[0], np.cumsum(np.bincount(self.cols, minlength=V))]).astype(np.uint64)
         self.out_deg = np.diff(self.off).astype(np.uint32)
         self.prev = None
@@ -108,22 +110,38 @@ class NumpyShardKernels:
         lo, hi = self._range(PUSH)
         self.prev = np.full(hi - lo, INF, np.uint32)
 
-    def sssp_round(self, keys) -> None:
+    def sssp_collect(self, keys, frontier) -> None:
         V = self.num_vertices
         lo, hi = self._range(PUSH)
-        k = keys.numpy().view(np.uint32)  # shares the tensor's memory
-        lab = k[:V] ^ BIAS
+        lab = keys.numpy().view(np.uint32)[:V] ^ BIAS
         own = lab[lo:hi].copy()
         act = np.nonzero(own < self.prev)[0]
         self.prev[act] = own[act]
-        for i in act:
-            v = lo + int(i)
-            e0, e1 = int(self.off[v]), int(self.off[v + 1])
-            w = np.ones(e1 - e0, np.uint64) if self.w is None else self.w[e0:e1].astype(np.uint64)
-            nd = np.minimum(np.uint64(own[i]) + w, np.uint64(0xFFFFFFFE)).astype(np.uint32)
-            np.minimum.at(lab, self.cols[e0:e1], nd)
+        self._active = (lo + act, own[act])
+        fe = int(self.out_deg[lo + act].astype(np.int64).sum())
+        frontier.copy_(torch.tensor([fe], dtype=torch.int64))
+
+    def sssp_relax(self, keys, frontier) -> None:
+        V, E = self.num_vertices, int(self.cols.shape[0])
+        k = keys.numpy().view(np.uint32)  # shares the tensor's memory
+        lab = k[:V] ^ BIAS
+        verts, labels = self._active
+        if int(frontier[0]) * 4 > E:  # pull sweep over this shard's rows of the PULL bounds
+            plo, phi = self._range(PULL)
+            e0, e1 = int(self.in_off[plo]), int(self.in_off[phi])
+            src = self.in_src[e0:e1]
+            w = np.ones(e1 - e0, np.uint64) if self.in_w is None else self.in_w[e0:e1].astype(np.uint64)
+            du = lab[src].astype(np.uint64)
+            cand = np.where(du == INF, np.uint64(INF), np.minimum(du + w, np.uint64(0xFFFFFFFE))).astype(np.uint32)
+            np.minimum.at(lab, self.in_dst[e0:e1], cand)
+        else:
+            for v, d in zip(verts, labels):
+                e0, e1 = int(self.off[v]), int(self.off[v + 1])
+                w = np.ones(e1 - e0, np.uint64) if self.w is None else self.w[e0:e1].astype(np.uint64)
+                nd = np.minimum(np.uint64(d) + w, np.uint64(0xFFFFFFFE)).astype(np.uint32)
+                np.minimum.at(lab, self.cols[e0:e1], nd)
         k[:V] = lab ^ BIAS
-        k[V] = 0 if act.size else 1
+        k[V] = 0 if verts.size else 1
 
     def sssp_labels(self, keys, out=None) -> np.ndarray:
         lab = keys.numpy().view(np.uint32)[: self.num_vertices] ^ BIAS

@@ -74,13 +74,19 @@ def _push(dg, parts, source):
     ks = [CudaShardKernels(dg, p, parts) for p in range(parts)]
     V = dg.num_vertices
     keys = torch.empty(V + 1, dtype=torch.int32, device="cuda")
+    counts = torch.empty(parts, dtype=torch.int64, device="cuda")
+    total = torch.empty(1, dtype=torch.int64, device="cuda")
     for k in ks:
         k.sssp_init(keys, source)
-    rounds = 0
+    rounds, pulls = 0, 0  # pulls: rounds whose summed frontier asks for a sweep
     while rounds < 4 * V + 1024:
+        for p, k in enumerate(ks):
+            k.sssp_collect(keys, counts[p:p + 1])
+        total.copy_(counts.sum().reshape(1))  # the exchange: one push / pull decision for every shard
+        pulls += int(int(total.item()) * 4 > dg.num_edges)
         idle = True
         for k in ks:
-            k.sssp_round(keys)
+            k.sssp_relax(keys, total)
             idle = idle and int(keys[V].item()) == 1
         rounds += 1
         if idle:
@@ -89,7 +95,7 @@ def _push(dg, parts, source):
     relaxed = sum(k.info(2)["edges_relaxed"] for k in ks)
     for k in ks:
         k.close()
-    return out, rounds, relaxed
+    return out, rounds, relaxed, pulls
 
 
 def test_shard_pagerank_matches_single_gpu(hyt, oracle, gpu):
@@ -120,15 +126,24 @@ def test_shard_ppr_matches_single_gpu(hyt, oracle, gpu):
 
 
 def test_shard_sssp_bit_exact(hyt, oracle, gpu):
+    swept = 0
     for g, flags in _graphs(hyt):
         srcs = hyt.pick_sources(g.row_offsets, 9, 2) if g.num_edges else np.zeros(1, np.uint32)
+        singles = {}
         with hyt.Graph(g, flags=hyt.capi.HYT_GRAPH_ALL | flags) as dg:
             for s in srcs:
                 single, _ = dg.sssp(int(s))
+                singles[int(s)] = single
                 for parts in (1, 2, 3, 5):
-                    d, rounds, relaxed = _push(dg, parts, int(s))
-                    assert np.array_equal(d, single), (g.num_vertices, int(s), parts)
+                    d, rounds, relaxed, pulls = _push(dg, parts, int(s))
+                    assert np.array_equal(d, single), (g.num_vertices, int(s), parts, pulls)
                     assert rounds >= 1 and relaxed >= 0
+                    swept += pulls
+        with hyt.Graph(g, flags=hyt.capi.HYT_GRAPH_PUSH) as dp:  # no CSC: push rounds only
+            s = int(srcs[0])
+            d, _, _, _ = _push(dp, 2, s)
+            assert np.array_equal(d, singles[s])
+    assert swept > 0  # the R-MAT cases reach dense rounds
 
 
 def test_shard_float_weights_and_errors(hyt, gpu):
@@ -142,8 +157,8 @@ def test_shard_float_weights_and_errors(hyt, gpu):
     with hyt.Graph(gf) as dg:
         s = int(hyt.pick_sources(g.row_offsets, 1, 1)[0])
         single, _ = dg.sssp(s)
-        d, _, _ = _push(dg, 3, s)
-        assert np.array_equal(d, single)
+        d, _, _, _ = _push(dg, 3, s)
+        assert np.array_equal(d, single)  # float weights (through the sweeps on dense rounds)
         b = np.zeros(3, np.uint32)
         hyt.capi.check(hyt.capi.lib.hyt_shard_bounds(dg.handle, 1, 2, b.ctypes.data))
         bad = b.copy()
