@@ -15,14 +15,18 @@
 // dangling sums (atomics and the collective, in no fixed order) round
 // differently in their last bits.
 //
-// SSSP (push).  Bellman-Ford rounds over the range's out-rows.  A round
-// expands every owned vertex whose label dropped since it was last expanded
-// and lowers the labels of its out-neighbours in this process's copy of the
-// whole label vector; the caller then min-reduces that vector over all
-// processes.  Labels are held as ordered keys (label XOR 0x80000000 read as
-// int32, so signed order is label order) because collective libraries
-// reduce signed 32-bit integers.  The word after the labels is the idle
-// flag: 1 when the shard expanded nothing this round, so the same min
+// SSSP (push shards).  Bellman-Ford rounds.  A round collects every owned
+// vertex whose label dropped since it was last expanded (the shard's
+// frontier) and counts its out-edges; the caller sums the count over the
+// processes, so all shards take the same choice: a sparse frontier is
+// pushed (its out-edges lower the labels of their heads in this process's
+// copy of the whole label vector), a dense one (more than E / 4 out-edges,
+// as hyt_sssp decides) makes every shard sweep its rows of the PULL bounds
+// over the CSC instead.  The caller then min-reduces the label vector over
+// all processes.  Labels are held as ordered keys (label XOR 0x80000000
+// read as int32, so signed order is label order) because collective
+// libraries reduce signed 32-bit integers.  The word after the labels is
+// the idle flag: 1 when the shard's frontier was empty, so the same min
 // reduction tells every process whether any shard still had work.  The
 // fixed point is the unique shortest-path labelling, so the labels are
 // bit-identical to hyt_sssp.
