@@ -162,3 +162,54 @@ def test_sharded_argument_errors():
     assert st["iterations"] == 1
     with pytest.raises(ValueError):
         hyt.ShardedGraph()
+
+
+def _group_main(rank: int, world: int, port: int, seed: int, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    import datetime
+
+    sys.path.insert(0, str(ROOT))
+    sys.path.insert(0, str(ROOT / "tests"))
+    from shard_standin import NumpyShardKernels
+
+    from hytgraph_b200.shard import ShardedGraph
+
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    try:
+        groups = [dist.new_group([0, 1]), dist.new_group([2, 3])]  # every rank creates every group
+        group = groups[rank // 2]
+        off, cols, w = _graph(seed)
+        part, parts = dist.get_rank(group), dist.get_world_size(group)
+        sg = ShardedGraph(group=group, kernels=NumpyShardKernels(off, cols, w, part, parts))
+        r, st = sg.pagerank()
+        d, _ = sg.sssp(7)
+        out[rank] = (r, st["part"], st["parts"], d)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_solves_inside_subgroups(oracle):
+    """Four processes as two independent two-shard solves (process groups
+    {0, 1} and {2, 3}): slice owners are addressed by their global ranks."""
+    seed = 11
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as m:
+        out = m.dict()
+        port = _free_port()
+        procs = [ctx.Process(target=_group_main, args=(r, 4, port, seed, out)) for r in range(4)]
+        for p in procs:
+            p.start()
+        for p in procs:
+            p.join(300)
+            assert p.exitcode == 0
+        res = dict(out)
+    off, cols, w = _graph(seed)
+    ref, _, _, _ = oracle.pagerank_f64(off, cols)
+    want, _, _ = oracle.sssp(off, cols, w.astype(np.float32), 7)
+    fin = np.isfinite(want)
+    want = np.where(fin, np.where(fin, want, 0).astype(np.uint64), 0xFFFFFFFF).astype(np.uint32)
+    assert [(res[r][1], res[r][2]) for r in range(4)] == [(0, 2), (1, 2), (0, 2), (1, 2)]
+    for r in range(4):
+        assert np.array_equal(res[r][0].view(np.uint32), res[0][0].view(np.uint32))
+        assert float(np.abs(res[r][0].astype(np.float64) - ref).sum()) <= L1_TOL
+        assert np.array_equal(res[r][3], want)
