@@ -289,10 +289,13 @@ def run_reference_arm(args, rank, pg):
     sample = (f"per step: 1 PageRank iteration + 1 SSSP round of the reference's pagerank_cpu/sssp_cpu "
               f"(each incl. its incoming-CSR build) on the full R-MAT s{args.scale} ef{args.edge_factor} graph; "
               f"E per iteration/round counted")
-    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/u32",
-            "data": "synthetic", "config": workload_config(args, int(off.shape[0] - 1), int(cols.shape[0])),
+    V, E = int(off.shape[0] - 1), int(cols.shape[0])
+    shard = args.workload == "shard"  # the same CPU work; the shard arm's metric and config
+    line = {"impl": "reference", "metric": SHARD_METRIC if shard else METRIC, "value": value, "unit": UNIT,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+            "higher_is_better": True, "scaling": "strong" if shard else "weak", "vs_baseline": None,
+            "dtype": "f32/u32", "data": "synthetic",
+            "config": shard_config(args, V, E, args.gpus) if shard else workload_config(args, V, E),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": kind, "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -1300,14 +1303,11 @@ def run_shard_workload(args, rank, world, local, pg):
     e2e_ms = max_over_ranks(pg, 1e3 * (time.perf_counter() - t0))
     e2e_value = (E * e2e_it + E * len(sources) * args.e2e_steps) / (e2e_ms / 1e3) / 1e9
     if rank == 0:
-        line = {"metric": "PR/SSSP GTEPS on one graph split over the ranks", "value": value, "unit": UNIT,
+        line = {"metric": SHARD_METRIC, "value": value, "unit": UNIT,
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
                 "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
                 "dtype": "f32 (PageRank) / u32 (SSSP)", "data": "synthetic",
-                "config": dict(workload_config(args, V, E), parallelism=f"vertex-range shards x{world} (NCCL)",
-                               workload=f"one R-MAT scale {args.scale} edge factor {args.edge_factor} graph split "
-                                        f"by vertex range: PageRank to L1<=1e-6 + SSSP from {args.sources} "
-                                        f"seeded sources"),
+                "config": shard_config(args, V, E, world),
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": (V + 1) * 8 + 8 * E,
                         "d2h_bytes_per_step": 4 * V * (1 + len(sources)), "ms_per_step": e2e_ms / args.e2e_steps,
                         "steps": args.e2e_steps},
@@ -1321,6 +1321,15 @@ def run_shard_workload(args, rank, world, local, pg):
                                 "pull_edges": pull["edges"], "push_vertices": push["vertex_end"] - push["vertex_begin"],
                                 "push_edges": push["edges"]}}
         print(json.dumps(line), flush=True)
+
+
+SHARD_METRIC = "PR/SSSP GTEPS on one graph split over the ranks"
+
+
+def shard_config(args, V, E, world):
+    return dict(workload_config(args, V, E), parallelism=f"vertex-range shards x{world} (NCCL)",
+                workload=f"one R-MAT scale {args.scale} edge factor {args.edge_factor} graph split by vertex "
+                         f"range: PageRank to L1<=1e-6 + SSSP from {args.sources} seeded sources")
 
 
 def workload_config(args, V, E):
