@@ -100,7 +100,9 @@ def test_sharded_solves_match_the_oracle(world, oracle):
         assert float(np.abs(r.astype(np.float64) - ref).sum()) <= L1_TOL
         assert st["iterations"] == res[0]["pr"][1]["iterations"]
         assert abs(st["iterations"] - it_ref) <= 1 and st["converged"] == conv_ref
-        assert st["parts"] == world and st["part"] == rank and st["exchanged_bytes"] > 0
+        assert st["parts"] == world and st["part"] == rank
+        V = off.shape[0] - 1  # one contribution vector per iteration + the final ranks
+        assert st["exchanged_bytes"] == 4 * V * (st["iterations"] + 1)
         ranges.add((st["vertex_begin"], st["vertex_end"]))
     # the ranges tile [0, V)
     b = sorted(ranges)
