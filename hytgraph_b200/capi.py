@@ -70,6 +70,8 @@ class hyt_graph_info(C.Structure):
         ("max_out_degree", C.c_uint64),
         ("dangling_vertices", C.c_uint64),
         ("build_ms", C.c_double),
+        ("device", C.c_int32),
+        ("pad", C.c_uint32),
     ]
 
 

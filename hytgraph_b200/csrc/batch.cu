@@ -1044,6 +1044,7 @@ int hyt_batch_create(hyt_graph *const *graphs, uint32_t num_graphs, const hyt_ba
         if (!graphs || num_graphs == 0) fail(HYT_E_INVALID, "a batch needs at least one graph");
         hyt_batch_options o{};
         if (options) o = *options;
+        o.device = resolve_device(o.device);
         auto b = std::make_unique<hyt_batch>();
         b->device = o.device;
         for (uint32_t i = 0; i < num_graphs; ++i) {

@@ -161,6 +161,7 @@ int hyt_graph_create(const hyt_csr *csr, const hyt_graph_options *options, hyt_g
         require_device();
         hyt_graph_options opt{};
         if (options) opt = *options;
+        opt.device = resolve_device(opt.device);
         auto *g = new hyt_graph();
         try {
             g->impl.device = opt.device;
@@ -210,6 +211,7 @@ int hyt_graph_get_info(const hyt_graph *graph, hyt_graph_info *out) {
         out->max_out_degree = g.max_out_degree;
         out->dangling_vertices = g.dangling;
         out->build_ms = g.build_ms;
+        out->device = g.device;
     });
 }
 

@@ -215,6 +215,15 @@ struct EventTimer {
 
 int sm_count();
 
+// A negative device ordinal in creation options selects the calling
+// thread's current device.
+inline int resolve_device(int device) {
+    if (device >= 0) return device;
+    int cur = 0;
+    HYT_CUDA(cudaGetDevice(&cur));
+    return cur;
+}
+
 inline unsigned grid_for(size_t n, unsigned block, unsigned cap = 148u * 32u) {
     size_t g = (n + block - 1) / block;
     if (g == 0) g = 1;

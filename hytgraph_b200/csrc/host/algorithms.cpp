@@ -43,6 +43,7 @@ struct DeviceGraph {
         csr.weight_kind = kind;
         hyt_graph_options opt{};
         opt.flags = flags;
+        opt.device = -1;  // the calling thread's current device, as the reference's solvers use
         check(hyt_graph_create(&csr, &opt, &g), entry);
     }
     ~DeviceGraph() {

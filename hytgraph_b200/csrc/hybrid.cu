@@ -670,8 +670,8 @@ HybridImpl *impl(hyt_hybrid *x) {
 HybridImpl *hybrid_create(const hyt_csr *csr, const hyt_csc *csc, const hyt_hybrid_options &o) {
     auto h = std::make_unique<HybridImpl>();
     GraphImpl &g = h->g;
-    g.device = o.device;
-    HYT_CUDA(cudaSetDevice(o.device));
+    g.device = resolve_device(o.device);
+    HYT_CUDA(cudaSetDevice(g.device));
     HYT_CUDA(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
     g.own_stream = true;
     g.host_scratch.allocate(64);

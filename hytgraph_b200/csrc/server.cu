@@ -191,6 +191,7 @@ int hyt_server_create(hyt_graph *const *graphs, uint32_t num_graphs, const hyt_s
         if (!graphs || num_graphs == 0) fail(HYT_E_INVALID, "a server needs at least one graph");
         hyt_server_options o{};
         if (options) o = *options;
+        o.device = resolve_device(o.device);
         auto sv = std::make_unique<hyt_server>();
         ServerImpl &s = sv->impl;
         s.device = o.device;

@@ -169,14 +169,16 @@ def pick_sources(row_offsets: np.ndarray, seed: int, count: int) -> np.ndarray:
 class Graph:
     """Device-resident graph (hyt_graph handle)."""
 
-    def __init__(self, csr, flags: int = capi.HYT_GRAPH_ALL, device: int = 0, stream: int = 0):
+    def __init__(self, csr, flags: int = capi.HYT_GRAPH_ALL, device: Optional[int] = None, stream: int = 0):
+        """device: CUDA ordinal; None = the calling thread's current device
+        (the one torch.cuda.set_device chose, as one process per GPU needs)."""
         self._csr_ref = csr  # keep host arrays alive during creation
-        opts = capi.hyt_graph_options(flags, device, stream or None)
+        opts = capi.hyt_graph_options(flags, -1 if device is None else device, stream or None)
         c = csr.to_c()
         h = C.c_void_p()
         check(lib.hyt_graph_create(C.byref(c), C.byref(opts), C.byref(h)))
         self._h = h
-        self.device = int(device)
+        self.device = int(self.info()["device"])
         self.num_vertices = int(c.num_vertices)
         self.num_edges = int(c.num_edges)
         self._csr_ref = None
@@ -306,7 +308,7 @@ class HybridGraph:
     PinnedBuffer objects (used in place); they must outlive the handle."""
 
     def __init__(self, row_offsets, column_indices, weights=None, in_offsets=None, in_sources=None,
-                 flags: int = capi.HYT_GRAPH_ALL, device: int = 0, budget_bytes: int = 0,
+                 flags: int = capi.HYT_GRAPH_ALL, device: Optional[int] = None, budget_bytes: int = 0,
                  partition_vertices: int = 0, host_threads: int = 0, force_engine: int = capi.HYT_ENGINE_AUTO,
                  alpha: float = 0.0, beta: float = 0.0, gamma: float = 0.0):
         def pin(x):
@@ -323,7 +325,8 @@ class HybridGraph:
         cc = None
         if ioff is not None:
             cc = capi.hyt_csc(V, isrc.count, ioff.data_ptr(), isrc.data_ptr())
-        opts = capi.hyt_hybrid_options(flags, device, budget_bytes, partition_vertices, host_threads, force_engine,
+        opts = capi.hyt_hybrid_options(flags, -1 if device is None else device, budget_bytes, partition_vertices,
+                                       host_threads, force_engine,
                                        alpha, beta, gamma)
         h = C.c_void_p()
         check(lib.hyt_hybrid_create(C.byref(c), C.byref(cc) if cc is not None else None, C.byref(opts),
@@ -387,9 +390,11 @@ class Batch:
     restart, tolerance, max_iterations, out (an array to receive the result;
     by default a numpy array is allocated per query)."""
 
-    def __init__(self, graphs, device: int = 0, state_budget_bytes: int = 0, delta_mult: int = 0,
+    def __init__(self, graphs, device: Optional[int] = None, state_budget_bytes: int = 0, delta_mult: int = 0,
                  hub_degree: int = 0, ctas_per_sm: int = 0, flags: int = 0):
         self._graphs = list(graphs)  # keep the graph handles alive
+        if device is None:  # the graphs' device
+            device = self._graphs[0].device if self._graphs else -1
         arr = (C.c_void_p * len(self._graphs))(*[g.handle.value for g in self._graphs])
         opts = capi.hyt_batch_options(device, state_budget_bytes,
                                       capi.hyt_batch_tuning(delta_mult, hub_degree, ctas_per_sm), flags)
@@ -465,9 +470,11 @@ class Server:
     any thread, poll() for completions.  A query's `out` array must stay
     alive until its completion has been polled."""
 
-    def __init__(self, graphs, device: int = 0, state_budget_bytes: int = 0, delta_mult: int = 0,
+    def __init__(self, graphs, device: Optional[int] = None, state_budget_bytes: int = 0, delta_mult: int = 0,
                  hub_degree: int = 0, ctas_per_sm: int = 0, max_running: int = 0):
         self._graphs = list(graphs)
+        if device is None:  # the graphs' device
+            device = self._graphs[0].device if self._graphs else -1
         arr = (C.c_void_p * len(self._graphs))(*[g.handle.value for g in self._graphs])
         opts = capi.hyt_server_options(device, state_budget_bytes,
                                        capi.hyt_batch_tuning(delta_mult, hub_degree, ctas_per_sm), max_running)

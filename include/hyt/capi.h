@@ -105,7 +105,7 @@ enum hyt_graph_flags {
 
 typedef struct hyt_graph_options {
     uint32_t flags;  /* HYT_GRAPH_* (0 = HYT_GRAPH_ALL) */
-    int device;      /* CUDA device ordinal */
+    int device;      /* CUDA device ordinal; < 0: the calling thread's current device */
     void *stream;    /* cudaStream_t used for the upload (NULL = own) */
 } hyt_graph_options;
 
@@ -128,6 +128,8 @@ typedef struct hyt_graph_info {
     uint64_t max_out_degree;
     uint64_t dangling_vertices; /* out-degree 0 */
     double build_ms;            /* device time of upload + CSC/tile build */
+    int32_t device;             /* CUDA device ordinal the graph lives on */
+    uint32_t pad;
 } hyt_graph_info;
 
 int hyt_graph_create(const hyt_csr *csr, const hyt_graph_options *options,
@@ -279,7 +281,7 @@ enum hyt_engine {
  * degrees, labels, ranks, frontiers) live in HBM outside the budget. */
 typedef struct hyt_hybrid_options {
     uint32_t flags;               /* HYT_GRAPH_* (0 = HYT_GRAPH_ALL) */
-    int device;
+    int device;                   /* < 0: the calling thread's current device */
     uint64_t device_budget_bytes; /* HBM for edge data: resident partitions +
                                      staging (0 = 8 GiB) */
     uint32_t partition_vertices;  /* power of two (0 = 2^20); <= 1024 parts */
@@ -367,7 +369,7 @@ typedef struct hyt_batch_tuning {
 } hyt_batch_tuning;
 
 typedef struct hyt_batch_options {
-    int device;
+    int device;                   /* < 0: the calling thread's current device */
     uint64_t state_budget_bytes;  /* device bytes for per-query state
                                      (0 = 16 GiB); larger batches run in
                                      waves that fit */
@@ -418,7 +420,7 @@ int hyt_batch_set_tuning(hyt_batch *batch, const hyt_batch_tuning *tuning);
 typedef struct hyt_server hyt_server;
 
 typedef struct hyt_server_options {
-    int device;
+    int device;                   /* < 0: the calling thread's current device */
     uint64_t state_budget_bytes;  /* 0 = 16 GiB */
     hyt_batch_tuning tuning;
     uint32_t max_running;         /* cap on concurrently running queries
