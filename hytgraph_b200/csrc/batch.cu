@@ -10,6 +10,7 @@
 
 #include "batch.cuh"
 #include "common.cuh"
+#include "host_checks.hpp"
 #include "graph.cuh"
 #include "pagerank_core.cuh"
 #include "sssp_core.cuh"
@@ -1042,8 +1043,7 @@ int hyt_batch_create(hyt_graph *const *graphs, uint32_t num_graphs, const hyt_ba
         if (!out) fail(HYT_E_INVALID, "out is NULL");
         *out = nullptr;
         if (!graphs || num_graphs == 0) fail(HYT_E_INVALID, "a batch needs at least one graph");
-        hyt_batch_options o{};
-        if (options) o = *options;
+        hyt_batch_options o = options_or_default(options);
         o.device = resolve_device(o.device);
         auto b = std::make_unique<hyt_batch>();
         b->device = o.device;

@@ -6,6 +6,7 @@
 #include <string>
 
 #include "common.cuh"
+#include "host_checks.hpp"
 #include "scratch.cuh"
 #include "graph.cuh"
 #include "solvers.cuh"
@@ -45,6 +46,19 @@ bool is_device_pointer(const void *p) {
         return false;
     }
     return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+}
+
+PointerPlace pointer_place(const void *p, int current_device, int *pointer_device) {
+    if (pointer_device) *pointer_device = -1;
+    if (!p) return PointerPlace::kHost;
+    cudaPointerAttributes attr{};
+    const cudaError_t e = cudaPointerGetAttributes(&attr, p);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        return PointerPlace::kHost;
+    }
+    if (pointer_device) *pointer_device = attr.device;
+    return classify_pointer(attr.type, attr.device, current_device);
 }
 
 void copy_to_device(void *dst, const void *src, size_t bytes, cudaStream_t s) {
@@ -159,8 +173,7 @@ int hyt_graph_create(const hyt_csr *csr, const hyt_graph_options *options, hyt_g
         if (!csr || !out) fail(HYT_E_INVALID, "csr/out is NULL");
         *out = nullptr;
         require_device();
-        hyt_graph_options opt{};
-        if (options) opt = *options;
+        hyt_graph_options opt = options_or_default(options);
         opt.device = resolve_device(opt.device);
         auto *g = new hyt_graph();
         try {

@@ -187,6 +187,12 @@ struct PinnedArray {
 // True when `p` is device (or managed) memory on some GPU.
 bool is_device_pointer(const void *p);
 
+enum class PointerPlace;
+// Where `p` lives relative to `current_device` (host_checks.hpp);
+// *pointer_device receives the ordinal cudaPointerGetAttributes reports
+// (-1 when it reports none).
+PointerPlace pointer_place(const void *p, int current_device, int *pointer_device);
+
 // Copies `bytes` from src (host or device) into device memory dst.
 void copy_to_device(void *dst, const void *src, size_t bytes, cudaStream_t s);
 // Copies `bytes` from device memory src into dst (host or device).

@@ -50,6 +50,8 @@ CSRGraph::weight_type CSRGraph::weight_at(offset_type edge_index) const {
 void CSRGraph::validate() const {
     if (row_offsets_.size() != static_cast<std::size_t>(num_vertices_) + 1U)
         throw std::invalid_argument("CSRGraph::validate: row_offsets must contain num_vertices + 1 entries");
+    // num_vertices == UINT64_MAX wraps the expected size to 0 above
+    if (row_offsets_.empty()) throw std::invalid_argument("CSRGraph::validate: row_offsets must not be empty");
     if (row_offsets_.front() != 0) throw std::invalid_argument("CSRGraph::validate: first row offset must be zero");
     if (std::adjacent_find(row_offsets_.begin(), row_offsets_.end(),
                            [](offset_type a, offset_type b) { return b < a; }) != row_offsets_.end())

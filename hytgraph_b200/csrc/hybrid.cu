@@ -32,6 +32,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "host_checks.hpp"
 #include "graph.cuh"
 #include "hybrid.cuh"
 #include "solvers.cuh"
@@ -842,8 +843,7 @@ int hyt_hybrid_create(const hyt_csr *csr, const hyt_csc *csc, const hyt_hybrid_o
             (void)cudaGetLastError();
             fail(HYT_E_NO_DEVICE, "no CUDA device is available");
         }
-        hyt_hybrid_options o{};
-        if (options) o = *options;
+        hyt_hybrid_options o = options_or_default(options);
         *out = reinterpret_cast<hyt_hybrid *>(hybrid_create(csr, csc, o));
     });
 }

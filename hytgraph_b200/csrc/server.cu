@@ -26,6 +26,7 @@
 
 #include "batch.cuh"
 #include "common.cuh"
+#include "host_checks.hpp"
 #include "graph.cuh"
 
 namespace hyt {
@@ -189,8 +190,7 @@ int hyt_server_create(hyt_graph *const *graphs, uint32_t num_graphs, const hyt_s
         if (!out) fail(HYT_E_INVALID, "out is NULL");
         *out = nullptr;
         if (!graphs || num_graphs == 0) fail(HYT_E_INVALID, "a server needs at least one graph");
-        hyt_server_options o{};
-        if (options) o = *options;
+        hyt_server_options o = options_or_default(options);
         o.device = resolve_device(o.device);
         auto sv = std::make_unique<hyt_server>();
         ServerImpl &s = sv->impl;

@@ -35,9 +35,11 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <utility>
 
 #include "common.cuh"
 #include "graph.cuh"
+#include "host_checks.hpp"
 #include "hybrid.cuh"
 #include "solvers.cuh"
 #include "sssp_core.cuh"
@@ -906,11 +908,28 @@ void sssp_noalloc(const hyt_csr &csr, uint32_t source, uint32_t *dist_out, void 
                                 std::to_string(kNoAllocMaxEdges) + " edges); use hyt_sssp for larger graphs");
     if (source >= V) fail(HYT_E_INVALID, "SSSP source vertex is out of range");
     if (csr.weight_kind > HYT_WEIGHTS_F32) fail(HYT_E_INVALID, "unknown weight_kind");
-    if (!is_device_pointer(csr.row_offsets) || (E && !is_device_pointer(csr.column_indices)) ||
-        (E && csr.weight_kind != HYT_WEIGHTS_NONE && !is_device_pointer(csr.weights)) || !is_device_pointer(dist_out))
-        fail(HYT_E_INVALID, "hyt_sssp_noalloc: the CSR arrays and dist_out must be device memory of the current device");
     int device = 0;
     HYT_CUDA(cudaGetDevice(&device));
+    // Every array is dereferenced by kernels on the current device: host
+    // memory and another GPU's memory are refused before any launch
+    // (column_indices and weights are read only when there are edges).
+    const bool edges = E > 0, weights = edges && csr.weight_kind != HYT_WEIGHTS_NONE;
+    const std::pair<const void *, const char *> arrays[] = {{csr.row_offsets, "row_offsets"},
+                                                           {csr.column_indices, edges ? "column_indices" : nullptr},
+                                                           {csr.weights, weights ? "weights" : nullptr},
+                                                           {dist_out, "dist_out"}};
+    for (const auto &[ptr, name] : arrays) {
+        if (!name) continue;
+        int owner = -1;
+        const PointerPlace place = pointer_place(ptr, device, &owner);
+        if (place == PointerPlace::kHost)
+            fail(HYT_E_INVALID, std::string("hyt_sssp_noalloc: ") + name +
+                                    " must be device memory of the current device (got host memory)");
+        if (place == PointerPlace::kOtherDevice)
+            fail(HYT_E_INVALID, std::string("hyt_sssp_noalloc: ") + name + " is device memory of GPU " +
+                                    std::to_string(owner) + ", not of the current device " +
+                                    std::to_string(device));
+    }
     unsigned char *scratch = noalloc_scratch(device);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     switch (csr.weight_kind) {

@@ -132,6 +132,8 @@ typedef struct hyt_graph_info {
     uint32_t pad;
 } hyt_graph_info;
 
+/* NULL options: all defaults, with the calling thread's current device
+ * (device ordinal -1); the current device is left unchanged. */
 int hyt_graph_create(const hyt_csr *csr, const hyt_graph_options *options,
                      hyt_graph **out);
 int hyt_graph_destroy(hyt_graph *graph);
@@ -321,6 +323,8 @@ typedef struct hyt_hybrid_stats {
     double h2d_peak_gbs;        /* measured pinned-copy peak */
 } hyt_hybrid_stats;
 
+/* NULL options: all defaults, with the calling thread's current device
+ * (device ordinal -1); the current device is left unchanged. */
 int hyt_hybrid_create(const hyt_csr *csr, const hyt_csc *csc, const hyt_hybrid_options *options,
                       hyt_hybrid **out);
 int hyt_hybrid_destroy(hyt_hybrid *hybrid);
@@ -390,7 +394,9 @@ typedef struct hyt_batch_stats {
 
 typedef struct hyt_batch hyt_batch;
 
-/* graphs: handles built with HYT_GRAPH_ALL (borrowed; keep them alive). */
+/* graphs: handles built with HYT_GRAPH_ALL (borrowed; keep them alive).
+ * NULL options: all defaults, with the calling thread's current device
+ * (device ordinal -1); the current device is left unchanged. */
 int hyt_batch_create(hyt_graph *const *graphs, uint32_t num_graphs, const hyt_batch_options *options,
                      hyt_batch **out);
 int hyt_batch_destroy(hyt_batch *batch);
@@ -443,7 +449,9 @@ typedef struct hyt_server_stats {
     double busy_ms;               /* worker time with queries running */
 } hyt_server_stats;
 
-/* graphs: handles built with HYT_GRAPH_ALL (borrowed; keep them alive). */
+/* graphs: handles built with HYT_GRAPH_ALL (borrowed; keep them alive).
+ * NULL options: all defaults, with the calling thread's current device
+ * (device ordinal -1); the current device is left unchanged. */
 int hyt_server_create(hyt_graph *const *graphs, uint32_t num_graphs, const hyt_server_options *options,
                       hyt_server **out);
 /* Thread-safe.  Validates the query (HYT_E_INVALID as hyt_batch_run) and

@@ -1,6 +1,6 @@
 """Regenerates the golden fixtures in this folder from the REFERENCE's own
-compiled CPU code (oracle/_ref/libhytref.so, built by `make -C oracle` from
-the reference sources).
+compiled CPU code (oracle/_ref/libhytref.so, built by
+`make -C oracle REF=<reference checkout>` from the reference sources).
 
     python tests/golden/make_golden.py
 

@@ -18,16 +18,20 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def _device_csr(hyt, g, torch, weighted=True):
-    off = torch.from_numpy(g.row_offsets.view(np.int64)).cuda()
-    cols = torch.from_numpy(g.column_indices.view(np.int32)).cuda()
-    w = torch.from_numpy(g.weights.view(np.int32)).cuda() if weighted else None
+def _device_csr(hyt, off, cols, w, torch):
+    """Device copies of host CSR arrays and the hyt_csr describing them."""
+    d_off = torch.from_numpy(np.ascontiguousarray(off).view(np.int64)).cuda()
+    d_cols = torch.from_numpy(np.ascontiguousarray(cols).view(np.int32)).cuda()
+    d_w = None if w is None else torch.from_numpy(np.ascontiguousarray(w).view(np.int32)).cuda()
     c = hyt.capi.hyt_csr()
-    c.num_vertices, c.num_edges = g.num_vertices, g.num_edges
-    c.row_offsets, c.column_indices = off.data_ptr(), cols.data_ptr()
-    c.weights = w.data_ptr() if weighted else 0
-    c.weight_kind = hyt.capi.HYT_WEIGHTS_U32 if weighted else hyt.capi.HYT_WEIGHTS_NONE
-    return c, (off, cols, w)
+    c.num_vertices, c.num_edges = off.shape[0] - 1, cols.shape[0]
+    c.row_offsets, c.column_indices = d_off.data_ptr(), d_cols.data_ptr()
+    c.weights = 0 if w is None else d_w.data_ptr()
+    if w is None:
+        c.weight_kind = hyt.capi.HYT_WEIGHTS_NONE
+    else:
+        c.weight_kind = hyt.capi.HYT_WEIGHTS_F32 if w.dtype == np.float32 else hyt.capi.HYT_WEIGHTS_U32
+    return c, (d_off, d_cols, d_w)
 
 
 def _noalloc(hyt, csr, source, out):
@@ -36,27 +40,37 @@ def _noalloc(hyt, csr, source, out):
     return rc, st
 
 
-def test_noalloc_matches_the_allocating_entry_point(hyt, gpu):
+def _memory(torch):
+    torch.cuda.synchronize()
+    return torch.cuda.mem_get_info()[0], torch.cuda.memory_reserved()
+
+
+@pytest.mark.parametrize("weights", ["u32", "none", "f32"])
+def test_noalloc_matches_the_allocating_entry_point(hyt, gpu, weights):
     """Two calls in a row (and a repeat of the first) agree bit for bit with
-    hyt_sssp, the allocating entry point; SSSP distances are exact."""
+    hyt_sssp, the allocating entry point (SSSP distances are exact), and no
+    call after the first changes the device's free memory or torch's
+    reserved memory."""
     import torch
 
     g = hyt.rmat(16, 16, 777)
+    w = {"u32": g.weights, "none": None, "f32": g.weights.astype(np.float32) / 4}[weights]
     sources = [int(s) for s in hyt.pick_sources(g.row_offsets, 31, 2)]
-    with hyt.Graph(g) as dg:
+    with hyt.Graph(hyt.CSR(g.row_offsets, g.column_indices, w)) as dg:
         want = [dg.sssp(s)[0] for s in sources]
-    for weighted in (True, False):
-        csr, keep = _device_csr(hyt, g, torch, weighted)
-        if not weighted:
-            with hyt.Graph(hyt.CSR(g.row_offsets, g.column_indices, None)) as dg:
-                want = [dg.sssp(s)[0] for s in sources]
-        for s, ref in zip(sources + sources[:1], want + want[:1]):
-            out = torch.full((g.num_vertices,), 7, dtype=torch.int32, device="cuda")
-            rc, st = _noalloc(hyt, csr, s, out)
-            assert rc == hyt.capi.HYT_OK, hyt.capi.last_error()
-            assert st.converged == 1 and st.iterations > 0
-            assert np.array_equal(out.cpu().numpy().view(np.uint32), ref)
-        del keep
+    csr, keep = _device_csr(hyt, g.row_offsets, g.column_indices, w, torch)
+    outs = [torch.full((g.num_vertices,), 7, dtype=torch.int32, device="cuda") for _ in range(3)]
+    rc, _ = _noalloc(hyt, csr, sources[0], outs[0])  # first call: the library looks up its array
+    assert rc == hyt.capi.HYT_OK, hyt.capi.last_error()
+    before = _memory(torch)
+    for s, ref, out in zip(sources + sources[:1], want + want[:1], outs):
+        out.fill_(7)
+        rc, st = _noalloc(hyt, csr, s, out)
+        assert rc == hyt.capi.HYT_OK, hyt.capi.last_error()
+        assert st.converged == 1 and st.iterations > 0
+        assert np.array_equal(out.cpu().numpy().view(np.uint32), ref)
+    assert _memory(torch) == before, "hyt_sssp_noalloc allocated device memory"
+    del keep
 
 
 def test_noalloc_rejects_graphs_beyond_its_capacity(hyt, gpu):
@@ -78,3 +92,34 @@ def test_noalloc_rejects_graphs_beyond_its_capacity(hyt, gpu):
     out_small = torch.empty(g.num_vertices, dtype=torch.int32, device="cuda")
     rc, _ = _noalloc(hyt, host, 0, out_small)
     assert rc == hyt.capi.HYT_E_INVALID and "device memory" in hyt.capi.last_error()
+
+
+def test_noalloc_rejects_malformed_csr(hyt, gpu):
+    """Malformed offsets, an out-of-range column and a negative float weight
+    are caught on the device before any solver kernel indexes with them."""
+    import torch
+
+    g = hyt.rmat(10, 8, 5)
+    out = torch.empty(g.num_vertices, dtype=torch.int32, device="cuda")
+    bad_off = g.row_offsets.copy()
+    bad_off[5], bad_off[6] = bad_off[6] + 1, bad_off[5]  # a decreasing pair
+    bad_cols = g.column_indices.copy()
+    bad_cols[g.num_edges // 2] = g.num_vertices  # destination out of range
+    bad_w = g.weights.astype(np.float32)
+    bad_w[3] = -1.0
+    cases = [(bad_off, g.column_indices, g.weights, "row offsets"),
+             (g.row_offsets, bad_cols, g.weights, "invalid destination"),
+             (g.row_offsets, g.column_indices, bad_w, "non-negative")]
+    for off, cols, w, msg in cases:
+        csr, keep = _device_csr(hyt, off, cols, w, torch)
+        rc, _ = _noalloc(hyt, csr, 0, out)
+        assert rc == hyt.capi.HYT_E_INVALID, msg
+        assert msg in hyt.capi.last_error()
+        del keep
+    # a valid call right after the rejections still matches hyt_sssp
+    csr, keep = _device_csr(hyt, g.row_offsets, g.column_indices, g.weights, torch)
+    src = int(hyt.pick_sources(g.row_offsets, 3, 1)[0])
+    rc, _ = _noalloc(hyt, csr, src, out)
+    assert rc == hyt.capi.HYT_OK, hyt.capi.last_error()
+    with hyt.Graph(g) as dg:
+        assert np.array_equal(out.cpu().numpy().view(np.uint32), dg.sssp(src)[0])
