@@ -101,6 +101,36 @@ class Oracle:
             raise ValueError(f"oracle_dijkstra_u32 rc={rc}")
         return d
 
+    def rmat(self, scale, edge_factor, seed, weight_min=1, weight_max=63, a=0.57, b=0.19, c=0.19):
+        """Seeded R-MAT CSR (the same bytes as the product's generator):
+        (row_offsets uint64[V+1], column_indices uint32[E], weights uint32[E]
+        or None)."""
+        off_p, cols_p, w_p = C.POINTER(C.c_uint64)(), C.POINTER(C.c_uint32)(), C.POINTER(C.c_uint32)()
+        E = C.c_uint64()
+        rc = self.lib.oracle_rmat(C.c_uint32(scale), C.c_uint32(edge_factor), C.c_uint64(seed), C.c_double(a),
+                                  C.c_double(b), C.c_double(c), C.c_uint32(weight_min), C.c_uint32(weight_max),
+                                  C.byref(off_p), C.byref(cols_p), C.byref(w_p), C.byref(E))
+        if rc:
+            raise ValueError(f"oracle_rmat rc={rc}")
+        V, E = 1 << scale, E.value
+        try:
+            off = np.ctypeslib.as_array(off_p, shape=(V + 1,)).copy()
+            cols = np.ctypeslib.as_array(cols_p, shape=(max(E, 1),))[:E].copy()
+            w = np.ctypeslib.as_array(w_p, shape=(max(E, 1),))[:E].copy() if w_p else None
+        finally:
+            for p in (off_p, cols_p, w_p):
+                if p:
+                    self.lib.oracle_free(p)
+        return off, cols, w
+
+    def pick_sources(self, off, seed, count):
+        out = np.zeros(max(count, 1), np.uint32)
+        rc = self.lib.oracle_pick_sources(_p(np.ascontiguousarray(off, np.uint64)), C.c_uint64(off.shape[0] - 1),
+                                          C.c_uint64(seed), C.c_uint32(count), _p(out))
+        if rc:
+            raise ValueError(f"oracle_pick_sources rc={rc}")
+        return out[:count]
+
     def hytm_partition(self, off, active_u8, vbegin, vend, opts: HytmOptions) -> HytmCosts:
         c = HytmCosts()
         self.lib.oracle_hytm_partition(_p(off), _p(active_u8), C.c_uint32(vbegin), C.c_uint32(vend),

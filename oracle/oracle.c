@@ -17,9 +17,66 @@
 #include "oracle.h"
 
 #include <math.h>
+#include <pthread.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <unistd.h>
+
+/* ---- threads ------------------------------------------------------------
+ * Row-parallel loops for large graphs.  Each block of rows writes only its
+ * own outputs, and every reduction that decides a result (residuals,
+ * dangling mass) stays a sequential pass in vertex order, so the results
+ * are bit-identical to the single-threaded loops for any thread count.
+ * ORACLE_THREADS caps the thread count (default: online cores, <= 64). */
+typedef void (*range_fn)(void *ctx, uint64_t begin, uint64_t end);
+
+typedef struct {
+    range_fn fn;
+    void *ctx;
+    uint64_t n, grain;
+    uint64_t next; /* next block, taken under the mutex */
+    pthread_mutex_t mu;
+} par_job;
+
+static void *par_worker(void *arg) {
+    par_job *j = (par_job *)arg;
+    for (;;) {
+        pthread_mutex_lock(&j->mu);
+        const uint64_t b = j->next;
+        j->next += j->grain;
+        pthread_mutex_unlock(&j->mu);
+        if (b >= j->n) break;
+        j->fn(j->ctx, b, b + j->grain < j->n ? b + j->grain : j->n);
+    }
+    return NULL;
+}
+
+static unsigned oracle_threads(void) {
+    const char *e = getenv("ORACLE_THREADS");
+    long t = e ? strtol(e, NULL, 10) : sysconf(_SC_NPROCESSORS_ONLN);
+    if (t < 1) t = 1;
+    if (t > 64) t = 64;
+    return (unsigned)t;
+}
+
+static void par_for(uint64_t n, uint64_t grain, range_fn fn, void *ctx) {
+    unsigned nt = oracle_threads();
+    if (grain == 0) grain = 1;
+    if (n <= grain || nt == 1) {
+        if (n) fn(ctx, 0, n);
+        return;
+    }
+    if ((uint64_t)nt > (n + grain - 1) / grain) nt = (unsigned)((n + grain - 1) / grain);
+    par_job j = {fn, ctx, n, grain, 0, PTHREAD_MUTEX_INITIALIZER};
+    pthread_t th[64];
+    unsigned started = 0;
+    for (unsigned t = 1; t < nt; ++t)
+        if (pthread_create(&th[started], NULL, par_worker, &j) == 0) ++started;
+    par_worker(&j);
+    for (unsigned t = 0; t < started; ++t) pthread_join(th[t], NULL);
+    pthread_mutex_destroy(&j.mu);
+}
 
 /* Incoming CSR (CSC) with sources in ascending order inside each row,
  * built with the same counting pass as src/algorithms/pagerank.cpp:19-60
@@ -60,8 +117,33 @@ static int pr_validate(uint64_t V, float damping, float tol, uint64_t max_iter) 
     return ORACLE_OK;
 }
 
+/* Row sums of one FP32 step (pagerank.cpp:126-147): each row adds
+ * x_u / deg_u over its in-edges in edge order, in float. */
+typedef struct {
+    const uint64_t *off, *in_off;
+    const uint32_t *in_src;
+    const float *cur;
+    float *nxt;
+    float base, dshare, damping;
+} pr32_rows;
+
+static void pr32_rows_fn(void *p, uint64_t b, uint64_t e) {
+    const pr32_rows *c = (const pr32_rows *)p;
+    for (uint64_t v = b; v < e; ++v) {
+        float sum = 0.0f;
+        for (uint64_t q = c->in_off[v]; q < c->in_off[v + 1]; ++q) {
+            const uint32_t u = c->in_src[q];
+            const uint64_t deg = c->off[u + 1] - c->off[u];
+            if (deg != 0) sum += c->cur[u] / (float)deg;
+        }
+        c->nxt[v] = c->base + c->dshare + c->damping * sum;
+    }
+}
+
 /* FP32 restatement of pagerank_cpu, src/algorithms/pagerank.cpp:89-163:
- * same operation order, so it reproduces the reference bit for bit. */
+ * same operation order, so it reproduces the reference bit for bit (the
+ * row sums run in parallel; the residual and dangling sums stay sequential
+ * passes in vertex order, as in the reference). */
 int oracle_pagerank_f32(uint64_t V, uint64_t E, const uint64_t *off, const uint32_t *cols, float damping,
                         float tol, uint64_t max_iter, float *ranks, uint64_t *iterations, float *residual_out,
                         int *converged) {
@@ -83,17 +165,10 @@ int oracle_pagerank_f32(uint64_t V, uint64_t E, const uint64_t *off, const uint3
         for (uint64_t u = 0; u < V; ++u)
             if (off[u + 1] == off[u]) dangling += cur[u];
         const float dshare = damping * dangling / n;
+        pr32_rows ctx = {off, in_off, in_src, cur, nxt, base, dshare, damping};
+        par_for(V, 1u << 15, pr32_rows_fn, &ctx);
         float residual = 0.0f;
-        for (uint64_t v = 0; v < V; ++v) {
-            float sum = 0.0f;
-            for (uint64_t p = in_off[v]; p < in_off[v + 1]; ++p) {
-                const uint32_t u = in_src[p];
-                const uint64_t deg = off[u + 1] - off[u];
-                if (deg != 0) sum += cur[u] / (float)deg;
-            }
-            nxt[v] = base + dshare + damping * sum;
-            residual += fabsf(nxt[v] - cur[v]);
-        }
+        for (uint64_t v = 0; v < V; ++v) residual += fabsf(nxt[v] - cur[v]);
         float *t = cur; cur = nxt; nxt = t;
         *iterations = it + 1;
         *residual_out = residual;
@@ -102,6 +177,28 @@ int oracle_pagerank_f32(uint64_t V, uint64_t E, const uint64_t *off, const uint3
     }
     free(cur); free(nxt); free(in_off); free(in_src);
     return ORACLE_OK;
+}
+
+/* Row sums of one FP64 step: x'[v] = add + d * sum_{u->v} contrib[u];
+ * personalized: x'[v] = d * sum + (v == source ? restart_mass : 0). */
+typedef struct {
+    const uint64_t *in_off;
+    const uint32_t *in_src;
+    const double *contrib;
+    double *nxt;
+    double add, d;
+    int personalized;
+    uint32_t source;
+    double restart_mass;
+} pr64_rows;
+
+static void pr64_rows_fn(void *p, uint64_t b, uint64_t e) {
+    const pr64_rows *c = (const pr64_rows *)p;
+    for (uint64_t v = b; v < e; ++v) {
+        double sum = 0.0;
+        for (uint64_t q = c->in_off[v]; q < c->in_off[v + 1]; ++q) sum += c->contrib[c->in_src[q]];
+        c->nxt[v] = c->personalized ? c->d * sum + (v == c->source ? c->restart_mass : 0.0) : c->add + c->d * sum;
+    }
 }
 
 /* FP64 restatement of the same iteration (pagerank.cpp:89-163 in double):
@@ -130,13 +227,10 @@ int oracle_pagerank_f64(uint64_t V, uint64_t E, const uint64_t *off, const uint3
             contrib[u] = deg ? cur[u] / (double)deg : 0.0;
         }
         const double dshare = damping * dangling / n;
+        pr64_rows ctx = {in_off, in_src, contrib, nxt, base + dshare, damping, 0, 0, 0.0};
+        par_for(V, 1u << 15, pr64_rows_fn, &ctx);
         double residual = 0.0;
-        for (uint64_t v = 0; v < V; ++v) {
-            double sum = 0.0;
-            for (uint64_t p = in_off[v]; p < in_off[v + 1]; ++p) sum += contrib[in_src[p]];
-            nxt[v] = base + dshare + damping * sum;
-            residual += fabs(nxt[v] - cur[v]);
-        }
+        for (uint64_t v = 0; v < V; ++v) residual += fabs(nxt[v] - cur[v]);
         double *t = cur; cur = nxt; nxt = t;
         *iterations = it + 1;
         *residual_out = residual;
@@ -174,13 +268,10 @@ int oracle_ppr_f64(uint64_t V, uint64_t E, const uint64_t *off, const uint32_t *
             if (deg == 0) dangling += cur[u];
             contrib[u] = deg ? cur[u] / (double)deg : 0.0;
         }
+        pr64_rows ctx = {in_off, in_src, contrib, nxt, 0.0, d, 1, source, (1.0 - d) + d * dangling};
+        par_for(V, 1u << 15, pr64_rows_fn, &ctx);
         double residual = 0.0;
-        for (uint64_t v = 0; v < V; ++v) {
-            double sum = 0.0;
-            for (uint64_t p = in_off[v]; p < in_off[v + 1]; ++p) sum += contrib[in_src[p]];
-            nxt[v] = d * sum + (v == source ? (1.0 - d) + d * dangling : 0.0);
-            residual += fabs(nxt[v] - cur[v]);
-        }
+        for (uint64_t v = 0; v < V; ++v) residual += fabs(nxt[v] - cur[v]);
         double *t = cur; cur = nxt; nxt = t;
         *iterations = it + 1;
         *residual_out = residual;
@@ -189,6 +280,37 @@ int oracle_ppr_f64(uint64_t V, uint64_t E, const uint64_t *off, const uint32_t *
     memcpy(ranks, cur, V * sizeof(double));
     free(cur); free(nxt); free(contrib); free(in_off); free(in_src);
     return ORACLE_OK;
+}
+
+/* One synchronous round over rows [b, e) (sssp.cpp:126-170): each row
+ * takes the minimum of its label and cur[u] + w over in-edges whose source
+ * was active in the previous round. */
+typedef struct {
+    const uint64_t *in_off;
+    const uint32_t *in_src;
+    const float *in_w, *cur;
+    float *nxt;
+    const unsigned char *active;
+    unsigned char *next_active;
+    int changed; /* set to 1 (atomically) by any block whose rows improved */
+} sssp_rows;
+
+static void sssp_rows_fn(void *p, uint64_t b, uint64_t e) {
+    sssp_rows *c = (sssp_rows *)p;
+    int changed = 0;
+    for (uint64_t v = b; v < e; ++v) {
+        float best = c->cur[v];
+        for (uint64_t q = c->in_off[v]; q < c->in_off[v + 1]; ++q) {
+            const uint32_t u = c->in_src[q];
+            if (!c->active[u] || !isfinite(c->cur[u])) continue;
+            const float cand = c->cur[u] + c->in_w[q];
+            if (cand < best) best = cand;
+        }
+        c->nxt[v] = best;
+        c->next_active[v] = best < c->cur[v];
+        changed |= best < c->cur[v];
+    }
+    if (changed) __atomic_store_n(&c->changed, 1, __ATOMIC_RELAXED);
 }
 
 /* FP32 restatement of sssp_cpu, src/algorithms/sssp.cpp:109-234: synchronous
@@ -217,20 +339,9 @@ int oracle_sssp(uint64_t V, uint64_t E, const uint64_t *off, const uint32_t *col
     if (max_iter == 0) max_iter = V;
     *iterations = 0; *converged = 0;
     for (uint64_t it = 0; it < max_iter; ++it) {
-        memcpy(nxt, cur, V * sizeof(float));
-        memset(next_active, 0, V);
-        int changed = 0;
-        for (uint64_t v = 0; v < V; ++v) {
-            float best = cur[v];
-            for (uint64_t p = in_off[v]; p < in_off[v + 1]; ++p) {
-                const uint32_t u = in_src[p];
-                if (!active[u] || !isfinite(cur[u])) continue;
-                const float cand = cur[u] + in_w[p];
-                if (cand < best) best = cand;
-            }
-            nxt[v] = best;
-            if (best < cur[v]) { next_active[v] = 1; changed = 1; }
-        }
+        sssp_rows ctx = {in_off, in_src, in_w, cur, nxt, active, next_active, 0};
+        par_for(V, 1u << 15, sssp_rows_fn, &ctx);
+        const int changed = ctx.changed != 0;
         float *t = cur; cur = nxt; nxt = t;
         unsigned char *ta = active; active = next_active; next_active = ta;
         *iterations = it + 1;
@@ -242,56 +353,241 @@ int oracle_sssp(uint64_t V, uint64_t E, const uint64_t *off, const uint32_t *col
 }
 
 /* Independent cross-check: Dijkstra with exact 64-bit integer distances on
- * uint32 weights (NULL = unit weights); UINT64_MAX marks unreachable. */
+ * uint32 weights (NULL = unit weights); UINT64_MAX marks unreachable.  An
+ * indexed binary heap with decrease-key holds at most V entries (16 B + a
+ * 4 B position each), so large graphs need O(V) extra memory, not O(E). */
 typedef struct { uint64_t d; uint32_t v; } heap_item;
 
-static void heap_push(heap_item *h, uint64_t *n, heap_item x) {
-    uint64_t i = (*n)++;
-    while (i > 0) {
-        uint64_t p = (i - 1) / 2;
-        if (h[p].d <= x.d) break;
-        h[i] = h[p];
-        i = p;
-    }
+static void heap_place(heap_item *h, uint32_t *pos, uint64_t i, heap_item x) {
     h[i] = x;
+    pos[x.v] = (uint32_t)i;
 }
 
-static heap_item heap_pop(heap_item *h, uint64_t *n) {
-    heap_item top = h[0], x = h[--(*n)];
+static void heap_up(heap_item *h, uint32_t *pos, uint64_t i, heap_item x) {
+    while (i > 0) {
+        const uint64_t p = (i - 1) / 2;
+        if (h[p].d <= x.d) break;
+        heap_place(h, pos, i, h[p]);
+        i = p;
+    }
+    heap_place(h, pos, i, x);
+}
+
+static heap_item heap_pop(heap_item *h, uint32_t *pos, uint64_t *n) {
+    const heap_item top = h[0], x = h[--(*n)];
+    pos[top.v] = UINT32_MAX;
+    if (*n == 0) return top;
     uint64_t i = 0;
     for (;;) {
         uint64_t c = 2 * i + 1;
         if (c >= *n) break;
         if (c + 1 < *n && h[c + 1].d < h[c].d) ++c;
         if (h[c].d >= x.d) break;
-        h[i] = h[c];
+        heap_place(h, pos, i, h[c]);
         i = c;
     }
-    if (*n) h[i] = x;
+    heap_place(h, pos, i, x);
     return top;
 }
 
 int oracle_dijkstra_u32(uint64_t V, uint64_t E, const uint64_t *off, const uint32_t *cols, const uint32_t *weights,
                         uint32_t source, uint64_t *dist) {
-    if (V == 0 || source >= V) return ORACLE_E_INVALID;
-    heap_item *h = (heap_item *)malloc((E + 1) * sizeof(heap_item));
-    if (!h) return ORACLE_E_NOMEM;
-    for (uint64_t v = 0; v < V; ++v) dist[v] = UINT64_MAX;
-    uint64_t n = 0;
+    (void)E;
+    if (V == 0 || source >= V || V >= UINT32_MAX) return ORACLE_E_INVALID;
+    heap_item *h = (heap_item *)malloc(V * sizeof(heap_item));
+    uint32_t *pos = (uint32_t *)malloc(V * sizeof(uint32_t));
+    if (!h || !pos) { free(h); free(pos); return ORACLE_E_NOMEM; }
+    for (uint64_t v = 0; v < V; ++v) { dist[v] = UINT64_MAX; pos[v] = UINT32_MAX; }
+    uint64_t n = 1;
     dist[source] = 0;
-    heap_push(h, &n, (heap_item){0, source});
+    heap_place(h, pos, 0, (heap_item){0, source});
     while (n) {
-        heap_item t = heap_pop(h, &n);
-        if (t.d != dist[t.v]) continue;
+        const heap_item t = heap_pop(h, pos, &n);
         for (uint64_t e = off[t.v]; e < off[t.v + 1]; ++e) {
+            const uint32_t u = cols[e];
             const uint64_t nd = t.d + (weights ? weights[e] : 1u);
-            if (nd < dist[cols[e]]) {
-                dist[cols[e]] = nd;
-                heap_push(h, &n, (heap_item){nd, cols[e]});
+            if (nd < dist[u]) {
+                dist[u] = nd;
+                const uint64_t i = pos[u] == UINT32_MAX ? n++ : pos[u];
+                heap_up(h, pos, i, (heap_item){nd, u});
             }
         }
     }
     free(h);
+    free(pos);
+    return ORACLE_OK;
+}
+
+/* ---- R-MAT generator and source picker ------------------------------------
+ * The seeded synthetic inputs (the reference ships no generator and no
+ * datasets), restated from their definition so that CPU-only consumers
+ * (the reference's CPU baseline) build the same graph bytes without the
+ * product library:
+ *   draw i (0 <= i < edge_factor * 2^scale) descends `scale` levels; level
+ *   l takes the 32-bit uniform u = half (l & 1) of
+ *   splitmix64(seed + golden * (16 i + l / 2)) and picks quadrant
+ *   (0,0) / (0,1) / (1,0) / (1,1) by u < a / a+b / a+b+c (thresholds scaled
+ *   to 2^32, saturating at 2^32 - 1); bit (scale - 1 - l) of the source
+ *   takes the row half, of the destination the column half.  Self-loops and
+ *   duplicate (u, v) are dropped, edges sorted by (u, v); weight of (u, v) =
+ *   wmin + splitmix64(((u << 32) | v) ^ wseed) % (wmax - wmin + 1), wseed =
+ *   splitmix64(seed ^ 0x5EEDF00DCAFEBABE); wmin = wmax = 0 means unweighted.
+ *   Sources: the j-th candidate (j = 1, 2, ...) is splitmix64(seed + golden
+ *   * j) % V; vertices without out-edges are skipped, and repeats while
+ *   distinct vertices with out-edges remain. */
+static const uint64_t kGolden = 0x9E3779B97F4A7C15ull;
+
+static uint64_t mix64(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+static uint32_t rmat_threshold(double x) {
+    const double v = x * 4294967296.0;
+    return v >= 4294967295.0 ? 0xFFFFFFFFu : (uint32_t)v;
+}
+
+typedef struct {
+    uint64_t seed, n;
+    uint32_t scale, ta, tab, tabc;
+    uint64_t *keys; /* (u << scale) | v, or UINT64_MAX for a self-loop */
+} rmat_job;
+
+static void rmat_draw_fn(void *p, uint64_t b, uint64_t e) {
+    const rmat_job *j = (const rmat_job *)p;
+    for (uint64_t i = b; i < e; ++i) {
+        uint32_t src = 0, dst = 0;
+        uint64_t word = 0;
+        for (uint32_t l = 0; l < j->scale; ++l) {
+            if ((l & 1u) == 0) word = mix64(j->seed + kGolden * (16ull * i + (l >> 1)));
+            const uint32_t r = (l & 1u) ? (uint32_t)(word >> 32) : (uint32_t)word;
+            const uint32_t bit = 1u << (j->scale - 1 - l);
+            if (r >= j->tabc) { src |= bit; dst |= bit; }
+            else if (r >= j->tab) src |= bit;
+            else if (r >= j->ta) dst |= bit;
+        }
+        j->keys[i] = (src == dst) ? UINT64_MAX : (((uint64_t)src << j->scale) | dst);
+    }
+}
+
+/* LSD radix sort of n keys on their low `bits` bits, 11 bits a pass,
+ * threads over contiguous slices (stable, so equal keys keep their order). */
+typedef struct {
+    const uint64_t *in;
+    uint64_t *out;
+    uint64_t n, slice;
+    unsigned shift, nslices;
+    uint64_t *hist; /* [nslices][2048] counts, then start offsets */
+} radix_job;
+
+static void radix_count_fn(void *p, uint64_t b, uint64_t e) {
+    radix_job *j = (radix_job *)p;
+    for (uint64_t t = b; t < e; ++t) {
+        uint64_t *h = j->hist + t * 2048;
+        memset(h, 0, 2048 * sizeof(uint64_t));
+        const uint64_t lo = t * j->slice, hi = lo + j->slice < j->n ? lo + j->slice : j->n;
+        for (uint64_t i = lo; i < hi; ++i) ++h[(j->in[i] >> j->shift) & 2047u];
+    }
+}
+
+static void radix_scatter_fn(void *p, uint64_t b, uint64_t e) {
+    radix_job *j = (radix_job *)p;
+    for (uint64_t t = b; t < e; ++t) {
+        uint64_t *h = j->hist + t * 2048;
+        const uint64_t lo = t * j->slice, hi = lo + j->slice < j->n ? lo + j->slice : j->n;
+        for (uint64_t i = lo; i < hi; ++i) j->out[h[(j->in[i] >> j->shift) & 2047u]++] = j->in[i];
+    }
+}
+
+static int radix_sort_u64(uint64_t *keys, uint64_t n, unsigned bits) {
+    if (n < 2) return ORACLE_OK;
+    uint64_t *tmp = (uint64_t *)malloc(n * sizeof(uint64_t));
+    const unsigned nslices = 64;
+    uint64_t *hist = (uint64_t *)malloc((uint64_t)nslices * 2048 * sizeof(uint64_t));
+    if (!tmp || !hist) { free(tmp); free(hist); return ORACLE_E_NOMEM; }
+    radix_job j = {keys, tmp, n, (n + nslices - 1) / nslices, 0, nslices, hist};
+    for (unsigned shift = 0; shift < bits; shift += 11) {
+        j.shift = shift;
+        par_for(nslices, 1, radix_count_fn, &j);
+        uint64_t run = 0;  /* digit-major, slice-minor starts keep the sort stable */
+        for (unsigned d = 0; d < 2048; ++d)
+            for (unsigned t = 0; t < nslices; ++t) {
+                const uint64_t c = hist[(uint64_t)t * 2048 + d];
+                hist[(uint64_t)t * 2048 + d] = run;
+                run += c;
+            }
+        par_for(nslices, 1, radix_scatter_fn, &j);
+        uint64_t *done = j.out;
+        j.out = (uint64_t *)j.in;
+        j.in = done;
+    }
+    if (j.in != keys) memcpy(keys, j.in, n * sizeof(uint64_t));
+    free(tmp);
+    free(hist);
+    return ORACLE_OK;
+}
+
+int oracle_rmat(uint32_t scale, uint32_t edge_factor, uint64_t seed, double a, double b, double c, uint32_t wmin,
+                uint32_t wmax, uint64_t **off_out, uint32_t **cols_out, uint32_t **w_out, uint64_t *E_out) {
+    *off_out = NULL; *cols_out = NULL; *w_out = NULL; *E_out = 0;
+    if (scale < 1 || scale > 31 || edge_factor == 0 || wmax < wmin) return ORACLE_E_INVALID;
+    if (!(a >= 0 && b >= 0 && c >= 0 && 1.0 - a - b - c >= -1e-12)) return ORACLE_E_INVALID;
+    const uint64_t V = 1ull << scale, n = (uint64_t)edge_factor * V;
+    uint64_t *keys = (uint64_t *)malloc(n * sizeof(uint64_t));
+    if (!keys) return ORACLE_E_NOMEM;
+    rmat_job j = {seed, n, scale, rmat_threshold(a), rmat_threshold(a + b), rmat_threshold(a + b + c), keys};
+    par_for(n, 1u << 16, rmat_draw_fn, &j);
+    uint64_t m = 0;  /* drop self-loops */
+    for (uint64_t i = 0; i < n; ++i)
+        if (keys[i] != UINT64_MAX) keys[m++] = keys[i];
+    int rc = radix_sort_u64(keys, m, 2 * scale);
+    if (rc) { free(keys); return rc; }
+    uint64_t E = 0;  /* drop duplicates */
+    for (uint64_t i = 0; i < m; ++i)
+        if (i == 0 || keys[i] != keys[i - 1]) keys[E++] = keys[i];
+    uint64_t *off = (uint64_t *)malloc((V + 1) * sizeof(uint64_t));
+    uint32_t *cols = (uint32_t *)malloc((E ? E : 1) * sizeof(uint32_t));
+    const int weighted = !(wmin == 0 && wmax == 0);
+    uint32_t *w = weighted ? (uint32_t *)malloc((E ? E : 1) * sizeof(uint32_t)) : NULL;
+    if (!off || !cols || (weighted && !w)) { free(keys); free(off); free(cols); free(w); return ORACLE_E_NOMEM; }
+    const uint64_t wseed = mix64(seed ^ 0x5EEDF00DCAFEBABEull);
+    const uint32_t span = wmax - wmin + 1u;
+    const uint64_t vmask = V - 1;
+    uint64_t e = 0;
+    for (uint64_t v = 0; v < V; ++v) {
+        off[v] = e;
+        while (e < E && (keys[e] >> scale) == v) {
+            const uint32_t dst = (uint32_t)(keys[e] & vmask);
+            cols[e] = dst;
+            if (w) w[e] = wmin + (uint32_t)(mix64(((v << 32) | dst) ^ wseed) % (span ? span : 1u));
+            ++e;
+        }
+    }
+    off[V] = E;
+    free(keys);
+    *off_out = off; *cols_out = cols; *w_out = w; *E_out = E;
+    return ORACLE_OK;
+}
+
+void oracle_free(void *p) { free(p); }
+
+int oracle_pick_sources(const uint64_t *off, uint64_t V, uint64_t seed, uint32_t count, uint32_t *out) {
+    if (V == 0) return ORACLE_E_INVALID;
+    uint64_t with_edges = 0;
+    for (uint64_t v = 0; v < V; ++v) with_edges += off[v + 1] > off[v];
+    if (with_edges == 0 && count) return ORACLE_E_INVALID;
+    const uint64_t want_unique = count < with_edges ? count : with_edges;
+    uint64_t chosen = 0, j = 0;
+    while (chosen < count) {
+        const uint64_t v = mix64(seed + kGolden * (++j)) % V;
+        if (off[v + 1] == off[v]) continue;
+        int seen = 0;
+        if (chosen < want_unique)
+            for (uint64_t k = 0; k < chosen; ++k) seen |= out[k] == (uint32_t)v;
+        if (seen) continue;
+        out[chosen++] = (uint32_t)v;
+    }
     return ORACLE_OK;
 }
 

@@ -25,6 +25,12 @@ int oracle_sssp(uint64_t V, uint64_t E, const uint64_t *off, const uint32_t *col
                 uint32_t source, uint64_t max_iter, float *dist, uint64_t *iterations, int *converged);
 int oracle_dijkstra_u32(uint64_t V, uint64_t E, const uint64_t *off, const uint32_t *cols, const uint32_t *weights,
                         uint32_t source, uint64_t *dist);
+/* Seeded R-MAT CSR (malloc'd arrays, release with oracle_free; *w_out NULL
+ * when wmin == wmax == 0) and seeded source vertices. */
+int oracle_rmat(uint32_t scale, uint32_t edge_factor, uint64_t seed, double a, double b, double c, uint32_t wmin,
+                uint32_t wmax, uint64_t **off_out, uint32_t **cols_out, uint32_t **w_out, uint64_t *E_out);
+void oracle_free(void *p);
+int oracle_pick_sources(const uint64_t *off, uint64_t V, uint64_t seed, uint32_t count, uint32_t *out);
 
 typedef struct {
     double alpha, beta, gamma, rtt, cpu_throughput;

@@ -31,6 +31,59 @@ def test_generator_matches_golden_digest(hyt, golden):
         assert _digest(g) == m["csr_sha256"], m["key"]
 
 
+def test_oracle_generator_matches_golden_and_product(hyt, oracle, golden):
+    """The oracle's restatement of the generator (used by the reference arm
+    of the bench, which loads no product library) gives the golden digests
+    and the product generator's bytes, and the same seeded sources."""
+    from types import SimpleNamespace
+
+    for m in golden["meta"]["graphs"]:
+        w = (1, 63) if m["weighted"] else (0, 0)
+        off, cols, wt = oracle.rmat(m["scale"], m["edge_factor"], m["seed"], *w)
+        assert _digest(SimpleNamespace(row_offsets=off, column_indices=cols, weights=wt)) == m["csr_sha256"], m["key"]
+    for scale, ef, seed, w in [(13, 16, 9, (1, 63)), (15, 8, 2024, (0, 0)), (17, 16, 20241203, (1, 63)),
+                               (12, 4, 3, (5, 9))]:
+        off, cols, wt = oracle.rmat(scale, ef, seed, *w)
+        g = hyt.rmat(scale, ef, seed, *w)
+        assert np.array_equal(off, g.row_offsets) and np.array_equal(cols, g.column_indices)
+        assert (wt is None and g.weights is None) or np.array_equal(wt, g.weights)
+        for count in (1, 8, 40):
+            assert np.array_equal(oracle.pick_sources(off, seed, count), hyt.pick_sources(off, seed, count))
+
+
+def test_oracle_threads_do_not_change_results():
+    """The row-parallel oracle loops give the same bits on one thread and on
+    seven (FP64 and FP32 PageRank, the SSSP restatement, Dijkstra)."""
+    import os
+    import subprocess
+    import sys
+
+    code = ("import sys, numpy as np; sys.path.insert(0, %r); from oracle.bindings import Oracle; o = Oracle(); "
+            "off, cols, w = o.rmat(15, 16, 4); r64 = o.pagerank_f64(off, cols)[0]; r32 = o.pagerank_f32(off, cols)[0]; "
+            "p64 = o.ppr_f64(off, cols, 3)[0]; d = o.sssp(off, cols, w.astype(np.float32), 3)[0]; "
+            "dj = o.dijkstra(off, cols, w, 3); "
+            "sys.stdout.buffer.write(r64.tobytes() + r32.tobytes() + p64.tobytes() + d.tobytes() + dj.tobytes())"
+            ) % str(ROOT)
+    outs = []
+    for threads in ("1", "7"):
+        env = dict(os.environ, ORACLE_THREADS=threads)
+        outs.append(subprocess.run([sys.executable, "-c", code], capture_output=True, env=env, check=True).stdout)
+    assert outs[0] == outs[1] and len(outs[0]) > 0
+
+
+def test_dijkstra_agrees_with_the_sssp_restatement(oracle):
+    """Two independent oracles of the same labels: Dijkstra (exact integers)
+    and the restatement of the reference's synchronous Bellman-Ford."""
+    off, cols, w = oracle.rmat(14, 16, 12)
+    for s in oracle.pick_sources(off, 12, 3):
+        dj = oracle.dijkstra(off, cols, w, int(s))
+        bf, _, conv = oracle.sssp(off, cols, w.astype(np.float32), int(s))
+        assert conv
+        reach = dj != np.iinfo(np.uint64).max
+        assert np.array_equal(np.isfinite(bf), reach)
+        assert np.array_equal(bf[reach].astype(np.uint64), dj[reach])
+
+
 def test_oracle_pagerank_f32_bit_identical_to_reference_golden(hyt, oracle, golden):
     for m in golden["meta"]["graphs"]:
         g = _graph(hyt, m)
