@@ -50,6 +50,7 @@ def parse_args():
     ap.add_argument("--seed", type=int, default=20241203)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-parity", action="store_true", help="skip the oracle check of the timed run's results")
     ap.add_argument("--workload", choices=["inhbm", "hybrid", "batch", "serve", "hubsort", "load", "contrib",
                                            "ppr8", "shard"],
                     default="inhbm",
@@ -198,26 +199,106 @@ def replica_value(units_per_rank: float, world: int, ms_max: float) -> float:
 
 
 # --------------------------------------------------------------------------
-# CPU baseline: the reference's own CPU solvers on a bounded sample
+# CPU side: the reference's own CPU solvers (oracle/_ref) timed with the GPU
+# arm's counting convention, and the parity checks against the oracle.
 # --------------------------------------------------------------------------
-def cpu_sample(off, cols, w_f32, source):
-    """One PageRank iteration and one SSSP round of the reference's own
-    pagerank_cpu / sssp_cpu (each including its incoming-CSR build) on the
-    full graph.  Returns (edges traversed, seconds, kind)."""
-    from oracle.bindings import Oracle, Reference
+class CpuSolvers:
+    """pagerank_cpu / sssp_cpu of the reference compiled from its sources
+    (oracle/_ref, single-threaded as in the reference), or the oracle's
+    restatements when _ref is absent."""
 
-    E = int(cols.shape[0])
-    if Reference.available():
-        ref, kind = Reference(), "reference"
-        t0 = time.perf_counter()
-        ref.pagerank_cpu(off, cols, 0.85, 1e-6, 1)
-        ref.sssp_cpu(off, cols, w_f32, int(source), 1)
-    else:
-        ref, kind = Oracle(), "port"
-        t0 = time.perf_counter()
-        ref.pagerank_f32(off, cols, 0.85, 1e-6, 1)
-        ref.sssp(off, cols, w_f32, int(source), 1)
-    return 2 * E, time.perf_counter() - t0, kind
+    def __init__(self):
+        from oracle.bindings import Oracle, Reference
+
+        if Reference.available():
+            r = Reference()
+            self.kind, self.cores = "reference", 1
+            self.pagerank = lambda off, cols, it: r.pagerank_cpu(off, cols, 0.85, 1e-6, it)
+            self.sssp = lambda off, cols, w, s, it: r.sssp_cpu(off, cols, w, int(s), it)
+        else:
+            o = Oracle()
+            self.kind, self.cores = "port", int(os.environ.get("ORACLE_THREADS", os.cpu_count() or 1))
+            self.pagerank = lambda off, cols, it: o.pagerank_f32(off, cols, 0.85, 1e-6, it)
+            self.sssp = lambda off, cols, w, s, it: o.sssp(off, cols, w, int(s), it)
+
+
+def time_call(f, *a):
+    t0 = time.perf_counter()
+    r = f(*a)
+    return time.perf_counter() - t0, r
+
+
+def host_rmat(args):
+    """The bench graph and its sources built on the host by the oracle's
+    restatement of the generator (byte-identical to the product's; the
+    reference arm loads no product library)."""
+    from oracle.bindings import Oracle
+
+    o = Oracle()
+    off, cols, w = o.rmat(args.scale, args.edge_factor, args.seed)
+    return off, cols, w, [int(x) for x in o.pick_sources(off, args.seed, args.sources)]
+
+
+def project_step(parts, n_sources):
+    """Full-solve step time (PageRank to convergence + n_sources SSSP solves)
+    projected from one sampled first iteration / first round (each with its
+    incoming-CSR build) plus the per-iteration and per-round costs."""
+    pr = parts["pr_first_s"] + (parts["pr_iterations"] - 1) * parts["pr_per_iteration_s"]
+    ss = parts["sssp_first_s"] + (parts["sssp_rounds"] - 1) * parts["sssp_per_round_s"]
+    return pr + n_sources * ss
+
+
+def cpu_baseline_sample(cpu, off, cols, w_f32, source, pr_iterations, sssp_rounds, n_sources):
+    """Bounded CPU baseline on the full graph: pagerank_cpu for 1 and 3
+    iterations and sssp_cpu for 1 and 3 rounds give the first-iteration and
+    per-iteration costs; the iteration / round counts of the full solves come
+    from the oracle's restatements, which reproduce the reference's counts
+    bit for bit.  Returns (projected full-step seconds, parts, sample seconds)."""
+    t_p1, _ = time_call(cpu.pagerank, off, cols, 1)
+    t_p3, _ = time_call(cpu.pagerank, off, cols, 3)
+    t_s1, _ = time_call(cpu.sssp, off, cols, w_f32, source, 1)
+    t_s3, _ = time_call(cpu.sssp, off, cols, w_f32, source, 3)
+    parts = {"pr_first_s": t_p1, "pr_per_iteration_s": max(t_p3 - t_p1, 0.0) / 2, "pr_iterations": pr_iterations,
+             "sssp_first_s": t_s1, "sssp_per_round_s": max(t_s3 - t_s1, 0.0) / 2, "sssp_rounds": sssp_rounds}
+    return project_step(parts, n_sources), parts, t_p1 + t_p3 + t_s1 + t_s3
+
+
+def parity_inhbm(off, cols, w, sources, ranks, dists, threads=None):
+    """The GPU results of the timed run against the oracle on the same graph:
+    PageRank L1 against the FP64 restatement (and the reference's FP32
+    solver's own L1, for context), SSSP labels of every source against
+    Dijkstra (exact 64-bit integers), cross-checked on the first source with
+    the restatement of the reference's synchronous Bellman-Ford."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from oracle.bindings import Oracle
+
+    o = Oracle()
+    w_f32 = w.astype(np.float32)
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=threads or (len(sources) + 3)) as ex:
+        f64 = ex.submit(o.pagerank_f64, off, cols, 0.85, 1e-6, 100)
+        f32 = ex.submit(o.pagerank_f32, off, cols, 0.85, 1e-6, 100)
+        bf = ex.submit(o.sssp, off, cols, w_f32, sources[0], 0)
+        dj = [ex.submit(o.dijkstra, off, cols, w, s) for s in sources]
+        r64, it64, _, _ = f64.result()
+        r32, it32, _, _ = f32.result()
+        want = []
+        for d in dj:
+            x = d.result()
+            want.append(np.where(x == np.iinfo(np.uint64).max, 0xFFFFFFFF, x).astype(np.uint32))
+        dbf, rounds_bf, _ = bf.result()
+    mism = [int(np.count_nonzero(np.asarray(g).view(np.uint32) != x)) for g, x in zip(dists, want)]
+    bf_u32 = np.where(np.isfinite(dbf), np.nan_to_num(dbf, posinf=0), 0).astype(np.uint32)
+    bf_u32[~np.isfinite(dbf)] = 0xFFFFFFFF
+    l1 = float(np.abs(np.asarray(ranks, np.float64) - r64).sum())
+    return {"pr_l1_vs_fp64": l1, "pr_l1_ref_fp32_vs_fp64": float(np.abs(r32.astype(np.float64) - r64).sum()),
+            "pr_l1_tolerance": 1e-5, "fp64_iterations": int(it64), "ref_fp32_iterations": int(it32),
+            "sssp_mismatches": int(sum(mism)), "sources_checked": len(sources),
+            "sssp_oracle": "Dijkstra, exact u64 labels, every source",
+            "sssp_bellman_ford_vs_dijkstra_mismatches": int(np.count_nonzero(bf_u32 != want[0])),
+            "ok": bool(l1 <= 1e-5 and sum(mism) == 0), "check_s": time.perf_counter() - t0,
+            "_ref_rounds_source0": int(rounds_bf), "_ref_iterations": int(it32)}
 
 
 def host_graph_from_device(dcsr):
@@ -236,16 +317,13 @@ def host_graph_from_device(dcsr):
 # --------------------------------------------------------------------------
 def run_reference_arm(args, rank, pg):
     """--impl reference: the reference's CPU implementation of the path on
-    this host's cores, same workload, metric and unit (rank 0 only)."""
+    this host's cores, same workload, metric, unit and counting convention
+    (rank 0 only).  Only oracle/ libraries are loaded: the graph comes from
+    the oracle's restatement of the generator."""
     if rank != 0:
         return
-    import hytgraph_b200 as hyt
-
     if args.workload == "hubsort":
-        d = hyt.rmat(args.scale, args.edge_factor, args.seed, device=True)
-        off_t, cols_t, w_t = host_graph_from_device(d)
-        d.free()
-        off, cols, w = off_t.numpy().view(np.uint64), cols_t.numpy().view(np.uint32), w_t.numpy().view(np.uint32)
+        off, cols, w, _ = host_rmat(args)
         V, E = int(off.shape[0] - 1), int(cols.shape[0])
         times, kind = [], "port"
         for i in range(args.warmup + args.steps):
@@ -265,39 +343,51 @@ def run_reference_arm(args, rank, pg):
         print(json.dumps(line), flush=True)
         return
 
-    g = hyt.rmat(args.scale, args.edge_factor, args.seed) if args.scale <= 20 else None
-    if g is None:
-        d = hyt.rmat(args.scale, args.edge_factor, args.seed, device=True)
-        off_t, cols_t, w_t = host_graph_from_device(d)
-        d.free()
-        off = off_t.numpy().view(np.uint64)
-        cols = cols_t.numpy().view(np.uint32)
-        w = w_t.numpy().view(np.uint32)
-    else:
-        off, cols, w = g.row_offsets, g.column_indices, g.weights
+    t_gen = time.perf_counter()
+    off, cols, w, sources = host_rmat(args)
+    t_gen = time.perf_counter() - t_gen
     w_f32 = w.astype(np.float32)
-    src = int(hyt.pick_sources(off, args.seed, 1)[0])
-    kind = "port"
-    times, edges = [], 0
-    for i in range(args.warmup + args.steps):
-        e, t, kind = cpu_sample(off, cols, w_f32, src)
-        if i >= args.warmup:
-            times.append(t)
-            edges += e
-    total = sum(times)
-    value = edges / total / 1e9
-    sample = (f"per step: 1 PageRank iteration + 1 SSSP round of the reference's pagerank_cpu/sssp_cpu "
-              f"(each incl. its incoming-CSR build) on the full R-MAT s{args.scale} ef{args.edge_factor} graph; "
-              f"E per iteration/round counted")
     V, E = int(off.shape[0] - 1), int(cols.shape[0])
+    cpu = CpuSolvers()
+    n_src = len(sources)
+    # Once, before the warm-up: the full solves give the iteration and round
+    # counts and, with the per-step samples, the per-iteration costs.
+    t_pr_full, (_, n_pr, _, _) = time_call(cpu.pagerank, off, cols, 100)
+    t_ss_full, (_, n_ss, _) = time_call(cpu.sssp, off, cols, w_f32, sources[0], 0)
+    samples = []
+    for i in range(args.warmup + args.steps):
+        t_p1, _ = time_call(cpu.pagerank, off, cols, 1)
+        t_s1, _ = time_call(cpu.sssp, off, cols, w_f32, sources[0], 1)
+        samples.append((t_p1, t_s1))
+    med_p1 = statistics.median(x[0] for x in samples)
+    med_s1 = statistics.median(x[1] for x in samples)
+    per_it = max(t_pr_full - med_p1, 0.0) / max(n_pr - 1, 1)
+    per_rd = max(t_ss_full - med_s1, 0.0) / max(n_ss - 1, 1)
+    steps = []
+    for t_p1, t_s1 in samples[args.warmup:]:
+        steps.append(project_step({"pr_first_s": t_p1, "pr_per_iteration_s": per_it, "pr_iterations": n_pr,
+                                   "sssp_first_s": t_s1, "sssp_per_round_s": per_rd, "sssp_rounds": n_ss}, n_src))
+    total = sum(steps)
+    traversed = args.steps * (E * n_pr + E * n_src)  # E per PageRank iteration + E per SSSP source
+    value = traversed / total / 1e9
+    parts = {"pr_full_s": t_pr_full, "pr_iterations": n_pr, "pr_first_iteration_s_median": med_p1,
+             "pr_per_iteration_s": per_it, "sssp_full_s": t_ss_full, "sssp_rounds": n_ss,
+             "sssp_first_round_s_median": med_s1, "sssp_per_round_s": per_rd, "graph_generation_s": t_gen}
+    sample = (f"once: a full pagerank_cpu ({n_pr} iterations, {t_pr_full:.1f} s) and a full sssp_cpu from the "
+              f"first source ({n_ss} rounds, {t_ss_full:.1f} s); per step: pagerank_cpu for 1 iteration and "
+              f"sssp_cpu for 1 round (each with its incoming-CSR build) on the full R-MAT s{args.scale} "
+              f"ef{args.edge_factor} graph; step time projected to PageRank to convergence + {n_src} full SSSP "
+              f"solves (the first source's round count for each), E counted per PageRank iteration and per SSSP "
+              f"source as in the GPU arm; single-threaded (the reference has no threads)")
     shard = args.workload == "shard"  # the same CPU work; the shard arm's metric and config
     line = {"impl": "reference", "metric": SHARD_METRIC if shard else METRIC, "value": value, "unit": UNIT,
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
             "higher_is_better": True, "scaling": "strong" if shard else "weak", "vs_baseline": None,
             "dtype": "f32/u32", "data": "synthetic",
             "config": shard_config(args, V, E, args.gpus) if shard else workload_config(args, V, E),
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": kind, "sample": sample},
-            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cpu.cores, "kind": cpu.kind, "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "projection": {"parts": parts, "step_s": steps}}
     print(json.dumps(line), flush=True)
 
 
@@ -1412,13 +1502,14 @@ def main():
     graph = hyt.Graph(dcsr, stream=sptr, flags=gflags)
     dcsr.free()
     ranks_out = torch.empty(V, dtype=torch.float32, device="cuda")
-    dist_out = torch.empty(V, dtype=torch.int32, device="cuda")
+    # one label array per source, so the timed run's results are all checked
+    dist_outs = [torch.empty(V, dtype=torch.int32, device="cuda") for _ in sources]
 
     def step(collect):
         _, st = graph.pagerank(out=ranks_out, stream=sptr)
         collect["pr"].append(st)
-        for s in sources:
-            _, ss = graph.sssp(s, out=dist_out, stream=sptr)
+        for s, d in zip(sources, dist_outs):
+            _, ss = graph.sssp(s, out=d, stream=sptr)
             collect["sssp"].append(ss)
 
     warm = {"pr": [], "sssp": []}
@@ -1474,6 +1565,11 @@ def main():
         roof["traffic_measured"] = bool(tr.get("measured", False))
 
     launches = sum(s["total_launches"] for s in timed["pr"]) + sum(s["total_launches"] for s in timed["sssp"])
+    # results of the timed run, for the parity check after the timed regions
+    torch.cuda.synchronize()
+    ranks_timed = ranks_out.cpu().numpy()
+    dists_timed = [d.cpu().numpy().view(np.uint32) for d in dist_outs]
+    del dist_outs
 
     # ---- e2e: the C-ABI with HOST (pinned) buffers, copies inside the timed region ----
     ranks_h = torch.empty(V, dtype=torch.float32, pin_memory=True)
@@ -1506,14 +1602,31 @@ def main():
     h2d = (V + 1) * 8 + E * 4 + E * 4
     d2h = V * 4 * (1 + len(sources))
 
+    # ---- parity of the timed run against the oracle (rank 0) ----
+    parity = None
+    if rank == 0 and not args.no_parity:
+        parity = parity_inhbm(off_np, csr_h.column_indices, csr_h.weights, sources, ranks_timed, dists_timed)
+        parity["gpu_pr_iterations"] = int(timed["pr"][-1]["iterations"])
+
     # ---- CPU baseline (rank 0, N=1 only) ----
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        e, t, kind = cpu_sample(off_np, csr_h.column_indices, csr_h.weights.astype(np.float32), sources[0])
-        cpu = {"value": e / t / 1e9, "unit": UNIT, "cores": 1, "kind": kind,
-               "sample": (f"1 PageRank iteration + 1 SSSP round of the reference's single-threaded "
-                          f"pagerank_cpu/sssp_cpu (each incl. its incoming-CSR build) on this graph, "
-                          f"{t:.1f} s; E counted per iteration/round")}
+        solvers = CpuSolvers()
+        n_pr = parity["_ref_iterations"] if parity else 100
+        n_ss = parity["_ref_rounds_source0"] if parity else 10
+        t_step, parts, t_sample = cpu_baseline_sample(solvers, off_np, csr_h.column_indices,
+                                                      csr_h.weights.astype(np.float32), sources[0], n_pr, n_ss,
+                                                      len(sources))
+        cpu = {"value": (E * n_pr + E * len(sources)) / t_step / 1e9, "unit": UNIT, "cores": solvers.cores,
+               "kind": solvers.kind,
+               "sample": (f"pagerank_cpu for 1 and 3 iterations and sssp_cpu for 1 and 3 rounds on this graph "
+                          f"({t_sample:.1f} s); projected to one step (PageRank to convergence in the reference's "
+                          f"{n_pr} iterations + {len(sources)} full SSSP solves of {n_ss} rounds), E counted per "
+                          f"PageRank iteration and per SSSP source as above"),
+               "projected_step_s": t_step, "parts": parts}
+    if parity:
+        parity.pop("_ref_iterations", None)
+        parity.pop("_ref_rounds_source0", None)
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -1522,7 +1635,7 @@ def main():
                 "data": "synthetic", "config": workload_config(args, V, E),
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "ms_per_step": e2e_ms / args.e2e_steps, "steps": args.e2e_steps},
-                "roofline": roof, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches,
+                "roofline": roof, "cpu_baseline": cpu, "parity": parity, "clocks": clk, "gpu_launches": launches,
                 "pagerank": {"iterations_per_solve": pr_it / args.steps, "ms_per_solve": pr_ms / args.steps,
                              "gteps": E * pr_it / (pr_ms / 1e3) / 1e9, "achieved_gbs": pr_gbs},
                 "sssp": {"solves": len(timed["sssp"]), "ms_per_solve": ss_ms / len(timed["sssp"]),
