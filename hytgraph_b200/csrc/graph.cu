@@ -295,11 +295,47 @@ void graph_copy_csc(const GraphImpl &g, uint64_t *in_offsets, uint32_t *in_sourc
 
 size_t GraphImpl::device_bytes() const {
     size_t b = row_offsets.bytes() + cols.bytes() + weights.bytes() + out_degree.bytes() + in_offsets.bytes() +
-               in_sources.bytes() + in_weights.bytes() + tile_start.bytes() + long_rows.bytes() + chunk_tasks.bytes();
+               in_sources.bytes() + in_weights.bytes() + tile_start.bytes() + long_rows.bytes() + chunk_tasks.bytes() +
+         pull_tasks.bytes();
     for (int i = 0; i < 2; ++i) b += rank[i].bytes() + contrib[i].bytes() + queue[i].bytes() + far[i].bytes();
     b += partial.bytes() + ticket.bytes() + pr_state.bytes() + dist.bytes() + stamp.bytes() + hub_tasks.bytes() +
          sssp_state.bytes();
     return b;
+}
+
+// Descriptor of pull task i (graph.cuh): chunks [0, num_chunks), then tiles.
+__global__ void pull_task_kernel(const uint64_t *in_off, const uint32_t *tile_start, const LongRow *long_rows,
+                                 const uint2 *chunk_tasks, uint64_t num_chunks, uint64_t num_tiles, uint32_t tile_cost,
+                                 uint4 *out) {
+    const uint64_t n = num_chunks + num_tiles, stride = uint64_t(gridDim.x) * blockDim.x;
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += stride) {
+        uint64_t e0 = 0, len = 0;
+        uint32_t a = 0, b = 0, chunk = 0;
+        if (i < num_chunks) {
+            const uint2 t = chunk_tasks[i];
+            const LongRow L = long_rows[t.x];
+            const uint64_t rb = in_off[L.row], re = in_off[L.row + 1];
+            e0 = rb + uint64_t(t.y) * kLongChunk;
+            len = ((e0 + kLongChunk < re) ? e0 + kLongChunk : re) - e0;
+            a = t.x;
+            b = t.y;
+            chunk = 1;
+        } else {
+            const uint64_t k = i - num_chunks;
+            const uint32_t r0 = tile_start[k], r1 = tile_start[k + 1];
+            a = b = r0;
+            e0 = in_off[r0];
+            if (r0 != r1) {
+                const uint64_t last_b = in_off[r1 - 1], last_e = in_off[r1];
+                const uint32_t rl = (last_e - last_b >= tile_cost) ? r1 - 1 : r1;  // a long last row is chunked
+                len = ((rl == r1) ? last_e : last_b) - e0;
+                b = rl;
+            }
+        }
+        out[i] = make_uint4(static_cast<uint32_t>(e0),
+                            static_cast<uint32_t>((e0 >> 32) & 0xFFu) | static_cast<uint32_t>(len << 8) | (chunk << 31),
+                            a, b);
+    }
 }
 
 // Work tiles and long-row chunks of the pull side, from g.in_offsets on the
@@ -351,6 +387,13 @@ void build_pull_tiles(GraphImpl &g, cudaStream_t s) {
     if (g.num_chunks)
         HYT_CUDA(cudaMemcpyAsync(g.chunk_tasks.get(), tasks.data(), tasks.size() * sizeof(uint2),
                                  cudaMemcpyHostToDevice, s));
+    // One descriptor per task (first edges below 2^40).
+    const uint64_t ntasks = g.num_chunks + g.num_tiles;
+    g.pull_tasks.allocate(ntasks);
+    pull_task_kernel<<<grid_for(ntasks, 256), 256, 0, s>>>(g.in_offsets.get(), g.tile_start.get(), g.long_rows.get(),
+                                                            g.chunk_tasks.get(), g.num_chunks, g.num_tiles, g.tile_cost,
+                                                            g.pull_tasks.get());
+    HYT_CUDA(cudaGetLastError());
     HYT_CUDA(cudaStreamSynchronize(s));
 }
 
@@ -366,7 +409,7 @@ void graph_build(GraphImpl &g, const hyt_csr &csr, uint32_t flags) {
         fail(HYT_E_INVALID, "weights is NULL for a weighted graph");
     if (flags == 0) flags = HYT_GRAPH_ALL;
     // PageRank decomposition knobs (same work, different tiling): tile cost
-    // in {64..512} and hot-source cache size, bounded by shared memory.
+    // in {64..256} and hot-source cache size, bounded by shared memory.
     g.tile_cost = kTileCostDefault;
     if (const char *t = std::getenv("HYT_PR_TILE")) {
         const unsigned long v = std::strtoul(t, nullptr, 10);

@@ -25,13 +25,26 @@ namespace hyt {
 // the tile and split into kLongChunk-edge chunks.  One warp processes one
 // task (tile or chunk), so a tile's staged contributions fit in a per-warp
 // shared-memory slice of 2 * tile_cost floats.
-constexpr uint32_t kTileCostDefault = 512;   // merge-path units per tile (tunable: HYT_PR_TILE)
-constexpr uint32_t kTileCostMax = 512;
+constexpr uint32_t kTileCostDefault = 256;   // merge-path units per tile (tunable: HYT_PR_TILE)
+constexpr uint32_t kTileCostMax = 256;       // a tile's edges (< 2 * tile_cost) fit one staging slot
 constexpr uint32_t kLongChunk = 4096;
 constexpr uint32_t kHotSourcesDefault = 8192;   // shared-memory source cache (tunable: HYT_PR_HOT)
 constexpr uint32_t kHotSourcesMax = 32768;
 constexpr uint32_t kPRSmemMax = 226 * 1024;     // dynamic shared memory per CTA (227 KB opt-in - static)
 constexpr uint32_t kHotTag = 0x80000000u;       // in_sources tag: source is hot slot (low bits)
+
+// Pull task descriptors (pull_tasks[i], chunks first, then tiles: the task
+// numbering of the pull kernels), 16 bytes each so a warp fetches its next
+// task with one load:
+//   x = first edge (low 32 bits)
+//   y = first edge bits 32..39 | edge count << 8 (< 2^23) | 1 << 31 for a chunk
+//   z, w = first row and end row of a tile (the end excludes a chunked long
+//          last row); long-row index and chunk number of a chunk
+__host__ __device__ __forceinline__ uint64_t task_first_edge(uint4 d) {
+    return uint64_t(d.x) | (uint64_t(d.y & 0xFFu) << 32);
+}
+__host__ __device__ __forceinline__ uint32_t task_edges(uint4 d) { return (d.y >> 8) & 0x7FFFFFu; }
+__host__ __device__ __forceinline__ bool task_is_chunk(uint4 d) { return (d.y >> 31) != 0; }
 
 struct LongRow {
     uint32_t row;
@@ -68,6 +81,7 @@ struct GraphImpl {
     GraphArray<uint32_t> tile_start;   // [num_tiles + 1]
     GraphArray<LongRow> long_rows;     // [num_long]
     GraphArray<uint2> chunk_tasks;     // [num_chunks] = (long row index, chunk)
+    GraphArray<uint4> pull_tasks;      // [num_chunks + num_tiles] descriptors (task_first_edge, ...)
     uint64_t num_tiles = 0, num_long = 0, num_chunks = 0;
     uint32_t tile_cost = kTileCostDefault;  // a row is long when its in-degree >= tile_cost
     // Hot sources: the num_hot vertices of largest out-degree.  Their

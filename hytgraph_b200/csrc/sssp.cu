@@ -43,6 +43,7 @@
 #include "hybrid.cuh"
 #include "solvers.cuh"
 #include "sssp_core.cuh"
+#include "stage.cuh"
 
 namespace hyt {
 namespace {
@@ -123,6 +124,7 @@ struct PullGraph {
     const LongRow *long_rows;
     const uint2 *chunk_tasks;
     const uint32_t *hot_vertex;
+    const uint4 *tasks;       // pull task descriptors (staged sweeps)
     uint64_t num_tiles, num_chunks;
     uint32_t tile_cost;
     uint32_t num_hot;
@@ -263,6 +265,134 @@ __global__ void __launch_bounds__(kPullThreads, 1) sssp_pull_kernel(const SSArgs
     }
 }
 
+// ---- staged pull sweeps (CSC in HBM; pipeline in stage.cuh) ----------------
+
+// Candidate labels d[u] + w of staged edges [lo, hi) (ids at slot[x - a0]):
+// lane l takes edges lo + 32k + l; weights stream straight from HBM while
+// the label gathers are in flight.  sink(i, candidate) receives edge lo + i.
+template <int WK, class Sink>
+__device__ __forceinline__ void pull_staged(const SSArgs &a, const PullGraph &pg, const uint32_t *s_hot,
+                                            const uint32_t *slot, uint64_t a0, uint64_t lo, uint64_t hi, uint64_t pol,
+                                            int lane, Sink &&sink) {
+    constexpr int kB = stage::kUnitEdges / 32;
+    const uint32_t n = static_cast<uint32_t>(hi - lo);
+    const uint32_t *ids = slot + (lo - a0);
+    uint32_t w[kB], du[kB];
+#pragma unroll
+    for (int k = 0; k < kB; ++k) {
+        const uint32_t i = 32 * k + lane;
+        w[k] = (i < n) ? edge_weight<WK>(pg.in_w, lo + i) : 0u;
+    }
+#pragma unroll
+    for (int k = 0; k < kB; ++k) {
+        const uint32_t i = 32 * k + lane;
+        uint32_t id = (i < n) ? ids[i] : 0u;
+        if (id & kHotTag) id = s_hot[id & ~kHotTag];  // hot slot -> vertex id
+        du[k] = dev::ld_keep_u32(a.dist + id, pol);
+    }
+#pragma unroll
+    for (int k = 0; k < kB; ++k) {
+        const uint32_t i = 32 * k + lane;
+        if (i < n) sink(i, du[k] == a.inf ? a.inf : extend<WK>(du[k], w[k]));
+    }
+}
+
+// pull_relax with the row's label read ahead of time: a stale (higher)
+// label only lets through an atomicMin that then finds no improvement.
+__device__ __forceinline__ bool pull_relax_seen(const SSArgs &a, const RoundView &rv, uint32_t r, uint32_t c,
+                                                uint32_t seen) {
+    if (c >= seen) return false;
+    const uint32_t old = atomicMin(a.dist + r, c);
+    if (c >= old) return false;
+    return atomicExch(a.stamp + r, rv.next_stamp) != rv.next_stamp;
+}
+
+template <int WK>
+__global__ void __launch_bounds__(kPullThreads, 1) sssp_pull_staged_kernel(const SSArgs *__restrict__ args,
+                                                                           PullGraph pg) {
+    extern __shared__ __align__(128) unsigned char s_stage[];
+    const SSArgs a = *args;
+    if (*(volatile uint32_t *)&a.hdr->done || !pull_round(a)) return;
+    const RoundView rv = round_view(a);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const stage::WarpStage ws = stage::warp_stage(s_stage, warp, lane);
+    uint32_t *s_hot = reinterpret_cast<uint32_t *>(s_stage + stage::kStageBytes);  // vertex ids of the hot slots
+    for (uint32_t i = threadIdx.x; i < pg.num_hot; i += blockDim.x) s_hot[i] = pg.hot_vertex[i];
+    __syncthreads();
+    const uint64_t pol = dev::policy_evict_last();
+    const uint64_t total = pg.num_chunks + pg.num_tiles;
+    const uint64_t nwarps = uint64_t(gridDim.x) * (kPullThreads / 32);
+    uint32_t best = a.inf;  // running minimum of the current chunk
+    const bool ok = stage::stage_pipeline(
+        pg.tasks, pg.in_src, uint64_t(blockIdx.x) * (kPullThreads / 32) + warp, nwarps, total, ws.slots, ws.bars,
+        lane, [&](uint4 d, uint64_t, uint32_t j, uint32_t nu, uint32_t *slot, uint64_t a0) {
+            if (task_is_chunk(d)) {
+                // slice of a long row: warp minimum, then one relaxation
+                const stage::Unit u = stage::unit_of(d, j);
+                if (j == 0) best = a.inf;
+                pull_staged<WK>(a, pg, s_hot, slot, a0, u.lo, u.hi, pol, lane,
+                                [&](uint32_t, uint32_t c) { best = min(best, c); });
+                if (j + 1 < nu) return;
+                uint32_t m = best;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) m = min(m, __shfl_xor_sync(0xffffffffu, m, o));
+                if (lane == 0) {
+                    const uint32_t row = pg.long_rows[d.z].row;
+                    if (pull_relax(a, rv, row, m)) append(rv.qnext, rv.qnext_size, row);
+                }
+                return;
+            }
+            // merge-path tile of short rows: candidates replace the ids in
+            // the slot, then each row takes its minimum
+            const uint32_t r0 = d.z, rl = d.w;
+            const uint64_t e0 = task_first_edge(d), e1 = e0 + task_edges(d);
+            const uint32_t r = r0 + lane;
+            const bool act0 = r < rl;
+            const uint64_t lo0 = act0 ? pg.in_off[r] : 0, hi0 = act0 ? pg.in_off[r + 1] : 0;  // in flight
+            const uint32_t seen0 = act0 ? __ldcg(a.dist + r) : 0u;
+            pull_staged<WK>(a, pg, s_hot, slot, a0, e0, e1, pol, lane,
+                            [&](uint32_t i, uint32_t c) { slot[e0 - a0 + i] = c; });
+            __syncwarp();
+            for (uint32_t rb = r0; rb < rl; rb += 32) {
+                const uint32_t rr = rb + lane;
+                const bool active = rr < rl;
+                const bool first = rb == r0;
+                const uint64_t lo = first ? lo0 : (active ? pg.in_off[rr] : 0);
+                const uint64_t hi = first ? hi0 : (active ? pg.in_off[rr + 1] : 0);
+                bool joined = false;
+                if (active && hi - lo < 64) {
+                    uint32_t m = a.inf;
+                    for (uint64_t x = lo; x < hi; ++x) m = min(m, slot[x - a0]);
+                    joined = first ? pull_relax_seen(a, rv, rr, m, seen0) : pull_relax(a, rv, rr, m);
+                }
+                uint32_t big = __ballot_sync(0xffffffffu, active && (hi - lo >= 64));
+                while (big) {
+                    const int src = __ffs(big) - 1;
+                    big &= big - 1;
+                    const uint64_t bb = __shfl_sync(0xffffffffu, lo, src);
+                    const uint64_t ee = __shfl_sync(0xffffffffu, hi, src);
+                    uint32_t m = a.inf;
+                    for (uint64_t x = bb + lane; x < ee; x += 32) m = min(m, slot[x - a0]);
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) m = min(m, __shfl_xor_sync(0xffffffffu, m, o));
+                    const bool jn = (lane == 0) && pull_relax(a, rv, rb + src, m);
+                    if (__shfl_sync(0xffffffffu, jn ? 1u : 0u, 0) && lane == src) joined = true;
+                }
+                const uint32_t vals[1] = {rr};
+                warp_append<1>(rv.qnext, rv.qnext_size, vals, joined ? 1u : 0u, lane);
+            }
+        });
+    if (!ok) {
+        atomicExch(&a.hdr->error, 1u);
+        atomicExch(&a.hdr->done, 1u);
+        if (a.use_cond) cudaGraphSetConditional(a.cond, 0);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        atomicAdd(&a.hdr->relaxations, static_cast<unsigned long long>(a.num_edges));
+        atomicAdd(&a.hdr->pull_rounds, 1u);
+    }
+}
+
 __global__ void sssp_round_end_kernel(const SSArgs *__restrict__ args) {
     const SSArgs a = *args;
     if (a.hdr->done) return;
@@ -394,16 +524,31 @@ uint32_t sssp_pull_div() {
 }
 
 template <int WK>
-int pull_grid(unsigned smem) {
+int pull_grid(bool staged, unsigned smem) {
     static bool attr = false;
     if (!attr) {
         HYT_CUDA(cudaFuncSetAttribute(sssp_pull_kernel<WK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       static_cast<int>(kPRSmemMax)));
+        HYT_CUDA(cudaFuncSetAttribute(sssp_pull_staged_kernel<WK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(kPRSmemMax)));
         attr = true;
     }
     int per_sm = 0;
-    HYT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sssp_pull_kernel<WK>, kPullThreads, smem));
+    if (staged)
+        HYT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sssp_pull_staged_kernel<WK>, kPullThreads, smem));
+    else
+        HYT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sssp_pull_kernel<WK>, kPullThreads, smem));
     return sm_count() * std::max(per_sm, 1);
+}
+
+// HYT_STAGED=0 selects the register-path pull sweep (same sweep; for
+// comparisons).
+bool pull_use_staged(const GraphImpl &g) {
+    static const bool env_off = [] {
+        const char *e = std::getenv("HYT_STAGED");
+        return e && e[0] == '0';
+    }();
+    return !env_off && g.pull_tasks.get() && stage::staged_shared_bytes(g.num_hot) <= kPRSmemMax;
 }
 
 template <int WK>
@@ -465,14 +610,19 @@ void sssp_solve(GraphImpl &g, uint32_t source, uint32_t delta, uint32_t max_roun
         pg.long_rows = g.long_rows.get();
         pg.chunk_tasks = g.chunk_tasks.get();
         pg.hot_vertex = g.hot_vertex.get();
+        pg.tasks = g.pull_tasks.get();
         pg.num_tiles = g.num_tiles;
         pg.num_chunks = g.num_chunks;
         pg.tile_cost = g.tile_cost;
         pg.num_hot = g.num_hot;
     }
+    const bool staged = a.pull_div && pull_use_staged(g);
     const unsigned pull_smem =
-        static_cast<unsigned>((g.num_hot + kPullThreads / 32 * (2 * size_t(g.tile_cost) + 8)) * 4);
-    const int pgrid = a.pull_div ? pull_grid<WK>(pull_smem) : 0;
+        staged ? static_cast<unsigned>(stage::staged_shared_bytes(g.num_hot))
+               : static_cast<unsigned>((g.num_hot + kPullThreads / 32 * (2 * size_t(g.tile_cost) + 8)) * 4);
+    const int pgrid = a.pull_div ? pull_grid<WK>(staged, pull_smem) : 0;
+    const void *pull_fn = staged ? reinterpret_cast<const void *>(sssp_pull_staged_kernel<WK>)
+                                 : reinterpret_cast<const void *>(sssp_pull_kernel<WK>);
 
     SSHeader h0{};
     h0.qsize[0] = 1;
@@ -528,7 +678,7 @@ void sssp_solve(GraphImpl &g, uint32_t source, uint32_t delta, uint32_t max_roun
         if (a.pull_div) add(reinterpret_cast<void *>(sssp_frontier_edges_kernel), dim3(grid), dim3(kSSThreads), 0, kargs);
         add(reinterpret_cast<void *>(sssp_expand_kernel<WK>), dim3(grid), dim3(kSSThreads), 0, kargs);
         add(reinterpret_cast<void *>(sssp_hub_kernel<WK>), dim3(grid), dim3(kSSThreads), 0, kargs);
-        if (a.pull_div) add(reinterpret_cast<void *>(sssp_pull_kernel<WK>), dim3(pgrid), dim3(kPullThreads), pull_smem, pargs);
+        if (a.pull_div) add(pull_fn, dim3(pgrid), dim3(kPullThreads), pull_smem, pargs);
         add(reinterpret_cast<void *>(sssp_round_end_kernel), dim3(1), dim3(1), 0, kargs);
         HYT_CUDA(cudaGraphInstantiate(&exec, graph, 0));
         HYT_CUDA(cudaGraphLaunch(exec, s));
@@ -540,7 +690,12 @@ void sssp_solve(GraphImpl &g, uint32_t source, uint32_t delta, uint32_t max_roun
             if (a.pull_div) sssp_frontier_edges_kernel<<<grid, kSSThreads, 0, s>>>(d_args);
             sssp_expand_kernel<WK><<<grid, kSSThreads, 0, s>>>(d_args);
             sssp_hub_kernel<WK><<<grid, kSSThreads, 0, s>>>(d_args);
-            if (a.pull_div) sssp_pull_kernel<WK><<<pgrid, kPullThreads, pull_smem, s>>>(d_args, pg);
+            if (a.pull_div) {
+                if (staged)
+                    sssp_pull_staged_kernel<WK><<<pgrid, kPullThreads, pull_smem, s>>>(d_args, pg);
+                else
+                    sssp_pull_kernel<WK><<<pgrid, kPullThreads, pull_smem, s>>>(d_args, pg);
+            }
             if (flags & HYT_RUN_PROFILE) kt.stop(s);
             sssp_round_end_kernel<<<1, 1, 0, s>>>(d_args);
             HYT_CUDA(cudaGetLastError());
@@ -560,6 +715,7 @@ void sssp_solve(GraphImpl &g, uint32_t source, uint32_t delta, uint32_t max_roun
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
     if (use_graph) launches += 4 * h.round;
+    if (h.error) fail(HYT_E_TIMEOUT, "SSSP: a bounded wait for a staged copy ran out");
     if (dist_out) graph_emit(g, dist_out, g.dist.get(), s);
     if (stats) {
         stats->iterations = h.round;

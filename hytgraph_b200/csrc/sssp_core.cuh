@@ -49,7 +49,7 @@ struct SSHeader {
     unsigned long long frontier_total;  // frontier vertices expanded
     unsigned long long frontier_edges;  // out-edges of this round's frontier (pull-capable solves)
     uint32_t pull_rounds;               // rounds run as pull sweeps
-    uint32_t pad;
+    uint32_t error;                     // 1: a bounded wait for a staged copy ran out
 };
 
 struct SSArgs {

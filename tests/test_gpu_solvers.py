@@ -82,6 +82,74 @@ def test_scale20_parity_with_the_oracle(hyt, oracle, gpu):
                 assert np.array_equal(dg.sssp(s)[0], w), (flags, s)
 
 
+_RANKS_SCRIPT = """
+import sys, numpy as np
+sys.path.insert(0, %r)
+import hytgraph_b200 as hyt
+g = hyt.rmat(20, 16, 7)
+with hyt.Graph(g, flags=hyt.capi.HYT_GRAPH_ALL | hyt.capi.HYT_GRAPH_HUB_ORDER) as dg:
+    r, st = dg.pagerank()
+    p, sp = dg.ppr(12345)
+sys.stdout.buffer.write(np.array([st["iterations"], sp["iterations"]], np.uint32).tobytes() + r.tobytes() + p.tobytes())
+"""
+
+
+def test_pagerank_bit_identical_across_runs_grids_and_kernels(hyt, gpu):
+    """PageRank and personalized PageRank give the same bits and iteration
+    counts on every run, under other persistent grid sizes, and with the
+    register-path kernel instead of the bulk-staged one: row sums and the
+    FP64 residual / dangling sums have fixed association orders."""
+    import os
+    import subprocess
+    import sys
+
+    from conftest import ROOT
+
+    g = hyt.rmat(20, 16, 7)
+    with hyt.Graph(g, flags=hyt.capi.HYT_GRAPH_ALL | hyt.capi.HYT_GRAPH_HUB_ORDER) as dg:
+        runs = [dg.pagerank() for _ in range(10)]
+        ppr = [dg.ppr(12345) for _ in range(3)]
+    for r, st in runs[1:]:
+        assert st["iterations"] == runs[0][1]["iterations"]
+        assert np.array_equal(r.view(np.uint32), runs[0][0].view(np.uint32))
+    for p, sp in ppr[1:]:
+        assert sp["iterations"] == ppr[0][1]["iterations"]
+        assert np.array_equal(p.view(np.uint32), ppr[0][0].view(np.uint32))
+    want = (np.array([runs[0][1]["iterations"], ppr[0][1]["iterations"]], np.uint32).tobytes() +
+            runs[0][0].tobytes() + ppr[0][0].tobytes())
+    for env in ({"HYT_PR_GRID": "37"}, {"HYT_PR_GRID": "300"}, {"HYT_STAGED": "0"}):
+        out = subprocess.run([sys.executable, "-c", _RANKS_SCRIPT % str(ROOT)], capture_output=True,
+                             env=dict(os.environ, **env), timeout=600)
+        assert out.returncode == 0, out.stderr.decode()[-2000:]
+        assert out.stdout == want, env
+
+
+def test_sssp_staged_and_register_sweeps_agree(hyt, gpu):
+    """The bulk-staged pull sweep and the register-path one reach the same
+    labels (the unique shortest-path fixed point) on a graph whose frontiers
+    trigger pull rounds (a pull sweep counts every edge as relaxed, so a
+    solve with one relaxes more edges than the graph has)."""
+    import os
+    import subprocess
+    import sys
+
+    from conftest import ROOT
+
+    code = ("import sys, numpy as np; sys.path.insert(0, %r); import hytgraph_b200 as hyt; "
+            "g = hyt.rmat(18, 16, 3); src = hyt.pick_sources(g.row_offsets, 3, 3); "
+            "dg = hyt.Graph(g, flags=hyt.capi.HYT_GRAPH_ALL | hyt.capi.HYT_GRAPH_HUB_ORDER); "
+            "out = [dg.sssp(int(s)) for s in src]; "
+            "assert all(st['edges_processed'] > g.num_edges for _, st in out), [st for _, st in out]; "
+            "sys.stdout.buffer.write(b''.join(d.tobytes() for d, _ in out))") % str(ROOT)
+    outs = []
+    for staged in ("1", "0"):
+        r = subprocess.run([sys.executable, "-c", code], capture_output=True, env=dict(os.environ, HYT_STAGED=staged),
+                           timeout=600)
+        assert r.returncode == 0, r.stderr.decode()[-2000:]
+        outs.append(r.stdout)
+    assert outs[0] == outs[1] and len(outs[0]) > 0
+
+
 def test_pagerank_deterministic_across_modes(hyt, gpu):
     g = hyt.rmat(15, 16, 11)
     with hyt.Graph(g) as dg:
