@@ -562,10 +562,17 @@ def run_batch_workload(args, rank, world, pg):
         e2e_wall = time.perf_counter() - t0
     traversed = sum(E_of[q["graph"]] * (r["iterations"] if q["kind"] == "ppr" else 1) for q, r in zip(queries, res))
     n_q = len(queries)
-    # one at a time: the same queries through hyt_sssp / hyt_ppr, outputs on the device
-    for q, o in zip(queries[:8], dev_out[:8]):
-        g = graphs[q["graph"]]
-        (g.sssp(q["source"], out=o) if q["kind"] == "sssp" else g.ppr(q["source"], out=o))
+    # a sample of the timed batch's results, checked against the oracle below
+    torch.cuda.synchronize()
+    sample_idx = list(range(0, n_q, max(1, n_q // 16)))[:16]
+    sample_out = {i: dev_out[i].cpu().numpy().copy() for i in sample_idx}
+    # one at a time: the same queries through hyt_sssp / hyt_ppr, outputs on
+    # the device; every graph's solver state is allocated before timing
+    for gi, g in enumerate(graphs):
+        src = next(q["source"] for q in queries if q["graph"] == gi)
+        o = torch.empty(V_of[gi], dtype=torch.float32, device="cuda")
+        g.sssp(src, out=o.view(torch.int32))
+        g.ppr(src, out=o)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
@@ -578,6 +585,9 @@ def run_batch_workload(args, rank, world, pg):
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu = batch_cpu_sample(hyt, specs, queries)
+    parity = None
+    if rank == 0 and not args.no_parity:
+        parity = query_parity(specs, queries, sample_out)
     if rank == 0:
         gteps = traversed * world / (ms / 1e3) / 1e9
         line = {"metric": METRIC, "value": gteps, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -606,11 +616,42 @@ def run_batch_workload(args, rank, world, pg):
                              "peak": load_peaks()[0], "unit": "GB/s",
                              "frac": st["algorithmic_bytes"] / (ms / 1e3) / 1e9 / load_peaks()[0],
                              "traffic": None, "peak_kind": load_peaks()[1]},
-                "cpu_baseline": cpu, "clocks": clk, "gpu_launches": st["kernel_launches"]}
+                "cpu_baseline": cpu, "parity": parity, "clocks": clk, "gpu_launches": st["kernel_launches"]}
         line["config"]["vertex_order"] = args.vertex_order
         print(json.dumps(line), flush=True)
     for g in graphs:
         g.close()
+
+
+def query_parity(specs, queries, results):
+    """Query results (index -> host array) against the oracle on the same
+    graphs, rebuilt by the oracle's generator: SSSP labels against Dijkstra
+    (exact), personalized PageRank L1 against the FP64 restatement."""
+    from oracle.bindings import Oracle
+
+    o = Oracle()
+    host = {}
+    sssp_n = sssp_bad = ppr_n = 0
+    worst_l1 = 0.0
+    for i, out in results.items():
+        q = queries[i]
+        gi = q["graph"]
+        if gi not in host:
+            sc, ef, gseed = specs[gi]
+            host[gi] = o.rmat(sc, ef, gseed)
+        off, cols, w = host[gi]
+        if q["kind"] == "sssp":
+            d = o.dijkstra(off, cols, w, q["source"])
+            want = np.where(d == np.iinfo(np.uint64).max, 0xFFFFFFFF, d).astype(np.uint32)
+            sssp_n += 1
+            sssp_bad += int(np.count_nonzero(out.view(np.uint32) != want))
+        else:
+            r, _, _, _ = o.ppr_f64(off, cols, q["source"], q["restart"], q["tolerance"])
+            ppr_n += 1
+            worst_l1 = max(worst_l1, float(np.abs(out.view(np.float32).astype(np.float64) - r).sum()))
+    return {"queries_checked": len(results), "sssp_checked": sssp_n, "sssp_mismatches": sssp_bad,
+            "ppr_checked": ppr_n, "ppr_max_l1_vs_fp64": worst_l1, "ppr_l1_tolerance": 1e-5,
+            "ok": bool(sssp_bad == 0 and worst_l1 <= 1e-5)}
 
 
 def batch_cpu_sample(hyt, specs, queries):

@@ -6,6 +6,9 @@
 #include <cstring>
 #include <limits>
 #include <memory>
+#include <tuple>
+#include <mutex>
+#include <map>
 #include <string>
 
 #include "batch.cuh"
@@ -1123,7 +1126,38 @@ int hyt_batch_run(hyt_batch *b, const hyt_query *queries, uint32_t num_queries, 
 // Coordinate descent over the tuning knobs on an evenly spaced sample of
 // the queries (at most 128, outputs dropped): bucket width first, then the
 // hub threshold, then the persistent grid; each candidate is timed twice
-// and scored by its faster run.
+// and scored by its faster run.  The choice is cached for the process per
+// size class of the sample -- device, log2 of its mean graph edges and of
+// its mean graph vertices, and its SSSP share in quarters -- so a later
+// batch of the same class reuses it without timing anything.
+namespace {
+struct TuneClass {
+    int device;
+    int log_edges, log_vertices, sssp_quarters;
+    bool operator<(const TuneClass &o) const {
+        return std::tie(device, log_edges, log_vertices, sssp_quarters) <
+               std::tie(o.device, o.log_edges, o.log_vertices, o.sssp_quarters);
+    }
+};
+std::mutex g_tune_mu;
+std::map<TuneClass, BatchTuning> g_tune_cache;
+
+TuneClass tune_class(const hyt_batch *b, const std::vector<hyt_query> &sample) {
+    double e = 0.0, v = 0.0;
+    uint32_t sssp = 0;
+    for (const hyt_query &q : sample) {
+        const GraphImpl &g = *b->graphs[q.graph];
+        e += static_cast<double>(g.E);
+        v += static_cast<double>(g.V);
+        sssp += q.kind == HYT_QUERY_SSSP ? 1u : 0u;
+    }
+    const double n = static_cast<double>(sample.size());
+    return TuneClass{b->device, static_cast<int>(std::lround(std::log2(std::max(e / n, 1.0)))),
+                     static_cast<int>(std::lround(std::log2(std::max(v / n, 1.0)))),
+                     static_cast<int>(std::lround(4.0 * sssp / n))};
+}
+}  // namespace
+
 int hyt_batch_autotune(hyt_batch *b, const hyt_query *queries, uint32_t num_queries, hyt_batch_tuning *chosen) {
     return guarded([&] {
         batch_impl(b);
@@ -1136,6 +1170,23 @@ int hyt_batch_autotune(hyt_batch *b, const hyt_query *queries, uint32_t num_quer
             sample[i].out = nullptr;
         }
         for (const hyt_query &q : sample) b->engine->validate(q);
+        auto report = [&](const BatchTuning &t) {
+            if (chosen) {
+                chosen->delta_mult = t.delta_mult;
+                chosen->hub_degree = t.hub_degree;
+                chosen->ctas_per_sm = t.ctas_per_sm;
+            }
+        };
+        const TuneClass cls = tune_class(b, sample);
+        {
+            std::lock_guard<std::mutex> lk(g_tune_mu);
+            const auto it = g_tune_cache.find(cls);
+            if (it != g_tune_cache.end()) {
+                b->tuning = it->second;
+                report(it->second);
+                return;
+            }
+        }
         auto time_it = [&](const BatchTuning &t) {
             b->tuning = t;
             double best = 1e30;
@@ -1171,11 +1222,11 @@ int hyt_batch_autotune(hyt_batch *b, const hyt_query *queries, uint32_t num_quer
         sweep([](BatchTuning &t, uint32_t v) { t.hub_degree = v; }, {32u, 64u, 128u, 256u});
         sweep([](BatchTuning &t, uint32_t v) { t.ctas_per_sm = v; }, {0u, 1u, 2u});
         b->tuning = best;
-        if (chosen) {
-            chosen->delta_mult = best.delta_mult;
-            chosen->hub_degree = best.hub_degree;
-            chosen->ctas_per_sm = best.ctas_per_sm;
+        {
+            std::lock_guard<std::mutex> lk(g_tune_mu);
+            g_tune_cache[cls] = best;
         }
+        report(best);
     });
 }
 

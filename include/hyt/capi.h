@@ -406,7 +406,10 @@ int hyt_batch_destroy(hyt_batch *batch);
 int hyt_batch_run(hyt_batch *batch, const hyt_query *queries, uint32_t num_queries,
                   hyt_query_result *results, hyt_batch_stats *stats);
 /* Times the batch on a sample of `queries` under a grid of tunings and
- * keeps the fastest for later runs; *chosen receives it. */
+ * keeps the fastest for later runs; *chosen receives it.  The choice is
+ * cached for the process per size class of the sample (device, log2 of its
+ * mean graph edges and vertices, SSSP share in quarters): a later call with
+ * a sample of the same class applies the cached tuning without timing. */
 int hyt_batch_autotune(hyt_batch *batch, const hyt_query *queries, uint32_t num_queries,
                        hyt_batch_tuning *chosen);
 int hyt_batch_set_tuning(hyt_batch *batch, const hyt_batch_tuning *tuning);

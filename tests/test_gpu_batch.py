@@ -108,6 +108,26 @@ def test_batch_autotune(hyt, gpu, world):
             assert float(np.abs(x.astype(np.float64) - y).sum()) <= 1e-6
 
 
+def test_batch_autotune_cache_per_size_class(hyt, gpu, world):
+    """A second autotune on a sample of the same size class (here the same
+    queries, in another batch handle) reuses the cached choice: same tuning,
+    no timing runs."""
+    import time
+
+    csrs, graphs, queries = world
+    with hyt.Batch(graphs) as b:
+        t0 = time.perf_counter()
+        first = b.autotune(queries)
+        t_first = time.perf_counter() - t0
+    with hyt.Batch(graphs) as b2:
+        t0 = time.perf_counter()
+        again = b2.autotune(queries)
+        t_again = time.perf_counter() - t0
+        b2.run(queries[:4])
+    assert again == first
+    assert t_again < t_first / 5, (t_again, t_first)
+
+
 def test_batch_errors(hyt, gpu, world):
     csrs, graphs, queries = world
     pull_only = hyt.Graph(csrs[0], flags=hyt.capi.HYT_GRAPH_PULL)
