@@ -478,6 +478,8 @@ _SIGNATURES = [
                                             C.POINTER(hyt_contribution_metrics)]),
     ("hyt_partition_contributions", C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_void_p]),
     ("hyt_trim_device_memory", C.c_int, [C.c_int]),
+    ("hyt_sssp_multi", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p,
+                                 C.POINTER(hyt_run_stats)]),
     ("hyt_ppr_multi", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_float, C.c_float, C.c_uint32, C.c_void_p,
                                 C.POINTER(hyt_run_stats)]),
     ("hyt_csr_reorder", C.c_int, [C.POINTER(hyt_csr), C.c_void_p, C.c_int, C.POINTER(hyt_csr_buffers),

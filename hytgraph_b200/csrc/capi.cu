@@ -282,6 +282,16 @@ int hyt_sssp(hyt_graph *graph, const hyt_sssp_params *params, uint32_t *dist_out
     });
 }
 
+int hyt_sssp_multi(hyt_graph *graph, const uint32_t *sources, uint32_t num_sources, uint32_t max_rounds,
+                   uint32_t *dist_out, hyt_run_stats *stats) {
+    return guarded([&] {
+        GraphImpl &g = impl(graph);
+        use_device(g);
+        if (stats) std::memset(stats, 0, sizeof(*stats));
+        sssp_multi(g, sources, num_sources, max_rounds, launch_flags(0), g.stream, dist_out, stats);
+    });
+}
+
 int hyt_sssp_noalloc(const hyt_csr *csr, uint32_t source, uint32_t *dist_out, void *stream, hyt_run_stats *stats) {
     return guarded([&] {
         if (!csr || !dist_out) fail(HYT_E_INVALID, "csr/dist_out is NULL");

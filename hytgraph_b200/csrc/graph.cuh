@@ -109,6 +109,8 @@ struct GraphImpl {
     GraphArray<uint32_t> far[2];
     GraphArray<uint2> hub_tasks;
     GraphArray<unsigned char> sssp_state;
+    GraphArray<uint32_t> ms_dist;          // multi-source labels [V][8]
+    GraphArray<unsigned char> ms_state;
     PinnedArray<uint64_t> host_scratch;  // small pinned readback area
 
     size_t device_bytes() const;

@@ -10,6 +10,8 @@ void ppr_run(GraphImpl &g, const hyt_ppr_params &p, float *ranks_out, hyt_run_st
 void ppr_multi(GraphImpl &g, const uint32_t *sources, uint32_t k, float restart, float tolerance, uint32_t max_iter,
                float *out, hyt_run_stats *stats);
 void sssp_run(GraphImpl &g, const hyt_sssp_params &p, uint32_t *dist_out, hyt_run_stats *stats);
+void sssp_multi(GraphImpl &g, const uint32_t *sources, uint32_t k, uint32_t max_rounds, uint32_t flags,
+                cudaStream_t s, uint32_t *out, hyt_run_stats *stats);
 void sssp_noalloc(const hyt_csr &csr, uint32_t source, uint32_t *dist_out, void *stream, hyt_run_stats *stats);
 
 void rmat_generate(const hyt_rmat_params &p, bool on_device, hyt_csr_buffers *out);

@@ -222,6 +222,17 @@ class Graph:
                                 _ptr(res) if res is not False else None, st))
         return res, [st[i].as_dict() for i in range(k)]
 
+    def sssp_multi(self, sources, max_rounds: int = 0, out=None):
+        """SSSP of 1-8 sources in one shared solve (hyt_sssp_multi): returns
+        (labels uint32 [k][V], stats of the call)."""
+        src = np.ascontiguousarray(sources, np.uint32)
+        k = int(src.shape[0])
+        res = np.empty((k, self.num_vertices), dtype=np.uint32) if out is None else out
+        st = capi.hyt_run_stats()
+        check(lib.hyt_sssp_multi(self.handle, _ptr(src) if k else None, k, max_rounds,
+                                 _ptr(res) if res is not False else None, C.byref(st)))
+        return res, st.as_dict()
+
     def pagerank_contributions(self, current_ranks, damping: float = 0.85, out=None):
         """|next - current| of one synchronous PageRank pull step per vertex
         (hyt_pagerank_contributions); float64 [V], numpy or a CUDA tensor."""

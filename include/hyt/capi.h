@@ -219,6 +219,16 @@ typedef struct hyt_sssp_params {
 int hyt_sssp(hyt_graph *graph, const hyt_sssp_params *params,
              uint32_t *dist_out, hyt_run_stats *stats);
 
+/* SSSP from 1 to 8 sources at once (no reference counterpart; each source
+ * as hyt_sssp defines it, the reference's sssp_cpu fixed point): the 8
+ * labels of a vertex share one 32-byte row, so every push round expands the
+ * union frontier once and every pull sweep reads each in-edge once for all
+ * sources.  Each source's labels are bit-identical to hyt_sssp's.
+ * dist_out: [num_sources][V] (host or device) or NULL; max_rounds 0 =
+ * unlimited; stats covers the whole call. */
+int hyt_sssp_multi(hyt_graph *graph, const uint32_t *sources, uint32_t num_sources, uint32_t max_rounds,
+                   uint32_t *dist_out, hyt_run_stats *stats);
+
 /* SSSP that allocates nothing.  No counterpart in the reference: it exists
  * for callers that cannot call cudaMalloc -- a host whose caching allocator
  * already holds the device's free memory, a latency-critical loop that must
