@@ -335,6 +335,7 @@ class hyt_server_options(C.Structure):
         ("state_budget_bytes", C.c_uint64),
         ("tuning", hyt_batch_tuning),
         ("max_running", C.c_uint32),
+        ("pack_min_edges", C.c_uint32),
     ]
 
 
@@ -360,6 +361,7 @@ class hyt_server_stats(C.Structure):
         ("state_bytes", C.c_uint64),
         ("peak_state_bytes", C.c_uint64),
         ("busy_ms", C.c_double),
+        ("packs", C.c_uint64),
     ]
 
     def as_dict(self) -> dict:

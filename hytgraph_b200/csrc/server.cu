@@ -13,6 +13,16 @@
 // Queries that arrive while others run join at the next superstep, and
 // their work shares the superstep's kernels with everything else running.
 // With nothing running the worker sleeps on a condition variable.
+//
+// Queries on large graphs (at least pack_min_edges edges) do not enter the
+// engine: one solve there already fills the GPU, so what pays is sharing
+// the graph passes between queries.  They wait in packs keyed by (graph,
+// kind, restart, tolerance, iteration cap); each worker pass runs the pack
+// whose oldest query is oldest, up to 8 queries at once, as one
+// hyt_sssp_multi / hyt_ppr_multi solve (each query's result is what that
+// solver gives it alone: SSSP labels equal hyt_sssp's), then one engine
+// superstep for the small-graph queries.  A pack's state is the graph's own
+// workspace, outside the per-query state budget.
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -20,7 +30,9 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <map>
 #include <thread>
+#include <tuple>
 #include <unordered_map>
 #include <vector>
 
@@ -28,6 +40,7 @@
 #include "common.cuh"
 #include "host_checks.hpp"
 #include "graph.cuh"
+#include "solvers.cuh"
 
 namespace hyt {
 namespace {
@@ -55,6 +68,23 @@ struct ServerImpl {
     struct Running {
         Clock::time_point submitted, admitted;
     };
+    // Queries of one pack share graph, kind and solver parameters.
+    struct PackKey {
+        uint32_t graph, kind, max_iter;
+        float restart, tolerance;
+        bool operator<(const PackKey &o) const {
+            return std::tie(graph, kind, max_iter, restart, tolerance) <
+                   std::tie(o.graph, o.kind, o.max_iter, o.restart, o.tolerance);
+        }
+    };
+    uint64_t pack_min_edges = uint64_t(1) << 22;
+    DeviceArray<uint32_t> pack_buf;  // [8][largest packed graph's V]
+    uint64_t packs_run = 0;
+
+    bool packable(const hyt_query &q) const { return graphs[q.graph]->E >= pack_min_edges; }
+    static PackKey pack_key(const hyt_query &q);
+    // Solves up to 8 queries of one key together; appends their completions.
+    void run_pack(std::vector<Pending> &pack, std::vector<hyt_completion> &out);
 
     std::mutex mu;  // submissions, completions, stats
     std::condition_variable cv_work, cv_done;
@@ -69,27 +99,129 @@ struct ServerImpl {
     std::thread worker;
 
     void loop();
-    void fail_all(const std::unordered_map<uint64_t, Running> &running, int code, const char *msg);
+    void fail_all(const std::vector<uint64_t> &tickets, int code, const char *msg);
 };
+
+ServerImpl::PackKey ServerImpl::pack_key(const hyt_query &q) {
+    PackKey k{q.graph, q.kind, q.max_iterations, 0.0f, 0.0f};
+    if (q.kind == HYT_QUERY_PPR) {
+        k.restart = q.restart > 0.0f ? q.restart : 0.15f;
+        k.tolerance = q.tolerance > 0.0f ? q.tolerance : 1e-6f;
+        if (!k.max_iter) k.max_iter = 100;
+    }
+    return k;
+}
+
+void ServerImpl::run_pack(std::vector<Pending> &pack, std::vector<hyt_completion> &out) {
+    const PackKey key = pack_key(pack.front().q);
+    GraphImpl &g = *graphs[key.graph];
+    const uint32_t k = static_cast<uint32_t>(pack.size());
+    const uint64_t V = g.V;
+    if (pack_buf.count < 8 * V) pack_buf.allocate(8 * V);
+    std::vector<uint32_t> src(k);
+    for (uint32_t i = 0; i < k; ++i) src[i] = pack[i].q.source;
+    hyt_run_stats st[8] = {};
+    if (key.kind == HYT_QUERY_SSSP) {
+        sssp_multi(g, src.data(), k, key.max_iter, 0, stream, pack_buf.get(), &st[0]);
+        for (uint32_t i = 1; i < k; ++i) st[i] = st[0];
+    } else {
+        ppr_multi(g, src.data(), k, key.restart, key.tolerance, key.max_iter, reinterpret_cast<float *>(pack_buf.get()),
+                  st);
+        HYT_CUDA(cudaStreamSynchronize(g.stream));
+    }
+    for (uint32_t i = 0; i < k; ++i)
+        if (pack[i].q.out)
+            HYT_CUDA(cudaMemcpyAsync(pack[i].q.out, pack_buf.get() + i * V, V * sizeof(uint32_t), cudaMemcpyDefault,
+                                     stream));
+    HYT_CUDA(cudaStreamSynchronize(stream));
+    const auto now = Clock::now();
+    for (uint32_t i = 0; i < k; ++i) {
+        hyt_completion c{};
+        c.ticket = pack[i].ticket;
+        c.status = HYT_OK;
+        c.result.iterations = st[i].iterations;
+        c.result.converged = st[i].converged;
+        c.result.residual = st[i].residual;
+        c.result.edges_processed = key.kind == HYT_QUERY_SSSP ? st[0].edges_processed / k : st[i].edges_processed;
+        c.queue_ms = 0.0;
+        c.latency_ms = ms_between(pack[i].submitted, now);
+        out.push_back(c);
+    }
+    ++packs_run;
+}
 
 void ServerImpl::loop() {
     cudaSetDevice(device);
     std::deque<Pending> waiting;
+    std::map<PackKey, std::deque<Pending>> packs;
+    size_t packed_waiting = 0;
+    std::vector<Pending> pack;  // the pack being solved
     std::unordered_map<uint64_t, Running> running;
     Clock::time_point busy_since{};
+    // On an error every query the worker holds completes with it.
+    auto held = [&] {
+        std::vector<uint64_t> t;
+        for (const auto &r : running) t.push_back(r.first);
+        for (const Pending &p : pack) t.push_back(p.ticket);
+        for (const auto &kv : packs)
+            for (const Pending &p : kv.second) t.push_back(p.ticket);
+        for (const Pending &p : waiting) t.push_back(p.ticket);
+        return t;
+    };
     try {
         for (;;) {
             {
                 std::unique_lock<std::mutex> lk(mu);
-                if (waiting.empty() && running.empty()) {
+                if (waiting.empty() && running.empty() && packed_waiting == 0) {
                     if (stop) break;
                     if (inbox.empty()) cv_work.wait_for(lk, std::chrono::milliseconds(20));
                 }
                 while (!inbox.empty()) {
-                    waiting.push_back(inbox.front());
+                    Pending p = inbox.front();
                     inbox.pop_front();
+                    if (packable(p.q)) {
+                        packs[pack_key(p.q)].push_back(p);
+                        ++packed_waiting;
+                    } else {
+                        waiting.push_back(p);
+                    }
                 }
-                if (stop) waiting.clear();  // destroy drops what was not admitted
+                if (stop) {  // destroy drops what was not admitted
+                    waiting.clear();
+                    packs.clear();
+                    packed_waiting = 0;
+                }
+            }
+            // one pack: the key whose oldest query is oldest, up to 8 queries
+            if (packed_waiting) {
+                if (busy_since == Clock::time_point{}) busy_since = Clock::now();
+                auto best = packs.end();
+                for (auto it = packs.begin(); it != packs.end(); ++it)
+                    if (best == packs.end() || it->second.front().submitted < best->second.front().submitted)
+                        best = it;
+                pack.clear();
+                while (!best->second.empty() && pack.size() < 8) {
+                    pack.push_back(best->second.front());
+                    best->second.pop_front();
+                }
+                if (best->second.empty()) packs.erase(best);
+                packed_waiting -= pack.size();
+                std::vector<hyt_completion> pout;
+                run_pack(pack, pout);
+                pack.clear();
+                const auto now = Clock::now();
+                {
+                    std::lock_guard<std::mutex> lk(mu);
+                    for (const hyt_completion &c : pout) done.push_back(c);
+                    st.completed += pout.size();
+                    st.packs = packs_run;
+                    st.waiting = static_cast<uint32_t>(waiting.size() + inbox.size() + packed_waiting);
+                    if (running.empty() && packed_waiting == 0) {
+                        st.busy_ms += ms_between(busy_since, now);
+                        busy_since = Clock::time_point{};
+                    }
+                }
+                cv_done.notify_all();
             }
             // admit, oldest first
             std::vector<hyt_completion> rejected;
@@ -146,7 +278,7 @@ void ServerImpl::loop() {
                 st.max_running = std::max<uint32_t>(st.max_running, st.running + static_cast<uint32_t>(out.size()));
                 st.state_bytes = engine->bytes_in_use();
                 st.peak_state_bytes = std::max(st.peak_state_bytes, st.state_bytes);
-                if (running.empty()) {
+                if (running.empty() && packed_waiting == 0) {
                     st.busy_ms += ms_between(busy_since, now);
                     busy_since = Clock::time_point{};
                 }
@@ -154,23 +286,31 @@ void ServerImpl::loop() {
             if (!out.empty()) cv_done.notify_all();
         }
     } catch (const Error &e) {
-        fail_all(running, e.code, e.what());
+        fail_all(held(), e.code, e.what());
     } catch (const std::exception &e) {
-        fail_all(running, HYT_E_INTERNAL, e.what());
+        fail_all(held(), HYT_E_INTERNAL, e.what());
     }
 }
 
-// The worker stopped on an error: every running query completes with it.
-void ServerImpl::fail_all(const std::unordered_map<uint64_t, Running> &running, int code, const char *msg) {
+// The worker stopped on an error: every query it held completes with it
+// (and later submissions are refused).
+void ServerImpl::fail_all(const std::vector<uint64_t> &tickets, int code, const char *msg) {
     std::lock_guard<std::mutex> lk(mu);
     failure = code;
     failure_msg = msg;
-    for (const auto &r : running) {
+    for (const uint64_t t : tickets) {
         hyt_completion c{};
-        c.ticket = r.first;
+        c.ticket = t;
         c.status = code;
         done.push_back(c);
     }
+    for (const Pending &p : inbox) {
+        hyt_completion c{};
+        c.ticket = p.ticket;
+        c.status = code;
+        done.push_back(c);
+    }
+    inbox.clear();
     cv_done.notify_all();
 }
 
@@ -216,6 +356,7 @@ int hyt_server_create(hyt_graph *const *graphs, uint32_t num_graphs, const hyt_s
         t.ctas_per_sm = o.tuning.ctas_per_sm;
         s.engine->set_tuning(t);
         s.max_running = o.max_running ? o.max_running : 4096u;
+        if (o.pack_min_edges) s.pack_min_edges = o.pack_min_edges == 0xFFFFFFFFu ? ~uint64_t(0) : o.pack_min_edges;
         s.worker = std::thread([&s] { s.loop(); });
         *out = sv.release();
     });

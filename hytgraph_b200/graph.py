@@ -482,13 +482,14 @@ class Server:
     alive until its completion has been polled."""
 
     def __init__(self, graphs, device: Optional[int] = None, state_budget_bytes: int = 0, delta_mult: int = 0,
-                 hub_degree: int = 0, ctas_per_sm: int = 0, max_running: int = 0):
+                 hub_degree: int = 0, ctas_per_sm: int = 0, max_running: int = 0, pack_min_edges: int = 0):
         self._graphs = list(graphs)
         if device is None:  # the graphs' device
             device = self._graphs[0].device if self._graphs else -1
         arr = (C.c_void_p * len(self._graphs))(*[g.handle.value for g in self._graphs])
         opts = capi.hyt_server_options(device, state_budget_bytes,
-                                       capi.hyt_batch_tuning(delta_mult, hub_degree, ctas_per_sm), max_running)
+                                       capi.hyt_batch_tuning(delta_mult, hub_degree, ctas_per_sm), max_running,
+                                       pack_min_edges)
         h = C.c_void_p()
         check(lib.hyt_server_create(arr, len(self._graphs), C.byref(opts), C.byref(h)))
         self._h = h

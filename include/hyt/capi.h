@@ -444,6 +444,12 @@ typedef struct hyt_server_options {
     hyt_batch_tuning tuning;
     uint32_t max_running;         /* cap on concurrently running queries
                                      (0 = slot table size, 4096) */
+    uint32_t pack_min_edges;      /* queries on graphs with at least this
+                                     many edges run in packs of up to 8 of
+                                     the same kind and parameters sharing
+                                     one solve (hyt_sssp_multi /
+                                     hyt_ppr_multi); 0 = 2^22, UINT32_MAX =
+                                     never */
 } hyt_server_options;
 
 typedef struct hyt_completion {
@@ -460,6 +466,7 @@ typedef struct hyt_server_stats {
     uint32_t running, waiting, max_running;
     uint64_t state_bytes, peak_state_bytes;
     double busy_ms;               /* worker time with queries running */
+    uint64_t packs;               /* packed solves run (pack_min_edges) */
 } hyt_server_stats;
 
 /* graphs: handles built with HYT_GRAPH_ALL (borrowed; keep them alive).

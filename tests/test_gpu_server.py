@@ -72,6 +72,40 @@ def test_server_results_equal_alone(hyt, gpu, served):
             assert c["latency_ms"] >= c["queue_ms"] >= 0.0
 
 
+def test_server_packs_equal_alone(hyt, gpu, served):
+    """Queries on graphs at or above pack_min_edges run in packs of up to 8
+    (hyt_sssp_multi / hyt_ppr_multi) next to the engine's queries on the
+    smaller graphs.  SSSP labels equal hyt_sssp's; a packed PPR equals the
+    same query packed alone (hyt_ppr_multi's result does not depend on its
+    companions) and lies within L1 1e-6 of hyt_ppr."""
+    csrs, graphs = served
+    rng = np.random.default_rng(11)
+    reqs = []
+    for i in range(60):
+        gi = int(rng.integers(0, len(graphs)))
+        kind = "sssp" if rng.random() < 0.6 else "ppr"
+        src = int(hyt.pick_sources(csrs[gi].row_offsets, 900 + i, 1)[0])
+        reqs.append((gi, kind, src))
+    # the two larger graphs pack, the two smaller go through the engine
+    with hyt.Server(graphs, pack_min_edges=csrs[2].num_edges) as srv:
+        tickets = {srv.submit(*r): r for r in reqs}
+        got = _drain(srv, len(reqs))
+        st = srv.stats()
+    assert st["packs"] > 0 and st["completed"] == len(reqs)
+    assert st["packs"] < sum(1 for g, _, _ in reqs if g >= 2)  # some packs held several queries
+    for c in got:
+        assert c["status"] == 0
+        gi, kind, src = tickets[c["ticket"]]
+        if kind == "sssp":
+            single, _ = graphs[gi].sssp(src)
+            assert np.array_equal(c["out"], single), (gi, src)
+        elif gi >= 2:
+            alone, _ = graphs[gi].ppr_multi([src])
+            assert np.array_equal(c["out"].view(np.uint32), alone[0].view(np.uint32)), (gi, src)
+            one, _ = graphs[gi].ppr(src)
+            assert float(np.abs(c["out"].astype(np.float64) - one).sum()) <= 1e-6
+
+
 def test_server_short_query_overtakes_long(hyt, gpu, served):
     csrs, graphs = served
     big = len(graphs) - 1
