@@ -5,11 +5,12 @@ vectors exchanged through torch.distributed (NCCL over NVLink / NVSwitch on
 a B200 node).
 
 PageRank / personalized PageRank, per iteration: every process runs the
-pull step over its rows; the owner of each range broadcasts its slice of
-the new contribution vector (4 bytes per vertex in total); one all-reduce
-sums the (L1 change, dangling mass) pair, so every process takes the same
-stop decision as the single-GPU solver (residual <= tolerance, or the
-iteration cap).
+pull step over its rows; one all-gather of the owners' slices of the new
+contribution vector (padded to the longest slice; 4 bytes per vertex of
+payload) gives every process the whole vector; one all-reduce sums the
+(L1 change, dangling mass) pair, so every process takes the same stop
+decision as the single-GPU solver (residual <= tolerance, or the iteration
+cap).
 
 SSSP, per round: every process collects its improved vertices and one
 all-reduce sums their out-edges; when that frontier is dense (more than
@@ -184,17 +185,34 @@ class ShardedGraph:
         return self.dist.get_global_rank(self.group, p) if self.group is not None else p
 
     def _share_slices(self, vec, bounds) -> int:
-        """Every owner broadcasts its slice of vec; returns the bytes this
-        process sent or received."""
-        moved = 0
+        """Every process receives every owner's slice of vec: one all-gather
+        of slices padded to the longest, then one gather back into place.
+        Returns the vector's bytes (4 per vertex for float32), the payload
+        every process ends up holding."""
         if self.dist is None:
             return 0
-        for p in range(self.parts):
-            lo, hi = bounds[p], bounds[p + 1]
-            if hi > lo:
-                self.dist.broadcast(vec[lo:hi], src=self._owner(p), group=self.group)
-                moved += (hi - lo) * vec.element_size()
-        return moved
+        import torch
+
+        P = self.parts
+        sizes = [bounds[p + 1] - bounds[p] for p in range(P)]
+        m = max(sizes)
+        if m == 0:
+            return 0
+        key = (tuple(bounds), vec.device, vec.dtype)
+        if getattr(self, "_gather_key", None) != key:
+            # idx[v] = position of vertex v in the padded all-gather buffer
+            owner = np.repeat(np.arange(P), sizes)
+            starts = np.asarray(bounds[:-1], np.int64)
+            idx = owner * m + (np.arange(bounds[-1], dtype=np.int64) - starts[owner])
+            self._gather_idx = torch.from_numpy(idx).to(vec.device)
+            self._gather_send = torch.zeros(m, dtype=vec.dtype, device=vec.device)
+            self._gather_recv = torch.empty(P * m, dtype=vec.dtype, device=vec.device)
+            self._gather_key = key
+        lo, hi = bounds[self.part], bounds[self.part + 1]
+        self._gather_send[: hi - lo].copy_(vec[lo:hi])
+        self.dist.all_gather_into_tensor(self._gather_recv, self._gather_send, group=self.group)
+        torch.index_select(self._gather_recv, 0, self._gather_idx, out=vec[: bounds[-1]])
+        return sum(sizes) * vec.element_size()
 
     def _sum(self, t) -> None:
         if self.dist is not None:
