@@ -25,6 +25,7 @@
 #include "graph.cuh"
 #include "scratch.cuh"
 #include "solvers.cuh"
+#include "stage.cuh"
 
 namespace hyt {
 namespace {
@@ -189,6 +190,149 @@ __global__ void ppr8_long_rows_kernel(const LongRow *__restrict__ long_rows, uin
     }
 }
 
+// ---- staged task pass (graph in HBM: pull task descriptors) -----------------
+//
+// The pull tasks (stage.cuh) replace the one-warp-per-row pass: a warp
+// stages each tile's (or chunk piece's) source ids in shared memory one
+// unit ahead, then
+//   tile rows  -- 4 rows at a time, thread t owning row rb + t / 8 and lane
+//                 t % 8: the 8 threads of a row read one id (a shared-memory
+//                 broadcast) and one 32-byte contribution sector per
+//                 in-edge, kUnroll edges in flight per thread; rows of >= 64
+//                 in-edges are taken by the whole warp in the 4-slot layout
+//                 of row_lane_sum;
+//   chunks     -- the 4-slot layout over the chunk's edges, one FP64 partial
+//                 per chunk and lane (summed by ppr8_long_rows_kernel).
+// Every sum is FP64 in a fixed edge order and the thread layout does not
+// depend on the lane count, so a query's bits do not depend on its
+// companions.  Residual partials are per block over a static task
+// assignment (fixed for a fixed grid).
+constexpr int kTaskThreads = 1024;
+constexpr int kUnroll = 8;
+
+// Sum over in-edges [b, e) of c[u][lane] from staged ids, thread t taking
+// edge slot t / 8 (4 slots) and lane t % 8; complete in every thread.
+__device__ __forceinline__ double staged_lane_sum(const uint32_t *slot, uint64_t a0, const uint32_t *s_hot,
+                                                  const float *__restrict__ c, uint64_t b, uint64_t e, int t) {
+    const int sl = t >> 3, lane = t & 7;
+    double acc = 0.0;
+    for (uint64_t i = b + sl; i < e; i += 4 * kUnroll) {
+        float g[kUnroll];
+#pragma unroll
+        for (int q = 0; q < kUnroll; ++q) {
+            const uint64_t x = i + 4 * q;
+            uint32_t u = x < e ? slot[x - a0] : 0u;
+            if (u & kHotTag) u = s_hot[u & ~kHotTag];
+            g[q] = x < e ? __ldcg(c + uint64_t(u) * kLanes + lane) : 0.0f;
+        }
+#pragma unroll
+        for (int q = 0; q < kUnroll; ++q) acc += double(g[q]);
+    }
+    acc += __shfl_xor_sync(0xffffffffu, acc, 8);
+    acc += __shfl_xor_sync(0xffffffffu, acc, 16);
+    return acc;
+}
+
+__global__ void __launch_bounds__(kTaskThreads, 1)
+    ppr8_tasks_kernel(const uint4 *__restrict__ tasks, uint64_t num_tasks, const uint64_t *__restrict__ in_off,
+                      const uint32_t *__restrict__ in_src, const uint32_t *__restrict__ hot_vertex, uint32_t num_hot,
+                      const LongRow *__restrict__ long_rows, const float *__restrict__ c,
+                      const float *__restrict__ x, LaneParams p, const double *__restrict__ dpart,
+                      float *__restrict__ nxt, double *__restrict__ chunk_sum, double *__restrict__ rpart,
+                      uint32_t *__restrict__ error) {
+    extern __shared__ __align__(128) unsigned char s_stage[];
+    __shared__ double s_dm[kLanes];
+    __shared__ double s_res[kLanes][kTaskThreads / 32];
+    lane_dangling(dpart, s_dm);
+    const int t = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const stage::WarpStage ws = stage::warp_stage(s_stage, warp, t);
+    uint32_t *s_hot = reinterpret_cast<uint32_t *>(s_stage + stage::kStageBytes);
+    for (uint32_t i = threadIdx.x; i < num_hot; i += blockDim.x) s_hot[i] = hot_vertex[i];
+    __syncthreads();
+    const uint64_t nwarps = uint64_t(gridDim.x) * (kTaskThreads / 32);
+    const int lane = t & 7, rsub = t >> 3;
+    double res = 0.0;  // this thread's lane, rows of this warp's tasks in task order
+    double acc = 0.0;  // running chunk sum
+    const bool ok = stage::stage_pipeline(
+        tasks, in_src, uint64_t(blockIdx.x) * (kTaskThreads / 32) + warp, nwarps, num_tasks, ws.slots, ws.bars, t,
+        [&](uint4 d, uint64_t, uint32_t j, uint32_t nu, uint32_t *slot, uint64_t a0) {
+            if (task_is_chunk(d)) {
+                const stage::Unit u = stage::unit_of(d, j);
+                if (j == 0) acc = 0.0;
+                // the 4-slot layout over the whole chunk: slot sl takes
+                // edges lo + sl, lo + sl + 4, ... of every piece in order
+                const int sl = t >> 3;
+                for (uint64_t i = u.lo + sl; i < u.hi; i += 4 * kUnroll) {
+                    float g[kUnroll];
+#pragma unroll
+                    for (int q = 0; q < kUnroll; ++q) {
+                        const uint64_t xx = i + 4 * q;
+                        uint32_t v = xx < u.hi ? slot[xx - a0] : 0u;
+                        if (v & kHotTag) v = s_hot[v & ~kHotTag];
+                        g[q] = xx < u.hi ? __ldcg(c + uint64_t(v) * kLanes + lane) : 0.0f;
+                    }
+#pragma unroll
+                    for (int q = 0; q < kUnroll; ++q) acc += double(g[q]);
+                }
+                if (j + 1 < nu) return;
+                double sum = acc;
+                sum += __shfl_xor_sync(0xffffffffu, sum, 8);
+                sum += __shfl_xor_sync(0xffffffffu, sum, 16);
+                if (t < kLanes) chunk_sum[(uint64_t(long_rows[d.z].first_chunk) + d.w) * kLanes + t] = sum;
+                return;
+            }
+            const uint32_t r0 = d.z, rl = d.w;
+            for (uint32_t rb = r0; rb < rl; rb += 4) {
+                const uint32_t r = rb + rsub;
+                const bool active = r < rl;
+                const uint64_t lo = active ? in_off[r] : 0, hi = active ? in_off[r + 1] : 0;
+                const bool small = active && hi - lo < 64;
+                double sum = 0.0;
+                if (small) {
+                    for (uint64_t i = lo; i < hi; i += kUnroll) {
+                        float g[kUnroll];
+#pragma unroll
+                        for (int q = 0; q < kUnroll; ++q) {
+                            const uint64_t xx = i + q;
+                            uint32_t v = xx < hi ? slot[xx - a0] : 0u;
+                            if (v & kHotTag) v = s_hot[v & ~kHotTag];
+                            g[q] = xx < hi ? __ldcg(c + uint64_t(v) * kLanes + lane) : 0.0f;
+                        }
+#pragma unroll
+                        for (int q = 0; q < kUnroll; ++q) sum += double(g[q]);
+                    }
+                }
+                // rows of >= 64 in-edges: the whole warp, one row at a time
+                uint32_t big = __ballot_sync(0xffffffffu, active && !small) & 0x01010101u;
+                while (big) {
+                    const int src = __ffs(big) - 1;
+                    big &= big - 1;
+                    const uint64_t bb = __shfl_sync(0xffffffffu, lo, src);
+                    const uint64_t ee = __shfl_sync(0xffffffffu, hi, src);
+                    const double s2 = staged_lane_sum(slot, a0, s_hot, c, bb, ee, t);
+                    if ((src >> 3) == rsub) sum = s2;
+                }
+                if (active) {
+                    const float cur = x[uint64_t(r) * kLanes + lane];
+                    const float nx = lane_next(r, lane, sum, p, s_dm, cur);
+                    nxt[uint64_t(r) * kLanes + lane] = nx;
+                    res += fabs(double(nx) - double(cur));
+                }
+            }
+        });
+    if (!ok) atomicExch(error, 1u);
+    // per-lane residual: the warp's 4 row slots, then the block's warps in order
+    res += __shfl_xor_sync(0xffffffffu, res, 8);
+    res += __shfl_xor_sync(0xffffffffu, res, 16);
+    if (t < kLanes) s_res[t][warp] = res;
+    __syncthreads();
+    if (threadIdx.x < kLanes) {
+        double a = 0.0;
+        for (int w = 0; w < kTaskThreads / 32; ++w) a += s_res[threadIdx.x][w];
+        rpart[blockIdx.x * kLanes + threadIdx.x] = a;
+    }
+}
+
 // residual[l] = rows partials then long-row partials, each in block order.
 __global__ void ppr8_residual_kernel(const double *__restrict__ rows, int nrows, const double *__restrict__ longs,
                                      int nlong, double *__restrict__ residual) {
@@ -237,7 +381,18 @@ void ppr_multi(GraphImpl &g, const uint32_t *sources, uint32_t k, float restart,
     for (uint32_t l = 0; l < kLanes; ++l) p.source[l] = l < k ? graph_vertex(g, sources[l], s) : 0xFFFFFFFFu;
     p.active = (1u << k) - 1u;
     p.d = 1.0 - double(restart);
-    const unsigned rows_grid = grid_sm(8);
+    // staged task pass when the graph carries task descriptors (in HBM)
+    const bool staged = g.pull_tasks.get() && stage::staged_shared_bytes(g.num_hot) <= kPRSmemMax;
+    const unsigned smem = static_cast<unsigned>(stage::staged_shared_bytes(g.num_hot));
+    if (staged) {
+        static bool attr = false;
+        if (!attr) {
+            HYT_CUDA(cudaFuncSetAttribute(ppr8_tasks_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          static_cast<int>(kPRSmemMax)));
+            attr = true;
+        }
+    }
+    const unsigned rows_grid = staged ? grid_sm(1) : grid_sm(8);
     const uint64_t chunks = g.num_long ? g.num_chunks : 0;
     const uint64_t long_from = g.num_long ? g.tile_cost : ~uint64_t(0);
     const unsigned long_grid = g.num_long ? grid_for(g.num_long * 32, 256) : 0;
@@ -245,6 +400,8 @@ void ppr_multi(GraphImpl &g, const uint32_t *sources, uint32_t k, float restart,
     Scratch<double> dpart(uint64_t(kPartBlocks) * kLanes, s), rpart(uint64_t(rows_grid) * kLanes, s),
         lpart(uint64_t(std::max(long_grid, 1u)) * kLanes, s), chunk_sum(std::max<uint64_t>(chunks, 1) * kLanes, s),
         residual(kLanes, s);
+    Scratch<uint32_t> err(1, s);
+    HYT_CUDA(cudaMemsetAsync(err.get(), 0, sizeof(uint32_t), s));
     double *h_res = reinterpret_cast<double *>(g.host_scratch.ptr);  // 64 pinned bytes
     float *x = xa.get(), *nx = xb.get();
     ppr8_init_kernel<<<grid_sm(8), 256, 0, s>>>(x, V, p, int(k));
@@ -256,10 +413,22 @@ void ppr_multi(GraphImpl &g, const uint32_t *sources, uint32_t k, float restart,
     uint64_t launches = 1;
     for (uint32_t it = 0; it < max_iter && p.active; ++it) {
         ppr8_prep_kernel<<<kPartBlocks, 256, 0, s>>>(g.out_degree.get(), x, V, c.get(), dpart.get());
-        ppr8_rows_kernel<<<rows_grid, 256, 0, s>>>(g.in_offsets.get(), g.in_sources.get(), g.hot_vertex.get(),
-                                                   c.get(), x, V, long_from, p, dpart.get(), nx, rpart.get());
         launches += 2;
-        if (chunks) {
+        if (staged) {
+            ppr8_tasks_kernel<<<rows_grid, kTaskThreads, smem, s>>>(
+                g.pull_tasks.get(), g.num_chunks + g.num_tiles, g.in_offsets.get(), g.in_sources.get(),
+                g.hot_vertex.get(), g.num_hot, g.long_rows.get(), c.get(), x, p, dpart.get(), nx, chunk_sum.get(),
+                rpart.get(), err.get());
+            if (chunks) {
+                ppr8_long_rows_kernel<<<long_grid, 256, 0, s>>>(g.long_rows.get(), g.num_long, chunk_sum.get(), x, p,
+                                                                dpart.get(), nx, lpart.get());
+                ++launches;
+            }
+        } else {
+            ppr8_rows_kernel<<<rows_grid, 256, 0, s>>>(g.in_offsets.get(), g.in_sources.get(), g.hot_vertex.get(),
+                                                       c.get(), x, V, long_from, p, dpart.get(), nx, rpart.get());
+        }
+        if (chunks && !staged) {
             ppr8_chunks_kernel<<<grid_sm(8), 256, 0, s>>>(g.in_offsets.get(), g.in_sources.get(), g.hot_vertex.get(),
                                                           c.get(), g.long_rows.get(), g.chunk_tasks.get(), chunks,
                                                           chunk_sum.get());
@@ -283,6 +452,10 @@ void ppr_multi(GraphImpl &g, const uint32_t *sources, uint32_t k, float restart,
     }
     timer.stop(s);
     const double ms = timer.ms();
+    uint32_t h_err = 0;
+    HYT_CUDA(cudaMemcpyAsync(&h_err, err.get(), sizeof(h_err), cudaMemcpyDeviceToHost, s));
+    HYT_CUDA(cudaStreamSynchronize(s));
+    if (h_err) fail(HYT_E_TIMEOUT, "hyt_ppr_multi: a bounded wait for a staged copy ran out");
     if (out) {
         Scratch<float> lane(V, s);
         for (uint32_t l = 0; l < k; ++l) {

@@ -77,7 +77,8 @@ def test_server_packs_equal_alone(hyt, gpu, served):
     (hyt_sssp_multi / hyt_ppr_multi) next to the engine's queries on the
     smaller graphs.  SSSP labels equal hyt_sssp's; a packed PPR equals the
     same query packed alone (hyt_ppr_multi's result does not depend on its
-    companions) and lies within L1 1e-6 of hyt_ppr."""
+    companions) and lies within L1 1e-5 of hyt_ppr (both are within 1e-5 of
+    the FP64 definition)."""
     csrs, graphs = served
     rng = np.random.default_rng(11)
     reqs = []
@@ -103,7 +104,7 @@ def test_server_packs_equal_alone(hyt, gpu, served):
             alone, _ = graphs[gi].ppr_multi([src])
             assert np.array_equal(c["out"].view(np.uint32), alone[0].view(np.uint32)), (gi, src)
             one, _ = graphs[gi].ppr(src)
-            assert float(np.abs(c["out"].astype(np.float64) - one).sum()) <= 1e-6
+            assert float(np.abs(c["out"].astype(np.float64) - one).sum()) <= 1e-5
 
 
 def test_server_short_query_overtakes_long(hyt, gpu, served):
