@@ -442,6 +442,29 @@ def run_hybrid(args, rank, world, pg):
 
     pr_l1 = float(np.abs(ranks.astype(np.float64) - ranks_hbm.astype(np.float64)).sum())
     sssp_equal = bool(np.array_equal(dist, dist_hbm))
+    # parity against the oracle on the same host arrays: PageRank against
+    # the FP64 restatement (on the CSC already in host memory), SSSP against
+    # Dijkstra for the source
+    parity = None
+    if rank == 0 and not args.no_parity:
+        from concurrent.futures import ThreadPoolExecutor
+
+        from oracle.bindings import Oracle
+
+        o = Oracle()
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(2) as ex:
+            f64 = ex.submit(o.pagerank_f64_csc, off.array, in_off.array, in_src.array, 0.85, 1e-6, 100)
+            dj = ex.submit(o.dijkstra, off.array, cols.array, w.array, src)
+            r64, it64, _, _ = f64.result()
+            d = dj.result()
+        want = np.where(d == np.iinfo(np.uint64).max, 0xFFFFFFFF, d).astype(np.uint32)
+        l1 = float(np.abs(ranks.astype(np.float64) - r64).sum())
+        mism = int(np.count_nonzero(np.asarray(dist).view(np.uint32) != want))
+        parity = {"pr_l1_vs_fp64": l1, "pr_l1_tolerance": 1e-5, "fp64_iterations": int(it64),
+                  "sssp_mismatches": mism, "sources_checked": 1,
+                  "sssp_oracle": "Dijkstra, exact u64 labels", "ok": bool(l1 <= 1e-5 and mism == 0),
+                  "check_s": time.perf_counter() - t0}
     ms = pr["device_ms"] + ss["device_ms"]
     traversed = E * pr["iterations"] + E
     value = traversed / (ms / 1e3) / 1e9
@@ -484,7 +507,7 @@ def run_hybrid(args, rank, world, pg):
                 "sssp": {"source": src, "rounds": ss["iterations"], "ms": ss["device_ms"], "wall_s": ss_wall,
                          "gteps": E / (ss["device_ms"] / 1e3) / 1e9, "identical_to_in_hbm": sssp_equal,
                          "in_hbm_ms": ss_hbm["device_ms"], **ss_link},
-                "clocks": clk, "gpu_launches": pr["total_launches"] + ss["total_launches"]}
+                "parity": parity, "clocks": clk, "gpu_launches": pr["total_launches"] + ss["total_launches"]}
         print(json.dumps(line), flush=True)
     for x in (off, cols, w, in_off, in_src):
         x.free()

@@ -71,6 +71,18 @@ class Oracle:
             raise ValueError(f"oracle_pagerank_f64 rc={rc}")
         return r, it.value, res.value, bool(conv.value)
 
+    def pagerank_f64_csc(self, off, in_off, in_src, damping=0.85, tol=1e-6, max_iter=100):
+        """pagerank_f64 on a given incoming CSR (sources ascending per row)."""
+        V = off.shape[0] - 1
+        r = np.empty(V, np.float64)
+        it, res, conv = C.c_uint64(), C.c_double(), C.c_int()
+        rc = self.lib.oracle_pagerank_f64_csc(C.c_uint64(V), _p(off), _p(in_off), _p(in_src), C.c_double(damping),
+                                              C.c_double(tol), C.c_uint64(max_iter), _p(r), C.byref(it),
+                                              C.byref(res), C.byref(conv))
+        if rc:
+            raise ValueError(f"oracle_pagerank_f64_csc rc={rc}")
+        return r, it.value, res.value, bool(conv.value)
+
     def ppr_f64(self, off, cols, source, restart=0.15, tol=1e-6, max_iter=100):
         V, E = off.shape[0] - 1, cols.shape[0]
         r = np.empty(V, np.float64)

@@ -203,22 +203,19 @@ static void pr64_rows_fn(void *p, uint64_t b, uint64_t e) {
 
 /* FP64 restatement of the same iteration (pagerank.cpp:89-163 in double):
  * x0 = 1/n; x' = (1-d)/n + d*dangling/n + d*sum x_u/deg_u; stop when the L1
- * change <= tol.  This is the accuracy reference for the FP32 solvers. */
-int oracle_pagerank_f64(uint64_t V, uint64_t E, const uint64_t *off, const uint32_t *cols, double damping,
-                        double tol, uint64_t max_iter, double *ranks, uint64_t *iterations, double *residual_out,
-                        int *converged) {
+ * change <= tol.  This is the accuracy reference for the FP32 solvers.
+ * The _csc form takes the incoming CSR (sources ascending within each row,
+ * as build_incoming makes it) instead of building it. */
+int oracle_pagerank_f64_csc(uint64_t V, const uint64_t *off, const uint64_t *in_off, const uint32_t *in_src,
+                            double damping, double tol, uint64_t max_iter, double *ranks, uint64_t *iterations,
+                            double *residual_out, int *converged) {
     if (V == 0 || !(damping >= 0.0 && damping < 1.0) || !(tol > 0.0) || max_iter == 0) return ORACLE_E_INVALID;
-    uint64_t *in_off;
-    uint32_t *in_src;
-    int rc = build_incoming(V, E, off, cols, NULL, &in_off, &in_src, NULL);
-    if (rc) return rc;
     const double n = (double)V, base = (1.0 - damping) / n;
     double *cur = (double *)malloc(V * sizeof(double)), *nxt = (double *)malloc(V * sizeof(double));
     double *contrib = (double *)malloc(V * sizeof(double));
-    if (!cur || !nxt || !contrib) { free(cur); free(nxt); free(contrib); free(in_off); free(in_src); return ORACLE_E_NOMEM; }
+    if (!cur || !nxt || !contrib) { free(cur); free(nxt); free(contrib); return ORACLE_E_NOMEM; }
     for (uint64_t v = 0; v < V; ++v) cur[v] = 1.0 / n;
     *iterations = 0; *residual_out = 0.0; *converged = 0;
-    memcpy(ranks, cur, V * sizeof(double));
     for (uint64_t it = 0; it < max_iter; ++it) {
         double dangling = 0.0;
         for (uint64_t u = 0; u < V; ++u) {
@@ -237,8 +234,22 @@ int oracle_pagerank_f64(uint64_t V, uint64_t E, const uint64_t *off, const uint3
         if (residual <= tol) { *converged = 1; break; }
     }
     memcpy(ranks, cur, V * sizeof(double));
-    free(cur); free(nxt); free(contrib); free(in_off); free(in_src);
+    free(cur); free(nxt); free(contrib);
     return ORACLE_OK;
+}
+
+int oracle_pagerank_f64(uint64_t V, uint64_t E, const uint64_t *off, const uint32_t *cols, double damping,
+                        double tol, uint64_t max_iter, double *ranks, uint64_t *iterations, double *residual_out,
+                        int *converged) {
+    if (V == 0 || !(damping >= 0.0 && damping < 1.0) || !(tol > 0.0) || max_iter == 0) return ORACLE_E_INVALID;
+    uint64_t *in_off;
+    uint32_t *in_src;
+    int rc = build_incoming(V, E, off, cols, NULL, &in_off, &in_src, NULL);
+    if (rc) return rc;
+    rc = oracle_pagerank_f64_csc(V, off, in_off, in_src, damping, tol, max_iter, ranks, iterations, residual_out,
+                                 converged);
+    free(in_off); free(in_src);
+    return rc;
 }
 
 /* Personalized PageRank in FP64 (no reference counterpart; defined by this

@@ -18,6 +18,9 @@ int oracle_pagerank_f32(uint64_t V, uint64_t E, const uint64_t *off, const uint3
 int oracle_pagerank_f64(uint64_t V, uint64_t E, const uint64_t *off, const uint32_t *cols, double damping,
                         double tol, uint64_t max_iter, double *ranks, uint64_t *iterations, double *residual,
                         int *converged);
+int oracle_pagerank_f64_csc(uint64_t V, const uint64_t *off, const uint64_t *in_off, const uint32_t *in_src,
+                            double damping, double tol, uint64_t max_iter, double *ranks, uint64_t *iterations,
+                            double *residual, int *converged);
 int oracle_ppr_f64(uint64_t V, uint64_t E, const uint64_t *off, const uint32_t *cols, uint32_t source,
                    double restart, double tol, uint64_t max_iter, double *ranks, uint64_t *iterations,
                    double *residual, int *converged);
