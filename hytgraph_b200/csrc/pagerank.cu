@@ -31,9 +31,9 @@
 //
 // Results are deterministic: every row sum has a fixed association order,
 // and the FP64 residual and dangling mass are summed in a fixed slot order
-// (PRSlots), independent of the grid size and of warp arrival order.  The
-// warp that completes the last slot group evaluates the stop rule and,
-// inside a CUDA graph, ends the conditional while-loop.
+// (PRSlots), independent of the grid size and of warp arrival order: each
+// task stores its slot, then pr_reduce_kernel sums the slots and evaluates
+// the stop rule, ending the CUDA-graph conditional while-loop when done.
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
@@ -84,8 +84,8 @@ __device__ __forceinline__ void load_hot(const PRArgs &a, const PRBuffers &b, fl
 // One launch processes chunk tasks [chunk_begin, chunk_end) and tiles
 // [tile_begin, tile_end); in_src is the base of the source ids, addressed by
 // global edge index (a device array, a staging slot offset by its first
-// edge, or mapped host memory).  An iteration may span several launches; it
-// closes itself when its last slot group completes.
+// edge, or mapped host memory).  An iteration may span several launches;
+// pr_reduce_kernel closes it after the last one.
 struct PRRange {
     const uint32_t *in_src;
     uint64_t chunk_begin, chunk_end, tile_begin, tile_end;
@@ -115,11 +115,11 @@ __global__ void __launch_bounds__(kPRThreads, 1) pr_iterate_kernel(const PRArgs 
         if (task < n_chunks) {
             const uint32_t row = chunk_task<true>(a, ps, b, rg.in_src, s_hot, rg.chunk_begin + task, pol, lane, res,
                                                   dang);
-            if (row != ~0u) slot_done(a, it, long_slot(row), dev::warp_sum(res), dev::warp_sum(dang), lane);
+            if (row != ~0u) slot_store(a, long_slot(row), dev::warp_sum(res), dev::warp_sum(dang), lane);
         } else {
             const uint64_t k = rg.tile_begin + (task - n_chunks);
             tile_task<true>(a, ps, b, rg.in_src, s_hot, sv, k, pol, lane, res, dang);
-            slot_done(a, it, tile_slot(a, k), dev::warp_sum(res), dev::warp_sum(dang), lane);
+            slot_store(a, tile_slot(a, k), dev::warp_sum(res), dev::warp_sum(dang), lane);
         }
     }
 }
@@ -206,8 +206,7 @@ __global__ void __launch_bounds__(kPRThreads, 1) pr_staged_kernel(const PRArgs *
                 }
                 row = dev::warp_reduce(row);
                 if (lane == 0) finalize_row(a, ps, L.row, row.value(), b.cur, b.nxt, b.cnxt, res, dang);
-                slot_done(a, it, long_slot(d.z), __shfl_sync(0xffffffffu, res, 0), __shfl_sync(0xffffffffu, dang, 0),
-                          lane);
+                slot_store(a, long_slot(d.z), res, dang, lane);  // lane 0 finalized the row
                 return;
             }
             // tile: rows [r0, rl), edges [e0, e0 + n); contributions replace
@@ -242,9 +241,53 @@ __global__ void __launch_bounds__(kPRThreads, 1) pr_staged_kernel(const PRArgs *
                     if (lane == 0) finalize_row(a, ps, rb + src, s.value(), b.cur, b.nxt, b.cnxt, res, dang);
                 }
             }
-            slot_done(a, it, tile_slot(a, task - a.num_chunks), dev::warp_sum(res), dev::warp_sum(dang), lane);
+            slot_store(a, tile_slot(a, task - a.num_chunks), dev::warp_sum(res), dev::warp_sum(dang), lane);
         });
     if (!ok) stage_failed(a);
+}
+
+// Closes an iteration: block b sums slot groups b, b + grid, ... (thread t
+// takes slots t, t + 256, ... of the group, then a fixed block tree); the
+// last block to finish sums the group sums in group order, then applies
+// the stop rule (ending the CUDA-graph loop when the solve is done).
+constexpr int kReduceThreads = 256;
+
+__global__ void __launch_bounds__(kReduceThreads) pr_reduce_kernel(const PRArgs *__restrict__ args) {
+    __shared__ double s_red[32];
+    __shared__ uint32_t s_last;
+    const PRArgs a = *args;
+    if (*(volatile uint32_t *)&a.hdr->done) return;
+    const uint32_t it = *(volatile uint32_t *)&a.hdr->iter;
+    const PRSlots &R = a.red;
+    for (uint32_t g = blockIdx.x; g < R.num_groups; g += gridDim.x) {
+        const uint32_t b = g * kSlotGroup, n = min(kSlotGroup, R.num_slots - b);
+        double r = 0.0, d = 0.0;
+        for (uint32_t i = threadIdx.x; i < n; i += kReduceThreads) {
+            const double2 x = __ldcg(R.slot + b + i);
+            r += x.x;
+            d += x.y;
+        }
+        r = dev::block_sum(r, s_red);
+        __syncthreads();
+        d = dev::block_sum(d, s_red);
+        if (threadIdx.x == 0) R.group_sum[g] = make_double2(r, d);
+        __syncthreads();
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = (atomicAdd(R.blocks_done, 1u) + 1u == (it + 1) * gridDim.x) ? 1u : 0u;
+    __syncthreads();
+    if (!s_last || threadIdx.x >= 32) return;
+    __threadfence();
+    double r = 0.0, d = 0.0;
+    for (uint32_t g = threadIdx.x; g < R.num_groups; g += 32) {
+        const double2 x = __ldcg(R.group_sum + g);
+        r += x.x;
+        d += x.y;
+    }
+    r = dev::warp_sum(r);
+    d = dev::warp_sum(d);
+    if (threadIdx.x == 0) close_iteration(a, it, r, d);
 }
 
 // Initial ranks and contributions; the initial dangling mass is summed in a
@@ -331,9 +374,9 @@ struct PRSolveState {
 };
 
 // pr_state layout: args | header | residual[max_iter] | dangling[max_iter+1]
-// | init partials | init counter | slot group counters, groups done | (8-byte
-// aligned) group sums | slots.  Everything from the header through the
-// counters is cleared at the start of a solve.
+// | init partials | init counter | reduce-blocks counter | (8-byte aligned)
+// group sums | slots.  Everything from the header through the counters is
+// cleared at the start of a solve.
 static PRSolveState pr_prepare(GraphImpl &g, bool personalized, uint32_t source, float damping, float tolerance,
                                uint32_t max_iter) {
     const uint64_t V = g.V;
@@ -351,7 +394,7 @@ static PRSolveState pr_prepare(GraphImpl &g, bool personalized, uint32_t source,
     auto up8 = [](size_t x) { return (x + 7) & ~size_t(7); };
     const size_t args_bytes = (sizeof(PRArgs) + 255) & ~size_t(255);
     const size_t head = sizeof(PRHeader) + size_t(max_iter) * sizeof(double) + size_t(max_iter + 1) * sizeof(double) +
-                        size_t(init_chunks) * sizeof(double) + sizeof(uint32_t) + size_t(num_groups + 1) * 4;
+                        size_t(init_chunks) * sizeof(double) + 2 * sizeof(uint32_t);
     const size_t sb = args_bytes + up8(head) + size_t(num_groups + num_slots) * sizeof(double2) + 64;
     if (g.pr_state.count < sb) g.pr_state.allocate(sb);
 
@@ -368,9 +411,7 @@ static PRSolveState pr_prepare(GraphImpl &g, bool personalized, uint32_t source,
     p += size_t(init_chunks) * sizeof(double);
     uint32_t *init_count = reinterpret_cast<uint32_t *>(p);
     p += sizeof(uint32_t);
-    uint32_t *group_count = reinterpret_cast<uint32_t *>(p);
-    p += size_t(num_groups) * 4;
-    uint32_t *groups_done = reinterpret_cast<uint32_t *>(p);
+    uint32_t *blocks_done = reinterpret_cast<uint32_t *>(p);
     p += 4;
     const size_t zero_bytes = static_cast<size_t>(p - reinterpret_cast<unsigned char *>(hdr));
     p = base + args_bytes + up8(head);
@@ -407,7 +448,7 @@ static PRSolveState pr_prepare(GraphImpl &g, bool personalized, uint32_t source,
     a.source = source;
     a.personalized = personalized ? 1u : 0u;
     a.use_cond = 0;
-    a.red = PRSlots{slots, group_sum, group_count, groups_done, static_cast<uint32_t>(num_slots),
+    a.red = PRSlots{slots, group_sum, blocks_done, static_cast<uint32_t>(num_slots),
                     static_cast<uint32_t>(num_groups)};
     a.tasks = g.pull_tasks.get();
 
@@ -417,6 +458,11 @@ static PRSolveState pr_prepare(GraphImpl &g, bool personalized, uint32_t source,
 static void pr_check_header(const PRHeader &h) {
     if (h.error) fail(HYT_E_TIMEOUT, "PageRank: a bounded wait for a staged copy ran out");
     if (h.iter == 0) fail(HYT_E_INTERNAL, "PageRank made no progress");
+}
+
+// Grid of the per-iteration reduce kernel (fixed for a solve).
+static unsigned pr_reduce_grid(const PRArgs &a) {
+    return static_cast<unsigned>(std::max<uint32_t>(1u, std::min<uint32_t>(a.red.num_groups, 148u * 4)));
 }
 
 static void pr_init(const PRSolveState &st, uint64_t V, cudaStream_t s) {
@@ -442,11 +488,13 @@ static void pr_solve(GraphImpl &g, bool personalized, uint32_t source, float dam
                                                        : pr_shared_bytes(g.num_hot, g.tile_cost));
     PRRange full{g.in_sources.get(), 0, g.num_chunks, 0, g.num_tiles};
     void *kargs[] = {&d_args, &full};
+    const unsigned rgrid = pr_reduce_grid(a);
     auto launch = [&] {
         if (staged)
             pr_staged_kernel<<<grid, kPRThreads, smem, s>>>(d_args);
         else
             pr_iterate_kernel<<<grid, kPRThreads, smem, s>>>(d_args, full);
+        pr_reduce_kernel<<<rgrid, kReduceThreads, 0, s>>>(d_args);
         HYT_CUDA(cudaGetLastError());
     };
 
@@ -485,8 +533,14 @@ static void pr_solve(GraphImpl &g, bool personalized, uint32_t source, float dam
         kp.blockDim = dim3(kPRThreads);
         kp.sharedMemBytes = smem;
         kp.kernelParams = kargs;
-        cudaGraphNode_t knode;
+        cudaGraphNode_t knode, rnode;
         HYT_CUDA(cudaGraphAddKernelNode(&knode, body, nullptr, 0, &kp));
+        cudaKernelNodeParams rp = {};
+        rp.func = reinterpret_cast<void *>(pr_reduce_kernel);
+        rp.gridDim = dim3(rgrid);
+        rp.blockDim = dim3(kReduceThreads);
+        rp.kernelParams = kargs;
+        HYT_CUDA(cudaGraphAddKernelNode(&rnode, body, &knode, 1, &rp));
         HYT_CUDA(cudaGraphInstantiate(&exec, graph, 0));
         HYT_CUDA(cudaGraphLaunch(exec, s));
     } else {
@@ -494,7 +548,7 @@ static void pr_solve(GraphImpl &g, bool personalized, uint32_t source, float dam
         for (uint32_t i = 0; i < max_iter; ++i) {
             if (flags & HYT_RUN_PROFILE) kt.start(s);
             launch();
-            ++launches;
+            launches += 2;
             if (flags & HYT_RUN_PROFILE) {
                 kt.stop(s);
                 const double ms = kt.ms();
@@ -518,7 +572,7 @@ static void pr_solve(GraphImpl &g, bool personalized, uint32_t source, float dam
     const double total_ms = total.ms();
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
-    if (use_graph) launches += h.iter;
+    if (use_graph) launches += 2 * h.iter;
     pr_check_header(h);
     if (ranks_out) graph_emit(g, ranks_out, g.rank[h.iter & 1].get(), s);
 
@@ -587,7 +641,10 @@ void pagerank_partitioned(GraphImpl &g, PullSource &src, bool personalized, uint
             ++launches;
             ++hot;
         }
-        // the iteration closed itself when its last slot group completed
+        pr_reduce_kernel<<<pr_reduce_grid(a), kReduceThreads, 0, s>>>(st0.d_args);
+        HYT_CUDA(cudaGetLastError());
+        ++launches;
+        // the reduce kernel closed the iteration
         HYT_CUDA(cudaMemcpyAsync(&h, st0.hdr, sizeof(h), cudaMemcpyDeviceToHost, s));
         HYT_CUDA(cudaStreamSynchronize(s));
         if (h.error) break;

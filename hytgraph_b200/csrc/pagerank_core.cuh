@@ -31,19 +31,19 @@ struct PRHeader {
 
 // Fixed-order reduction of an iteration's residual and dangling mass.
 // Every task owns a slot: tile k -> num_long + k, long row i -> i (written
-// by the warp that finalizes the row).  The warp whose slot completes a
-// group of kSlotGroup slots sums that group in slot order; the warp that
-// completes the last group sums the group sums in group order and closes the
-// iteration.  The result is the same for any grid, launch split or arrival
-// order.  Counters only grow (each iteration adds exactly the group size),
-// so they are cleared once per solve.
+// by the warp that finalizes the row) -- a plain store, nothing waits on it.
+// After the iteration's tasks, pr_reduce_kernel sums each group of
+// kSlotGroup slots in slot order (a fixed block tree), and its last block
+// sums the group sums in group order and closes the iteration.  The result
+// is the same for any grid, launch split or arrival order.  The counter
+// only grows (each iteration adds the reduce grid), so it is cleared once
+// per solve.
 constexpr uint32_t kSlotGroup = 1024;
 
 struct PRSlots {
     double2 *slot;          // [num_slots] (residual, dangling)
     double2 *group_sum;     // [num_groups]
-    uint32_t *group_count;  // [num_groups]
-    uint32_t *groups_done;  // [1]
+    uint32_t *blocks_done;  // [1] reduce blocks finished, over the whole solve
     uint32_t num_slots, num_groups;
 };
 
@@ -189,50 +189,9 @@ __device__ __forceinline__ void close_iteration(const PRArgs &a, uint32_t it, do
     }
 }
 
-// Records task slot `slot`'s (res, dang) of iteration `it` and, when that
-// completes a group (and then the last group), performs the fixed-order
-// sums described at PRSlots.  res / dang must be equal on all lanes; must
-// be called by all 32 lanes.
-__device__ __forceinline__ void slot_done(const PRArgs &a, uint32_t it, uint32_t slot, double res, double dang,
-                                          int lane) {
-    const PRSlots &R = a.red;
-    const uint32_t g = slot / kSlotGroup;
-    const uint32_t gsize = min(kSlotGroup, R.num_slots - g * kSlotGroup);
-    uint32_t last = 0;
-    if (lane == 0) {
-        R.slot[slot] = make_double2(res, dang);
-        __threadfence();
-        const uint32_t c = atomicAdd(&R.group_count[g], 1u) + 1u;
-        last = (c == (it + 1) * gsize) ? 1u : 0u;
-    }
-    if (!__shfl_sync(0xffffffffu, last, 0)) return;
-    __threadfence();
-    double r = 0.0, d = 0.0;
-    for (uint32_t i = lane; i < gsize; i += 32) {
-        const double2 x = __ldcg(R.slot + g * kSlotGroup + i);
-        r += x.x;
-        d += x.y;
-    }
-    r = dev::warp_sum(r);
-    d = dev::warp_sum(d);
-    last = 0;
-    if (lane == 0) {
-        R.group_sum[g] = make_double2(r, d);
-        __threadfence();
-        const uint32_t c = atomicAdd(R.groups_done, 1u) + 1u;
-        last = (c == (it + 1) * R.num_groups) ? 1u : 0u;
-    }
-    if (!__shfl_sync(0xffffffffu, last, 0)) return;
-    __threadfence();
-    r = d = 0.0;
-    for (uint32_t i = lane; i < R.num_groups; i += 32) {
-        const double2 x = __ldcg(R.group_sum + i);
-        r += x.x;
-        d += x.y;
-    }
-    r = dev::warp_sum(r);
-    d = dev::warp_sum(d);
-    if (lane == 0) close_iteration(a, it, r, d);
+// Records task slot `slot`'s (res, dang); lane 0 stores, no wait.
+__device__ __forceinline__ void slot_store(const PRArgs &a, uint32_t slot, double res, double dang, int lane) {
+    if (lane == 0) a.red.slot[slot] = make_double2(res, dang);
 }
 
 // Solver scalars of an iteration whose dangling mass (sum of x over
