@@ -374,7 +374,7 @@ struct PRSolveState {
 };
 
 // pr_state layout: args | header | residual[max_iter] | dangling[max_iter+1]
-// | init partials | init counter | reduce-blocks counter | (8-byte aligned)
+// | init partials | init counter | reduce-blocks counter | (16-byte aligned)
 // group sums | slots.  Everything from the header through the counters is
 // cleared at the start of a solve.
 static PRSolveState pr_prepare(GraphImpl &g, bool personalized, uint32_t source, float damping, float tolerance,
@@ -391,11 +391,11 @@ static PRSolveState pr_prepare(GraphImpl &g, bool personalized, uint32_t source,
     if (num_slots > 0xFFFFFFFFull) fail(HYT_E_UNSUPPORTED, "PageRank: too many pull tasks for one graph");
     const uint64_t num_groups = (num_slots + kSlotGroup - 1) / kSlotGroup;
     const uint64_t init_chunks = (V + kInitChunk - 1) / kInitChunk;
-    auto up8 = [](size_t x) { return (x + 7) & ~size_t(7); };
+    auto up16 = [](size_t x) { return (x + 15) & ~size_t(15); };  // double2 needs 16-byte alignment
     const size_t args_bytes = (sizeof(PRArgs) + 255) & ~size_t(255);
     const size_t head = sizeof(PRHeader) + size_t(max_iter) * sizeof(double) + size_t(max_iter + 1) * sizeof(double) +
                         size_t(init_chunks) * sizeof(double) + 2 * sizeof(uint32_t);
-    const size_t sb = args_bytes + up8(head) + size_t(num_groups + num_slots) * sizeof(double2) + 64;
+    const size_t sb = args_bytes + up16(head) + size_t(num_groups + num_slots) * sizeof(double2) + 64;
     if (g.pr_state.count < sb) g.pr_state.allocate(sb);
 
     unsigned char *base = g.pr_state.get();
@@ -414,10 +414,13 @@ static PRSolveState pr_prepare(GraphImpl &g, bool personalized, uint32_t source,
     uint32_t *blocks_done = reinterpret_cast<uint32_t *>(p);
     p += 4;
     const size_t zero_bytes = static_cast<size_t>(p - reinterpret_cast<unsigned char *>(hdr));
-    p = base + args_bytes + up8(head);
+    p = base + args_bytes + up16(head);
     double2 *group_sum = reinterpret_cast<double2 *>(p);
     p += size_t(num_groups) * sizeof(double2);
     double2 *slots = reinterpret_cast<double2 *>(p);
+    if (reinterpret_cast<uintptr_t>(base) % 256 || reinterpret_cast<uintptr_t>(group_sum) % 16 ||
+        reinterpret_cast<uintptr_t>(slots) % 16 || reinterpret_cast<uintptr_t>(residual) % 8)
+        fail(HYT_E_INTERNAL, "PageRank state layout is misaligned");
 
     PRArgs a{};
     a.in_off = g.in_offsets.get();
