@@ -1311,7 +1311,9 @@ def run_contrib_workload(args, rank, world, local, pg):
 def run_ppr8_workload(args, rank, world, local, pg):
     """One step = 8 personalized PageRank queries (restart 0.15, tol 1e-6)
     from seeded sources, packed into one hyt_ppr_multi call; the same 8
-    queries through hyt_ppr one at a time are timed beside it."""
+    queries through hyt_ppr one at a time are timed beside it.  The line
+    also reports 8 SSSP sources in one hyt_sssp_multi solve against the
+    same sources through hyt_sssp (device time, labels compared)."""
     import torch
 
     import hytgraph_b200 as hyt
@@ -1363,6 +1365,33 @@ def run_ppr8_workload(args, rank, world, local, pg):
     iters = sum(max(y["iterations"] for y in x) for x in timed) / args.steps
     kb = timed[0][0]["algorithmic_bytes"] / max(max(y["iterations"] for y in timed[0]), 1)
     it_ms = dev_ms / max(iters, 1)
+    # 8 SSSP sources in one hyt_sssp_multi solve against the same sources
+    # one at a time (hyt_sssp): labels identical, timed on the device
+    ss_out = torch.empty((8, V), dtype=torch.int32, device="cuda")
+    ss_one = torch.empty(V, dtype=torch.int32, device="cuda")
+    src8 = sources()
+    g.sssp_multi(src8, out=ss_out)
+    torch.cuda.synchronize()
+    ms_multi, ms_single, multi_st = [], [], None
+    for _ in range(max(args.steps, 1)):
+        src8 = sources()
+        _, multi_st = g.sssp_multi(src8, out=ss_out)
+        ms_multi.append(multi_st["device_ms"])
+        tot = 0.0
+        for lane, s_ in enumerate(src8):
+            _, st1 = g.sssp(int(s_), out=ss_one)
+            tot += st1["device_ms"]
+            if lane == 0:
+                torch.cuda.synchronize()
+                same = bool(torch.equal(ss_one, ss_out[0]))
+                if not same:
+                    raise SystemExit("hyt_sssp_multi lane 0 differs from hyt_sssp")
+        ms_single.append(tot)
+    sssp8 = {"sources_per_solve": 8, "ms_per_solve": statistics.median(ms_multi),
+             "one_at_a_time_ms_for_8": statistics.median(ms_single),
+             "speedup_vs_one_at_a_time": statistics.median(ms_single) / statistics.median(ms_multi),
+             "rounds": multi_st["iterations"], "relaxations_per_edge": multi_st["edges_processed"] / E,
+             "gteps": 8 * E / (statistics.median(ms_multi) / 1e3) / 1e9}
     roof = {"kernel": "ppr8 iteration (prep + rows + long rows)", "bound": "hbm",
             "achieved": kb / (it_ms / 1e3) / 1e9, "peak": peak_gbs, "unit": "GB/s",
             "frac": kb / (it_ms / 1e3) / 1e9 / peak_gbs, "traffic": None, "peak_kind": peak_kind,
@@ -1395,7 +1424,7 @@ def run_ppr8_workload(args, rank, world, local, pg):
                 "one_at_a_time": {"queries_per_s": 8 / (single_ms / 1e3), "ms_per_query": single_ms / 8,
                                   "iterations": [s_["iterations"] for s_ in singles]},
                 "speedup_vs_one_at_a_time": value / (8 / (single_ms / 1e3)),
-                "packed": {"device_ms_per_solve": dev_ms, "iterations_per_solve": iters},
+                "packed": {"device_ms_per_solve": dev_ms, "iterations_per_solve": iters}, "sssp8": sssp8,
                 "roofline": roof, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": None}
         print(json.dumps(line), flush=True)
 
