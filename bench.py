@@ -1667,8 +1667,12 @@ def main():
     # pure kernel time of one PageRank iteration (per-launch events), same inputs
     _, prof = graph.pagerank(out=ranks_out, stream=sptr, flags=capi.HYT_RUN_PROFILE)
     kern_ms = prof["kernel_ms"] / max(prof["kernel_launches"], 1)
-    dominant = "pr_iterate_kernel" if pr_ms >= ss_ms else "sssp_pull_kernel+sssp_expand_kernel+sssp_hub_kernel"
-    if pr_ms >= ss_ms:
+    pr_name = "pr_staged_kernel+pr_reduce_kernel" if os.environ.get("HYT_STAGED", "1") != "0" else \
+        "pr_iterate_kernel+pr_reduce_kernel"
+    ss_name = ("sssp_pull_staged_kernel" if os.environ.get("HYT_STAGED", "1") != "0" else "sssp_pull_kernel") + \
+        "+sssp_expand_kernel+sssp_hub_kernel"
+    dominant = pr_name if pr_ms >= ss_ms else ss_name
+    if dominant == pr_name:
         roof = {"kernel": dominant, "bound": "hbm", "achieved": pr_gbs, "peak": peak_gbs, "unit": "GB/s",
                 "frac": pr_gbs / peak_gbs, "traffic": None, "peak_kind": peak_kind,
                 "algorithmic_bytes_per_launch": pr_bytes / max(pr_it, 1), "avg_launch_ms": pr_launch_ms,
@@ -1683,7 +1687,7 @@ def main():
     traffic_file = ROOT / "profiles" / "traffic.json"
     if traffic_file.exists():
         tr = json.loads(traffic_file.read_text()).get(f"s{args.scale}_ef{args.edge_factor}", {})
-        roof["traffic"] = tr.get("pr_iterate_kernel" if dominant == "pr_iterate_kernel" else "sssp_solve")
+        roof["traffic"] = tr.get("pr_iteration" if dominant == pr_name else "sssp_solve")
         roof["traffic_measured"] = bool(tr.get("measured", False))
 
     launches = sum(s["total_launches"] for s in timed["pr"]) + sum(s["total_launches"] for s in timed["sssp"])
