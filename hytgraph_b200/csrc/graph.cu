@@ -67,29 +67,26 @@ __global__ void out_degree_kernel(const uint64_t *off, uint64_t V, uint32_t *deg
 // Writes the source vertex of every CSR edge.  A CTA owns 256 consecutive
 // rows; their edges are spread over all threads via an in-CTA prefix of the
 // degrees, so rows of any length are load-balanced inside the CTA.
-__global__ void __launch_bounds__(256) expand_sources_kernel(const uint64_t *off, uint64_t V, uint32_t *src) {
-    __shared__ uint64_t s_first[257];
-    const uint64_t v0 = uint64_t(blockIdx.x) * 256;
-    for (uint64_t base = v0; base < V; base += uint64_t(gridDim.x) * 256) {
-        const uint64_t v = base + threadIdx.x;
-        const uint64_t hi = (base + 256 < V) ? base + 256 : V;
-        if (v <= hi) s_first[threadIdx.x] = off[v];
-        if (threadIdx.x == 0) s_first[hi - base] = off[hi];
-        __syncthreads();
-        const uint64_t e0 = s_first[0], e1 = s_first[hi - base];
-        const int nrows = static_cast<int>(hi - base);
-        for (uint64_t e = e0 + threadIdx.x; e < e1; e += 256) {
-            // last row r with s_first[r] <= e
-            int lo = 0, hi2 = nrows - 1;
-            while (lo < hi2) {
-                const int mid = (lo + hi2 + 1) >> 1;
-                if (s_first[mid] <= e) lo = mid; else hi2 = mid - 1;
-            }
-            src[e] = static_cast<uint32_t>(base + lo);
-        }
-        __syncthreads();
+// Source row of every edge, in two balanced passes (no block walks a hub
+// row alone): each non-empty row writes its id at its first edge, then an
+// inclusive max-scan over the edges carries it to the rest of the row
+// (row ids are non-decreasing along the edge array).
+__global__ void mark_row_starts_kernel(const uint64_t *off, uint64_t V, uint32_t *src) {
+    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+    for (uint64_t v = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; v < V; v += stride) {
+        const uint64_t b = off[v];
+        if (off[v + 1] > b) src[b] = static_cast<uint32_t>(v);
     }
 }
+
+void expand_sources(const uint64_t *off, uint64_t V, uint64_t E, uint32_t *src, cudaStream_t s) {
+    if (E == 0) return;
+    Scratch<uint32_t> marks(E, s);
+    HYT_CUDA(cudaMemsetAsync(marks.get(), 0, E * sizeof(uint32_t), s));
+    mark_row_starts_kernel<<<grid_for(V, 256), 256, 0, s>>>(off, V, marks.get());
+    HYT_CUDA(cudaGetLastError());
+    prims::inclusive_max_scan_u32(marks.get(), src, E, s);
+}  // marks is freed in stream order, after the scan
 
 // Row offsets of a sorted key array: off[v] = first position with key >= v.
 __global__ void offsets_from_sorted_kernel(const uint32_t *keys, uint64_t E, uint64_t V, uint64_t *off) {
@@ -493,23 +490,20 @@ void graph_build(GraphImpl &g, const hyt_csr &csr, uint32_t flags) {
         const bool csc_weights = (flags & HYT_GRAPH_PUSH) && keep_weights && g.weights.get();
         if (E) {
             HYT_CUDA(cudaMemcpyAsync(keys.get(), g.cols.get(), E * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
-            const unsigned blocks = static_cast<unsigned>(std::min<uint64_t>((V + 255) / 256, 148ull * 64));
             if (csc_weights) {
                 Scratch<uint32_t> perm(E, s);
                 iota_kernel<<<grid_for(E, 256), 256, 0, s>>>(perm.get(), E);
                 HYT_CUDA(cudaGetLastError());
                 prims::sort_pairs_u32(keys.get(), perm.get(), E, bits_for(V - 1), s);
                 Scratch<uint32_t> src(E, s);
-                expand_sources_kernel<<<blocks, 256, 0, s>>>(g.row_offsets.get(), V, src.get());
-                HYT_CUDA(cudaGetLastError());
+                expand_sources(g.row_offsets.get(), V, E, src.get(), s);
                 gather_u32_kernel<<<grid_for(E, 256), 256, 0, s>>>(src.get(), perm.get(), E, g.in_sources.get());
                 g.in_weights.allocate(E);
                 gather_u32_kernel<<<grid_for(E, 256), 256, 0, s>>>(g.weights.get(), perm.get(), E, g.in_weights.get());
                 HYT_CUDA(cudaGetLastError());
                 HYT_CUDA(cudaStreamSynchronize(s));
             } else {
-                expand_sources_kernel<<<blocks, 256, 0, s>>>(g.row_offsets.get(), V, g.in_sources.get());
-                HYT_CUDA(cudaGetLastError());
+                expand_sources(g.row_offsets.get(), V, E, g.in_sources.get(), s);
                 prims::sort_pairs_u32(keys.get(), g.in_sources.get(), E, bits_for(V - 1), s);
             }
         }

@@ -55,6 +55,14 @@ void sort_pairs_desc_u64(uint64_t *keys, uint32_t *vals, size_t n, cudaStream_t 
     HYT_CUDA(cudaStreamSynchronize(s));
 }
 
+void inclusive_max_scan_u32(const uint32_t *in, uint32_t *out, size_t n, cudaStream_t s) {
+    if (n == 0) return;
+    size_t tb = 0;
+    HYT_CUDA(cub::DeviceScan::InclusiveScan(nullptr, tb, in, out, cub::Max(), static_cast<int64_t>(n), s));
+    Scratch<uint8_t> tmp(tb, s);
+    HYT_CUDA(cub::DeviceScan::InclusiveScan(tmp.get(), tb, in, out, cub::Max(), static_cast<int64_t>(n), s));
+}
+
 void sort_keys_u64(uint64_t *keys, size_t n, int end_bit, cudaStream_t s) {
     if (n < 2) return;
     Scratch<uint64_t> k2(n, s);

@@ -28,6 +28,9 @@ void sort_keys_u64(uint64_t *keys, size_t n, int end_bit, cudaStream_t s);
 void exclusive_scan_u64(const uint64_t *in, uint64_t *out, size_t n, cudaStream_t s);
 void exclusive_scan_u32(const uint32_t *in, uint32_t *out, size_t n, cudaStream_t s);
 
+// out[i] = max_{j<=i} in[j] (inclusive max scan); in and out distinct.
+void inclusive_max_scan_u32(const uint32_t *in, uint32_t *out, size_t n, cudaStream_t s);
+
 // Keeps in[i] where flags[i] != 0 (order preserved); returns the count.
 size_t select_flagged_u64(const uint64_t *in, const uint8_t *flags, uint64_t *out, size_t n,
                           cudaStream_t s);
