@@ -382,14 +382,16 @@ void ppr_multi(GraphImpl &g, const uint32_t *sources, uint32_t k, float restart,
     p.active = (1u << k) - 1u;
     p.d = 1.0 - double(restart);
     // staged task pass when the graph carries task descriptors (in HBM)
-    const bool staged = g.pull_tasks.get() && stage::staged_shared_bytes(g.num_hot) <= kPRSmemMax;
+    const bool staged = g.pull_tasks.get() && stage::staged_shared_bytes(g.num_hot) + 4096 <= kPRSmemMax;
     const unsigned smem = static_cast<unsigned>(stage::staged_shared_bytes(g.num_hot));
     if (staged) {
-        static bool attr = false;
-        if (!attr) {
+        // the kernel's static shared memory counts against the same
+        // per-block limit, so ask for exactly what this launch uses
+        static unsigned attr = 0;
+        if (smem > attr) {
             HYT_CUDA(cudaFuncSetAttribute(ppr8_tasks_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          static_cast<int>(kPRSmemMax)));
-            attr = true;
+                                          static_cast<int>(smem)));
+            attr = smem;
         }
     }
     const unsigned rows_grid = staged ? grid_sm(1) : grid_sm(8);
