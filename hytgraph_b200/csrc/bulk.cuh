@@ -58,14 +58,19 @@ __device__ __forceinline__ uint64_t policy_evict_first() {
     return pol;
 }
 
+// Waits for the phase with the given parity, letting the hardware suspend
+// the thread for up to kSuspendNs while the phase is incomplete (a parked
+// warp leaves its issue slots to the others); true once the phase is done.
+constexpr uint32_t kSuspendNs = 1000000;
+
 __device__ __forceinline__ bool mbar_test_parity(uint64_t *bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(ok)
-        : "r"(smem_addr(bar)), "r"(parity)
+        : "r"(smem_addr(bar)), "r"(parity), "r"(kSuspendNs)
         : "memory");
     return ok != 0;
 }

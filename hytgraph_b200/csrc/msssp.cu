@@ -43,7 +43,7 @@ using ssc::kHubDegree;
 
 constexpr int kML = 8;             // labels per vertex row (32 bytes)
 constexpr int kMSThreads = 256;    // push kernels
-constexpr int kMPThreads = 1024;   // pull sweep (one CTA per SM)
+constexpr int kMPThreads = stage::kStageThreads;   // pull sweep (one CTA per SM)
 
 struct MSHeader {
     uint32_t round, done, converged, error;
@@ -327,7 +327,7 @@ __global__ void __launch_bounds__(kMPThreads, 1) ms_pull_kernel(const MSArgs *__
     const uint64_t nwarps = uint64_t(gridDim.x) * (kMPThreads / 32);
     Row8 acc;  // per-lane minima of the current chunk
     const bool ok = stage::stage_pipeline(
-        a.tasks, a.in_src, uint64_t(blockIdx.x) * (kMPThreads / 32) + warp, nwarps, a.num_tasks, ws.slots, ws.bars,
+        a.tasks, a.in_src, uint64_t(blockIdx.x) * (kMPThreads / 32) + warp, nwarps, a.num_tasks, ws,
         lane, [&](uint4 d, uint64_t, uint32_t j, uint32_t nu, uint32_t *slot, uint64_t a0) {
             if (task_is_chunk(d)) {
                 const stage::Unit u = stage::unit_of(d, j);

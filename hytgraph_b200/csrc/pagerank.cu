@@ -61,11 +61,12 @@ __device__ __forceinline__ uint32_t tile_slot(const PRArgs &a, uint64_t k) {
 
 // Hot-source contributions of this iteration, loaded once per CTA.
 __device__ __forceinline__ void load_hot(const PRArgs &a, const PRBuffers &b, float *s_hot) {
-    for (uint32_t i0 = 0; i0 < a.num_hot; i0 += 8 * kPRThreads) {
+    const uint32_t nt = blockDim.x;
+    for (uint32_t i0 = 0; i0 < a.num_hot; i0 += 8 * nt) {
         uint32_t hv[8];
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
-            const uint32_t i = i0 + k * kPRThreads + threadIdx.x;
+            const uint32_t i = i0 + k * nt + threadIdx.x;
             hv[k] = (i < a.num_hot) ? a.hot_vertex[i] : 0u;
         }
         float hc[8];
@@ -73,7 +74,7 @@ __device__ __forceinline__ void load_hot(const PRArgs &a, const PRBuffers &b, fl
         for (int k = 0; k < 8; ++k) hc[k] = b.ccur[hv[k]];
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
-            const uint32_t i = i0 + k * kPRThreads + threadIdx.x;
+            const uint32_t i = i0 + k * nt + threadIdx.x;
             if (i < a.num_hot) s_hot[i] = hc[k];
         }
     }
@@ -156,7 +157,7 @@ __device__ __forceinline__ void gather_staged(const uint32_t *slot, uint64_t a0,
     }
 }
 
-__global__ void __launch_bounds__(kPRThreads, 1) pr_staged_kernel(const PRArgs *__restrict__ args) {
+__global__ void __launch_bounds__(kStageThreads, 1) pr_staged_kernel(const PRArgs *__restrict__ args) {
     extern __shared__ __align__(128) unsigned char s_stage[];
     const PRArgs a = *args;
     const uint32_t it = *(volatile uint32_t *)&a.hdr->iter;
@@ -172,10 +173,10 @@ __global__ void __launch_bounds__(kPRThreads, 1) pr_staged_kernel(const PRArgs *
     __syncthreads();
 
     const uint64_t total = a.num_chunks + a.num_tiles;
-    const uint64_t nwarps = uint64_t(gridDim.x) * (kPRThreads / 32);
+    const uint64_t nwarps = uint64_t(gridDim.x) * kStageWarps;
     dev::CSum acc;  // running sum of the current chunk
     const bool ok = stage_pipeline(
-        a.tasks, a.in_src, uint64_t(blockIdx.x) * (kPRThreads / 32) + warp, nwarps, total, ws.slots, ws.bars, lane,
+        a.tasks, a.in_src, uint64_t(blockIdx.x) * kStageWarps + warp, nwarps, total, ws, lane,
         [&](uint4 d, uint64_t task, uint32_t j, uint32_t nu, uint32_t *slot, uint64_t a0) {
             double res = 0.0, dang = 0.0;
             if (task_is_chunk(d)) {
@@ -350,6 +351,19 @@ int pr_occupancy_grid() {
     return grid;
 }
 
+// Grid of the staged kernel: one CTA per SM, or HYT_PR_GRID CTAs.
+int pr_staged_grid() {
+    static int grid = 0;
+    if (grid == 0) {
+        grid = sm_count();
+        if (const char *e = std::getenv("HYT_PR_GRID")) {
+            const long v = std::strtol(e, nullptr, 10);
+            if (v > 0 && v <= 65535) grid = static_cast<int>(v);
+        }
+    }
+    return grid;
+}
+
 // HYT_STAGED=0 selects the register-path kernel for in-HBM solves too
 // (same tasks, same sums; for comparisons).
 bool pr_use_staged(const GraphImpl &g) {
@@ -485,6 +499,7 @@ static void pr_solve(GraphImpl &g, bool personalized, uint32_t source, float dam
     const bool use_graph = !(flags & HYT_RUN_NO_GRAPH) && !(flags & HYT_RUN_PROFILE);
     const int grid = pr_occupancy_grid();
     const bool staged = pr_use_staged(g);
+    const int sgrid = pr_staged_grid();
     const void *kfunc = staged ? reinterpret_cast<const void *>(pr_staged_kernel)
                                : reinterpret_cast<const void *>(pr_iterate_kernel);
     const unsigned smem = static_cast<unsigned>(staged ? staged_shared_bytes(g.num_hot)
@@ -494,7 +509,7 @@ static void pr_solve(GraphImpl &g, bool personalized, uint32_t source, float dam
     const unsigned rgrid = pr_reduce_grid(a);
     auto launch = [&] {
         if (staged)
-            pr_staged_kernel<<<grid, kPRThreads, smem, s>>>(d_args);
+            pr_staged_kernel<<<sgrid, kStageThreads, smem, s>>>(d_args);
         else
             pr_iterate_kernel<<<grid, kPRThreads, smem, s>>>(d_args, full);
         pr_reduce_kernel<<<rgrid, kReduceThreads, 0, s>>>(d_args);
@@ -532,8 +547,8 @@ static void pr_solve(GraphImpl &g, bool personalized, uint32_t source, float dam
         cudaGraph_t body = cp.conditional.phGraph_out[0];
         cudaKernelNodeParams kp = {};
         kp.func = const_cast<void *>(kfunc);
-        kp.gridDim = dim3(grid);
-        kp.blockDim = dim3(kPRThreads);
+        kp.gridDim = dim3(staged ? sgrid : grid);
+        kp.blockDim = dim3(staged ? kStageThreads : kPRThreads);
         kp.sharedMemBytes = smem;
         kp.kernelParams = kargs;
         cudaGraphNode_t knode, rnode;

@@ -207,7 +207,7 @@ __global__ void ppr8_long_rows_kernel(const LongRow *__restrict__ long_rows, uin
 // depend on the lane count, so a query's bits do not depend on its
 // companions.  Residual partials are per block over a static task
 // assignment (fixed for a fixed grid).
-constexpr int kTaskThreads = 1024;
+constexpr int kTaskThreads = stage::kStageThreads;
 constexpr int kUnroll = 8;
 
 // Sum over in-edges [b, e) of c[u][lane] from staged ids, thread t taking
@@ -254,7 +254,7 @@ __global__ void __launch_bounds__(kTaskThreads, 1)
     double res = 0.0;  // this thread's lane, rows of this warp's tasks in task order
     double acc = 0.0;  // running chunk sum
     const bool ok = stage::stage_pipeline(
-        tasks, in_src, uint64_t(blockIdx.x) * (kTaskThreads / 32) + warp, nwarps, num_tasks, ws.slots, ws.bars, t,
+        tasks, in_src, uint64_t(blockIdx.x) * (kTaskThreads / 32) + warp, nwarps, num_tasks, ws, t,
         [&](uint4 d, uint64_t, uint32_t j, uint32_t nu, uint32_t *slot, uint64_t a0) {
             if (task_is_chunk(d)) {
                 const stage::Unit u = stage::unit_of(d, j);

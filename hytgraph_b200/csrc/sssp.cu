@@ -308,8 +308,8 @@ __device__ __forceinline__ bool pull_relax_seen(const SSArgs &a, const RoundView
 }
 
 template <int WK>
-__global__ void __launch_bounds__(kPullThreads, 1) sssp_pull_staged_kernel(const SSArgs *__restrict__ args,
-                                                                           PullGraph pg) {
+__global__ void __launch_bounds__(stage::kStageThreads, 1) sssp_pull_staged_kernel(const SSArgs *__restrict__ args,
+                                                                                   PullGraph pg) {
     extern __shared__ __align__(128) unsigned char s_stage[];
     const SSArgs a = *args;
     if (*(volatile uint32_t *)&a.hdr->done || !pull_round(a)) return;
@@ -321,10 +321,10 @@ __global__ void __launch_bounds__(kPullThreads, 1) sssp_pull_staged_kernel(const
     __syncthreads();
     const uint64_t pol = dev::policy_evict_last();
     const uint64_t total = pg.num_chunks + pg.num_tiles;
-    const uint64_t nwarps = uint64_t(gridDim.x) * (kPullThreads / 32);
+    const uint64_t nwarps = uint64_t(gridDim.x) * stage::kStageWarps;
     uint32_t best = a.inf;  // running minimum of the current chunk
     const bool ok = stage::stage_pipeline(
-        pg.tasks, pg.in_src, uint64_t(blockIdx.x) * (kPullThreads / 32) + warp, nwarps, total, ws.slots, ws.bars,
+        pg.tasks, pg.in_src, uint64_t(blockIdx.x) * stage::kStageWarps + warp, nwarps, total, ws,
         lane, [&](uint4 d, uint64_t, uint32_t j, uint32_t nu, uint32_t *slot, uint64_t a0) {
             if (task_is_chunk(d)) {
                 // slice of a long row: warp minimum, then one relaxation
@@ -535,7 +535,8 @@ int pull_grid(bool staged, unsigned smem) {
     }
     int per_sm = 0;
     if (staged)
-        HYT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sssp_pull_staged_kernel<WK>, kPullThreads, smem));
+        HYT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sssp_pull_staged_kernel<WK>,
+                                                               stage::kStageThreads, smem));
     else
         HYT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sssp_pull_kernel<WK>, kPullThreads, smem));
     return sm_count() * std::max(per_sm, 1);
@@ -678,7 +679,7 @@ void sssp_solve(GraphImpl &g, uint32_t source, uint32_t delta, uint32_t max_roun
         if (a.pull_div) add(reinterpret_cast<void *>(sssp_frontier_edges_kernel), dim3(grid), dim3(kSSThreads), 0, kargs);
         add(reinterpret_cast<void *>(sssp_expand_kernel<WK>), dim3(grid), dim3(kSSThreads), 0, kargs);
         add(reinterpret_cast<void *>(sssp_hub_kernel<WK>), dim3(grid), dim3(kSSThreads), 0, kargs);
-        if (a.pull_div) add(pull_fn, dim3(pgrid), dim3(kPullThreads), pull_smem, pargs);
+        if (a.pull_div) add(pull_fn, dim3(pgrid), dim3(staged ? stage::kStageThreads : kPullThreads), pull_smem, pargs);
         add(reinterpret_cast<void *>(sssp_round_end_kernel), dim3(1), dim3(1), 0, kargs);
         HYT_CUDA(cudaGraphInstantiate(&exec, graph, 0));
         HYT_CUDA(cudaGraphLaunch(exec, s));
@@ -692,7 +693,7 @@ void sssp_solve(GraphImpl &g, uint32_t source, uint32_t delta, uint32_t max_roun
             sssp_hub_kernel<WK><<<grid, kSSThreads, 0, s>>>(d_args);
             if (a.pull_div) {
                 if (staged)
-                    sssp_pull_staged_kernel<WK><<<pgrid, kPullThreads, pull_smem, s>>>(d_args, pg);
+                    sssp_pull_staged_kernel<WK><<<pgrid, stage::kStageThreads, pull_smem, s>>>(d_args, pg);
                 else
                     sssp_pull_kernel<WK><<<pgrid, kPullThreads, pull_smem, s>>>(d_args, pg);
             }

@@ -21,30 +21,52 @@ namespace hyt::stage {
 
 constexpr uint32_t kUnitEdges = 512;  // edges of one staged unit (a tile, or a piece of a chunk)
 constexpr uint32_t kSlotWords = 520;  // unit + 16-byte alignment at both ends, in 4-byte words
-constexpr int kStageSlots = 2;        // staging slots per warp (double buffering)
+#ifndef HYT_STAGE_SLOTS
+#define HYT_STAGE_SLOTS 3
+#endif
+#ifndef HYT_STAGE_WARPS
+#define HYT_STAGE_WARPS 24
+#endif
+constexpr int kStageSlots = HYT_STAGE_SLOTS;  // staging slots per warp: units staged ahead + 1
+constexpr int kStageWarps = HYT_STAGE_WARPS;  // warps per CTA of the staged kernels
+constexpr int kStageThreads = kStageWarps * 32;
+static_assert(kStageSlots >= 2, "at least double buffering");
 // A tile's edges: the rows starting inside a tile span < tile_cost merge
 // units, and its last short row adds < tile_cost more, so < 2 * tile_cost.
 static_assert(2 * kTileCostMax - 1 + 6 <= kSlotWords, "a tile's edges must fit one staging slot");
 static_assert(kLongChunk % kUnitEdges == 0, "chunks split into whole units");
 
-// Dynamic shared memory of the staged kernels: per-warp mbarriers and slots,
-// then the hot-source table.
-constexpr size_t kStageHead = size_t(kPRThreads / 32) * kStageSlots * sizeof(uint64_t);
-constexpr size_t kStageBytes = kStageHead + size_t(kPRThreads / 32) * kStageSlots * kSlotWords * 4;
+// The unit a slot holds (written by lane 0 when its copy is issued).
+struct UnitMeta {
+    uint4 d;     // task descriptor
+    uint64_t t;  // task index
+    uint32_t j;  // unit of the task
+    uint32_t pad;
+};
+
+// Dynamic shared memory of the staged kernels: per-warp mbarriers, unit
+// records and slots, then the hot-source table.
+constexpr size_t kStageBars = size_t(kStageWarps) * kStageSlots * sizeof(uint64_t);
+constexpr size_t kStageMeta = size_t(kStageWarps) * kStageSlots * sizeof(UnitMeta);
+constexpr size_t kStageHead = ((kStageBars + kStageMeta + 127) / 128) * 128;
+constexpr size_t kStageBytes = kStageHead + size_t(kStageWarps) * kStageSlots * kSlotWords * 4;
 
 inline size_t staged_shared_bytes(uint32_t num_hot) { return kStageBytes + size_t(num_hot) * 4; }
 
 #ifdef __CUDACC__
 
-// This warp's barriers and slots in the kernel's dynamic shared memory
-// (kStageBytes from its start); lane 0 initialises the barriers.
+// This warp's barriers, unit records and slots in the kernel's dynamic
+// shared memory (kStageBytes from its start); lane 0 initialises the
+// barriers.
 struct WarpStage {
     uint64_t *bars;
+    UnitMeta *meta;
     uint32_t *slots;
 };
 __device__ __forceinline__ WarpStage warp_stage(unsigned char *smem, int warp, int lane) {
     WarpStage w;
     w.bars = reinterpret_cast<uint64_t *>(smem) + warp * kStageSlots;
+    w.meta = reinterpret_cast<UnitMeta *>(smem + kStageBars) + warp * kStageSlots;
     w.slots = reinterpret_cast<uint32_t *>(smem + kStageHead) + size_t(warp) * kStageSlots * kSlotWords;
     if (lane == 0)
         for (int i = 0; i < kStageSlots; ++i) bulk::mbar_init(w.bars + i);
@@ -80,54 +102,65 @@ __device__ __forceinline__ void stage_unit(const uint32_t *in_src, Unit u, uint3
 }
 
 // Drives one warp through its tasks (first, first + stride, ... < total):
-// stages unit after unit into the warp's slots, one copy ahead, and calls
-// consume(d, task, j, units, slot words, first staged edge) for each unit
-// once its ids have landed.  false: a wait ran out (the copy still in
-// flight has been waited for, within the same budget).
+// keeps kStageSlots - 1 units staged ahead of the one being worked on, and
+// calls consume(d, task, j, units, slot words, first staged edge) for each
+// unit once its ids have landed.  false: a wait ran out (the copies still in
+// flight have been waited for, within the same budget).
 template <class Consume>
 __device__ __forceinline__ bool stage_pipeline(const uint4 *tasks, const uint32_t *in_src, uint64_t first,
-                                               uint64_t stride, uint64_t total, uint32_t *slots, uint64_t *bars,
-                                               int lane, Consume &&consume) {
+                                               uint64_t stride, uint64_t total, const WarpStage &ws, int lane,
+                                               Consume &&consume) {
     if (first >= total) return true;
     const uint64_t pol = bulk::policy_evict_first();
-    uint4 d = tasks[first];
-    uint64_t t = first, nt = first + stride;
+    // producer cursor: the next unit to stage
+    uint4 pd = tasks[first];
+    uint64_t pt = first, nt = first + stride;
     uint4 dn = nt < total ? tasks[nt] : make_uint4(0, 0, 0, 0);
-    uint32_t j = 0, phase = 0;
-    int s = 0;
-    stage_unit(in_src, unit_of(d, 0), slots, bars, pol, lane);
-    for (;;) {
-        const uint32_t nu = units_of(d);
-        bool more = true;
-        uint4 d2 = d;
-        uint64_t t2 = t;
-        uint32_t j2 = j + 1;
-        if (j2 >= nu) {
-            more = nt < total;
-            d2 = dn;
-            t2 = nt;
-            j2 = 0;
-            if (more) {
+    uint32_t pj = 0;
+    bool pvalid = true;
+    auto produce = [&](int slot) {
+        if (lane == 0) ws.meta[slot] = UnitMeta{pd, pt, pj, 0};
+        stage_unit(in_src, unit_of(pd, pj), ws.slots + slot * kSlotWords, ws.bars + slot, pol, lane);
+        if (pj + 1 < units_of(pd)) {
+            ++pj;
+        } else {
+            pvalid = nt < total;
+            pd = dn;
+            pt = nt;
+            pj = 0;
+            if (pvalid) {
                 nt += stride;
                 dn = nt < total ? tasks[nt] : make_uint4(0, 0, 0, 0);
             }
         }
-        if (more) stage_unit(in_src, unit_of(d2, j2), slots + (s ^ 1) * kSlotWords, bars + (s ^ 1), pol, lane);
-        if (!bulk::mbar_wait(bars + s, (phase >> s) & 1u)) {
-            if (more) bulk::mbar_wait(bars + (s ^ 1), (phase >> (s ^ 1)) & 1u);
+    };
+    uint64_t issued = 0, consumed = 0;
+    for (int s = 0; s < kStageSlots && pvalid; ++s, ++issued) produce(s);
+    __syncwarp();
+    uint32_t phase = 0;
+    while (consumed < issued) {
+        const int s = static_cast<int>(consumed % kStageSlots);
+        if (!bulk::mbar_wait(ws.bars + s, (phase >> s) & 1u)) {
+            for (uint64_t c = consumed + 1; c < issued; ++c) {  // copies still in flight
+                const int o = static_cast<int>(c % kStageSlots);
+                bulk::mbar_wait(ws.bars + o, (phase >> o) & 1u);
+            }
             return false;
         }
         phase ^= 1u << s;
-        const Unit u = unit_of(d, j);
-        consume(d, t, j, nu, slots + s * kSlotWords, u.lo & ~uint64_t(3));
+        const UnitMeta m = ws.meta[s];
+        const Unit u = unit_of(m.d, m.j);
+        consume(m.d, m.t, m.j, units_of(m.d), ws.slots + s * kSlotWords, u.lo & ~uint64_t(3));
         bulk::fence_proxy_async_smem();  // this slot's generic accesses before its next bulk copy
         __syncwarp();
-        if (!more) return true;
-        d = d2;
-        t = t2;
-        j = j2;
-        s ^= 1;
+        ++consumed;
+        if (pvalid) {
+            produce(s);
+            ++issued;
+            __syncwarp();
+        }
     }
+    return true;
 }
 
 #endif  // __CUDACC__
