@@ -16,6 +16,7 @@
 #include "prims.cuh"
 #include "scratch.cuh"
 #include "solvers.cuh"
+#include "stage.cuh"
 
 namespace hyt {
 namespace {
@@ -406,8 +407,9 @@ void graph_build(GraphImpl &g, const hyt_csr &csr, uint32_t flags) {
         fail(HYT_E_INVALID, "weights is NULL for a weighted graph");
     if (flags == 0) flags = HYT_GRAPH_ALL;
     // PageRank decomposition knobs (same work, different tiling): tile cost
-    // in {64..256} and hot-source cache size, bounded by shared memory.
-    g.tile_cost = kTileCostDefault;
+    // in {64..512} and hot-source cache size, bounded by shared memory.  The
+    // staged kernels (HYT_STAGED=1) need tiles that fit one staging slot.
+    g.tile_cost = stage::staged_requested() ? kStageTileMax : kTileCostDefault;
     if (const char *t = std::getenv("HYT_PR_TILE")) {
         const unsigned long v = std::strtoul(t, nullptr, 10);
         if (v >= 64 && v <= kTileCostMax) g.tile_cost = static_cast<uint32_t>(v);

@@ -25,8 +25,9 @@ namespace hyt {
 // the tile and split into kLongChunk-edge chunks.  One warp processes one
 // task (tile or chunk), so a tile's staged contributions fit in a per-warp
 // shared-memory slice of 2 * tile_cost floats.
-constexpr uint32_t kTileCostDefault = 256;   // merge-path units per tile (tunable: HYT_PR_TILE)
-constexpr uint32_t kTileCostMax = 256;       // a tile's edges (< 2 * tile_cost) fit one staging slot
+constexpr uint32_t kTileCostDefault = 512;   // merge-path units per tile (tunable: HYT_PR_TILE)
+constexpr uint32_t kTileCostMax = 512;       // register-path tiles; bulk-staged tasks need <= kStageTileMax
+constexpr uint32_t kStageTileMax = 256;      // a tile's edges (< 2 * tile_cost) fit one staging slot
 constexpr uint32_t kLongChunk = 4096;
 constexpr uint32_t kHotSourcesDefault = 8192;   // shared-memory source cache (tunable: HYT_PR_HOT)
 constexpr uint32_t kHotSourcesMax = 32768;

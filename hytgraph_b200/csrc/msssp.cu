@@ -312,23 +312,25 @@ __device__ __forceinline__ void pull_edges(const MSArgs &a, const uint32_t *s_ho
     }
 }
 
-template <int WK>
+// kStaged: ids staged into shared memory by bulk copies (tiles fit a
+// staging slot); otherwise read from global memory in place.
+template <int WK, bool kStaged>
 __global__ void __launch_bounds__(kMPThreads, 1) ms_pull_kernel(const MSArgs *__restrict__ args) {
     extern __shared__ __align__(128) unsigned char s_stage[];
     const MSArgs a = *args;
     if (*(volatile uint32_t *)&a.hdr->done || !pull_round(a)) return;
     const View w = view(a);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const stage::WarpStage ws = stage::warp_stage(s_stage, warp, lane);
-    uint32_t *s_hot = reinterpret_cast<uint32_t *>(s_stage + stage::kStageBytes);
+    stage::WarpStage ws{};
+    if constexpr (kStaged) ws = stage::warp_stage(s_stage, warp, lane);
+    uint32_t *s_hot = reinterpret_cast<uint32_t *>(s_stage + (kStaged ? stage::kStageBytes : 0));
     for (uint32_t i = threadIdx.x; i < a.num_hot; i += blockDim.x) s_hot[i] = a.hot_vertex[i];
     __syncthreads();
     const uint64_t pol = dev::policy_evict_last();
     const uint64_t nwarps = uint64_t(gridDim.x) * (kMPThreads / 32);
+    const uint64_t first = uint64_t(blockIdx.x) * (kMPThreads / 32) + warp;
     Row8 acc;  // per-lane minima of the current chunk
-    const bool ok = stage::stage_pipeline(
-        a.tasks, a.in_src, uint64_t(blockIdx.x) * (kMPThreads / 32) + warp, nwarps, a.num_tasks, ws,
-        lane, [&](uint4 d, uint64_t, uint32_t j, uint32_t nu, uint32_t *slot, uint64_t a0) {
+    auto task = [&](uint4 d, uint64_t, uint32_t j, uint32_t nu, const uint32_t *slot, uint64_t a0) {
             if (task_is_chunk(d)) {
                 const stage::Unit u = stage::unit_of(d, j);
                 if (j == 0)
@@ -383,7 +385,12 @@ __global__ void __launch_bounds__(kMPThreads, 1) ms_pull_kernel(const MSArgs *__
                 const uint32_t vals[1] = {rr};
                 ssc::warp_append<1>(w.qnext, w.qnext_size, vals, joined ? 1u : 0u, lane);
             }
-        });
+        };
+    bool ok = true;
+    if constexpr (kStaged)
+        ok = stage::stage_pipeline(a.tasks, a.in_src, first, nwarps, a.num_tasks, ws, lane, task);
+    else
+        stage::direct_tasks(a.tasks, a.in_src, first, nwarps, a.num_tasks, task);
     if (!ok) {
         atomicExch(&a.hdr->error, 1u);
         atomicExch(&a.hdr->done, 1u);
@@ -466,8 +473,10 @@ void ms_solve(GraphImpl &g, const uint32_t *sources, uint32_t k, uint32_t max_ro
     a.inf = (WK == HYT_WEIGHTS_F32) ? 0x7F800000u : HYT_DIST_INF_U32;
     a.num_edges = g.E;
     for (uint32_t l = 0; l < k; ++l) a.sources[l] = graph_vertex(g, sources[l], s);
+    // staged pull when the graph's tiles fit a staging slot, else ids read in place
+    const bool staged = g.tile_cost <= kStageTileMax && stage::staged_shared_bytes(g.num_hot) <= kPRSmemMax;
     const bool pull_ok = (g.flags & HYT_GRAPH_PULL) && (WK == HYT_WEIGHTS_NONE || g.in_weights.get()) && g.E > 0 &&
-                         g.pull_tasks.get() && stage::staged_shared_bytes(g.num_hot) <= kPRSmemMax;
+                         g.pull_tasks.get() && size_t(g.num_hot) * 4 <= kPRSmemMax;
     a.pull_div = pull_ok ? 4u : 0u;
     if (pull_ok) {
         a.in_off = g.in_offsets.get();
@@ -479,10 +488,15 @@ void ms_solve(GraphImpl &g, const uint32_t *sources, uint32_t k, uint32_t max_ro
         a.num_tasks = g.num_chunks + g.num_tiles;
         a.num_hot = g.num_hot;
     }
-    const unsigned pull_smem = static_cast<unsigned>(stage::staged_shared_bytes(g.num_hot));
+    const unsigned pull_smem =
+        static_cast<unsigned>(staged ? stage::staged_shared_bytes(g.num_hot) : size_t(g.num_hot) * 4);
+    const void *pull_fn = staged ? reinterpret_cast<const void *>(ms_pull_kernel<WK, true>)
+                                 : reinterpret_cast<const void *>(ms_pull_kernel<WK, false>);
     static bool attr = false;
     if (!attr) {
-        HYT_CUDA(cudaFuncSetAttribute(ms_pull_kernel<WK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        HYT_CUDA(cudaFuncSetAttribute(ms_pull_kernel<WK, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(kPRSmemMax)));
+        HYT_CUDA(cudaFuncSetAttribute(ms_pull_kernel<WK, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       static_cast<int>(kPRSmemMax)));
         attr = true;
     }
@@ -531,7 +545,7 @@ void ms_solve(GraphImpl &g, const uint32_t *sources, uint32_t k, uint32_t max_ro
         if (a.pull_div) add(reinterpret_cast<void *>(ms_frontier_edges_kernel), dim3(grid), dim3(kMSThreads), 0);
         add(reinterpret_cast<void *>(ms_expand_kernel<WK>), dim3(grid), dim3(kMSThreads), 0);
         add(reinterpret_cast<void *>(ms_hub_kernel<WK>), dim3(grid), dim3(kMSThreads), 0);
-        if (a.pull_div) add(reinterpret_cast<void *>(ms_pull_kernel<WK>), dim3(pgrid), dim3(kMPThreads), pull_smem);
+        if (a.pull_div) add(pull_fn, dim3(pgrid), dim3(kMPThreads), pull_smem);
         add(reinterpret_cast<void *>(ms_round_end_kernel), dim3(1), dim3(1), 0);
         HYT_CUDA(cudaGraphInstantiate(&exec, graph, 0));
         HYT_CUDA(cudaGraphLaunch(exec, s));
@@ -540,7 +554,10 @@ void ms_solve(GraphImpl &g, const uint32_t *sources, uint32_t k, uint32_t max_ro
             if (a.pull_div) ms_frontier_edges_kernel<<<grid, kMSThreads, 0, s>>>(d_args);
             ms_expand_kernel<WK><<<grid, kMSThreads, 0, s>>>(d_args);
             ms_hub_kernel<WK><<<grid, kMSThreads, 0, s>>>(d_args);
-            if (a.pull_div) ms_pull_kernel<WK><<<pgrid, kMPThreads, pull_smem, s>>>(d_args);
+            if (a.pull_div) {
+                void *pargs[] = {&d_args};
+                HYT_CUDA(cudaLaunchKernel(pull_fn, dim3(pgrid), dim3(kMPThreads), pargs, pull_smem, s));
+            }
             ms_round_end_kernel<<<1, 1, 0, s>>>(d_args);
             HYT_CUDA(cudaGetLastError());
             launches += a.pull_div ? 5 : 3;

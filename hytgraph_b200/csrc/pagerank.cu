@@ -364,14 +364,11 @@ int pr_staged_grid() {
     return grid;
 }
 
-// HYT_STAGED=0 selects the register-path kernel for in-HBM solves too
-// (same tasks, same sums; for comparisons).
+// In-HBM solves use the staged kernel when it was asked for (HYT_STAGED=1)
+// and the graph's tiles fit a staging slot.
 bool pr_use_staged(const GraphImpl &g) {
-    static const bool env_off = [] {
-        const char *e = std::getenv("HYT_STAGED");
-        return e && e[0] == '0';
-    }();
-    return !env_off && g.pull_tasks.get() && staged_shared_bytes(g.num_hot) <= kPRSmemMax;
+    return stage::staged_requested() && g.tile_cost <= kStageTileMax && g.pull_tasks.get() &&
+           staged_shared_bytes(g.num_hot) <= kPRSmemMax;
 }
 
 }  // namespace

@@ -382,7 +382,8 @@ void ppr_multi(GraphImpl &g, const uint32_t *sources, uint32_t k, float restart,
     p.active = (1u << k) - 1u;
     p.d = 1.0 - double(restart);
     // staged task pass when the graph carries task descriptors (in HBM)
-    const bool staged = g.pull_tasks.get() && stage::staged_shared_bytes(g.num_hot) + 4096 <= kPRSmemMax;
+    const bool staged = g.pull_tasks.get() && g.tile_cost <= kStageTileMax &&
+                        stage::staged_shared_bytes(g.num_hot) + 4096 <= kPRSmemMax;
     const unsigned smem = static_cast<unsigned>(stage::staged_shared_bytes(g.num_hot));
     if (staged) {
         // the kernel's static shared memory counts against the same

@@ -542,14 +542,11 @@ int pull_grid(bool staged, unsigned smem) {
     return sm_count() * std::max(per_sm, 1);
 }
 
-// HYT_STAGED=0 selects the register-path pull sweep (same sweep; for
-// comparisons).
+// Staged pull sweeps when asked for (HYT_STAGED=1) and the graph's tiles
+// fit a staging slot.
 bool pull_use_staged(const GraphImpl &g) {
-    static const bool env_off = [] {
-        const char *e = std::getenv("HYT_STAGED");
-        return e && e[0] == '0';
-    }();
-    return !env_off && g.pull_tasks.get() && stage::staged_shared_bytes(g.num_hot) <= kPRSmemMax;
+    return stage::staged_requested() && g.tile_cost <= kStageTileMax && g.pull_tasks.get() &&
+           stage::staged_shared_bytes(g.num_hot) <= kPRSmemMax;
 }
 
 template <int WK>

@@ -8,9 +8,18 @@
 // dependent gathers instead.
 //
 // Sources are this GPU's own memory only (no multicast).
+//
+// The staged kernels are opt-in (HYT_STAGED=1, which also selects
+// kStageTileMax-unit tiles so that a tile fits one slot).  On R-MAT graphs
+// the register-path kernels with 512-unit tiles ran faster: the pull
+// kernels are bound by instruction issue over the dependent gathers, not by
+// the id stream, and half-size tiles leave half of each unit's gather
+// slots and row lanes idle.
 #pragma once
 
 #include <cuda_runtime.h>
+
+#include <cstdlib>
 
 #include <cstdint>
 
@@ -33,7 +42,7 @@ constexpr int kStageThreads = kStageWarps * 32;
 static_assert(kStageSlots >= 2, "at least double buffering");
 // A tile's edges: the rows starting inside a tile span < tile_cost merge
 // units, and its last short row adds < tile_cost more, so < 2 * tile_cost.
-static_assert(2 * kTileCostMax - 1 + 6 <= kSlotWords, "a tile's edges must fit one staging slot");
+static_assert(2 * kStageTileMax - 1 + 6 <= kSlotWords, "a tile's edges must fit one staging slot");
 static_assert(kLongChunk % kUnitEdges == 0, "chunks split into whole units");
 
 // The unit a slot holds (written by lane 0 when its copy is issued).
@@ -52,6 +61,15 @@ constexpr size_t kStageHead = ((kStageBars + kStageMeta + 127) / 128) * 128;
 constexpr size_t kStageBytes = kStageHead + size_t(kStageWarps) * kStageSlots * kSlotWords * 4;
 
 inline size_t staged_shared_bytes(uint32_t num_hot) { return kStageBytes + size_t(num_hot) * 4; }
+
+// HYT_STAGED=1: in-HBM PageRank and SSSP pull sweeps use the staged kernels.
+inline bool staged_requested() {
+    static const bool on = [] {
+        const char *e = std::getenv("HYT_STAGED");
+        return e && e[0] == '1';
+    }();
+    return on;
+}
 
 #ifdef __CUDACC__
 
@@ -161,6 +179,19 @@ __device__ __forceinline__ bool stage_pipeline(const uint4 *tasks, const uint32_
         }
     }
     return true;
+}
+
+// The same walk without staging, for graphs whose tiles exceed a slot:
+// consume(d, task, j, units, in_src, 0) for every unit of every task, the
+// consumer reading ids from global memory in place.
+template <class Consume>
+__device__ __forceinline__ void direct_tasks(const uint4 *tasks, const uint32_t *in_src, uint64_t first,
+                                             uint64_t stride, uint64_t total, Consume &&consume) {
+    for (uint64_t t = first; t < total; t += stride) {
+        const uint4 d = tasks[t];
+        const uint32_t nu = units_of(d);
+        for (uint32_t j = 0; j < nu; ++j) consume(d, t, j, nu, in_src, uint64_t(0));
+    }
 }
 
 #endif  // __CUDACC__

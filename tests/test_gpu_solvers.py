@@ -96,9 +96,10 @@ sys.stdout.buffer.write(np.array([st["iterations"], sp["iterations"]], np.uint32
 
 def test_pagerank_bit_identical_across_runs_grids_and_kernels(hyt, gpu):
     """PageRank and personalized PageRank give the same bits and iteration
-    counts on every run, under other persistent grid sizes, and with the
-    register-path kernel instead of the bulk-staged one: row sums and the
-    FP64 residual / dangling sums have fixed association orders."""
+    counts on every run and under other persistent grid sizes; on the same
+    tiling the bulk-staged kernel gives the register-path kernel's bits: row
+    sums and the FP64 residual / dangling sums have fixed association
+    orders."""
     import os
     import subprocess
     import sys
@@ -117,11 +118,18 @@ def test_pagerank_bit_identical_across_runs_grids_and_kernels(hyt, gpu):
         assert np.array_equal(p.view(np.uint32), ppr[0][0].view(np.uint32))
     want = (np.array([runs[0][1]["iterations"], ppr[0][1]["iterations"]], np.uint32).tobytes() +
             runs[0][0].tobytes() + ppr[0][0].tobytes())
-    for env in ({"HYT_PR_GRID": "37"}, {"HYT_PR_GRID": "300"}, {"HYT_STAGED": "0"}):
+    def ranks(env):
         out = subprocess.run([sys.executable, "-c", _RANKS_SCRIPT % str(ROOT)], capture_output=True,
                              env=dict(os.environ, **env), timeout=600)
         assert out.returncode == 0, out.stderr.decode()[-2000:]
-        assert out.stdout == want, env
+        return out.stdout
+
+    for env in ({"HYT_PR_GRID": "37"}, {"HYT_PR_GRID": "300"}):
+        assert ranks(env) == want, env
+    # 256-unit tiles: staged kernel (HYT_STAGED=1 selects them) vs register path
+    staged = ranks({"HYT_STAGED": "1"})
+    assert staged == ranks({"HYT_STAGED": "0", "HYT_PR_TILE": "256"})
+    assert staged == ranks({"HYT_STAGED": "1", "HYT_PR_GRID": "37"})
 
 
 def test_sssp_staged_and_register_sweeps_agree(hyt, gpu):

@@ -54,3 +54,27 @@ def test_sssp_multi_duplicates_device_output_and_errors(hyt, gpu):
             with pytest.raises(hyt.HytError) as e:
                 dg.sssp_multi(bad)
             assert e.value.code == hyt.capi.HYT_E_INVALID
+
+
+def test_sssp_multi_staged_pull_matches(hyt, gpu):
+    """With HYT_STAGED=1 (256-unit tiles) the pull sweeps stage ids by bulk
+    copies instead of reading them in place; the labels are the same fixed
+    point, equal to the default build's for all 8 lanes."""
+    import os
+    import subprocess
+    import sys
+
+    from conftest import ROOT
+
+    code = ("import sys; sys.path.insert(0, %r); import hytgraph_b200 as hyt; "
+            "g = hyt.rmat(20, 16, 5); src = [int(s) for s in hyt.pick_sources(g.row_offsets, 99, 8)]; "
+            "dg = hyt.Graph(g, flags=hyt.capi.HYT_GRAPH_ALL | hyt.capi.HYT_GRAPH_HUB_ORDER); "
+            "d, st = dg.sssp_multi(src); assert st['edges_processed'] >= g.num_edges, st; "
+            "sys.stdout.buffer.write(d.tobytes())") % str(ROOT)
+    outs = []
+    for staged in ("1", "0"):
+        r = subprocess.run([sys.executable, "-c", code], capture_output=True,
+                           env=dict(os.environ, HYT_STAGED=staged), timeout=600)
+        assert r.returncode == 0, r.stderr.decode()[-2000:]
+        outs.append(r.stdout)
+    assert outs[0] == outs[1] and len(outs[0]) > 0
