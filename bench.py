@@ -1667,10 +1667,9 @@ def main():
     # pure kernel time of one PageRank iteration (per-launch events), same inputs
     _, prof = graph.pagerank(out=ranks_out, stream=sptr, flags=capi.HYT_RUN_PROFILE)
     kern_ms = prof["kernel_ms"] / max(prof["kernel_launches"], 1)
-    pr_name = "pr_staged_kernel+pr_reduce_kernel" if os.environ.get("HYT_STAGED", "1") != "0" else \
-        "pr_iterate_kernel+pr_reduce_kernel"
-    ss_name = ("sssp_pull_staged_kernel" if os.environ.get("HYT_STAGED", "1") != "0" else "sssp_pull_kernel") + \
-        "+sssp_expand_kernel+sssp_hub_kernel"
+    staged = os.environ.get("HYT_STAGED") == "1"  # bulk-staged kernels are opt-in
+    pr_name = "pr_staged_kernel+pr_reduce_kernel" if staged else "pr_iterate_kernel+pr_reduce_kernel"
+    ss_name = ("sssp_pull_staged_kernel" if staged else "sssp_pull_kernel") + "+sssp_expand_kernel+sssp_hub_kernel"
     dominant = pr_name if pr_ms >= ss_ms else ss_name
     if dominant == pr_name:
         roof = {"kernel": dominant, "bound": "hbm", "achieved": pr_gbs, "peak": peak_gbs, "unit": "GB/s",

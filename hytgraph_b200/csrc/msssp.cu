@@ -296,19 +296,43 @@ __device__ __forceinline__ bool pull_lower(const MSArgs &a, const View &w, uint3
     return improved && atomicExch(a.stamp + r, w.next_stamp) != w.next_stamp;
 }
 
-// Per-lane minimum of d[u] + w over in-edges [lo, hi) into m (ids staged
-// at slot[x - a0]); each thread of the caller walks its own edges.
+// Per-lane minimum of d[u] + w over in-edges [lo, hi) into m (ids at
+// slot[x - a0]: staged, or the CSC itself); each thread of the caller walks
+// its own edges lo, lo + step, ..., kPullU of them loaded before any is
+// relaxed so that their label-row gathers overlap.  Labels are read live
+// (not snapshotted): rows lowered earlier in the same sweep -- the hub rows,
+// whose chunks come first -- feed the rows after them.
+constexpr int kPullU = 4;
+
 template <int WK>
 __device__ __forceinline__ void pull_edges(const MSArgs &a, const uint32_t *s_hot, const uint32_t *slot, uint64_t a0,
                                            uint64_t lo, uint64_t hi, uint64_t step, uint64_t pol, Row8 &m) {
-    for (uint64_t x = lo; x < hi; x += step) {
-        uint32_t u = slot[x - a0];
-        if (u & kHotTag) u = s_hot[u & ~kHotTag];
-        const uint32_t wt = ssc::edge_weight<WK>(a.in_w, x);
-        const Row8 du = load_row_keep(a.dist, u, pol);
+    for (uint64_t x0 = lo; x0 < hi; x0 += step * kPullU) {
+        uint32_t u[kPullU], wt[kPullU];
 #pragma unroll
-        for (int l = 0; l < kML; ++l)
-            if (du.d[l] != a.inf) m.d[l] = min(m.d[l], extend<WK>(du.d[l], wt));
+        for (int j = 0; j < kPullU; ++j) {
+            const uint64_t x = x0 + j * step;
+            u[j] = x < hi ? slot[x - a0] : 0u;
+            wt[j] = x < hi ? ssc::edge_weight<WK>(a.in_w, x) : 0u;
+        }
+#pragma unroll
+        for (int j = 0; j < kPullU; ++j)
+            if (u[j] & kHotTag) u[j] = s_hot[u[j] & ~kHotTag];
+        Row8 du[kPullU];
+#pragma unroll
+        for (int j = 0; j < kPullU; ++j) {
+            if (x0 + j * step < hi) {
+                du[j] = load_row_keep(a.dist, u[j], pol);
+            } else {
+#pragma unroll
+                for (int l = 0; l < kML; ++l) du[j].d[l] = a.inf;
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kPullU; ++j)
+#pragma unroll
+            for (int l = 0; l < kML; ++l)
+                if (du[j].d[l] != a.inf) m.d[l] = min(m.d[l], extend<WK>(du[j].d[l], wt[j]));
     }
 }
 

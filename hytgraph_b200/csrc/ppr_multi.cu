@@ -106,7 +106,11 @@ __device__ __forceinline__ float lane_next(uint64_t v, int lane, double sum, con
                                            float cur) {
     if (!((p.active >> lane) & 1u)) return cur;
     double nx = p.d * sum;
-    if (v == p.source[lane]) nx += (1.0 - p.d) + p.d * s_dm[lane];
+    uint32_t src = 0xFFFFFFFFu;  // p.source[lane] without a local-memory copy of p
+#pragma unroll
+    for (int l = 0; l < kLanes; ++l)
+        if (l == lane) src = p.source[l];
+    if (v == src) nx += (1.0 - p.d) + p.d * s_dm[lane];
     return float(nx);
 }
 
