@@ -120,40 +120,61 @@ constexpr int kBatch = HYT_PR_BATCH;
 
 // kSmemHot: hot sources (tagged ids) read their contribution from the
 // CTA's shared-memory copy s_hot; otherwise from ccur[hot_vertex[slot]].
+// One pass of kK = 4 * kG batches (edges src[base + 32k + lane], k < kK).
+template <int kK, bool kSmemHot, class Sink>
+__device__ __forceinline__ void gather_pass(const uint32_t *src, uint32_t base, uint32_t n, const float *ccur,
+                                            const float *s_hot, const uint32_t *hot_vertex, uint64_t pol, int lane,
+                                            Sink &sink) {
+    uint32_t id[kK];
+#pragma unroll
+    for (int k = 0; k < kK; ++k) {
+        const uint32_t i = base + 32 * k + lane;
+        id[k] = (i < n) ? dev::ld_stream(src + i) : 0u;
+    }
+    float v[kK];
+#pragma unroll
+    for (int k = 0; k < kK; ++k) {
+        v[k] = 0.0f;
+        if (!(id[k] & kHotTag)) v[k] = dev::ld_keep(ccur + id[k], pol);
+    }
+#pragma unroll
+    for (int k = 0; k < kK; ++k) {
+        if (id[k] & kHotTag) {
+            if constexpr (kSmemHot) {
+                v[k] = s_hot[id[k] & ~kHotTag];
+            } else {
+                v[k] = ccur[hot_vertex[id[k] & ~kHotTag]];
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < kK; ++k) {
+        const uint32_t i = base + 32 * k + lane;
+        if (i < n) sink(i, v[k]);
+    }
+}
+
+// A pass over the last, partial batch group issues only the 4-batch groups
+// that hold edges (a warp-uniform choice), so short tiles do not pay for
+// kBatch gather slots; the edges and their order are the same.
 template <bool kSmemHot, class Sink>
 __device__ __forceinline__ void gather_span(const uint32_t *in_src, const float *ccur, const float *s_hot,
                                             const uint32_t *hot_vertex, uint64_t lo, uint64_t hi, uint64_t pol,
                                             int lane, Sink &&sink) {
+    static_assert(kBatch % 4 == 0 && kBatch >= 4, "batches come in groups of 4");
     const uint32_t n = static_cast<uint32_t>(hi - lo);
     const uint32_t *src = in_src + lo;
     for (uint32_t base = 0; base < n; base += 32 * kBatch) {
-        uint32_t id[kBatch];
-#pragma unroll
-        for (int k = 0; k < kBatch; ++k) {
-            const uint32_t i = base + 32 * k + lane;
-            id[k] = (i < n) ? dev::ld_stream(src + i) : 0u;
-        }
-        float v[kBatch];
-#pragma unroll
-        for (int k = 0; k < kBatch; ++k) {
-            v[k] = 0.0f;
-            if (!(id[k] & kHotTag)) v[k] = dev::ld_keep(ccur + id[k], pol);
-        }
-#pragma unroll
-        for (int k = 0; k < kBatch; ++k) {
-            if (id[k] & kHotTag) {
-                if constexpr (kSmemHot) {
-                    v[k] = s_hot[id[k] & ~kHotTag];
-                } else {
-                    v[k] = ccur[hot_vertex[id[k] & ~kHotTag]];
-                }
-            }
-        }
-#pragma unroll
-        for (int k = 0; k < kBatch; ++k) {
-            const uint32_t i = base + 32 * k + lane;
-            if (i < n) sink(i, v[k]);
-        }
+        const uint32_t groups = (n - base + 127) / 128;  // 4-batch groups holding edges
+        if (groups >= kBatch / 4)
+            gather_pass<kBatch, kSmemHot>(src, base, n, ccur, s_hot, hot_vertex, pol, lane, sink);
+        else if (groups == 1)
+            gather_pass<4, kSmemHot>(src, base, n, ccur, s_hot, hot_vertex, pol, lane, sink);
+        else if (groups == 2)
+            gather_pass<8, kSmemHot>(src, base, n, ccur, s_hot, hot_vertex, pol, lane, sink);
+        else
+            gather_pass<(kBatch >= 12 ? 12 : kBatch), kSmemHot>(src, base, n, ccur, s_hot, hot_vertex, pol, lane,
+                                                                sink);
     }
 }
 
@@ -289,7 +310,8 @@ __device__ __forceinline__ void tile_task(const PRArgs &a, const PRState &ps, co
         const uint64_t hi = active ? a.in_off[r + 1] : 0;
         if (active && hi - lo < kWarpRowDegree) {
             dev::CSum acc;
-            for (uint64_t x = lo; x < hi; ++x) acc.add(sv[x - e0]);
+            const uint32_t xe = static_cast<uint32_t>(hi - e0);
+            for (uint32_t x = static_cast<uint32_t>(lo - e0); x < xe; ++x) acc.add(sv[x]);
             finalize_row(a, ps, r, acc.value(), b.cur, b.nxt, b.cnxt, res, dang);
         }
         uint32_t big = __ballot_sync(0xffffffffu, active && (hi - lo >= kWarpRowDegree));

@@ -163,28 +163,46 @@ __device__ __forceinline__ bool pull_relax(const SSArgs &a, const RoundView &rv,
 #endif
 constexpr int kPullBatch = HYT_PULL_BATCH;
 
+// One pass of kK batches (edges lo + base + 32k + lane, k < kK).
+template <int kK, int WK, class Sink>
+__device__ __forceinline__ void pull_pass(const SSArgs &a, const PullGraph &pg, const uint32_t *s_hot, uint64_t lo,
+                                          uint32_t base, uint32_t n, uint64_t pol, int lane, Sink &sink) {
+    uint32_t id[kK], w[kK], du[kK];
+#pragma unroll
+    for (int k = 0; k < kK; ++k) {
+        const uint32_t i = base + 32 * k + lane;
+        id[k] = (i < n) ? dev::ld_stream(pg.in_src + lo + i) : 0u;
+        w[k] = (i < n) ? edge_weight<WK>(pg.in_w, lo + i) : 0u;
+    }
+#pragma unroll
+    for (int k = 0; k < kK; ++k)
+        if (id[k] & kHotTag) id[k] = s_hot[id[k] & ~kHotTag];  // hot slot -> vertex id
+#pragma unroll
+    for (int k = 0; k < kK; ++k) du[k] = dev::ld_keep_u32(a.dist + id[k], pol);
+#pragma unroll
+    for (int k = 0; k < kK; ++k) {
+        const uint32_t i = base + 32 * k + lane;
+        if (i < n) sink(i, du[k] == a.inf ? a.inf : extend<WK>(du[k], w[k]));
+    }
+}
+
+// The last, partial pass issues only the 4-batch groups that hold edges
+// (a warp-uniform choice); the edges and their order are the same.
 template <int WK, class Sink>
 __device__ __forceinline__ void pull_span(const SSArgs &a, const PullGraph &pg, const uint32_t *s_hot, uint64_t lo,
                                           uint64_t hi, uint64_t pol, int lane, Sink &&sink) {
+    static_assert(kPullBatch % 4 == 0 && kPullBatch >= 4, "batches come in groups of 4");
     const uint32_t n = static_cast<uint32_t>(hi - lo);
     for (uint32_t base = 0; base < n; base += 32 * kPullBatch) {
-        uint32_t id[kPullBatch], w[kPullBatch], du[kPullBatch];
-#pragma unroll
-        for (int k = 0; k < kPullBatch; ++k) {
-            const uint32_t i = base + 32 * k + lane;
-            id[k] = (i < n) ? dev::ld_stream(pg.in_src + lo + i) : 0u;
-            w[k] = (i < n) ? edge_weight<WK>(pg.in_w, lo + i) : 0u;
-        }
-#pragma unroll
-        for (int k = 0; k < kPullBatch; ++k)
-            if (id[k] & kHotTag) id[k] = s_hot[id[k] & ~kHotTag];  // hot slot -> vertex id
-#pragma unroll
-        for (int k = 0; k < kPullBatch; ++k) du[k] = dev::ld_keep_u32(a.dist + id[k], pol);
-#pragma unroll
-        for (int k = 0; k < kPullBatch; ++k) {
-            const uint32_t i = base + 32 * k + lane;
-            if (i < n) sink(i, du[k] == a.inf ? a.inf : extend<WK>(du[k], w[k]));
-        }
+        const uint32_t groups = (n - base + 127) / 128;
+        if (groups >= kPullBatch / 4)
+            pull_pass<kPullBatch, WK>(a, pg, s_hot, lo, base, n, pol, lane, sink);
+        else if (groups == 1)
+            pull_pass<4, WK>(a, pg, s_hot, lo, base, n, pol, lane, sink);
+        else if (groups == 2)
+            pull_pass<8, WK>(a, pg, s_hot, lo, base, n, pol, lane, sink);
+        else
+            pull_pass<(kPullBatch >= 12 ? 12 : kPullBatch), WK>(a, pg, s_hot, lo, base, n, pol, lane, sink);
     }
 }
 
@@ -237,7 +255,8 @@ __global__ void __launch_bounds__(kPullThreads, 1) sssp_pull_kernel(const SSArgs
                 bool joined = false;
                 if (active && hi - lo < 64) {
                     uint32_t best = a.inf;
-                    for (uint64_t x = lo; x < hi; ++x) best = min(best, sv[x - e0]);
+                    const uint32_t xe = static_cast<uint32_t>(hi - e0);
+                    for (uint32_t x = static_cast<uint32_t>(lo - e0); x < xe; ++x) best = min(best, sv[x]);
                     joined = pull_relax(a, rv, r, best);
                 }
                 uint32_t big = __ballot_sync(0xffffffffu, active && (hi - lo >= 64));
