@@ -114,33 +114,76 @@ __device__ __forceinline__ float lane_next(uint64_t v, int lane, double sum, con
     return float(nx);
 }
 
-// One warp per short row: next values and per-block residual partials.
-__global__ void ppr8_rows_kernel(const uint64_t *__restrict__ in_off, const uint32_t *__restrict__ in_src,
-                                 const uint32_t *__restrict__ hot_vertex, const float *__restrict__ c,
-                                 const float *__restrict__ x, uint64_t V, uint64_t long_from, LaneParams p,
-                                 const double *__restrict__ dpart, float *__restrict__ nxt, double *__restrict__ rpart) {
+// Short rows, 4 per warp: thread t takes row v0 + t / 8 and lane t % 8, and
+// sums that row's in-edges for its lane in edge order (4 edges loaded
+// before any is added; the 8 threads of a row read the same id and one
+// 32-byte contribution sector per edge).  Rows of kWideRow or more in-edges
+// (below the long-row threshold) are summed by the whole warp in the 4-slot
+// layout of row_lane_sum.  Every thread then writes its (row, lane) value;
+// per-block residual partials per lane in a fixed order.
+constexpr uint32_t kWideRow = 32;
+constexpr int kRowThreads = 256;
+
+__global__ void __launch_bounds__(kRowThreads) ppr8_rows_kernel(
+    const uint64_t *__restrict__ in_off, const uint32_t *__restrict__ in_src, const uint32_t *__restrict__ hot_vertex,
+    const float *__restrict__ c, const float *__restrict__ x, uint64_t V, uint64_t long_from, LaneParams p,
+    const double *__restrict__ dpart, float *__restrict__ nxt, double *__restrict__ rpart) {
     __shared__ double s_dm[kLanes];
-    __shared__ double s_res[kLanes][8];
+    __shared__ double s_res[kLanes][kRowThreads / 32];
     lane_dangling(dpart, s_dm);
-    const int t = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint64_t warps = uint64_t(gridDim.x) * (blockDim.x >> 5);
-    double res = 0.0;  // lane t (t < 8)
-    for (uint64_t v = (blockIdx.x * uint64_t(blockDim.x) + threadIdx.x) >> 5; v < V; v += warps) {
-        const uint64_t b = in_off[v], e = in_off[v + 1];
-        if (e - b >= long_from) continue;  // summed by the chunk kernels
-        const double sum = row_lane_sum(in_src, hot_vertex, c, b, e, t);
-        if (t < kLanes) {
-            const float cur = x[v * kLanes + t];
-            const float nx = lane_next(v, t, sum, p, s_dm, cur);
-            nxt[v * kLanes + t] = nx;
+    const int t = threadIdx.x & 31, warp = threadIdx.x >> 5, q = t >> 3, lane = t & 7;
+    const uint64_t warps = uint64_t(gridDim.x) * (kRowThreads / 32);
+    double res = 0.0;  // this thread's lane
+    for (uint64_t v0 = ((blockIdx.x * uint64_t(kRowThreads) + threadIdx.x) >> 5) * 4; v0 < V; v0 += warps * 4) {
+        const uint64_t v = v0 + q;
+        uint64_t b = 0, e = 0;
+        if (v < V) {
+            b = in_off[v];
+            e = in_off[v + 1];
+        }
+        const uint64_t deg = e - b;
+        const bool mine = v < V && deg < long_from;  // long rows: the chunk kernels
+        double acc = 0.0;
+        if (mine && deg < kWideRow) {
+            for (uint64_t i0 = b; i0 < e; i0 += 4) {
+                uint32_t u[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) u[j] = (i0 + j < e) ? __ldcs(in_src + i0 + j) : 0u;
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    if (u[j] & kHotTag) u[j] = hot_vertex[u[j] & ~kHotTag];
+                float cv[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) cv[j] = (i0 + j < e) ? c[uint64_t(u[j]) * kLanes + lane] : 0.0f;
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    if (i0 + j < e) acc += double(cv[j]);
+            }
+        }
+        // wide rows of the group, one at a time by the whole warp
+        uint32_t wide = __ballot_sync(0xffffffffu, mine && deg >= kWideRow && lane == 0);
+        while (wide) {
+            const int src = __ffs(wide) - 1;
+            wide &= wide - 1;
+            const uint64_t bb = __shfl_sync(0xffffffffu, b, src), ee = __shfl_sync(0xffffffffu, e, src);
+            const double sum = row_lane_sum(in_src, hot_vertex, c, bb, ee, t);  // lane t % 8, in every thread
+            if (q == (src >> 3)) acc = sum;
+        }
+        if (mine) {
+            const float cur = x[v * kLanes + lane];
+            const float nx = lane_next(v, lane, acc, p, s_dm, cur);
+            nxt[v * kLanes + lane] = nx;
             res += fabs(double(nx) - double(cur));
         }
     }
+    // fixed-order residual partials: the 4 row slots of the warp, then warps
+    res += __shfl_xor_sync(0xffffffffu, res, 8);
+    res += __shfl_xor_sync(0xffffffffu, res, 16);
     if (t < kLanes) s_res[t][warp] = res;
     __syncthreads();
     if (threadIdx.x < kLanes) {
         double a = 0.0;
-        for (int w = 0; w < 8; ++w) a += s_res[threadIdx.x][w];
+        for (int w = 0; w < kRowThreads / 32; ++w) a += s_res[threadIdx.x][w];
         rpart[blockIdx.x * kLanes + threadIdx.x] = a;
     }
 }
@@ -399,7 +442,13 @@ void ppr_multi(GraphImpl &g, const uint32_t *sources, uint32_t k, float restart,
             attr = smem;
         }
     }
-    const unsigned rows_grid = staged ? grid_sm(1) : grid_sm(8);
+    // one persistent wave of the rows pass (its partials are summed in block order)
+    static int rows_per_sm = 0;
+    if (!staged && rows_per_sm == 0) {
+        HYT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rows_per_sm, ppr8_rows_kernel, kRowThreads, 0));
+        rows_per_sm = std::max(rows_per_sm, 1);
+    }
+    const unsigned rows_grid = staged ? grid_sm(1) : grid_sm(rows_per_sm);
     const uint64_t chunks = g.num_long ? g.num_chunks : 0;
     const uint64_t long_from = g.num_long ? g.tile_cost : ~uint64_t(0);
     const unsigned long_grid = g.num_long ? grid_for(g.num_long * 32, 256) : 0;
@@ -432,8 +481,9 @@ void ppr_multi(GraphImpl &g, const uint32_t *sources, uint32_t k, float restart,
                 ++launches;
             }
         } else {
-            ppr8_rows_kernel<<<rows_grid, 256, 0, s>>>(g.in_offsets.get(), g.in_sources.get(), g.hot_vertex.get(),
-                                                       c.get(), x, V, long_from, p, dpart.get(), nx, rpart.get());
+            ppr8_rows_kernel<<<rows_grid, kRowThreads, 0, s>>>(g.in_offsets.get(), g.in_sources.get(),
+                                                               g.hot_vertex.get(), c.get(), x, V, long_from, p,
+                                                               dpart.get(), nx, rpart.get());
         }
         if (chunks && !staged) {
             ppr8_chunks_kernel<<<grid_sm(8), 256, 0, s>>>(g.in_offsets.get(), g.in_sources.get(), g.hot_vertex.get(),
