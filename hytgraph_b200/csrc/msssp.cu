@@ -284,8 +284,30 @@ __global__ void __launch_bounds__(kMSThreads) ms_hub_kernel(const MSArgs *__rest
     }
 }
 
+// Tile row r: lowers its labels to m where that improves them, with plain
+// stores -- a tile row has exactly one writer during a sweep (the warp that
+// owns its tile) and no push runs beside a sweep; true when r joins the
+// next frontier.
+__device__ __forceinline__ bool pull_store_row(const MSArgs &a, const View &w, uint32_t r, const Row8 &m) {
+    const Row8 cur = load_row(a.dist, r);
+    Row8 nx;
+    bool improved = false;
+#pragma unroll
+    for (int l = 0; l < kML; ++l) {
+        const bool lower = l < static_cast<int>(a.k) && m.d[l] < cur.d[l];
+        nx.d[l] = lower ? m.d[l] : cur.d[l];
+        improved |= lower;
+    }
+    if (!improved) return false;
+    uint4 *p = reinterpret_cast<uint4 *>(a.dist + size_t(r) * kML);
+    p[0] = make_uint4(nx.d[0], nx.d[1], nx.d[2], nx.d[3]);
+    p[1] = make_uint4(nx.d[4], nx.d[5], nx.d[6], nx.d[7]);
+    a.stamp[r] = w.next_stamp;
+    return true;
+}
+
 // Lowers row r's labels to m (lanes that improve); true when r joins the
-// next frontier now.
+// next frontier now.  Long rows: every chunk of the row may lower it.
 __device__ __forceinline__ bool pull_lower(const MSArgs &a, const View &w, uint32_t r, const Row8 &m) {
     const Row8 cur = load_row(a.dist, r);
     bool improved = false;
@@ -386,7 +408,7 @@ __global__ void __launch_bounds__(kMPThreads, 1) ms_pull_kernel(const MSArgs *__
 #pragma unroll
                     for (int l = 0; l < kML; ++l) m.d[l] = a.inf;
                     pull_edges<WK>(a, s_hot, slot, a0, lo, hi, 1, pol, m);
-                    joined = pull_lower(a, w, rr, m);
+                    joined = pull_store_row(a, w, rr, m);
                 }
                 uint32_t big = __ballot_sync(0xffffffffu, active && (hi - lo >= 64));
                 while (big) {
@@ -403,7 +425,7 @@ __global__ void __launch_bounds__(kMPThreads, 1) ms_pull_kernel(const MSArgs *__
 #pragma unroll
                         for (int o = 16; o > 0; o >>= 1)
                             m.d[l] = min(m.d[l], __shfl_xor_sync(0xffffffffu, m.d[l], o));
-                    const bool jn = (lane == 0) && pull_lower(a, w, rb + src, m);
+                    const bool jn = (lane == 0) && pull_store_row(a, w, rb + src, m);
                     if (__shfl_sync(0xffffffffu, jn ? 1u : 0u, 0) && lane == src) joined = true;
                 }
                 const uint32_t vals[1] = {rr};

@@ -89,6 +89,23 @@ struct PRState {
     bool personalized;
 };
 
+// Row r's next rank, contribution, L1 change and dangling share from its
+// in-edge sum, given its current rank `old` and out-degree `od`.
+__device__ __forceinline__ void finalize_row_with(const PRState &ps, uint32_t r, float sum, float old, uint32_t od,
+                                                  float *nxt, float *cnxt, double &res, double &dang) {
+    float nx;
+    if (ps.personalized) {
+        nx = __fmul_rn(ps.damping, sum);
+        if (r == ps.source) nx = __fadd_rn(ps.tele, nx);
+    } else {
+        nx = __fadd_rn(ps.dshare, __fmul_rn(ps.damping, sum));
+    }
+    res += fabs(static_cast<double>(nx) - static_cast<double>(old));
+    nxt[r] = nx;
+    cnxt[r] = od ? __fdiv_rn(nx, static_cast<float>(od)) : 0.0f;
+    if (od == 0) dang += static_cast<double>(nx);
+}
+
 __device__ __forceinline__ void finalize_row(const PRArgs &a, const PRState &ps, uint32_t r, float sum,
                                              const float *cur, float *nxt, float *cnxt, double &res, double &dang) {
     float nx;
@@ -300,30 +317,47 @@ __device__ __forceinline__ void tile_task(const PRArgs &a, const PRState &ps, co
     const uint32_t rl = (last_e - last_b >= a.tile_cost) ? r1 - 1 : r1;  // long last row is chunked
     const uint64_t e0 = a.in_off[r0];
     const uint64_t e1 = (rl == r1) ? last_e : last_b;
+    // the first 32 rows' bounds (relative to e0), ranks and out-degrees,
+    // loaded before the gathers so that they arrive with them
+    uint32_t lo_p = 0, hi_p = 0, od_p = 0;
+    float old_p = 0.0f;
+    if (r0 + lane < rl) {
+        lo_p = static_cast<uint32_t>(a.in_off[r0 + lane] - e0);
+        hi_p = static_cast<uint32_t>(a.in_off[r0 + lane + 1] - e0);
+        old_p = b.cur[r0 + lane];
+        od_p = a.out_deg[r0 + lane];
+    }
     gather_span<kSmemHot>(in_src, b.ccur, s_hot, a.hot_vertex, e0, e1, pol, lane,
                           [&](uint32_t i, float v) { sv[i] = v; });
     __syncwarp();
     for (uint32_t rb = r0; rb < rl; rb += 32) {
         const uint32_t r = rb + lane;
         const bool active = r < rl;
-        const uint64_t lo = active ? a.in_off[r] : 0;
-        const uint64_t hi = active ? a.in_off[r + 1] : 0;
+        uint32_t lo = lo_p, hi = hi_p, od = od_p;
+        float old = old_p;
+        if (rb != r0) {
+            lo = active ? static_cast<uint32_t>(a.in_off[r] - e0) : 0u;
+            hi = active ? static_cast<uint32_t>(a.in_off[r + 1] - e0) : 0u;
+            old = active ? b.cur[r] : 0.0f;
+            od = active ? a.out_deg[r] : 0u;
+        }
         if (active && hi - lo < kWarpRowDegree) {
             dev::CSum acc;
-            const uint32_t xe = static_cast<uint32_t>(hi - e0);
-            for (uint32_t x = static_cast<uint32_t>(lo - e0); x < xe; ++x) acc.add(sv[x]);
-            finalize_row(a, ps, r, acc.value(), b.cur, b.nxt, b.cnxt, res, dang);
+            for (uint32_t x = lo; x < hi; ++x) acc.add(sv[x]);
+            finalize_row_with(ps, r, acc.value(), old, od, b.nxt, b.cnxt, res, dang);
         }
         uint32_t big = __ballot_sync(0xffffffffu, active && (hi - lo >= kWarpRowDegree));
         while (big) {
             const int src = __ffs(big) - 1;
             big &= big - 1;
-            const uint64_t bb = __shfl_sync(0xffffffffu, lo, src);
-            const uint64_t ee = __shfl_sync(0xffffffffu, hi, src);
+            const uint32_t bb = __shfl_sync(0xffffffffu, lo, src);
+            const uint32_t ee = __shfl_sync(0xffffffffu, hi, src);
+            const float o_src = __shfl_sync(0xffffffffu, old, src);
+            const uint32_t d_src = __shfl_sync(0xffffffffu, od, src);
             dev::CSum acc;
-            for (uint64_t x = bb + lane; x < ee; x += 32) acc.add(sv[x - e0]);
+            for (uint32_t x = bb + lane; x < ee; x += 32) acc.add(sv[x]);
             acc = dev::warp_reduce(acc);
-            if (lane == 0) finalize_row(a, ps, rb + src, acc.value(), b.cur, b.nxt, b.cnxt, res, dang);
+            if (lane == 0) finalize_row_with(ps, rb + src, acc.value(), o_src, d_src, b.nxt, b.cnxt, res, dang);
         }
     }
     __syncwarp();

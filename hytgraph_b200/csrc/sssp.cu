@@ -145,6 +145,19 @@ __global__ void __launch_bounds__(kSSThreads) sssp_frontier_edges_kernel(const S
     if ((threadIdx.x & 31) == 0 && sum) atomicAdd(&a.hdr->frontier_edges, sum);
 }
 
+// Lowers tile row r's label from `seen` to c if that improves it; true when
+// r joins the next frontier.  A tile row has exactly one writer during a
+// sweep (the warp that owns its tile) and no push runs beside a sweep, so
+// `seen` -- read before the tile's gathers -- is the row's label, and plain
+// stores replace the atomics.
+__device__ __forceinline__ bool pull_store(const SSArgs &a, const RoundView &rv, uint32_t r, uint32_t c,
+                                           uint32_t seen) {
+    if (c >= seen) return false;
+    a.dist[r] = c;
+    a.stamp[r] = rv.next_stamp;
+    return true;
+}
+
 // Lowers row r's label to c if that improves it; returns true when r joins
 // the next frontier for the first time this round.
 __device__ __forceinline__ bool pull_relax(const SSArgs &a, const RoundView &rv, uint32_t r, uint32_t c) {
@@ -159,7 +172,7 @@ __device__ __forceinline__ bool pull_relax(const SSArgs &a, const RoundView &rv,
 // CTA's shared-memory table, all labels gathered evict-last from L2, then
 // the sink.  Unreached sources give infinity.
 #ifndef HYT_PULL_BATCH
-#define HYT_PULL_BATCH 16
+#define HYT_PULL_BATCH 8  // 16: register spills and 5 % slower sweeps at R-MAT scale 24
 #endif
 constexpr int kPullBatch = HYT_PULL_BATCH;
 
@@ -167,18 +180,24 @@ constexpr int kPullBatch = HYT_PULL_BATCH;
 template <int kK, int WK, class Sink>
 __device__ __forceinline__ void pull_pass(const SSArgs &a, const PullGraph &pg, const uint32_t *s_hot, uint64_t lo,
                                           uint32_t base, uint32_t n, uint64_t pol, int lane, Sink &sink) {
+    // ids, then the label gathers, then the weights (streamed; issued after
+    // the gathers so that ids and weights are not live together)
     uint32_t id[kK], w[kK], du[kK];
 #pragma unroll
     for (int k = 0; k < kK; ++k) {
         const uint32_t i = base + 32 * k + lane;
         id[k] = (i < n) ? dev::ld_stream(pg.in_src + lo + i) : 0u;
-        w[k] = (i < n) ? edge_weight<WK>(pg.in_w, lo + i) : 0u;
     }
 #pragma unroll
     for (int k = 0; k < kK; ++k)
         if (id[k] & kHotTag) id[k] = s_hot[id[k] & ~kHotTag];  // hot slot -> vertex id
 #pragma unroll
     for (int k = 0; k < kK; ++k) du[k] = dev::ld_keep_u32(a.dist + id[k], pol);
+#pragma unroll
+    for (int k = 0; k < kK; ++k) {
+        const uint32_t i = base + 32 * k + lane;
+        w[k] = (i < n) ? edge_weight<WK>(pg.in_w, lo + i) : 0u;
+    }
 #pragma unroll
     for (int k = 0; k < kK; ++k) {
         const uint32_t i = base + 32 * k + lane;
@@ -245,31 +264,43 @@ __global__ void __launch_bounds__(kPullThreads, 1) sssp_pull_kernel(const SSArgs
             const uint32_t rl = (last_e - last_b >= pg.tile_cost) ? r1 - 1 : r1;  // long last row is chunked
             const uint64_t e0 = pg.in_off[r0];
             const uint64_t e1 = (rl == r1) ? last_e : last_b;
+            // the first 32 rows' bounds (relative to e0) and labels, loaded
+            // before the gathers so that they arrive with them
+            uint32_t lo_p = 0, hi_p = 0, seen_p = 0;
+            if (r0 + lane < rl) {
+                lo_p = static_cast<uint32_t>(pg.in_off[r0 + lane] - e0);
+                hi_p = static_cast<uint32_t>(pg.in_off[r0 + lane + 1] - e0);
+                seen_p = __ldcg(a.dist + r0 + lane);
+            }
             pull_span<WK>(a, pg, s_hot, e0, e1, pol, lane, [&](uint32_t i, uint32_t c) { sv[i] = c; });
             __syncwarp();
             for (uint32_t rb = r0; rb < rl; rb += 32) {
                 const uint32_t r = rb + lane;
                 const bool active = r < rl;
-                const uint64_t lo = active ? pg.in_off[r] : 0;
-                const uint64_t hi = active ? pg.in_off[r + 1] : 0;
+                uint32_t lo = lo_p, hi = hi_p, seen = seen_p;
+                if (rb != r0) {
+                    lo = active ? static_cast<uint32_t>(pg.in_off[r] - e0) : 0u;
+                    hi = active ? static_cast<uint32_t>(pg.in_off[r + 1] - e0) : 0u;
+                    seen = active ? __ldcg(a.dist + r) : 0u;
+                }
                 bool joined = false;
                 if (active && hi - lo < 64) {
                     uint32_t best = a.inf;
-                    const uint32_t xe = static_cast<uint32_t>(hi - e0);
-                    for (uint32_t x = static_cast<uint32_t>(lo - e0); x < xe; ++x) best = min(best, sv[x]);
-                    joined = pull_relax(a, rv, r, best);
+                    for (uint32_t x = lo; x < hi; ++x) best = min(best, sv[x]);
+                    joined = pull_store(a, rv, r, best, seen);
                 }
                 uint32_t big = __ballot_sync(0xffffffffu, active && (hi - lo >= 64));
                 while (big) {
                     const int src = __ffs(big) - 1;
                     big &= big - 1;
-                    const uint64_t bb = __shfl_sync(0xffffffffu, lo, src);
-                    const uint64_t ee = __shfl_sync(0xffffffffu, hi, src);
+                    const uint32_t bb = __shfl_sync(0xffffffffu, lo, src);
+                    const uint32_t ee = __shfl_sync(0xffffffffu, hi, src);
+                    const uint32_t sn = __shfl_sync(0xffffffffu, seen, src);
                     uint32_t best = a.inf;
-                    for (uint64_t x = bb + lane; x < ee; x += 32) best = min(best, sv[x - e0]);
+                    for (uint32_t x = bb + lane; x < ee; x += 32) best = min(best, sv[x]);
 #pragma unroll
                     for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(0xffffffffu, best, o));
-                    const bool j = (lane == 0) && pull_relax(a, rv, rb + src, best);
+                    const bool j = (lane == 0) && pull_store(a, rv, rb + src, best, sn);
                     if (__shfl_sync(0xffffffffu, j ? 1u : 0u, 0) && lane == src) joined = true;
                 }
                 const uint32_t vals[1] = {r};
