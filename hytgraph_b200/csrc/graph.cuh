@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstring>
 #include <vector>
 
 #include "common.cuh"
@@ -52,6 +53,35 @@ struct LongRow {
     uint32_t first_chunk;  // index of its first partial-sum slot
     uint32_t num_chunks;
     uint32_t pad;
+};
+
+// An instantiated CUDA graph holding a solver's conditional while-loop,
+// kept with the graph object and reused by later solves while the loop's
+// shape (`key`: kernels, launch shapes, argument pointers) is unchanged.
+// Its conditional handle is set to 1 at every launch.
+struct LoopGraph {
+    std::vector<unsigned char> key;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaGraphConditionalHandle cond = 0;
+
+    LoopGraph() = default;
+    LoopGraph(const LoopGraph &) = delete;
+    LoopGraph &operator=(const LoopGraph &) = delete;
+    ~LoopGraph() { reset(); }
+    void reset() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+        key.clear();
+    }
+    bool matches(const void *k, size_t n) const {
+        return exec && key.size() == n && std::memcmp(key.data(), k, n) == 0;
+    }
+    void set_key(const void *k, size_t n) {
+        key.assign(static_cast<const unsigned char *>(k), static_cast<const unsigned char *>(k) + n);
+    }
 };
 
 struct GraphImpl {
@@ -113,6 +143,7 @@ struct GraphImpl {
     GraphArray<uint32_t> ms_dist;          // multi-source labels [V][8]
     GraphArray<unsigned char> ms_state;
     PinnedArray<uint64_t> host_scratch;  // small pinned readback area
+    LoopGraph sssp_loop;                 // instantiated SSSP round loop (reused while its shape holds)
 
     size_t device_bytes() const;
 };

@@ -53,7 +53,8 @@ struct MSHeader {
     unsigned long long relaxations;     // push: frontier out-edges; pull: E per sweep
     unsigned long long frontier_total;  // frontier vertices expanded
     unsigned long long frontier_edges;  // out-edges of this round's frontier
-    uint32_t pull_rounds, pad;
+    uint32_t pull_rounds, close_ticket;  // close_ticket: blocks of the round-close kernel finished
+    unsigned long long frontier_edges_next;  // out-edges of the next frontier, summed at round close
 };
 
 struct MSArgs {
@@ -164,24 +165,12 @@ __global__ void ms_sources_kernel(const MSArgs *__restrict__ args) {
         if (!seen) {
             a.queue[0][n++] = s;
             a.stamp[s] = 0u;
+            a.hdr->frontier_edges += a.row_off[s + 1] - a.row_off[s];  // round 0's frontier
         }
     }
     a.hdr->qsize[0] = n;
 }
 
-__global__ void __launch_bounds__(kMSThreads) ms_frontier_edges_kernel(const MSArgs *__restrict__ args) {
-    const MSArgs a = *args;
-    if (*(volatile uint32_t *)&a.hdr->done) return;
-    const View w = view(a);
-    unsigned long long sum = 0;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < w.qn; i += gridDim.x * blockDim.x) {
-        const uint32_t v = w.q[i];
-        sum += a.row_off[v + 1] - a.row_off[v];
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
-    if ((threadIdx.x & 31) == 0 && sum) atomicAdd(&a.hdr->frontier_edges, sum);
-}
 
 // Push round: a warp takes 32 frontier vertices; rows shorter than
 // kHubDegree are walked as one combined edge list (each lane finds its
@@ -448,10 +437,8 @@ __global__ void __launch_bounds__(kMPThreads, 1) ms_pull_kernel(const MSArgs *__
     }
 }
 
-__global__ void ms_round_end_kernel(const MSArgs *__restrict__ args) {
-    const MSArgs a = *args;
-    MSHeader *h = a.hdr;
-    if (h->done) return;
+// Round-end bookkeeping (one thread): true when the solve is finished.
+__device__ __forceinline__ bool ms_end_round(const MSArgs &a, MSHeader *h) {
     const uint32_t r = h->round;
     const uint32_t n_next = h->qsize[(r + 1) & 1];
     h->frontier_total += h->qsize[r & 1];
@@ -464,7 +451,50 @@ __global__ void ms_round_end_kernel(const MSArgs *__restrict__ args) {
         h->done = 1;
         h->converged = conv ? 1u : 0u;
         if (a.use_cond) cudaGraphSetConditional(a.cond, 0);
+        return true;
     }
+    return false;
+}
+
+__global__ void ms_round_end_kernel(const MSArgs *__restrict__ args) {
+    const MSArgs a = *args;
+    MSHeader *h = a.hdr;
+    if (h->done) return;
+    ms_end_round(a, h);
+}
+
+// End of a round of a pull-capable solve, in one grid launch: the whole
+// grid sums the out-edges of the next frontier (the next round's push /
+// pull decision), then the last block to finish ends the round.
+__global__ void __launch_bounds__(kMSThreads) ms_round_close_kernel(const MSArgs *__restrict__ args) {
+    const MSArgs a = *args;
+    MSHeader *h = a.hdr;
+    if (*(volatile uint32_t *)&h->done) return;
+    const uint32_t r = *(volatile uint32_t *)&h->round;
+    const uint32_t qn = *(volatile uint32_t *)&h->qsize[(r + 1) & 1];
+    const uint32_t *q = ((r + 1) & 1) ? a.queue[1] : a.queue[0];
+    unsigned long long sum = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < qn; i += gridDim.x * blockDim.x) {
+        const uint32_t v = q[i];
+        sum += a.row_off[v + 1] - a.row_off[v];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    if ((threadIdx.x & 31) == 0 && sum) atomicAdd(&h->frontier_edges_next, sum);
+    __shared__ uint32_t s_last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicAdd(&h->close_ticket, 1u) == gridDim.x - 1 ? 1u : 0u;
+    }
+    __syncthreads();
+    if (!s_last || threadIdx.x != 0) return;
+    __threadfence();
+    const unsigned long long fe = atomicAdd(&h->frontier_edges_next, 0ull);
+    h->frontier_edges_next = 0;
+    h->close_ticket = 0;
+    ms_end_round(a, h);
+    h->frontier_edges = fe;
 }
 
 // out[l][c] = dist[inv[c]][l] (caller order c; inv NULL: identity).
@@ -588,25 +618,30 @@ void ms_solve(GraphImpl &g, const uint32_t *sources, uint32_t k, uint32_t max_ro
             HYT_CUDA(cudaGraphAddKernelNode(&node, body, prev ? &prev : nullptr, prev ? 1 : 0, &kp));
             prev = node;
         };
-        if (a.pull_div) add(reinterpret_cast<void *>(ms_frontier_edges_kernel), dim3(grid), dim3(kMSThreads), 0);
         add(reinterpret_cast<void *>(ms_expand_kernel<WK>), dim3(grid), dim3(kMSThreads), 0);
         add(reinterpret_cast<void *>(ms_hub_kernel<WK>), dim3(grid), dim3(kMSThreads), 0);
-        if (a.pull_div) add(pull_fn, dim3(pgrid), dim3(kMPThreads), pull_smem);
-        add(reinterpret_cast<void *>(ms_round_end_kernel), dim3(1), dim3(1), 0);
+        if (a.pull_div) {
+            add(pull_fn, dim3(pgrid), dim3(kMPThreads), pull_smem);
+            add(reinterpret_cast<void *>(ms_round_close_kernel), dim3(grid), dim3(kMSThreads), 0);
+        } else {
+            add(reinterpret_cast<void *>(ms_round_end_kernel), dim3(1), dim3(1), 0);
+        }
         HYT_CUDA(cudaGraphInstantiate(&exec, graph, 0));
         HYT_CUDA(cudaGraphLaunch(exec, s));
     } else {
         for (uint32_t r = 0; r < max_rounds; ++r) {
-            if (a.pull_div) ms_frontier_edges_kernel<<<grid, kMSThreads, 0, s>>>(d_args);
             ms_expand_kernel<WK><<<grid, kMSThreads, 0, s>>>(d_args);
             ms_hub_kernel<WK><<<grid, kMSThreads, 0, s>>>(d_args);
             if (a.pull_div) {
                 void *pargs[] = {&d_args};
                 HYT_CUDA(cudaLaunchKernel(pull_fn, dim3(pgrid), dim3(kMPThreads), pargs, pull_smem, s));
             }
-            ms_round_end_kernel<<<1, 1, 0, s>>>(d_args);
+            if (a.pull_div)
+                ms_round_close_kernel<<<grid, kMSThreads, 0, s>>>(d_args);
+            else
+                ms_round_end_kernel<<<1, 1, 0, s>>>(d_args);
             HYT_CUDA(cudaGetLastError());
-            launches += a.pull_div ? 5 : 3;
+            launches += a.pull_div ? 4 : 3;
             uint32_t done = 0;
             HYT_CUDA(cudaMemcpyAsync(&done, &hdr->done, sizeof(done), cudaMemcpyDeviceToHost, s));
             HYT_CUDA(cudaStreamSynchronize(s));
@@ -619,7 +654,7 @@ void ms_solve(GraphImpl &g, const uint32_t *sources, uint32_t k, uint32_t max_ro
     const double total_ms = total.ms();
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
-    if (use_graph) launches += (a.pull_div ? 5 : 3) * h.round;
+    if (use_graph) launches += (a.pull_div ? 4 : 3) * h.round;
     if (h.error) fail(HYT_E_TIMEOUT, "hyt_sssp_multi: a bounded wait for a staged copy ran out");
     if (out) {
         if (is_device_pointer(out)) {

@@ -130,20 +130,6 @@ struct PullGraph {
     uint32_t num_hot;
 };
 
-// Out-edges of the current frontier (for the push / pull decision).
-__global__ void __launch_bounds__(kSSThreads) sssp_frontier_edges_kernel(const SSArgs *__restrict__ args) {
-    const SSArgs a = *args;
-    if (*(volatile uint32_t *)&a.hdr->done) return;
-    const RoundView rv = round_view(a);
-    unsigned long long sum = 0;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < rv.qn; i += gridDim.x * blockDim.x) {
-        const uint32_t v = rv.q[i];
-        sum += a.row_off[v + 1] - a.row_off[v];
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
-    if ((threadIdx.x & 31) == 0 && sum) atomicAdd(&a.hdr->frontier_edges, sum);
-}
 
 // Lowers tile row r's label from `seen` to c if that improves it; true when
 // r joins the next frontier.  A tile row has exactly one writer during a
@@ -443,6 +429,41 @@ __global__ void __launch_bounds__(stage::kStageThreads, 1) sssp_pull_staged_kern
     }
 }
 
+// End of a round of a pull-capable solve, in one grid launch: the whole
+// grid sums the out-edges of the next frontier (the next round's push /
+// pull decision), then the last block to finish runs the round-end logic.
+__global__ void __launch_bounds__(kSSThreads) sssp_round_close_kernel(const SSArgs *__restrict__ args) {
+    const SSArgs a = *args;
+    SSHeader *h = a.hdr;
+    if (*(volatile uint32_t *)&h->done) return;
+    const uint32_t r = *(volatile uint32_t *)&h->round;
+    const uint32_t qn = *(volatile uint32_t *)&h->qsize[(r + 1) & 1];
+    const uint32_t *q = ((r + 1) & 1) ? a.queue[1] : a.queue[0];
+    unsigned long long sum = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < qn; i += gridDim.x * blockDim.x) {
+        const uint32_t v = q[i];
+        sum += a.row_off[v + 1] - a.row_off[v];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    if ((threadIdx.x & 31) == 0 && sum) atomicAdd(&h->frontier_edges_next, sum);
+    __shared__ uint32_t s_last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicAdd(&h->close_ticket, 1u) == gridDim.x - 1 ? 1u : 0u;
+    }
+    __syncthreads();
+    if (!s_last || threadIdx.x != 0) return;
+    __threadfence();
+    const unsigned long long fe = atomicAdd(&h->frontier_edges_next, 0ull);
+    h->frontier_edges_next = 0;
+    h->close_ticket = 0;
+    const bool finish = round_end(h);
+    h->frontier_edges = fe;
+    if (finish && a.use_cond) cudaGraphSetConditional(a.cond, 0);
+}
+
 __global__ void sssp_round_end_kernel(const SSArgs *__restrict__ args) {
     const SSArgs a = *args;
     if (a.hdr->done) return;
@@ -453,7 +474,10 @@ __global__ void sssp_init_kernel(const SSArgs *__restrict__ args) {
     const SSArgs a = *args;
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < a.V; v += stride) init_vertex(a, v);
-    if (blockIdx.x == 0 && threadIdx.x == 0) a.queue[0][0] = a.source;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.queue[0][0] = a.source;
+        a.hdr->frontier_edges = a.row_off[a.source + 1] - a.row_off[a.source];  // round 0's frontier
+    }
 }
 
 // ---- partitioned (out-of-HBM) solves -------------------------------------
@@ -677,16 +701,39 @@ void sssp_solve(GraphImpl &g, uint32_t source, uint32_t delta, uint32_t max_roun
     h0.max_rounds = max_rounds;
     h0.delta = delta;
     h0.threshold = (WK == HYT_WEIGHTS_F32 || delta == kNoDelta) ? 0xFFFFFFFFu : delta;
+    const bool far_pile = h0.threshold != 0xFFFFFFFFu;  // labels above the threshold wait in the far pile
 
     const bool use_graph = !(flags & HYT_RUN_NO_GRAPH) && !(flags & HYT_RUN_PROFILE);
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
+    const int grid = expand_grid<WK>();
+    // The round loop's shape; an instantiated loop of the same shape (kept
+    // with the graph object) is launched again instead of being rebuilt.
+    struct LoopKey {
+        int wk, grid, pgrid;
+        uint32_t far_pile, pull_div, staged, pull_smem;
+        const void *args;
+        PullGraph pg;
+    } key;
+    std::memset(&key, 0, sizeof(key));
+    key.wk = WK;
+    key.grid = grid;
+    key.pgrid = pgrid;
+    key.far_pile = far_pile;
+    key.pull_div = a.pull_div;
+    key.staged = staged;
+    key.pull_smem = pull_smem;
+    key.args = d_args;
+    key.pg = pg;
+    LoopGraph &loop = g.sssp_loop;
+    const bool reuse = use_graph && loop.matches(&key, sizeof(key));
+    if (use_graph && !reuse) {
+        loop.reset();
+        HYT_CUDA(cudaGraphCreate(&loop.graph, 0));
+        HYT_CUDA(cudaGraphConditionalHandleCreate(&loop.cond, loop.graph, 1, cudaGraphCondAssignDefault));
+    }
     if (use_graph) {
-        HYT_CUDA(cudaGraphCreate(&graph, 0));
-        HYT_CUDA(cudaGraphConditionalHandleCreate(&a.cond, graph, 1, cudaGraphCondAssignDefault));
+        a.cond = loop.cond;
         a.use_cond = 1;
     }
-    const int grid = expand_grid<WK>();
 
     EventTimer total;
     total.start(s);
@@ -696,46 +743,54 @@ void sssp_solve(GraphImpl &g, uint32_t source, uint32_t delta, uint32_t max_roun
     HYT_CUDA(cudaGetLastError());
     uint32_t launches = 1, hot = 0;
     double kernel_ms = 0.0;
+    // split (finite bucket width), expand, hub, pull sweep + round close or round end
+    const uint32_t per_round = (far_pile ? 1u : 0u) + 3u + (a.pull_div ? 1u : 0u);
 
     if (use_graph) {
-        cudaGraphNodeParams cp = {};
-        cp.type = cudaGraphNodeTypeConditional;
-        cp.conditional.handle = a.cond;
-        cp.conditional.type = cudaGraphCondTypeWhile;
-        cp.conditional.size = 1;
-        cudaGraphNode_t cnode;
-        HYT_CUDA(cudaGraphAddNode(&cnode, graph, nullptr, 0, &cp));
-        cudaGraph_t body = cp.conditional.phGraph_out[0];
-        void *kargs[] = {&d_args};
-        cudaKernelNodeParams kp = {};
-        kp.kernelParams = kargs;
-        kp.blockDim = dim3(kSSThreads);
-        kp.gridDim = dim3(grid);
-        cudaGraphNode_t prev = nullptr, node;
-        auto add = [&](const void *f, dim3 gd, dim3 bd, unsigned smem, void **params) {
-            kp.func = const_cast<void *>(f);
-            kp.gridDim = gd;
-            kp.blockDim = bd;
-            kp.sharedMemBytes = smem;
-            kp.kernelParams = params;
-            HYT_CUDA(cudaGraphAddKernelNode(&node, body, prev ? &prev : nullptr, prev ? 1 : 0, &kp));
-            prev = node;
-        };
-        void *pargs[] = {&d_args, &pg};
-        add(reinterpret_cast<void *>(sssp_split_kernel), dim3(grid), dim3(kSSThreads), 0, kargs);
-        if (a.pull_div) add(reinterpret_cast<void *>(sssp_frontier_edges_kernel), dim3(grid), dim3(kSSThreads), 0, kargs);
-        add(reinterpret_cast<void *>(sssp_expand_kernel<WK>), dim3(grid), dim3(kSSThreads), 0, kargs);
-        add(reinterpret_cast<void *>(sssp_hub_kernel<WK>), dim3(grid), dim3(kSSThreads), 0, kargs);
-        if (a.pull_div) add(pull_fn, dim3(pgrid), dim3(staged ? stage::kStageThreads : kPullThreads), pull_smem, pargs);
-        add(reinterpret_cast<void *>(sssp_round_end_kernel), dim3(1), dim3(1), 0, kargs);
-        HYT_CUDA(cudaGraphInstantiate(&exec, graph, 0));
-        HYT_CUDA(cudaGraphLaunch(exec, s));
+        if (!reuse) {
+            cudaGraphNodeParams cp = {};
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = loop.cond;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            cudaGraphNode_t cnode;
+            HYT_CUDA(cudaGraphAddNode(&cnode, loop.graph, nullptr, 0, &cp));
+            cudaGraph_t body = cp.conditional.phGraph_out[0];
+            void *kargs[] = {&d_args};
+            cudaKernelNodeParams kp = {};
+            kp.kernelParams = kargs;
+            kp.blockDim = dim3(kSSThreads);
+            kp.gridDim = dim3(grid);
+            cudaGraphNode_t prev = nullptr, node;
+            auto add = [&](const void *f, dim3 gd, dim3 bd, unsigned smem, void **params) {
+                kp.func = const_cast<void *>(f);
+                kp.gridDim = gd;
+                kp.blockDim = bd;
+                kp.sharedMemBytes = smem;
+                kp.kernelParams = params;
+                HYT_CUDA(cudaGraphAddKernelNode(&node, body, prev ? &prev : nullptr, prev ? 1 : 0, &kp));
+                prev = node;
+            };
+            void *pargs[] = {&d_args, &pg};
+            // one bucket (no threshold): the far pile stays empty, nothing to split
+            if (far_pile) add(reinterpret_cast<void *>(sssp_split_kernel), dim3(grid), dim3(kSSThreads), 0, kargs);
+            add(reinterpret_cast<void *>(sssp_expand_kernel<WK>), dim3(grid), dim3(kSSThreads), 0, kargs);
+            add(reinterpret_cast<void *>(sssp_hub_kernel<WK>), dim3(grid), dim3(kSSThreads), 0, kargs);
+            if (a.pull_div) {
+                add(pull_fn, dim3(pgrid), dim3(staged ? stage::kStageThreads : kPullThreads), pull_smem, pargs);
+                add(reinterpret_cast<void *>(sssp_round_close_kernel), dim3(grid), dim3(kSSThreads), 0, kargs);
+            } else {
+                add(reinterpret_cast<void *>(sssp_round_end_kernel), dim3(1), dim3(1), 0, kargs);
+            }
+            HYT_CUDA(cudaGraphInstantiate(&loop.exec, loop.graph, 0));
+            loop.set_key(&key, sizeof(key));
+        }
+        HYT_CUDA(cudaGraphLaunch(loop.exec, s));
     } else {
         EventTimer kt;
         for (uint32_t r = 0; r < max_rounds; ++r) {
             if (flags & HYT_RUN_PROFILE) kt.start(s);
-            sssp_split_kernel<<<grid, kSSThreads, 0, s>>>(d_args);
-            if (a.pull_div) sssp_frontier_edges_kernel<<<grid, kSSThreads, 0, s>>>(d_args);
+            if (far_pile) sssp_split_kernel<<<grid, kSSThreads, 0, s>>>(d_args);
             sssp_expand_kernel<WK><<<grid, kSSThreads, 0, s>>>(d_args);
             sssp_hub_kernel<WK><<<grid, kSSThreads, 0, s>>>(d_args);
             if (a.pull_div) {
@@ -744,11 +799,13 @@ void sssp_solve(GraphImpl &g, uint32_t source, uint32_t delta, uint32_t max_roun
                 else
                     sssp_pull_kernel<WK><<<pgrid, kPullThreads, pull_smem, s>>>(d_args, pg);
             }
+            if (a.pull_div)
+                sssp_round_close_kernel<<<grid, kSSThreads, 0, s>>>(d_args);  // frontier-edge count + round end
             if (flags & HYT_RUN_PROFILE) kt.stop(s);
-            sssp_round_end_kernel<<<1, 1, 0, s>>>(d_args);
+            if (!a.pull_div) sssp_round_end_kernel<<<1, 1, 0, s>>>(d_args);
             HYT_CUDA(cudaGetLastError());
-            launches += a.pull_div ? 6 : 4;
-            hot += a.pull_div ? 5 : 3;
+            launches += per_round;
+            hot += a.pull_div ? per_round : per_round - 1;
             uint32_t done = 0;
             HYT_CUDA(cudaMemcpyAsync(&done, &hdr->done, sizeof(done), cudaMemcpyDeviceToHost, s));
             HYT_CUDA(cudaStreamSynchronize(s));
@@ -760,9 +817,7 @@ void sssp_solve(GraphImpl &g, uint32_t source, uint32_t delta, uint32_t max_roun
     HYT_CUDA(cudaMemcpyAsync(&h, hdr, sizeof(h), cudaMemcpyDeviceToHost, s));
     total.stop(s);
     const double total_ms = total.ms();
-    if (exec) cudaGraphExecDestroy(exec);
-    if (graph) cudaGraphDestroy(graph);
-    if (use_graph) launches += 4 * h.round;
+    if (use_graph) launches += per_round * h.round;
     if (h.error) fail(HYT_E_TIMEOUT, "SSSP: a bounded wait for a staged copy ran out");
     if (dist_out) graph_emit(g, dist_out, g.dist.get(), s);
     if (stats) {
@@ -977,6 +1032,8 @@ constexpr uint64_t kNoAllocHubCap = kNoAllocMaxVertices + kNoAllocMaxEdges / kHu
 // args (256 B) | header (256 B) | check word (64 B) | stamp+fstamp u32[2V] |
 // queue u32[2][V] | far u32[2][V] | hub tasks uint2[hub cap]
 constexpr size_t kNoAllocHeadBytes = 1024;
+// head: arguments at 0, header at 256, validation flags at 512
+static_assert(sizeof(SSArgs) <= 256 && sizeof(SSHeader) <= 256, "no-alloc head layout");
 constexpr size_t kNoAllocScratchBytes =
     kNoAllocHeadBytes + 6 * sizeof(uint32_t) * kNoAllocMaxVertices + sizeof(uint2) * kNoAllocHubCap;
 

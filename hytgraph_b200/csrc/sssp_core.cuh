@@ -50,6 +50,9 @@ struct SSHeader {
     unsigned long long frontier_edges;  // out-edges of this round's frontier (pull-capable solves)
     uint32_t pull_rounds;               // rounds run as pull sweeps
     uint32_t error;                     // 1: a bounded wait for a staged copy ran out
+    unsigned long long frontier_edges_next;  // out-edges of the next frontier, summed at round close
+    uint32_t close_ticket;                   // blocks of the round-close kernel finished
+    uint32_t pad;
 };
 
 struct SSArgs {
