@@ -177,6 +177,23 @@ __global__ void invert_kernel(const uint32_t *__restrict__ perm, uint64_t V, uin
         inv[perm[n]] = static_cast<uint32_t>(n);
 }
 
+// out[i] = hi[i] << 32 | lo[i].
+__global__ void pack_pairs_kernel(const uint32_t *__restrict__ hi, const uint32_t *__restrict__ lo, uint64_t n,
+                                  uint64_t *__restrict__ out) {
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x)
+        out[i] = (uint64_t(hi[i]) << 32) | lo[i];
+}
+
+// hi[i] = in[i] >> 32, lo[i] = in[i] & 0xFFFFFFFF.
+__global__ void unpack_pairs_kernel(const uint64_t *__restrict__ in, uint64_t n, uint32_t *__restrict__ hi,
+                                    uint32_t *__restrict__ lo) {
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
+        const uint64_t v = in[i];
+        hi[i] = static_cast<uint32_t>(v >> 32);
+        lo[i] = static_cast<uint32_t>(v);
+    }
+}
+
 // dst[v] = src[inv[v]]: values back in the caller's vertex order.
 __global__ void emit_kernel(const uint32_t *__restrict__ src, const uint32_t *__restrict__ inv, uint64_t V,
                             uint32_t *__restrict__ dst) {
@@ -236,14 +253,29 @@ void graph_create(GraphImpl &g, const hyt_csr &csr, uint32_t flags) {
     g.inv.allocate(V);
     invert_kernel<<<grid_for(V, 256), 256, 0, g.stream>>>(perm.get(), V, g.inv.get());
     HYT_CUDA(cudaGetLastError());
-    g.h_inv.resize(V);
-    HYT_CUDA(cudaMemcpyAsync(g.h_inv.data(), g.inv.get(), V * 4, cudaMemcpyDeviceToHost, g.stream));
     HYT_CUDA(cudaStreamSynchronize(g.stream));
     g.perm = std::move(perm);
 }
 
-uint32_t graph_vertex(const GraphImpl &g, uint32_t v, cudaStream_t) {
-    return g.h_inv.empty() ? v : g.h_inv[v];
+uint32_t graph_vertex(const GraphImpl &g, uint32_t v, cudaStream_t s) {
+    if (!g.inv.get()) return v;
+    if (!g.h_inv.empty()) return g.h_inv[v];
+    // one entry of the device map: a single-source solve pays one small
+    // read instead of a copy of the whole map at graph creation
+    uint32_t local = 0;
+    uint32_t *h = g.host_scratch.ptr ? reinterpret_cast<uint32_t *>(g.host_scratch.ptr) : &local;
+    HYT_CUDA(cudaMemcpyAsync(h, g.inv.get() + v, sizeof(uint32_t), cudaMemcpyDeviceToHost, s ? s : g.stream));
+    HYT_CUDA(cudaStreamSynchronize(s ? s : g.stream));
+    return *h;
+}
+
+void graph_vertex_map(GraphImpl &g) {
+    if (!g.inv.get() || !g.h_inv.empty()) return;
+    HYT_CUDA(cudaSetDevice(g.device));
+    std::vector<uint32_t> m(g.V);
+    HYT_CUDA(cudaMemcpyAsync(m.data(), g.inv.get(), g.V * 4, cudaMemcpyDeviceToHost, g.stream));
+    HYT_CUDA(cudaStreamSynchronize(g.stream));
+    g.h_inv = std::move(m);
 }
 
 void graph_emit(const GraphImpl &g, void *dst, const void *src, cudaStream_t s) {
@@ -493,15 +525,19 @@ void graph_build(GraphImpl &g, const hyt_csr &csr, uint32_t flags) {
         if (E) {
             HYT_CUDA(cudaMemcpyAsync(keys.get(), g.cols.get(), E * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
             if (csc_weights) {
-                Scratch<uint32_t> perm(E, s);
-                iota_kernel<<<grid_for(E, 256), 256, 0, s>>>(perm.get(), E);
-                HYT_CUDA(cudaGetLastError());
-                prims::sort_pairs_u32(keys.get(), perm.get(), E, bits_for(V - 1), s);
-                Scratch<uint32_t> src(E, s);
-                expand_sources(g.row_offsets.get(), V, E, src.get(), s);
-                gather_u32_kernel<<<grid_for(E, 256), 256, 0, s>>>(src.get(), perm.get(), E, g.in_sources.get());
+                // (source, weight) packed into one 64-bit value travels with
+                // its destination key: every pass streams, no gathers
+                Scratch<uint64_t> sw(E, s);
+                {
+                    Scratch<uint32_t> src(E, s);
+                    expand_sources(g.row_offsets.get(), V, E, src.get(), s);
+                    pack_pairs_kernel<<<grid_for(E, 256), 256, 0, s>>>(src.get(), g.weights.get(), E, sw.get());
+                    HYT_CUDA(cudaGetLastError());
+                }
+                prims::sort_pairs_u32_u64(keys.get(), sw.get(), E, bits_for(V - 1), s);
                 g.in_weights.allocate(E);
-                gather_u32_kernel<<<grid_for(E, 256), 256, 0, s>>>(g.weights.get(), perm.get(), E, g.in_weights.get());
+                unpack_pairs_kernel<<<grid_for(E, 256), 256, 0, s>>>(sw.get(), E, g.in_sources.get(),
+                                                                      g.in_weights.get());
                 HYT_CUDA(cudaGetLastError());
                 HYT_CUDA(cudaStreamSynchronize(s));
             } else {

@@ -103,7 +103,7 @@ struct GraphImpl {
     // HYT_GRAPH_HUB_ORDER: perm[new] = caller id, inv[caller id] = new
     // (empty otherwise)
     GraphArray<uint32_t> perm, inv;
-    std::vector<uint32_t> h_inv;  // host copy of inv: sources map without a device round trip
+    std::vector<uint32_t> h_inv;  // host copy of inv, filled by graph_vertex_map (engines mapping many sources)
 
     // pull side
     GraphArray<uint64_t> in_offsets;
@@ -162,8 +162,13 @@ void graph_build(GraphImpl &g, const hyt_csr &csr, uint32_t flags);
 void graph_copy_csc(const GraphImpl &g, uint64_t *in_offsets, uint32_t *in_sources);
 // Builds the graph; with HYT_GRAPH_HUB_ORDER in flags, in hub order.
 void graph_create(GraphImpl &g, const hyt_csr &csr, uint32_t flags);
-// The internal id of a caller's vertex (identity without a hub order).
+// The internal id of a caller's vertex (identity without a hub order):
+// from the host copy of the map when graph_vertex_map has made one, else
+// one 4-byte read of the device map on stream s.
 uint32_t graph_vertex(const GraphImpl &g, uint32_t v, cudaStream_t s);
+// Makes the host copy of a hub-ordered graph's vertex map (once), for
+// callers that map many sources; no-op without a hub order.
+void graph_vertex_map(GraphImpl &g);
 // Writes V 4-byte per-vertex values (internal order, device) to dst (host
 // or device) in the caller's vertex order.
 void graph_emit(const GraphImpl &g, void *dst, const void *src, cudaStream_t s);

@@ -23,6 +23,23 @@ void sort_pairs_u32(uint32_t *keys, uint32_t *vals, size_t n, int end_bit, cudaS
     HYT_CUDA(cudaStreamSynchronize(s));
 }
 
+void sort_pairs_u32_u64(uint32_t *keys, uint64_t *vals, size_t n, int end_bit, cudaStream_t s) {
+    if (n < 2) return;
+    Scratch<uint32_t> k2(n, s);
+    Scratch<uint64_t> v2(n, s);
+    cub::DoubleBuffer<uint32_t> kb(keys, k2.get());
+    cub::DoubleBuffer<uint64_t> vb(vals, v2.get());
+    size_t tb = 0;
+    HYT_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, kb, vb, static_cast<int64_t>(n), 0, end_bit, s));
+    Scratch<uint8_t> tmp(tb, s);
+    HYT_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), tb, kb, vb, static_cast<int64_t>(n), 0, end_bit, s));
+    if (kb.Current() != keys)
+        HYT_CUDA(cudaMemcpyAsync(keys, kb.Current(), n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+    if (vb.Current() != vals)
+        HYT_CUDA(cudaMemcpyAsync(vals, vb.Current(), n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
+    HYT_CUDA(cudaStreamSynchronize(s));
+}
+
 void sort_pairs_desc_u32(uint32_t *keys, uint32_t *vals, size_t n, cudaStream_t s) {
     if (n < 2) return;
     Scratch<uint32_t> k2(n, s), v2(n, s);

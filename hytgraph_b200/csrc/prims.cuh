@@ -15,6 +15,10 @@ namespace hyt::prims {
 // keys/vals are sorted in place (temporary double buffers are allocated).
 void sort_pairs_u32(uint32_t *keys, uint32_t *vals, size_t n, int end_bit, cudaStream_t s);
 
+// Stable LSD radix sort of (u32 key, u64 value) pairs on key bits
+// [0, end_bit), in place.
+void sort_pairs_u32_u64(uint32_t *keys, uint64_t *vals, size_t n, int end_bit, cudaStream_t s);
+
 // Same, descending by key (stable: equal keys keep their input order).
 void sort_pairs_desc_u32(uint32_t *keys, uint32_t *vals, size_t n, cudaStream_t s);
 

@@ -339,6 +339,7 @@ int hyt_server_create(hyt_graph *const *graphs, uint32_t num_graphs, const hyt_s
             if (!graphs[i]) fail(HYT_E_INVALID, "graph handle is NULL");
             if (graphs[i]->impl.device != o.device) fail(HYT_E_INVALID, "every graph must live on the server's device");
             s.graphs.push_back(&graphs[i]->impl);
+            graph_vertex_map(graphs[i]->impl);  // queries map their sources on the host
         }
         HYT_CUDA(cudaSetDevice(o.device));
         HYT_CUDA(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
