@@ -228,14 +228,21 @@ void graph_create(GraphImpl &g, const hyt_csr &csr, uint32_t flags) {
         copy_to_device(d_cols.get(), csr.column_indices, E * 4, g.stream);
         dev.column_indices = d_cols.get();
     }
+    // the weights are first needed by the reorder: their upload runs on the
+    // graph's stream while the hub sort (its own stream) ranks the vertices
     if (weighted && csr.weights && !is_device_pointer(csr.weights)) {
         d_w.allocate(E);
-        copy_to_device(d_w.get(), csr.weights, E * 4, g.stream);
+        HYT_CUDA(cudaMemcpyAsync(d_w.get(), csr.weights, E * 4, cudaMemcpyHostToDevice, g.stream));
         dev.weights = d_w.get();
     }
-    HYT_CUDA(cudaStreamSynchronize(g.stream));
     GraphArray<uint32_t> perm(V);
-    hub_sort(dev, 1.0, perm.get(), nullptr, nullptr, nullptr);
+    try {
+        hub_sort(dev, 1.0, perm.get(), nullptr, nullptr, nullptr);
+    } catch (...) {
+        cudaStreamSynchronize(g.stream);  // the weights copy lands before its buffer is freed
+        throw;
+    }
+    HYT_CUDA(cudaStreamSynchronize(g.stream));
     hyt_csr_buffers b{};
     csr_reorder(dev, perm.get(), true, &b, nullptr, true);
     d_off.release();

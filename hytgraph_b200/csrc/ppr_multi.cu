@@ -8,11 +8,13 @@
 //   <= tolerance.
 // The 8 lanes of a vertex are stored together (32 bytes), so one in-edge
 // costs one source id and one 32-byte sector of contributions for all 8
-// queries, instead of 8 id reads and 8 scattered gathers.  A warp takes a
-// row 4 in-edges at a time (thread t: edge t / 8, lane t % 8), sums in FP64
-// and folds the 4 edge slots with shuffles; rows at or above the graph's
-// long-row threshold use its 4096-edge chunk tasks, summed per row in chunk
-// order.  The thread layout does not depend on how many lanes are in use,
+// queries, instead of 8 id reads and 8 scattered gathers.  A thread takes
+// four of a vertex's queries with one 16-byte load per in-edge: short rows
+// 16 per warp (two threads per row), longer rows by the whole warp in 16
+// edge slots; sums are FP64, folded with shuffles in a fixed order, and
+// rows at or above the graph's long-row threshold use its 4096-edge chunk
+// tasks, summed per row in chunk order.  The thread layout does not depend
+// on how many lanes are in use,
 // so a query's result is the same bit for bit alone or packed with others.
 // A lane whose step met its tolerance stops (its values are carried
 // unchanged) while the others continue.
@@ -69,21 +71,40 @@ __global__ void ppr8_prep_kernel(const uint32_t *__restrict__ deg, const float *
     }
 }
 
-// Sum over in-edges [b, e) of c[u][lane]: thread t takes edge slot t / 8 and
-// lane t % 8; the result is complete in every thread of the lane.
-__device__ __forceinline__ double row_lane_sum(const uint32_t *__restrict__ in_src,
-                                               const uint32_t *__restrict__ hot_vertex, const float *__restrict__ c,
-                                               uint64_t b, uint64_t e, int t) {
-    const int slot = t >> 3, lane = t & 7;
-    double acc = 0.0;
-    for (uint64_t i = b + slot; i < e; i += 4) {
-        uint32_t u = in_src[i];
-        if (u & kHotTag) u = hot_vertex[u & ~kHotTag];
-        acc += double(c[uint64_t(u) * kLanes + lane]);
+// Sums over in-edges [b, e) of c[u][4h .. 4h + 3], h = t % 2: thread t
+// takes edge slot t / 2 (16 slots) and adds its edges b + t/2, b + t/2 + 16,
+// ... in that order, four queries at a time from one 16-byte load (two
+// edges loaded before either is added); the slots are then folded by
+// shuffles, so every thread of half h holds the four sums.
+__device__ __forceinline__ void row_quad_sum(const uint32_t *__restrict__ in_src,
+                                             const uint32_t *__restrict__ hot_vertex, const float *__restrict__ c,
+                                             uint64_t b, uint64_t e, int t, double (&acc)[4]) {
+    const int slot = t >> 1, h = t & 1;
+    const float4 *c4 = reinterpret_cast<const float4 *>(c);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) acc[k] = 0.0;
+    for (uint64_t i0 = b + slot; i0 < e; i0 += 32) {
+        const bool two = i0 + 16 < e;
+        uint32_t u0 = __ldcs(in_src + i0), u1 = two ? __ldcs(in_src + i0 + 16) : 0u;
+        if (u0 & kHotTag) u0 = hot_vertex[u0 & ~kHotTag];
+        if (u1 & kHotTag) u1 = hot_vertex[u1 & ~kHotTag];
+        const float4 a = c4[uint64_t(u0) * 2 + h];
+        const float4 z = two ? c4[uint64_t(u1) * 2 + h] : make_float4(0.f, 0.f, 0.f, 0.f);
+        acc[0] += double(a.x);
+        acc[1] += double(a.y);
+        acc[2] += double(a.z);
+        acc[3] += double(a.w);
+        if (two) {
+            acc[0] += double(z.x);
+            acc[1] += double(z.y);
+            acc[2] += double(z.z);
+            acc[3] += double(z.w);
+        }
     }
-    acc += __shfl_xor_sync(0xffffffffu, acc, 8);
-    acc += __shfl_xor_sync(0xffffffffu, acc, 16);
-    return acc;
+#pragma unroll
+    for (int o = 2; o < 32; o <<= 1)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
 }
 
 struct LaneParams {
@@ -114,13 +135,12 @@ __device__ __forceinline__ float lane_next(uint64_t v, int lane, double sum, con
     return float(nx);
 }
 
-// Short rows, 4 per warp: thread t takes row v0 + t / 8 and lane t % 8, and
-// sums that row's in-edges for its lane in edge order (4 edges loaded
-// before any is added; the 8 threads of a row read the same id and one
-// 32-byte contribution sector per edge).  Rows of kWideRow or more in-edges
-// (below the long-row threshold) are summed by the whole warp in the 4-slot
-// layout of row_lane_sum.  Every thread then writes its (row, lane) value;
-// per-block residual partials per lane in a fixed order.
+// Short rows, 16 per warp: threads 2q and 2q + 1 take row v0 + q, queries
+// 0-3 and 4-7 (one 16-byte contribution load per in-edge each), and add the
+// row's in-edges in edge order, 4 loaded before any is added.  Rows of
+// kWideRow or more in-edges (below the long-row threshold) are summed by
+// the whole warp (row_quad_sum).  Each thread then writes its row's four
+// values; per-block residual partials per query in a fixed order.
 constexpr uint32_t kWideRow = 32;
 constexpr int kRowThreads = 256;
 
@@ -131,10 +151,11 @@ __global__ void __launch_bounds__(kRowThreads) ppr8_rows_kernel(
     __shared__ double s_dm[kLanes];
     __shared__ double s_res[kLanes][kRowThreads / 32];
     lane_dangling(dpart, s_dm);
-    const int t = threadIdx.x & 31, warp = threadIdx.x >> 5, q = t >> 3, lane = t & 7;
+    const int t = threadIdx.x & 31, warp = threadIdx.x >> 5, q = t >> 1, h = t & 1;
+    const float4 *c4 = reinterpret_cast<const float4 *>(c);
     const uint64_t warps = uint64_t(gridDim.x) * (kRowThreads / 32);
-    double res = 0.0;  // this thread's lane
-    for (uint64_t v0 = ((blockIdx.x * uint64_t(kRowThreads) + threadIdx.x) >> 5) * 4; v0 < V; v0 += warps * 4) {
+    double res[4] = {0.0, 0.0, 0.0, 0.0};  // queries 4h .. 4h + 3
+    for (uint64_t v0 = ((blockIdx.x * uint64_t(kRowThreads) + threadIdx.x) >> 5) * 16; v0 < V; v0 += warps * 16) {
         const uint64_t v = v0 + q;
         uint64_t b = 0, e = 0;
         if (v < V) {
@@ -143,7 +164,7 @@ __global__ void __launch_bounds__(kRowThreads) ppr8_rows_kernel(
         }
         const uint64_t deg = e - b;
         const bool mine = v < V && deg < long_from;  // long rows: the chunk kernels
-        double acc = 0.0;
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
         if (mine && deg < kWideRow) {
             for (uint64_t i0 = b; i0 < e; i0 += 4) {
                 uint32_t u[4];
@@ -152,34 +173,53 @@ __global__ void __launch_bounds__(kRowThreads) ppr8_rows_kernel(
 #pragma unroll
                 for (int j = 0; j < 4; ++j)
                     if (u[j] & kHotTag) u[j] = hot_vertex[u[j] & ~kHotTag];
-                float cv[4];
-#pragma unroll
-                for (int j = 0; j < 4; ++j) cv[j] = (i0 + j < e) ? c[uint64_t(u[j]) * kLanes + lane] : 0.0f;
+                float4 cv[4];
 #pragma unroll
                 for (int j = 0; j < 4; ++j)
-                    if (i0 + j < e) acc += double(cv[j]);
+                    cv[j] = (i0 + j < e) ? c4[uint64_t(u[j]) * 2 + h] : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    if (i0 + j < e) {
+                        acc[0] += double(cv[j].x);
+                        acc[1] += double(cv[j].y);
+                        acc[2] += double(cv[j].z);
+                        acc[3] += double(cv[j].w);
+                    }
+                }
             }
         }
         // wide rows of the group, one at a time by the whole warp
-        uint32_t wide = __ballot_sync(0xffffffffu, mine && deg >= kWideRow && lane == 0);
+        uint32_t wide = __ballot_sync(0xffffffffu, mine && deg >= kWideRow && h == 0);
         while (wide) {
             const int src = __ffs(wide) - 1;
             wide &= wide - 1;
             const uint64_t bb = __shfl_sync(0xffffffffu, b, src), ee = __shfl_sync(0xffffffffu, e, src);
-            const double sum = row_lane_sum(in_src, hot_vertex, c, bb, ee, t);  // lane t % 8, in every thread
-            if (q == (src >> 3)) acc = sum;
+            double sum[4];
+            row_quad_sum(in_src, hot_vertex, c, bb, ee, t, sum);  // queries 4h .. 4h + 3, in every thread
+            if (q == (src >> 1))
+#pragma unroll
+                for (int k = 0; k < 4; ++k) acc[k] = sum[k];
         }
         if (mine) {
-            const float cur = x[v * kLanes + lane];
-            const float nx = lane_next(v, lane, acc, p, s_dm, cur);
-            nxt[v * kLanes + lane] = nx;
-            res += fabs(double(nx) - double(cur));
+            const float4 cur = reinterpret_cast<const float4 *>(x)[v * 2 + h];
+            const float cv[4] = {cur.x, cur.y, cur.z, cur.w};
+            float nx[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                nx[k] = lane_next(v, 4 * h + k, acc[k], p, s_dm, cv[k]);
+                res[k] += fabs(double(nx[k]) - double(cv[k]));
+            }
+            reinterpret_cast<float4 *>(nxt)[v * 2 + h] = make_float4(nx[0], nx[1], nx[2], nx[3]);
         }
     }
-    // fixed-order residual partials: the 4 row slots of the warp, then warps
-    res += __shfl_xor_sync(0xffffffffu, res, 8);
-    res += __shfl_xor_sync(0xffffffffu, res, 16);
-    if (t < kLanes) s_res[t][warp] = res;
+    // fixed-order residual partials: the 16 row slots of the warp, then warps
+#pragma unroll
+    for (int o = 2; o < 32; o <<= 1)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) res[k] += __shfl_xor_sync(0xffffffffu, res[k], o);
+    if (t < 2)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) s_res[4 * t + k][warp] = res[k];
     __syncthreads();
     if (threadIdx.x < kLanes) {
         double a = 0.0;
@@ -200,8 +240,11 @@ __global__ void ppr8_chunks_kernel(const uint64_t *__restrict__ in_off, const ui
         const LongRow lr = long_rows[task.x];
         const uint64_t b = in_off[lr.row] + uint64_t(task.y) * kLongChunk;
         const uint64_t e = min(b + kLongChunk, in_off[lr.row + 1]);
-        const double sum = row_lane_sum(in_src, hot_vertex, c, b, e, t);
-        if (t < kLanes) chunk_sum[(uint64_t(lr.first_chunk) + task.y) * kLanes + t] = sum;
+        double sum[4];
+        row_quad_sum(in_src, hot_vertex, c, b, e, t, sum);
+        if (t < 2)
+#pragma unroll
+            for (int k = 0; k < 4; ++k) chunk_sum[(uint64_t(lr.first_chunk) + task.y) * kLanes + 4 * t + k] = sum[k];
     }
 }
 
@@ -246,10 +289,11 @@ __global__ void ppr8_long_rows_kernel(const LongRow *__restrict__ long_rows, uin
 //                 t % 8: the 8 threads of a row read one id (a shared-memory
 //                 broadcast) and one 32-byte contribution sector per
 //                 in-edge, kUnroll edges in flight per thread; rows of >= 64
-//                 in-edges are taken by the whole warp in the 4-slot layout
-//                 of row_lane_sum;
-//   chunks     -- the 4-slot layout over the chunk's edges, one FP64 partial
-//                 per chunk and lane (summed by ppr8_long_rows_kernel).
+//                 in-edges are taken by the whole warp in a 4-slot layout
+//                 (thread t: edge slot t / 8, lane t % 8);
+//   chunks     -- the same 4-slot layout over the chunk's edges, one FP64
+//                 partial per chunk and lane (summed by
+//                 ppr8_long_rows_kernel).
 // Every sum is FP64 in a fixed edge order and the thread layout does not
 // depend on the lane count, so a query's bits do not depend on its
 // companions.  Residual partials are per block over a static task
