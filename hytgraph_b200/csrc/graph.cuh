@@ -48,6 +48,24 @@ __host__ __device__ __forceinline__ uint64_t task_first_edge(uint4 d) {
 __host__ __device__ __forceinline__ uint32_t task_edges(uint4 d) { return (d.y >> 8) & 0x7FFFFFu; }
 __host__ __device__ __forceinline__ bool task_is_chunk(uint4 d) { return (d.y >> 31) != 0; }
 
+#ifndef HYT_PULL_PREFETCH
+#define HYT_PULL_PREFETCH 1
+#endif
+#ifdef __CUDACC__
+// Warms L2 with the edge arrays a0 (and a1 when not NULL) of pull task d:
+// lane l touches the 128-byte lines at edges l*32, l*32 + 1024, ... of the
+// task, so the next task's streaming loads find their lines in L2.
+__device__ __forceinline__ void prefetch_task(uint4 d, const uint32_t *a0, const uint32_t *a1, int lane) {
+    if constexpr (HYT_PULL_PREFETCH) {
+        const uint64_t e0 = task_first_edge(d), n = task_edges(d);
+        for (uint64_t x = uint64_t(lane) * 32; x < n; x += 32 * 32) {
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(a0 + e0 + x));
+            if (a1) asm volatile("prefetch.global.L2 [%0];" ::"l"(a1 + e0 + x));
+        }
+    }
+}
+#endif
+
 struct LongRow {
     uint32_t row;
     uint32_t first_chunk;  // index of its first partial-sum slot

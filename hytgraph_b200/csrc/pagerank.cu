@@ -90,6 +90,7 @@ __device__ __forceinline__ void load_hot(const PRArgs &a, const PRBuffers &b, fl
 struct PRRange {
     const uint32_t *in_src;
     uint64_t chunk_begin, chunk_end, tile_begin, tile_end;
+    const uint4 *tasks;  // the graph's task descriptors (whole-graph launches; NULL: no prefetch)
 };
 
 __global__ void __launch_bounds__(kPRThreads, 1) pr_iterate_kernel(const PRArgs *__restrict__ args, PRRange rg) {
@@ -113,13 +114,17 @@ __global__ void __launch_bounds__(kPRThreads, 1) pr_iterate_kernel(const PRArgs 
 
     for (uint64_t task = uint64_t(blockIdx.x) * (kPRThreads / 32) + warp; task < total_tasks; task += nwarps) {
         double res = 0.0, dang = 0.0;
+        // whole-graph launches index the descriptors like their tasks
+        const uint64_t next = task + nwarps;
+        const uint4 nd = (rg.tasks && next < total_tasks) ? rg.tasks[next] : make_uint4(0, 0, 0, 0);
+        const uint4 *pf = rg.tasks ? &nd : nullptr;
         if (task < n_chunks) {
             const uint32_t row = chunk_task<true>(a, ps, b, rg.in_src, s_hot, rg.chunk_begin + task, pol, lane, res,
-                                                  dang);
+                                                  dang, pf);
             if (row != ~0u) slot_store(a, long_slot(row), dev::warp_sum(res), dev::warp_sum(dang), lane);
         } else {
             const uint64_t k = rg.tile_begin + (task - n_chunks);
-            tile_task<true>(a, ps, b, rg.in_src, s_hot, sv, k, pol, lane, res, dang);
+            tile_task<true>(a, ps, b, rg.in_src, s_hot, sv, k, pol, lane, res, dang, pf);
             slot_store(a, tile_slot(a, k), dev::warp_sum(res), dev::warp_sum(dang), lane);
         }
     }
@@ -501,7 +506,7 @@ static void pr_solve(GraphImpl &g, bool personalized, uint32_t source, float dam
                                : reinterpret_cast<const void *>(pr_iterate_kernel);
     const unsigned smem = static_cast<unsigned>(staged ? staged_shared_bytes(g.num_hot)
                                                        : pr_shared_bytes(g.num_hot, g.tile_cost));
-    PRRange full{g.in_sources.get(), 0, g.num_chunks, 0, g.num_tiles};
+    PRRange full{g.in_sources.get(), 0, g.num_chunks, 0, g.num_tiles, g.pull_tasks.get()};
     void *kargs[] = {&d_args, &full};
     const unsigned rgrid = pr_reduce_grid(a);
     auto launch = [&] {

@@ -268,7 +268,8 @@ __device__ __forceinline__ PRBuffers buffers(const PRArgs &a, uint32_t it) {
 template <bool kSmemHot>
 __device__ __forceinline__ uint32_t chunk_task(const PRArgs &a, const PRState &ps, const PRBuffers &b,
                                                const uint32_t *in_src, const float *s_hot, uint64_t ci, uint64_t pol,
-                                               int lane, double &res, double &dang) {
+                                               int lane, double &res, double &dang,
+                                               const uint4 *prefetch = nullptr) {
     const uint2 t = a.chunk_tasks[ci];
     const LongRow L = a.long_rows[t.x];
     const uint64_t rb = a.in_off[L.row], re = a.in_off[L.row + 1];
@@ -277,6 +278,7 @@ __device__ __forceinline__ uint32_t chunk_task(const PRArgs &a, const PRState &p
     dev::CSum acc;
     gather_span<kSmemHot>(in_src, b.ccur, s_hot, a.hot_vertex, lo, hi, pol, lane,
                           [&](uint32_t, float v) { acc.add(v); });
+    if (prefetch) prefetch_task(*prefetch, in_src, nullptr, lane);
     acc = dev::warp_reduce(acc);
     uint32_t last = 0;
     if (lane == 0) {
@@ -306,10 +308,13 @@ __device__ __forceinline__ uint32_t chunk_task(const PRArgs &a, const PRState &p
 // shared-memory slice sv, then summed lane-per-row (in-degree <
 // kWarpRowDegree) or warp-per-row, in edge order.  Must be called by all 32
 // lanes.
+// prefetch (optional): the warp's next pull task, whose edge lines are
+// warmed in L2 once this task's gathers are issued.
 template <bool kSmemHot>
 __device__ __forceinline__ void tile_task(const PRArgs &a, const PRState &ps, const PRBuffers &b,
                                           const uint32_t *in_src, const float *s_hot, float *sv, uint64_t k,
-                                          uint64_t pol, int lane, double &res, double &dang) {
+                                          uint64_t pol, int lane, double &res, double &dang,
+                                          const uint4 *prefetch = nullptr) {
     const uint32_t r0 = a.tile_start[k];
     const uint32_t r1 = a.tile_start[k + 1];
     if (r0 == r1) return;
@@ -329,6 +334,7 @@ __device__ __forceinline__ void tile_task(const PRArgs &a, const PRState &ps, co
     }
     gather_span<kSmemHot>(in_src, b.ccur, s_hot, a.hot_vertex, e0, e1, pol, lane,
                           [&](uint32_t i, float v) { sv[i] = v; });
+    if (prefetch) prefetch_task(*prefetch, in_src, nullptr, lane);
     __syncwarp();
     for (uint32_t rb = r0; rb < rl; rb += 32) {
         const uint32_t r = rb + lane;

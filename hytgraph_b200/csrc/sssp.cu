@@ -124,7 +124,7 @@ struct PullGraph {
     const LongRow *long_rows;
     const uint2 *chunk_tasks;
     const uint32_t *hot_vertex;
-    const uint4 *tasks;       // pull task descriptors (staged sweeps)
+    const uint4 *tasks;       // pull task descriptors (next-task prefetch, staged sweeps)
     uint64_t num_tiles, num_chunks;
     uint32_t tile_cost;
     uint32_t num_hot;
@@ -228,7 +228,12 @@ __global__ void __launch_bounds__(kPullThreads, 1) sssp_pull_kernel(const SSArgs
     const uint64_t pol = dev::policy_evict_last();
     const uint64_t total = pg.num_chunks + pg.num_tiles;
     const uint64_t nwarps = uint64_t(gridDim.x) * (kPullThreads / 32);
+    const uint32_t *pf_w = (WK == HYT_WEIGHTS_NONE) ? nullptr : pg.in_w;
     for (uint64_t task = uint64_t(blockIdx.x) * (kPullThreads / 32) + warp; task < total; task += nwarps) {
+        // the next task's descriptor now; its edge lines are warmed in L2
+        // once this task's gathers are issued
+        const uint64_t next = task + nwarps;
+        const uint4 nd = next < total ? pg.tasks[next] : make_uint4(0, 0, 0, 0);
         if (task < pg.num_chunks) {
             // slice of a long row: warp minimum, then one relaxation
             const uint2 t = pg.chunk_tasks[task];
@@ -238,6 +243,7 @@ __global__ void __launch_bounds__(kPullThreads, 1) sssp_pull_kernel(const SSArgs
             const uint64_t hi = (lo + kLongChunk < re) ? lo + kLongChunk : re;
             uint32_t best = a.inf;
             pull_span<WK>(a, pg, s_hot, lo, hi, pol, lane, [&](uint32_t, uint32_t c) { best = min(best, c); });
+            prefetch_task(nd, pg.in_src, pf_w, lane);
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(0xffffffffu, best, o));
             if (lane == 0 && pull_relax(a, rv, L.row, best)) append(rv.qnext, rv.qnext_size, L.row);
@@ -259,6 +265,7 @@ __global__ void __launch_bounds__(kPullThreads, 1) sssp_pull_kernel(const SSArgs
                 seen_p = __ldcg(a.dist + r0 + lane);
             }
             pull_span<WK>(a, pg, s_hot, e0, e1, pol, lane, [&](uint32_t i, uint32_t c) { sv[i] = c; });
+            prefetch_task(nd, pg.in_src, pf_w, lane);
             __syncwarp();
             for (uint32_t rb = r0; rb < rl; rb += 32) {
                 const uint32_t r = rb + lane;
