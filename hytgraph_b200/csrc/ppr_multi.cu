@@ -73,9 +73,14 @@ __global__ void ppr8_prep_kernel(const uint32_t *__restrict__ deg, const float *
 
 // Sums over in-edges [b, e) of c[u][4h .. 4h + 3], h = t % 2: thread t
 // takes edge slot t / 2 (16 slots) and adds its edges b + t/2, b + t/2 + 16,
-// ... in that order, four queries at a time from one 16-byte load (two
-// edges loaded before either is added); the slots are then folded by
+// ... in that order, four queries at a time from one 16-byte load
+// (kQuadInFlight edges loaded before any is added); the slots are then folded by
 // shuffles, so every thread of half h holds the four sums.
+#ifndef HYT_PPR_QUAD_INFLIGHT
+#define HYT_PPR_QUAD_INFLIGHT 4
+#endif
+constexpr int kQuadInFlight = HYT_PPR_QUAD_INFLIGHT;  // edges loaded per thread before any is added
+
 __device__ __forceinline__ void row_quad_sum(const uint32_t *__restrict__ in_src,
                                              const uint32_t *__restrict__ hot_vertex, const float *__restrict__ c,
                                              uint64_t b, uint64_t e, int t, double (&acc)[4]) {
@@ -83,22 +88,25 @@ __device__ __forceinline__ void row_quad_sum(const uint32_t *__restrict__ in_src
     const float4 *c4 = reinterpret_cast<const float4 *>(c);
 #pragma unroll
     for (int k = 0; k < 4; ++k) acc[k] = 0.0;
-    for (uint64_t i0 = b + slot; i0 < e; i0 += 32) {
-        const bool two = i0 + 16 < e;
-        uint32_t u0 = __ldcs(in_src + i0), u1 = two ? __ldcs(in_src + i0 + 16) : 0u;
-        if (u0 & kHotTag) u0 = hot_vertex[u0 & ~kHotTag];
-        if (u1 & kHotTag) u1 = hot_vertex[u1 & ~kHotTag];
-        const float4 a = c4[uint64_t(u0) * 2 + h];
-        const float4 z = two ? c4[uint64_t(u1) * 2 + h] : make_float4(0.f, 0.f, 0.f, 0.f);
-        acc[0] += double(a.x);
-        acc[1] += double(a.y);
-        acc[2] += double(a.z);
-        acc[3] += double(a.w);
-        if (two) {
-            acc[0] += double(z.x);
-            acc[1] += double(z.y);
-            acc[2] += double(z.z);
-            acc[3] += double(z.w);
+    for (uint64_t i0 = b + slot; i0 < e; i0 += 16 * kQuadInFlight) {
+        uint32_t u[kQuadInFlight];
+#pragma unroll
+        for (int j = 0; j < kQuadInFlight; ++j) u[j] = (i0 + 16 * j < e) ? __ldcs(in_src + i0 + 16 * j) : 0u;
+#pragma unroll
+        for (int j = 0; j < kQuadInFlight; ++j)
+            if (u[j] & kHotTag) u[j] = hot_vertex[u[j] & ~kHotTag];
+        float4 v[kQuadInFlight];
+#pragma unroll
+        for (int j = 0; j < kQuadInFlight; ++j)
+            v[j] = (i0 + 16 * j < e) ? c4[uint64_t(u[j]) * 2 + h] : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int j = 0; j < kQuadInFlight; ++j) {
+            if (i0 + 16 * j < e) {
+                acc[0] += double(v[j].x);
+                acc[1] += double(v[j].y);
+                acc[2] += double(v[j].z);
+                acc[3] += double(v[j].w);
+            }
         }
     }
 #pragma unroll
