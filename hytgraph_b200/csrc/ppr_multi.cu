@@ -121,14 +121,37 @@ struct LaneParams {
     double d;                  // damping
 };
 
-// Per-lane dangling mass from the prep partials (fixed order).
-__device__ __forceinline__ void lane_dangling(const double *__restrict__ dpart, double *s_dm) {
-    if (threadIdx.x < kLanes) {
-        double a = 0.0;
-        for (int i = 0; i < kPartBlocks; ++i) a += dpart[i * kLanes + threadIdx.x];
-        s_dm[threadIdx.x] = a;
-    }
+// The iteration's per-lane dangling mass (dm[8], summed once per
+// iteration by ppr8_lane_sums_kernel), into shared memory.
+__device__ __forceinline__ void lane_dangling(const double *__restrict__ dm, double *s_dm) {
+    if (threadIdx.x < kLanes) s_dm[threadIdx.x] = dm[threadIdx.x];
     __syncthreads();
+}
+
+// Fixed-order per-lane sums of per-block partials: out[l] = sum over
+// a[i][l] (i < na) and b[i][l] (i < nb).  One block of kSumThreads: thread t
+// sums group t / 8 (partials g, g + G, g + 2G, ...; G = kSumThreads / 8),
+// then thread l < 8 adds the G group sums in order.  Every thread holds a
+// few dependent adds instead of one thread walking all partials (one L2
+// round trip per partial).
+constexpr int kSumThreads = 1024;
+
+__global__ void __launch_bounds__(kSumThreads) ppr8_lane_sums_kernel(const double *__restrict__ a, int na,
+                                                                     const double *__restrict__ b, int nb,
+                                                                     double *__restrict__ out) {
+    constexpr int kGroups = kSumThreads / kLanes;
+    __shared__ double s[kGroups][kLanes];
+    const int l = threadIdx.x & (kLanes - 1), g = threadIdx.x / kLanes;
+    double x = 0.0;
+    for (int i = g; i < na; i += kGroups) x += a[size_t(i) * kLanes + l];
+    for (int i = g; i < nb; i += kGroups) x += b[size_t(i) * kLanes + l];
+    s[g][l] = x;
+    __syncthreads();
+    if (threadIdx.x < kLanes) {
+        double r = 0.0;
+        for (int j = 0; j < kGroups; ++j) r += s[j][threadIdx.x];
+        out[threadIdx.x] = r;
+    }
 }
 
 __device__ __forceinline__ float lane_next(uint64_t v, int lane, double sum, const LaneParams &p, const double *s_dm,
@@ -432,17 +455,6 @@ __global__ void __launch_bounds__(kTaskThreads, 1)
     }
 }
 
-// residual[l] = rows partials then long-row partials, each in block order.
-__global__ void ppr8_residual_kernel(const double *__restrict__ rows, int nrows, const double *__restrict__ longs,
-                                     int nlong, double *__restrict__ residual) {
-    if (threadIdx.x < kLanes) {
-        double a = 0.0;
-        for (int i = 0; i < nrows; ++i) a += rows[i * kLanes + threadIdx.x];
-        for (int i = 0; i < nlong; ++i) a += longs[i * kLanes + threadIdx.x];
-        residual[threadIdx.x] = a;
-    }
-}
-
 __global__ void ppr8_init_kernel(float *__restrict__ x, uint64_t V, LaneParams p, int k) {
     for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < V * kLanes;
          i += uint64_t(gridDim.x) * blockDim.x) {
@@ -507,7 +519,7 @@ void ppr_multi(GraphImpl &g, const uint32_t *sources, uint32_t k, float restart,
     Scratch<float> xa(V * kLanes, s), xb(V * kLanes, s), c(V * kLanes, s);
     Scratch<double> dpart(uint64_t(kPartBlocks) * kLanes, s), rpart(uint64_t(rows_grid) * kLanes, s),
         lpart(uint64_t(std::max(long_grid, 1u)) * kLanes, s), chunk_sum(std::max<uint64_t>(chunks, 1) * kLanes, s),
-        residual(kLanes, s);
+        residual(kLanes, s), dm(kLanes, s);
     Scratch<uint32_t> err(1, s);
     HYT_CUDA(cudaMemsetAsync(err.get(), 0, sizeof(uint32_t), s));
     double *h_res = reinterpret_cast<double *>(g.host_scratch.ptr);  // 64 pinned bytes
@@ -521,32 +533,33 @@ void ppr_multi(GraphImpl &g, const uint32_t *sources, uint32_t k, float restart,
     uint64_t launches = 1;
     for (uint32_t it = 0; it < max_iter && p.active; ++it) {
         ppr8_prep_kernel<<<kPartBlocks, 256, 0, s>>>(g.out_degree.get(), x, V, c.get(), dpart.get());
-        launches += 2;
+        ppr8_lane_sums_kernel<<<1, kSumThreads, 0, s>>>(dpart.get(), kPartBlocks, nullptr, 0, dm.get());
+        launches += 3;
         if (staged) {
             ppr8_tasks_kernel<<<rows_grid, kTaskThreads, smem, s>>>(
                 g.pull_tasks.get(), g.num_chunks + g.num_tiles, g.in_offsets.get(), g.in_sources.get(),
-                g.hot_vertex.get(), g.num_hot, g.long_rows.get(), c.get(), x, p, dpart.get(), nx, chunk_sum.get(),
+                g.hot_vertex.get(), g.num_hot, g.long_rows.get(), c.get(), x, p, dm.get(), nx, chunk_sum.get(),
                 rpart.get(), err.get());
             if (chunks) {
                 ppr8_long_rows_kernel<<<long_grid, 256, 0, s>>>(g.long_rows.get(), g.num_long, chunk_sum.get(), x, p,
-                                                                dpart.get(), nx, lpart.get());
+                                                                dm.get(), nx, lpart.get());
                 ++launches;
             }
         } else {
             ppr8_rows_kernel<<<rows_grid, kRowThreads, 0, s>>>(g.in_offsets.get(), g.in_sources.get(),
                                                                g.hot_vertex.get(), c.get(), x, V, long_from, p,
-                                                               dpart.get(), nx, rpart.get());
+                                                               dm.get(), nx, rpart.get());
         }
         if (chunks && !staged) {
             ppr8_chunks_kernel<<<grid_sm(8), 256, 0, s>>>(g.in_offsets.get(), g.in_sources.get(), g.hot_vertex.get(),
                                                           c.get(), g.long_rows.get(), g.chunk_tasks.get(), chunks,
                                                           chunk_sum.get());
             ppr8_long_rows_kernel<<<long_grid, 256, 0, s>>>(g.long_rows.get(), g.num_long, chunk_sum.get(), x, p,
-                                                            dpart.get(), nx, lpart.get());
+                                                            dm.get(), nx, lpart.get());
             launches += 2;
         }
-        ppr8_residual_kernel<<<1, 32, 0, s>>>(rpart.get(), int(rows_grid), lpart.get(), int(chunks ? long_grid : 0),
-                                              residual.get());
+        ppr8_lane_sums_kernel<<<1, kSumThreads, 0, s>>>(rpart.get(), int(rows_grid), lpart.get(),
+                                                        int(chunks ? long_grid : 0), residual.get());
         ++launches;
         HYT_CUDA(cudaGetLastError());
         HYT_CUDA(cudaMemcpyAsync(h_res, residual.get(), kLanes * 8, cudaMemcpyDeviceToHost, s));
