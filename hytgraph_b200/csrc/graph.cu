@@ -336,7 +336,7 @@ size_t GraphImpl::device_bytes() const {
          pull_tasks.bytes();
     for (int i = 0; i < 2; ++i) b += rank[i].bytes() + contrib[i].bytes() + queue[i].bytes() + far[i].bytes();
     b += partial.bytes() + ticket.bytes() + pr_state.bytes() + dist.bytes() + stamp.bytes() + hub_tasks.bytes() +
-         sssp_state.bytes() + ms_dist.bytes() + ms_state.bytes();
+         sssp_state.bytes() + ms_dist.bytes() + ms_state.bytes() + ppr_wide.bytes();
     return b;
 }
 

@@ -158,6 +158,9 @@ struct GraphImpl {
     GraphArray<uint32_t> far[2];
     GraphArray<uint2> hub_tasks;
     GraphArray<unsigned char> sssp_state;
+    GraphArray<uint32_t> ppr_wide;         // packed PPR: rows of 32+ in-edges below the long-row threshold
+    uint64_t ppr_wide_n = 0;
+    bool ppr_wide_ready = false;
     GraphArray<uint32_t> ms_dist;          // multi-source labels [V][8]
     GraphArray<unsigned char> ms_state;
     PinnedArray<uint64_t> host_scratch;  // small pinned readback area

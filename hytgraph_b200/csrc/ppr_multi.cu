@@ -25,6 +25,7 @@
 
 #include "common.cuh"
 #include "graph.cuh"
+#include "prims.cuh"
 #include "scratch.cuh"
 #include "solvers.cuh"
 #include "stage.cuh"
@@ -129,7 +130,7 @@ __device__ __forceinline__ void lane_dangling(const double *__restrict__ dm, dou
 }
 
 // Fixed-order per-lane sums of per-block partials: out[l] = sum over
-// a[i][l] (i < na) and b[i][l] (i < nb).  One block of kSumThreads: thread t
+// a[i][l] (i < na), b[i][l] (i < nb) and w[i][l] (i < nw).  One block of kSumThreads: thread t
 // sums group t / 8 (partials g, g + G, g + 2G, ...; G = kSumThreads / 8),
 // then thread l < 8 adds the G group sums in order.  Every thread holds a
 // few dependent adds instead of one thread walking all partials (one L2
@@ -138,6 +139,7 @@ constexpr int kSumThreads = 1024;
 
 __global__ void __launch_bounds__(kSumThreads) ppr8_lane_sums_kernel(const double *__restrict__ a, int na,
                                                                      const double *__restrict__ b, int nb,
+                                                                     const double *__restrict__ w, int nw,
                                                                      double *__restrict__ out) {
     constexpr int kGroups = kSumThreads / kLanes;
     __shared__ double s[kGroups][kLanes];
@@ -145,6 +147,7 @@ __global__ void __launch_bounds__(kSumThreads) ppr8_lane_sums_kernel(const doubl
     double x = 0.0;
     for (int i = g; i < na; i += kGroups) x += a[size_t(i) * kLanes + l];
     for (int i = g; i < nb; i += kGroups) x += b[size_t(i) * kLanes + l];
+    for (int i = g; i < nw; i += kGroups) x += w[size_t(i) * kLanes + l];
     s[g][l] = x;
     __syncthreads();
     if (threadIdx.x < kLanes) {
@@ -166,12 +169,12 @@ __device__ __forceinline__ float lane_next(uint64_t v, int lane, double sum, con
     return float(nx);
 }
 
-// Short rows, 16 per warp: threads 2q and 2q + 1 take row v0 + q, queries
-// 0-3 and 4-7 (one 16-byte contribution load per in-edge each), and add the
-// row's in-edges in edge order, 4 loaded before any is added.  Rows of
-// kWideRow or more in-edges (below the long-row threshold) are summed by
-// the whole warp (row_quad_sum).  Each thread then writes its row's four
-// values; per-block residual partials per query in a fixed order.
+// Short rows (fewer than kWideRow in-edges), 16 per warp: threads 2q and
+// 2q + 1 take row v0 + q, queries 0-3 and 4-7 (one 16-byte contribution
+// load per in-edge each), and add the row's in-edges in edge order, 4
+// loaded before any is added.  Each thread then writes its row's four
+// values; per-block residual partials per query in a fixed order.  Wider
+// rows go to ppr8_wide_kernel, long rows to the chunk kernels.
 constexpr uint32_t kWideRow = 32;
 constexpr int kRowThreads = 256;
 
@@ -194,9 +197,10 @@ __global__ void __launch_bounds__(kRowThreads) ppr8_rows_kernel(
             e = in_off[v + 1];
         }
         const uint64_t deg = e - b;
-        const bool mine = v < V && deg < long_from;  // long rows: the chunk kernels
+        // wide rows: ppr8_wide_kernel; long rows: the chunk kernels
+        const bool mine = v < V && deg < kWideRow && deg < long_from;
         double acc[4] = {0.0, 0.0, 0.0, 0.0};
-        if (mine && deg < kWideRow) {
+        if (mine) {
             for (uint64_t i0 = b; i0 < e; i0 += 4) {
                 uint32_t u[4];
 #pragma unroll
@@ -218,18 +222,6 @@ __global__ void __launch_bounds__(kRowThreads) ppr8_rows_kernel(
                     }
                 }
             }
-        }
-        // wide rows of the group, one at a time by the whole warp
-        uint32_t wide = __ballot_sync(0xffffffffu, mine && deg >= kWideRow && h == 0);
-        while (wide) {
-            const int src = __ffs(wide) - 1;
-            wide &= wide - 1;
-            const uint64_t bb = __shfl_sync(0xffffffffu, b, src), ee = __shfl_sync(0xffffffffu, e, src);
-            double sum[4];
-            row_quad_sum(in_src, hot_vertex, c, bb, ee, t, sum);  // queries 4h .. 4h + 3, in every thread
-            if (q == (src >> 1))
-#pragma unroll
-                for (int k = 0; k < 4; ++k) acc[k] = sum[k];
         }
         if (mine) {
             const float4 cur = reinterpret_cast<const float4 *>(x)[v * 2 + h];
@@ -259,28 +251,86 @@ __global__ void __launch_bounds__(kRowThreads) ppr8_rows_kernel(
     }
 }
 
-// One warp per chunk of a long row: per-lane partial sums.
+// Rows of kWideRow or more in-edges below the long-row threshold (the
+// graph's list `wide`), one per warp across the whole grid: hub order puts
+// them together at the front of the vertex range, where warps that took
+// them 16 at a time in the rows pass held up its end.  The whole warp sums
+// a row (row_quad_sum); threads 0 and 1 write queries 0-3 and 4-7.
+__global__ void __launch_bounds__(kRowThreads) ppr8_wide_kernel(
+    const uint32_t *__restrict__ wide, uint64_t num_wide, const uint64_t *__restrict__ in_off,
+    const uint32_t *__restrict__ in_src, const uint32_t *__restrict__ hot_vertex, const float *__restrict__ c,
+    const float *__restrict__ x, LaneParams p, const double *__restrict__ dm, float *__restrict__ nxt,
+    double *__restrict__ wpart) {
+    __shared__ double s_dm[kLanes];
+    __shared__ double s_res[kLanes][kRowThreads / 32];
+    lane_dangling(dm, s_dm);
+    const int t = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t warps = uint64_t(gridDim.x) * (kRowThreads / 32);
+    double res[4] = {0.0, 0.0, 0.0, 0.0};
+    for (uint64_t i = (blockIdx.x * uint64_t(kRowThreads) + threadIdx.x) >> 5; i < num_wide; i += warps) {
+        const uint64_t v = wide[i];
+        double sum[4];
+        row_quad_sum(in_src, hot_vertex, c, in_off[v], in_off[v + 1], t, sum);  // queries 4h .. 4h + 3
+        if (t < 2) {
+            const float4 cur = reinterpret_cast<const float4 *>(x)[v * 2 + t];
+            const float cv[4] = {cur.x, cur.y, cur.z, cur.w};
+            float nx[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                nx[q] = lane_next(v, 4 * t + q, sum[q], p, s_dm, cv[q]);
+                res[q] += fabs(double(nx[q]) - double(cv[q]));
+            }
+            reinterpret_cast<float4 *>(nxt)[v * 2 + t] = make_float4(nx[0], nx[1], nx[2], nx[3]);
+        }
+    }
+    if (t < 2)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) s_res[4 * t + q][warp] = res[q];
+    __syncthreads();
+    if (threadIdx.x < kLanes) {
+        double a = 0.0;
+        for (int w = 0; w < kRowThreads / 32; ++w) a += s_res[threadIdx.x][w];
+        wpart[blockIdx.x * kLanes + threadIdx.x] = a;
+    }
+}
+
+// flags[v] = 1 for rows with kWideRow <= in-degree < long_from.
+__global__ void ppr8_wide_flags_kernel(const uint64_t *__restrict__ in_off, uint64_t V, uint64_t long_from,
+                                       uint8_t *__restrict__ flags) {
+    for (uint64_t v = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; v < V; v += uint64_t(gridDim.x) * blockDim.x) {
+        const uint64_t d = in_off[v + 1] - in_off[v];
+        flags[v] = (d >= kWideRow && d < long_from) ? 1 : 0;
+    }
+}
+
+// One warp per piece of a long-row chunk (each chunk cut into `pieces`
+// equal pieces, so that graphs with few chunks still fill the GPU):
+// per-lane partial sums, stored at (chunk * pieces + piece).
 __global__ void ppr8_chunks_kernel(const uint64_t *__restrict__ in_off, const uint32_t *__restrict__ in_src,
                                    const uint32_t *__restrict__ hot_vertex, const float *__restrict__ c,
                                    const LongRow *__restrict__ long_rows, const uint2 *__restrict__ tasks,
-                                   uint64_t num_tasks, double *__restrict__ chunk_sum) {
+                                   uint64_t num_tasks, uint32_t pieces, double *__restrict__ chunk_sum) {
     const int t = threadIdx.x & 31;
     const uint64_t warps = uint64_t(gridDim.x) * (blockDim.x >> 5);
-    for (uint64_t k = (blockIdx.x * uint64_t(blockDim.x) + threadIdx.x) >> 5; k < num_tasks; k += warps) {
-        const uint2 task = tasks[k];
+    const uint64_t piece_edges = (kLongChunk + pieces - 1) / pieces;
+    for (uint64_t k = (blockIdx.x * uint64_t(blockDim.x) + threadIdx.x) >> 5; k < num_tasks * pieces; k += warps) {
+        const uint64_t ci = k / pieces, pc = k % pieces;
+        const uint2 task = tasks[ci];
         const LongRow lr = long_rows[task.x];
-        const uint64_t b = in_off[lr.row] + uint64_t(task.y) * kLongChunk;
-        const uint64_t e = min(b + kLongChunk, in_off[lr.row + 1]);
+        const uint64_t cb = in_off[lr.row] + uint64_t(task.y) * kLongChunk;
+        const uint64_t ce = min(cb + kLongChunk, in_off[lr.row + 1]);
+        const uint64_t b = min(cb + pc * piece_edges, ce), e = min(b + piece_edges, ce);
         double sum[4];
         row_quad_sum(in_src, hot_vertex, c, b, e, t, sum);
         if (t < 2)
 #pragma unroll
-            for (int k = 0; k < 4; ++k) chunk_sum[(uint64_t(lr.first_chunk) + task.y) * kLanes + 4 * t + k] = sum[k];
+            for (int q = 0; q < 4; ++q)
+                chunk_sum[((uint64_t(lr.first_chunk) + task.y) * pieces + pc) * kLanes + 4 * t + q] = sum[q];
     }
 }
 
 // One warp per long row: chunk partials in order, next values, residual.
-__global__ void ppr8_long_rows_kernel(const LongRow *__restrict__ long_rows, uint64_t num_long,
+__global__ void ppr8_long_rows_kernel(const LongRow *__restrict__ long_rows, uint64_t num_long, uint32_t pieces,
                                       const double *__restrict__ chunk_sum, const float *__restrict__ x, LaneParams p,
                                       const double *__restrict__ dpart, float *__restrict__ nxt,
                                       double *__restrict__ rpart) {
@@ -294,7 +344,8 @@ __global__ void ppr8_long_rows_kernel(const LongRow *__restrict__ long_rows, uin
         const LongRow lr = long_rows[i];
         if (t < kLanes) {
             double sum = 0.0;
-            for (uint32_t k = 0; k < lr.num_chunks; ++k) sum += chunk_sum[(uint64_t(lr.first_chunk) + k) * kLanes + t];
+            const uint64_t first = uint64_t(lr.first_chunk) * pieces, n = uint64_t(lr.num_chunks) * pieces;
+            for (uint64_t k = 0; k < n; ++k) sum += chunk_sum[(first + k) * kLanes + t];
             const uint64_t v = lr.row;
             const float cur = x[v * kLanes + t];
             const float nx = lane_next(v, t, sum, p, s_dm, cur);
@@ -516,10 +567,31 @@ void ppr_multi(GraphImpl &g, const uint32_t *sources, uint32_t k, float restart,
     const uint64_t chunks = g.num_long ? g.num_chunks : 0;
     const uint64_t long_from = g.num_long ? g.tile_cost : ~uint64_t(0);
     const unsigned long_grid = g.num_long ? grid_for(g.num_long * 32, 256) : 0;
+    // chunks cut into pieces until there are enough warp tasks to fill the
+    // GPU (a function of the graph alone, so results do not depend on it)
+    uint32_t pieces = 1;
+    if (!staged)
+        while (pieces < 8 && chunks * pieces < 16384) pieces *= 2;
+    // the graph's wide rows (once per graph)
+    if (!staged && !g.ppr_wide_ready) {
+        Scratch<uint8_t> flags(V, s);
+        ppr8_wide_flags_kernel<<<grid_for(V, 256), 256, 0, s>>>(g.in_offsets.get(), V, long_from, flags.get());
+        HYT_CUDA(cudaGetLastError());
+        g.ppr_wide.allocate(std::max<uint64_t>(V, 1));
+        g.ppr_wide_n = prims::select_flagged_index(flags.get(), g.ppr_wide.get(), V, s);
+        g.ppr_wide_ready = true;
+    }
+    const uint64_t num_wide = staged ? 0 : g.ppr_wide_n;
+    static int wide_per_sm = 0;
+    if (wide_per_sm == 0) {
+        HYT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&wide_per_sm, ppr8_wide_kernel, kRowThreads, 0));
+        wide_per_sm = std::max(wide_per_sm, 1);
+    }
+    const unsigned wide_grid = num_wide ? grid_sm(wide_per_sm) : 0;
     Scratch<float> xa(V * kLanes, s), xb(V * kLanes, s), c(V * kLanes, s);
     Scratch<double> dpart(uint64_t(kPartBlocks) * kLanes, s), rpart(uint64_t(rows_grid) * kLanes, s),
-        lpart(uint64_t(std::max(long_grid, 1u)) * kLanes, s), chunk_sum(std::max<uint64_t>(chunks, 1) * kLanes, s),
-        residual(kLanes, s), dm(kLanes, s);
+        lpart(uint64_t(std::max(long_grid, 1u)) * kLanes, s), chunk_sum(std::max<uint64_t>(chunks * pieces, 1) * kLanes, s),
+        residual(kLanes, s), dm(kLanes, s), wpart(uint64_t(std::max(wide_grid, 1u)) * kLanes, s);
     Scratch<uint32_t> err(1, s);
     HYT_CUDA(cudaMemsetAsync(err.get(), 0, sizeof(uint32_t), s));
     double *h_res = reinterpret_cast<double *>(g.host_scratch.ptr);  // 64 pinned bytes
@@ -533,7 +605,7 @@ void ppr_multi(GraphImpl &g, const uint32_t *sources, uint32_t k, float restart,
     uint64_t launches = 1;
     for (uint32_t it = 0; it < max_iter && p.active; ++it) {
         ppr8_prep_kernel<<<kPartBlocks, 256, 0, s>>>(g.out_degree.get(), x, V, c.get(), dpart.get());
-        ppr8_lane_sums_kernel<<<1, kSumThreads, 0, s>>>(dpart.get(), kPartBlocks, nullptr, 0, dm.get());
+        ppr8_lane_sums_kernel<<<1, kSumThreads, 0, s>>>(dpart.get(), kPartBlocks, nullptr, 0, nullptr, 0, dm.get());
         launches += 3;
         if (staged) {
             ppr8_tasks_kernel<<<rows_grid, kTaskThreads, smem, s>>>(
@@ -541,25 +613,32 @@ void ppr_multi(GraphImpl &g, const uint32_t *sources, uint32_t k, float restart,
                 g.hot_vertex.get(), g.num_hot, g.long_rows.get(), c.get(), x, p, dm.get(), nx, chunk_sum.get(),
                 rpart.get(), err.get());
             if (chunks) {
-                ppr8_long_rows_kernel<<<long_grid, 256, 0, s>>>(g.long_rows.get(), g.num_long, chunk_sum.get(), x, p,
-                                                                dm.get(), nx, lpart.get());
+                ppr8_long_rows_kernel<<<long_grid, 256, 0, s>>>(g.long_rows.get(), g.num_long, 1u, chunk_sum.get(),
+                                                                x, p, dm.get(), nx, lpart.get());
                 ++launches;
             }
         } else {
             ppr8_rows_kernel<<<rows_grid, kRowThreads, 0, s>>>(g.in_offsets.get(), g.in_sources.get(),
                                                                g.hot_vertex.get(), c.get(), x, V, long_from, p,
                                                                dm.get(), nx, rpart.get());
+            if (num_wide) {
+                ppr8_wide_kernel<<<wide_grid, kRowThreads, 0, s>>>(g.ppr_wide.get(), num_wide, g.in_offsets.get(),
+                                                                   g.in_sources.get(), g.hot_vertex.get(), c.get(), x,
+                                                                   p, dm.get(), nx, wpart.get());
+                ++launches;
+            }
         }
         if (chunks && !staged) {
             ppr8_chunks_kernel<<<grid_sm(8), 256, 0, s>>>(g.in_offsets.get(), g.in_sources.get(), g.hot_vertex.get(),
                                                           c.get(), g.long_rows.get(), g.chunk_tasks.get(), chunks,
-                                                          chunk_sum.get());
-            ppr8_long_rows_kernel<<<long_grid, 256, 0, s>>>(g.long_rows.get(), g.num_long, chunk_sum.get(), x, p,
-                                                            dm.get(), nx, lpart.get());
+                                                          pieces, chunk_sum.get());
+            ppr8_long_rows_kernel<<<long_grid, 256, 0, s>>>(g.long_rows.get(), g.num_long, pieces, chunk_sum.get(), x,
+                                                            p, dm.get(), nx, lpart.get());
             launches += 2;
         }
         ppr8_lane_sums_kernel<<<1, kSumThreads, 0, s>>>(rpart.get(), int(rows_grid), lpart.get(),
-                                                        int(chunks ? long_grid : 0), residual.get());
+                                                        int(chunks ? long_grid : 0), wpart.get(), int(wide_grid),
+                                                        residual.get());
         ++launches;
         HYT_CUDA(cudaGetLastError());
         HYT_CUDA(cudaMemcpyAsync(h_res, residual.get(), kLanes * 8, cudaMemcpyDeviceToHost, s));
