@@ -211,7 +211,10 @@ __device__ __forceinline__ void pull_span(const SSArgs &a, const PullGraph &pg, 
     }
 }
 
-constexpr int kPullThreads = 1024;  // one CTA per SM, like the PageRank kernel
+#ifndef HYT_PULL_THREADS
+#define HYT_PULL_THREADS 1024
+#endif
+constexpr int kPullThreads = HYT_PULL_THREADS;  // one CTA per SM, like the PageRank kernel
 
 template <int WK>
 __global__ void __launch_bounds__(kPullThreads, 1) sssp_pull_kernel(const SSArgs *__restrict__ args, PullGraph pg) {
