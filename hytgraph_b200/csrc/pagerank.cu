@@ -18,16 +18,19 @@
 //                   tile_cost; each warp writes a compensated partial, the
 //                   last arriving warp of a row merges the partials in chunk
 //                   order;
-//   tile tasks   -- merge-path tiles of consecutive shorter rows; the tile's
-//                   contributions are gathered, then summed lane-per-row
-//                   (in-degree < kWarpRowDegree) or warp-per-row.
-// In HBM the source ids of each task are staged in shared memory by bulk
-// copies (cp.async.bulk, completion on an mbarrier), double-buffered per
-// warp (stage.cuh): while a warp gathers and sums one unit (a tile, or a
-// 512-edge piece of a chunk), the copy of its next unit is in flight, so the
-// id stream never stalls the gathers and no registers hold ids.  The
-// out-of-HBM solver, whose ids come from staging slots or mapped host
-// memory, loads them with 128-bit streaming loads instead.
+//   tile tasks   -- merge-path tiles of consecutive shorter rows (512
+//                   units by default); the tile's contributions are
+//                   gathered, 16 per lane in flight, into the warp's
+//                   shared-memory slice, then summed lane-per-row (in-degree
+//                   < kWarpRowDegree) or warp-per-row.  The first 32 rows'
+//                   bounds, ranks and out-degrees are loaded with the
+//                   gathers, and before its row phase a warp warms L2 with
+//                   its next task's id lines.
+// With HYT_STAGED=1 (256-unit tiles) pr_staged_kernel stages each task's
+// source ids in shared memory by bulk copies (cp.async.bulk, completion on
+// an mbarrier; stage.cuh) instead; on R-MAT graphs it ran slower than the
+// register path.  The out-of-HBM solver, whose ids come from staging slots
+// or mapped host memory, runs the register path over its partitions.
 //
 // Results are deterministic: every row sum has a fixed association order,
 // and the FP64 residual and dangling mass are summed in a fixed slot order

@@ -25,8 +25,15 @@
 // grid-wide kernel, so no warp owns more than ~2K edges of a round.  Each
 // lane keeps 4 edges in flight through loads and atomics (relax_batch).  A
 // vertex joins a frontier once per round (round stamp) and the far pile once
-// per phase (phase stamp), appended with one warp-aggregated atomic.  All round state lives on the device; inside a
-// CUDA graph the rounds run as a conditional while-loop.
+// per phase (phase stamp), appended with one warp-aggregated atomic.
+//
+// With one bucket and a CSC, a round whose frontier carries more than
+// E / pull_div out-edges runs as a pull sweep over the CSC instead
+// (sssp_pull_kernel: 512-unit tiles, labels gathered 8 per lane in flight,
+// tile rows written with plain stores).  All round state lives on the
+// device; inside a CUDA graph the rounds run as a conditional while-loop
+// (expand, hub chunks, pull sweep, round close), instantiated once per
+// graph and launched again by later solves.
 #include <cooperative_groups.h>
 
 #include <algorithm>
