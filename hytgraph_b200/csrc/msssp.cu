@@ -17,8 +17,11 @@
 //   pull sweep -- when the frontier's out-edges exceed E / 4, every row
 //                 takes, per lane, the minimum of d[u] + w over its
 //                 in-edges: one id and one 32-byte label row per in-edge
-//                 for all lanes.  Source ids are staged by bulk copies
-//                 (stage.cuh) as in the single-source sweep.
+//                 for all lanes, 4 label rows in flight per thread; ids
+//                 read in place on the default 512-unit tiles, or staged
+//                 by bulk copies (stage.cuh) on 256-unit tiles
+//                 (HYT_STAGED=1).  Tile rows are written with plain stores
+//                 (one writer per row during a sweep).
 // Per edge the memory traffic is about that of one single-source
 // relaxation, whatever the number of lanes; the rounds are those of the
 // deepest source.  Rounds run as a CUDA-graph conditional while-loop.
