@@ -7,7 +7,7 @@
 //   PageRank: |next(v) - current(v)| of one synchronous pull step,
 //     next(v) = (1 - d)/n + d * dangling / n + d * sum_{u->v} current(u)/deg(u);
 //     here the sums run in FP64 (one warp per row, a fixed-order warp
-//     tree; dangling mass by per-block partials summed in block order), so
+//     tree; dangling mass by per-block partials summed in a fixed order), so
 //     the values are deterministic and agree with the reference's FP32 to
 //     within its rounding;
 //   SSSP: current - candidate when both are finite and the improvement
@@ -71,9 +71,15 @@ __device__ __forceinline__ double row_sum(const uint32_t *__restrict__ in_src, c
     return acc;
 }
 
-__device__ __forceinline__ double base_share(const double *__restrict__ partial, int parts, uint64_t V, double d) {
+// (1 - d)/n + d * dangling / n from the per-block dangling partials, summed
+// by the block's first warp in a fixed order (lane l: partials l, l + 32,
+// ...; then a shuffle tree), so no thread waits on one load per partial.
+// Called by the first 32 threads; the result is in all of them.
+__device__ __forceinline__ double base_share(const double *__restrict__ partial, int parts, uint64_t V, double d,
+                                             int lane) {
     double dm = 0.0;
-    for (int i = 0; i < parts; ++i) dm += partial[i];
+    for (int i = lane; i < parts; i += 32) dm += partial[i];
+    dm = dev::warp_sum(dm);
     return (1.0 - d) / double(V) + d * dm / double(V);
 }
 
@@ -83,7 +89,10 @@ __global__ void pagerank_contrib_kernel(const uint64_t *__restrict__ in_off, con
                                         const float *__restrict__ rank, uint64_t V, uint64_t long_from, double damping,
                                         const double *__restrict__ partial, int parts, double *__restrict__ out) {
     __shared__ double s_share;
-    if (threadIdx.x == 0) s_share = base_share(partial, parts, V, damping);
+    if (threadIdx.x < 32) {
+        const double sh = base_share(partial, parts, V, damping, threadIdx.x);
+        if (threadIdx.x == 0) s_share = sh;
+    }
     __syncthreads();
     const double share = s_share;
     const int lane = threadIdx.x & 31;
@@ -119,7 +128,10 @@ __global__ void contrib_long_rows_kernel(const LongRow *__restrict__ long_rows, 
                                          uint64_t V, double damping, const double *__restrict__ partial, int parts,
                                          double *__restrict__ out) {
     __shared__ double s_share;
-    if (threadIdx.x == 0) s_share = base_share(partial, parts, V, damping);
+    if (threadIdx.x < 32) {
+        const double sh = base_share(partial, parts, V, damping, threadIdx.x);
+        if (threadIdx.x == 0) s_share = sh;
+    }
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const uint64_t warps = uint64_t(gridDim.x) * (blockDim.x >> 5);
