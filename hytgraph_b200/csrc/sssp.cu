@@ -84,7 +84,7 @@ __global__ void __launch_bounds__(kSSThreads) sssp_expand_kernel(const SSArgs *_
         for (uint32_t c = 0; c < nch; ++c) a.hubs[base + c] = make_uint2(v, c);
     };
     for (uint32_t w = gwarp; uint64_t(w) * 32 < rv.qn; w += nwarps)
-        expand_warp<WK, HYB>(a, rv, w * 32, lane, kHubDegree, relaxed, improved, hub);
+        expand_warp<WK, HYB, HYB ? kEdgeBatch : 16>(a, rv, w * 32, lane, kHubDegree, relaxed, improved, hub);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) relaxed += __shfl_xor_sync(0xffffffffu, relaxed, o);
     if (lane == 0 && relaxed) atomicAdd(&a.hdr->relaxations, relaxed);

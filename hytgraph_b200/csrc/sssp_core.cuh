@@ -204,7 +204,10 @@ __device__ __forceinline__ void relax_batch(const SSArgs &a, const RoundView &rv
 // are handed to hub(v, chunks) as kHubChunk-edge tasks.  HYB: the edges of
 // a vertex's partition are reached through a.loc (out-of-HBM solves).
 // Must be called by all 32 lanes.
-template <int WK, bool HYB, class HubSink>
+// kB: 32-edge batches in flight.  The in-HBM solver's expansion takes 16;
+// the batch engine's and the out-of-HBM expansion keep kEdgeBatch (with 16
+// their kernels spill registers).
+template <int WK, bool HYB, int kB = kEdgeBatch, class HubSink>
 __device__ __forceinline__ void expand_warp(const SSArgs &a, const RoundView &rv, uint32_t i0, int lane,
                                             uint32_t hub_degree, unsigned long long &relaxed,
                                             unsigned long long &improved, HubSink &&hub) {
@@ -238,10 +241,10 @@ __device__ __forceinline__ void expand_warp(const SSArgs &a, const RoundView &rv
         if (lane >= o) incl += y;
     }
     const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-    for (uint32_t base = 0; base < total; base += 32 * kEdgeBatch) {
-        uint32_t u[kEdgeBatch], nd[kEdgeBatch], du[kEdgeBatch];
+    for (uint32_t base = 0; base < total; base += 32 * kB) {
+        uint32_t u[kB], nd[kB], du[kB];
 #pragma unroll
-        for (int k = 0; k < kEdgeBatch; ++k) {
+        for (int k = 0; k < kB; ++k) {
             const uint32_t j = base + 32 * k + lane;
             // owner = first lane whose inclusive prefix exceeds j
             uint32_t lo = 0;
@@ -270,8 +273,8 @@ __device__ __forceinline__ void expand_warp(const SSArgs &a, const RoundView &rv
             }
         }
 #pragma unroll
-        for (int k = 0; k < kEdgeBatch; ++k) du[k] = __ldcg(a.dist + u[k]);
-        relax_batch<kEdgeBatch>(a, rv, u, nd, du, lane, improved);
+        for (int k = 0; k < kB; ++k) du[k] = __ldcg(a.dist + u[k]);
+        relax_batch<kB>(a, rv, u, nd, du, lane, improved);
     }
 }
 
