@@ -161,6 +161,8 @@ struct GraphImpl {
     GraphArray<uint32_t> ppr_wide;         // packed PPR: rows of 32+ in-edges below the long-row threshold
     uint64_t ppr_wide_n = 0;
     bool ppr_wide_ready = false;
+    uint32_t min_in_weight = 0;            // smallest CSC weight (bit pattern, sign of -0.0 cleared)
+    bool min_in_weight_ready = false;
     GraphArray<uint32_t> ms_dist;          // multi-source labels [V][8]
     GraphArray<unsigned char> ms_state;
     PinnedArray<uint64_t> host_scratch;  // small pinned readback area

@@ -47,6 +47,7 @@
 #include "common.cuh"
 #include "graph.cuh"
 #include "host_checks.hpp"
+#include "scratch.cuh"
 #include "hybrid.cuh"
 #include "solvers.cuh"
 #include "sssp_core.cuh"
@@ -169,52 +170,57 @@ __device__ __forceinline__ bool pull_relax(const SSArgs &a, const RoundView &rv,
 #endif
 constexpr int kPullBatch = HYT_PULL_BATCH;
 
-// One pass of kK batches (edges lo + base + 32k + lane, k < kK).
-template <int kK, int WK, class Sink>
+// One pass of kK batches (edges lo + base + 32k + lane, k < kK).  With
+// kMask, edges whose bit is set in `skip` (bit i of word i / 32) belong to
+// skipped rows: they are neither read nor gathered.
+template <int kK, int WK, bool kMask, class Sink>
 __device__ __forceinline__ void pull_pass(const SSArgs &a, const PullGraph &pg, const uint32_t *s_hot, uint64_t lo,
-                                          uint32_t base, uint32_t n, uint64_t pol, int lane, Sink &sink) {
+                                          uint32_t base, uint32_t n, uint64_t pol, int lane, const uint32_t *skip,
+                                          Sink &sink) {
     // ids, then the label gathers, then the weights (streamed; issued after
     // the gathers so that ids and weights are not live together)
     uint32_t id[kK], w[kK], du[kK];
+    bool live[kK];
 #pragma unroll
     for (int k = 0; k < kK; ++k) {
         const uint32_t i = base + 32 * k + lane;
-        id[k] = (i < n) ? dev::ld_stream(pg.in_src + lo + i) : 0u;
+        live[k] = i < n && !(kMask && ((skip[(base >> 5) + k] >> lane) & 1u));
+        id[k] = live[k] ? dev::ld_stream(pg.in_src + lo + i) : 0u;
     }
 #pragma unroll
     for (int k = 0; k < kK; ++k)
         if (id[k] & kHotTag) id[k] = s_hot[id[k] & ~kHotTag];  // hot slot -> vertex id
 #pragma unroll
-    for (int k = 0; k < kK; ++k) du[k] = dev::ld_keep_u32(a.dist + id[k], pol);
+    for (int k = 0; k < kK; ++k) du[k] = (!kMask || live[k]) ? dev::ld_keep_u32(a.dist + id[k], pol) : a.inf;
 #pragma unroll
     for (int k = 0; k < kK; ++k) {
         const uint32_t i = base + 32 * k + lane;
-        w[k] = (i < n) ? edge_weight<WK>(pg.in_w, lo + i) : 0u;
+        w[k] = live[k] ? edge_weight<WK>(pg.in_w, lo + i) : 0u;
     }
 #pragma unroll
     for (int k = 0; k < kK; ++k) {
         const uint32_t i = base + 32 * k + lane;
-        if (i < n) sink(i, du[k] == a.inf ? a.inf : extend<WK>(du[k], w[k]));
+        if (live[k]) sink(i, du[k] == a.inf ? a.inf : extend<WK>(du[k], w[k]));
     }
 }
 
 // The last, partial pass issues only the 4-batch groups that hold edges
 // (a warp-uniform choice); the edges and their order are the same.
-template <int WK, class Sink>
+template <int WK, bool kMask, class Sink>
 __device__ __forceinline__ void pull_span(const SSArgs &a, const PullGraph &pg, const uint32_t *s_hot, uint64_t lo,
-                                          uint64_t hi, uint64_t pol, int lane, Sink &&sink) {
+                                          uint64_t hi, uint64_t pol, int lane, const uint32_t *skip, Sink &&sink) {
     static_assert(kPullBatch % 4 == 0 && kPullBatch >= 4, "batches come in groups of 4");
     const uint32_t n = static_cast<uint32_t>(hi - lo);
     for (uint32_t base = 0; base < n; base += 32 * kPullBatch) {
         const uint32_t groups = (n - base + 127) / 128;
         if (groups >= kPullBatch / 4)
-            pull_pass<kPullBatch, WK>(a, pg, s_hot, lo, base, n, pol, lane, sink);
+            pull_pass<kPullBatch, WK, kMask>(a, pg, s_hot, lo, base, n, pol, lane, skip, sink);
         else if (groups == 1)
-            pull_pass<4, WK>(a, pg, s_hot, lo, base, n, pol, lane, sink);
+            pull_pass<4, WK, kMask>(a, pg, s_hot, lo, base, n, pol, lane, skip, sink);
         else if (groups == 2)
-            pull_pass<8, WK>(a, pg, s_hot, lo, base, n, pol, lane, sink);
+            pull_pass<8, WK, kMask>(a, pg, s_hot, lo, base, n, pol, lane, skip, sink);
         else
-            pull_pass<(kPullBatch >= 12 ? 12 : kPullBatch), WK>(a, pg, s_hot, lo, base, n, pol, lane, sink);
+            pull_pass<(kPullBatch >= 12 ? 12 : kPullBatch), WK, kMask>(a, pg, s_hot, lo, base, n, pol, lane, skip, sink);
     }
 }
 
@@ -222,6 +228,33 @@ __device__ __forceinline__ void pull_span(const SSArgs &a, const PullGraph &pg, 
 #define HYT_PULL_THREADS 1024
 #endif
 constexpr int kPullThreads = HYT_PULL_THREADS;  // one CTA per SM, like the PageRank kernel
+
+// Words of a warp's edge mask: one bit per edge of a tile (< 2 * tile_cost).
+__host__ __device__ constexpr uint32_t skip_words(uint32_t tile_cost) { return (2 * tile_cost + 31) / 32; }
+
+// Row skipping.  Let F be this round's frontier (every vertex whose label
+// dropped since its out-edges were last relaxed) and fmin its lowest label.
+// An in-edge (u, v) can lower d[v] this round only if u is in F, and then
+// its candidate is d[u] + w >= fmin + min_w.  So a row with
+// d[v] <= extend(fmin, min_w) cannot improve: its in-edges are neither
+// read nor gathered.  A vertex lowered during the round joins the next
+// frontier, so the argument holds again next round; distances are
+// unchanged.
+template <int WK>
+__device__ __forceinline__ uint32_t skip_bound(const SSArgs &a, bool &on) {
+    const uint32_t fmin = *(volatile const uint32_t *)&a.hdr->fmin;
+    on = a.skip_rows && fmin < a.inf;
+    return on ? extend<WK>(fmin, a.min_w) : 0u;
+}
+
+// Sets bits [lo, hi) of a warp's edge mask (shared-memory words).
+__device__ __forceinline__ void mask_range(uint32_t *mw, uint32_t lo, uint32_t hi) {
+    for (uint32_t x = lo; x < hi;) {
+        const uint32_t b = x & 31, cnt = min(32u - b, hi - x);
+        atomicOr(mw + (x >> 5), (cnt == 32 ? 0xFFFFFFFFu : ((1u << cnt) - 1u)) << b);
+        x += cnt;
+    }
+}
 
 template <int WK>
 __global__ void __launch_bounds__(kPullThreads, 1) sssp_pull_kernel(const SSArgs *__restrict__ args, PullGraph pg) {
@@ -235,10 +268,15 @@ __global__ void __launch_bounds__(kPullThreads, 1) sssp_pull_kernel(const SSArgs
     for (uint32_t i = threadIdx.x; i < pg.num_hot; i += blockDim.x) s_hot[i] = pg.hot_vertex[i];
     __syncthreads();
     uint32_t *sv = s_dyn_u + pg.num_hot + warp * (2 * pg.tile_cost + 8);
+    const uint32_t mwords = skip_words(pg.tile_cost);
+    uint32_t *mw = s_dyn_u + pg.num_hot + (kPullThreads / 32) * (2 * pg.tile_cost + 8) + warp * mwords;
     const uint64_t pol = dev::policy_evict_last();
     const uint64_t total = pg.num_chunks + pg.num_tiles;
     const uint64_t nwarps = uint64_t(gridDim.x) * (kPullThreads / 32);
     const uint32_t *pf_w = (WK == HYT_WEIGHTS_NONE) ? nullptr : pg.in_w;
+    bool skip_on;
+    const uint32_t skip_at = skip_bound<WK>(a, skip_on);
+    unsigned long long relaxed = 0;  // in-edges this lane's warp relaxed (lane 0 counts tiles and chunks)
     for (uint64_t task = uint64_t(blockIdx.x) * (kPullThreads / 32) + warp; task < total; task += nwarps) {
         // the next task's descriptor now; its edge lines are warmed in L2
         // once this task's gathers are issued
@@ -251,8 +289,11 @@ __global__ void __launch_bounds__(kPullThreads, 1) sssp_pull_kernel(const SSArgs
             const uint64_t rb = pg.in_off[L.row], re = pg.in_off[L.row + 1];
             const uint64_t lo = rb + uint64_t(t.y) * kLongChunk;
             const uint64_t hi = (lo + kLongChunk < re) ? lo + kLongChunk : re;
+            if (skip_on && __shfl_sync(0xffffffffu, __ldcg(a.dist + L.row), 0) <= skip_at) continue;
+            if (lane == 0) relaxed += hi - lo;
             uint32_t best = a.inf;
-            pull_span<WK>(a, pg, s_hot, lo, hi, pol, lane, [&](uint32_t, uint32_t c) { best = min(best, c); });
+            pull_span<WK, false>(a, pg, s_hot, lo, hi, pol, lane, nullptr,
+                                 [&](uint32_t, uint32_t c) { best = min(best, c); });
             prefetch_task(nd, pg.in_src, pf_w, lane);
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(0xffffffffu, best, o));
@@ -274,7 +315,37 @@ __global__ void __launch_bounds__(kPullThreads, 1) sssp_pull_kernel(const SSArgs
                 hi_p = static_cast<uint32_t>(pg.in_off[r0 + lane + 1] - e0);
                 seen_p = __ldcg(a.dist + r0 + lane);
             }
-            pull_span<WK>(a, pg, s_hot, e0, e1, pol, lane, [&](uint32_t i, uint32_t c) { sv[i] = c; });
+            if (lane == 0) relaxed += e1 - e0;
+            // rows that cannot improve: their edges' bits in the warp's mask
+            const uint32_t *skip = nullptr;
+            if (skip_on) {
+                const uint32_t words = static_cast<uint32_t>((e1 - e0 + 31) >> 5);
+                for (uint32_t x = lane; x < words; x += 32) mw[x] = 0u;
+                __syncwarp();
+                uint32_t any = 0;
+                for (uint32_t rb = r0; rb < rl; rb += 32) {
+                    const uint32_t r = rb + lane;
+                    uint32_t lo = lo_p, hi = hi_p, seen = seen_p;
+                    if (rb != r0 && r < rl) {
+                        lo = static_cast<uint32_t>(pg.in_off[r] - e0);
+                        hi = static_cast<uint32_t>(pg.in_off[r + 1] - e0);
+                        seen = __ldcg(a.dist + r);
+                    }
+                    const bool sk = r < rl && seen <= skip_at;
+                    any |= __ballot_sync(0xffffffffu, sk);
+                    if (sk) {
+                        relaxed -= hi - lo;
+                        mask_range(mw, lo, hi);
+                    }
+                }
+                __syncwarp();
+                if (any) skip = mw;
+            }
+            if (skip)
+                pull_span<WK, true>(a, pg, s_hot, e0, e1, pol, lane, skip, [&](uint32_t i, uint32_t c) { sv[i] = c; });
+            else
+                pull_span<WK, false>(a, pg, s_hot, e0, e1, pol, lane, nullptr,
+                                     [&](uint32_t i, uint32_t c) { sv[i] = c; });
             prefetch_task(nd, pg.in_src, pf_w, lane);
             __syncwarp();
             for (uint32_t rb = r0; rb < rl; rb += 32) {
@@ -287,12 +358,13 @@ __global__ void __launch_bounds__(kPullThreads, 1) sssp_pull_kernel(const SSArgs
                     seen = active ? __ldcg(a.dist + r) : 0u;
                 }
                 bool joined = false;
-                if (active && hi - lo < 64) {
+                const bool live = active && !(skip && seen <= skip_at);  // skipped rows were not gathered
+                if (live && hi - lo < 64) {
                     uint32_t best = a.inf;
                     for (uint32_t x = lo; x < hi; ++x) best = min(best, sv[x]);
                     joined = pull_store(a, rv, r, best, seen);
                 }
-                uint32_t big = __ballot_sync(0xffffffffu, active && (hi - lo >= 64));
+                uint32_t big = __ballot_sync(0xffffffffu, live && (hi - lo >= 64));
                 while (big) {
                     const int src = __ffs(big) - 1;
                     big &= big - 1;
@@ -312,10 +384,10 @@ __global__ void __launch_bounds__(kPullThreads, 1) sssp_pull_kernel(const SSArgs
             __syncwarp();
         }
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        atomicAdd(&a.hdr->relaxations, static_cast<unsigned long long>(a.num_edges));
-        atomicAdd(&a.hdr->pull_rounds, 1u);
-    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) relaxed += __shfl_xor_sync(0xffffffffu, relaxed, o);
+    if (lane == 0 && relaxed) atomicAdd(&a.hdr->relaxations, relaxed);
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&a.hdr->pull_rounds, 1u);
 }
 
 // ---- staged pull sweeps (CSC in HBM; pipeline in stage.cuh) ----------------
@@ -448,7 +520,8 @@ __global__ void __launch_bounds__(stage::kStageThreads, 1) sssp_pull_staged_kern
 
 // End of a round of a pull-capable solve, in one grid launch: the whole
 // grid sums the out-edges of the next frontier (the next round's push /
-// pull decision), then the last block to finish runs the round-end logic.
+// pull decision) and, with row skipping, finds its lowest label; then the
+// last block to finish runs the round-end logic.
 __global__ void __launch_bounds__(kSSThreads) sssp_round_close_kernel(const SSArgs *__restrict__ args) {
     const SSArgs a = *args;
     SSHeader *h = a.hdr;
@@ -457,13 +530,19 @@ __global__ void __launch_bounds__(kSSThreads) sssp_round_close_kernel(const SSAr
     const uint32_t qn = *(volatile uint32_t *)&h->qsize[(r + 1) & 1];
     const uint32_t *q = ((r + 1) & 1) ? a.queue[1] : a.queue[0];
     unsigned long long sum = 0;
+    uint32_t low = 0xFFFFFFFFu;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < qn; i += gridDim.x * blockDim.x) {
         const uint32_t v = q[i];
         sum += a.row_off[v + 1] - a.row_off[v];
+        if (a.skip_rows) low = min(low, __ldcg(a.dist + v));
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
     if ((threadIdx.x & 31) == 0 && sum) atomicAdd(&h->frontier_edges_next, sum);
+    if (a.skip_rows) {
+        low = __reduce_min_sync(0xffffffffu, low);
+        if ((threadIdx.x & 31) == 0 && low != 0xFFFFFFFFu) atomicMax(&h->fmin_inv, ~low);
+    }
     __shared__ uint32_t s_last;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -476,6 +555,8 @@ __global__ void __launch_bounds__(kSSThreads) sssp_round_close_kernel(const SSAr
     const unsigned long long fe = atomicAdd(&h->frontier_edges_next, 0ull);
     h->frontier_edges_next = 0;
     h->close_ticket = 0;
+    h->fmin = ~atomicAdd(&h->fmin_inv, 0u);  // all ones when the next frontier is empty
+    h->fmin_inv = 0;
     const bool finish = round_end(h);
     h->frontier_edges = fe;
     if (finish && a.use_cond) cudaGraphSetConditional(a.cond, 0);
@@ -603,6 +684,45 @@ __global__ void __launch_bounds__(kSSThreads) sssp_expand_packed_kernel(const SS
     if (lane == 0 && relaxed) atomicAdd(&a.hdr->relaxations, relaxed);
 }
 
+// Row skipping in pull sweeps (env HYT_SSSP_PULL_SKIP, 0 = off; default on).
+bool sssp_pull_skip() {
+    static bool on = [] {
+        const char *e = std::getenv("HYT_SSSP_PULL_SKIP");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
+// Smallest of n weights (bit patterns of u32 or non-negative f32 weights;
+// -0.0 counts as 0) into *out, which starts at all ones.
+__global__ void min_weight_kernel(const uint32_t *__restrict__ w, uint64_t n, uint32_t f32, uint32_t *out) {
+    uint32_t m = 0xFFFFFFFFu;
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
+        const uint32_t x = __ldcs(w + i);
+        m = min(m, f32 ? (x & 0x7FFFFFFFu) : x);
+    }
+    m = __reduce_min_sync(0xffffffffu, m);
+    if ((threadIdx.x & 31) == 0) atomicMin(out, m);
+}
+
+// The graph's smallest CSC weight, found once per graph.
+uint32_t graph_min_in_weight(GraphImpl &g, bool f32, cudaStream_t s) {
+    if (!g.min_in_weight_ready) {
+        Scratch<uint32_t> m(1, s);
+        HYT_CUDA(cudaMemsetAsync(m.get(), 0xFF, sizeof(uint32_t), s));
+        min_weight_kernel<<<grid_for(g.E, 256, 148 * 8), 256, 0, s>>>(g.in_weights.get(), g.E, f32 ? 1u : 0u,
+                                                                       m.get());
+        HYT_CUDA(cudaGetLastError());
+        uint32_t local = 0;
+        uint32_t *h = g.host_scratch.ptr ? reinterpret_cast<uint32_t *>(g.host_scratch.ptr) : &local;
+        HYT_CUDA(cudaMemcpyAsync(h, m.get(), sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        HYT_CUDA(cudaStreamSynchronize(s));
+        g.min_in_weight = *h;
+        g.min_in_weight_ready = true;
+    }
+    return g.min_in_weight;
+}
+
 // Pull sweeps when the frontier's out-edges exceed E / div (env
 // HYT_SSSP_PULL_DIV, 0 = never; default 4: a sweep reads every in-edge once,
 // which costs about what pushing a quarter of them does).
@@ -706,9 +826,16 @@ void sssp_solve(GraphImpl &g, uint32_t source, uint32_t delta, uint32_t max_roun
         pg.num_hot = g.num_hot;
     }
     const bool staged = a.pull_div && pull_use_staged(g);
+    // row skipping (register-path sweeps): the smallest edge weight bounds
+    // what any in-edge adds
+    if (a.pull_div && !staged && sssp_pull_skip()) {
+        a.skip_rows = 1;
+        a.min_w = (WK == HYT_WEIGHTS_NONE) ? 1u : graph_min_in_weight(g, WK == HYT_WEIGHTS_F32, s);
+    }
     const unsigned pull_smem =
         staged ? static_cast<unsigned>(stage::staged_shared_bytes(g.num_hot))
-               : static_cast<unsigned>((g.num_hot + kPullThreads / 32 * (2 * size_t(g.tile_cost) + 8)) * 4);
+               : static_cast<unsigned>((g.num_hot + kPullThreads / 32 * (2 * size_t(g.tile_cost) + 8 +
+                                                                         skip_words(g.tile_cost))) * 4);
     const int pgrid = a.pull_div ? pull_grid<WK>(staged, pull_smem) : 0;
     const void *pull_fn = staged ? reinterpret_cast<const void *>(sssp_pull_staged_kernel<WK>)
                                  : reinterpret_cast<const void *>(sssp_pull_kernel<WK>);

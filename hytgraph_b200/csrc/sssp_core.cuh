@@ -52,6 +52,8 @@ struct SSHeader {
     uint32_t error;                     // 1: a bounded wait for a staged copy ran out
     unsigned long long frontier_edges_next;  // out-edges of the next frontier, summed at round close
     uint32_t close_ticket;                   // blocks of the round-close kernel finished
+    uint32_t fmin;      // lowest label in this round's frontier (pull-capable solves with row skipping)
+    uint32_t fmin_inv;  // ~(lowest label) of the next frontier, gathered at round close
     uint32_t pad;
 };
 
@@ -75,6 +77,8 @@ struct SSArgs {
     uint32_t part_shift;  // partition of vertex v = v >> part_shift
     uint32_t pull_div;    // > 0: a round whose frontier has more than E / pull_div out-edges is a pull sweep
     uint64_t num_edges;
+    uint32_t skip_rows;   // 1: pull sweeps skip rows whose label no in-edge can lower (needs fmin)
+    uint32_t min_w;       // smallest edge weight (bit pattern; 1 when unweighted)
 };
 
 // True when this round runs as a pull sweep over the CSC instead of a push
