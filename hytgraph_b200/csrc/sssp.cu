@@ -229,9 +229,6 @@ __device__ __forceinline__ void pull_span(const SSArgs &a, const PullGraph &pg, 
 #endif
 constexpr int kPullThreads = HYT_PULL_THREADS;  // one CTA per SM, like the PageRank kernel
 
-// Words of a warp's edge mask: one bit per edge of a tile (< 2 * tile_cost).
-__host__ __device__ constexpr uint32_t skip_words(uint32_t tile_cost) { return (2 * tile_cost + 31) / 32; }
-
 // Row skipping.  Let F be this round's frontier (every vertex whose label
 // dropped since its out-edges were last relaxed) and fmin its lowest label.
 // An in-edge (u, v) can lower d[v] this round only if u is in F, and then
@@ -268,8 +265,6 @@ __global__ void __launch_bounds__(kPullThreads, 1) sssp_pull_kernel(const SSArgs
     for (uint32_t i = threadIdx.x; i < pg.num_hot; i += blockDim.x) s_hot[i] = pg.hot_vertex[i];
     __syncthreads();
     uint32_t *sv = s_dyn_u + pg.num_hot + warp * (2 * pg.tile_cost + 8);
-    const uint32_t mwords = skip_words(pg.tile_cost);
-    uint32_t *mw = s_dyn_u + pg.num_hot + (kPullThreads / 32) * (2 * pg.tile_cost + 8) + warp * mwords;
     const uint64_t pol = dev::policy_evict_last();
     const uint64_t total = pg.num_chunks + pg.num_tiles;
     const uint64_t nwarps = uint64_t(gridDim.x) * (kPullThreads / 32);
@@ -316,10 +311,13 @@ __global__ void __launch_bounds__(kPullThreads, 1) sssp_pull_kernel(const SSArgs
                 seen_p = __ldcg(a.dist + r0 + lane);
             }
             if (lane == 0) relaxed += e1 - e0;
-            // rows that cannot improve: their edges' bits in the warp's mask
+            // rows that cannot improve: their edges' bits in a mask kept at
+            // the end of the warp's slice, past the tile's candidates (no
+            // shared memory beyond the slice: more would shrink L1)
             const uint32_t *skip = nullptr;
-            if (skip_on) {
-                const uint32_t words = static_cast<uint32_t>((e1 - e0 + 31) >> 5);
+            const uint32_t words = static_cast<uint32_t>((e1 - e0 + 31) >> 5);
+            if (skip_on && (e1 - e0) + words <= 2 * pg.tile_cost + 8) {
+                uint32_t *mw = sv + (2 * pg.tile_cost + 8) - words;
                 for (uint32_t x = lane; x < words; x += 32) mw[x] = 0u;
                 __syncwarp();
                 uint32_t any = 0;
@@ -834,8 +832,7 @@ void sssp_solve(GraphImpl &g, uint32_t source, uint32_t delta, uint32_t max_roun
     }
     const unsigned pull_smem =
         staged ? static_cast<unsigned>(stage::staged_shared_bytes(g.num_hot))
-               : static_cast<unsigned>((g.num_hot + kPullThreads / 32 * (2 * size_t(g.tile_cost) + 8 +
-                                                                         skip_words(g.tile_cost))) * 4);
+               : static_cast<unsigned>((g.num_hot + kPullThreads / 32 * (2 * size_t(g.tile_cost) + 8)) * 4);
     const int pgrid = a.pull_div ? pull_grid<WK>(staged, pull_smem) : 0;
     const void *pull_fn = staged ? reinterpret_cast<const void *>(sssp_pull_staged_kernel<WK>)
                                  : reinterpret_cast<const void *>(sssp_pull_kernel<WK>);
