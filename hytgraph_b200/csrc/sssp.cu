@@ -30,7 +30,10 @@
 // With one bucket and a CSC, a round whose frontier carries more than
 // E / pull_div out-edges runs as a pull sweep over the CSC instead
 // (sssp_pull_kernel: 512-unit tiles, labels gathered 8 per lane in flight,
-// tile rows written with plain stores).  All round state lives on the
+// tile rows written with plain stores).  A sweep skips the rows whose label
+// is at most (lowest frontier label + smallest weight): no in-edge can
+// lower them, so their in-edges are neither read nor gathered (the round
+// close finds the frontier's lowest label).  All round state lives on the
 // device; inside a CUDA graph the rounds run as a conditional while-loop
 // (expand, hub chunks, pull sweep, round close), instantiated once per
 // graph and launched again by later solves.
